@@ -1,0 +1,155 @@
+"""Seeded synthetic liquid scenes.
+
+The reference seeds liquid from signed-distance "source" fields with jittered
+resampling that draws ``rand()`` inside TBB loops
+(libWetCloth/Core/DistanceFields.cpp:157-240), so its particle sets are not
+reproducible.  These generators replace it with numpy ``default_rng`` streams;
+per-particle attributes follow ``TwoDScene::sampleLiquidDistanceFields``
+(libWetCloth/Core/TwoDScene.cpp:5564-5605): radius r, volume 4/3*pi*r^3,
+mass rho*volume, zero affine matrix.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+
+@dataclasses.dataclass
+class SceneParams:
+    """Scene-wide parameters of the fluid step (the liquid subset of
+    ``LiquidInfo``, libWetCloth/Core/TwoDScene.h:35-91, plus bucket info and the
+    solid box walls)."""
+
+    dx: float = 1.0 / 64.0
+    gravity: tuple = (0.0, -9.81, 0.0)
+    liquid_density: float = 1000.0
+    flip_coeff: float = 0.99
+    liquid_boundary_friction: float = 0.0
+    box_center: tuple = (0.5, 0.5, 0.5)
+    box_half: tuple = (0.5, 0.5, 0.5)
+    box_radius: float = 0.0
+    criterion: float = 1e-6
+    maxiters: int = 1000
+
+
+def particle_radius(dx: float, ppc: int) -> float:
+    """Radius whose sphere volume is dx^3/ppc (one particle per 1/ppc of a
+    cell), i.e. particle_cell_multiplier * dx / sqrt(3) with the multiplier
+    chosen so that every particle is classified 'optimal' by the reference."""
+    return dx * (3.0 / (4.0 * math.pi * ppc)) ** (1.0 / 3.0)
+
+
+def attributes(n: int, dx: float, ppc: int, rho: float):
+    r = particle_radius(dx, ppc)
+    vol = 4.0 / 3.0 * math.pi * r * r * r
+    return (np.full(n, rho * vol), np.full(n, vol), np.full(n, r))
+
+
+def liquid_block(dx: float, lo, hi, ppc: int, seed: int) -> np.ndarray:
+    """Jittered particles filling the box [lo, hi].
+
+    ppc == 8: one particle per (dx/2)^3 sub-cell whose centre lies in the box,
+    uniformly jittered inside its sub-cell.  Other ppc: ppc particles per cell
+    whose centre lies in the box, uniform inside the cell.
+    """
+    rng = np.random.default_rng(seed)
+    lo = np.asarray(lo, dtype=np.float64)
+    hi = np.asarray(hi, dtype=np.float64)
+    if ppc == 8:
+        h = dx * 0.5
+        per = 1
+    else:
+        h = dx
+        per = ppc
+    i0 = np.floor(lo / h).astype(np.int64)
+    i1 = np.ceil(hi / h).astype(np.int64)
+    axes = [np.arange(i0[d], i1[d]) for d in range(3)]
+    cz, cy, cx = np.meshgrid(axes[2], axes[1], axes[0], indexing="ij")
+    cells = np.stack([cx.ravel(), cy.ravel(), cz.ravel()], axis=1)
+    centre = (cells + 0.5) * h
+    keep = np.all((centre >= lo) & (centre <= hi), axis=1)
+    cells = cells[keep]
+    cells = np.repeat(cells, per, axis=0)
+    jitter = rng.random((cells.shape[0], 3))
+    return (cells + jitter) * h
+
+
+def curl_noise_velocity(x: np.ndarray, n: int, sigma_cells: float,
+                        amplitude: float, seed: int) -> np.ndarray:
+    """Divergence-free velocity: curl of Gaussian-smoothed white noise on an
+    n^3 grid over the unit box (sigma in cells), scaled so that max |v| equals
+    ``amplitude`` on the grid, trilinearly interpolated to ``x``."""
+    rng = np.random.default_rng(seed)
+    k = np.fft.fftfreq(n) * 2.0 * math.pi
+    kx, ky, kz = np.meshgrid(k, k, k, indexing="ij")
+    g = np.exp(-0.5 * (sigma_cells ** 2) * (kx * kx + ky * ky + kz * kz))
+    psi = []
+    for _ in range(3):
+        w = rng.standard_normal((n, n, n))
+        psi.append(np.real(np.fft.ifftn(np.fft.fftn(w) * g)))
+    h = 1.0 / n
+
+    def d(f, axis):
+        return (np.roll(f, -1, axis) - np.roll(f, 1, axis)) / (2.0 * h)
+
+    vx = d(psi[2], 1) - d(psi[1], 2)
+    vy = d(psi[0], 2) - d(psi[2], 0)
+    vz = d(psi[1], 0) - d(psi[0], 1)
+    vmax = float(np.sqrt(vx * vx + vy * vy + vz * vz).max())
+    s = amplitude / vmax
+    vel = np.stack([vx * s, vy * s, vz * s], axis=-1)
+    # trilinear interpolation at sample points (grid values at cell centres)
+    p = x / h - 0.5
+    i = np.floor(p).astype(np.int64)
+    f = p - i
+    out = np.zeros_like(x)
+    for dz in (0, 1):
+        for dy in (0, 1):
+            for dxx in (0, 1):
+                w = ((f[:, 0] if dxx else 1 - f[:, 0]) *
+                     (f[:, 1] if dy else 1 - f[:, 1]) *
+                     (f[:, 2] if dz else 1 - f[:, 2]))
+                ii = np.clip(i[:, 0] + dxx, 0, n - 1)
+                jj = np.clip(i[:, 1] + dy, 0, n - 1)
+                kk = np.clip(i[:, 2] + dz, 0, n - 1)
+                out += w[:, None] * vel[ii, jj, kk]
+    return out
+
+
+@dataclasses.dataclass
+class Scene:
+    params: SceneParams
+    x: np.ndarray
+    v: np.ndarray
+    mass: np.ndarray
+    vol: np.ndarray
+    radius: np.ndarray
+    C: np.ndarray | None = None
+    name: str = ""
+
+
+def dam_break(n_cells: int = 64, ppc: int = 8, seed: int = 0,
+              block_hi=(0.4, 0.8, 0.4)) -> Scene:
+    """Liquid dam break in the unit box: block [0, block_hi] at ppc particles
+    per cell, zero initial velocity, rho 1000, g -9.81 y, free-slip walls."""
+    dx = 1.0 / n_cells
+    prm = SceneParams(dx=dx)
+    x = liquid_block(dx, (0.0, 0.0, 0.0), block_hi, ppc, seed)
+    m, vol, r = attributes(x.shape[0], dx, ppc, prm.liquid_density)
+    return Scene(prm, x, np.zeros_like(x), m, vol, r,
+                 name=f"dam_break_{n_cells}^3_{ppc}ppc")
+
+
+def half_box(n_cells: int = 256, ppc: int = 2, seed: int = 1,
+             amplitude: float = 0.5, sigma_cells: float = 4.0) -> Scene:
+    """Half-filled unit box (y < 0.5) at ppc particles per cell with a random
+    divergence-free initial velocity (curl of Gaussian noise)."""
+    dx = 1.0 / n_cells
+    prm = SceneParams(dx=dx)
+    x = liquid_block(dx, (0.0, 0.0, 0.0), (1.0, 0.5, 1.0), ppc, seed)
+    v = curl_noise_velocity(x, n_cells, sigma_cells, amplitude, seed)
+    m, vol, r = attributes(x.shape[0], dx, ppc, prm.liquid_density)
+    return Scene(prm, x, v, m, vol, r,
+                 name=f"half_box_{n_cells}^3_{ppc}ppc")

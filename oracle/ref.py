@@ -1,0 +1,113 @@
+"""ctypes binding of oracle/_ref/libwcref*.so (the reference Core + harness).
+
+TEST INFRASTRUCTURE ONLY (checker and timed CPU baseline).  Built by
+``make -f oracle/ref.mk``; see oracle/ref_harness.cpp for what each call runs.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_D = ctypes.POINTER(ctypes.c_double)
+_L = ctypes.POINTER(ctypes.c_longlong)
+
+
+def lib_path(omp: bool = False) -> str:
+    return os.path.join(HERE, "_ref", "libwcref_omp.so" if omp else "libwcref.so")
+
+
+def available(omp: bool = False) -> bool:
+    return os.path.exists(lib_path(omp))
+
+
+_libs = {}
+
+
+def _lib(omp: bool):
+    if omp not in _libs:
+        L = ctypes.CDLL(lib_path(omp))
+        L.wcref_create.restype = ctypes.c_void_p
+        L.wcref_create.argtypes = [ctypes.c_double, _D, ctypes.c_double,
+                                   ctypes.c_double, ctypes.c_double, _D, _D,
+                                   ctypes.c_double, ctypes.c_double,
+                                   ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                   _D, _D, _D, _D, _D, _D]
+        L.wcref_destroy.argtypes = [ctypes.c_void_p]
+        L.wcref_step.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
+        L.wcref_step.restype = ctypes.c_int
+        L.wcref_substep.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
+        L.wcref_num_substeps.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        L.wcref_size.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+        L.wcref_size.restype = ctypes.c_longlong
+        L.wcref_get_f.argtypes = [ctypes.c_void_p, ctypes.c_char_p, _D]
+        L.wcref_get_i.argtypes = [ctypes.c_void_p, ctypes.c_char_p, _L]
+        L.wcref_solver_stats.argtypes = [ctypes.c_void_p,
+                                         ctypes.POINTER(ctypes.c_int), _D]
+        L.wcref_timers.argtypes = [ctypes.c_void_p, _D]
+        _libs[omp] = L
+    return _libs[omp]
+
+
+def _dp(a):
+    return a.ctypes.data_as(_D)
+
+
+class RefScene:
+    """One reference TwoDScene + LinearizedImplicitEuler, liquid only."""
+
+    def __init__(self, scene, mic: bool = True, omp: bool = False):
+        self.L = _lib(omp)
+        p = scene.params
+        self._keep = []
+
+        def arr(a, n=None):
+            a = np.ascontiguousarray(a, dtype=np.float64)
+            self._keep.append(a)
+            return _dp(a)
+
+        C = None if scene.C is None else arr(scene.C.reshape(-1))
+        self.h = self.L.wcref_create(
+            p.dx, arr(p.gravity), p.liquid_density, p.flip_coeff,
+            p.liquid_boundary_friction, arr(p.box_center), arr(p.box_half),
+            p.box_radius, p.criterion, p.maxiters, 1 if mic else 0,
+            scene.x.shape[0], arr(scene.x.reshape(-1)), arr(scene.v.reshape(-1)),
+            C, arr(scene.mass), arr(scene.vol), arr(scene.radius))
+
+    def close(self):
+        if self.h:
+            self.L.wcref_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, dt: float, snapshot: bool = True) -> int:
+        return self.L.wcref_step(self.h, dt, 1 if snapshot else 0)
+
+    def get(self, name: str) -> np.ndarray:
+        n = self.L.wcref_size(self.h, name.encode())
+        if n < 0:
+            raise KeyError(name)
+        out = np.empty(n, dtype=np.float64)
+        if self.L.wcref_get_f(self.h, name.encode(), _dp(out)) == 0:
+            return out
+        out = np.empty(n, dtype=np.int64)
+        self.L.wcref_get_i(self.h, name.encode(), out.ctypes.data_as(_L))
+        return out
+
+    def solver_stats(self):
+        it = ctypes.c_int(0)
+        res = ctypes.c_double(0)
+        self.L.wcref_solver_stats(self.h, ctypes.byref(it), ctypes.byref(res))
+        return it.value, res.value
+
+    def timers(self) -> np.ndarray:
+        out = np.zeros(12)
+        self.L.wcref_timers(self.h, _dp(out))
+        return out

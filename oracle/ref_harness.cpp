@@ -1,0 +1,577 @@
+// Harness around the libWetCloth reference Core (compiled from the reference
+// sources by oracle/ref.mk).  TEST INFRASTRUCTURE ONLY: it is the checker that
+// pins the C restatement (oracle/wc_oracle.c) and the timed CPU baseline; no
+// product code links it.
+//
+// It builds a liquid-only TwoDScene programmatically (the XML parser TU needs
+// GL headers), replays the fluid hot path in WetClothCore::stepSystem order
+// (libWetCloth/Core/WetClothCore.cpp:115-258, minus the particle maintenance,
+// elasto and surface-tension calls which are no-ops or out of scope for a
+// liquid scene) and snapshots every hot-path field into dense bucket-major
+// arrays (bucket index * 64 + local node index, libWetCloth/Core/Sorter.h:63,
+// TwoDScene.cpp:3746) that Python reads through ctypes.
+//
+// Scene set-up follows TwoDScene::sampleLiquidDistanceFields
+// (Core/TwoDScene.cpp:5564-5605) for the per-particle attributes and
+// TwoDSceneXMLParser::loadLiquidInfo (App/TwoDSceneXMLParser.cpp:1851-1904) for
+// the LiquidInfo defaults.  Walls are one DistanceFieldObject of type DFT_BOX,
+// usage DFU_SOLID, inside=true (Core/DistanceFields.cpp:478-516).
+//
+// Pressure: the reference's default solver is the multigrid PCG
+// (Core/Pressure.cpp:797).  With mic=1 the harness re-solves the very matrix
+// and rhs that solveNodePressure assembled with the reference's own
+// robertbridson::PCGSolver<double> (MIC(0), omega 0.97, min ratio 0.25,
+// Core/PCGSolver/PCGSolver.h:245-330) and scatters that solution into the
+// scene's pressure field, so the rest of the step uses the MIC(0) pressures.
+// Standard-library and Eigen headers first, so the access override below only
+// reaches the reference's own classes.
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <fstream>
+#include <functional>
+#include <iostream>
+#include <limits>
+#include <list>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <set>
+#include <sstream>
+#include <stack>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <unordered_set>
+#include <vector>
+#include "MathDefs.h"
+#include <Eigen/Geometry>
+#define private public
+#define protected public
+#include "LinearizedImplicitEuler.h"
+#include "PCGSolver/PCGSolver.h"
+#include "SimpleGravityForce.h"
+#include "TwoDScene.h"
+#include "DistanceFields.h"
+#undef private
+#undef protected
+
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+namespace {
+
+struct Params {
+  double dx;
+  double gravity[3];
+  double liquid_density;
+  double flip_coeff;
+  double liquid_boundary_friction;
+  double box_center[3];
+  double box_half[3];
+  double box_radius;
+  double criterion;
+  int maxiters;
+  int mic;
+};
+
+struct Harness {
+  std::shared_ptr<TwoDScene> scene;
+  std::shared_ptr<LinearizedImplicitEuler> stepper;
+  Params p;
+  std::map<std::string, std::vector<double>> f;    // dense double snapshots
+  std::map<std::string, std::vector<long long>> ii;  // integer snapshots
+  double timers[12];
+  int last_iters_amg = 0, last_iters_mic = 0;
+  double last_res_amg = 0, last_res_mic = 0;
+};
+
+double now() {
+  return std::chrono::duration<double>(
+             std::chrono::steady_clock::now().time_since_epoch())
+      .count();
+}
+
+// dense copy of a per-bucket node field; inactive buckets are NaN
+void dense(Harness& h, const std::string& name,
+           const std::vector<VectorXs>& v, int per_node = 1) {
+  const int nb = h.scene->getNumBuckets();
+  const int nn = h.scene->getDefaultNumNodes();
+  const int count = nn * nn * nn;
+  std::vector<double>& out = h.f[name];
+  out.assign((size_t)nb * count * per_node,
+             std::numeric_limits<double>::quiet_NaN());
+  for (int b = 0; b < nb && b < (int)v.size(); ++b) {
+    if ((int)v[b].size() != count * per_node) continue;
+    for (int i = 0; i < count * per_node; ++i)
+      out[(size_t)b * count * per_node + i] = v[b][i];
+  }
+}
+
+void dense_uc(Harness& h, const std::string& name,
+              const std::vector<VectorXuc>& v) {
+  const int nb = h.scene->getNumBuckets();
+  const int count = 64;
+  std::vector<long long>& out = h.ii[name];
+  out.assign((size_t)nb * count, -1);
+  for (int b = 0; b < nb && b < (int)v.size(); ++b) {
+    if ((int)v[b].size() != count) continue;
+    for (int i = 0; i < count; ++i) out[(size_t)b * count + i] = v[b][i];
+  }
+}
+
+void dense_vi(Harness& h, const std::string& name,
+              const std::vector<VectorXi>& v) {
+  const int nb = h.scene->getNumBuckets();
+  const int count = 64;
+  std::vector<long long>& out = h.ii[name];
+  out.assign((size_t)nb * count, -2);
+  for (int b = 0; b < nb && b < (int)v.size(); ++b) {
+    if ((int)v[b].size() != count) continue;
+    for (int i = 0; i < count; ++i) out[(size_t)b * count + i] = v[b][i];
+  }
+}
+
+void snap_particles(Harness& h, const std::string& tag) {
+  TwoDScene& s = *h.scene;
+  const int np = s.getNumParticles();
+  std::vector<double>& x = h.f[tag + "x"];
+  std::vector<double>& v = h.f[tag + "v"];
+  std::vector<double>& c = h.f[tag + "C"];
+  x.resize((size_t)np * 3);
+  v.resize((size_t)np * 3);
+  c.resize((size_t)np * 9);
+  for (int i = 0; i < np; ++i) {
+    for (int r = 0; r < 3; ++r) {
+      x[i * 3 + r] = s.m_x(i * 4 + r);
+      v[i * 3 + r] = s.m_fluid_v(i * 4 + r);
+      for (int q = 0; q < 3; ++q) c[i * 9 + r * 3 + q] = s.m_fB(i * 3 + r, q);
+    }
+  }
+}
+
+void snap_grid(Harness& h) {
+  TwoDScene& s = *h.scene;
+  const Sorter& b = s.m_particle_buckets;
+  h.f["grid_origin"] = {s.m_grid_mincorner(0), s.m_grid_mincorner(1),
+                        s.m_grid_mincorner(2)};
+  h.f["bbx"] = {s.m_bbx_min(0), s.m_bbx_min(1), s.m_bbx_min(2),
+                s.m_bbx_max(0), s.m_bbx_max(1), s.m_bbx_max(2)};
+  h.ii["grid_dims"] = {b.ni, b.nj, b.nk};
+  std::vector<long long>& keys = h.ii["array_idx"];
+  keys.assign(b.array_idx.begin(), b.array_idx.end());
+  std::vector<long long>& sup = h.ii["array_sup"];
+  sup.resize(b.array_sup.size() * 2);
+  for (size_t i = 0; i < b.array_sup.size(); ++i) {
+    sup[i * 2] = b.array_sup[i].first;
+    sup[i * 2 + 1] = b.array_sup[i].second;
+  }
+  std::vector<long long>& act = h.ii["active"];
+  act.assign(s.m_bucket_activated.begin(), s.m_bucket_activated.end());
+  // first stencil node of each particle per node kind, as global node ijk
+  const int np = s.getNumParticles();
+  const int nn = s.getDefaultNumNodes();
+  const std::vector<Matrix27x2i>* kinds[5] = {
+      &s.m_particle_nodes_x, &s.m_particle_nodes_y, &s.m_particle_nodes_z,
+      &s.m_particle_nodes_solid_phi, &s.m_particle_nodes_p};
+  std::vector<long long>& base = h.ii["stencil_base"];
+  base.resize((size_t)np * 15);
+  for (int pidx = 0; pidx < np; ++pidx)
+    for (int k = 0; k < 5; ++k) {
+      const Matrix27x2i& m = (*kinds[k])[pidx];
+      Vector3i bh = b.bucket_handle(m(0, 0));
+      Vector3i nh = s.getNodeHandle(m(0, 1));
+      for (int r = 0; r < 3; ++r)
+        base[(size_t)pidx * 15 + k * 3 + r] = (long long)bh(r) * nn + nh(r);
+    }
+  std::vector<long long>& inside = h.ii["inside"];
+  inside.assign(s.m_inside.data(), s.m_inside.data() + s.m_inside.size());
+}
+
+void snap_p2g(Harness& h) {
+  TwoDScene& s = *h.scene;
+  dense(h, "mass_fluid_x", s.m_node_mass_fluid_x);
+  dense(h, "mass_fluid_y", s.m_node_mass_fluid_y);
+  dense(h, "mass_fluid_z", s.m_node_mass_fluid_z);
+  dense(h, "vel_fluid_x", s.m_node_vel_fluid_x);
+  dense(h, "vel_fluid_y", s.m_node_vel_fluid_y);
+  dense(h, "vel_fluid_z", s.m_node_vel_fluid_z);
+  dense(h, "vol_fluid_x", s.m_node_vol_fluid_x);
+  dense(h, "vol_fluid_y", s.m_node_vol_fluid_y);
+  dense(h, "vol_fluid_z", s.m_node_vol_fluid_z);
+  dense(h, "mass_x", s.m_node_mass_x);
+  dense(h, "mass_y", s.m_node_mass_y);
+  dense(h, "mass_z", s.m_node_mass_z);
+  dense(h, "vol_x", s.m_node_vol_x);
+  dense(h, "vol_y", s.m_node_vol_y);
+  dense(h, "vol_z", s.m_node_vol_z);
+  dense(h, "psi_x", s.m_node_psi_x);
+  dense(h, "psi_y", s.m_node_psi_y);
+  dense(h, "psi_z", s.m_node_psi_z);
+  dense(h, "sat_x", s.m_node_sat_x);
+  dense(h, "sat_y", s.m_node_sat_y);
+  dense(h, "sat_z", s.m_node_sat_z);
+  dense(h, "sat_p", s.m_node_sat_p);
+  dense(h, "psi_p", s.m_node_psi_p);
+  dense(h, "pore_pressure_p", s.m_node_pore_pressure_p);
+  dense(h, "liquid_phi", s.m_node_liquid_phi);
+  dense(h, "solid_phi", s.m_node_solid_phi);
+  dense(h, "solid_weight_x", s.m_node_solid_weight_x);
+  dense(h, "solid_weight_y", s.m_node_solid_weight_y);
+  dense(h, "solid_weight_z", s.m_node_solid_weight_z);
+  dense(h, "solid_vel_x", s.m_node_solid_vel_x);
+  dense(h, "solid_vel_y", s.m_node_solid_vel_y);
+  dense(h, "solid_vel_z", s.m_node_solid_vel_z);
+}
+
+void snap_predict(Harness& h) {
+  LinearizedImplicitEuler& e = *h.stepper;
+  dense(h, "v_star_x", e.m_node_v_fluid_plus_x);
+  dense(h, "v_star_y", e.m_node_v_fluid_plus_y);
+  dense(h, "v_star_z", e.m_node_v_fluid_plus_z);
+  dense(h, "rhs_fluid_x", e.m_node_rhs_fluid_x);
+  dense(h, "rhs_fluid_y", e.m_node_rhs_fluid_y);
+  dense(h, "rhs_fluid_z", e.m_node_rhs_fluid_z);
+  dense(h, "inv_C_x", e.m_node_inv_C_x);
+  dense(h, "inv_C_y", e.m_node_inv_C_y);
+  dense(h, "inv_C_z", e.m_node_inv_C_z);
+  dense(h, "psi_fs_x", e.m_node_psi_fs_x);
+  dense(h, "psi_fs_y", e.m_node_psi_fs_y);
+  dense(h, "psi_fs_z", e.m_node_psi_fs_z);
+}
+
+void snap_system(Harness& h) {
+  LinearizedImplicitEuler& e = *h.stepper;
+  const robertbridson::SparseMatrix<scalar>& A = e.m_fine_pressure_matrix;
+  std::vector<long long>& rs = h.ii["A_rowstart"];
+  std::vector<long long>& ci = h.ii["A_col"];
+  std::vector<double>& va = h.f["A_val"];
+  rs.assign(1, 0);
+  ci.clear();
+  va.clear();
+  for (unsigned i = 0; i < A.n; ++i) {
+    for (size_t k = 0; k < A.index[i].size(); ++k) {
+      ci.push_back(A.index[i][k]);
+      va.push_back(A.value[i][k]);
+    }
+    rs.push_back((long long)ci.size());
+  }
+  h.f["b"] = e.m_fine_pressure_rhs;
+  h.f["b"].resize(A.n);
+  dense_vi(h, "dof_index", e.m_fine_global_indices);
+}
+
+}  // namespace
+
+extern "C" {
+
+// params: dx, g[3], rho, flip, friction, box_c[3], box_half[3], box_r,
+// criterion, maxiters, mic
+void* wcref_create(double dx, const double* g, double rho, double flip,
+                   double friction, const double* box_c,
+                   const double* box_half, double box_r, double criterion,
+                   int maxiters, int mic, int np, const double* x3,
+                   const double* v3, const double* C9, const double* fmass,
+                   const double* fvol, const double* radius) {
+  Harness* h = new Harness();
+  memset(h->timers, 0, sizeof(h->timers));
+  Params& p = h->p;
+  p.dx = dx;
+  for (int r = 0; r < 3; ++r) {
+    p.gravity[r] = g[r];
+    p.box_center[r] = box_c[r];
+    p.box_half[r] = box_half[r];
+  }
+  p.liquid_density = rho;
+  p.flip_coeff = flip;
+  p.liquid_boundary_friction = friction;
+  p.box_radius = box_r;
+  p.criterion = criterion;
+  p.maxiters = maxiters;
+  p.mic = mic;
+
+  h->scene = std::make_shared<TwoDScene>();
+  TwoDScene& s = *h->scene;
+
+  // LiquidInfo defaults of App/TwoDSceneXMLParser.cpp:1851-1904, liquid-only.
+  LiquidInfo info;
+  info.air_density = 1.2041e-3;
+  info.liquid_density = rho;
+  info.rest_contact_angle = 40.8 / 180.0 * M_PI;
+  info.surf_tension_coeff = 72.8;
+  info.yazdchi_power = 1.6;
+  info.viscosity = 8.9e-3;
+  info.air_viscosity = 1.81e-4;
+  info.pore_radius = 0.005;
+  info.yarn_diameter = 0.01;
+  info.rest_volume_fraction = 0.4;
+  info.lambda = 2.0;
+  info.cohesion_coeff = 0.002;
+  info.correction_step = 8;
+  info.correction_multiplier = 2.0;
+  info.correction_strength = 0.0;
+  info.flip_coeff = flip;
+  info.elasto_flip_asym_coeff = 1.0;
+  info.elasto_flip_coeff = 0.95;
+  info.elasto_advect_coeff = 1.0;
+  info.particle_cell_multiplier = 0.3535533906;
+  info.bending_scheme = 2;
+  info.levelset_young_modulus = 6.6e6;
+  info.liquid_boundary_friction = friction;
+  info.use_surf_tension = false;
+  info.surf_tension_smoothing_step = 7;
+  info.use_cohesion = false;
+  info.soft_cohesion = false;
+  info.solid_cohesion = false;
+  info.use_drag = true;
+  info.use_nonlinear_drag = true;
+  info.solve_solid = false;
+  info.apply_pressure_solid = false;
+  info.use_levelset_force = false;
+  info.use_twist = false;
+  info.apply_pressure_manifold = false;
+  info.apply_pore_pressure_solid = false;
+  info.use_bicgstab = false;
+  info.use_amgpcg_solid = false;
+  info.use_pcr = true;
+  info.propagate_solid_velocity = false;
+  info.check_divergence = false;
+  info.use_varying_fraction = false;
+  info.compute_viscosity = false;
+  info.implicit_viscosity = true;
+  info.drag_by_future_solid = false;
+  info.drag_by_air = false;
+  info.init_nonuniform_fraction = false;
+  info.use_group_precondition = false;
+  info.use_lagrangian_mpm = false;
+  info.use_cosolve_angular = false;
+  info.levelset_thickness = 0.25;
+  info.iteration_print_step = 0;
+  info.elasto_capture_rate = 1.0;
+  s.setLiquidInfo(info);
+  s.setBucketInfo(dx * 4.0, 4, 2);  // kernel order is the constant 2
+
+  // walls: solid box, inside (App/TwoDSceneXMLParser.cpp loadDistanceFields)
+  VectorXs par(4);
+  par << box_half[0], box_half[1], box_half[2], box_r;
+  std::vector<DF_SOURCE_DURATION> dur;
+  auto box = std::make_shared<DistanceFieldObject>(
+      Vector3s(box_c[0], box_c[1], box_c[2]), par, DFT_BOX, DFU_SOLID, true,
+      Vector3s(0, 1, 0), 0.0, 0, 0, false, dur);
+  s.m_distance_fields.push_back(box);
+  s.resizeGroups(1);
+  s.initGroupPos();
+
+  // liquid particles (attribute set of sampleLiquidDistanceFields)
+  s.resizeParticleSystem(np);
+  s.m_fluids.resize(np);
+  for (int i = 0; i < np; ++i) {
+    s.m_x.segment<4>(i * 4) = Vector4s(x3[i * 3], x3[i * 3 + 1], x3[i * 3 + 2], 0.0);
+    s.m_rest_x.segment<4>(i * 4) = s.m_x.segment<4>(i * 4);
+    s.m_v.segment<4>(i * 4).setZero();
+    s.m_dv.segment<4>(i * 4).setZero();
+    s.m_fluid_v.segment<4>(i * 4) =
+        Vector4s(v3[i * 3], v3[i * 3 + 1], v3[i * 3 + 2], 0.0);
+    s.m_m.segment<4>(i * 4).setZero();
+    s.m_fluid_m.segment<3>(i * 4).setConstant(fmass[i]);
+    s.m_fluid_m(i * 4 + 3) = fmass[i] * radius[i] * radius[i] * 0.4;
+    s.m_fluid_vol(i) = fvol[i];
+    s.m_vol(i) = 0.0;
+    s.m_rest_vol(i) = 0.0;
+    s.m_shape_factor(i) = 0.0;
+    s.m_radius(i * 2 + 0) = s.m_radius(i * 2 + 1) = radius[i];
+    s.m_volume_fraction(i) = 0.0;
+    s.m_rest_volume_fraction(i) = 0.0;
+    s.m_fixed[i] = 0U;
+    s.m_twist[i] = false;
+    s.m_particle_rest_length(i) = radius[i] * 2.0;
+    s.m_particle_rest_area(i) = M_PI * radius[i] * radius[i];
+    s.m_particle_group[i] = 0;
+    for (int r = 0; r < 3; ++r)
+      for (int q = 0; q < 3; ++q)
+        s.m_fB(i * 3 + r, q) = C9 ? C9[i * 9 + r * 3 + q] : 0.0;
+    s.m_B.block<3, 3>(i * 3, 0).setZero();
+    s.m_is_strand_tip[i] = false;
+    s.m_div[i].resize(0);
+    s.m_particle_to_surfel[i] = -1;
+    s.m_inside[i] = 0U;
+    s.m_classifier[i] = PC_o;
+    s.m_orientation.segment<3>(i * 3).setZero();
+    s.m_fluids[i] = i;
+  }
+  s.updateRestPos();
+
+  s.insertForce(std::make_shared<SimpleGravityForce>(
+      Vector3s(g[0], g[1], g[2])));
+
+  h->stepper = std::make_shared<LinearizedImplicitEuler>(
+      1e-6, criterion, 1e-6, 1e-6, maxiters, 1, 1, 1);
+  h->stepper->setUseApic(true);
+  return h;
+}
+
+void wcref_destroy(void* hp) { delete (Harness*)hp; }
+
+// Number of CFL sub-steps WetClothCore::stepSystem would take for dt
+// (Core/WetClothCore.cpp:50-62).
+int wcref_num_substeps(void* hp, double dt) {
+  Harness* h = (Harness*)hp;
+  TwoDScene& s = *h->scene;
+  const scalar max_elasto_vel = s.getMaxVelocity();
+  const scalar max_fluid_vel = s.getMaxFluidVelocity();
+  const scalar dx = s.getCellSize();
+  const scalar max_elasto_dt =
+      std::min(dx / std::max(1e-63, max_elasto_vel) / 3.0, 1.0 / 30.0);
+  const scalar max_fluid_dt =
+      std::min(dx / std::max(1e-63, max_fluid_vel) * 3.0, 1.0 / 30.0);
+  const scalar max_dt = std::min(max_elasto_dt, max_fluid_dt);
+  return std::max(1, (int)ceil(dt / max_dt));
+}
+
+// One sub-step of the fluid hot path, in WetClothCore::stepSystem order.
+// snapshot != 0 records every intermediate field.
+int wcref_substep(void* hp, double sub_dt, int snapshot) {
+  Harness* h = (Harness*)hp;
+  TwoDScene& s = *h->scene;
+  LinearizedImplicitEuler& e = *h->stepper;
+  double t0 = now(), t1;
+
+  s.updateParticleBoundingBox();
+  s.rebucketizeParticles();
+  s.resampleNodes();
+  t1 = now(); h->timers[1] += t1 - t0; t0 = t1;
+  if (snapshot) snap_grid(*h);
+
+  s.computeWeights(sub_dt);
+  s.updateLiquidPhi(sub_dt);
+  s.updateSolidPhi();
+  s.updateSolidWeights();
+  s.saveParticleVelocity();
+  t1 = now(); h->timers[2] += t1 - t0; t0 = t1;
+
+  s.mapParticleNodesAPIC();
+  s.saveFluidVelocity();
+  s.mapParticleSaturationPsiNodes();
+  s.updatePorePressureNodes();
+  t1 = now(); h->timers[3] += t1 - t0; t0 = t1;
+  if (snapshot) snap_p2g(*h);
+
+  e.stepVelocity(s, sub_dt);
+  t1 = now(); h->timers[4] += t1 - t0; t0 = t1;
+  if (snapshot) snap_predict(*h);
+
+  e.projectFine(s, sub_dt);
+  if (snapshot) {
+    snap_system(*h);
+    dense(*h, "pressure_amg", s.m_node_pressure);
+  }
+  if (h->p.mic) {
+    const unsigned n = e.m_fine_pressure_matrix.n;
+    if (n > 0 && e.m_fine_pressure_rhs.size() >= n) {
+      robertbridson::PCGSolver<double> solver;
+      solver.set_solver_parameters(h->p.criterion, h->p.maxiters, 0.97, 0.25);
+      std::vector<double> rhs(e.m_fine_pressure_rhs.begin(),
+                              e.m_fine_pressure_rhs.begin() + n);
+      std::vector<double> result(n, 0.0);
+      double res = 0;
+      int iters = 0;
+      solver.solve(e.m_fine_pressure_matrix, rhs, result, res, iters);
+      h->last_iters_mic = iters;
+      h->last_res_mic = res;
+      const int nb = s.getNumBuckets();
+      for (int b = 0; b < nb; ++b) {
+        const VectorXi& gi = e.m_fine_global_indices[b];
+        for (int i = 0; i < (int)gi.size(); ++i)
+          if (gi[i] >= 0) s.m_node_pressure[b][i] = result[gi[i]];
+      }
+    }
+  }
+  t1 = now(); h->timers[5] += t1 - t0; t0 = t1;
+  if (snapshot) dense(*h, "pressure", s.m_node_pressure);
+
+  e.applyPressureDragFluid(s, sub_dt);
+  e.acceptVelocity(s);
+  t1 = now(); h->timers[7] += t1 - t0; t0 = t1;
+  if (snapshot) {
+    dense_uc(*h, "valid_x", s.m_node_liquid_valid_x);
+    dense_uc(*h, "valid_y", s.m_node_liquid_valid_y);
+    dense_uc(*h, "valid_z", s.m_node_liquid_valid_z);
+    dense(*h, "u_proj_x", s.m_node_vel_fluid_x);
+    dense(*h, "u_proj_y", s.m_node_vel_fluid_y);
+    dense(*h, "u_proj_z", s.m_node_vel_fluid_z);
+  }
+
+  s.constrainLiquidVelocity();
+  t1 = now(); h->timers[8] += t1 - t0; t0 = t1;
+  if (snapshot) {
+    dense(*h, "u_final_x", s.m_node_vel_fluid_x);
+    dense(*h, "u_final_y", s.m_node_vel_fluid_y);
+    dense(*h, "u_final_z", s.m_node_vel_fluid_z);
+  }
+
+  s.mapNodeParticlesAPIC();
+  t1 = now(); h->timers[9] += t1 - t0; t0 = t1;
+  if (snapshot) snap_particles(*h, "g2p_");
+
+  e.advectScene(s, sub_dt);
+  t1 = now(); h->timers[10] += t1 - t0; t0 = t1;
+  if (snapshot) snap_particles(*h, "adv_");
+  return 0;
+}
+
+// Full step: CFL sub-stepping as WetClothCore::stepSystem.
+int wcref_step(void* hp, double dt, int snapshot) {
+  const int n = wcref_num_substeps(hp, dt);
+  const double sub_dt = dt / (double)n;
+  for (int k = 0; k < n; ++k) wcref_substep(hp, sub_dt, snapshot);
+  return n;
+}
+
+long long wcref_size(void* hp, const char* name) {
+  Harness* h = (Harness*)hp;
+  auto it = h->f.find(name);
+  if (it != h->f.end()) return (long long)it->second.size();
+  auto jt = h->ii.find(name);
+  if (jt != h->ii.end()) return (long long)jt->second.size();
+  return -1;
+}
+
+int wcref_get_f(void* hp, const char* name, double* out) {
+  Harness* h = (Harness*)hp;
+  auto it = h->f.find(name);
+  if (it == h->f.end()) return -1;
+  memcpy(out, it->second.data(), it->second.size() * sizeof(double));
+  return 0;
+}
+
+int wcref_get_i(void* hp, const char* name, long long* out) {
+  Harness* h = (Harness*)hp;
+  auto it = h->ii.find(name);
+  if (it == h->ii.end()) return -1;
+  memcpy(out, it->second.data(), it->second.size() * sizeof(long long));
+  return 0;
+}
+
+void wcref_solver_stats(void* hp, int* iters_mic, double* res_mic) {
+  Harness* h = (Harness*)hp;
+  *iters_mic = h->last_iters_mic;
+  *res_mic = h->last_res_mic;
+}
+
+// cumulative phase timers (seconds), slots as WetClothCore timing_buffer
+void wcref_timers(void* hp, double* out12) {
+  memcpy(out12, ((Harness*)hp)->timers, sizeof(double) * 12);
+}
+
+int wcref_num_particles(void* hp) {
+  return ((Harness*)hp)->scene->getNumParticles();
+}
+
+}  // extern "C"
