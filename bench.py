@@ -1,0 +1,408 @@
+#!/usr/bin/env python
+"""Fluid-step benchmark: ms per step (bucket sort + P2G + MIC(0)-PCG pressure
+projection + G2P + advection) of a 256^3 grid / ~16.8M-particle liquid scene on
+one B200, FP32 transfers and PCG with FP64 reductions and iterative refinement
+to a 1e-6 relative residual, beside the plain FP64 GPU step.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+One JSON line on stdout (rank 0).  Multi-GPU runs (torchrun) are independent
+replicas: the path has no exchange step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "ms/step P2G+PCG+G2P @256³/16M, FP32+refine vs FP64 GPU @1e-6 resid; HBM %"
+DT = 1e-3
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=256, help="grid cells per axis")
+    ap.add_argument("--ppc", type=int, default=2)
+    ap.add_argument("--fp64-steps", type=int, default=None,
+                    help="timed steps of the FP64 arm (default: --steps)")
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-n", type=int, default=64,
+                    help="grid of the bounded CPU-baseline sample")
+    ap.add_argument("--profile-steps", type=int, default=2)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-i", str(self.dev), "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = max(smax, float(f[2]))
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+# Algorithmic bytes per phase (w = bytes per value).  Per particle: sort 4+8
+# bytes of keys plus the 17-value permutation gather; P2G reads x(3) v(3) C(9)
+# m V = 17 values; G2P+advect reads x(3), writes v(3) C(9) x(3) = 18 values.
+# Per active cell: P2G writes 3 faces x (m, u, V) + phi + sat + psi = 12;
+# grid update reads 12 and writes 8.  Per DOF: each triangular sweep 6 values,
+# the factorisation 6, one PCG iteration's vector work 20 (SpMV 6, s.q 2,
+# x 3, r 3, |r| 1, z.r 2, s 3).
+def phase_bytes(phase, w, np_, ncell, ndof, iters, nsweeps):
+    if phase == "grid_build_sort":
+        return np_ * (12 + 17 * w)
+    if phase == "p2g":
+        return np_ * 17 * w + ncell * 12 * w
+    if phase == "g2p_advect":
+        return np_ * 18 * w + ncell * 3 * w
+    if phase == "grid_ops":
+        return ncell * 20 * w
+    if phase == "mic_sweep":
+        return ndof * 6 * w * nsweeps
+    if phase == "mic_factor":
+        return ndof * 6 * w
+    if phase == "pcg_vector":
+        return ndof * 20 * w * iters
+    return 0
+
+
+def traffic_per_launch(kernel_phase, ndof, np_):
+    """DRAM bytes per launch from the committed ncu capture (profiles/),
+    scaled to this workload's units; None if no capture is committed."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if not os.path.exists(p):
+        return None
+    d = json.load(open(p))
+    e = d.get(kernel_phase)
+    if not e:
+        return None
+    units = ndof if e.get("unit") == "dof" else np_
+    return e["bytes_per_unit"] * units
+
+
+# ---------------------------------------------------------------------------
+def run_ours(args, rank, world, dev):
+    import numpy as np
+    import torch
+    from libwetcloth_b200 import scenes
+    from libwetcloth_b200._capi import WCG_FP32_REFINE, WCG_FP64
+    from libwetcloth_b200.solver import FluidScene
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    t0 = time.time()
+    sc = scenes.half_box(args.n, args.ppc, seed=1 + rank)
+    gen_s = time.time() - t0
+    np_ = sc.x.shape[0]
+
+    def timed(precision, steps, warmup, sample_clocks=False):
+        sim = FluidScene(sc, precision=precision)
+        for _ in range(warmup):
+            sim.step(DT)
+        stream = torch.cuda.ExternalStream(sim.stream_ptr, device=f"cuda:{dev}")
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        barrier()
+        torch.cuda.synchronize(dev)
+        clk = ClockSampler(dev) if sample_clocks else None
+        if clk:
+            clk.start()
+            time.sleep(0.3)
+        l0 = sim.launch_count
+        iters = []
+        e0.record(stream)
+        w0 = time.perf_counter()
+        for _ in range(steps):
+            sim.step(DT)
+            st = sim.stats()
+            iters.append(st["pcg_iters"])
+        e1.record(stream)
+        e1.synchronize()
+        wall = time.perf_counter() - w0
+        torch.cuda.synchronize(dev)
+        clocks = clk.stop() if clk else None
+        barrier()
+        ms = max_over_ranks(e0.elapsed_time(e1) / steps)
+        launches = sim.launch_count - l0
+        info = dict(ms=ms, wall_ms=wall * 1000 / steps, launches=launches,
+                    iters=iters, stats=sim.stats(), clocks=clocks)
+        return sim, info
+
+    # headline arm: FP32 transfers + FP32 PCG + FP64 refinement
+    sim, main = timed(WCG_FP32_REFINE, args.steps, args.warmup, sample_clocks=True)
+    st = main["stats"]
+    # per-phase breakdown (separate pass; events around each phase)
+    sim.profile_begin()
+    for _ in range(args.profile_steps):
+        sim.step(DT)
+    prof = sim.profile_end()
+    pst = sim.stats()
+    ncell = pst["nactive_buckets"] * 64
+    ndof = pst["ndof"]
+    # e2e through the public C-ABI with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        x, v, C = sim.download()
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+        hx, hv, hC = pin(x), pin(v), pin(C)
+        hm, hV, hr = pin(sc.mass), pin(sc.vol), pin(sc.radius)
+        ox, ov, oC = (torch.empty_like(t).pin_memory() for t in (hx, hv, hC))
+        from libwetcloth_b200._capi import check
+        L = sim.L
+        ptr = lambda t: __import__("ctypes").cast(t.data_ptr(), __import__("ctypes").POINTER(
+            __import__("ctypes").c_double))
+        stream = torch.cuda.ExternalStream(sim.stream_ptr, device=f"cuda:{dev}")
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        nsub = __import__("ctypes").c_int(0)
+        k_e2e = max(2, min(args.steps, 5))
+        barrier()
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        for _ in range(k_e2e):
+            check(L.wcg_upload_liquid(sim.h, np_, ptr(hx), ptr(hv), ptr(hC), ptr(hm),
+                                      ptr(hV), ptr(hr)))
+            check(L.wcg_step(sim.h, DT, __import__("ctypes").byref(nsub)))
+            check(L.wcg_download_liquid(sim.h, ptr(ox), ptr(ov), ptr(oC)))
+            hx, ox = ox, hx
+            hv, ov = ov, hv
+            hC, oC = oC, hC
+        e1.record(stream)
+        e1.synchronize()
+        e2e_ms = max_over_ranks(e0.elapsed_time(e1) / k_e2e)
+        h2d = np_ * (3 + 3 + 9 + 3) * 8
+        d2h = np_ * (3 + 3 + 9) * 8
+        e2e = {"value": round(e2e_ms, 3), "unit": "ms/step",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": k_e2e}
+    sim.close()
+    # FP64 GPU arm at the same residual
+    fp64 = None
+    if not args.no_fp64:
+        k64 = args.fp64_steps if args.fp64_steps is not None else args.steps
+        sim64, info64 = timed(WCG_FP64, k64, args.warmup)
+        sim64.close()
+        fp64 = info64
+    # roofline of the dominant phase
+    peak, peak_kind = measured_peaks()
+    w = 4
+    iters_prof = max(pst["pcg_iters"], 1)
+    dom = max(prof.items(), key=lambda kv: kv[1][0])
+    dom_name, (dom_ms, dom_launch) = dom
+    dom_ms_step = dom_ms / args.profile_steps
+    nsweeps = max(dom_launch // args.profile_steps, 1) if dom_name == "mic_sweep" else 1
+    per_launch_ms = dom_ms / max(dom_launch, 1)
+    bytes_step = phase_bytes(dom_name, w, np_, ncell, ndof, iters_prof, nsweeps)
+    bytes_launch = bytes_step / max(dom_launch / args.profile_steps, 1)
+    achieved = bytes_launch / (per_launch_ms * 1e-3) / 1e9 if per_launch_ms > 0 else 0.0
+    traffic = traffic_per_launch(dom_name, ndof, np_)
+    roofline = {"bound": "hbm", "kernel": dom_name, "achieved": round(achieved, 1),
+                "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "peak_kind": peak_kind, "traffic": traffic,
+                "bytes_per_launch": int(bytes_launch),
+                "ms_per_launch": round(per_launch_ms, 4)}
+    phases = {k: {"ms_per_step": round(v[0] / args.profile_steps, 3),
+                  "launches_per_step": v[1] // args.profile_steps}
+              for k, v in prof.items()}
+    # transfer-kernel HBM fractions
+    transfers = {}
+    for k in ("p2g", "g2p_advect"):
+        ms_k = prof[k][0] / args.profile_steps
+        if ms_k > 0:
+            gbs = phase_bytes(k, w, np_, ncell, ndof, 1, 1) / (ms_k * 1e-3) / 1e9
+            transfers[k] = {"GB/s": round(gbs, 1), "frac": round(gbs / peak, 4)}
+    out = {
+        "metric": METRIC,
+        "value": round(main["ms"], 3),
+        "unit": "ms/step",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(main["ms"], 3),
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded half-filled box, curl-noise velocity)",
+        "config": {
+            "workload": f"half_box {args.n}^3, {args.ppc} ppc, {np_} particles, dt {DT}, "
+                        "MIC(0)-PCG FP32 + FP64 refinement to 1e-6",
+            "grid": args.n, "particles": np_, "active_buckets": pst["nactive_buckets"],
+            "pressure_dofs": ndof, "precision": "fp32 transfers+PCG, fp64 reductions/refine",
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            "l2": "inputs larger than L2 (particle state %.1f GB)" % (np_ * 80 / 1e9),
+        },
+        "particle_updates_per_s": round(world * np_ / (main["ms"] * 1e-3), 1),
+        "pcg_iters_per_step": main["iters"],
+        "refinements": st["refinements"],
+        "final_residual_rel": st["residual"] / max(st["rhs_norm"], 1e-300),
+        "gpu_launches": int(main["launches"]),
+        "launches_per_step": round(main["launches"] / args.steps, 1),
+        "phases": phases,
+        "roofline": roofline,
+        "transfers_hbm": transfers,
+        "clocks": main["clocks"],
+        "e2e": e2e,
+        "scene_gen_s": round(gen_s, 1),
+    }
+    if fp64:
+        out["fp64"] = {"ms_per_step": round(fp64["ms"], 3), "pcg_iters_per_step": fp64["iters"],
+                       "speedup_fp32_refine_vs_fp64": round(fp64["ms"] / main["ms"], 3)}
+    return out
+
+
+# ---------------------------------------------------------------------------
+def run_reference_cpu(args, sample_n, steps=2, warmup=1):
+    """The reference Core (oracle/_ref, OpenMP stand-in for TBB, all host
+    threads) on a bounded sample: the same scene type at sample_n^3, ms/step
+    scaled by particle count to the full workload."""
+    from libwetcloth_b200 import scenes
+    from oracle import ref as oref
+    if not oref.available(omp=True):
+        return None, "oracle/_ref/libwcref_omp.so not built"
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    sc = scenes.half_box(sample_n, args.ppc, seed=1)
+    full_np = None
+    r = oref.RefScene(sc, mic=False, omp=True)
+    for _ in range(warmup):
+        r.step(DT, snapshot=False)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        r.step(DT, snapshot=False)
+    dt = (time.perf_counter() - t0) / steps
+    r.close()
+    n_sample = sc.x.shape[0]
+    # full-workload particle count of the same generator
+    full_np = args.ppc * args.n * (args.n // 2) * args.n
+    scale = full_np / n_sample
+    return {"value": round(dt * 1000 * scale, 1), "unit": "ms/step",
+            "cores": int(os.environ.get("OMP_NUM_THREADS", cores)), "kind": "reference",
+            "sample": f"reference Core (multigrid-PCG default solver) on half_box "
+                      f"{sample_n}^3/{n_sample} particles, {steps} steps after {warmup} "
+                      f"warm-up, {dt*1000:.1f} ms/step x {scale:.1f} (particle ratio); "
+                      f"OpenMP stand-in for TBB"}, None
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        cpu, why = run_reference_cpu(args, args.cpu_sample_n, steps=max(1, min(args.steps, 3)),
+                                     warmup=min(args.warmup, 1))
+        if cpu is None:
+            print(json.dumps({"impl": "reference", "unavailable": why}))
+            return 0
+        print(json.dumps({
+            "metric": METRIC, "value": cpu["value"], "unit": "ms/step", "impl": "reference",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": cpu["value"], "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"half_box {args.n}^3, {args.ppc} ppc (bounded sample, "
+                                   "scaled)"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": cpu["value"], "unit": "ms/step", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}))
+        return 0
+    import torch
+    if world > 1:
+        torch.cuda.set_device(local)
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    out = run_ours(args, rank, world, dev)
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu, why = run_reference_cpu(args, args.cpu_sample_n)
+        out["cpu_baseline"] = cpu if cpu else {"unavailable": why}
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,162 @@
+/* libwcgpu: the libWetCloth fluid-step hot path on one NVIDIA B200 (sm_100a).
+ *
+ * C ABI (plain pointers and sizes).  Every call returns an int status
+ * (WCG_OK == 0); the message of the last failure on the calling thread is
+ * available from wcg_last_error().
+ *
+ * The entry points mirror the reference's call sites for the liquid path
+ * (libWetCloth/Core/WetClothCore.cpp:115-258): the TwoDScene methods
+ * rebucketizeParticles / resampleNodes / computeWeights / updateLiquidPhi /
+ * updateSolidPhi / updateSolidWeights / mapParticleNodesAPIC /
+ * mapParticleSaturationPsiNodes / constrainLiquidVelocity /
+ * mapNodeParticlesAPIC, the SceneStepper virtuals stepVelocity / projectFine /
+ * applyPressureDragFluid / acceptVelocity / advectScene, and the whole
+ * WetClothCore::stepSystem.  Particle and grid state stays resident on the GPU
+ * between calls; upload/download calls move it to and from host (or device)
+ * buffers in the reference's layouts.
+ */
+#ifndef WETCLOTH_GPU_H
+#define WETCLOTH_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  WCG_OK = 0,
+  WCG_ERR_ARG = 1,        /* invalid argument */
+  WCG_ERR_CUDA = 2,       /* CUDA runtime error (message has the details) */
+  WCG_ERR_NOT_CONVERGED = 3, /* pressure solve hit maxiters or rho was 0/NaN */
+  WCG_ERR_DEVICE = 4,     /* a kernel recorded an error (wait limit, index) */
+  WCG_ERR_STATE = 5       /* call out of order (e.g. no grid built yet) */
+};
+
+enum { WCG_FP64 = 0, WCG_FP32_REFINE = 1 };
+
+/* Scene parameters: the liquid subset of LiquidInfo
+ * (libWetCloth/Core/TwoDScene.h:35-91) plus bucket info (numcells fixed at 4,
+ * kernel order 2) and one solid box whose inside holds the fluid
+ * (DistanceFieldObject DFT_BOX / DFU_SOLID / inside=true). */
+typedef struct wcg_params {
+  double dx;                       /* cell size = bucket size / 4 */
+  double gravity[3];               /* SimpleGravityForce */
+  double liquid_density;
+  double flip_coeff;               /* LiquidInfo::flip_coeff */
+  double liquid_boundary_friction; /* LiquidInfo::liquid_boundary_friction */
+  double box_center[3];
+  double box_half[3];
+  double box_radius;
+  int walls;                       /* 1: the box above is present */
+  double criterion;                /* pressure criterion: ||r||_inf <= c ||b||_inf */
+  int maxiters;                    /* PCG iteration limit */
+  int precision;                   /* WCG_FP64 or WCG_FP32_REFINE */
+  double refine_inner_tol;         /* FP32 inner-solve relative tolerance (0: aim at criterion) */
+  int max_refinements;             /* FP64 refinement sweeps (0: 20) */
+} wcg_params;
+
+typedef struct wcg_ctx wcg_ctx;
+
+typedef struct wcg_stats {
+  int substeps;
+  int pcg_iters;
+  int refinements;
+  int converged;
+  double residual;   /* final ||b - A p||_inf */
+  double rhs_norm;   /* ||b||_inf */
+  long long ndof;
+  long long nactive_buckets;
+} wcg_stats;
+
+const char* wcg_last_error(void);
+void wcg_default_params(wcg_params* p);
+
+/* TwoDScene + LinearizedImplicitEuler + WetClothCore construction. */
+int wcg_create(const wcg_params* params, wcg_ctx** out);
+int wcg_destroy(wcg_ctx* ctx);
+
+/* Liquid particles (TwoDScene::sampleLiquidDistanceFields attribute set,
+ * TwoDScene.cpp:5564-5605): positions x3[3n], fluid velocities v3[3n], affine
+ * matrices C9[9n] row-major (m_fB rows; may be NULL = zero), fluid mass,
+ * fluid volume and radius per particle.  Host pointers. */
+int wcg_upload_liquid(wcg_ctx* ctx, long long n, const double* x3,
+                      const double* v3, const double* C9, const double* mass,
+                      const double* vol, const double* radius);
+/* Same with device pointers (state already resident in HBM). */
+int wcg_upload_liquid_device(wcg_ctx* ctx, long long n, const double* x3,
+                             const double* v3, const double* C9,
+                             const double* mass, const double* vol,
+                             const double* radius);
+/* Particle state in the original particle order (any pointer may be NULL). */
+int wcg_download_liquid(wcg_ctx* ctx, double* x3, double* v3, double* C9);
+int wcg_download_liquid_device(wcg_ctx* ctx, double* x3, double* v3,
+                               double* C9);
+long long wcg_num_particles(const wcg_ctx* ctx);
+
+/* ---- the reference call sequence (WetClothCore::stepSystem order) ---- */
+/* updateParticleBoundingBox + rebucketizeParticles + resampleNodes
+ * (TwoDScene.cpp:1588, :1657, :5069): grid, particle sort, bucket activation */
+int wcg_rebucketize_and_resample(wcg_ctx* ctx);
+/* computeWeights + updateLiquidPhi + updateSolidPhi + updateSolidWeights +
+ * mapParticleNodesAPIC + mapParticleSaturationPsiNodes +
+ * updatePorePressureNodes (TwoDScene.cpp:2246, :3286, :7940, :1871, :6609,
+ * :5952, :5933) */
+int wcg_map_particle_nodes(wcg_ctx* ctx);
+/* LinearizedImplicitEuler::stepVelocity (+acceptVelocity of u*),
+ * LinearizedImplicitEuler.cpp:224 */
+int wcg_step_velocity(wcg_ctx* ctx, double dt);
+/* LinearizedImplicitEuler::projectFine -> pressure::solveNodePressure
+ * (Pressure.cpp:285) with MIC(0)-PCG */
+int wcg_project_fine(wcg_ctx* ctx, double dt);
+/* applyPressureDragFluid + acceptVelocity (LinearizedImplicitEuler.cpp:2435,
+ * :2176) */
+int wcg_apply_pressure_drag_fluid(wcg_ctx* ctx, double dt);
+/* TwoDScene::constrainLiquidVelocity (TwoDScene.cpp:1827) */
+int wcg_constrain_liquid_velocity(wcg_ctx* ctx);
+/* TwoDScene::mapNodeParticlesAPIC (TwoDScene.cpp:6936) */
+int wcg_map_node_particles(wcg_ctx* ctx);
+/* SceneStepper::advectScene (SceneStepper.cpp:17) */
+int wcg_advect(wcg_ctx* ctx, double dt);
+/* One CFL sub-step of everything above (G2P and advection fused). */
+int wcg_substep(wcg_ctx* ctx, double dt);
+/* WetClothCore::stepSystem (WetClothCore.cpp:45): CFL sub-stepping + sub-steps */
+int wcg_step(wcg_ctx* ctx, double dt, int* substeps_out);
+int wcg_num_substeps(wcg_ctx* ctx, double dt, int* n_out);
+
+int wcg_get_stats(const wcg_ctx* ctx, wcg_stats* out);
+
+/* ---- parity downloads in the reference's dense bucket-major layout ---- */
+/* grid: dims[3] buckets, origin[3] (m_grid_mincorner), bbx[6] */
+int wcg_grid_info(const wcg_ctx* ctx, int* dims, double* origin, double* bbx);
+/* number of values of a named field (-1 if unknown) */
+long long wcg_field_size(wcg_ctx* ctx, const char* name);
+/* double field by name, nb*64 values, NaN in inactive buckets */
+int wcg_download_field(wcg_ctx* ctx, const char* name, double* out, long long n);
+/* integer field by name ("active", "dof_index", "valid_x", "array_idx",
+ * "array_sup", "stencil_base", "grid_dims") */
+int wcg_download_ifield(wcg_ctx* ctx, const char* name, long long* out, long long n);
+/* assembled pressure system in the reference's DOF order and CSR layout of
+ * robertbridson::SparseMatrix (sorted columns).  With rowstart == NULL only
+ * the sizes are returned. */
+int wcg_export_pressure_system(wcg_ctx* ctx, long long* ndof, long long* nnz,
+                               long long* rowstart, long long* col,
+                               double* val, double* rhs);
+
+/* ---- instrumentation ---- */
+/* the cudaStream_t all of this context's kernels run on */
+void* wcg_stream(const wcg_ctx* ctx);
+/* number of kernels this context has launched so far */
+long long wcg_launch_count(const wcg_ctx* ctx);
+/* per-phase CUDA-event timing: begin, run steps, end; end fills ms[ncat] and
+ * launches[ncat] with totals per phase (names from wcg_profile_phase_name) */
+int wcg_profile_begin(wcg_ctx* ctx);
+int wcg_profile_end(wcg_ctx* ctx, double* ms, long long* launches, int ncat);
+int wcg_profile_num_phases(void);
+const char* wcg_profile_phase_name(int i);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WETCLOTH_GPU_H */

@@ -1,0 +1,132 @@
+"""ctypes binding of libwcgpu.so (include/wetcloth_gpu.h).
+
+The CUDA library is the only implementation: if it is missing or cannot be
+loaded this module raises; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libwcgpu.so")
+
+_D = ctypes.POINTER(ctypes.c_double)
+_L = ctypes.POINTER(ctypes.c_longlong)
+_I = ctypes.POINTER(ctypes.c_int)
+
+WCG_OK = 0
+WCG_ERR_ARG = 1
+WCG_ERR_CUDA = 2
+WCG_ERR_NOT_CONVERGED = 3
+WCG_ERR_DEVICE = 4
+WCG_ERR_STATE = 5
+WCG_FP64 = 0
+WCG_FP32_REFINE = 1
+
+
+class WcgParams(ctypes.Structure):
+    _fields_ = [
+        ("dx", ctypes.c_double),
+        ("gravity", ctypes.c_double * 3),
+        ("liquid_density", ctypes.c_double),
+        ("flip_coeff", ctypes.c_double),
+        ("liquid_boundary_friction", ctypes.c_double),
+        ("box_center", ctypes.c_double * 3),
+        ("box_half", ctypes.c_double * 3),
+        ("box_radius", ctypes.c_double),
+        ("walls", ctypes.c_int),
+        ("criterion", ctypes.c_double),
+        ("maxiters", ctypes.c_int),
+        ("precision", ctypes.c_int),
+        ("refine_inner_tol", ctypes.c_double),
+        ("max_refinements", ctypes.c_int),
+    ]
+
+
+class WcgStats(ctypes.Structure):
+    _fields_ = [
+        ("substeps", ctypes.c_int),
+        ("pcg_iters", ctypes.c_int),
+        ("refinements", ctypes.c_int),
+        ("converged", ctypes.c_int),
+        ("residual", ctypes.c_double),
+        ("rhs_norm", ctypes.c_double),
+        ("ndof", ctypes.c_longlong),
+        ("nactive_buckets", ctypes.c_longlong),
+    ]
+
+
+# every symbol include/wetcloth_gpu.h declares, with (restype, argtypes)
+SIGNATURES = {
+    "wcg_last_error": (ctypes.c_char_p, []),
+    "wcg_default_params": (None, [ctypes.POINTER(WcgParams)]),
+    "wcg_create": (ctypes.c_int, [ctypes.POINTER(WcgParams), ctypes.POINTER(ctypes.c_void_p)]),
+    "wcg_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "wcg_upload_liquid": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, _D, _D, _D, _D, _D, _D]),
+    "wcg_upload_liquid_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_void_p,
+                                                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                ctypes.c_void_p, ctypes.c_void_p]),
+    "wcg_download_liquid": (ctypes.c_int, [ctypes.c_void_p, _D, _D, _D]),
+    "wcg_download_liquid_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p,
+                                                  ctypes.c_void_p, ctypes.c_void_p]),
+    "wcg_num_particles": (ctypes.c_longlong, [ctypes.c_void_p]),
+    "wcg_rebucketize_and_resample": (ctypes.c_int, [ctypes.c_void_p]),
+    "wcg_map_particle_nodes": (ctypes.c_int, [ctypes.c_void_p]),
+    "wcg_step_velocity": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
+    "wcg_project_fine": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
+    "wcg_apply_pressure_drag_fluid": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
+    "wcg_constrain_liquid_velocity": (ctypes.c_int, [ctypes.c_void_p]),
+    "wcg_map_node_particles": (ctypes.c_int, [ctypes.c_void_p]),
+    "wcg_advect": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
+    "wcg_substep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
+    "wcg_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _I]),
+    "wcg_num_substeps": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _I]),
+    "wcg_get_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(WcgStats)]),
+    "wcg_grid_info": (ctypes.c_int, [ctypes.c_void_p, _I, _D, _D]),
+    "wcg_field_size": (ctypes.c_longlong, [ctypes.c_void_p, ctypes.c_char_p]),
+    "wcg_download_field": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, _D, ctypes.c_longlong]),
+    "wcg_download_ifield": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, _L, ctypes.c_longlong]),
+    "wcg_export_pressure_system": (ctypes.c_int, [ctypes.c_void_p, _L, _L, _L, _L, _D, _D]),
+    "wcg_stream": (ctypes.c_void_p, [ctypes.c_void_p]),
+    "wcg_launch_count": (ctypes.c_longlong, [ctypes.c_void_p]),
+    "wcg_profile_begin": (ctypes.c_int, [ctypes.c_void_p]),
+    "wcg_profile_end": (ctypes.c_int, [ctypes.c_void_p, _D, _L, ctypes.c_int]),
+    "wcg_profile_num_phases": (ctypes.c_int, []),
+    "wcg_profile_phase_name": (ctypes.c_char_p, [ctypes.c_int]),
+}
+
+_lib = None
+
+
+def load():
+    """Load libwcgpu.so (raises OSError if it is not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"libwcgpu.so not built ({LIB_PATH}); run __graft_entry__.build()")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+class WcgError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"libwcgpu error {code}: {msg}")
+        self.code = code
+
+
+def check(code):
+    if code != WCG_OK:
+        raise WcgError(code, load().wcg_last_error().decode(errors="replace"))
+    return code
+
+
+def _dp(a):
+    return a.ctypes.data_as(_D) if a is not None else None

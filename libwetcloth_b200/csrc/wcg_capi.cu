@@ -1,0 +1,650 @@
+// extern "C" surface of libwcgpu (declared in include/wetcloth_gpu.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <vector>
+
+#include "../../include/wetcloth_gpu.h"
+#include "wcg_context.h"
+
+struct wcg_ctx {
+  wcg::Context c;
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+int cuda_status(wcg::Context& c, cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    c.last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return fail(WCG_ERR_CUDA, c.last_error);
+  }
+  return WCG_OK;
+}
+
+// check the device error word after a stage
+int device_status(wcg::Context& c, const char* what) {
+  int h = 0;
+  cudaError_t e = cudaMemcpyAsync(&h, c.derr.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
+  if (e != cudaSuccess) return cuda_status(c, e, what);
+  if (h != 0) {
+    cudaMemsetAsync(c.derr.p, 0, sizeof(int), c.stream);
+    cudaStreamSynchronize(c.stream);
+    return fail(WCG_ERR_DEVICE, std::string(what) + ": device error code " +
+                                    std::to_string(h) +
+                                    (h == wcg::kErrWaitTimeout
+                                         ? " (wavefront wait limit reached)"
+                                         : " (index out of range, access skipped)"));
+  }
+  return WCG_OK;
+}
+
+#define WCG_CHECK_CTX(ctx)                                        \
+  do {                                                            \
+    if (!(ctx)) return fail(WCG_ERR_ARG, "null context");         \
+  } while (0)
+
+#define WCG_CALL(ctx, expr, what)                                 \
+  do {                                                            \
+    int s_ = cuda_status((ctx)->c, (expr), (what));               \
+    if (s_) return s_;                                            \
+  } while (0)
+
+struct FieldName {
+  const char* name;
+  int field;  // wcg::GField, or -1 for an all-zero field
+};
+
+// P2G/step outputs that are identically zero for liquid-only scenes (no
+// elasto particles, static walls): solid volume fraction psi, solid velocity,
+// pore pressure.
+const FieldName kFields[] = {
+    {"mass_fluid_x", wcg::G_MASS}, {"mass_fluid_y", wcg::G_MASS + 1},
+    {"mass_fluid_z", wcg::G_MASS + 2}, {"vel_fluid_x", wcg::G_VEL},
+    {"vel_fluid_y", wcg::G_VEL + 1}, {"vel_fluid_z", wcg::G_VEL + 2},
+    {"vol_fluid_x", wcg::G_VOL}, {"vol_fluid_y", wcg::G_VOL + 1},
+    {"vol_fluid_z", wcg::G_VOL + 2}, {"sat_x", wcg::G_SAT},
+    {"sat_y", wcg::G_SAT + 1}, {"sat_z", wcg::G_SAT + 2},
+    {"psi_x", -1}, {"psi_y", -1}, {"psi_z", -1},
+    {"solid_weight_x", wcg::G_WEIGHT}, {"solid_weight_y", wcg::G_WEIGHT + 1},
+    {"solid_weight_z", wcg::G_WEIGHT + 2}, {"solid_vel_x", -1},
+    {"solid_vel_y", -1}, {"solid_vel_z", -1},
+    {"v_star_x", wcg::G_VSTAR}, {"v_star_y", wcg::G_VSTAR + 1},
+    {"v_star_z", wcg::G_VSTAR + 2}, {"rhs_fluid_x", wcg::G_RHS},
+    {"rhs_fluid_y", wcg::G_RHS + 1}, {"rhs_fluid_z", wcg::G_RHS + 2},
+    {"inv_C_x", wcg::G_INVC}, {"inv_C_y", wcg::G_INVC + 1},
+    {"inv_C_z", wcg::G_INVC + 2}, {"psi_fs_x", wcg::G_PSIFS},
+    {"psi_fs_y", wcg::G_PSIFS + 1}, {"psi_fs_z", wcg::G_PSIFS + 2},
+    {"u_x", wcg::G_U}, {"u_y", wcg::G_U + 1}, {"u_z", wcg::G_U + 2},
+    {"liquid_phi", wcg::G_LPHI}, {"sat_p", wcg::G_SATP}, {"psi_p", -1},
+    {"pore_pressure_p", -1}, {"solid_phi", wcg::G_SPHI},
+    {"pressure", wcg::G_PRESSURE}, {"A_diag", wcg::G_ADIAG},
+    {"A_x", wcg::G_AX}, {"A_y", wcg::G_AY}, {"A_z", wcg::G_AZ},
+    {"b_dense", wcg::G_B}, {"mic_invdiag", wcg::G_INVDIAG},
+};
+
+int lookup_field(const char* name) {
+  for (const FieldName& f : kFields)
+    if (!strcmp(f.name, name)) return f.field;
+  return -2;
+}
+
+std::vector<unsigned char> host_active(wcg::Context& c) {
+  std::vector<unsigned char> a((size_t)c.g.nb);
+  if (c.g.nb)
+    cudaMemcpy(a.data(), c.active.p, (size_t)c.g.nb, cudaMemcpyDeviceToHost);
+  return a;
+}
+
+// raw field (converted to double) over all nodes
+std::vector<double> host_field(wcg::Context& c, int field) {
+  const long long nn = c.g.nnode;
+  std::vector<double> out((size_t)nn, 0.0);
+  if (field < 0 || nn == 0) return out;
+  if (c.prm.precision == 0) {
+    cudaMemcpy(out.data(), c.gfield.as<double>() + (size_t)field * c.gcap,
+               nn * sizeof(double), cudaMemcpyDeviceToHost);
+  } else {
+    std::vector<float> f((size_t)nn);
+    cudaMemcpy(f.data(), c.gfield.as<float>() + (size_t)field * c.gcap,
+               nn * sizeof(float), cudaMemcpyDeviceToHost);
+    for (long long i = 0; i < nn; ++i) out[i] = f[i];
+  }
+  return out;
+}
+
+std::vector<unsigned char> host_bytes(const void* dev, long long n) {
+  std::vector<unsigned char> v((size_t)n);
+  if (n) cudaMemcpy(v.data(), dev, (size_t)n, cudaMemcpyDeviceToHost);
+  return v;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* wcg_last_error(void) { return g_err.c_str(); }
+
+void wcg_default_params(wcg_params* p) {
+  if (!p) return;
+  memset(p, 0, sizeof(*p));
+  p->dx = 1.0 / 64.0;
+  p->gravity[1] = -9.81;
+  p->liquid_density = 1000.0;
+  p->flip_coeff = 0.99;
+  p->liquid_boundary_friction = 0.0;
+  for (int a = 0; a < 3; ++a) {
+    p->box_center[a] = 0.5;
+    p->box_half[a] = 0.5;
+  }
+  p->box_radius = 0.0;
+  p->walls = 1;
+  p->criterion = 1e-6;
+  p->maxiters = 1000;
+  p->precision = WCG_FP64;
+  p->refine_inner_tol = 0.0;
+  p->max_refinements = 20;
+}
+
+int wcg_create(const wcg_params* params, wcg_ctx** out) {
+  if (!params || !out) return fail(WCG_ERR_ARG, "null argument");
+  if (!(params->dx > 0)) return fail(WCG_ERR_ARG, "dx must be positive");
+  if (params->precision != WCG_FP64 && params->precision != WCG_FP32_REFINE)
+    return fail(WCG_ERR_ARG, "precision must be WCG_FP64 or WCG_FP32_REFINE");
+  if (params->maxiters < 0) return fail(WCG_ERR_ARG, "maxiters must be >= 0");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(WCG_ERR_CUDA, "no CUDA device available");
+  wcg_ctx* ctx = new wcg_ctx();
+  wcg::Params& p = ctx->c.prm;
+  p.dx = params->dx;
+  for (int a = 0; a < 3; ++a) {
+    p.gravity[a] = params->gravity[a];
+    p.box_center[a] = params->box_center[a];
+    p.box_half[a] = params->box_half[a];
+  }
+  p.liquid_density = params->liquid_density;
+  p.flip_coeff = params->flip_coeff;
+  p.liquid_boundary_friction = params->liquid_boundary_friction;
+  p.box_radius = params->box_radius;
+  p.walls = params->walls;
+  p.criterion = params->criterion;
+  p.maxiters = params->maxiters;
+  p.precision = params->precision;
+  p.refine_inner_tol = params->refine_inner_tol > 0 ? params->refine_inner_tol : 0.0;
+  p.max_refinements = params->max_refinements > 0 ? params->max_refinements : 20;
+  cudaError_t e = wcg::ctx_init(ctx->c);
+  if (e != cudaSuccess) {
+    std::string m = std::string("context init: ") + cudaGetErrorString(e);
+    wcg::ctx_free(ctx->c);
+    delete ctx;
+    return fail(WCG_ERR_CUDA, m);
+  }
+  *out = ctx;
+  return WCG_OK;
+}
+
+int wcg_destroy(wcg_ctx* ctx) {
+  if (!ctx) return WCG_OK;
+  cudaStreamSynchronize(ctx->c.stream);
+  wcg::ctx_free(ctx->c);
+  delete ctx;
+  return WCG_OK;
+}
+
+static int upload(wcg_ctx* ctx, long long n, const double* x3, const double* v3,
+                  const double* C9, const double* mass, const double* vol,
+                  const double* radius, bool dev) {
+  WCG_CHECK_CTX(ctx);
+  if (n < 0 || n > 2000000000ll) return fail(WCG_ERR_ARG, "particle count out of range");
+  if (n > 0 && (!x3 || !v3 || !mass || !vol || !radius))
+    return fail(WCG_ERR_ARG, "null particle array");
+  if (!dev && n > 0) {
+    for (long long i = 0; i < 3 * n; ++i)
+      if (!std::isfinite(x3[i]) || !std::isfinite(v3[i]))
+        return fail(WCG_ERR_ARG, "non-finite particle position or velocity");
+    for (long long i = 0; i < n; ++i)
+      if (!(mass[i] >= 0) || !(vol[i] >= 0) || !(radius[i] >= 0))
+        return fail(WCG_ERR_ARG, "negative or NaN particle mass/volume/radius");
+  }
+  WCG_CALL(ctx, wcg::upload_particles(ctx->c, n, x3, v3, C9, mass, vol, radius, dev),
+           "upload");
+  ctx->c.have_grid = false;
+  return WCG_OK;
+}
+
+int wcg_upload_liquid(wcg_ctx* ctx, long long n, const double* x3, const double* v3,
+                      const double* C9, const double* mass, const double* vol,
+                      const double* radius) {
+  return upload(ctx, n, x3, v3, C9, mass, vol, radius, false);
+}
+
+int wcg_upload_liquid_device(wcg_ctx* ctx, long long n, const double* x3,
+                             const double* v3, const double* C9, const double* mass,
+                             const double* vol, const double* radius) {
+  return upload(ctx, n, x3, v3, C9, mass, vol, radius, true);
+}
+
+int wcg_download_liquid(wcg_ctx* ctx, double* x3, double* v3, double* C9) {
+  WCG_CHECK_CTX(ctx);
+  WCG_CALL(ctx, wcg::download_particles(ctx->c, x3, v3, C9, false), "download");
+  return WCG_OK;
+}
+
+int wcg_download_liquid_device(wcg_ctx* ctx, double* x3, double* v3, double* C9) {
+  WCG_CHECK_CTX(ctx);
+  WCG_CALL(ctx, wcg::download_particles(ctx->c, x3, v3, C9, true), "download");
+  return WCG_OK;
+}
+
+long long wcg_num_particles(const wcg_ctx* ctx) { return ctx ? ctx->c.np : -1; }
+
+int wcg_rebucketize_and_resample(wcg_ctx* ctx) {
+  WCG_CHECK_CTX(ctx);
+  WCG_CALL(ctx, wcg::build_grid(ctx->c), "rebucketize/resample");
+  return device_status(ctx->c, "rebucketize/resample");
+}
+
+#define WCG_NEED_GRID(ctx)                                                     \
+  do {                                                                         \
+    if (!(ctx)->c.have_grid)                                                   \
+      return fail(WCG_ERR_STATE, "no grid: call wcg_rebucketize_and_resample"); \
+  } while (0)
+
+int wcg_map_particle_nodes(wcg_ctx* ctx) {
+  WCG_CHECK_CTX(ctx);
+  WCG_NEED_GRID(ctx);
+  WCG_CALL(ctx, wcg::map_particles_to_grid(ctx->c), "mapParticleNodesAPIC");
+  return device_status(ctx->c, "mapParticleNodesAPIC");
+}
+
+int wcg_step_velocity(wcg_ctx* ctx, double dt) {
+  WCG_CHECK_CTX(ctx);
+  WCG_NEED_GRID(ctx);
+  if (!(dt > 0)) return fail(WCG_ERR_ARG, "dt must be positive");
+  WCG_CALL(ctx, wcg::step_velocity(ctx->c, dt), "stepVelocity");
+  return device_status(ctx->c, "stepVelocity");
+}
+
+int wcg_project_fine(wcg_ctx* ctx, double dt) {
+  WCG_CHECK_CTX(ctx);
+  WCG_NEED_GRID(ctx);
+  if (!(dt > 0)) return fail(WCG_ERR_ARG, "dt must be positive");
+  WCG_CALL(ctx, wcg::project_fine(ctx->c, dt), "projectFine");
+  int s = device_status(ctx->c, "projectFine");
+  if (s) return s;
+  if (!ctx->c.stats.converged)
+    return fail(WCG_ERR_NOT_CONVERGED,
+                "pressure PCG did not converge (residual " +
+                    std::to_string(ctx->c.stats.residual) + ", iterations " +
+                    std::to_string(ctx->c.stats.pcg_iters) + ")");
+  return WCG_OK;
+}
+
+int wcg_apply_pressure_drag_fluid(wcg_ctx* ctx, double dt) {
+  WCG_CHECK_CTX(ctx);
+  WCG_NEED_GRID(ctx);
+  WCG_CALL(ctx, wcg::apply_pressure_and_extrapolate(ctx->c, dt), "applyPressureDragFluid");
+  return device_status(ctx->c, "applyPressureDragFluid");
+}
+
+int wcg_constrain_liquid_velocity(wcg_ctx* ctx) {
+  WCG_CHECK_CTX(ctx);
+  WCG_NEED_GRID(ctx);
+  WCG_CALL(ctx, wcg::constrain_liquid_velocity(ctx->c), "constrainLiquidVelocity");
+  return device_status(ctx->c, "constrainLiquidVelocity");
+}
+
+int wcg_map_node_particles(wcg_ctx* ctx) {
+  WCG_CHECK_CTX(ctx);
+  WCG_NEED_GRID(ctx);
+  WCG_CALL(ctx, wcg::map_grid_to_particles_and_advect(ctx->c, 0.0, false),
+           "mapNodeParticlesAPIC");
+  return device_status(ctx->c, "mapNodeParticlesAPIC");
+}
+
+int wcg_advect(wcg_ctx* ctx, double dt) {
+  WCG_CHECK_CTX(ctx);
+  WCG_CALL(ctx, wcg::advect_only(ctx->c, dt), "advectScene");
+  ctx->c.have_grid = false;
+  return device_status(ctx->c, "advectScene");
+}
+
+int wcg_substep(wcg_ctx* ctx, double dt) {
+  WCG_CHECK_CTX(ctx);
+  if (!(dt > 0)) return fail(WCG_ERR_ARG, "dt must be positive");
+  WCG_CALL(ctx, wcg::substep(ctx->c, dt), "substep");
+  int s = device_status(ctx->c, "substep");
+  if (s) return s;
+  ctx->c.have_grid = false;
+  if (!ctx->c.stats.converged)
+    return fail(WCG_ERR_NOT_CONVERGED, "pressure PCG did not converge");
+  return WCG_OK;
+}
+
+int wcg_num_substeps(wcg_ctx* ctx, double dt, int* n_out) {
+  WCG_CHECK_CTX(ctx);
+  if (!n_out || !(dt > 0)) return fail(WCG_ERR_ARG, "bad argument");
+  WCG_CALL(ctx, wcg::num_substeps(ctx->c, dt, n_out), "num_substeps");
+  return WCG_OK;
+}
+
+int wcg_step(wcg_ctx* ctx, double dt, int* substeps_out) {
+  WCG_CHECK_CTX(ctx);
+  if (!(dt > 0)) return fail(WCG_ERR_ARG, "dt must be positive");
+  int n = 1;
+  WCG_CALL(ctx, wcg::num_substeps(ctx->c, dt, &n), "num_substeps");
+  const double sub = dt / (double)n;
+  int status = WCG_OK;
+  for (int k = 0; k < n; ++k) {
+    int s = wcg_substep(ctx, sub);
+    if (s == WCG_ERR_NOT_CONVERGED) {
+      status = s;  // the reference warns and continues (Pressure.cpp:803-811)
+      continue;
+    }
+    if (s) return s;
+  }
+  ctx->c.stats.substeps = n;
+  if (substeps_out) *substeps_out = n;
+  return status;
+}
+
+int wcg_get_stats(const wcg_ctx* ctx, wcg_stats* out) {
+  if (!ctx || !out) return fail(WCG_ERR_ARG, "null argument");
+  const wcg::Stats& s = ctx->c.stats;
+  out->substeps = s.substeps;
+  out->pcg_iters = s.pcg_iters;
+  out->refinements = s.refinements;
+  out->converged = s.converged;
+  out->residual = s.residual;
+  out->rhs_norm = s.rhs_norm;
+  out->ndof = s.ndof;
+  out->nactive_buckets = s.nactive;
+  return WCG_OK;
+}
+
+int wcg_grid_info(const wcg_ctx* ctx, int* dims, double* origin, double* bbx) {
+  if (!ctx) return fail(WCG_ERR_ARG, "null context");
+  if (!ctx->c.have_grid && ctx->c.g.nb == 0) return fail(WCG_ERR_STATE, "no grid");
+  const wcg::GridDesc& g = ctx->c.g;
+  if (dims) {
+    dims[0] = g.ni;
+    dims[1] = g.nj;
+    dims[2] = g.nk;
+  }
+  if (origin) {
+    origin[0] = g.ox;
+    origin[1] = g.oy;
+    origin[2] = g.oz;
+  }
+  if (bbx)
+    for (int a = 0; a < 3; ++a) {
+      bbx[a] = ctx->c.bbx_min[a];
+      bbx[3 + a] = ctx->c.bbx_max[a];
+    }
+  return WCG_OK;
+}
+
+long long wcg_field_size(wcg_ctx* ctx, const char* name) {
+  if (!ctx || !name) return -1;
+  const wcg::Context& c = ctx->c;
+  if (lookup_field(name) >= -1) return c.g.nnode;
+  if (!strcmp(name, "active")) return c.g.nb;
+  if (!strcmp(name, "dof_index") || !strcmp(name, "valid_x") ||
+      !strcmp(name, "valid_y") || !strcmp(name, "valid_z"))
+    return c.g.nnode;
+  if (!strcmp(name, "array_idx")) return c.np;
+  if (!strcmp(name, "array_sup")) return 2 * c.g.nb;
+  if (!strcmp(name, "stencil_base")) return 15 * c.np;
+  if (!strcmp(name, "grid_dims")) return 3;
+  return -1;
+}
+
+int wcg_download_field(wcg_ctx* ctx, const char* name, double* out, long long n) {
+  WCG_CHECK_CTX(ctx);
+  if (!name || !out) return fail(WCG_ERR_ARG, "null argument");
+  wcg::Context& c = ctx->c;
+  const int f = lookup_field(name);
+  if (f < -1) return fail(WCG_ERR_ARG, std::string("unknown field ") + name);
+  if (n < c.g.nnode) return fail(WCG_ERR_ARG, "output buffer too small");
+  cudaStreamSynchronize(c.stream);
+  std::vector<double> v = host_field(c, f);
+  std::vector<unsigned char> act = host_active(c);
+  const double nan = std::numeric_limits<double>::quiet_NaN();
+  for (long long i = 0; i < c.g.nnode; ++i) out[i] = act[i >> 6] ? v[i] : nan;
+  cudaError_t e = cudaGetLastError();
+  return cuda_status(c, e, "download_field");
+}
+
+int wcg_download_ifield(wcg_ctx* ctx, const char* name, long long* out, long long n) {
+  WCG_CHECK_CTX(ctx);
+  if (!name || !out) return fail(WCG_ERR_ARG, "null argument");
+  wcg::Context& c = ctx->c;
+  const long long need = wcg_field_size(ctx, name);
+  if (need < 0) return fail(WCG_ERR_ARG, std::string("unknown field ") + name);
+  if (n < need) return fail(WCG_ERR_ARG, "output buffer too small");
+  cudaStreamSynchronize(c.stream);
+  const wcg::GridDesc& g = c.g;
+  if (!strcmp(name, "grid_dims")) {
+    out[0] = g.ni;
+    out[1] = g.nj;
+    out[2] = g.nk;
+    return WCG_OK;
+  }
+  if (!strcmp(name, "active")) {
+    std::vector<unsigned char> a = host_active(c);
+    for (long long i = 0; i < g.nb; ++i) out[i] = a[i];
+    return WCG_OK;
+  }
+  if (!strcmp(name, "dof_index")) {
+    std::vector<unsigned char> a = host_active(c);
+    std::vector<unsigned char> d = host_bytes(c.gdof.p, g.nnode);
+    long long k = 0;
+    for (long long i = 0; i < g.nnode; ++i) {
+      if (!a[i >> 6]) out[i] = -2;
+      else out[i] = d[i] ? k++ : -1;
+    }
+    return WCG_OK;
+  }
+  if (!strncmp(name, "valid_", 6)) {
+    const int comp = name[6] - 'x';
+    std::vector<unsigned char> a = host_active(c);
+    std::vector<unsigned char> v =
+        host_bytes((const unsigned char*)c.gvalid.p + (size_t)comp * c.gcap, g.nnode);
+    for (long long i = 0; i < g.nnode; ++i) out[i] = a[i >> 6] ? v[i] : -1;
+    return WCG_OK;
+  }
+  const long long np = c.np;
+  std::vector<int> pid(np), pb(np), dl(np);
+  std::vector<long long> key(np);
+  if (np) {
+    cudaMemcpy(pid.data(), c.pid[c.cur].p, np * sizeof(int), cudaMemcpyDeviceToHost);
+    cudaMemcpy(pb.data(), c.pbucket.as<int>() + c.cur * c.pcap, np * sizeof(int),
+               cudaMemcpyDeviceToHost);
+    cudaMemcpy(dl.data(), c.pdelta.as<int>() + c.cur * c.pcap, np * sizeof(int),
+               cudaMemcpyDeviceToHost);
+    cudaMemcpy(key.data(), c.pkey.as<long long>() + c.cur * c.pcap, np * sizeof(long long),
+               cudaMemcpyDeviceToHost);
+  }
+  if (!strcmp(name, "array_idx") || !strcmp(name, "array_sup")) {
+    // Sorter::sort keys (bucket << 32 | particle), sorted
+    std::vector<unsigned long long> keys(np);
+    for (long long s = 0; s < np; ++s)
+      keys[s] = ((unsigned long long)(unsigned)pb[s] << 32) | (unsigned)pid[s];
+    std::sort(keys.begin(), keys.end());
+    if (!strcmp(name, "array_idx")) {
+      for (long long s = 0; s < np; ++s) out[s] = (long long)keys[s];
+    } else {
+      for (long long b = 0; b < 2 * g.nb; ++b) out[b] = 0;
+      for (long long s = 0; s < np; ++s) {
+        const long long b = (long long)(keys[s] >> 32);
+        if (s == 0 || (long long)(keys[s - 1] >> 32) != b) out[2 * b] = s;
+        if (s == np - 1 || (long long)(keys[s + 1] >> 32) != b) out[2 * b + 1] = s + 1;
+      }
+    }
+    return WCG_OK;
+  }
+  if (!strcmp(name, "stencil_base")) {
+    for (long long s = 0; s < np; ++s) {
+      const long long k = key[s];
+      const long long b = k >> 6;
+      const int l = (int)(k & 63);
+      const long long bk = b / ((long long)g.ni * g.nj);
+      const long long rem = b - bk * g.ni * g.nj;
+      const long long bj = rem / g.ni;
+      const long long bi = rem - bj * g.ni;
+      const long long P[3] = {bi * 4 + (l & 3) - 1, bj * 4 + ((l >> 2) & 3) - 1,
+                              bk * 4 + (l >> 4) - 1};
+      long long d[3];
+      for (int a = 0; a < 3; ++a) d[a] = ((dl[s] >> (4 * a)) & 15) - 4;
+      long long* o = out + (long long)pid[s] * 15;
+      for (int t = 0; t < 5; ++t)
+        for (int a = 0; a < 3; ++a) {
+          const bool zero = (t == 3) || (t == a);
+          o[t * 3 + a] = P[a] + (zero ? d[a] : 0);
+        }
+    }
+    return WCG_OK;
+  }
+  return fail(WCG_ERR_ARG, std::string("unknown field ") + name);
+}
+
+int wcg_export_pressure_system(wcg_ctx* ctx, long long* ndof, long long* nnz,
+                               long long* rowstart, long long* col, double* val,
+                               double* rhs) {
+  WCG_CHECK_CTX(ctx);
+  WCG_NEED_GRID(ctx);
+  wcg::Context& c = ctx->c;
+  cudaStreamSynchronize(c.stream);
+  const wcg::GridDesc& g = c.g;
+  std::vector<unsigned char> a = host_active(c);
+  std::vector<unsigned char> d = host_bytes(c.gdof.p, g.nnode);
+  std::vector<double> AD = host_field(c, wcg::G_ADIAG), AX = host_field(c, wcg::G_AX),
+                      AY = host_field(c, wcg::G_AY), AZ = host_field(c, wcg::G_AZ),
+                      B = host_field(c, wcg::G_B);
+  std::vector<long long> num((size_t)g.nnode, -1);
+  long long k = 0;
+  for (long long i = 0; i < g.nnode; ++i)
+    if (a[i >> 6] && d[i]) num[i] = k++;
+  auto lin = [&](int I, int J, int K) -> long long {
+    if (I < 0 || J < 0 || K < 0 || I >= g.NI || J >= g.NJ || K >= g.NK) return -1;
+    const long long q = wcg::node_linear(g, I, J, K);
+    return num[q];
+  };
+  // Structural entries come from the assembly flags (bit1-3: +x/+y/+z
+  // coupling, bit4: diagonal); values may be exact zeros.
+  long long nz = 0;
+  std::vector<std::pair<long long, double>> row;
+  for (long long i = 0; i < g.nnode; ++i) {
+    if (num[i] < 0) continue;
+    int I, J, K;
+    {
+      const long long b = i >> 6;
+      const int l = (int)(i & 63);
+      const long long bk = b / ((long long)g.ni * g.nj);
+      const long long rem = b - bk * g.ni * g.nj;
+      const long long bj = rem / g.ni;
+      const long long bi = rem - bj * g.ni;
+      I = (int)(bi * 4 + (l & 3));
+      J = (int)(bj * 4 + ((l >> 2) & 3));
+      K = (int)(bk * 4 + (l >> 4));
+    }
+    row.clear();
+    if (d[i] & 16) row.push_back({num[i], AD[i]});
+    const long long nl[6] = {lin(I - 1, J, K), lin(I + 1, J, K), lin(I, J - 1, K),
+                             lin(I, J + 1, K), lin(I, J, K - 1), lin(I, J, K + 1)};
+    const long long lo[3] = {I > 0 ? wcg::node_linear(g, I - 1, J, K) : -1,
+                             J > 0 ? wcg::node_linear(g, I, J - 1, K) : -1,
+                             K > 0 ? wcg::node_linear(g, I, J, K - 1) : -1};
+    const double* AA[3] = {AX.data(), AY.data(), AZ.data()};
+    for (int a = 0; a < 3; ++a) {
+      if (nl[2 * a] >= 0 && (d[lo[a]] & (2 << a)))
+        row.push_back({nl[2 * a], AA[a][lo[a]]});
+      if (nl[2 * a + 1] >= 0 && (d[i] & (2 << a))) row.push_back({nl[2 * a + 1], AA[a][i]});
+    }
+    std::sort(row.begin(), row.end(),
+              [](const std::pair<long long, double>& x, const std::pair<long long, double>& y) {
+                return x.first < y.first;
+              });
+    const long long r = num[i];
+    if (rowstart) {
+      rowstart[r] = nz;
+      for (auto& e : row) {
+        col[nz] = e.first;
+        val[nz] = e.second;
+        ++nz;
+      }
+      if (rhs) rhs[r] = B[i];
+    } else {
+      nz += (long long)row.size();
+    }
+  }
+  if (rowstart) rowstart[k] = nz;
+  if (ndof) *ndof = k;
+  if (nnz) *nnz = nz;
+  c.stats.ndof = k;
+  return WCG_OK;
+}
+
+void* wcg_stream(const wcg_ctx* ctx) { return ctx ? (void*)ctx->c.stream : nullptr; }
+
+long long wcg_launch_count(const wcg_ctx* ctx) { return ctx ? ctx->c.launches : -1; }
+
+int wcg_profile_begin(wcg_ctx* ctx) {
+  WCG_CHECK_CTX(ctx);
+  wcg::Context& c = ctx->c;
+  cudaStreamSynchronize(c.stream);
+  for (auto& r : c.prof_recs) {
+    c.prof_pool.push_back(r.a);
+    c.prof_pool.push_back(r.b);
+  }
+  c.prof_recs.clear();
+  c.prof_on = true;
+  return WCG_OK;
+}
+
+int wcg_profile_end(wcg_ctx* ctx, double* ms, long long* launches, int ncat) {
+  WCG_CHECK_CTX(ctx);
+  wcg::Context& c = ctx->c;
+  c.prof_on = false;
+  WCG_CALL(ctx, cudaStreamSynchronize(c.stream), "profile_end");
+  for (int k = 0; k < ncat; ++k) {
+    if (ms) ms[k] = 0;
+    if (launches) launches[k] = 0;
+  }
+  for (auto& r : c.prof_recs) {
+    float t = 0;
+    cudaEventElapsedTime(&t, r.a, r.b);
+    if (r.cat < ncat) {
+      if (ms) ms[r.cat] += t;
+      if (launches) launches[r.cat] += r.nlaunch;
+    }
+    c.prof_pool.push_back(r.a);
+    c.prof_pool.push_back(r.b);
+  }
+  c.prof_recs.clear();
+  return WCG_OK;
+}
+
+int wcg_profile_num_phases(void) { return wcg::kNumProfCats; }
+
+const char* wcg_profile_phase_name(int i) {
+  static const char* names[] = {"grid_build_sort", "p2g", "grid_ops", "mic_factor",
+                                "mic_sweep", "pcg_vector", "refine_fp64", "g2p_advect",
+                                "other"};
+  return (i >= 0 && i < wcg::kNumProfCats) ? names[i] : "";
+}
+
+}  // extern "C"

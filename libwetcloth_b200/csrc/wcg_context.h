@@ -1,0 +1,210 @@
+// Device state of one scene and the host-side orchestration of the fluid step.
+// Everything here is internal to libwcgpu.so; the public surface is the C-ABI
+// in include/wetcloth_gpu.h.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "wcg_common.cuh"
+
+namespace wcg {
+
+struct Params {
+  double dx;
+  double gravity[3];
+  double liquid_density;
+  double flip_coeff;
+  double liquid_boundary_friction;
+  double box_center[3];
+  double box_half[3];
+  double box_radius;
+  int walls;
+  double criterion;
+  int maxiters;
+  int precision;  // 0: FP64, 1: FP32 transfers + FP32 PCG with FP64 refinement
+  double refine_inner_tol;  // relative tolerance of each FP32 inner solve
+  int max_refinements;
+};
+
+// A device allocation that grows and never shrinks.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  cudaError_t ensure(size_t n);
+  void release();
+  template <typename T>
+  T* as() const { return (T*)p; }
+};
+
+// Per-step solver and step statistics.
+struct Stats {
+  int substeps = 0;
+  int pcg_iters = 0;          // total inner PCG iterations of the last solve
+  int refinements = 0;        // FP64 outer iterations of the last solve
+  double residual = 0;        // final ||b - A p||_inf of the last solve
+  double rhs_norm = 0;        // ||b||_inf of the last solve
+  int converged = 1;
+  long long ndof = 0;
+  long long nactive = 0;
+};
+
+// Names of the particle columns (SoA, sorted order).
+enum PCol : int {
+  PX = 0, PY, PZ, VX, VY, VZ,
+  C00, C01, C02, C10, C11, C12, C20, C21, C22,
+  PM, PV, PR,
+  kNumPCols
+};
+
+// Dense grid field identifiers (nnode values each).
+enum GField : int {
+  // faces, component-major: field + 0/1/2 for x/y/z
+  G_MASS = 0,          // m_node_mass_fluid_{x,y,z}
+  G_VEL = 3,           // m_node_vel_fluid_{x,y,z} after P2G
+  G_VOL = 6,           // m_node_vol_fluid_{x,y,z}
+  G_SAT = 9,           // m_node_sat_{x,y,z}
+  G_WEIGHT = 12,       // m_node_solid_weight_{x,y,z}
+  G_VSTAR = 15,        // m_node_v_fluid_plus after stepVelocity
+  G_RHS = 18,          // m_node_rhs_fluid
+  G_INVC = 21,         // m_node_inv_C
+  G_PSIFS = 24,        // m_node_psi_fs
+  G_U = 27,            // final face velocity (after projection/extrapolation)
+  G_UTMP = 30,         // extrapolation double buffer
+  // cells
+  G_LPHI = 33,         // m_node_liquid_phi
+  G_SATP = 34,         // m_node_sat_p
+  G_SPHI = 35,         // m_node_solid_phi (corner nodes)
+  G_PRESSURE = 36,     // m_node_pressure
+  G_ADIAG = 37,        // Poisson matrix diagonal
+  G_AX = 38,           // coupling to the +x neighbour
+  G_AY = 39,
+  G_AZ = 40,
+  G_B = 41,            // rhs (divergence)
+  G_INVDIAG = 42,      // MIC(0) 1/L_ii
+  G_R = 43, G_Z = 44, G_S = 45, G_Q = 46, G_X = 47,
+  G_S2 = 48,           // second search-direction buffer (ping-pong)
+  G_Y = 49,            // forward-sweep output L^{-1} r
+  G_SX = 50,           // MIC(0) scaled couplings S_a = A_a * invdiag
+  G_SY = 51,
+  G_SZ = 52,
+  kNumGFields = 53
+};
+
+struct Context {
+  Params prm;
+  cudaStream_t stream = nullptr;
+  int device = 0;
+  std::string last_error;
+
+  // particles
+  long long np = 0;
+  long long pcap = 0;
+  DevBuf pbuf[2];          // kNumPCols * pcap Reals each (ping-pong)
+  int cur = 0;             // which pbuf holds the sorted state
+  DevBuf pid[2];           // original particle index, int32
+  DevBuf pkey;             // key node (p-stencil centre), int64
+  DevBuf pdelta;           // packed stencil offsets, int32
+  DevBuf pbucket;          // reference bucket index, int32
+  DevBuf perm;             // sorted slot -> source slot, int32
+  DevBuf hostorder;        // scratch for downloads in original order
+
+  // grid
+  GridDesc g{};
+  bool have_grid = false;
+  double bbx_min[3] = {0, 0, 0}, bbx_max[3] = {0, 0, 0};
+  DevBuf active_pre, active;     // uint8 per bucket
+  DevBuf cell_start;             // int32 per node + 1
+  DevBuf cell_cursor;            // int32 per node
+  DevBuf gfield;                 // kNumGFields * gcap Reals
+  DevBuf gvalid;                 // 3 * gcap uint8 (+3 tmp)
+  DevBuf gdof;                   // uint8 per node
+  long long gcap = 0;            // nodes allocated per field
+  DevBuf wave_list;              // active 8^3-cell tiles ordered by ti+tj+tk
+  DevBuf wave_count;             // per wave index
+  DevBuf tile_flag;              // int per tile (epoch of completion)
+  DevBuf tile_active;            // uint8 per tile
+  DevBuf tile_part;              // per-ticket partial sums / maxima (double)
+  int tile_epoch = 0;
+  int nti = 0, ntj = 0, ntk = 0; // tiles per axis (2x2x2 buckets each)
+  long long n_tiles = 0;         // active tiles
+  long long n_active = 0;
+  int drange_h[6] = {0, 0, 0, 1, 1, 1};  // min/max stencil offset per axis
+  DevBuf active_list;            // compacted active buckets (int32)
+
+  // FP64 refinement vectors (precision 1)
+  DevBuf rx64, rr64, rb64;       // nnode doubles each
+
+  // reductions / scratch
+  DevBuf scratch;                // scan tiles and reduction partials
+  DevBuf dscalars;               // device scalars (doubles)
+  double* hscalars = nullptr;    // pinned mirror
+  DevBuf derr;                   // device error word
+  DevBuf ticket;                 // wavefront ticket counters
+
+  Stats stats;
+
+  // launch accounting and optional per-phase CUDA-event timing
+  long long launches = 0;
+  bool prof_on = false;
+  struct ProfRec {
+    int cat;
+    int nlaunch;
+    cudaEvent_t a, b;
+  };
+  std::vector<ProfRec> prof_recs;
+  std::vector<cudaEvent_t> prof_pool;
+
+  int real_bytes() const { return prm.precision == 0 ? 8 : 4; }
+};
+
+// Timed phases (wcg_profile_*): each groups the kernels of one reference call.
+enum ProfCat : int {
+  P_GRID = 0,      // bbox, particle pass, activation, sort, gather
+  P_P2G = 1,       // P2G gather + liquid phi + solid phi/weights
+  P_GRIDOPS = 2,   // predict, assembly, pressure gradient, extrapolation, constraint
+  P_MICFACTOR = 3, // MIC(0) factorisation wavefront
+  P_MICSWEEP = 4,  // forward/backward triangular-solve wavefronts
+  P_PCGVEC = 5,    // SpMV, dots, norms, vector updates
+  P_REFINE = 6,    // FP64 residual / refinement kernels
+  P_G2P = 7,       // G2P + advection
+  P_OTHER = 8,     // CFL reduction, uploads/downloads
+  kNumProfCats = 9
+};
+
+// RAII scope recording CUDA events around the kernels of one phase.
+struct ProfScope {
+  Context& c;
+  int cat;
+  long long l0;
+  cudaEvent_t a = nullptr;
+  ProfScope(Context& cc, int category);
+  ~ProfScope();
+};
+
+// ---- orchestration (defined in the .cu files) -------------------------------
+cudaError_t ctx_init(Context& c);
+void ctx_free(Context& c);
+cudaError_t upload_particles(Context& c, long long n, const double* x3,
+                             const double* v3, const double* C9,
+                             const double* mass, const double* vol,
+                             const double* radius, bool device_ptrs);
+cudaError_t download_particles(Context& c, double* x3, double* v3, double* C9,
+                               bool device_ptrs);
+
+// reference call sequence
+cudaError_t build_grid(Context& c);                 // bbox + rebucketize + resampleNodes
+cudaError_t map_particles_to_grid(Context& c);      // weights, liquid phi, solid phi/weights, P2G, sat/psi
+cudaError_t step_velocity(Context& c, double dt);
+cudaError_t project_fine(Context& c, double dt);
+cudaError_t apply_pressure_and_extrapolate(Context& c, double dt);
+cudaError_t constrain_liquid_velocity(Context& c);
+cudaError_t map_grid_to_particles_and_advect(Context& c, double dt, bool advect);
+cudaError_t advect_only(Context& c, double dt);
+cudaError_t num_substeps(Context& c, double dt, int* n);
+cudaError_t substep(Context& c, double dt);
+
+}  // namespace wcg

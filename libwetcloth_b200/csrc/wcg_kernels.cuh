@@ -1,0 +1,723 @@
+// Kernels of the fluid step, templated on the arithmetic type R (double for
+// the FP64 form, float for the mixed-precision form).  Every kernel cites the
+// reference routine whose arithmetic it restates.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "wcg_common.cuh"
+#include "wcg_context.h"
+
+namespace wcg {
+
+// ---- precision-specific rounding helpers ------------------------------------
+__device__ inline double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ inline double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+__device__ inline double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ inline double div_rn(double a, double b) { return __ddiv_rn(a, b); }
+__device__ inline float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ inline float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ inline float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ inline float div_rn(float a, float b) { return __fdiv_rn(a, b); }
+
+template <typename R>
+__device__ inline R coord(R origin, R bs, R dx, int node, R offset) {
+  const int h = node >> 2;
+  const int l = node & 3;
+  R c = add_rn(mul_rn((R)h, bs), origin);
+  c = add_rn(c, mul_rn((R)l, dx));
+  return add_rn(c, mul_rn(offset, dx));
+}
+
+// Stencil base node of one axis, as TwoDScene::findNodes
+// (TwoDScene.cpp:3692-3715): local = (x - corner)/dx with
+// corner = (handle*bs + origin) + offset*dx; base = handle*4 + floor(local)
+// + (frac(local) > 0.5 ? 0 : -1).
+template <typename R>
+__device__ inline int stencil_base(R x, R origin, R bs, R dx, int handle,
+                                   R offset) {
+  R corner = add_rn(mul_rn((R)handle, bs), origin);
+  corner = add_rn(corner, mul_rn(offset, dx));
+  const R lp = div_rn(sub_rn(x, corner), dx);
+  const R fl = floor(lp);
+  const R fr = sub_rn(lp, fl);
+  return handle * 4 + (int)fl + (fr > R(0.5) ? 0 : -1);
+}
+
+struct DeltaRange {
+  int lo[3];
+  int hi[3];
+};
+
+// packed per-particle stencil offsets: delta_a = base(offset 0) - base(offset
+// 0.5) on axis a, stored as delta+4 in 4 bits per axis.
+__device__ inline int unpack_delta(int packed, int axis) {
+  return ((packed >> (4 * axis)) & 15) - 4;
+}
+
+// ---- particle pass: buckets, stencil bases, activation, cell counts ---------
+// Sorter::sort key (Sorter.h:126-140, TwoDScene::rebucketizeParticles
+// :1694-1699), findNodes activation (TwoDScene.cpp:3683-3760) for the u, v, w,
+// solid-phi and pressure stencils of every (soft) liquid particle.
+template <typename R>
+__global__ void k_particle_prepass(GridDesc g, const R* __restrict__ P,
+                                   long long pcap, long long np,
+                                   long long* __restrict__ key,
+                                   int* __restrict__ delta,
+                                   int* __restrict__ pbucket,
+                                   unsigned char* __restrict__ active_pre,
+                                   int* __restrict__ cell_count,
+                                   int* __restrict__ drange, int* err) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = i < np;
+  int d[3] = {0, 0, 0};
+  int dmin[3] = {1 << 20, 1 << 20, 1 << 20}, dmax[3] = {-(1 << 20), -(1 << 20), -(1 << 20)};
+  if (live) {
+    const R org[3] = {(R)g.ox, (R)g.oy, (R)g.oz};
+    const int nbk[3] = {g.ni, g.nj, g.nk};
+    const R bs = (R)g.bs, dx = (R)g.dx;
+    int b0[3], b5[3], bh[3];
+    for (int a = 0; a < 3; ++a) {
+      const R x = P[(PX + a) * pcap + i];
+      int h = (int)floor(div_rn(sub_rn(x, org[a]), bs));
+      h = h < 0 ? 0 : (h > nbk[a] - 1 ? nbk[a] - 1 : h);
+      bh[a] = h;
+      b0[a] = stencil_base<R>(x, org[a], bs, dx, h, R(0));
+      b5[a] = stencil_base<R>(x, org[a], bs, dx, h, R(0.5));
+    }
+    pbucket[i] = (bh[2] * g.nj + bh[1]) * g.ni + bh[0];
+    int packed = 0;
+    for (int a = 0; a < 3; ++a) {
+      d[a] = b0[a] - b5[a];
+      dmin[a] = dmax[a] = d[a];
+      const int dc = d[a] < -4 ? -4 : (d[a] > 11 ? 11 : d[a]);
+      packed |= (dc + 4) << (4 * a);
+    }
+    delta[i] = packed;
+    const int KX = b5[0] + 1, KY = b5[1] + 1, KZ = b5[2] + 1;
+    if (!in_grid(g, KX, KY, KZ)) {
+      record_error(err, kErrIndex);
+      key[i] = -1;
+    } else {
+      const long long k = node_linear(g, KX, KY, KZ);
+      key[i] = k;
+      atomicAdd(&cell_count[k], 1);
+    }
+    // activation of the buckets under the five 3x3x3 stencils
+    for (int t = 0; t < 5; ++t) {
+      // offsets: u(0,.5,.5) v(.5,0,.5) w(.5,.5,0) solid-phi(0,0,0) p(.5,.5,.5)
+      int lo[3];
+      for (int a = 0; a < 3; ++a) {
+        const bool zero = (t == 3) || (t == a);
+        lo[a] = zero ? b0[a] : b5[a];
+      }
+      const int bx0 = lo[0] >> 2, bx1 = (lo[0] + 2) >> 2;
+      const int by0 = lo[1] >> 2, by1 = (lo[1] + 2) >> 2;
+      const int bz0 = lo[2] >> 2, bz1 = (lo[2] + 2) >> 2;
+      for (int bz = bz0; bz <= bz1; ++bz)
+        for (int by = by0; by <= by1; ++by)
+          for (int bx = bx0; bx <= bx1; ++bx) {
+            if (bx < 0 || by < 0 || bz < 0 || bx >= g.ni || by >= g.nj ||
+                bz >= g.nk) {
+              record_error(err, kErrIndex);
+              continue;
+            }
+            const long long b = ((long long)bz * g.nj + by) * g.ni + bx;
+            if (!active_pre[b]) active_pre[b] = 1;
+          }
+    }
+  }
+  // stencil-offset range: one atomic per warp and axis
+  for (int a = 0; a < 3; ++a) {
+    const int mn = __reduce_min_sync(0xffffffffu, dmin[a]);
+    const int mx = __reduce_max_sync(0xffffffffu, dmax[a]);
+    if ((threadIdx.x & 31) == 0) {
+      if (mn < (1 << 20)) atomicMin(&drange[a], mn);
+      if (mx > -(1 << 20)) atomicMax(&drange[3 + a], mx);
+    }
+  }
+}
+
+// expandFluidNodesMarked(1) (TwoDScene.cpp:5021-5064): a bucket becomes active
+// if any of its 26 neighbours was active before the pass.
+__global__ void k_dilate(GridDesc g, const unsigned char* __restrict__ pre,
+                         unsigned char* __restrict__ act) {
+  const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= g.nb) return;
+  const int bk = (int)(b / ((long long)g.ni * g.nj));
+  const int rem = (int)(b - (long long)bk * g.ni * g.nj);
+  const int bj = rem / g.ni;
+  const int bi = rem - bj * g.ni;
+  unsigned char a = pre[b];
+  for (int t = -1; t <= 1 && !a; ++t)
+    for (int s = -1; s <= 1 && !a; ++s)
+      for (int r = -1; r <= 1 && !a; ++r) {
+        const int x = bi + r, y = bj + s, z = bk + t;
+        if (x < 0 || y < 0 || z < 0 || x >= g.ni || y >= g.nj || z >= g.nk)
+          continue;
+        if (pre[((long long)z * g.nj + y) * g.ni + x]) a = 1;
+      }
+  act[b] = a;
+}
+
+__global__ void k_flag_to_int(const unsigned char* __restrict__ f, long long n,
+                              int* __restrict__ out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = f[i] ? 1 : 0;
+}
+
+__global__ void k_compact(const unsigned char* __restrict__ f,
+                          const int* __restrict__ pos, long long n,
+                          int* __restrict__ list) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && f[i]) list[pos[i]] = (int)i;
+}
+
+// active buckets bucketed by wave index bi+bj+bk (wavefront order)
+__global__ void k_wave_count(GridDesc g, const int* __restrict__ active_list,
+                             long long nact, int* __restrict__ wave_count) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nact) return;
+  const int b = active_list[e];
+  const int bk = b / (g.ni * g.nj);
+  const int rem = b - bk * g.ni * g.nj;
+  const int bj = rem / g.ni;
+  const int bi = rem - bj * g.ni;
+  atomicAdd(&wave_count[bi + bj + bk], 1);
+}
+
+__global__ void k_wave_scatter(GridDesc g, const int* __restrict__ active_list,
+                               long long nact, int* __restrict__ wave_cursor,
+                               int* __restrict__ wave_list) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nact) return;
+  const int b = active_list[e];
+  const int bk = b / (g.ni * g.nj);
+  const int rem = b - bk * g.ni * g.nj;
+  const int bj = rem / g.ni;
+  const int bi = rem - bj * g.ni;
+  const int slot = atomicAdd(&wave_cursor[bi + bj + bk], 1);
+  wave_list[slot] = b;
+}
+
+// ---- counting sort by key node ---------------------------------------------
+__global__ void k_sort_scatter(const long long* __restrict__ key, long long np,
+                               const int* __restrict__ start,
+                               int* __restrict__ cursor, int* __restrict__ perm) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= np) return;
+  const long long k = key[i];
+  if (k < 0) return;
+  const int slot = start[k] + atomicAdd(&cursor[k], 1);
+  perm[slot] = (int)i;
+}
+
+// Order each cell's particles by original index so the sorted order (and
+// with it every floating-point sum) is deterministic.
+__global__ void k_sort_cells(const int* __restrict__ start, long long nnode,
+                             const int* __restrict__ pid, int* __restrict__ perm) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nnode) return;
+  const int s0 = start[c], s1 = start[c + 1];
+  for (int a = s0 + 1; a < s1; ++a) {
+    const int v = perm[a];
+    const int kv = pid[v];
+    int b = a - 1;
+    while (b >= s0 && pid[perm[b]] > kv) {
+      perm[b + 1] = perm[b];
+      --b;
+    }
+    perm[b + 1] = v;
+  }
+}
+
+template <typename R>
+__global__ void k_gather_particles(const int* __restrict__ perm, long long np,
+                                   long long pcap, const R* __restrict__ src,
+                                   R* __restrict__ dst,
+                                   const int* __restrict__ pid_src,
+                                   int* __restrict__ pid_dst,
+                                   const long long* __restrict__ key_src,
+                                   long long* __restrict__ key_dst,
+                                   const int* __restrict__ delta_src,
+                                   int* __restrict__ delta_dst,
+                                   const int* __restrict__ pb_src,
+                                   int* __restrict__ pb_dst) {
+  const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= np) return;
+  const int i = perm[s];
+#pragma unroll
+  for (int c = 0; c < kNumPCols; ++c) dst[c * pcap + s] = src[c * pcap + i];
+  pid_dst[s] = pid_src[i];
+  key_dst[s] = key_src[i];
+  delta_dst[s] = delta_src[i];
+  pb_dst[s] = pb_src[i];
+}
+
+// ---- P2G: gather per node ---------------------------------------------------
+// mapParticleNodesAPIC (TwoDScene.cpp:6609-6919), liquid branch:
+//   p_f += (v_a + C.row(a).(x_n - x_p)) * m * w;  m_f += m * w;  V_f += V * w
+//   u_f = p_f / m_f if m_f > 1e-20; psi = 0; sat = clamp(V_f/max(1e-20,dV),0,1)
+// updateLiquidPhi (TwoDScene.cpp:3286-3345) at cell centres and
+// mapParticleSaturationPsiNodes (:5952-5992).  Each node sums the particles
+// whose stencil contains it (exactly the reference's per-node pair lists,
+// buildNodeParticlePairs :2257-2355), visiting them in key-cell order, so the
+// result is deterministic and needs no atomics.
+// Block: one active bucket; threads [0,64) u-faces, [64,128) v-faces,
+// [128,192) w-faces, [192,256) cell centres.
+template <typename R>
+__global__ void __launch_bounds__(256)
+    k_p2g(GridDesc g, const int* __restrict__ active_list,
+          const unsigned char* __restrict__ active, const R* __restrict__ P,
+          long long pcap, const int* __restrict__ start,
+          const int* __restrict__ delta, DeltaRange dr, R* __restrict__ F,
+          long long fstride, Walls walls) {
+  const int b = active_list[blockIdx.x];
+  const int type = threadIdx.x >> 6;
+  const int l = threadIdx.x & 63;
+  const int bk = b / (g.ni * g.nj);
+  const int rem = b - bk * g.ni * g.nj;
+  const int bj = rem / g.ni;
+  const int bi = rem - bj * g.ni;
+  const int I = bi * 4 + (l & 3), J = bj * 4 + ((l >> 2) & 3), K = bk * 4 + (l >> 4);
+  const long long n = (long long)b * 64 + l;
+  const R org[3] = {(R)g.ox, (R)g.oy, (R)g.oz};
+  const R bs = (R)g.bs, dx = (R)g.dx;
+  const R invh = R(1) / dx;
+  const int IJK[3] = {I, J, K};
+  const R* px = P + PX * pcap;
+  const R* py = P + PY * pcap;
+  const R* pz = P + PZ * pcap;
+  const R dV = dx * dx * dx;
+
+  if (type < 3) {
+    const int a = type;
+    R np_[3];
+    for (int q = 0; q < 3; ++q)
+      np_[q] = coord<R>(org[q], bs, dx, IJK[q], q == a ? R(0) : R(0.5));
+    int lo[3], hi[3];
+    for (int q = 0; q < 3; ++q) {
+      if (q == a) {
+        lo[q] = IJK[q] - 1 - dr.hi[q];
+        hi[q] = IJK[q] + 1 - dr.lo[q];
+      } else {
+        lo[q] = IJK[q] - 1;
+        hi[q] = IJK[q] + 1;
+      }
+      lo[q] = lo[q] < 0 ? 0 : lo[q];
+    }
+    hi[0] = hi[0] > g.NI - 1 ? g.NI - 1 : hi[0];
+    hi[1] = hi[1] > g.NJ - 1 ? g.NJ - 1 : hi[1];
+    hi[2] = hi[2] > g.NK - 1 ? g.NK - 1 : hi[2];
+    const R* va = P + (VX + a) * pcap;
+    const R* c0 = P + (C00 + 3 * a) * pcap;
+    const R* c1 = P + (C00 + 3 * a + 1) * pcap;
+    const R* c2 = P + (C00 + 3 * a + 2) * pcap;
+    const R* pm = P + PM * pcap;
+    const R* pv = P + PV * pcap;
+    R mom = 0, mass = 0, vol = 0;
+    for (int KZ = lo[2]; KZ <= hi[2]; ++KZ)
+      for (int KY = lo[1]; KY <= hi[1]; ++KY)
+        for (int KX = lo[0]; KX <= hi[0]; ++KX) {
+          const long long c = node_linear(g, KX, KY, KZ);
+          const int s1 = start[c + 1];
+          const int Ka = a == 0 ? KX : (a == 1 ? KY : KZ);
+          for (int s = start[c]; s < s1; ++s) {
+            const int base = Ka - 1 + unpack_delta(delta[s], a);
+            const int off = IJK[a] - base;
+            if (off < 0 || off > 2) continue;
+            const R x = px[s], y = py[s], z = pz[s];
+            const R w = quad_kernel<R>((x - np_[0]) * invh) *
+                        quad_kernel<R>((y - np_[1]) * invh) *
+                        quad_kernel<R>((z - np_[2]) * invh);
+            if (!(w > R(0))) continue;
+            const R m = pm[s];
+            const R vel = va[s] + (c0[s] * (np_[0] - x) + c1[s] * (np_[1] - y)) +
+                          c2[s] * (np_[2] - z);
+            mom += vel * m * w;
+            mass += m * w;
+            vol += pv[s] * w;
+          }
+        }
+    F[(G_MASS + a) * fstride + n] = mass;
+    F[(G_VEL + a) * fstride + n] = mass > R(1e-20) ? mom / mass : R(0);
+    F[(G_VOL + a) * fstride + n] = vol;
+    const R den = dV > R(1e-20) ? dV : R(1e-20);
+    F[(G_SAT + a) * fstride + n] = clamp01<R>(vol / den);
+  } else {
+    // cell centre: liquid level set + saturation; corner: solid phi
+    R np_[3];
+    for (int q = 0; q < 3; ++q) np_[q] = coord<R>(org[q], bs, dx, IJK[q], R(0.5));
+    const R* pr = P + PR * pcap;
+    const R* pv = P + PV * pcap;
+    const R rmin = dx * (R)kLiquidPhiRadius;
+    R phi = R(3) * bs;
+    R vliq = 0;
+    const int lo0 = I - 1 < 0 ? 0 : I - 1, hi0 = I + 1 > g.NI - 1 ? g.NI - 1 : I + 1;
+    const int lo1 = J - 1 < 0 ? 0 : J - 1, hi1 = J + 1 > g.NJ - 1 ? g.NJ - 1 : J + 1;
+    const int lo2 = K - 1 < 0 ? 0 : K - 1, hi2 = K + 1 > g.NK - 1 ? g.NK - 1 : K + 1;
+    for (int KZ = lo2; KZ <= hi2; ++KZ)
+      for (int KY = lo1; KY <= hi1; ++KY)
+        for (int KX = lo0; KX <= hi0; ++KX) {
+          const long long c = node_linear(g, KX, KY, KZ);
+          const int s1 = start[c + 1];
+          for (int s = start[c]; s < s1; ++s) {
+            const R x = px[s], y = py[s], z = pz[s];
+            const R ddx = x - np_[0], ddy = y - np_[1], ddz = z - np_[2];
+            const R r = pr[s];
+            const R d = sqrt((ddx * ddx + ddy * ddy) + ddz * ddz) -
+                        (rmin > r ? rmin : r);
+            phi = d < phi ? d : phi;
+            const R w = quad_kernel<R>(ddx * invh) * quad_kernel<R>(ddy * invh) *
+                        quad_kernel<R>(ddz * invh);
+            if (w > R(0)) vliq += pv[s] * w;
+          }
+        }
+    const double three_bs = 3.0 * g.bs;
+    const double sphi_c = wall_phi(walls, (double)np_[0], (double)np_[1],
+                                   (double)np_[2], three_bs);
+    if (sphi_c < 0.0) phi = R(-0.5) * dx;
+    F[G_LPHI * fstride + n] = phi;
+    const R den = dV > R(1e-20) ? dV : R(1e-20);
+    F[G_SATP * fstride + n] = clamp01<R>(vliq / den);
+    // solid phi at the corner node (TwoDScene::updateSolidPhi :7940-7960)
+    const double cx = (double)coord<R>(org[0], bs, dx, I, R(0));
+    const double cy = (double)coord<R>(org[1], bs, dx, J, R(0));
+    const double cz = (double)coord<R>(org[2], bs, dx, K, R(0));
+    F[G_SPHI * fstride + n] = (R)wall_phi(walls, cx, cy, cz, three_bs);
+  }
+}
+
+// Solid face weights: updateSolidWeights (TwoDScene.cpp:1871-1962); corner
+// phis of missing corner nodes (outside the grid or in an inactive bucket)
+// default to 0.5*dx.  Corner ordering per connectSolidPhiNodes (:4433-4596).
+template <typename R>
+__global__ void __launch_bounds__(192)
+    k_solid_weights(GridDesc g, const int* __restrict__ active_list,
+                    const unsigned char* __restrict__ active,
+                    R* __restrict__ F, long long fstride, Walls walls) {
+  const int b = active_list[blockIdx.x];
+  const int a = threadIdx.x >> 6;
+  const int l = threadIdx.x & 63;
+  const int bk = b / (g.ni * g.nj);
+  const int rem = b - bk * g.ni * g.nj;
+  const int bj = rem / g.ni;
+  const int bi = rem - bj * g.ni;
+  const int I = bi * 4 + (l & 3), J = bj * 4 + ((l >> 2) & 3), K = bk * 4 + (l >> 4);
+  const long long n = (long long)b * 64 + l;
+  const R org[3] = {(R)g.ox, (R)g.oy, (R)g.oz};
+  const R bs = (R)g.bs, dx = (R)g.dx;
+  const double three_bs = 3.0 * g.bs;
+  R phi[4];
+  for (int r = 0; r < 2; ++r)
+    for (int s = 0; s < 2; ++s) {
+      int ci = I, cj = J, ck = K;
+      if (a == 0) { cj += s; ck += r; }
+      else if (a == 1) { ci += r; ck += s; }
+      else { ci += r; cj += s; }
+      R v = R(0.5) * dx;
+      if (in_grid(g, ci, cj, ck) && active[bucket_of(g, ci, cj, ck)]) {
+        const double cx = (double)coord<R>(org[0], bs, dx, ci, R(0));
+        const double cy = (double)coord<R>(org[1], bs, dx, cj, R(0));
+        const double cz = (double)coord<R>(org[2], bs, dx, ck, R(0));
+        v = (R)wall_phi(walls, cx, cy, cz, three_bs);
+      }
+      phi[r * 2 + s] = v;
+    }
+  F[(G_WEIGHT + a) * fstride + n] =
+      clamp01<R>(R(1) - fraction_inside4<R>(phi[0], phi[1], phi[2], phi[3]));
+}
+
+// stepVelocity for liquid nodes (LinearizedImplicitEuler.cpp:224-337):
+// constructNodeForce (:548-667) with SimpleGravityForce::addLiquidGradEToNode
+// (SimpleGravityForce.cpp:25-52, coeff -dt) and the node momentum;
+// constructHDV/constructInvMDV/constructPsiSF (:846-1149) with no solid
+// (drag 0, Q_s = 1, inv_C = 1/m_f or 1); performLocalSolve (:128-170).
+template <typename R>
+__global__ void __launch_bounds__(192)
+    k_predict(GridDesc g, const int* __restrict__ active_list, R* __restrict__ F,
+              long long fstride, R gx, R gy, R gz, R dt) {
+  const int b = active_list[blockIdx.x];
+  const int a = threadIdx.x >> 6;
+  const long long n = (long long)b * 64 + (threadIdx.x & 63);
+  const R grav = a == 0 ? gx : (a == 1 ? gy : gz);
+  const R m = F[(G_MASS + a) * fstride + n];
+  const R u = F[(G_VEL + a) * fstride + n];
+  R rhs = R(0) - (m * grav) * (-dt);
+  rhs += m * u;
+  const bool heavy = m > R(1e-20);
+  const R invC = heavy ? R(1) / m : R(1);
+  F[(G_RHS + a) * fstride + n] = rhs;
+  F[(G_INVC + a) * fstride + n] = invC;
+  F[(G_VSTAR + a) * fstride + n] = heavy ? rhs / m : rhs;
+  F[(G_PSIFS + a) * fstride + n] = invC * m;
+}
+
+// Pressure system (pressure::solveNodePressure, Core/Pressure.cpp:350-791):
+// DOF iff liquid phi < 0 and some existing face has solid weight > 0; per face
+// rhs += -/+ ((u* psi_fs) w)/dx; if w > 0, term = (w dt/dx^2)(inv_C V_f); a
+// liquid neighbour couples (diag += term, off = -term), an air neighbour adds
+// term/max(fraction_inside(phi_c,phi_n), 0.01) to the diagonal.  Face order
+// left, right, bottom, top, near, far.  Couplings are stored at the lower cell
+// (A_x[c] = A(c, c+x)), giving a matrix-free symmetric 7-point operator.
+template <typename R>
+__global__ void __launch_bounds__(64)
+    k_assemble(GridDesc g, const int* __restrict__ active_list,
+               const unsigned char* __restrict__ active, R* __restrict__ F,
+               long long fstride, unsigned char* __restrict__ dof, R dt) {
+  const int b = active_list[blockIdx.x];
+  const int l = threadIdx.x;
+  const int bk = b / (g.ni * g.nj);
+  const int rem = b - bk * g.ni * g.nj;
+  const int bj = rem / g.ni;
+  const int bi = rem - bj * g.ni;
+  const int I = bi * 4 + (l & 3), J = bj * 4 + ((l >> 2) & 3), K = bk * 4 + (l >> 4);
+  const long long n = (long long)b * 64 + l;
+  const R dx = (R)g.dx;
+  const R coeff = dt / (dx * dx);
+  const R phic = F[G_LPHI * fstride + n];
+  // faces: axis, face node, neighbour cell, sign of the rhs term
+  const int fI[6] = {I, I + 1, I, I, I, I};
+  const int fJ[6] = {J, J, J, J + 1, J, J};
+  const int fK[6] = {K, K, K, K, K, K + 1};
+  const int cI[6] = {I - 1, I + 1, I, I, I, I};
+  const int cJ[6] = {J, J, J - 1, J + 1, J, J};
+  const int cK[6] = {K, K, K, K, K - 1, K + 1};
+  bool exists[6];
+  long long fn[6];
+  bool open = false;
+  for (int f = 0; f < 6; ++f) {
+    exists[f] = in_grid(g, fI[f], fJ[f], fK[f]) &&
+                active[bucket_of(g, fI[f], fJ[f], fK[f])];
+    fn[f] = exists[f] ? node_linear(g, fI[f], fJ[f], fK[f]) : -1;
+    if (exists[f] && F[(G_WEIGHT + (f >> 1)) * fstride + fn[f]] > R(0)) open = true;
+  }
+  const bool isdof = (phic < R(0)) && open;
+  // dof byte: bit0 DOF, bits1-3 a +x/+y/+z coupling entry exists, bit4 a
+  // diagonal entry exists (entries can hold an exact zero when V_f == 0, and
+  // the reference's sparse matrix still stores them).
+  int flags = isdof ? 1 : 0;
+  R diag = 0, rhs = 0, off[3] = {0, 0, 0};
+  if (isdof) {
+    for (int f = 0; f < 6; ++f) {
+      if (!exists[f]) continue;
+      const int a = f >> 1;
+      const long long q = fn[f];
+      const R w = F[(G_WEIGHT + a) * fstride + q];
+      const R t = ((F[(G_VSTAR + a) * fstride + q] * F[(G_PSIFS + a) * fstride + q]) * w) / dx;
+      if (f & 1) rhs -= t; else rhs += t;
+      if (w > R(0)) {
+        const R term = (w * coeff) * (F[(G_INVC + a) * fstride + q] * F[(G_VOL + a) * fstride + q]);
+        if (in_grid(g, cI[f], cJ[f], cK[f]) &&
+            active[bucket_of(g, cI[f], cJ[f], cK[f])]) {
+          const R phin = F[G_LPHI * fstride + node_linear(g, cI[f], cJ[f], cK[f])];
+          flags |= 16;
+          if (phin < R(0)) {
+            diag += term;
+            if (f & 1) {
+              off[a] = -term;
+              flags |= 2 << a;
+            }
+          } else {
+            R theta = fraction_inside2<R>(phic, phin);
+            theta = theta > R(kThetaCriterion) ? theta : R(kThetaCriterion);
+            diag += term / theta;
+          }
+        }
+      }
+    }
+  }
+  dof[n] = (unsigned char)flags;
+  F[G_ADIAG * fstride + n] = diag;
+  F[G_AX * fstride + n] = off[0];
+  F[G_AY * fstride + n] = off[1];
+  F[G_AZ * fstride + n] = off[2];
+  F[G_B * fstride + n] = rhs;
+}
+
+// applyPressureGradsFluidRHS (Pressure.cpp:1137-1314) then performInvLocalSolve
+// (LinearizedImplicitEuler.cpp:65-98): valid iff w > 0 and a side cell is
+// liquid; rhs -= ((p_r - p_l)/(dx theta)) dt V_f;  u = rhs inv_C.
+template <typename R>
+__global__ void __launch_bounds__(192)
+    k_apply_pressure(GridDesc g, const int* __restrict__ active_list,
+                     const unsigned char* __restrict__ active, R* __restrict__ F,
+                     long long fstride, unsigned char* __restrict__ valid, R dt) {
+  const int b = active_list[blockIdx.x];
+  const int a = threadIdx.x >> 6;
+  const int l = threadIdx.x & 63;
+  const int bk = b / (g.ni * g.nj);
+  const int rem = b - bk * g.ni * g.nj;
+  const int bj = rem / g.ni;
+  const int bi = rem - bj * g.ni;
+  const int I = bi * 4 + (l & 3), J = bj * 4 + ((l >> 2) & 3), K = bk * 4 + (l >> 4);
+  const long long n = (long long)b * 64 + l;
+  const R dx = (R)g.dx;
+  R rhs = F[(G_RHS + a) * fstride + n];
+  unsigned char v = 0;
+  const R w = F[(G_WEIGHT + a) * fstride + n];
+  if (w > R(0)) {
+    const int lI = I - (a == 0), lJ = J - (a == 1), lK = K - (a == 2);
+    const bool hl = in_grid(g, lI, lJ, lK) && active[bucket_of(g, lI, lJ, lK)];
+    const bool hr = in_grid(g, I, J, K);  // the cell shares the face's bucket
+    const long long nl = hl ? node_linear(g, lI, lJ, lK) : -1;
+    const R phil = hl ? F[G_LPHI * fstride + nl] : R(0);
+    const R phir = hr ? F[G_LPHI * fstride + n] : R(0);
+    if (phil < R(0) || phir < R(0)) {
+      R theta = 1;
+      if (phir >= R(0) || phil >= R(0)) {
+        theta = fraction_inside2<R>(phil, phir);
+        theta = theta > R(kThetaCriterion) ? theta : R(kThetaCriterion);
+      }
+      R pg = 0;
+      if (hl) pg -= F[G_PRESSURE * fstride + nl];
+      if (hr) pg += F[G_PRESSURE * fstride + n];
+      pg /= (dx * theta);
+      const R term = pg * dt * F[(G_VOL + a) * fstride + n];
+      rhs -= term;
+      v = 1;
+    }
+  }
+  F[(G_RHS + a) * fstride + n] = rhs;
+  F[(G_U + a) * fstride + n] = rhs * F[(G_INVC + a) * fstride + n];
+  valid[a * fstride + n] = v;
+}
+
+// One layer of pressure::extrapolate (Pressure.cpp:1826-1903): an invalid face
+// takes the mean of its valid 6-neighbours (order -x,+x,-y,+y,-z,+z) from the
+// previous layer.
+template <typename R>
+__global__ void __launch_bounds__(192)
+    k_extrapolate(GridDesc g, const int* __restrict__ active_list,
+                  const unsigned char* __restrict__ active,
+                  const R* __restrict__ uin, R* __restrict__ uout,
+                  const unsigned char* __restrict__ vin,
+                  unsigned char* __restrict__ vout, long long fstride) {
+  const int b = active_list[blockIdx.x];
+  const int a = threadIdx.x >> 6;
+  const int l = threadIdx.x & 63;
+  const int bk = b / (g.ni * g.nj);
+  const int rem = b - bk * g.ni * g.nj;
+  const int bj = rem / g.ni;
+  const int bi = rem - bj * g.ni;
+  const int I = bi * 4 + (l & 3), J = bj * 4 + ((l >> 2) & 3), K = bk * 4 + (l >> 4);
+  const long long n = (long long)b * 64 + l;
+  const R* ui = uin + a * fstride;
+  const unsigned char* vi = vin + a * fstride;
+  R out = ui[n];
+  unsigned char vv = vi[n];
+  if (!vv) {
+    R sum = 0;
+    int count = 0;
+    const int dI[6] = {-1, 1, 0, 0, 0, 0};
+    const int dJ[6] = {0, 0, -1, 1, 0, 0};
+    const int dK[6] = {0, 0, 0, 0, -1, 1};
+    for (int r = 0; r < 6; ++r) {
+      const int x = I + dI[r], y = J + dJ[r], z = K + dK[r];
+      if (!in_grid(g, x, y, z) || !active[bucket_of(g, x, y, z)]) continue;
+      const long long q = node_linear(g, x, y, z);
+      if (!vi[q]) continue;
+      sum += ui[q];
+      ++count;
+    }
+    if (count > 0) {
+      out = sum / (R)count;
+      vv = 1;
+    }
+  }
+  uout[a * fstride + n] = out;
+  vout[a * fstride + n] = vv;
+}
+
+// constrainLiquidVelocity (TwoDScene.cpp:1827-1869): faces fully inside the
+// solid (weight 0) blend towards the (static, zero) solid velocity.
+template <typename R>
+__global__ void __launch_bounds__(192)
+    k_constrain(const int* __restrict__ active_list, R* __restrict__ F,
+                long long fstride, R friction) {
+  const int b = active_list[blockIdx.x];
+  const int a = threadIdx.x >> 6;
+  const long long n = (long long)b * 64 + (threadIdx.x & 63);
+  if (F[(G_WEIGHT + a) * fstride + n] == R(0)) {
+    const R u = F[(G_U + a) * fstride + n];
+    const R us = R(0);
+    F[(G_U + a) * fstride + n] = (R(1) - friction) * u + friction * us;
+  }
+}
+
+// G2P + advection (mapNodeParticlesAPIC TwoDScene.cpp:6936-7000 liquid branch,
+// SceneStepper::advectScene SceneStepper.cpp:17-41): over the particle's own
+// 27-node stencils (nodes of inactive buckets skipped),
+//   v_a = sum u w;  C.row(a) = flip * sum u w (x_n - x_p) 4/h^2;  x += v dt.
+template <typename R>
+__global__ void __launch_bounds__(128)
+    k_g2p(GridDesc g, const unsigned char* __restrict__ active, R* __restrict__ P,
+          long long pcap, long long np, const long long* __restrict__ key,
+          const int* __restrict__ delta, const R* __restrict__ F,
+          long long fstride, R flip, R dt, int advect) {
+  const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= np) return;
+  const R org[3] = {(R)g.ox, (R)g.oy, (R)g.oz};
+  const R bs = (R)g.bs, dx = (R)g.dx;
+  const R invh = R(1) / dx;
+  const R invD = R(4) / (dx * dx);
+  const R x = P[PX * pcap + s], y = P[PY * pcap + s], z = P[PZ * pcap + s];
+  const long long kn = key[s];
+  if (kn < 0) return;
+  int KI, KJ, KK;
+  node_ijk(g, kn, KI, KJ, KK);
+  const int kp[3] = {KI - 1, KJ - 1, KK - 1};
+  const int dl = delta[s];
+  R v[3], C[9];
+  for (int a = 0; a < 3; ++a) {
+    int base[3];
+    for (int q = 0; q < 3; ++q) base[q] = kp[q] + (q == a ? unpack_delta(dl, a) : 0);
+    // per-axis node coordinates and weights
+    R cx[3], cy[3], cz[3], wx[3], wy[3], wz[3];
+    for (int t = 0; t < 3; ++t) {
+      cx[t] = coord<R>(org[0], bs, dx, base[0] + t, a == 0 ? R(0) : R(0.5));
+      cy[t] = coord<R>(org[1], bs, dx, base[1] + t, a == 1 ? R(0) : R(0.5));
+      cz[t] = coord<R>(org[2], bs, dx, base[2] + t, a == 2 ? R(0) : R(0.5));
+      wx[t] = quad_kernel<R>((x - cx[t]) * invh);
+      wy[t] = quad_kernel<R>((y - cy[t]) * invh);
+      wz[t] = quad_kernel<R>((z - cz[t]) * invh);
+    }
+    R fv = 0, b0 = 0, b1 = 0, b2 = 0;
+    const R* U = F + (G_U + a) * fstride;
+    for (int k = 0; k < 3; ++k)
+      for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 3; ++i) {
+          const int NI_ = base[0] + i, NJ_ = base[1] + j, NK_ = base[2] + k;
+          if (!in_grid(g, NI_, NJ_, NK_) || !active[bucket_of(g, NI_, NJ_, NK_)])
+            continue;
+          const R un = U[node_linear(g, NI_, NJ_, NK_)];
+          const R w = wx[i] * wy[j] * wz[k];
+          const R uw = un * w;
+          fv += uw;
+          b0 += uw * (cx[i] - x) * invD;
+          b1 += uw * (cy[j] - y) * invD;
+          b2 += uw * (cz[k] - z) * invD;
+        }
+    v[a] = fv;
+    C[a * 3 + 0] = b0 * flip;
+    C[a * 3 + 1] = b1 * flip;
+    C[a * 3 + 2] = b2 * flip;
+  }
+  for (int a = 0; a < 3; ++a) P[(VX + a) * pcap + s] = v[a];
+  for (int q = 0; q < 9; ++q) P[(C00 + q) * pcap + s] = C[q];
+  if (advect) {
+    P[PX * pcap + s] = x + v[0] * dt;
+    P[PY * pcap + s] = y + v[1] * dt;
+    P[PZ * pcap + s] = z + v[2] * dt;
+  }
+}
+
+template <typename R>
+__global__ void k_advect(R* __restrict__ P, long long pcap, long long np, R dt) {
+  const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= np) return;
+  for (int a = 0; a < 3; ++a)
+    P[(PX + a) * pcap + s] = P[(PX + a) * pcap + s] + P[(VX + a) * pcap + s] * dt;
+}
+
+}  // namespace wcg

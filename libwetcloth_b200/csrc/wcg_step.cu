@@ -1,0 +1,966 @@
+// Host orchestration of the fluid step: one function per reference call,
+// dispatching on the precision of the context.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "wcg_context.h"
+#include "wcg_kernels.cuh"
+#include "wcg_pcg.cuh"
+#include "wcg_scan.cuh"
+
+namespace wcg {
+
+#define WCG_TRY(x)                          \
+  do {                                      \
+    cudaError_t e_ = (x);                   \
+    if (e_ != cudaSuccess) return e_;       \
+  } while (0)
+
+cudaError_t DevBuf::ensure(size_t n) {
+  if (n <= bytes && p) return cudaSuccess;
+  if (p) cudaFree(p);
+  p = nullptr;
+  bytes = 0;
+  if (n == 0) return cudaSuccess;
+  cudaError_t e = cudaMalloc(&p, n);
+  if (e == cudaSuccess) bytes = n;
+  return e;
+}
+
+void DevBuf::release() {
+  if (p) cudaFree(p);
+  p = nullptr;
+  bytes = 0;
+}
+
+static inline unsigned nblk(long long n, int t) {
+  return (unsigned)((n + t - 1) / t);
+}
+
+cudaError_t ctx_init(Context& c) {
+  WCG_TRY(cudaGetDevice(&c.device));
+  WCG_TRY(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+  WCG_TRY(cudaMallocHost((void**)&c.hscalars, 64 * sizeof(double)));
+  WCG_TRY(c.dscalars.ensure(64 * sizeof(double)));
+  WCG_TRY(c.derr.ensure(sizeof(int)));
+  WCG_TRY(c.ticket.ensure(16 * sizeof(int)));
+  WCG_TRY(cudaMemsetAsync(c.derr.p, 0, sizeof(int), c.stream));
+  return cudaStreamSynchronize(c.stream);
+}
+
+void ctx_free(Context& c) {
+  DevBuf* bufs[] = {&c.pbuf[0], &c.pbuf[1], &c.pid[0], &c.pid[1], &c.pkey,
+                    &c.pdelta, &c.pbucket, &c.perm, &c.hostorder,
+                    &c.active_pre, &c.active, &c.cell_start, &c.cell_cursor,
+                    &c.gfield, &c.gvalid, &c.gdof, &c.wave_list, &c.wave_count,
+                    &c.tile_flag, &c.active_list, &c.rx64, &c.rr64, &c.rb64,
+                    &c.scratch, &c.dscalars, &c.derr, &c.ticket};
+  for (DevBuf* b : bufs) b->release();
+  if (c.hscalars) cudaFreeHost(c.hscalars);
+  c.hscalars = nullptr;
+  if (c.stream) cudaStreamDestroy(c.stream);
+  c.stream = nullptr;
+}
+
+ProfScope::ProfScope(Context& cc, int category) : c(cc), cat(category), l0(cc.launches) {
+  if (!c.prof_on) return;
+  if (c.prof_pool.empty()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    c.prof_pool.push_back(e);
+  }
+  a = c.prof_pool.back();
+  c.prof_pool.pop_back();
+  cudaEventRecord(a, c.stream);
+}
+
+ProfScope::~ProfScope() {
+  if (!c.prof_on || !a) return;
+  cudaEvent_t b;
+  if (c.prof_pool.empty()) {
+    cudaEventCreate(&b);
+  } else {
+    b = c.prof_pool.back();
+    c.prof_pool.pop_back();
+  }
+  cudaEventRecord(b, c.stream);
+  c.prof_recs.push_back({cat, (int)(c.launches - l0), a, b});
+}
+
+// ---------------------------------------------------------------------------
+// particles
+template <typename R>
+__global__ void k_load_particles(long long n, long long pcap, const double* x3,
+                                 const double* v3, const double* C9,
+                                 const double* m, const double* vol,
+                                 const double* rad, R* P, int* pid) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int a = 0; a < 3; ++a) {
+    P[(PX + a) * pcap + i] = (R)x3[i * 3 + a];
+    P[(VX + a) * pcap + i] = (R)v3[i * 3 + a];
+  }
+  for (int q = 0; q < 9; ++q) P[(C00 + q) * pcap + i] = C9 ? (R)C9[i * 9 + q] : R(0);
+  P[PM * pcap + i] = (R)m[i];
+  P[PV * pcap + i] = (R)vol[i];
+  P[PR * pcap + i] = (R)rad[i];
+  pid[i] = (int)i;
+}
+
+// scatter sorted state back to original particle order (x3, v3, C9 AoS)
+template <typename R>
+__global__ void k_store_particles(long long n, long long pcap, const R* P,
+                                  const int* pid, double* out) {
+  const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const long long i = pid[s];
+  double* o = out + i * 15;
+  for (int a = 0; a < 3; ++a) {
+    o[a] = (double)P[(PX + a) * pcap + s];
+    o[3 + a] = (double)P[(VX + a) * pcap + s];
+  }
+  for (int q = 0; q < 9; ++q) o[6 + q] = (double)P[(C00 + q) * pcap + s];
+}
+
+cudaError_t upload_particles(Context& c, long long n, const double* x3,
+                             const double* v3, const double* C9,
+                             const double* mass, const double* vol,
+                             const double* radius, bool device_ptrs) {
+  const int rb = c.real_bytes();
+  if (n > c.pcap) {
+    const long long cap = n;
+    for (int k = 0; k < 2; ++k) {
+      WCG_TRY(c.pbuf[k].ensure((size_t)kNumPCols * cap * rb));
+      WCG_TRY(c.pid[k].ensure((size_t)cap * sizeof(int)));
+    }
+    WCG_TRY(c.pkey.ensure((size_t)2 * cap * sizeof(long long)));
+    WCG_TRY(c.pdelta.ensure((size_t)2 * cap * sizeof(int)));
+    WCG_TRY(c.pbucket.ensure((size_t)2 * cap * sizeof(int)));
+    WCG_TRY(c.perm.ensure((size_t)cap * sizeof(int)));
+    WCG_TRY(c.hostorder.ensure((size_t)cap * 15 * sizeof(double)));
+    c.pcap = cap;
+  }
+  c.np = n;
+  c.cur = 0;
+  if (n == 0) return cudaSuccess;
+  // stage host arrays into the scratch copy (device side, doubles)
+  double* stage = c.hostorder.as<double>();
+  const double* dx3 = x3;
+  const double* dv3 = v3;
+  const double* dC9 = C9;
+  const double* dm = mass;
+  const double* dvol = vol;
+  const double* drad = radius;
+  if (!device_ptrs) {
+    double* s = stage;
+    WCG_TRY(cudaMemcpyAsync(s, x3, n * 3 * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    dx3 = s; s += n * 3;
+    WCG_TRY(cudaMemcpyAsync(s, v3, n * 3 * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    dv3 = s; s += n * 3;
+    if (C9) {
+      WCG_TRY(cudaMemcpyAsync(s, C9, n * 9 * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+      dC9 = s; s += n * 9;
+    }
+    // mass/vol/radius reuse the pkey buffer (3n doubles fit in 2n int64 + ...)
+    double* t = (double*)c.pkey.p;
+    WCG_TRY(cudaMemcpyAsync(t, mass, n * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    WCG_TRY(cudaMemcpyAsync(t + n, vol, n * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    // radius goes to the delta+bucket buffers viewed as doubles
+    double* t2 = (double*)c.pdelta.p;
+    WCG_TRY(cudaMemcpyAsync(t2, radius, n * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    dm = t;
+    dvol = t + n;
+    drad = t2;
+  }
+  if (c.prm.precision == 0)
+    ++c.launches, k_load_particles<double><<<nblk(n, 256), 256, 0, c.stream>>>(
+        n, c.pcap, dx3, dv3, dC9, dm, dvol, drad, c.pbuf[0].as<double>(),
+        c.pid[0].as<int>());
+  else
+    ++c.launches, k_load_particles<float><<<nblk(n, 256), 256, 0, c.stream>>>(
+        n, c.pcap, dx3, dv3, dC9, dm, dvol, drad, c.pbuf[0].as<float>(),
+        c.pid[0].as<int>());
+  WCG_TRY(cudaGetLastError());
+  return cudaStreamSynchronize(c.stream);
+}
+
+cudaError_t download_particles(Context& c, double* x3, double* v3, double* C9,
+                               bool device_ptrs) {
+  const long long n = c.np;
+  if (n == 0) return cudaSuccess;
+  double* st = c.hostorder.as<double>();
+  if (c.prm.precision == 0)
+    ++c.launches, k_store_particles<double><<<nblk(n, 256), 256, 0, c.stream>>>(
+        n, c.pcap, c.pbuf[c.cur].as<double>(), c.pid[c.cur].as<int>(), st);
+  else
+    ++c.launches, k_store_particles<float><<<nblk(n, 256), 256, 0, c.stream>>>(
+        n, c.pcap, c.pbuf[c.cur].as<float>(), c.pid[c.cur].as<int>(), st);
+  WCG_TRY(cudaGetLastError());
+  const cudaMemcpyKind kind =
+      device_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  // AoS 15-wide -> three strided copies
+  if (x3)
+    WCG_TRY(cudaMemcpy2DAsync(x3, 3 * sizeof(double), st, 15 * sizeof(double),
+                              3 * sizeof(double), n, kind, c.stream));
+  if (v3)
+    WCG_TRY(cudaMemcpy2DAsync(v3, 3 * sizeof(double), st + 3, 15 * sizeof(double),
+                              3 * sizeof(double), n, kind, c.stream));
+  if (C9)
+    WCG_TRY(cudaMemcpy2DAsync(C9, 9 * sizeof(double), st + 6, 15 * sizeof(double),
+                              9 * sizeof(double), n, kind, c.stream));
+  return cudaStreamSynchronize(c.stream);
+}
+
+// ---------------------------------------------------------------------------
+// bounding box
+template <typename R>
+__global__ void k_minmax(const R* __restrict__ P, long long pcap, long long n,
+                         double* __restrict__ partial) {
+  __shared__ double sm[kRedThreads];
+  double mn[3] = {1e20, 1e20, 1e20}, mx[3] = {-1e20, -1e20, -1e20};
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    for (int a = 0; a < 3; ++a) {
+      const double v = (double)P[(PX + a) * pcap + i];
+      mn[a] = v < mn[a] ? v : mn[a];
+      mx[a] = v > mx[a] ? v : mx[a];
+    }
+  for (int a = 0; a < 3; ++a) {
+    const double lo = -block_max<double>(-mn[a], sm);
+    const double hi = block_max<double>(mx[a], sm);
+    if (threadIdx.x == 0) {
+      partial[blockIdx.x * 6 + a] = lo;
+      partial[blockIdx.x * 6 + 3 + a] = hi;
+    }
+  }
+}
+
+__global__ void k_minmax_final(const double* __restrict__ partial, int nb,
+                               double* __restrict__ out) {
+  if (threadIdx.x != 0) return;
+  double r[6] = {1e20, 1e20, 1e20, -1e20, -1e20, -1e20};
+  for (int b = 0; b < nb; ++b)
+    for (int a = 0; a < 3; ++a) {
+      r[a] = partial[b * 6 + a] < r[a] ? partial[b * 6 + a] : r[a];
+      r[3 + a] = partial[b * 6 + 3 + a] > r[3 + a] ? partial[b * 6 + 3 + a] : r[3 + a];
+    }
+  for (int k = 0; k < 6; ++k) out[k] = r[k];
+}
+
+// max over particles of |v|^2 (TwoDScene::getMaxFluidVelocity :4180-4188)
+template <typename R>
+__global__ void k_maxvel2(const R* __restrict__ P, long long pcap, long long n,
+                          double* __restrict__ partial) {
+  __shared__ double sm[kRedThreads];
+  double m = 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double vx = P[VX * pcap + i], vy = P[VY * pcap + i], vz = P[VZ * pcap + i];
+    const double s = (vx * vx + vy * vy) + vz * vz;
+    m = s > m ? s : m;
+  }
+  m = block_max<double>(m, sm);
+  if (threadIdx.x == 0) partial[blockIdx.x] = m;
+}
+
+static cudaError_t ensure_scratch(Context& c, size_t bytes) {
+  return c.scratch.ensure(std::max(bytes, (size_t)(kRedBlocks * 8 * sizeof(double))));
+}
+
+template <typename R>
+static cudaError_t build_grid_t(Context& c) {
+  ProfScope prof(c, P_GRID);
+  const long long n = c.np;
+  R* P = c.pbuf[c.cur].as<R>();
+  WCG_TRY(ensure_scratch(c, 0));
+  double* part = c.scratch.as<double>();
+  double* dsc = c.dscalars.as<double>();
+  // 1. bounding box (TwoDScene::updateParticleBoundingBox :1588-1612)
+  ++c.launches, k_minmax<R><<<kRedBlocks, kRedThreads, 0, c.stream>>>(P, c.pcap, n, part);
+  ++c.launches, k_minmax_final<<<1, 32, 0, c.stream>>>(part, kRedBlocks, dsc);
+  WCG_TRY(cudaMemcpyAsync(c.hscalars, dsc, 6 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  WCG_TRY(cudaStreamSynchronize(c.stream));
+  double bbmin[3] = {1e20, 1e20, 1e20}, bbmax[3] = {-1e20, -1e20, -1e20};
+  if (n > 0)
+    for (int a = 0; a < 3; ++a) {
+      bbmin[a] = c.hscalars[a];
+      bbmax[a] = c.hscalars[3 + a];
+    }
+  const double cell = c.prm.dx;
+  const double bs = cell * 4.0;  // bucket size (numcells = 4)
+  const double d2 = bs * 2.0;
+  for (int a = 0; a < 3; ++a) {
+    c.bbx_min[a] = std::floor(bbmin[a] / d2) * d2;
+    c.bbx_max[a] = std::ceil(bbmax[a] / d2) * d2;
+  }
+  // 2. TwoDScene::rebucketizeParticles (:1657-1710)
+  const double extra = 3.0;
+  int nbk[3];
+  double org[3];
+  for (int a = 0; a < 3; ++a) {
+    const double content = (c.bbx_max[a] - c.bbx_min[a]) + bs * extra * 2.0;
+    const int cells = std::max(1, (int)std::ceil(content / cell));
+    const double gsize = (double)cells * cell;
+    org[a] = c.bbx_min[a] - bs * extra;
+    nbk[a] = std::max(1, (int)std::ceil(gsize / bs));
+  }
+  GridDesc& g = c.g;
+  g.ni = nbk[0]; g.nj = nbk[1]; g.nk = nbk[2];
+  g.NI = g.ni * 4; g.NJ = g.nj * 4; g.NK = g.nk * 4;
+  g.nb = (long long)g.ni * g.nj * g.nk;
+  g.nnode = g.nb * 64;
+  g.ox = org[0]; g.oy = org[1]; g.oz = org[2];
+  g.bs = bs;
+  g.dx = cell;
+  c.have_grid = true;
+  const int rb = c.real_bytes();
+  // 3. storage
+  if (g.nnode > c.gcap) {
+    const long long cap = g.nnode + g.nnode / 8;
+    WCG_TRY(c.gfield.ensure((size_t)kNumGFields * cap * rb));
+    WCG_TRY(c.gvalid.ensure((size_t)6 * cap));
+    WCG_TRY(c.gdof.ensure((size_t)cap));
+    WCG_TRY(c.cell_start.ensure((size_t)(cap + 1) * sizeof(int)));
+    WCG_TRY(c.cell_cursor.ensure((size_t)(cap + cap / 64 + 64) * sizeof(int)));
+    if (c.prm.precision != 0) {
+      WCG_TRY(c.rx64.ensure((size_t)cap * sizeof(double)));
+      WCG_TRY(c.rr64.ensure((size_t)cap * sizeof(double)));
+      WCG_TRY(c.rb64.ensure((size_t)cap * sizeof(double)));
+    }
+    c.gcap = cap;
+  }
+  const long long bcap = c.gcap / 64 + 1;
+  if ((size_t)bcap > c.active.bytes) {
+    WCG_TRY(c.active_pre.ensure((size_t)bcap));
+    WCG_TRY(c.active.ensure((size_t)bcap));
+    WCG_TRY(c.active_list.ensure((size_t)bcap * sizeof(int)));
+  }
+  c.nti = (g.ni + 1) / 2;
+  c.ntj = (g.nj + 1) / 2;
+  c.ntk = (g.nk + 1) / 2;
+  const long long ntot = (long long)c.nti * c.ntj * c.ntk;
+  if ((size_t)ntot * sizeof(int) > c.tile_flag.bytes) {
+    const long long tcap = ntot + ntot / 4 + 64;
+    WCG_TRY(c.tile_flag.ensure((size_t)tcap * sizeof(int)));
+    WCG_TRY(cudaMemsetAsync(c.tile_flag.p, 0, c.tile_flag.bytes, c.stream));
+    WCG_TRY(c.tile_active.ensure((size_t)tcap));
+    WCG_TRY(c.wave_list.ensure((size_t)tcap * sizeof(int)));
+    WCG_TRY(c.tile_part.ensure((size_t)tcap * sizeof(double)));
+  }
+  const int nwave = c.nti + c.ntj + c.ntk;
+  WCG_TRY(c.wave_count.ensure((size_t)(2 * (nwave + 2)) * sizeof(int)));
+  const long long scan_tiles = (std::max(g.nnode + 1, (long long)n) + kScanTile - 1) / kScanTile + 1;
+  WCG_TRY(ensure_scratch(c, (size_t)scan_tiles * sizeof(long long) + 64));
+  part = c.scratch.as<double>();
+  // 4. particle pass
+  int* drange = (int*)(dsc + 8);
+  {
+    int init[6] = {1 << 20, 1 << 20, 1 << 20, -(1 << 20), -(1 << 20), -(1 << 20)};
+    WCG_TRY(cudaMemcpyAsync(drange, init, sizeof(init), cudaMemcpyHostToDevice, c.stream));
+  }
+  WCG_TRY(cudaMemsetAsync(c.active_pre.p, 0, g.nb, c.stream));
+  int* cstart = c.cell_start.as<int>();
+  WCG_TRY(cudaMemsetAsync(cstart, 0, (g.nnode + 1) * sizeof(int), c.stream));
+  const int half = c.cur;
+  long long* key_cur = c.pkey.as<long long>() + half * c.pcap;
+  int* delta_cur = c.pdelta.as<int>() + half * c.pcap;
+  int* pb_cur = c.pbucket.as<int>() + half * c.pcap;
+  if (n > 0)
+    ++c.launches, k_particle_prepass<R><<<nblk(n, 256), 256, 0, c.stream>>>(
+        g, P, c.pcap, n, key_cur, delta_cur, pb_cur, c.active_pre.as<unsigned char>(),
+        cstart, drange, c.derr.as<int>());
+  WCG_TRY(cudaGetLastError());
+  // 5. dilation
+  ++c.launches, k_dilate<<<nblk(g.nb, 256), 256, 0, c.stream>>>(g, c.active_pre.as<unsigned char>(),
+                                                  c.active.as<unsigned char>());
+  // 6. active list
+  int* tmpi = c.cell_cursor.as<int>();
+  ++c.launches, k_flag_to_int<<<nblk(g.nb, 256), 256, 0, c.stream>>>(c.active.as<unsigned char>(), g.nb, tmpi);
+  int* dtotal = (int*)(dsc + 16);
+  exclusive_scan<int, int>(tmpi, g.nb, tmpi, (int*)part, dtotal, c.stream);
+  ++c.launches, k_compact<<<nblk(g.nb, 256), 256, 0, c.stream>>>(c.active.as<unsigned char>(), tmpi, g.nb,
+                                                   c.active_list.as<int>());
+  // tiles (2x2x2 buckets) with an active bucket, compacted into tile_part as ints
+  int* ttmp = tmpi + g.nb + 1;
+  int* tlist = (int*)c.tile_part.p;
+  ++c.launches, k_tile_active<<<nblk(ntot, 256), 256, 0, c.stream>>>(
+      g, c.nti, c.ntj, c.ntk, c.active.as<unsigned char>(), c.tile_active.as<unsigned char>());
+  ++c.launches, k_flag_to_int<<<nblk(ntot, 256), 256, 0, c.stream>>>(
+      c.tile_active.as<unsigned char>(), ntot, ttmp);
+  exclusive_scan<int, int>(ttmp, ntot, ttmp, (int*)part, dtotal + 1, c.stream);
+  ++c.launches, k_compact<<<nblk(ntot, 256), 256, 0, c.stream>>>(
+      c.tile_active.as<unsigned char>(), ttmp, ntot, tlist);
+  WCG_TRY(cudaMemcpyAsync(c.hscalars + 8, dsc + 8, 9 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  WCG_TRY(cudaStreamSynchronize(c.stream));
+  {
+    const int* hr = (const int*)(c.hscalars + 8);
+    c.n_active = *(const int*)(c.hscalars + 16);
+    c.n_tiles = *((const int*)(c.hscalars + 16) + 1);
+    c.stats.nactive = c.n_active;
+    for (int k = 0; k < 6; ++k) c.drange_h[k] = n > 0 ? hr[k] : (k < 3 ? 0 : 1);
+  }
+  // 7. wave ordering of the active tiles (ti+tj+tk)
+  int* wcount = c.wave_count.as<int>();
+  int* wcursor = wcount + (nwave + 2);
+  WCG_TRY(cudaMemsetAsync(wcount, 0, (nwave + 2) * sizeof(int), c.stream));
+  if (c.n_tiles > 0) {
+    ++c.launches, k_tile_wave_count<<<nblk(c.n_tiles, 256), 256, 0, c.stream>>>(
+        c.nti, c.ntj, tlist, c.n_tiles, wcount);
+    exclusive_scan<int, int>(wcount, nwave + 1, wcursor, (int*)part, nullptr, c.stream);
+    ++c.launches, k_tile_wave_scatter<<<nblk(c.n_tiles, 256), 256, 0, c.stream>>>(
+        c.nti, c.ntj, tlist, c.n_tiles, wcursor, c.wave_list.as<int>());
+  }
+  // 8. counting sort by key node, deterministic within a cell
+  exclusive_scan<int, int>(cstart, g.nnode, cstart, (int*)part, cstart + g.nnode, c.stream);
+  WCG_TRY(cudaMemsetAsync(tmpi, 0, g.nnode * sizeof(int), c.stream));
+  if (n > 0) {
+    ++c.launches, k_sort_scatter<<<nblk(n, 256), 256, 0, c.stream>>>(key_cur, n, cstart, tmpi,
+                                                       c.perm.as<int>());
+    ++c.launches, k_sort_cells<<<nblk(g.nnode, 256), 256, 0, c.stream>>>(cstart, g.nnode,
+                                                           c.pid[c.cur].as<int>(),
+                                                           c.perm.as<int>());
+    const int nxt = c.cur ^ 1;
+    ++c.launches, k_gather_particles<R><<<nblk(n, 256), 256, 0, c.stream>>>(
+        c.perm.as<int>(), n, c.pcap, P, c.pbuf[nxt].as<R>(), c.pid[c.cur].as<int>(),
+        c.pid[nxt].as<int>(), key_cur, c.pkey.as<long long>() + nxt * c.pcap, delta_cur,
+        c.pdelta.as<int>() + nxt * c.pcap, pb_cur, c.pbucket.as<int>() + nxt * c.pcap);
+    c.cur = nxt;
+  }
+  WCG_TRY(cudaGetLastError());
+  return cudaSuccess;
+}
+
+cudaError_t build_grid(Context& c) {
+  return c.prm.precision == 0 ? build_grid_t<double>(c) : build_grid_t<float>(c);
+}
+
+static Walls make_walls(const Context& c) {
+  Walls w;
+  w.cx = c.prm.box_center[0]; w.cy = c.prm.box_center[1]; w.cz = c.prm.box_center[2];
+  w.ex = c.prm.box_half[0]; w.ey = c.prm.box_half[1]; w.ez = c.prm.box_half[2];
+  w.radius = c.prm.box_radius;
+  w.sign = -1.0;
+  w.enabled = c.prm.walls;
+  return w;
+}
+
+template <typename R>
+static cudaError_t map_particles_to_grid_t(Context& c) {
+  if (c.n_active == 0) return cudaSuccess;
+  ProfScope prof(c, P_P2G);
+  DeltaRange dr;
+  for (int a = 0; a < 3; ++a) {
+    dr.lo[a] = c.drange_h[a];
+    dr.hi[a] = c.drange_h[3 + a];
+  }
+  R* F = c.gfield.as<R>();
+  const Walls w = make_walls(c);
+  ++c.launches, k_p2g<R><<<(unsigned)c.n_active, 256, 0, c.stream>>>(
+      c.g, c.active_list.as<int>(), c.active.as<unsigned char>(), c.pbuf[c.cur].as<R>(),
+      c.pcap, c.cell_start.as<int>(), c.pdelta.as<int>() + c.cur * c.pcap, dr, F, c.gcap, w);
+  ++c.launches, k_solid_weights<R><<<(unsigned)c.n_active, 192, 0, c.stream>>>(
+      c.g, c.active_list.as<int>(), c.active.as<unsigned char>(), F, c.gcap, w);
+  return cudaGetLastError();
+}
+
+cudaError_t map_particles_to_grid(Context& c) {
+  return c.prm.precision == 0 ? map_particles_to_grid_t<double>(c)
+                              : map_particles_to_grid_t<float>(c);
+}
+
+template <typename R>
+static cudaError_t step_velocity_t(Context& c, double dt) {
+  if (c.n_active == 0) return cudaSuccess;
+  ProfScope prof(c, P_GRIDOPS);
+  ++c.launches, k_predict<R><<<(unsigned)c.n_active, 192, 0, c.stream>>>(
+      c.g, c.active_list.as<int>(), c.gfield.as<R>(), c.gcap, (R)c.prm.gravity[0],
+      (R)c.prm.gravity[1], (R)c.prm.gravity[2], (R)dt);
+  return cudaGetLastError();
+}
+
+cudaError_t step_velocity(Context& c, double dt) {
+  return c.prm.precision == 0 ? step_velocity_t<double>(c, dt)
+                              : step_velocity_t<float>(c, dt);
+}
+
+// ---------------------------------------------------------------------------
+// PCG
+template <typename R>
+static SweepArgs<R> sweep_args(Context& c) {
+  SweepArgs<R> a{};
+  a.g = c.g;
+  a.nti = c.nti;
+  a.ntj = c.ntj;
+  a.ntk = c.ntk;
+  a.tile_list = c.wave_list.as<int>();
+  a.ntiles = (int)c.n_tiles;
+  a.ticket = c.ticket.as<int>();
+  a.flags = c.tile_flag.as<int>();
+  a.active = c.active.as<unsigned char>();
+  a.tile_active = c.tile_active.as<unsigned char>();
+  a.dof = c.gdof.as<unsigned char>();
+  a.F = c.gfield.as<R>();
+  a.fs = c.gcap;
+  a.sc = c.dscalars.as<double>();
+  a.omega = (R)0.97;
+  a.min_ratio = (R)0.25;
+  a.err = c.derr.as<int>();
+  return a;
+}
+
+// one wavefront launch (factorisation, forward or backward sweep)
+template <typename R>
+static cudaError_t sweep(Context& c, int mode, SweepArgs<R> a) {
+  if (c.n_tiles == 0) return cudaSuccess;
+  ProfScope prof(c, mode == kFactor ? P_MICFACTOR : P_MICSWEEP);
+  a.epoch = ++c.tile_epoch;
+  WCG_TRY(cudaMemsetAsync(c.ticket.p, 0, sizeof(int), c.stream));
+  const unsigned nt = (unsigned)c.n_tiles;
+  if (mode == kFactor) ++c.launches, k_sweep<R, kFactor><<<nt, kSweepThreads, 0, c.stream>>>(a);
+  else if (mode == kForward) ++c.launches, k_sweep<R, kForward><<<nt, kSweepThreads, 0, c.stream>>>(a);
+  else ++c.launches, k_sweep<R, kBackward><<<nt, kSweepThreads, 0, c.stream>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename R>
+static void dot(Context& c, const R* a, const R* b, double* out) {
+  ProfScope prof(c, P_PCGVEC);
+  const long long nent = c.n_active * 64;
+  double* part = c.scratch.as<double>();
+  ++c.launches, k_dot_partial<R><<<kRedBlocks, kRedThreads, 0, c.stream>>>(
+      c.active_list.as<int>(), nent, c.gdof.as<unsigned char>(), a, b, part);
+  ++c.launches, k_reduce_sum<<<1, kRedThreads, 0, c.stream>>>(part, kRedBlocks, out);
+}
+
+template <typename R>
+static void absmax(Context& c, const R* a, double* out) {
+  ProfScope prof(c, P_PCGVEC);
+  const long long nent = c.n_active * 64;
+  double* part = c.scratch.as<double>();
+  ++c.launches, k_absmax_partial<R><<<kRedBlocks, kRedThreads, 0, c.stream>>>(
+      c.active_list.as<int>(), nent, c.gdof.as<unsigned char>(), a, part);
+  ++c.launches, k_reduce_max<<<1, kRedThreads, 0, c.stream>>>(part, kRedBlocks, out);
+}
+
+static cudaError_t fetch(Context& c, const double* d, int k, double* h) {
+  WCG_TRY(cudaMemcpyAsync(h, d, k * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  return cudaStreamSynchronize(c.stream);
+}
+
+static cudaError_t set_scalars(Context& c, int slot, const double* v, int k) {
+  return cudaMemcpyAsync(c.dscalars.as<double>() + slot, v, k * sizeof(double),
+                         cudaMemcpyHostToDevice, c.stream);
+}
+
+constexpr int kPcgBatch = 8;  // iterations launched per host check
+
+// Inner MIC(0)-PCG (PCGSolver<T>::solve, PCGSolver.h:260-308) on the system
+// already assembled and factored: solves A x = r0 from x = 0 (x must be zero
+// on entry), r is overwritten with the residual.  tol_abs is the absolute
+// infinity-norm target.  Convergence is tested on the device after every
+// iteration; the host checks every kPcgBatch iterations.
+template <typename R>
+static cudaError_t pcg_inner(Context& c, R* r, R* x, double tol_abs, int maxiters,
+                             int* iters, int* conv, double* res) {
+  R* F = c.gfield.as<R>();
+  R* z = F + G_Z * c.gcap;
+  R* s0 = F + G_S * c.gcap;
+  R* s1 = F + G_S2 * c.gcap;
+  R* q = F + G_Q * c.gcap;
+  R* y = F + G_Y * c.gcap;
+  double* sc = c.dscalars.as<double>();
+  double* part = c.scratch.as<double>();
+  double* tpart = c.tile_part.as<double>();
+  const long long nent = c.n_active * 64;
+  const int* al = c.active_list.as<int>();
+  const unsigned char* dof = c.gdof.as<unsigned char>();
+  *iters = 0;
+  *conv = 0;
+  *res = 0;
+  if (maxiters <= 0) return cudaSuccess;
+  {
+    const double init[9] = {0.0, 0.0, 0.0, 0.0, 0.0, tol_abs, 0.0, (double)maxiters, 0.0};
+    WCG_TRY(set_scalars(c, S_RHO, init, 9));  // clears S_DONE too
+  }
+  WCG_TRY(cudaMemsetAsync(s0, 0, c.gcap * sizeof(R), c.stream));
+  WCG_TRY(cudaMemsetAsync(s1, 0, c.gcap * sizeof(R), c.stream));
+  // z = M^-1 r, rho = z.r
+  SweepArgs<R> fa = sweep_args<R>(c);
+  fa.in = r;
+  fa.out = y;
+  fa.update = 0;
+  fa.part = nullptr;
+  WCG_TRY(sweep<R>(c, kForward, fa));
+  SweepArgs<R> ba = sweep_args<R>(c);
+  ba.in = y;
+  ba.out = z;
+  ba.r = r;
+  ba.part = tpart;
+  WCG_TRY(sweep<R>(c, kBackward, ba));
+  {
+    ProfScope prof(c, P_PCGVEC);
+    ++c.launches, k_red_beta<<<1, kRedThreads, 0, c.stream>>>(tpart, (int)c.n_tiles, sc, 1);
+  }
+  double h[9];
+  WCG_TRY(fetch(c, sc + S_RHO, 1, h));
+  if (h[0] == 0 || h[0] != h[0]) return cudaSuccess;  // PCGSolver.h:276-279
+  // forward sweeps with the fused x/r update
+  fa.update = 1;
+  fa.r = r;
+  fa.x = x;
+  fa.q = q;
+  fa.part = tpart;
+  R* sold = s0;
+  R* snew = s1;
+  for (;;) {
+    for (int b = 0; b < kPcgBatch; ++b) {
+      {
+        ProfScope prof(c, P_PCGVEC);
+        ++c.launches, k_spmv_s<R><<<kRedBlocks, kRedThreads, 0, c.stream>>>(
+            c.g, al, nent, c.active.as<unsigned char>(), dof, F, c.gcap, z, sold, snew, q, sc,
+            part);
+        ++c.launches, k_red_alpha<<<1, kRedThreads, 0, c.stream>>>(part, kRedBlocks, sc);
+      }
+      fa.s = snew;
+      WCG_TRY(sweep<R>(c, kForward, fa));
+      {
+        ProfScope prof(c, P_PCGVEC);
+        ++c.launches, k_red_conv<<<1, kRedThreads, 0, c.stream>>>(tpart, (int)c.n_tiles, sc);
+      }
+      WCG_TRY(sweep<R>(c, kBackward, ba));
+      {
+        ProfScope prof(c, P_PCGVEC);
+        ++c.launches, k_red_beta<<<1, kRedThreads, 0, c.stream>>>(tpart, (int)c.n_tiles, sc, 0);
+      }
+      R* t = sold;
+      sold = snew;
+      snew = t;
+    }
+    WCG_TRY(fetch(c, sc + S_RES, 6, h));  // res, beta, tol, iter, maxit, done
+    const int done = *(const int*)&h[5];
+    *res = h[0];
+    *iters = (int)h[3];
+    if (done) {
+      *conv = done == 1 ? 1 : 0;
+      break;
+    }
+  }
+  return cudaGetLastError();
+}
+
+// FP64 residual r64 = b64 - A x64 with the (promoted) assembled coefficients
+template <typename R>
+__global__ void __launch_bounds__(kRedThreads)
+    k_residual64(GridDesc g, const int* __restrict__ active_list, long long nent,
+                 const unsigned char* __restrict__ active,
+                 const unsigned char* __restrict__ dof, const R* __restrict__ F,
+                 long long fstride, const double* __restrict__ b,
+                 const double* __restrict__ x, double* __restrict__ r,
+                 double* __restrict__ partial) {
+  __shared__ double sm[kRedThreads];
+  double m = 0;
+  const R* AD = F + G_ADIAG * fstride;
+  const R* AX = F + G_AX * fstride;
+  const R* AY = F + G_AY * fstride;
+  const R* AZ = F + G_AZ * fstride;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nent;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long n = active_node(active_list, e);
+    if (!dof[n]) continue;
+    int I, J, K;
+    node_ijk(g, n, I, J, K);
+    double acc = (double)AD[n] * x[n];
+    if (I > 0) { const long long q = node_linear(g, I - 1, J, K); if (active[q >> 6] && dof[q]) acc += (double)AX[q] * x[q]; }
+    if (J > 0) { const long long q = node_linear(g, I, J - 1, K); if (active[q >> 6] && dof[q]) acc += (double)AY[q] * x[q]; }
+    if (K > 0) { const long long q = node_linear(g, I, J, K - 1); if (active[q >> 6] && dof[q]) acc += (double)AZ[q] * x[q]; }
+    if (I + 1 < g.NI) { const long long q = node_linear(g, I + 1, J, K); if (active[q >> 6] && dof[q]) acc += (double)AX[n] * x[q]; }
+    if (J + 1 < g.NJ) { const long long q = node_linear(g, I, J + 1, K); if (active[q >> 6] && dof[q]) acc += (double)AY[n] * x[q]; }
+    if (K + 1 < g.NK) { const long long q = node_linear(g, I, J, K + 1); if (active[q >> 6] && dof[q]) acc += (double)AZ[n] * x[q]; }
+    const double rv = b[n] - acc;
+    r[n] = rv;
+    const double av = fabs(rv);
+    m = av > m ? av : m;
+  }
+  m = block_max<double>(m, sm);
+  if (threadIdx.x == 0) partial[blockIdx.x] = m;
+}
+
+template <typename R>
+__global__ void k_promote(const int* __restrict__ active_list, long long nent,
+                          const unsigned char* __restrict__ dof, const R* __restrict__ a,
+                          double* __restrict__ o) {
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nent;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long n = active_node(active_list, e);
+    o[n] = dof[n] ? (double)a[n] : 0.0;
+  }
+}
+
+// r32 = r64 * scale; used to hand the FP64 residual to the FP32 inner solve
+template <typename R>
+__global__ void k_demote_scaled(const int* __restrict__ active_list, long long nent,
+                                const unsigned char* __restrict__ dof,
+                                const double* __restrict__ a, const double* __restrict__ sc,
+                                R* __restrict__ o, R* __restrict__ x) {
+  const double scale = 1.0 / sc[0];
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nent;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long n = active_node(active_list, e);
+    o[n] = dof[n] ? (R)(a[n] * scale) : R(0);
+    x[n] = R(0);
+  }
+}
+
+// x64 += e32 * norm
+template <typename R>
+__global__ void k_accumulate(const int* __restrict__ active_list, long long nent,
+                             const unsigned char* __restrict__ dof,
+                             const R* __restrict__ e32, const double* __restrict__ sc,
+                             double* __restrict__ x) {
+  const double s = sc[0];
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nent;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long n = active_node(active_list, e);
+    if (dof[n]) x[n] += (double)e32[n] * s;
+  }
+}
+
+template <typename R>
+__global__ void k_store_pressure(const int* __restrict__ active_list, long long nent,
+                                 const unsigned char* __restrict__ dof,
+                                 const R* __restrict__ x32, const double* __restrict__ x64,
+                                 R* __restrict__ p) {
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nent;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long n = active_node(active_list, e);
+    p[n] = dof[n] ? (x64 ? (R)x64[n] : x32[n]) : R(0);
+  }
+}
+
+template <typename R>
+static cudaError_t project_fine_t(Context& c, double dt) {
+  c.stats.pcg_iters = 0;
+  c.stats.refinements = 0;
+  c.stats.residual = 0;
+  c.stats.rhs_norm = 0;
+  c.stats.converged = 1;
+  if (c.n_active == 0) return cudaSuccess;
+  R* F = c.gfield.as<R>();
+  const int* al = c.active_list.as<int>();
+  const unsigned char* act = c.active.as<unsigned char>();
+  unsigned char* dof = c.gdof.as<unsigned char>();
+  const long long nent = c.n_active * 64;
+  {
+    ProfScope prof(c, P_GRIDOPS);
+    ++c.launches, k_assemble<R><<<(unsigned)c.n_active, 64, 0, c.stream>>>(c.g, al, act, F, c.gcap, dof, (R)dt);
+  }
+  WCG_TRY(cudaGetLastError());
+  double* dsc = c.dscalars.as<double>();
+  double* part = c.scratch.as<double>();
+  R* r = F + G_R * c.gcap;
+  R* x = F + G_X * c.gcap;
+  const R* b = F + G_B * c.gcap;
+  double h[4];
+  // ||b||_inf and the number of DOFs
+  absmax<R>(c, b, dsc + 4);
+  {
+    ProfScope prof(c, P_PCGVEC);
+    ++c.launches, k_count_dof<<<kRedBlocks, kRedThreads, 0, c.stream>>>(al, nent, dof, part);
+    ++c.launches, k_reduce_sum<<<1, kRedThreads, 0, c.stream>>>(part, kRedBlocks, dsc + 5);
+  }
+  WCG_TRY(fetch(c, dsc + 4, 2, h));
+  const double bnorm = h[0];
+  c.stats.rhs_norm = bnorm;
+  c.stats.ndof = (long long)h[1];
+  if (bnorm < 1e-30) {
+    // PCGSolver::solve returns x = 0 after zero iterations (PCGSolver.h:268-272)
+    WCG_TRY(cudaMemsetAsync(F + G_PRESSURE * c.gcap, 0, c.gcap * sizeof(R), c.stream));
+    return cudaGetLastError();
+  }
+  const double tol = c.prm.criterion * bnorm;
+  // MIC(0) factor (PCGSolver::form_preconditioner)
+  {
+    const double zero = 0.0;
+    WCG_TRY(set_scalars(c, S_DONE, &zero, 1));
+  }
+  WCG_TRY(sweep<R>(c, kFactor, sweep_args<R>(c)));
+  WCG_TRY(cudaMemsetAsync(x, 0, c.gcap * sizeof(R), c.stream));
+  if (c.prm.precision == 0) {
+    {
+      ProfScope prof(c, P_PCGVEC);
+      ++c.launches, k_copy_dof<R><<<kRedBlocks, kRedThreads, 0, c.stream>>>(al, nent, dof, b, r);
+    }
+    int iters = 0, conv = 0;
+    double res = bnorm;
+    WCG_TRY(pcg_inner<R>(c, r, x, tol, c.prm.maxiters, &iters, &conv, &res));
+    c.stats.pcg_iters = iters;
+    c.stats.converged = conv;
+    c.stats.residual = res;
+    ++c.launches, k_store_pressure<R><<<kRedBlocks, kRedThreads, 0, c.stream>>>(al, nent, dof, x, nullptr,
+                                                                  F + G_PRESSURE * c.gcap);
+    return cudaGetLastError();
+  }
+  // mixed precision: FP32 inner PCG, FP64 residual and solution
+  double* x64 = c.rx64.as<double>();
+  double* r64 = c.rr64.as<double>();
+  double* b64 = c.rb64.as<double>();
+  WCG_TRY(cudaMemsetAsync(x64, 0, c.gcap * sizeof(double), c.stream));
+  ++c.launches, k_promote<R><<<kRedBlocks, kRedThreads, 0, c.stream>>>(al, nent, dof, b, b64);
+  ++c.launches, k_promote<R><<<kRedBlocks, kRedThreads, 0, c.stream>>>(al, nent, dof, b, r64);
+  double res = bnorm;
+  int total = 0, k = 0;
+  bool conv = false;
+  // inner target: the remaining factor to the final tolerance (or a fixed
+  // relative reduction when refine_inner_tol > 0)
+  const double inner_rel = c.prm.refine_inner_tol > 0 ? c.prm.refine_inner_tol : 0.0;
+  for (k = 0; k <= c.prm.max_refinements; ++k) {
+    if (res <= tol) {
+      conv = true;
+      break;
+    }
+    if (total >= c.prm.maxiters || k == c.prm.max_refinements) break;
+    // scaled residual (||r32||_inf == 1) into r, x = 0
+    WCG_TRY(cudaMemcpyAsync(dsc + 5, &res, sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    {
+      ProfScope prof(c, P_REFINE);
+      ++c.launches, k_demote_scaled<R><<<kRedBlocks, kRedThreads, 0, c.stream>>>(
+          al, nent, dof, r64, dsc + 5, r, x);
+    }
+    const double want = std::max(inner_rel, 0.5 * tol / res);
+    int iters = 0, ic = 0;
+    double ires = 0;
+    WCG_TRY(pcg_inner<R>(c, r, x, want, c.prm.maxiters - total, &iters, &ic, &ires));
+    total += iters;
+    ProfScope prof3(c, P_REFINE);
+    ++c.launches, k_accumulate<R><<<kRedBlocks, kRedThreads, 0, c.stream>>>(al, nent, dof, x, dsc + 5, x64);
+    ++c.launches, k_residual64<R><<<kRedBlocks, kRedThreads, 0, c.stream>>>(
+        c.g, al, nent, act, dof, F, c.gcap, b64, x64, r64, part);
+    ++c.launches, k_reduce_max<<<1, kRedThreads, 0, c.stream>>>(part, kRedBlocks, dsc + 6);
+    WCG_TRY(fetch(c, dsc + 6, 1, h));
+    res = h[0];
+    if (iters == 0) break;
+  }
+  c.stats.pcg_iters = total;
+  c.stats.refinements = k;
+  c.stats.converged = conv ? 1 : 0;
+  c.stats.residual = res;
+  ++c.launches, k_store_pressure<R><<<kRedBlocks, kRedThreads, 0, c.stream>>>(al, nent, dof, x, x64,
+                                                                F + G_PRESSURE * c.gcap);
+  return cudaGetLastError();
+}
+
+cudaError_t project_fine(Context& c, double dt) {
+  return c.prm.precision == 0 ? project_fine_t<double>(c, dt) : project_fine_t<float>(c, dt);
+}
+
+template <typename R>
+static cudaError_t apply_pressure_t(Context& c, double dt) {
+  if (c.n_active == 0) return cudaSuccess;
+  ProfScope prof(c, P_GRIDOPS);
+  R* F = c.gfield.as<R>();
+  const int* al = c.active_list.as<int>();
+  const unsigned char* act = c.active.as<unsigned char>();
+  unsigned char* valid = c.gvalid.as<unsigned char>();
+  unsigned char* vtmp = valid + 3 * c.gcap;
+  ++c.launches, k_apply_pressure<R><<<(unsigned)c.n_active, 192, 0, c.stream>>>(c.g, al, act, F, c.gcap,
+                                                                  valid, (R)dt);
+  R* U = F + G_U * c.gcap;
+  R* UT = F + G_UTMP * c.gcap;
+  ++c.launches, k_extrapolate<R><<<(unsigned)c.n_active, 192, 0, c.stream>>>(c.g, al, act, U, UT, valid,
+                                                               vtmp, c.gcap);
+  ++c.launches, k_extrapolate<R><<<(unsigned)c.n_active, 192, 0, c.stream>>>(c.g, al, act, UT, U, vtmp,
+                                                               valid, c.gcap);
+  return cudaGetLastError();
+}
+
+cudaError_t apply_pressure_and_extrapolate(Context& c, double dt) {
+  return c.prm.precision == 0 ? apply_pressure_t<double>(c, dt)
+                              : apply_pressure_t<float>(c, dt);
+}
+
+cudaError_t constrain_liquid_velocity(Context& c) {
+  if (c.n_active == 0) return cudaSuccess;
+  ProfScope prof(c, P_GRIDOPS);
+  if (c.prm.precision == 0)
+    ++c.launches, k_constrain<double><<<(unsigned)c.n_active, 192, 0, c.stream>>>(
+        c.active_list.as<int>(), c.gfield.as<double>(), c.gcap,
+        c.prm.liquid_boundary_friction);
+  else
+    ++c.launches, k_constrain<float><<<(unsigned)c.n_active, 192, 0, c.stream>>>(
+        c.active_list.as<int>(), c.gfield.as<float>(), c.gcap,
+        (float)c.prm.liquid_boundary_friction);
+  return cudaGetLastError();
+}
+
+template <typename R>
+static cudaError_t g2p_t(Context& c, double dt, bool advect) {
+  if (c.np == 0) return cudaSuccess;
+  ProfScope prof(c, P_G2P);
+  ++c.launches, k_g2p<R><<<nblk(c.np, 128), 128, 0, c.stream>>>(
+      c.g, c.active.as<unsigned char>(), c.pbuf[c.cur].as<R>(), c.pcap, c.np,
+      c.pkey.as<long long>() + c.cur * c.pcap, c.pdelta.as<int>() + c.cur * c.pcap,
+      c.gfield.as<R>(), c.gcap, (R)c.prm.flip_coeff, (R)dt, advect ? 1 : 0);
+  return cudaGetLastError();
+}
+
+cudaError_t map_grid_to_particles_and_advect(Context& c, double dt, bool advect) {
+  return c.prm.precision == 0 ? g2p_t<double>(c, dt, advect) : g2p_t<float>(c, dt, advect);
+}
+
+cudaError_t advect_only(Context& c, double dt) {
+  if (c.np == 0) return cudaSuccess;
+  ProfScope prof(c, P_G2P);
+  if (c.prm.precision == 0)
+    ++c.launches, k_advect<double><<<nblk(c.np, 256), 256, 0, c.stream>>>(c.pbuf[c.cur].as<double>(), c.pcap,
+                                                            c.np, dt);
+  else
+    ++c.launches, k_advect<float><<<nblk(c.np, 256), 256, 0, c.stream>>>(c.pbuf[c.cur].as<float>(), c.pcap,
+                                                           c.np, (float)dt);
+  return cudaGetLastError();
+}
+
+// WetClothCore::stepSystem sub-stepping (WetClothCore.cpp:50-62)
+cudaError_t num_substeps(Context& c, double dt, int* n) {
+  WCG_TRY(ensure_scratch(c, 0));
+  ProfScope prof(c, P_OTHER);
+  double* part = c.scratch.as<double>();
+  double* dsc = c.dscalars.as<double>();
+  if (c.np > 0) {
+    if (c.prm.precision == 0)
+      ++c.launches, k_maxvel2<double><<<kRedBlocks, kRedThreads, 0, c.stream>>>(c.pbuf[c.cur].as<double>(),
+                                                                 c.pcap, c.np, part);
+    else
+      ++c.launches, k_maxvel2<float><<<kRedBlocks, kRedThreads, 0, c.stream>>>(c.pbuf[c.cur].as<float>(),
+                                                                c.pcap, c.np, part);
+    ++c.launches, k_reduce_max<<<1, kRedThreads, 0, c.stream>>>(part, kRedBlocks, dsc + 7);
+  } else {
+    WCG_TRY(cudaMemsetAsync(dsc + 7, 0, sizeof(double), c.stream));
+  }
+  double h;
+  WCG_TRY(fetch(c, dsc + 7, 1, &h));
+  const double max_fluid_vel = std::sqrt(h);
+  const double max_elasto_vel = 0.0;
+  const double cell = c.prm.dx;
+  const double max_elasto_dt = std::min(cell / std::max(1e-63, max_elasto_vel) / 3.0, 1.0 / 30.0);
+  const double max_fluid_dt = std::min(cell / std::max(1e-63, max_fluid_vel) * 3.0, 1.0 / 30.0);
+  const double max_dt = std::min(max_elasto_dt, max_fluid_dt);
+  *n = std::max(1, (int)std::ceil(dt / max_dt));
+  return cudaSuccess;
+}
+
+cudaError_t substep(Context& c, double dt) {
+  WCG_TRY(build_grid(c));
+  WCG_TRY(map_particles_to_grid(c));
+  WCG_TRY(step_velocity(c, dt));
+  WCG_TRY(project_fine(c, dt));
+  WCG_TRY(apply_pressure_and_extrapolate(c, dt));
+  WCG_TRY(constrain_liquid_velocity(c));
+  WCG_TRY(map_grid_to_particles_and_advect(c, dt, true));
+  return cudaSuccess;
+}
+
+}  // namespace wcg

@@ -1,0 +1,187 @@
+"""Python view of one GPU scene, mirroring the reference's call sequence.
+
+``FluidScene`` wraps a ``wcg_ctx``: the methods are named after the
+``TwoDScene`` / ``LinearizedImplicitEuler`` / ``WetClothCore`` calls they
+replace (libWetCloth/Core/WetClothCore.cpp:115-258).  All arithmetic runs in
+libwcgpu.so on the GPU.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _capi
+from ._capi import check, _dp
+
+
+def make_params(p, precision=_capi.WCG_FP64, refine_inner_tol=0.0,
+                max_refinements=20) -> _capi.WcgParams:
+    prm = _capi.WcgParams()
+    _capi.load().wcg_default_params(ctypes.byref(prm))
+    prm.dx = p.dx
+    for a in range(3):
+        prm.gravity[a] = p.gravity[a]
+        prm.box_center[a] = p.box_center[a]
+        prm.box_half[a] = p.box_half[a]
+    prm.liquid_density = p.liquid_density
+    prm.flip_coeff = p.flip_coeff
+    prm.liquid_boundary_friction = p.liquid_boundary_friction
+    prm.box_radius = p.box_radius
+    prm.walls = 1
+    prm.criterion = p.criterion
+    prm.maxiters = p.maxiters
+    prm.precision = precision
+    prm.refine_inner_tol = refine_inner_tol
+    prm.max_refinements = max_refinements
+    return prm
+
+
+class FluidScene:
+    def __init__(self, scene=None, precision=_capi.WCG_FP64, params=None, **kw):
+        self.L = _capi.load()
+        prm = params if params is not None else make_params(scene.params, precision, **kw)
+        h = ctypes.c_void_p()
+        check(self.L.wcg_create(ctypes.byref(prm), ctypes.byref(h)))
+        self.h = h
+        self.precision = prm.precision
+        if scene is not None:
+            self.upload(scene.x, scene.v, scene.C, scene.mass, scene.vol, scene.radius)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.wcg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- particles ----
+    def upload(self, x, v, C, mass, vol, radius):
+        arr = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+        x, v, C, mass, vol, radius = map(arr, (x, v, C, mass, vol, radius))
+        n = mass.shape[0]
+        check(self.L.wcg_upload_liquid(self.h, n, _dp(x), _dp(v), _dp(C), _dp(mass),
+                                       _dp(vol), _dp(radius)))
+
+    def upload_device(self, n, x, v, C, mass, vol, radius):
+        """Arguments are device pointers (ints) to contiguous float64 arrays."""
+        check(self.L.wcg_upload_liquid_device(self.h, n, x, v, C, mass, vol, radius))
+
+    @property
+    def num_particles(self):
+        return self.L.wcg_num_particles(self.h)
+
+    def download(self):
+        n = self.num_particles
+        x = np.empty((n, 3))
+        v = np.empty((n, 3))
+        C = np.empty((n, 9))
+        check(self.L.wcg_download_liquid(self.h, _dp(x), _dp(v), _dp(C)))
+        return x, v, C
+
+    # ---- reference call sequence ----
+    def rebucketize_and_resample(self):
+        check(self.L.wcg_rebucketize_and_resample(self.h))
+
+    def map_particle_nodes(self):
+        check(self.L.wcg_map_particle_nodes(self.h))
+
+    def step_velocity(self, dt):
+        check(self.L.wcg_step_velocity(self.h, dt))
+
+    def project_fine(self, dt):
+        check(self.L.wcg_project_fine(self.h, dt))
+
+    def apply_pressure_drag_fluid(self, dt):
+        check(self.L.wcg_apply_pressure_drag_fluid(self.h, dt))
+
+    def constrain_liquid_velocity(self):
+        check(self.L.wcg_constrain_liquid_velocity(self.h))
+
+    def map_node_particles(self):
+        check(self.L.wcg_map_node_particles(self.h))
+
+    def advect(self, dt):
+        check(self.L.wcg_advect(self.h, dt))
+
+    def substep(self, dt):
+        check(self.L.wcg_substep(self.h, dt))
+
+    def num_substeps(self, dt):
+        n = ctypes.c_int(0)
+        check(self.L.wcg_num_substeps(self.h, dt, ctypes.byref(n)))
+        return n.value
+
+    def step(self, dt):
+        n = ctypes.c_int(0)
+        check(self.L.wcg_step(self.h, dt, ctypes.byref(n)))
+        return n.value
+
+    def stats(self):
+        s = _capi.WcgStats()
+        check(self.L.wcg_get_stats(self.h, ctypes.byref(s)))
+        return {k: getattr(s, k) for k, _ in _capi.WcgStats._fields_}
+
+    # ---- parity downloads ----
+    def grid_info(self):
+        dims = (ctypes.c_int * 3)()
+        org = (ctypes.c_double * 3)()
+        bbx = (ctypes.c_double * 6)()
+        check(self.L.wcg_grid_info(self.h, dims, org, bbx))
+        return np.array(dims[:]), np.array(org[:]), np.array(bbx[:])
+
+    def field(self, name):
+        n = self.L.wcg_field_size(self.h, name.encode())
+        if n < 0:
+            raise KeyError(name)
+        out = np.empty(n, dtype=np.float64)
+        check(self.L.wcg_download_field(self.h, name.encode(), _dp(out), n))
+        return out
+
+    def ifield(self, name):
+        n = self.L.wcg_field_size(self.h, name.encode())
+        if n < 0:
+            raise KeyError(name)
+        out = np.empty(n, dtype=np.int64)
+        check(self.L.wcg_download_ifield(self.h, name.encode(),
+                                         out.ctypes.data_as(_capi._L), n))
+        return out
+
+    def pressure_system(self):
+        ndof = ctypes.c_longlong(0)
+        nnz = ctypes.c_longlong(0)
+        check(self.L.wcg_export_pressure_system(self.h, ctypes.byref(ndof), ctypes.byref(nnz),
+                                                None, None, None, None))
+        rs = np.empty(ndof.value + 1, dtype=np.int64)
+        col = np.empty(max(nnz.value, 1), dtype=np.int64)
+        val = np.empty(max(nnz.value, 1), dtype=np.float64)
+        rhs = np.empty(max(ndof.value, 1), dtype=np.float64)
+        check(self.L.wcg_export_pressure_system(
+            self.h, ctypes.byref(ndof), ctypes.byref(nnz), rs.ctypes.data_as(_capi._L),
+            col.ctypes.data_as(_capi._L), _dp(val), _dp(rhs)))
+        return rs, col[:nnz.value], val[:nnz.value], rhs[:ndof.value]
+
+    # ---- instrumentation ----
+    @property
+    def stream_ptr(self):
+        return self.L.wcg_stream(self.h)
+
+    @property
+    def launch_count(self):
+        return self.L.wcg_launch_count(self.h)
+
+    def profile_begin(self):
+        check(self.L.wcg_profile_begin(self.h))
+
+    def profile_end(self):
+        n = self.L.wcg_profile_num_phases()
+        ms = np.zeros(n)
+        cnt = np.zeros(n, dtype=np.int64)
+        check(self.L.wcg_profile_end(self.h, _dp(ms), cnt.ctypes.data_as(_capi._L), n))
+        names = [self.L.wcg_profile_phase_name(i).decode() for i in range(n)]
+        return {names[i]: (float(ms[i]), int(cnt[i])) for i in range(n)}
+

@@ -25,6 +25,8 @@ PFLAGS := $(BASEFLAGS) -fopenmp -DWCREF_OMP
 # Link the process-wide shared libstdc++ (the one Python already has loaded)
 # rather than a private static copy, so std::cout and locales are shared.
 STDCXX := $(firstword $(wildcard /usr/lib/x86_64-linux-gnu/libstdc++.so.6 /usr/lib64/libstdc++.so.6))
+# OpenMP runtime linked directly (the compiler driver's libgomp.spec may be absent)
+GOMP := $(firstword $(wildcard /usr/lib/x86_64-linux-gnu/libgomp.so.1 /usr/lib64/libgomp.so.1))
 
 all: $(OUT)/libwcref.so $(OUT)/libwcref_omp.so
 
@@ -48,6 +50,6 @@ $(OUT)/libwcref.so: $(OBJS_S) $(OUT)/harness-serial.o
 	$(CXX) -shared -o $@ $^ $(STDCXX) -lpthread
 
 $(OUT)/libwcref_omp.so: $(OBJS_P) $(OUT)/harness-omp.o
-	$(CXX) -shared -fopenmp -o $@ $^ $(STDCXX) -lpthread
+	$(CXX) -shared -o $@ $^ $(STDCXX) $(GOMP) -lpthread
 
 .PHONY: all
