@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
 #include <string>
@@ -185,6 +186,8 @@ int wcg_create(const wcg_params* params, wcg_ctx** out) {
   p.precision = params->precision;
   p.refine_inner_tol = params->refine_inner_tol > 0 ? params->refine_inner_tol : 0.0;
   p.max_refinements = params->max_refinements > 0 ? params->max_refinements : 20;
+  // wavefront tile shape (performance knob; both compute identical results)
+  if (const char* v = getenv("WCG_SWEEP_TILE")) ctx->c.sweep_variant = !strcmp(v, "warp") ? 1 : 0;
   cudaError_t e = wcg::ctx_init(ctx->c);
   if (e != cudaSuccess) {
     std::string m = std::string("context init: ") + cudaGetErrorString(e);

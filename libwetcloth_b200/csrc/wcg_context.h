@@ -129,7 +129,8 @@ struct Context {
   DevBuf tile_active;            // uint8 per tile
   DevBuf tile_part;              // per-ticket partial sums / maxima (double)
   int tile_epoch = 0;
-  int nti = 0, ntj = 0, ntk = 0; // tiles per axis (2x2x2 buckets each)
+  int nti = 0, ntj = 0, ntk = 0; // tiles per axis
+  int sweep_variant = 0;         // 0: 8x8x8 block tiles, 1: 8x4x8 warp tiles
   long long n_tiles = 0;         // active tiles
   long long n_active = 0;
   int drange_h[6] = {0, 0, 0, 1, 1, 1};  // min/max stencil offset per axis

@@ -10,6 +10,7 @@
 #include "wcg_context.h"
 #include "wcg_kernels.cuh"
 #include "wcg_pcg.cuh"
+#include "wcg_wsweep.cuh"
 #include "wcg_scan.cuh"
 
 namespace wcg {
@@ -339,8 +340,9 @@ static cudaError_t build_grid_t(Context& c) {
     WCG_TRY(c.active.ensure((size_t)bcap));
     WCG_TRY(c.active_list.ensure((size_t)bcap * sizeof(int)));
   }
+  // wavefront tiles: 8x8x8 cells (2x2x2 buckets) or 8x4x8 (2x1x2)
   c.nti = (g.ni + 1) / 2;
-  c.ntj = (g.nj + 1) / 2;
+  c.ntj = c.sweep_variant == 1 ? g.nj : (g.nj + 1) / 2;
   c.ntk = (g.nk + 1) / 2;
   const long long ntot = (long long)c.nti * c.ntj * c.ntk;
   if ((size_t)ntot * sizeof(int) > c.tile_flag.bytes) {
@@ -387,8 +389,12 @@ static cudaError_t build_grid_t(Context& c) {
   // tiles (2x2x2 buckets) with an active bucket, compacted into tile_part as ints
   int* ttmp = tmpi + g.nb + 1;
   int* tlist = (int*)c.tile_part.p;
-  ++c.launches, k_tile_active<<<nblk(ntot, 256), 256, 0, c.stream>>>(
-      g, c.nti, c.ntj, c.ntk, c.active.as<unsigned char>(), c.tile_active.as<unsigned char>());
+  if (c.sweep_variant == 1)
+    ++c.launches, k_wtile_active<<<nblk(ntot, 256), 256, 0, c.stream>>>(
+        g, c.nti, c.ntj, c.ntk, c.active.as<unsigned char>(), c.tile_active.as<unsigned char>());
+  else
+    ++c.launches, k_tile_active<<<nblk(ntot, 256), 256, 0, c.stream>>>(
+        g, c.nti, c.ntj, c.ntk, c.active.as<unsigned char>(), c.tile_active.as<unsigned char>());
   ++c.launches, k_flag_to_int<<<nblk(ntot, 256), 256, 0, c.stream>>>(
       c.tile_active.as<unsigned char>(), ntot, ttmp);
   exclusive_scan<int, int>(ttmp, ntot, ttmp, (int*)part, dtotal + 1, c.stream);
@@ -520,9 +526,15 @@ static cudaError_t sweep(Context& c, int mode, SweepArgs<R> a) {
   a.epoch = ++c.tile_epoch;
   WCG_TRY(cudaMemsetAsync(c.ticket.p, 0, sizeof(int), c.stream));
   const unsigned nt = (unsigned)c.n_tiles;
-  if (mode == kFactor) ++c.launches, k_sweep<R, kFactor><<<nt, kSweepThreads, 0, c.stream>>>(a);
-  else if (mode == kForward) ++c.launches, k_sweep<R, kForward><<<nt, kSweepThreads, 0, c.stream>>>(a);
-  else ++c.launches, k_sweep<R, kBackward><<<nt, kSweepThreads, 0, c.stream>>>(a);
+  if (c.sweep_variant == 1) {
+    if (mode == kFactor) ++c.launches, k_wfactor<R><<<nt, 32, 0, c.stream>>>(a);
+    else if (mode == kForward) ++c.launches, k_wsweep<R, kForward><<<nt, 32, 0, c.stream>>>(a);
+    else ++c.launches, k_wsweep<R, kBackward><<<nt, 32, 0, c.stream>>>(a);
+  } else {
+    if (mode == kFactor) ++c.launches, k_sweep<R, kFactor><<<nt, kSweepThreads, 0, c.stream>>>(a);
+    else if (mode == kForward) ++c.launches, k_sweep<R, kForward><<<nt, kSweepThreads, 0, c.stream>>>(a);
+    else ++c.launches, k_sweep<R, kBackward><<<nt, kSweepThreads, 0, c.stream>>>(a);
+  }
   return cudaGetLastError();
 }
 
