@@ -155,6 +155,29 @@ int wcg_profile_end(wcg_ctx* ctx, double* ms, long long* launches, int ncat);
 int wcg_profile_num_phases(void);
 const char* wcg_profile_phase_name(int i);
 
+/* ---- allocation-free pressure solve ----
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * (an application that owns and pre-reserves all device memory, a strict
+ * memory pool or budget, code that must not allocate between frames): solves
+ * an already assembled pressure system with the same FP64 MIC(0)-PCG as
+ * wcg_project_fine, taking all solver scratch from one static device array
+ * of about 17 MB that every GPU loading this library holds until exit.
+ * Inputs are dense bucket-major device arrays over ni*nj*nk buckets (64 cells
+ * each, index bucket*64 + k*16 + j*4 + i): the DOF mask (nonzero = unknown),
+ * the diagonal, the couplings a_x/a_y/a_z between a cell and its +x/+y/+z
+ * neighbour, and the rhs; pressure (device, same layout) receives the
+ * solution (0 off the DOFs).  Stops when ||r||_inf <= criterion ||rhs||_inf.
+ * At most 2048 buckets (131072 cells); larger grids are rejected with
+ * WCG_ERR_ARG.  The first call on a device looks up the array's device
+ * address (make that first call before any stream capture).  Calls share the
+ * array: calls whose GPU work overlaps race and must be serialised. */
+int wcg_pressure_solve_noalloc(int ni, int nj, int nk, const unsigned char* dof,
+                               const double* a_diag, const double* a_x,
+                               const double* a_y, const double* a_z,
+                               const double* rhs, double* pressure,
+                               double criterion, int maxiters, void* stream,
+                               int* iters_out, double* residual_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -96,6 +96,12 @@ SIGNATURES = {
     "wcg_profile_end": (ctypes.c_int, [ctypes.c_void_p, _D, _L, ctypes.c_int]),
     "wcg_profile_num_phases": (ctypes.c_int, []),
     "wcg_profile_phase_name": (ctypes.c_char_p, [ctypes.c_int]),
+    "wcg_pressure_solve_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                  ctypes.c_void_p, ctypes.c_void_p,
+                                                  ctypes.c_void_p, ctypes.c_void_p,
+                                                  ctypes.c_void_p, ctypes.c_void_p,
+                                                  ctypes.c_void_p, ctypes.c_double,
+                                                  ctypes.c_int, ctypes.c_void_p, _I, _D]),
 }
 
 _lib = None

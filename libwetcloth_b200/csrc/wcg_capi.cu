@@ -134,6 +134,11 @@ std::vector<unsigned char> host_bytes(const void* dev, long long n) {
 
 }  // namespace
 
+int wcg::set_last_error(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
 extern "C" {
 
 const char* wcg_last_error(void) { return g_err.c_str(); }

@@ -207,5 +207,11 @@ cudaError_t map_grid_to_particles_and_advect(Context& c, double dt, bool advect)
 cudaError_t advect_only(Context& c, double dt);
 cudaError_t num_substeps(Context& c, double dt, int* n);
 cudaError_t substep(Context& c, double dt);
+// record the message returned by wcg_last_error() on this thread; returns code
+int set_last_error(int code, const std::string& msg);
+// FP64 MIC(0)-PCG on a system already placed in the context's fields
+// (G_ADIAG, G_AX/AY/AZ, G_B) with caller-provided buffers; writes p to out.
+cudaError_t prepared_solve_fp64(Context& c, double* out, int* iters, double* res,
+                                int* converged, double* rhs_norm);
 
 }  // namespace wcg

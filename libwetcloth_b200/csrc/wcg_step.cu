@@ -964,6 +964,87 @@ cudaError_t num_substeps(Context& c, double dt, int* n) {
   return cudaSuccess;
 }
 
+// ---------------------------------------------------------------------------
+// Solve of a caller-assembled system on a context whose buffers were set up
+// by the caller (used by the allocation-free entry point in wcg_noalloc.cu).
+// Every bucket counts as active; the DOF mask selects the unknowns.  FP64,
+// the same MIC(0)-PCG as project_fine.
+cudaError_t prepared_solve_fp64(Context& c, double* out, int* iters, double* res,
+                                int* converged, double* rhs_norm) {
+  const GridDesc& g = c.g;
+  double* F = c.gfield.as<double>();
+  double* dsc = c.dscalars.as<double>();
+  double* part = c.scratch.as<double>();
+  int* tmpi = c.cell_cursor.as<int>();
+  unsigned char* act = c.active.as<unsigned char>();
+  *iters = 0;
+  *res = 0;
+  *converged = 1;
+  *rhs_norm = 0;
+  // all buckets active, list = 0..nb-1
+  WCG_TRY(cudaMemsetAsync(act, 1, g.nb, c.stream));
+  ++c.launches, k_flag_to_int<<<nblk(g.nb, 256), 256, 0, c.stream>>>(act, g.nb, tmpi);
+  exclusive_scan<int, int>(tmpi, g.nb, tmpi, (int*)part, (int*)(dsc + 16), c.stream);
+  ++c.launches, k_compact<<<nblk(g.nb, 256), 256, 0, c.stream>>>(act, tmpi, g.nb,
+                                                                 c.active_list.as<int>());
+  c.n_active = g.nb;
+  // wavefront tiles (8x8x8 cells) ordered by wave
+  c.sweep_variant = 0;
+  c.nti = (g.ni + 1) / 2;
+  c.ntj = (g.nj + 1) / 2;
+  c.ntk = (g.nk + 1) / 2;
+  const long long ntot = (long long)c.nti * c.ntj * c.ntk;
+  const int nwave = c.nti + c.ntj + c.ntk;
+  int* ttmp = tmpi + g.nb + 1;
+  int* tlist = (int*)c.tile_part.p;
+  ++c.launches, k_tile_active<<<nblk(ntot, 256), 256, 0, c.stream>>>(
+      g, c.nti, c.ntj, c.ntk, act, c.tile_active.as<unsigned char>());
+  ++c.launches, k_flag_to_int<<<nblk(ntot, 256), 256, 0, c.stream>>>(
+      c.tile_active.as<unsigned char>(), ntot, ttmp);
+  exclusive_scan<int, int>(ttmp, ntot, ttmp, (int*)part, (int*)(dsc + 16) + 1, c.stream);
+  ++c.launches, k_compact<<<nblk(ntot, 256), 256, 0, c.stream>>>(
+      c.tile_active.as<unsigned char>(), ttmp, ntot, tlist);
+  int* wcount = c.wave_count.as<int>();
+  int* wcursor = wcount + (nwave + 2);
+  WCG_TRY(cudaMemsetAsync(wcount, 0, (nwave + 2) * sizeof(int), c.stream));
+  ++c.launches, k_tile_wave_count<<<nblk(ntot, 256), 256, 0, c.stream>>>(c.nti, c.ntj, tlist,
+                                                                         ntot, wcount);
+  exclusive_scan<int, int>(wcount, nwave + 1, wcursor, (int*)part, nullptr, c.stream);
+  ++c.launches, k_tile_wave_scatter<<<nblk(ntot, 256), 256, 0, c.stream>>>(
+      c.nti, c.ntj, tlist, ntot, wcursor, c.wave_list.as<int>());
+  c.n_tiles = ntot;
+  WCG_TRY(cudaGetLastError());
+  // the solve (project_fine_t minus assembly)
+  const int* al = c.active_list.as<int>();
+  const unsigned char* dof = c.gdof.as<unsigned char>();
+  const long long nent = c.n_active * 64;
+  double h[2];
+  absmax<double>(c, F + G_B * c.gcap, dsc + 4);
+  WCG_TRY(fetch(c, dsc + 4, 1, h));
+  const double bnorm = h[0];
+  *rhs_norm = bnorm;
+  if (bnorm < 1e-30) {
+    WCG_TRY(cudaMemsetAsync(out, 0, g.nnode * sizeof(double), c.stream));
+    return cudaStreamSynchronize(c.stream);
+  }
+  {
+    const double zero = 0.0;
+    WCG_TRY(set_scalars(c, S_DONE, &zero, 1));
+  }
+  WCG_TRY(sweep<double>(c, kFactor, sweep_args<double>(c)));
+  double* r = F + G_R * c.gcap;
+  double* x = F + G_X * c.gcap;
+  WCG_TRY(cudaMemsetAsync(x, 0, g.nnode * sizeof(double), c.stream));
+  ++c.launches, k_copy_dof<double><<<kRedBlocks, kRedThreads, 0, c.stream>>>(
+      al, nent, dof, F + G_B * c.gcap, r);
+  int conv = 0;
+  WCG_TRY(pcg_inner<double>(c, r, x, c.prm.criterion * bnorm, c.prm.maxiters, iters, &conv, res));
+  *converged = conv;
+  ++c.launches, k_copy_dof<double><<<kRedBlocks, kRedThreads, 0, c.stream>>>(al, nent, dof, x, out);
+  WCG_TRY(cudaGetLastError());
+  return cudaStreamSynchronize(c.stream);
+}
+
 cudaError_t substep(Context& c, double dt) {
   WCG_TRY(build_grid(c));
   WCG_TRY(map_particles_to_grid(c));
