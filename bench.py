@@ -148,6 +148,17 @@ def traffic_per_launch(kernel_phase, ndof, np_):
     return e["bytes_per_unit"] * units
 
 
+def reduce_max(x, world, device):
+    """Maximum of a per-rank scalar over all ranks (the timing rule: a
+    multi-GPU time is the slowest rank's)."""
+    if world == 1:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
 # ---------------------------------------------------------------------------
 def run_ours(args, rank, world, dev):
     import numpy as np
@@ -161,11 +172,7 @@ def run_ours(args, rank, world, dev):
             torch.distributed.barrier()
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(x, world, f"cuda:{dev}")
 
     t0 = time.time()
     sc = scenes.half_box(args.n, args.ppc, seed=1 + rank)

@@ -132,6 +132,7 @@ struct Context {
   int nti = 0, ntj = 0, ntk = 0; // tiles per axis
   int sweep_variant = 0;         // 0: 8x8x8 block tiles, 1: 8x4x8 warp tiles
   long long n_tiles = 0;         // active tiles
+  long long n_tiles_total = 0;   // all tiles of the grid (partials are indexed by tile id)
   long long n_active = 0;
   int drange_h[6] = {0, 0, 0, 1, 1, 1};  // min/max stencil offset per axis
   DevBuf active_list;            // compacted active buckets (int32)

@@ -117,7 +117,7 @@ struct SweepArgs {
   const R* q;
   double* sc;      // device scalars
   int update;      // forward: apply the PCG x/r update first
-  double* part;    // per-ticket partial: forward max|r|, backward z.r
+  double* part;    // per-tile partial (indexed by tile id): forward max|r|, backward z.r
   R omega, min_ratio;
   int* err;
 };
@@ -335,11 +335,11 @@ __global__ void __launch_bounds__(kSweepThreads)
   }
   if (MODE == kForward && a.update && a.part) {
     const double m = block_max<double>(rmax, red);
-    if (tid == 0) a.part[t] = m;
+    if (tid == 0) a.part[tl] = m;
   }
   if (MODE == kBackward && a.part) {
     const double sm = block_sum<double>(dsum, red);
-    if (tid == 0) a.part[t] = sm;
+    if (tid == 0) a.part[tl] = sm;
   }
   __threadfence();
   __syncthreads();

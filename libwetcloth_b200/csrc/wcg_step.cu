@@ -420,6 +420,10 @@ static cudaError_t build_grid_t(Context& c) {
     ++c.launches, k_tile_wave_scatter<<<nblk(c.n_tiles, 256), 256, 0, c.stream>>>(
         c.nti, c.ntj, tlist, c.n_tiles, wcursor, c.wave_list.as<int>());
   }
+  // per-tile partials are indexed by tile id and reduced over all tiles in
+  // index order (deterministic whatever order a wave's tiles were listed in)
+  c.n_tiles_total = ntot;
+  WCG_TRY(cudaMemsetAsync(c.tile_part.p, 0, ntot * sizeof(double), c.stream));
   // 8. counting sort by key node, deterministic within a cell
   exclusive_scan<int, int>(cstart, g.nnode, cstart, (int*)part, cstart + g.nnode, c.stream);
   WCG_TRY(cudaMemsetAsync(tmpi, 0, g.nnode * sizeof(int), c.stream));
@@ -615,7 +619,7 @@ static cudaError_t pcg_inner(Context& c, R* r, R* x, double tol_abs, int maxiter
   WCG_TRY(sweep<R>(c, kBackward, ba));
   {
     ProfScope prof(c, P_PCGVEC);
-    ++c.launches, k_red_beta<<<1, kRedThreads, 0, c.stream>>>(tpart, (int)c.n_tiles, sc, 1);
+    ++c.launches, k_red_beta<<<1, kRedThreads, 0, c.stream>>>(tpart, (int)c.n_tiles_total, sc, 1);
   }
   double h[9];
   WCG_TRY(fetch(c, sc + S_RHO, 1, h));
@@ -641,12 +645,12 @@ static cudaError_t pcg_inner(Context& c, R* r, R* x, double tol_abs, int maxiter
       WCG_TRY(sweep<R>(c, kForward, fa));
       {
         ProfScope prof(c, P_PCGVEC);
-        ++c.launches, k_red_conv<<<1, kRedThreads, 0, c.stream>>>(tpart, (int)c.n_tiles, sc);
+        ++c.launches, k_red_conv<<<1, kRedThreads, 0, c.stream>>>(tpart, (int)c.n_tiles_total, sc);
       }
       WCG_TRY(sweep<R>(c, kBackward, ba));
       {
         ProfScope prof(c, P_PCGVEC);
-        ++c.launches, k_red_beta<<<1, kRedThreads, 0, c.stream>>>(tpart, (int)c.n_tiles, sc, 0);
+        ++c.launches, k_red_beta<<<1, kRedThreads, 0, c.stream>>>(tpart, (int)c.n_tiles_total, sc, 0);
       }
       R* t = sold;
       sold = snew;
@@ -1013,6 +1017,8 @@ cudaError_t prepared_solve_fp64(Context& c, double* out, int* iters, double* res
   ++c.launches, k_tile_wave_scatter<<<nblk(ntot, 256), 256, 0, c.stream>>>(
       c.nti, c.ntj, tlist, ntot, wcursor, c.wave_list.as<int>());
   c.n_tiles = ntot;
+  c.n_tiles_total = ntot;
+  WCG_TRY(cudaMemsetAsync(c.tile_part.p, 0, ntot * sizeof(double), c.stream));
   WCG_TRY(cudaGetLastError());
   // the solve (project_fine_t minus assembly)
   const int* al = c.active_list.as<int>();

@@ -299,13 +299,13 @@ __global__ void __launch_bounds__(32)
       const double v = __shfl_xor_sync(kFull, rmax, o);
       rmax = v > rmax ? v : rmax;
     }
-    if (lane == 0) a.part[t] = rmax;
+    if (lane == 0) a.part[tl] = rmax;
   }
   if (MODE == kBackward && a.part) {
     // fixed butterfly order: deterministic
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) dsum += __shfl_xor_sync(kFull, dsum, o);
-    if (lane == 0) a.part[t] = dsum;
+    if (lane == 0) a.part[tl] = dsum;
   }
   __threadfence();
   __syncwarp();

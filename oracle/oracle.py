@@ -1,0 +1,120 @@
+"""ctypes binding of oracle/_build/libwcoracle.so, the C restatement of the
+liquid fluid-step hot path (oracle/wc_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: the checker for libwcgpu.  Same snapshot API as
+oracle/ref.py (the compiled reference), so tests can compare any pair.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "libwcoracle.so")
+_D = ctypes.POINTER(ctypes.c_double)
+_L = ctypes.POINTER(ctypes.c_longlong)
+_I = ctypes.POINTER(ctypes.c_int)
+_lib = None
+
+
+def available() -> bool:
+    return os.path.exists(LIB)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        L = ctypes.CDLL(LIB)
+        L.wco_create.restype = ctypes.c_void_p
+        L.wco_create.argtypes = [ctypes.c_double, _D, ctypes.c_double, ctypes.c_double,
+                                 ctypes.c_double, _D, _D, ctypes.c_double, ctypes.c_double,
+                                 ctypes.c_int, ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _D, _D]
+        L.wco_destroy.argtypes = [ctypes.c_void_p]
+        L.wco_step.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
+        L.wco_step.restype = ctypes.c_int
+        L.wco_substep.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
+        L.wco_size.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+        L.wco_size.restype = ctypes.c_longlong
+        L.wco_get_f.argtypes = [ctypes.c_void_p, ctypes.c_char_p, _D]
+        L.wco_get_i.argtypes = [ctypes.c_void_p, ctypes.c_char_p, _L]
+        L.wco_solver_stats.argtypes = [ctypes.c_void_p, _I, _D]
+        L.wco_pcg_solve.restype = ctypes.c_int
+        L.wco_pcg_solve.argtypes = [ctypes.c_int, _I, _I, _D, _D, _D, ctypes.c_double,
+                                    ctypes.c_int, ctypes.c_double, ctypes.c_double, _D, _I]
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(_D)
+
+
+class OracleScene:
+    """The C restatement of one liquid scene (same API as oracle.ref.RefScene)."""
+
+    def __init__(self, scene):
+        L = lib()
+        p = scene.params
+        self._keep = []
+
+        def arr(a):
+            a = np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+            self._keep.append(a)
+            return _dp(a)
+
+        C = None if scene.C is None else arr(scene.C)
+        self.h = L.wco_create(p.dx, arr(p.gravity), p.liquid_density, p.flip_coeff,
+                              p.liquid_boundary_friction, arr(p.box_center), arr(p.box_half),
+                              p.box_radius, p.criterion, p.maxiters, 1, scene.x.shape[0],
+                              arr(scene.x), arr(scene.v), C, arr(scene.mass), arr(scene.vol),
+                              arr(scene.radius))
+        self.L = L
+
+    def close(self):
+        if self.h:
+            self.L.wco_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, dt, snapshot=True):
+        return self.L.wco_step(self.h, dt, 1 if snapshot else 0)
+
+    def get(self, name):
+        n = self.L.wco_size(self.h, name.encode())
+        if n < 0:
+            raise KeyError(name)
+        out = np.empty(n, dtype=np.float64)
+        if self.L.wco_get_f(self.h, name.encode(), _dp(out)) == 0:
+            return out
+        out = np.empty(n, dtype=np.int64)
+        self.L.wco_get_i(self.h, name.encode(), out.ctypes.data_as(_L))
+        return out
+
+    def solver_stats(self):
+        it = ctypes.c_int(0)
+        res = ctypes.c_double(0)
+        self.L.wco_solver_stats(self.h, ctypes.byref(it), ctypes.byref(res))
+        return it.value, res.value
+
+
+def pcg_solve(rowstart, col, val, rhs, tol, maxiters, omega=0.97, min_ratio=0.25):
+    """MIC(0)-PCG of robertbridson::PCGSolver on a CSR matrix (sorted rows)."""
+    L = lib()
+    n = len(rhs)
+    rs = np.ascontiguousarray(rowstart, dtype=np.int32)
+    cl = np.ascontiguousarray(col, dtype=np.int32)
+    va = np.ascontiguousarray(val, dtype=np.float64)
+    b = np.ascontiguousarray(rhs, dtype=np.float64)
+    x = np.zeros(n)
+    res = ctypes.c_double(0)
+    it = ctypes.c_int(0)
+    ok = L.wco_pcg_solve(n, rs.ctypes.data_as(_I), cl.ctypes.data_as(_I), _dp(va), _dp(b), _dp(x),
+                         tol, maxiters, omega, min_ratio, ctypes.byref(res), ctypes.byref(it))
+    return x, bool(ok), it.value, res.value

@@ -1,0 +1,1323 @@
+/*
+ * wc_oracle.c -- CPU restatement of libWetCloth's liquid fluid-step hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is the checker for libwcgpu (tests,
+ * __graft_entry__.smoke and bench.py's CPU-baseline leg may use it); no
+ * product code links it.  It restates, in plain C99 and serially, the
+ * algorithm of the reference for a liquid-only scene with box walls, in the
+ * reference's own orders (sort keys, 27-colour bucket traversal, per-node
+ * particle lists, sorted sparse rows, column-oriented MIC(0)), and is pinned
+ * against the compiled reference (oracle/_ref) by the CPU tests and the
+ * golden fixtures under tests/golden/.
+ *
+ * Every function cites the reference routine (file:line under
+ * libWetCloth/Core/) it restates.  Node fields are stored densely over all
+ * buckets (bucket * 64 + k*16 + j*4 + i); inactive buckets read back as NaN.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define NN 4          /* nodes per bucket side (bucketinfo numcells) */
+#define NPB 64        /* nodes per bucket */
+
+typedef struct {
+  double dx, g[3], rho, flip, friction, bc[3], bh[3], br, criterion;
+  int maxiters, mic;
+} Params;
+
+typedef struct {
+  char name[32];
+  int is_int;
+  long long n;
+  double* f;
+  long long* i;
+} Snap;
+
+typedef struct {
+  /* CSR list of (particle, slot) pairs per node */
+  int* start; /* nnode + 1 */
+  int* pid;
+  int* slot;
+} Pairs;
+
+typedef struct {
+  Params p;
+  int np;
+  double *x, *v, *C, *m, *vol, *rad;  /* particle state (x3, v3, C9) */
+  /* grid */
+  double bbmin[3], bbmax[3], org[3], bs;
+  int ni, nj, nk;
+  long long nb, nnode;
+  uint64_t* keys;
+  int* sup; /* 2 per bucket */
+  unsigned char *act;
+  int* base; /* np * 15: u, v, w, sphi, p stencil base (global node ijk) */
+  unsigned char* inside;
+  double *wu, *wv, *ww, *wp; /* np * 27 */
+  Pairs pu, pv, pw, pp;
+  /* node fields */
+  double *mass[3], *vel[3], *vol_f[3], *sat[3], *psi[3], *wgt[3], *svel[3];
+  double *sat_p, *psi_p, *pore_p, *lphi, *sphi, *pressure;
+  double *rhs[3], *vstar[3], *invC[3], *psifs[3], *psisf[3], *mshdvm[3], *mfhdvm[3];
+  unsigned char* valid[3];
+  /* pressure system */
+  long long* dofidx;
+  int ndof;
+  int *rowstart, *col;
+  double* val;
+  double* b;
+  int last_iters;
+  double last_res;
+  double timers[12];
+  Snap snaps[160];
+  int nsnaps;
+} Scene;
+
+/* ---------------------------------------------------------------------- */
+static void snap_put_f(Scene* s, const char* name, const double* a, long long n) {
+  Snap* t = NULL;
+  for (int k = 0; k < s->nsnaps; ++k)
+    if (!strcmp(s->snaps[k].name, name)) t = &s->snaps[k];
+  if (!t) {
+    t = &s->snaps[s->nsnaps++];
+    memset(t, 0, sizeof(*t));
+    strncpy(t->name, name, 31);
+  }
+  free(t->f);
+  free(t->i);
+  t->i = NULL;
+  t->is_int = 0;
+  t->n = n;
+  t->f = (double*)malloc(sizeof(double) * (n > 0 ? n : 1));
+  memcpy(t->f, a, sizeof(double) * n);
+}
+
+static void snap_put_i(Scene* s, const char* name, const long long* a, long long n) {
+  Snap* t = NULL;
+  for (int k = 0; k < s->nsnaps; ++k)
+    if (!strcmp(s->snaps[k].name, name)) t = &s->snaps[k];
+  if (!t) {
+    t = &s->snaps[s->nsnaps++];
+    memset(t, 0, sizeof(*t));
+    strncpy(t->name, name, 31);
+  }
+  free(t->f);
+  free(t->i);
+  t->f = NULL;
+  t->is_int = 1;
+  t->n = n;
+  t->i = (long long*)malloc(sizeof(long long) * (n > 0 ? n : 1));
+  memcpy(t->i, a, sizeof(long long) * n);
+}
+
+/* dense node field, NaN in inactive buckets */
+static void snap_node(Scene* s, const char* name, const double* a) {
+  double* t = (double*)malloc(sizeof(double) * s->nnode);
+  for (long long n = 0; n < s->nnode; ++n) t[n] = s->act[n >> 6] ? a[n] : NAN;
+  snap_put_f(s, name, t, s->nnode);
+  free(t);
+}
+
+/* ---------------------------------------------------------------------- */
+static inline long long bucket_index(const Scene* s, int i, int j, int k) {
+  return ((long long)k * s->nj + j) * s->ni + i;
+}
+
+/* global node (I,J,K) -> dense index; -1 outside the grid */
+static inline long long node_of(const Scene* s, int I, int J, int K) {
+  if (I < 0 || J < 0 || K < 0 || I >= s->ni * NN || J >= s->nj * NN || K >= s->nk * NN)
+    return -1;
+  return bucket_index(s, I / NN, J / NN, K / NN) * NPB + (K % NN) * 16 + (J % NN) * 4 + (I % NN);
+}
+
+static inline int node_active(const Scene* s, long long n) { return n >= 0 && s->act[n >> 6]; }
+
+/* TwoDScene::getNodePos{X,Y,Z,P,SolidPhi} for an active bucket
+ * (TwoDScene.cpp:3776-3813 with generateNodes :3870-3876):
+ * m_node_pos = (handle*bs + origin) + local*dx, then + offset*dx;
+ * for an inactive bucket nodePosFromBucket (:2064-2078). */
+static double node_coord(const Scene* s, int a, int I, double off) {
+  const int h = I >= 0 ? I / NN : (I - NN + 1) / NN;
+  const int l = I - h * NN;
+  double c = (double)h * s->bs + s->org[a];
+  c = c + (double)l * s->p.dx;
+  return c + off * s->p.dx;
+}
+
+static double node_coord_inactive(const Scene* s, int a, int I, double off) {
+  const int h = I >= 0 ? I / NN : (I - NN + 1) / NN;
+  const int l = I - h * NN;
+  const double corner = s->org[a] + (double)h * s->bs;
+  return corner + ((double)l + off) * s->p.dx;
+}
+
+/* quad_kernel, MathUtilities.h:416-424 */
+static double quad_kernel(double x) {
+  const double d = fabs(x);
+  if (d < 0.5) return 0.75 - d * d;
+  if (d < 1.5) return 0.5 * (1.5 - d) * (1.5 - d);
+  return 0.0;
+}
+
+/* fraction_inside (2 values), MathUtilities.h:286-293 */
+static double frac_in2(double l, double r) {
+  if (l < 0 && r < 0) return 1;
+  if (l < 0 && r >= 0) return l / (l - r);
+  if (l >= 0 && r < 0) return r / (r - l);
+  return 0;
+}
+
+static void cycle4(double* a) {
+  const double t = a[0];
+  a[0] = a[1];
+  a[1] = a[2];
+  a[2] = a[3];
+  a[3] = t;
+}
+
+/* fraction_inside (4 corners), MathUtilities.h:301-376 */
+static double frac_in4(double bl, double br, double tl, double tr) {
+  const int inside = (bl < 0) + (tl < 0) + (br < 0) + (tr < 0);
+  double l[4] = {bl, br, tr, tl};
+  if (inside == 4) return 1.;
+  if (inside == 3) {
+    while (l[0] < 0) cycle4(l);
+    const double s0 = 1. - frac_in2(l[0], l[3]);
+    const double s1 = 1. - frac_in2(l[0], l[1]);
+    return 1. - 0.5 * s0 * s1;
+  }
+  if (inside == 2) {
+    while (l[0] >= 0 || !(l[1] < 0 || l[2] < 0)) cycle4(l);
+    if (l[1] < 0) return 0.5 * (frac_in2(l[0], l[3]) + frac_in2(l[1], l[2]));
+    if (0.25 * (l[0] + l[1] + l[2] + l[3]) < 0) {
+      double area = 0.;
+      area += 0.5 * (1. - frac_in2(l[0], l[3])) * (1. - frac_in2(l[2], l[3]));
+      area += 0.5 * (1 - frac_in2(l[0], l[1])) * (1 - frac_in2(l[2], l[1]));
+      return 1. - area;
+    }
+    double area = 0.;
+    area += 0.5 * frac_in2(l[0], l[1]) * frac_in2(l[0], l[3]);
+    area += 0.5 * frac_in2(l[2], l[1]) * frac_in2(l[2], l[3]);
+    return area;
+  }
+  if (inside == 1) {
+    while (l[0] >= 0) cycle4(l);
+    return 0.5 * frac_in2(l[0], l[3]) * frac_in2(l[0], l[1]);
+  }
+  return 0;
+}
+
+static double clampd(double a, double lo, double hi) { return a < lo ? lo : (a > hi ? hi : a); }
+
+/* Solid walls: DistanceFieldObject DFT_BOX, inside (sign -1)
+ * (DistanceFields.cpp:68-78, :607-615) under a DFT_UNION operator
+ * (:866-880, start 1e20) and TwoDScene::computePhiVel (TwoDScene.cpp:5427-5448,
+ * running minimum from 3*bucket_size).  Static: velocity 0. */
+static double wall_phi(const Scene* s, double px, double py, double pz) {
+  const double p[3] = {px, py, pz};
+  double d[3], da[3];
+  for (int a = 0; a < 3; ++a) {
+    const double rp = (p[a] - s->p.bc[a]) + s->p.bc[a];
+    d[a] = fabs(rp - s->p.bc[a]) - s->p.bh[a];
+    da[a] = d[a] > 0.0 ? d[a] : 0.0;
+  }
+  double m = d[0] > d[1] ? d[0] : d[1];
+  m = m > d[2] ? m : d[2];
+  m = m < 0.0 ? m : 0.0;
+  const double box = m + sqrt(da[0] * da[0] + da[1] * da[1] + da[2] * da[2]) - s->p.br;
+  const double phi = -1.0 * box;
+  double u = 1e20;
+  if (phi < u) u = phi;
+  double r = 3.0 * s->bs;
+  if (u < r) r = u;
+  return r;
+}
+
+/* ---------------------------------------------------------------------- */
+/* TwoDScene::updateParticleBoundingBox (TwoDScene.cpp:1588-1612) and
+ * rebucketizeParticles (:1657-1710) */
+static void build_grid(Scene* s) {
+  double mn[3] = {1e20, 1e20, 1e20}, mx[3] = {-1e20, -1e20, -1e20};
+  for (int i = 0; i < s->np; ++i)
+    for (int a = 0; a < 3; ++a) {
+      const double v = s->x[i * 3 + a];
+      if (v < mn[a]) mn[a] = v;
+      if (v > mx[a]) mx[a] = v;
+    }
+  const double d2 = s->bs * 2.0;
+  int nbk[3];
+  for (int a = 0; a < 3; ++a) {
+    s->bbmin[a] = floor(mn[a] / d2) * d2;
+    s->bbmax[a] = ceil(mx[a] / d2) * d2;
+    const double content = (s->bbmax[a] - s->bbmin[a]) + s->bs * 3.0 * 2.0;
+    int cells = (int)ceil(content / s->p.dx);
+    if (cells < 1) cells = 1;
+    const double gsize = (double)cells * s->p.dx;
+    s->org[a] = s->bbmin[a] - s->bs * 3.0;
+    nbk[a] = (int)ceil(gsize / s->bs);
+    if (nbk[a] < 1) nbk[a] = 1;
+  }
+  s->ni = nbk[0];
+  s->nj = nbk[1];
+  s->nk = nbk[2];
+  s->nb = (long long)s->ni * s->nj * s->nk;
+  s->nnode = s->nb * NPB;
+}
+
+static int cmp_u64(const void* a, const void* b) {
+  const uint64_t x = *(const uint64_t*)a, y = *(const uint64_t*)b;
+  return x < y ? -1 : (x > y ? 1 : 0);
+}
+
+/* Sorter::sort (Sorter.h:126-163) */
+static void sort_particles(Scene* s) {
+  free(s->keys);
+  free(s->sup);
+  s->keys = (uint64_t*)malloc(sizeof(uint64_t) * (s->np > 0 ? s->np : 1));
+  s->sup = (int*)calloc((size_t)s->nb * 2, sizeof(int));
+  const int nbk[3] = {s->ni, s->nj, s->nk};
+  for (int p = 0; p < s->np; ++p) {
+    int h[3];
+    for (int a = 0; a < 3; ++a) {
+      h[a] = (int)floor((s->x[p * 3 + a] - s->org[a]) / s->bs);
+      if (h[a] < 0) h[a] = 0;
+      if (h[a] > nbk[a] - 1) h[a] = nbk[a] - 1;
+    }
+    s->keys[p] = ((uint64_t)bucket_index(s, h[0], h[1], h[2]) << 32) | (uint64_t)p;
+  }
+  qsort(s->keys, s->np, sizeof(uint64_t), cmp_u64);
+  for (int q = 0; q < s->np; ++q) {
+    const unsigned b = (unsigned)(s->keys[q] >> 32);
+    const unsigned bp = q > 0 ? (unsigned)(s->keys[q - 1] >> 32) : 0xffffffffu;
+    const unsigned bn = q + 1 < s->np ? (unsigned)(s->keys[q + 1] >> 32) : 0xffffffffu;
+    if (b != bp) s->sup[b * 2] = q;
+    if (b != bn) s->sup[b * 2 + 1] = q + 1;
+  }
+}
+
+/* TwoDScene::findNodes (TwoDScene.cpp:3683-3760): stencil base per axis and
+ * bucket activation; resampleNodes (:5069-5119) runs it for the u, v, w,
+ * solid-phi and pressure offsets, then expandFluidNodesMarked(1)
+ * (:5021-5064) and markInsideOut (:447-490). */
+static void resample_nodes(Scene* s) {
+  free(s->act);
+  free(s->base);
+  free(s->inside);
+  s->act = (unsigned char*)calloc((size_t)s->nb, 1);
+  s->base = (int*)malloc(sizeof(int) * 15 * (s->np > 0 ? s->np : 1));
+  s->inside = (unsigned char*)malloc(s->np > 0 ? s->np : 1);
+  static const double offs[5][3] = {{0.0, 0.5, 0.5}, {0.5, 0.0, 0.5}, {0.5, 0.5, 0.0},
+                                    {0.0, 0.0, 0.0}, {0.5, 0.5, 0.5}};
+  for (int q = 0; q < s->np; ++q) {
+    const int p = (int)(s->keys[q] & 0xffffffffu);
+    const long long b = (long long)(s->keys[q] >> 32);
+    const int bk = (int)(b / ((long long)s->ni * s->nj));
+    const int bj = (int)((b - (long long)bk * s->ni * s->nj) / s->ni);
+    const int bi = (int)(b - ((long long)bk * s->ni * s->nj + (long long)bj * s->ni));
+    const int bh[3] = {bi, bj, bk};
+    for (int t = 0; t < 5; ++t) {
+      int lo[3];
+      for (int a = 0; a < 3; ++a) {
+        const double corner = ((double)bh[a] * s->bs + s->org[a]) + offs[t][a] * s->p.dx;
+        const double local = (s->x[p * 3 + a] - corner) / s->p.dx;
+        const double fl = floor(local);
+        const double fr = local - fl;
+        lo[a] = bh[a] * NN + (int)fl + (fr > 0.5 ? 0 : -1);
+        s->base[p * 15 + t * 3 + a] = lo[a];
+      }
+      for (int k = 0; k < 3; ++k)
+        for (int j = 0; j < 3; ++j)
+          for (int i = 0; i < 3; ++i) {
+            const int I = lo[0] + i, J = lo[1] + j, K = lo[2] + k;
+            const int hi = I >= 0 ? I / NN : -1, hj = J >= 0 ? J / NN : -1, hk = K >= 0 ? K / NN : -1;
+            if (hi < 0 || hj < 0 || hk < 0 || hi >= s->ni || hj >= s->nj || hk >= s->nk) continue;
+            s->act[bucket_index(s, hi, hj, hk)] = 1;  /* liquid particles are soft */
+          }
+    }
+  }
+  unsigned char* pre = (unsigned char*)malloc((size_t)s->nb);
+  memcpy(pre, s->act, (size_t)s->nb);
+  for (int k = 0; k < s->nk; ++k)
+    for (int j = 0; j < s->nj; ++j)
+      for (int i = 0; i < s->ni; ++i) {
+        const long long b = bucket_index(s, i, j, k);
+        if (pre[b]) continue;
+        int any = 0;
+        for (int t = -1; t <= 1 && !any; ++t)
+          for (int u = -1; u <= 1 && !any; ++u)
+            for (int r = -1; r <= 1 && !any; ++r) {
+              if (!t && !u && !r) continue;
+              const int x = i + r, y = j + u, z = k + t;
+              if (x < 0 || y < 0 || z < 0 || x >= s->ni || y >= s->nj || z >= s->nk) continue;
+              if (pre[bucket_index(s, x, y, z)]) any = 1;
+            }
+        if (any) s->act[b] = 1;
+      }
+  free(pre);
+  for (int p = 0; p < s->np; ++p) {
+    int comp = 0, uncomp = 0;
+    for (int t = 0; t < 3; ++t)
+      for (int k = 0; k < 3; ++k)
+        for (int j = 0; j < 3; ++j)
+          for (int i = 0; i < 3; ++i) {
+            const long long n = node_of(s, s->base[p * 15 + t * 3] + i, s->base[p * 15 + t * 3 + 1] + j,
+                                        s->base[p * 15 + t * 3 + 2] + k);
+            if (node_active(s, n)) comp = 1;
+            else uncomp = 1;
+          }
+    s->inside[p] = comp ? (uncomp ? 1 : 2) : 0;
+  }
+}
+
+/* getNodePos* of stencil node: active bucket formula or nodePosFromBucket */
+static void stencil_node_pos(const Scene* s, int I, int J, int K, const double* off, double* np) {
+  const long long n = node_of(s, I, J, K);
+  const int a = node_active(s, n);
+  np[0] = a ? node_coord(s, 0, I, off[0]) : node_coord_inactive(s, 0, I, off[0]);
+  np[1] = a ? node_coord(s, 1, J, off[1]) : node_coord_inactive(s, 1, J, off[1]);
+  np[2] = a ? node_coord(s, 2, K, off[2]) : node_coord_inactive(s, 2, K, off[2]);
+}
+
+/* TwoDScene::updateParticleWeights (TwoDScene.cpp:2084-2174):
+ * w = N_kernel<2>((x_p - x_n)/h) for the 27 nodes of each stencil */
+static void compute_weights(Scene* s) {
+  static const double offs[4][3] = {{0.0, 0.5, 0.5}, {0.5, 0.0, 0.5}, {0.5, 0.5, 0.0},
+                                    {0.5, 0.5, 0.5}};
+  double* W[4] = {s->wu, s->wv, s->ww, s->wp};
+  const int tmap[4] = {0, 1, 2, 4};
+  const double h = s->p.dx;
+  for (int p = 0; p < s->np; ++p) {
+    if (s->inside[p] == 0) continue;
+    for (int t = 0; t < 4; ++t) {
+      const int* lo = &s->base[p * 15 + tmap[t] * 3];
+      for (int k = 0; k < 3; ++k)
+        for (int j = 0; j < 3; ++j)
+          for (int i = 0; i < 3; ++i) {
+            double np[3];
+            stencil_node_pos(s, lo[0] + i, lo[1] + j, lo[2] + k, offs[t], np);
+            const double dxv[3] = {(s->x[p * 3] - np[0]) / h, (s->x[p * 3 + 1] - np[1]) / h,
+                                   (s->x[p * 3 + 2] - np[2]) / h};
+            W[t][p * 27 + k * 9 + j * 3 + i] =
+                quad_kernel(dxv[0]) * quad_kernel(dxv[1]) * quad_kernel(dxv[2]);
+          }
+    }
+  }
+}
+
+/* TwoDScene::buildNodeParticlePairs (TwoDScene.cpp:2257-2355): per-node
+ * (particle, slot) lists, appended in the 27-colour bucket traversal of
+ * Sorter::for_each_bucket_particles_colored (Sorter.h:403-437, numcolors 3). */
+static void build_pairs(Scene* s, Pairs* P, const double* W, int t) {
+  free(P->start);
+  free(P->pid);
+  free(P->slot);
+  P->start = (int*)calloc((size_t)s->nnode + 1, sizeof(int));
+  int* cursor = (int*)calloc((size_t)s->nnode, sizeof(int));
+  const int nc = 3;
+  const int sni = (s->ni + nc - 1) / nc, snj = (s->nj + nc - 1) / nc, snk = (s->nk + nc - 1) / nc;
+  for (int pass = 0; pass < 2; ++pass) {
+    if (pass == 1) {
+      for (long long n = 0; n < s->nnode; ++n) P->start[n + 1] += P->start[n];
+      const int tot = P->start[s->nnode];
+      P->pid = (int*)malloc(sizeof(int) * (tot > 0 ? tot : 1));
+      P->slot = (int*)malloc(sizeof(int) * (tot > 0 ? tot : 1));
+    }
+    for (int ct = 0; ct < nc; ++ct)
+      for (int cs = 0; cs < nc; ++cs)
+        for (int cr = 0; cr < nc; ++cr)
+          for (long long sb = 0; sb < (long long)sni * snj * snk; ++sb) {
+            const int sk = (int)(sb / ((long long)sni * snj));
+            const int sj = (int)((sb - (long long)sk * sni * snj) / sni);
+            const int si = (int)(sb - (long long)sk * sni * snj - (long long)sj * sni);
+            const int k = sk * nc + ct, j = sj * nc + cs, i = si * nc + cr;
+            if (k >= s->nk || j >= s->nj || i >= s->ni) continue;
+            const long long b = bucket_index(s, i, j, k);
+            if (!s->act[b]) continue;
+            for (int q = s->sup[b * 2]; q < s->sup[b * 2 + 1]; ++q) {
+              const int p = (int)(s->keys[q] & 0xffffffffu);
+              const int* lo = &s->base[p * 15 + t * 3];
+              for (int sl = 0; sl < 27; ++sl) {
+                const int di = sl % 3, dj = (sl / 3) % 3, dk = sl / 9;
+                const long long n = node_of(s, lo[0] + di, lo[1] + dj, lo[2] + dk);
+                if (!node_active(s, n) || !(W[p * 27 + sl] > 0.0)) continue;
+                if (pass == 0) {
+                  P->start[n + 1]++;
+                } else {
+                  const int at = P->start[n] + cursor[n]++;
+                  P->pid[at] = p;
+                  P->slot[at] = sl;
+                }
+              }
+            }
+          }
+  }
+  free(cursor);
+}
+
+/* TwoDScene::mapParticleNodesAPIC liquid branch (TwoDScene.cpp:6609-6919) */
+static void p2g(Scene* s) {
+  const double dV = s->p.dx * s->p.dx * s->p.dx;
+  Pairs* PP[3] = {&s->pu, &s->pv, &s->pw};
+  double* W[3] = {s->wu, s->wv, s->ww};
+  for (int a = 0; a < 3; ++a) {
+    for (long long n = 0; n < s->nnode; ++n) {
+      s->mass[a][n] = s->vel[a][n] = s->vol_f[a][n] = 0;
+      s->psi[a][n] = s->sat[a][n] = 0;
+      if (!s->act[n >> 6]) continue;
+      const int I = (int)((n >> 6) % s->ni) * NN + (int)(n & 3);
+      const long long bb = n >> 6;
+      const int bk = (int)(bb / ((long long)s->ni * s->nj));
+      const int bj = (int)((bb - (long long)bk * s->ni * s->nj) / s->ni);
+      const int J = bj * NN + (int)((n >> 2) & 3), K = bk * NN + (int)(n >> 4 & 3);
+      const double off[3] = {a == 0 ? 0.0 : 0.5, a == 1 ? 0.0 : 0.5, a == 2 ? 0.0 : 0.5};
+      const double np[3] = {node_coord(s, 0, I, off[0]), node_coord(s, 1, J, off[1]),
+                            node_coord(s, 2, K, off[2])};
+      double pf = 0, mf = 0, vf = 0, vs = 0, vfe = 0;
+      for (int e = PP[a]->start[n]; e < PP[a]->start[n + 1]; ++e) {
+        const int p = PP[a]->pid[e];
+        const double w = W[a][p * 27 + PP[a]->slot[e]];
+        const double* C = &s->C[p * 9 + a * 3];
+        const double dot = (C[0] * (np[0] - s->x[p * 3]) + C[1] * (np[1] - s->x[p * 3 + 1])) +
+                           C[2] * (np[2] - s->x[p * 3 + 2]);
+        const double vel = s->v[p * 3 + a] + dot;
+        pf += vel * s->m[p] * w;
+        mf += s->m[p] * w;
+        vf += s->vol[p] * w;
+      }
+      if (mf > 1e-20) s->vel[a][n] = pf / mf;
+      s->mass[a][n] = mf;
+      s->vol_f[a][n] = vf;
+      s->psi[a][n] = clampd(vs / dV, 0.0, 1.0);
+      s->sat[a][n] = clampd((vf + vfe) / fmax(1e-20, dV - vs), 0.0, 1.0);
+    }
+  }
+}
+
+/* updateLiquidPhi (TwoDScene.cpp:3286-3345) */
+static void liquid_phi(Scene* s) {
+  const double dx = s->p.dx;
+  for (long long n = 0; n < s->nnode; ++n) {
+    s->lphi[n] = 3.0 * s->bs;
+    s->pressure[n] = 0.0;
+  }
+  const int nc = 3;
+  const int sni = (s->ni + nc - 1) / nc, snj = (s->nj + nc - 1) / nc, snk = (s->nk + nc - 1) / nc;
+  const double off[3] = {0.5, 0.5, 0.5};
+  for (int ct = 0; ct < nc; ++ct)
+    for (int cs = 0; cs < nc; ++cs)
+      for (int cr = 0; cr < nc; ++cr)
+        for (long long sb = 0; sb < (long long)sni * snj * snk; ++sb) {
+          const int sk = (int)(sb / ((long long)sni * snj));
+          const int sj = (int)((sb - (long long)sk * sni * snj) / sni);
+          const int si = (int)(sb - (long long)sk * sni * snj - (long long)sj * sni);
+          const int k = sk * nc + ct, j = sj * nc + cs, i = si * nc + cr;
+          if (k >= s->nk || j >= s->nj || i >= s->ni) continue;
+          const long long b = bucket_index(s, i, j, k);
+          for (int q = s->sup[b * 2]; q < s->sup[b * 2 + 1]; ++q) {
+            const int p = (int)(s->keys[q] & 0xffffffffu);
+            const int* lo = &s->base[p * 15 + 12];
+            for (int sl = 0; sl < 27; ++sl) {
+              const int I = lo[0] + sl % 3, J = lo[1] + (sl / 3) % 3, K = lo[2] + sl / 9;
+              const long long n = node_of(s, I, J, K);
+              if (!node_active(s, n)) continue;
+              double np[3];
+              stencil_node_pos(s, I, J, K, off, np);
+              const double d0 = s->x[p * 3] - np[0], d1 = s->x[p * 3 + 1] - np[1],
+                           d2 = s->x[p * 3 + 2] - np[2];
+              const double r = fmax(dx * 0.883644, s->rad[p]);
+              const double phi = sqrt(d0 * d0 + d1 * d1 + d2 * d2) - r;
+              if (phi < s->lphi[n]) s->lphi[n] = phi;
+            }
+          }
+        }
+  for (long long n = 0; n < s->nnode; ++n) {
+    if (!s->act[n >> 6]) continue;
+    const long long bb = n >> 6;
+    const int bk = (int)(bb / ((long long)s->ni * s->nj));
+    const int bj = (int)((bb - (long long)bk * s->ni * s->nj) / s->ni);
+    const int bi = (int)(bb - (long long)bk * s->ni * s->nj - (long long)bj * s->ni);
+    const int I = bi * NN + (int)(n & 3), J = bj * NN + (int)((n >> 2) & 3), K = bk * NN + (int)((n >> 4) & 3);
+    const double np[3] = {node_coord(s, 0, I, 0.5), node_coord(s, 1, J, 0.5), node_coord(s, 2, K, 0.5)};
+    if (wall_phi(s, np[0], np[1], np[2]) < 0.0) s->lphi[n] = -0.5 * dx;
+  }
+}
+
+static void node_ijk(const Scene* s, long long n, int* I, int* J, int* K) {
+  const long long bb = n >> 6;
+  const int bk = (int)(bb / ((long long)s->ni * s->nj));
+  const int bj = (int)((bb - (long long)bk * s->ni * s->nj) / s->ni);
+  const int bi = (int)(bb - (long long)bk * s->ni * s->nj - (long long)bj * s->ni);
+  *I = bi * NN + (int)(n & 3);
+  *J = bj * NN + (int)((n >> 2) & 3);
+  *K = bk * NN + (int)((n >> 4) & 3);
+}
+
+/* updateSolidPhi (TwoDScene.cpp:7940-7967) and updateSolidWeights
+ * (:1871-1962; corner order of connectSolidPhiNodes :4433-4596) */
+static void solid_phi_and_weights(Scene* s) {
+  for (long long n = 0; n < s->nnode; ++n) {
+    s->sphi[n] = 0;
+    for (int a = 0; a < 3; ++a) s->svel[a][n] = 0;
+    if (!s->act[n >> 6]) continue;
+    int I, J, K;
+    node_ijk(s, n, &I, &J, &K);
+    s->sphi[n] = wall_phi(s, node_coord(s, 0, I, 0.0), node_coord(s, 1, J, 0.0), node_coord(s, 2, K, 0.0));
+  }
+  for (long long n = 0; n < s->nnode; ++n) {
+    for (int a = 0; a < 3; ++a) s->wgt[a][n] = 0;
+    if (!s->act[n >> 6]) continue;
+    int I, J, K;
+    node_ijk(s, n, &I, &J, &K);
+    for (int a = 0; a < 3; ++a) {
+      double phi[4];
+      for (int r = 0; r < 2; ++r)
+        for (int t = 0; t < 2; ++t) {
+          int ci = I, cj = J, ck = K;
+          if (a == 0) { cj += t; ck += r; }
+          else if (a == 1) { ci += r; ck += t; }
+          else { ci += r; cj += t; }
+          const long long q = node_of(s, ci, cj, ck);
+          phi[r * 2 + t] = node_active(s, q) ? s->sphi[q] : 0.5 * s->p.dx;
+        }
+      s->wgt[a][n] = clampd(1.0 - frac_in4(phi[0], phi[1], phi[2], phi[3]), 0.0, 1.0);
+    }
+  }
+}
+
+/* mapParticleSaturationPsiNodes (TwoDScene.cpp:5952-5992) and
+ * updatePorePressureNodes (:5933-5950, getCapillaryPressure :563-571) */
+static void sat_psi_p(Scene* s) {
+  const double dV = s->p.dx * s->p.dx * s->p.dx;
+  const double pore_radius = 0.005, stc = 72.8, angle = 40.8 / 180.0 * M_PI;
+  for (long long n = 0; n < s->nnode; ++n) {
+    double vl = 0, vs = 0;
+    for (int e = s->pp.start[n]; e < s->pp.start[n + 1]; ++e) {
+      const int p = s->pp.pid[e];
+      const double w = s->wp[p * 27 + s->pp.slot[e]];
+      vl += s->vol[p] * w;
+      vs += 0.0 * w * 0.0;  /* rest volume x rest fraction of liquid particles */
+    }
+    s->psi_p[n] = clampd(vs / dV, 0.0, 1.0);
+    s->sat_p[n] = clampd(vl / fmax(1e-20, dV - vs), 0.0, 1.0);
+    double cp = 0.0;
+    const double psi = s->psi_p[n];
+    if (!(1.0 - psi < 1e-20 || pore_radius < 1e-20))
+      cp = (psi / (1. - psi)) * stc * cos(angle) / pore_radius;
+    s->pore_p[n] = cp * (1.0 - s->sat_p[n]);
+  }
+}
+
+/* LinearizedImplicitEuler::stepVelocity for liquid nodes
+ * (LinearizedImplicitEuler.cpp:224-337): constructNodeForce (:548-667),
+ * SimpleGravityForce::addLiquidGradEToNode (SimpleGravityForce.cpp:25-52),
+ * pressure::computePorePressureGrads (Pressure.cpp:26-110, orientation 0),
+ * constructHDV (:846-965, no drag), constructInvMDV (:1109-1148),
+ * performLocalSolve (:128-170), acceptVelocity (:2176-2212),
+ * constructPsiSF (:1052-1107). */
+static void step_velocity(Scene* s, double dt) {
+  for (int a = 0; a < 3; ++a)
+    for (long long n = 0; n < s->nnode; ++n) {
+      s->rhs[a][n] = s->vstar[a][n] = s->invC[a][n] = s->psifs[a][n] = s->psisf[a][n] = 0;
+      s->mshdvm[a][n] = s->mfhdvm[a][n] = 0;
+      if (!s->act[n >> 6]) continue;
+      const double m = s->mass[a][n];
+      double r = 0.0;
+      r -= m * s->p.g[a] * (-dt);
+      if (s->vol_f[a][n] > 0.0 && s->wgt[a][n] > 0.0) {
+        int I, J, K;
+        node_ijk(s, n, &I, &J, &K);
+        const long long l = node_of(s, I - (a == 0), J - (a == 1), K - (a == 2));
+        const double pp0 = node_active(s, l) ? s->pore_p[l] : 0.0;
+        const double pp1 = s->pore_p[n];
+        const double grad = (pp1 - pp0) / s->p.dx;
+        /* get_rotated_pore_coeff_* with a zero orientation (MathUtilities.h:792-818) */
+        const double coeff = 0.0 / fmax(1e-63, 0.0);
+        r += grad * s->vol_f[a][n] * dt * s->sat[a][n] * s->wgt[a][n] * coeff;
+      }
+      r += m * s->vel[a][n];
+      const double hdV = dt * 0.0 * (0.0 + s->vol_f[a][n]);
+      const double mf = m + hdV, ms = 0.0 + hdV;
+      s->mfhdvm[a][n] = mf > 1e-20 ? hdV / mf : 1.0;
+      s->mshdvm[a][n] = ms > 1e-20 ? hdV / ms : 1.0;
+      const double C = m + s->mshdvm[a][n] * 0.0;
+      s->invC[a][n] = C > 1e-20 ? 1.0 / C : 1.0;
+      s->rhs[a][n] = r;
+      s->vstar[a][n] = m > 1e-20 ? r / m : r;
+      const double psi = s->psi[a][n], invCs = 0.0;
+      s->psifs[a][n] = ((1.0 - psi) * s->invC[a][n] + psi * invCs * s->mfhdvm[a][n]) * m;
+      s->psisf[a][n] = (psi * invCs + (1.0 - psi) * s->invC[a][n] * s->mshdvm[a][n]) * 0.0;
+    }
+}
+
+/* robertbridson::SparseMatrix::add_to_element (SparseMatrix.h:64-80) on a
+ * row stored as a small sorted array */
+typedef struct {
+  int n;
+  int col[8];
+  double val[8];
+} Row;
+
+static void row_add(Row* r, int j, double v) {
+  int k = 0;
+  for (; k < r->n; ++k) {
+    if (r->col[k] == j) {
+      r->val[k] += v;
+      return;
+    }
+    if (r->col[k] > j) break;
+  }
+  for (int m = r->n; m > k; --m) {
+    r->col[m] = r->col[m - 1];
+    r->val[m] = r->val[m - 1];
+  }
+  r->col[k] = j;
+  r->val[k] = v;
+  r->n++;
+}
+
+/* pressure::solveNodePressure assembly (Pressure.cpp:350-791) */
+static void assemble(Scene* s, double dt) {
+  free(s->dofidx);
+  s->dofidx = (long long*)malloc(sizeof(long long) * s->nnode);
+  int k = 0;
+  for (long long n = 0; n < s->nnode; ++n) {
+    if (!s->act[n >> 6]) {
+      s->dofidx[n] = -2;
+      continue;
+    }
+    s->dofidx[n] = -1;
+    if (!(s->lphi[n] < 0)) continue;
+    int I, J, K;
+    node_ijk(s, n, &I, &J, &K);
+    const long long f[6] = {n, node_of(s, I + 1, J, K), n, node_of(s, I, J + 1, K), n,
+                            node_of(s, I, J, K + 1)};
+    int open = 0;
+    for (int q = 0; q < 6; ++q)
+      if (node_active(s, f[q]) && s->wgt[q >> 1][f[q]] > 0) open = 1;
+    if (open) s->dofidx[n] = k++;
+  }
+  s->ndof = k;
+  Row* rows = (Row*)calloc(k > 0 ? k : 1, sizeof(Row));
+  free(s->b);
+  s->b = (double*)calloc(k > 0 ? k : 1, sizeof(double));
+  const double dx = s->p.dx;
+  const double coeff = dt / (dx * dx);
+  for (long long n = 0; n < s->nnode; ++n) {
+    const long long d = s->dofidx[n];
+    if (d < 0) continue;
+    int I, J, K;
+    node_ijk(s, n, &I, &J, &K);
+    const double cphi = s->lphi[n];
+    /* left, right, bottom, top, near, far */
+    for (int q = 0; q < 6; ++q) {
+      const int a = q >> 1, up = q & 1;
+      const long long f = up ? node_of(s, I + (a == 0), J + (a == 1), K + (a == 2)) : n;
+      if (!node_active(s, f)) continue;
+      const double w = s->wgt[a][f];
+      const double t = ((s->vstar[a][f] * s->psifs[a][f] + 0.0 * s->psisf[a][f]) * w +
+                        s->svel[a][f] * (1.0 - w)) / dx;
+      if (up) s->b[d] -= t; else s->b[d] += t;
+      if (w > 0.0) {
+        double term = w * coeff;
+        const double psi = s->psi[a][f];
+        term *= (1.0 - psi) * s->invC[a][f] * (s->vol_f[a][f] + 0.0 * s->mshdvm[a][f]) +
+                psi * 0.0 * (0.0 + s->vol_f[a][f] * s->mfhdvm[a][f]);
+        const long long c = up ? f : node_of(s, I - (a == 0), J - (a == 1), K - (a == 2));
+        if (!node_active(s, c)) continue;
+        const double nphi = s->lphi[c];
+        if (nphi < 0.0) {
+          const long long dn = s->dofidx[c];
+          if (dn >= 0) {
+            row_add(&rows[d], (int)d, term);
+            row_add(&rows[d], (int)dn, -term);
+          }
+        } else {
+          double theta = frac_in2(cphi, nphi);
+          if (theta < 0.01) theta = 0.01;
+          row_add(&rows[d], (int)d, term / theta);
+        }
+      }
+    }
+  }
+  free(s->rowstart);
+  free(s->col);
+  free(s->val);
+  s->rowstart = (int*)malloc(sizeof(int) * (k + 1));
+  int nz = 0;
+  for (int r = 0; r < k; ++r) nz += rows[r].n;
+  s->col = (int*)malloc(sizeof(int) * (nz > 0 ? nz : 1));
+  s->val = (double*)malloc(sizeof(double) * (nz > 0 ? nz : 1));
+  nz = 0;
+  for (int r = 0; r < k; ++r) {
+    s->rowstart[r] = nz;
+    for (int m = 0; m < rows[r].n; ++m) {
+      s->col[nz] = rows[r].col[m];
+      s->val[nz] = rows[r].val[m];
+      ++nz;
+    }
+  }
+  s->rowstart[k] = nz;
+  free(rows);
+}
+
+/* ---------------------------------------------------------------------- */
+/* MIC(0)-PCG: factor_modified_incomplete_cholesky0, solve_lower,
+ * solve_lower_transpose_in_place and PCGSolver::solve
+ * (PCGSolver/PCGSolver.h:97-308), on the CSR matrix (sorted rows). */
+typedef struct {
+  int n;
+  double *invdiag, *adiag, *value;
+  int *rowindex, *colstart;
+} Factor;
+
+static int row_has(const int* rs, const int* col, int j, int c) {
+  for (int k = rs[j]; k < rs[j + 1]; ++k) {
+    if (col[k] == c) return 1;
+    if (col[k] > c) return 0;
+  }
+  return 0;
+}
+
+int wco_mic0_factor(int n, const int* rs, const int* col, const double* val, double omega,
+                    double min_ratio, Factor* F) {
+  F->n = n;
+  F->invdiag = (double*)calloc(n > 0 ? n : 1, sizeof(double));
+  F->adiag = (double*)calloc(n > 0 ? n : 1, sizeof(double));
+  F->colstart = (int*)malloc(sizeof(int) * (n + 1));
+  int nl = 0;
+  for (int i = 0; i < n; ++i)
+    for (int k = rs[i]; k < rs[i + 1]; ++k)
+      if (col[k] > i) ++nl;
+  F->value = (double*)malloc(sizeof(double) * (nl > 0 ? nl : 1));
+  F->rowindex = (int*)malloc(sizeof(int) * (nl > 0 ? nl : 1));
+  nl = 0;
+  for (int i = 0; i < n; ++i) {
+    F->colstart[i] = nl;
+    for (int k = rs[i]; k < rs[i + 1]; ++k) {
+      if (col[k] > i) {
+        F->rowindex[nl] = col[k];
+        F->value[nl] = val[k];
+        ++nl;
+      } else if (col[k] == i) {
+        F->invdiag[i] = F->adiag[i] = val[k];
+      }
+    }
+  }
+  F->colstart[n] = nl;
+  for (int k = 0; k < n; ++k) {
+    if (F->adiag[k] == 0) continue;
+    if (F->invdiag[k] < min_ratio * F->adiag[k])
+      F->invdiag[k] = 1 / sqrt(F->adiag[k]);
+    else
+      F->invdiag[k] = 1 / sqrt(F->invdiag[k]);
+    for (int p = F->colstart[k]; p < F->colstart[k + 1]; ++p) F->value[p] *= F->invdiag[k];
+    for (int p = F->colstart[k]; p < F->colstart[k + 1]; ++p) {
+      const int j = F->rowindex[p];
+      const double mult = F->value[p];
+      double missing = 0;
+      int a = F->colstart[k];
+      /* dropped entries above the diagonal of column j: row j of A lacks them */
+      while (a < F->colstart[k + 1] && F->rowindex[a] < j) {
+        if (!row_has(rs, col, j, F->rowindex[a])) missing += F->value[a];
+        ++a;
+      }
+      if (a < F->colstart[k + 1] && F->rowindex[a] == j) F->invdiag[j] -= mult * F->value[a];
+      ++a;
+      int b = F->colstart[j];
+      while (a < F->colstart[k + 1] && b < F->colstart[j + 1]) {
+        if (F->rowindex[b] < F->rowindex[a]) {
+          ++b;
+        } else if (F->rowindex[b] == F->rowindex[a]) {
+          F->value[b] -= mult * F->value[a];
+          ++a;
+          ++b;
+        } else {
+          missing += F->value[a];
+          ++a;
+        }
+      }
+      while (a < F->colstart[k + 1]) {
+        missing += F->value[a];
+        ++a;
+      }
+      F->invdiag[j] -= omega * mult * missing;
+    }
+  }
+  return 0;
+}
+
+static void factor_free(Factor* F) {
+  free(F->invdiag);
+  free(F->adiag);
+  free(F->value);
+  free(F->rowindex);
+  free(F->colstart);
+}
+
+static void apply_precond(const Factor* F, const double* x, double* out) {
+  for (int i = 0; i < F->n; ++i) out[i] = x[i];
+  for (int i = 0; i < F->n; ++i) {
+    out[i] *= F->invdiag[i];
+    for (int j = F->colstart[i]; j < F->colstart[i + 1]; ++j)
+      out[F->rowindex[j]] -= F->value[j] * out[i];
+  }
+  for (int i = F->n - 1; i >= 0; --i) {
+    for (int j = F->colstart[i]; j < F->colstart[i + 1]; ++j)
+      out[i] -= F->value[j] * out[F->rowindex[j]];
+    out[i] *= F->invdiag[i];
+  }
+}
+
+static double dotv(const double* a, const double* b, int n) {
+  double s = 0;
+  for (int i = 0; i < n; ++i) s += a[i] * b[i];
+  return s;
+}
+
+static double absmaxv(const double* a, int n) {
+  double m = 0;
+  for (int i = 0; i < n; ++i)
+    if (fabs(a[i]) > m) m = fabs(a[i]);
+  return m;
+}
+
+/* PCGSolver<double>::solve (PCGSolver.h:260-308); returns 1 on convergence */
+int wco_pcg_solve(int n, const int* rs, const int* col, const double* val, const double* rhs,
+                  double* result, double tol_factor, int maxiters, double omega,
+                  double min_ratio, double* residual_out, int* iters_out) {
+  for (int i = 0; i < n; ++i) result[i] = 0;
+  double* r = (double*)malloc(sizeof(double) * (n > 0 ? n : 1));
+  double* z = (double*)malloc(sizeof(double) * (n > 0 ? n : 1));
+  double* sv = (double*)malloc(sizeof(double) * (n > 0 ? n : 1));
+  for (int i = 0; i < n; ++i) r[i] = rhs[i];
+  int ok = 0;
+  *residual_out = absmaxv(r, n);
+  *iters_out = 0;
+  if (*residual_out < 1e-30) {
+    ok = 1;
+    goto done;
+  }
+  {
+    if (tol_factor < 1e-30) tol_factor = 1e-30;
+    const double tol = tol_factor * *residual_out;
+    Factor F;
+    wco_mic0_factor(n, rs, col, val, omega, min_ratio, &F);
+    apply_precond(&F, r, z);
+    double rho = dotv(z, r, n);
+    if (rho == 0 || rho != rho) {
+      factor_free(&F);
+      goto done;
+    }
+    for (int i = 0; i < n; ++i) sv[i] = z[i];
+    int it;
+    for (it = 0; it < maxiters; ++it) {
+      for (int i = 0; i < n; ++i) {
+        double acc = 0;
+        for (int k = rs[i]; k < rs[i + 1]; ++k) acc += val[k] * sv[col[k]];
+        z[i] = acc;
+      }
+      const double alpha = rho / dotv(sv, z, n);
+      for (int i = 0; i < n; ++i) result[i] += alpha * sv[i];
+      for (int i = 0; i < n; ++i) r[i] += -alpha * z[i];
+      *residual_out = absmaxv(r, n);
+      if (*residual_out <= tol) {
+        *iters_out = it + 1;
+        ok = 1;
+        break;
+      }
+      apply_precond(&F, r, z);
+      const double rho_new = dotv(z, r, n);
+      const double beta = rho_new / rho;
+      for (int i = 0; i < n; ++i) z[i] += beta * sv[i];
+      double* t = sv;
+      sv = z;
+      z = t;
+      rho = rho_new;
+    }
+    if (!ok) *iters_out = it;
+    factor_free(&F);
+  }
+done:
+  free(r);
+  free(z);
+  free(sv);
+  return ok;
+}
+
+/* applyPressureGradsFluidRHS (Pressure.cpp:1137-1314), performInvLocalSolve
+ * (LinearizedImplicitEuler.cpp:65-98), extrapolate (Pressure.cpp:1826-1903),
+ * acceptVelocity and constrainLiquidVelocity (TwoDScene.cpp:1827-1869). */
+static void apply_pressure(Scene* s, double dt) {
+  const double dx = s->p.dx;
+  double* u[3];
+  for (int a = 0; a < 3; ++a) {
+    u[a] = s->vel[a];  /* reused: the node fluid velocity after acceptVelocity */
+    for (long long n = 0; n < s->nnode; ++n) {
+      s->valid[a][n] = 0;
+      if (!s->act[n >> 6]) continue;
+      /* addSolidDragRHS (LinearizedImplicitEuler.cpp:713-739): + 1 * 0 * 0 */
+      s->rhs[a][n] += s->mshdvm[a][n] * 0.0 * 0.0;
+      if (s->wgt[a][n] > 0.) {
+        int I, J, K;
+        node_ijk(s, n, &I, &J, &K);
+        const long long l = node_of(s, I - (a == 0), J - (a == 1), K - (a == 2));
+        const int hl = node_active(s, l);
+        const double lphi = hl ? s->lphi[l] : 0, rphi = s->lphi[n];
+        if (lphi < 0.0 || rphi < 0.0) {
+          double theta = 1.;
+          if (rphi >= 0.0 || lphi >= 0.0) {
+            theta = frac_in2(lphi, rphi);
+            if (theta < 0.01) theta = 0.01;
+          }
+          double pg = 0;
+          if (hl) pg -= s->pressure[l];
+          pg += s->pressure[n];
+          pg /= (dx * theta);
+          const double term = pg * dt * (s->vol_f[a][n] + 0.0 * s->mshdvm[a][n]);
+          s->rhs[a][n] -= term;
+          s->valid[a][n] = 1;
+        }
+      }
+      u[a][n] = s->rhs[a][n] * s->invC[a][n];
+    }
+    /* two layers of 6-neighbour averaging */
+    double* cu = (double*)malloc(sizeof(double) * s->nnode);
+    unsigned char* cv = (unsigned char*)malloc((size_t)s->nnode);
+    for (int layer = 0; layer < 2; ++layer) {
+      memcpy(cu, u[a], sizeof(double) * s->nnode);
+      memcpy(cv, s->valid[a], (size_t)s->nnode);
+      for (long long n = 0; n < s->nnode; ++n) {
+        if (!s->act[n >> 6] || cv[n]) continue;
+        int I, J, K;
+        node_ijk(s, n, &I, &J, &K);
+        static const int o[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
+        double sum = 0;
+        int cnt = 0;
+        for (int r = 0; r < 6; ++r) {
+          const long long q = node_of(s, I + o[r][0], J + o[r][1], K + o[r][2]);
+          if (!node_active(s, q) || !cv[q]) continue;
+          sum += cu[q];
+          ++cnt;
+        }
+        if (cnt > 0) {
+          u[a][n] = sum / (double)cnt;
+          s->valid[a][n] = 1;
+        }
+      }
+    }
+    free(cu);
+    free(cv);
+  }
+}
+
+static void constrain(Scene* s) {
+  for (int a = 0; a < 3; ++a)
+    for (long long n = 0; n < s->nnode; ++n) {
+      if (!s->act[n >> 6]) continue;
+      if (s->wgt[a][n] == 0.0)
+        s->vel[a][n] = (1 - s->p.friction) * s->vel[a][n] + s->p.friction * s->svel[a][n];
+    }
+}
+
+/* mapNodeParticlesAPIC liquid branch (TwoDScene.cpp:6936-7000) */
+static void g2p(Scene* s) {
+  const double invD = 4.0 / (s->p.dx * s->p.dx);
+  double* W[3] = {s->wu, s->wv, s->ww};
+  for (int p = 0; p < s->np; ++p) {
+    if (s->inside[p] == 0) continue;
+    double fv[3] = {0, 0, 0}, B[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int a = 0; a < 3; ++a) {
+      const int* lo = &s->base[p * 15 + a * 3];
+      const double off[3] = {a == 0 ? 0.0 : 0.5, a == 1 ? 0.0 : 0.5, a == 2 ? 0.0 : 0.5};
+      for (int sl = 0; sl < 27; ++sl) {
+        const int I = lo[0] + sl % 3, J = lo[1] + (sl / 3) % 3, K = lo[2] + sl / 9;
+        const long long n = node_of(s, I, J, K);
+        if (!node_active(s, n)) continue;
+        double np[3];
+        stencil_node_pos(s, I, J, K, off, np);
+        const double fnv = s->vel[a][n];
+        const double w = W[a][p * 27 + sl];
+        fv[a] += fnv * w;
+        for (int q = 0; q < 3; ++q) B[a * 3 + q] += fnv * w * (np[q] - s->x[p * 3 + q]) * invD;
+      }
+    }
+    for (int a = 0; a < 3; ++a) s->v[p * 3 + a] = fv[a];
+    for (int q = 0; q < 9; ++q) s->C[p * 9 + q] = B[q] * s->p.flip;
+  }
+}
+
+/* ---------------------------------------------------------------------- */
+static void alloc_nodes(Scene* s) {
+  const size_t n = (size_t)s->nnode;
+  for (int a = 0; a < 3; ++a) {
+    double** F[] = {&s->mass[a], &s->vel[a], &s->vol_f[a], &s->sat[a], &s->psi[a], &s->wgt[a],
+                    &s->svel[a], &s->rhs[a], &s->vstar[a], &s->invC[a], &s->psifs[a],
+                    &s->psisf[a], &s->mshdvm[a], &s->mfhdvm[a]};
+    for (size_t k = 0; k < sizeof(F) / sizeof(F[0]); ++k) {
+      free(*F[k]);
+      *F[k] = (double*)calloc(n, sizeof(double));
+    }
+    free(s->valid[a]);
+    s->valid[a] = (unsigned char*)calloc(n, 1);
+  }
+  double** G[] = {&s->sat_p, &s->psi_p, &s->pore_p, &s->lphi, &s->sphi, &s->pressure};
+  for (size_t k = 0; k < sizeof(G) / sizeof(G[0]); ++k) {
+    free(*G[k]);
+    *G[k] = (double*)calloc(n, sizeof(double));
+  }
+  const size_t np = (size_t)(s->np > 0 ? s->np : 1);
+  double** Wt[] = {&s->wu, &s->wv, &s->ww, &s->wp};
+  for (int k = 0; k < 4; ++k) {
+    free(*Wt[k]);
+    *Wt[k] = (double*)calloc(np * 27, sizeof(double));
+  }
+}
+
+static void snap_particles(Scene* s, const char* tag) {
+  char nm[32];
+  snprintf(nm, sizeof nm, "%sx", tag);
+  snap_put_f(s, nm, s->x, (long long)s->np * 3);
+  snprintf(nm, sizeof nm, "%sv", tag);
+  snap_put_f(s, nm, s->v, (long long)s->np * 3);
+  snprintf(nm, sizeof nm, "%sC", tag);
+  snap_put_f(s, nm, s->C, (long long)s->np * 9);
+}
+
+/* one sub-step in WetClothCore::stepSystem order (WetClothCore.cpp:115-258) */
+int wco_substep(Scene* s, double dt, int snapshot) {
+  build_grid(s);
+  sort_particles(s);
+  resample_nodes(s);
+  alloc_nodes(s);
+  if (snapshot) {
+    const double org[3] = {s->org[0], s->org[1], s->org[2]};
+    const double bbx[6] = {s->bbmin[0], s->bbmin[1], s->bbmin[2], s->bbmax[0], s->bbmax[1], s->bbmax[2]};
+    const long long dims[3] = {s->ni, s->nj, s->nk};
+    snap_put_f(s, "grid_origin", org, 3);
+    snap_put_f(s, "bbx", bbx, 6);
+    snap_put_i(s, "grid_dims", dims, 3);
+    long long* t = (long long*)malloc(sizeof(long long) * (s->np + 2 * s->nb + 15 * (long long)s->np + s->nb + 2));
+    for (int q = 0; q < s->np; ++q) t[q] = (long long)s->keys[q];
+    snap_put_i(s, "array_idx", t, s->np);
+    for (long long b = 0; b < 2 * s->nb; ++b) t[b] = s->sup[b];
+    snap_put_i(s, "array_sup", t, 2 * s->nb);
+    for (long long b = 0; b < s->nb; ++b) t[b] = s->act[b];
+    snap_put_i(s, "active", t, s->nb);
+    for (long long k = 0; k < 15 * (long long)s->np; ++k) t[k] = s->base[k];
+    snap_put_i(s, "stencil_base", t, 15 * (long long)s->np);
+    for (int q = 0; q < s->np; ++q) t[q] = s->inside[q];
+    snap_put_i(s, "inside", t, s->np);
+    free(t);
+  }
+  compute_weights(s);
+  build_pairs(s, &s->pu, s->wu, 0);
+  build_pairs(s, &s->pv, s->wv, 1);
+  build_pairs(s, &s->pw, s->ww, 2);
+  build_pairs(s, &s->pp, s->wp, 4);
+  liquid_phi(s);
+  solid_phi_and_weights(s);
+  p2g(s);
+  sat_psi_p(s);
+  if (snapshot) {
+    static const char* xyz = "xyz";
+    char nm[32];
+    for (int a = 0; a < 3; ++a) {
+      snprintf(nm, sizeof nm, "mass_fluid_%c", xyz[a]); snap_node(s, nm, s->mass[a]);
+      snprintf(nm, sizeof nm, "vel_fluid_%c", xyz[a]); snap_node(s, nm, s->vel[a]);
+      snprintf(nm, sizeof nm, "vol_fluid_%c", xyz[a]); snap_node(s, nm, s->vol_f[a]);
+      snprintf(nm, sizeof nm, "sat_%c", xyz[a]); snap_node(s, nm, s->sat[a]);
+      snprintf(nm, sizeof nm, "psi_%c", xyz[a]); snap_node(s, nm, s->psi[a]);
+      snprintf(nm, sizeof nm, "solid_weight_%c", xyz[a]); snap_node(s, nm, s->wgt[a]);
+      snprintf(nm, sizeof nm, "solid_vel_%c", xyz[a]); snap_node(s, nm, s->svel[a]);
+    }
+    snap_node(s, "sat_p", s->sat_p);
+    snap_node(s, "psi_p", s->psi_p);
+    snap_node(s, "pore_pressure_p", s->pore_p);
+    snap_node(s, "liquid_phi", s->lphi);
+    snap_node(s, "solid_phi", s->sphi);
+  }
+  step_velocity(s, dt);
+  if (snapshot) {
+    static const char* xyz = "xyz";
+    char nm[32];
+    for (int a = 0; a < 3; ++a) {
+      snprintf(nm, sizeof nm, "v_star_%c", xyz[a]); snap_node(s, nm, s->vstar[a]);
+      snprintf(nm, sizeof nm, "rhs_fluid_%c", xyz[a]); snap_node(s, nm, s->rhs[a]);
+      snprintf(nm, sizeof nm, "inv_C_%c", xyz[a]); snap_node(s, nm, s->invC[a]);
+      snprintf(nm, sizeof nm, "psi_fs_%c", xyz[a]); snap_node(s, nm, s->psifs[a]);
+    }
+  }
+  /* acceptVelocity: the scene's node fluid velocity becomes u* */
+  for (int a = 0; a < 3; ++a) memcpy(s->vel[a], s->vstar[a], sizeof(double) * s->nnode);
+  assemble(s, dt);
+  if (snapshot) {
+    long long* rs = (long long*)malloc(sizeof(long long) * (s->ndof + 1));
+    long long* cl = (long long*)malloc(sizeof(long long) * (s->rowstart[s->ndof] + 1));
+    for (int r = 0; r <= s->ndof; ++r) rs[r] = s->rowstart[r];
+    for (int k = 0; k < s->rowstart[s->ndof]; ++k) cl[k] = s->col[k];
+    snap_put_i(s, "A_rowstart", rs, s->ndof + 1);
+    snap_put_i(s, "A_col", cl, s->rowstart[s->ndof]);
+    snap_put_f(s, "A_val", s->val, s->rowstart[s->ndof]);
+    snap_put_f(s, "b", s->b, s->ndof);
+    snap_put_i(s, "dof_index", s->dofidx, s->nnode);
+    free(rs);
+    free(cl);
+  }
+  double* res = (double*)calloc(s->ndof > 0 ? s->ndof : 1, sizeof(double));
+  double rr = 0;
+  int it = 0;
+  if (s->ndof > 0)
+    wco_pcg_solve(s->ndof, s->rowstart, s->col, s->val, s->b, res, s->p.criterion,
+                  s->p.maxiters, 0.97, 0.25, &rr, &it);
+  s->last_iters = it;
+  s->last_res = rr;
+  for (long long n = 0; n < s->nnode; ++n)
+    if (s->dofidx[n] >= 0) s->pressure[n] = res[s->dofidx[n]];
+  free(res);
+  if (snapshot) snap_node(s, "pressure", s->pressure);
+  apply_pressure(s, dt);
+  if (snapshot) {
+    static const char* xyz = "xyz";
+    char nm[32];
+    for (int a = 0; a < 3; ++a) {
+      snprintf(nm, sizeof nm, "u_proj_%c", xyz[a]); snap_node(s, nm, s->vel[a]);
+      long long* t = (long long*)malloc(sizeof(long long) * s->nnode);
+      for (long long n = 0; n < s->nnode; ++n) t[n] = s->act[n >> 6] ? s->valid[a][n] : -1;
+      snprintf(nm, sizeof nm, "valid_%c", xyz[a]);
+      snap_put_i(s, nm, t, s->nnode);
+      free(t);
+    }
+  }
+  constrain(s);
+  if (snapshot) {
+    static const char* xyz = "xyz";
+    char nm[32];
+    for (int a = 0; a < 3; ++a) {
+      snprintf(nm, sizeof nm, "u_final_%c", xyz[a]);
+      snap_node(s, nm, s->vel[a]);
+    }
+  }
+  g2p(s);
+  if (snapshot) snap_particles(s, "g2p_");
+  /* SceneStepper::advectScene (SceneStepper.cpp:17-41) */
+  for (int p = 0; p < s->np; ++p)
+    for (int a = 0; a < 3; ++a) s->x[p * 3 + a] += s->v[p * 3 + a] * dt;
+  if (snapshot) snap_particles(s, "adv_");
+  return 0;
+}
+
+/* WetClothCore::stepSystem CFL sub-stepping (WetClothCore.cpp:50-62) */
+int wco_num_substeps(Scene* s, double dt) {
+  double mv = 0.0;
+  for (int p = 0; p < s->np; ++p) {
+    const double q = s->v[p * 3] * s->v[p * 3] + s->v[p * 3 + 1] * s->v[p * 3 + 1] +
+                     s->v[p * 3 + 2] * s->v[p * 3 + 2];
+    if (q > mv) mv = q;
+  }
+  mv = sqrt(mv);
+  const double dx = s->p.dx;
+  double me = dx / 1e-63 / 3.0;
+  if (me > 1.0 / 30.0) me = 1.0 / 30.0;
+  double mf = dx / (mv > 1e-63 ? mv : 1e-63) * 3.0;
+  if (mf > 1.0 / 30.0) mf = 1.0 / 30.0;
+  const double md = me < mf ? me : mf;
+  int n = (int)ceil(dt / md);
+  return n > 1 ? n : 1;
+}
+
+int wco_step(Scene* s, double dt, int snapshot) {
+  const int n = wco_num_substeps(s, dt);
+  for (int k = 0; k < n; ++k) wco_substep(s, dt / (double)n, snapshot);
+  return n;
+}
+
+Scene* wco_create(double dx, const double* g, double rho, double flip, double friction,
+                  const double* bc, const double* bh, double br, double criterion,
+                  int maxiters, int mic, int np, const double* x3, const double* v3,
+                  const double* C9, const double* mass, const double* vol, const double* radius) {
+  Scene* s = (Scene*)calloc(1, sizeof(Scene));
+  s->p.dx = dx;
+  for (int a = 0; a < 3; ++a) {
+    s->p.g[a] = g[a];
+    s->p.bc[a] = bc[a];
+    s->p.bh[a] = bh[a];
+  }
+  s->p.rho = rho;
+  s->p.flip = flip;
+  s->p.friction = friction;
+  s->p.br = br;
+  s->p.criterion = criterion;
+  s->p.maxiters = maxiters;
+  s->p.mic = mic;
+  s->bs = dx * 4.0;
+  s->np = np;
+  const size_t n = (size_t)(np > 0 ? np : 1);
+  s->x = (double*)malloc(sizeof(double) * 3 * n);
+  s->v = (double*)malloc(sizeof(double) * 3 * n);
+  s->C = (double*)calloc(9 * n, sizeof(double));
+  s->m = (double*)malloc(sizeof(double) * n);
+  s->vol = (double*)malloc(sizeof(double) * n);
+  s->rad = (double*)malloc(sizeof(double) * n);
+  memcpy(s->x, x3, sizeof(double) * 3 * np);
+  memcpy(s->v, v3, sizeof(double) * 3 * np);
+  if (C9) memcpy(s->C, C9, sizeof(double) * 9 * np);
+  memcpy(s->m, mass, sizeof(double) * np);
+  memcpy(s->vol, vol, sizeof(double) * np);
+  memcpy(s->rad, radius, sizeof(double) * np);
+  return s;
+}
+
+void wco_destroy(Scene* s) {
+  if (!s) return;
+  for (int k = 0; k < s->nsnaps; ++k) {
+    free(s->snaps[k].f);
+    free(s->snaps[k].i);
+  }
+  void* ptrs[] = {s->x, s->v, s->C, s->m, s->vol, s->rad, s->keys, s->sup, s->act, s->base,
+                  s->inside, s->wu, s->wv, s->ww, s->wp, s->pu.start, s->pu.pid, s->pu.slot,
+                  s->pv.start, s->pv.pid, s->pv.slot, s->pw.start, s->pw.pid, s->pw.slot,
+                  s->pp.start, s->pp.pid, s->pp.slot, s->sat_p, s->psi_p, s->pore_p, s->lphi,
+                  s->sphi, s->pressure, s->dofidx, s->rowstart, s->col, s->val, s->b};
+  for (size_t k = 0; k < sizeof(ptrs) / sizeof(ptrs[0]); ++k) free(ptrs[k]);
+  for (int a = 0; a < 3; ++a) {
+    void* q[] = {s->mass[a], s->vel[a], s->vol_f[a], s->sat[a], s->psi[a], s->wgt[a], s->svel[a],
+                 s->rhs[a], s->vstar[a], s->invC[a], s->psifs[a], s->psisf[a], s->mshdvm[a],
+                 s->mfhdvm[a], s->valid[a]};
+    for (size_t k = 0; k < sizeof(q) / sizeof(q[0]); ++k) free(q[k]);
+  }
+  free(s);
+}
+
+long long wco_size(Scene* s, const char* name) {
+  for (int k = 0; k < s->nsnaps; ++k)
+    if (!strcmp(s->snaps[k].name, name)) return s->snaps[k].n;
+  return -1;
+}
+
+int wco_get_f(Scene* s, const char* name, double* out) {
+  for (int k = 0; k < s->nsnaps; ++k)
+    if (!strcmp(s->snaps[k].name, name) && !s->snaps[k].is_int) {
+      memcpy(out, s->snaps[k].f, sizeof(double) * s->snaps[k].n);
+      return 0;
+    }
+  return -1;
+}
+
+int wco_get_i(Scene* s, const char* name, long long* out) {
+  for (int k = 0; k < s->nsnaps; ++k)
+    if (!strcmp(s->snaps[k].name, name) && s->snaps[k].is_int) {
+      memcpy(out, s->snaps[k].i, sizeof(long long) * s->snaps[k].n);
+      return 0;
+    }
+  return -1;
+}
+
+void wco_solver_stats(Scene* s, int* iters, double* res) {
+  *iters = s->last_iters;
+  *res = s->last_res;
+}
+
+int wco_num_particles(Scene* s) { return s->np; }

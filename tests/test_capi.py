@@ -1,0 +1,68 @@
+"""C-ABI checks that need no GPU: the library loads, exports every function
+include/wetcloth_gpu.h declares, and reports argument errors."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from libwetcloth_b200 import _capi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    txt = open(os.path.join(ROOT, "include", "wetcloth_gpu.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(wcg_[a-z0-9_]+)\s*\(", txt)))
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    assert len(names) >= 30
+    assert "wcg_step" in names and "wcg_pressure_solve_noalloc" in names
+
+
+def test_library_exports_every_declared_symbol():
+    L = _capi.load()
+    for name in declared_functions():
+        assert hasattr(L, name), f"libwcgpu.so does not export {name}"
+        assert name in _capi.SIGNATURES, f"no ctypes signature for {name}"
+
+
+def test_default_params():
+    L = _capi.load()
+    p = _capi.WcgParams()
+    L.wcg_default_params(ctypes.byref(p))
+    assert p.criterion == 1e-6 and p.maxiters == 1000 and p.walls == 1
+    assert p.precision == _capi.WCG_FP64
+
+
+def test_argument_errors_without_device():
+    L = _capi.load()
+    h = ctypes.c_void_p()
+    assert L.wcg_create(None, ctypes.byref(h)) == _capi.WCG_ERR_ARG
+    p = _capi.WcgParams()
+    L.wcg_default_params(ctypes.byref(p))
+    p.dx = -1.0
+    assert L.wcg_create(ctypes.byref(p), ctypes.byref(h)) == _capi.WCG_ERR_ARG
+    assert b"dx" in L.wcg_last_error()
+    p.dx = 1.0 / 16
+    p.precision = 7
+    assert L.wcg_create(ctypes.byref(p), ctypes.byref(h)) == _capi.WCG_ERR_ARG
+    # calls on a null context fail cleanly
+    assert L.wcg_step(None, 1e-3, None) == _capi.WCG_ERR_ARG
+    assert L.wcg_rebucketize_and_resample(None) == _capi.WCG_ERR_ARG
+    assert L.wcg_num_particles(None) == -1
+
+
+def test_noalloc_size_limit_checked_before_device_work():
+    L = _capi.load()
+    it = ctypes.c_int(0)
+    res = ctypes.c_double(0)
+    rc = L.wcg_pressure_solve_noalloc(64, 64, 64, 1, 1, 1, 1, 1, 1, 1, 1e-6, 10, None,
+                                      ctypes.byref(it), ctypes.byref(res))
+    assert rc == _capi.WCG_ERR_ARG and b"limit" in L.wcg_last_error()
+    rc = L.wcg_pressure_solve_noalloc(0, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1e-6, 10, None,
+                                      ctypes.byref(it), ctypes.byref(res))
+    assert rc == _capi.WCG_ERR_ARG

@@ -1,22 +1,25 @@
-"""GPU FP64 path against the compiled reference Core, stage by stage.
+"""GPU FP64 path against the oracle, stage by stage.
 
-The reference (oracle/_ref, built from the libWetCloth sources) runs one
-sub-step of the fluid hot path on the same seeded scene and snapshots every
+Checkers: the C restatement oracle (oracle/wc_oracle.c, always built) and,
+when it is built, the compiled reference Core (oracle/_ref).  Both run one
+sub-step of the fluid hot path on the same seeded scene and snapshot every
 field; the GPU runs the same sub-step through the C-ABI stage calls.
-Tolerances: integer/index data bit-exact; FP64 fields within 1e-10 relative
-to the field's max magnitude (the solver-dependent pressures and everything
-after them within 1e-9, since PCG iterates accumulate rounding differently).
+Tolerances: integer/index data bit-exact (sort keys, bucket ranges,
+activation masks, stencil indices, DOF numbering, matrix structure, valid
+masks); FP64 fields within 1e-10 relative to the field's max magnitude; the
+PCG-dependent pressure and everything after it within 1e-9 (the same MIC(0)
+iterates, accumulated in a different order).
 """
 import numpy as np
 import pytest
 
-from oracle import ref as oref
 from libwetcloth_b200 import scenes
 from libwetcloth_b200.solver import FluidScene
+from oracle import oracle as oo
+from oracle import ref as oref
 from tests.parity import assert_close, assert_dense_close
 
-pytestmark = [pytest.mark.gpu,
-              pytest.mark.skipif(not oref.available(), reason="oracle/_ref not built")]
+pytestmark = pytest.mark.gpu
 
 DT = 1e-3
 
@@ -31,20 +34,56 @@ PREDICT_FIELDS = ["v_star_x", "v_star_y", "v_star_z", "rhs_fluid_x",
                   "psi_fs_x", "psi_fs_y", "psi_fs_z"]
 
 
-def _scene(kind):
+def boundary_lattice():
+    """Particles exactly on cell faces, edges, corners and half-cells: every
+    floor/frac tie of the stencil bases (frac == 0 and frac == 0.5)."""
+    dx = 1.0 / 16
+    g = np.arange(4, 13) * (dx / 2)
+    z, y, x = np.meshgrid(g, np.arange(0, 9) * (dx / 2), g, indexing="ij")
+    pts = np.stack([x.ravel(), y.ravel(), z.ravel()], 1)
+    m, vol, r = scenes.attributes(pts.shape[0], dx, 8, 1000.0)
+    return scenes.Scene(scenes.SceneParams(dx=dx), pts, np.zeros_like(pts), m, vol, r,
+                        name="boundary_lattice")
+
+
+def crowded_cell():
+    """A dam-break block plus 64 extra particles packed into one cell."""
+    sc = scenes.dam_break(16, 8, 2, block_hi=(0.3, 0.3, 0.3))
+    rng = np.random.default_rng(9)
+    extra = (np.array([0.4, 0.05, 0.4]) + rng.random((64, 3)) * (1 / 16))
+    x = np.concatenate([sc.x, extra])
+    m, vol, r = scenes.attributes(x.shape[0], sc.params.dx, 8, 1000.0)
+    return scenes.Scene(sc.params, x, np.zeros_like(x), m, vol, r, name="crowded")
+
+
+def make(kind):
     if kind == "dam16":
         return scenes.dam_break(16, 8, 0)
-    if kind == "dam32":
-        return scenes.dam_break(32, 8, 3)
     if kind == "curl32":
         return scenes.half_box(32, 2, 5, amplitude=0.5, sigma_cells=2.0)
+    if kind == "boundary":
+        return boundary_lattice()
+    if kind == "crowded":
+        return crowded_cell()
     raise ValueError(kind)
 
 
-@pytest.fixture(scope="module", params=["dam16", "curl32"])
+def checker(name, sc):
+    if name == "oracle":
+        return oo.OracleScene(sc)
+    if not oref.available():
+        pytest.skip("oracle/_ref not built")
+    return oref.RefScene(sc, mic=True)
+
+
+@pytest.fixture(scope="module",
+                params=[("dam16", "oracle"), ("curl32", "oracle"), ("boundary", "oracle"),
+                        ("crowded", "oracle"), ("dam16", "reference"), ("curl32", "reference")],
+                ids=lambda p: f"{p[0]}-{p[1]}")
 def pair(request, wcg):
-    sc = _scene(request.param)
-    r = oref.RefScene(sc, mic=True)
+    kind, chk = request.param
+    sc = make(kind)
+    r = checker(chk, sc)
     r.step(DT, snapshot=True)
     g = FluidScene(sc)
     out = {}
@@ -118,6 +157,7 @@ def test_pressure_mic_pcg(pair):
     st = out["stats"]
     assert abs(st["pcg_iters"] - it_ref) <= 1, (st["pcg_iters"], it_ref)
     assert st["converged"] == 1
+    assert st["residual"] <= sc.params.criterion * st["rhs_norm"]
     assert_dense_close(out["pressure"], r.get("pressure"), 1e-9, "pressure")
 
 
@@ -137,9 +177,10 @@ def test_g2p_and_advect(pair):
     assert_close(out["adv_x"], r.get("adv_x").reshape(n, 3), 1e-12, "advected x")
 
 
-def test_multi_step_state(wcg):
-    sc = _scene("dam16")
-    r = oref.RefScene(sc, mic=True)
+@pytest.mark.parametrize("chk", ["oracle", "reference"])
+def test_multi_step_state(chk, wcg):
+    sc = make("dam16")
+    r = checker(chk, sc)
     g = FluidScene(sc)
     for k in range(3):
         r.step(DT, snapshot=(k == 2))

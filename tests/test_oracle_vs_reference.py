@@ -1,0 +1,79 @@
+"""The C restatement oracle against the compiled reference Core on seeded
+scenes (skipped when oracle/_ref is not built).  Runs on CPU."""
+import numpy as np
+import pytest
+
+from libwetcloth_b200 import scenes
+from oracle import oracle as oo
+from oracle import ref as oref
+
+pytestmark = pytest.mark.skipif(not (oref.available() and oo.available()),
+                                reason="oracle/_ref or the oracle not built")
+DT = 1e-3
+EXACT = ["grid_dims", "grid_origin", "bbx", "array_idx", "array_sup", "active",
+         "stencil_base", "inside", "dof_index", "A_rowstart", "A_col", "valid_x",
+         "valid_y", "valid_z"]
+CLOSE = ["mass_fluid_x", "vel_fluid_y", "vol_fluid_z", "sat_p", "liquid_phi", "solid_phi",
+         "solid_weight_x", "solid_weight_z", "v_star_y", "rhs_fluid_y", "inv_C_x",
+         "psi_fs_z", "A_val", "b", "pressure", "u_proj_x", "u_final_y", "g2p_v", "g2p_C",
+         "adv_x"]
+
+
+def _scene(kind):
+    if kind == "dam16":
+        return scenes.dam_break(16, 8, 0)
+    if kind == "curl16":
+        return scenes.half_box(16, 2, 7, amplitude=1.0, sigma_cells=1.5)
+    if kind == "dam24_tall":
+        return scenes.dam_break(24, 8, 4, block_hi=(0.3, 0.9, 0.6))
+    raise ValueError(kind)
+
+
+@pytest.mark.parametrize("kind", ["dam16", "curl16", "dam24_tall"])
+def test_first_step(kind):
+    sc = _scene(kind)
+    r = oref.RefScene(sc, mic=True)
+    o = oo.OracleScene(sc)
+    r.step(DT, snapshot=True)
+    o.step(DT, snapshot=True)
+    for k in EXACT:
+        assert np.array_equal(r.get(k), o.get(k)), k
+    assert r.solver_stats()[0] == o.solver_stats()[0]
+    for k in CLOSE:
+        a, b = r.get(k), o.get(k)
+        m = ~np.isnan(a)
+        assert np.array_equal(m, ~np.isnan(b)), k
+        if m.any():
+            assert np.abs(a[m] - b[m]).max() <= 1e-12 * max(np.abs(a[m]).max(), 1e-300), k
+
+
+def test_five_steps_dam16():
+    sc = _scene("dam16")
+    r = oref.RefScene(sc, mic=True)
+    o = oo.OracleScene(sc)
+    for k in range(5):
+        r.step(DT, snapshot=(k == 4))
+        o.step(DT, snapshot=(k == 4))
+    for k in ("adv_x", "g2p_v", "g2p_C"):
+        a, b = r.get(k), o.get(k)
+        assert np.abs(a - b).max() <= 1e-10 * np.abs(a).max(), k
+
+
+def test_mic0_pcg_on_reference_matrix():
+    """robertbridson::PCGSolver restated on the reference's assembled system."""
+    sc = _scene("curl16")
+    r = oref.RefScene(sc, mic=True)
+    r.step(DT, snapshot=True)
+    rs, col, val, b = r.get("A_rowstart"), r.get("A_col"), r.get("A_val"), r.get("b")
+    x, ok, it, res = oo.pcg_solve(rs, col, val, b, sc.params.criterion, sc.params.maxiters)
+    it_ref, _ = r.solver_stats()
+    assert ok and it == it_ref
+    p = r.get("pressure")
+    dof = r.get("dof_index")
+    pref = p[dof >= 0][np.argsort(dof[dof >= 0])]
+    assert np.abs(x - pref).max() <= 1e-12 * np.abs(pref).max()
+    # the residual criterion of the reference: ||b - A x||_inf <= tol ||b||_inf
+    Ax = np.zeros_like(b)
+    for i in range(len(b)):
+        Ax[i] = np.dot(val[rs[i]:rs[i + 1]], x[col[rs[i]:rs[i + 1]]])
+    assert np.abs(b - Ax).max() <= sc.params.criterion * np.abs(b).max() * 1.0001
