@@ -193,6 +193,8 @@ int wcg_create(const wcg_params* params, wcg_ctx** out) {
   p.max_refinements = params->max_refinements > 0 ? params->max_refinements : 20;
   // wavefront tile shape (performance knob; both compute identical results)
   if (const char* v = getenv("WCG_SWEEP_TILE")) ctx->c.sweep_variant = !strcmp(v, "warp") ? 1 : 0;
+  // layout of the pressure solve (performance knob; same arithmetic)
+  if (const char* v = getenv("WCG_PCG_LAYOUT")) ctx->c.pcg_layout = !strcmp(v, "tiles") ? 1 : 0;
   cudaError_t e = wcg::ctx_init(ctx->c);
   if (e != cudaSuccess) {
     std::string m = std::string("context init: ") + cudaGetErrorString(e);

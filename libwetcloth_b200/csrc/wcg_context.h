@@ -94,6 +94,28 @@ enum GField : int {
   kNumGFields = 53
 };
 
+// Geometry of the pencil layout of one pressure solve (wcg_pencil.cuh).
+struct PencilGeom {
+  int ax_s, ax_a, ax_c;  // physical axis (0 x, 1 y, 2 z) of s, a, c
+  int lo[3];             // low corner of the DOF box (grid cells, physical axes)
+  int Ls, NA, NC;        // box extent along s, a, c
+  int nPA, nPC;          // patches along a, c
+  int R;                 // rows per patch (Ls + 2 * (patch edge - 1))
+  long long npatch;      // nPA * nPC
+  long long len;         // elements per array (npatch * R * lines per patch)
+};
+
+// Arrays of the pencil layout (Reals, len each; PL64_* are doubles).
+// PL_COEF spans four arrays: the MIC(0) factor interleaved per cell,
+// {1/sqrt(d'), S_s, S_a, S_c}.
+enum PlField : int {
+  PL_AD = 0, PL_AS, PL_AA, PL_AC, PL_B,        // assembled system
+  PL_COEF,                                     // MIC(0) factor (4 arrays)
+  PL_R = PL_COEF + 4, PL_X, PL_S0, PL_S1, PL_Q, PL_Y, PL_Z,  // PCG vectors
+  kNumPlFields
+};
+enum Pl64Field : int { PL64_X = 0, PL64_R, kNumPl64Fields };
+
 struct Context {
   Params prm;
   cudaStream_t stream = nullptr;
@@ -136,6 +158,18 @@ struct Context {
   long long n_active = 0;
   int drange_h[6] = {0, 0, 0, 1, 1, 1};  // min/max stencil offset per axis
   DevBuf active_list;            // compacted active buckets (int32)
+
+  // pressure solve in the pencil layout (default) or on 8^3 tiles
+  int pcg_layout = 0;            // 0: pencil layout, 1: bucket-major tiles
+  PencilGeom plg{};
+  DevBuf pl;                     // kNumPlFields * pl_cap Reals
+  DevBuf pl64;                   // kNumPl64Fields * pl_cap doubles
+  DevBuf pl_edge;                // tagged edge words
+  DevBuf pl_order;               // patches in wave order (int32)
+  DevBuf pl_part;                // per-patch partials (double)
+  long long pl_cap = 0;
+  int pl_tickets = 0;            // sweep tickets handed out in this solve
+  std::vector<int> pl_order_h;
 
   // FP64 refinement vectors (precision 1)
   DevBuf rx64, rr64, rb64;       // nnode doubles each

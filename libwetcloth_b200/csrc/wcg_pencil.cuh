@@ -1,0 +1,673 @@
+// MIC(0)-PCG in the skewed pencil layout.
+//
+// The pressure unknowns of one solve (the bounding box of the DOF cells) are
+// copied once into a layout built for the triangular sweeps.  One grid axis is
+// the stream axis s (the longest extent of the box); the other two (a, c) are
+// cut into patches of 16 x 16 lines.  Line (al, cl) of a patch is skewed by
+// d = al + cl rows: cell (s, a, c) sits at row t = s + d of its patch, and
+// element (patch, t, line) is stored at ((patch * R + t) * 256 + line) with
+// line = al + 16 cl and R = Ls + 30 rows.  Rows outside a line's range and
+// lines outside the box hold zeros.
+//
+// In this layout every MIC(0) hyperplane dependency is one row back (one row
+// forward for the backward sweep):
+//   (s-1, a, c): row t-1 of the same line
+//   (s, a-1, c): row t-1 of line - 1
+//   (s, a, c-1): row t-1 of line - 16
+// so a CTA of 256 threads (one per line) walks its patch row by row, one
+// barrier per row, every load and store a coalesced row, rows prefetched kPre
+// ahead in registers.  The factor is stored interleaved per cell
+// {1/sqrt(d'), S_s, S_a, S_c} so a sweep reads it with one vector load.  Values
+// crossing a patch edge go through a global buffer of tagged 64-bit words,
+// (epoch << 32 | 32 data bits), one word per 32 bits of payload: the consumer
+// re-reads its word until the tag equals the launch's epoch, so no fence or
+// flag is needed and a patch waits only for the rows it reads.
+// Patches are handed out by an atomic ticket in wave order (PAi + PCi), so a
+// patch's upstream patches always started before it.
+//
+// The arithmetic is that of the tile sweeps in wcg_pcg.cuh (restating
+// robertbridson's factor_modified_incomplete_cholesky0 / solve_lower /
+// solve_lower_transpose_in_place, libWetCloth/Core/PCGSolver/PCGSolver.h:
+// 97-239): per DOF j, d_j = A_jj - sum over the three lower neighbours k of
+// [L^2 + omega L miss], L = A(k, j) / sqrt(d_k'), miss = the other two upper
+// couplings of k over sqrt(d_k'); forward y_j = (r_j - sum S_k y_k) / sqrt(d_j');
+// backward z_j = (y_j - sum S_j z_k) / sqrt(d_j').  The lower neighbours are
+// taken in the order c, a, s (z, y, x when s is x).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "wcg_common.cuh"
+#include "wcg_context.h"
+#include "wcg_pcg.cuh"
+
+namespace wcg {
+
+constexpr int kPatch = 16;                    // lines per patch edge
+constexpr int kPatchLines = kPatch * kPatch;  // threads of a sweep CTA
+constexpr int kPre = 4;                       // rows prefetched ahead
+constexpr int kPlBlocks = 592;                // streaming kernels: 4 x 148 SMs
+
+__host__ __device__ inline long long pl_index(const PencilGeom& G, long long p, int t, int l) {
+  return (p * G.R + t) * kPatchLines + l;
+}
+
+// ---- tagged edge words -----------------------------------------------------------
+typedef unsigned long long u64;
+
+__device__ inline u64 ld_relaxed_u64(const u64* p) {
+  u64 v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p));
+  return v;
+}
+
+__device__ inline void st_relaxed_u64(u64* p, u64 v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v));
+}
+
+template <typename R>
+struct TagWords;
+template <>
+struct TagWords<float> {
+  static constexpr int W = 1;
+  __device__ static void pack(float v, unsigned tag, u64* w) {
+    w[0] = ((u64)tag << 32) | (u64)__float_as_uint(v);
+  }
+  __device__ static float unpack(const u64* w) { return __uint_as_float((unsigned)w[0]); }
+};
+template <>
+struct TagWords<double> {
+  static constexpr int W = 2;
+  __device__ static void pack(double v, unsigned tag, u64* w) {
+    const u64 b = (u64)__double_as_longlong(v);
+    w[0] = ((u64)tag << 32) | (b & 0xffffffffull);
+    w[1] = ((u64)tag << 32) | (b >> 32);
+  }
+  __device__ static double unpack(const u64* w) {
+    return __longlong_as_double((long long)((w[1] << 32) | (w[0] & 0xffffffffull)));
+  }
+};
+
+// Words of the edge buffer: entry (producer patch, side, s, k), EW words each.
+// side 0: the a-face (k = cl), side 1: the c-face (k = al).
+__device__ inline long long edge_word(const PencilGeom& G, long long p, int side, int s, int k,
+                                      int EW) {
+  return (((p * 2 + side) * G.Ls + s) * kPatch + k) * EW;
+}
+
+// The MIC(0) factor of a cell, interleaved: {1/sqrt(d'), S_s, S_a, S_c}.
+__device__ inline void ld_coef(const float* p, float* c) {
+  const float4 t = __ldcs(reinterpret_cast<const float4*>(p));
+  c[0] = t.x; c[1] = t.y; c[2] = t.z; c[3] = t.w;
+}
+__device__ inline void ld_coef(const double* p, double* c) {
+  const double2 a = __ldcs(reinterpret_cast<const double2*>(p));
+  const double2 b = __ldcs(reinterpret_cast<const double2*>(p) + 1);
+  c[0] = a.x; c[1] = a.y; c[2] = b.x; c[3] = b.y;
+}
+__device__ inline void st_coef(float* p, float a, float b, float c, float d) {
+  *reinterpret_cast<float4*>(p) = make_float4(a, b, c, d);
+}
+__device__ inline void st_coef(double* p, double a, double b, double c, double d) {
+  reinterpret_cast<double2*>(p)[0] = make_double2(a, b);
+  reinterpret_cast<double2*>(p)[1] = make_double2(c, d);
+}
+
+template <typename R>
+struct PencilSweepArgs {
+  PencilGeom G;
+  const int* order;   // patches in wave order
+  int* ticket;
+  int ticket_base;    // tickets already handed out this solve
+  unsigned epoch;     // tag of this launch's edge words
+  u64* edge;
+  // factorisation input
+  const R* AD;
+  const R* AS;
+  const R* AA;
+  const R* AC;
+  R* coef;      // factor: 4 per cell {1/sqrt(d'), S_s, S_a, S_c}
+  // sweeps
+  const R* in;  // forward: r; backward: y
+  R* out;       // forward: y; backward: z
+  R* r;         // forward (update): r updated in place; backward: r for z.r
+  const R* q;   // forward (update)
+  const double* sc;
+  double* part;  // per-patch partial: forward max|r|, backward z.r
+  R omega, min_ratio;
+  int* err;
+};
+
+// MODE: kFactor, kForward, kBackward.  UPD: the forward sweep first applies
+// r -= alpha q (and reports max|r|); the matching x += alpha s is applied by
+// the next SpMV (k_pl_spmv_s) or, after the last iteration, by k_pl_axpy.
+//
+// One thread per line, tid = al + 16 cl, warp w holding cl = 2w and 2w + 1;
+// the CTA advances one row per step with one barrier.  The a-neighbour and the
+// c-neighbour inside the warp come by shuffle of the previous step's outputs,
+// the c-neighbour in the adjacent warp through shared memory, and values across
+// the patch faces through the tagged edge words.
+template <typename R, int MODE, bool UPD>
+__global__ void __launch_bounds__(kPatchLines, 1)
+    k_pencil_sweep(const PencilSweepArgs<R> A) {
+  constexpr bool BWD = MODE == kBackward;
+  constexpr int PW = MODE == kFactor ? 2 : 1;  // values sent across an edge
+  constexpr int TW = TagWords<R>::W;
+  constexpr int EW = PW * TW;
+  // prefetched per cell: factor A_d, A_s, A_a, A_c; forward in, coef[4] (, q);
+  // backward in, coef[4], r
+  constexpr int NF = MODE == kFactor ? 4 : (MODE == kForward ? (UPD ? 6 : 5) : 6);
+  constexpr int RS = BWD ? -kPatchLines : kPatchLines;  // element step per row
+  constexpr int NW = kPatchLines / 32;
+  __shared__ int s_ticket;
+  __shared__ R xc[2][NW][kPatch][PW];
+  __shared__ double red[kPatchLines];
+  const PencilGeom& G = A.G;
+  const int tid = threadIdx.x;
+  const int lane = tid & 31, w = tid >> 5;
+  if (tid == 0) s_ticket = atomicAdd(A.ticket, 1) - A.ticket_base;
+  for (int i = tid; i < 2 * NW * kPatch * PW; i += kPatchLines) (&xc[0][0][0][0])[i] = R(0);
+  __syncthreads();
+  if (*(const int*)(A.sc + S_DONE)) return;
+  const int tk = s_ticket;
+  if (tk < 0 || tk >= (int)G.npatch) {
+    if (tid == 0) record_error(A.err, kErrIndex);
+    return;
+  }
+  const int p = BWD ? A.order[G.npatch - 1 - tk] : A.order[tk];
+  const int PAi = p % G.nPA, PCi = p / G.nPA;
+  const int al = tid & (kPatch - 1), cl = tid / kPatch;
+  const bool line = PAi * kPatch + al < G.NA && PCi * kPatch + cl < G.NC;
+  const int dl = al + cl;
+  const int Ls = G.Ls, NR = G.R;
+  const int u0 = BWD ? (NR - Ls) - dl : dl;  // first live step
+  int up_a = -1, up_c = -1;
+  bool pub_a, pub_c;
+  if (!BWD) {
+    if (al == 0 && PAi > 0) up_a = p - 1;
+    if (cl == 0 && PCi > 0) up_c = p - G.nPA;
+    pub_a = al == kPatch - 1 && PAi + 1 < G.nPA;
+    pub_c = cl == kPatch - 1 && PCi + 1 < G.nPC;
+  } else {
+    if (al == kPatch - 1 && PAi + 1 < G.nPA) up_a = p + 1;
+    if (cl == kPatch - 1 && PCi + 1 < G.nPC) up_c = p + G.nPA;
+    pub_a = al == 0 && PAi > 0;
+    pub_c = cl == 0 && PCi > 0;
+  }
+  if (!line) up_a = up_c = -1;
+  const bool a_edge = al == (BWD ? kPatch - 1 : 0);  // no in-warp a source
+  const bool c_prod = BWD ? lane < 16 : lane >= 16;  // half read by the next warp
+  const int w_src = BWD ? w + 1 : w - 1;
+  const bool has_wsrc = BWD ? w + 1 < NW : w > 0;
+  constexpr int ES = kPatch * EW;  // words between consecutive s of one entry
+  const u64* ea_src = up_a >= 0 ? A.edge + edge_word(G, up_a, 0, 0, cl, EW) : nullptr;
+  const u64* ec_src = up_c >= 0 ? A.edge + edge_word(G, up_c, 1, 0, al, EW) : nullptr;
+  u64* ea_dst = pub_a ? A.edge + edge_word(G, p, 0, 0, cl, EW) : nullptr;
+  u64* ec_dst = pub_c ? A.edge + edge_word(G, p, 1, 0, al, EW) : nullptr;
+  const unsigned ep = A.epoch;
+  const R al_r = (MODE == kForward && UPD) ? (R)A.sc[S_ALPHA] : R(0);
+  const R omega = A.omega, min_ratio = A.min_ratio;
+  // per-thread base pointers (patch and line applied); rows by 32-bit offset
+  const long long pb = (long long)p * NR * kPatchLines + tid;
+  const R* __restrict__ f0 = MODE == kFactor ? A.AD + pb : A.in + pb;
+  const R* __restrict__ f1 = MODE == kFactor ? A.AS + pb : nullptr;
+  const R* __restrict__ f2 = MODE == kFactor ? A.AA + pb : nullptr;
+  const R* __restrict__ f3 = MODE == kFactor ? A.AC + pb : nullptr;
+  R* __restrict__ pcoef = A.coef + 4 * pb;
+  const R* __restrict__ fx = MODE == kForward ? (UPD ? A.q + pb : nullptr)
+                                              : (BWD ? A.r + pb : nullptr);
+  R* __restrict__ o_out = MODE == kFactor ? nullptr : A.out + pb;
+  R* __restrict__ o_r = (MODE == kForward && UPD) ? A.r + pb : nullptr;
+  const int off0 = BWD ? (NR - 1) * kPatchLines : 0;
+  auto s_at = [&](int u) { return BWD ? (NR - 1 - u) - dl : u - dl; };
+  auto live_at = [&](int u) { return line && (unsigned)(u - u0) < (unsigned)Ls; };
+  // rows outside a line's range hold zeros, so whole rows are read and every
+  // cell is computed (zeros stay zeros); only the edge words need liveness
+  auto load = [&](int off, R* f) {
+    f[0] = __ldcs(f0 + off);
+    if (MODE == kFactor) {
+      f[1] = __ldcs(f1 + off);
+      f[2] = __ldcs(f2 + off);
+      f[3] = __ldcs(f3 + off);
+    } else {
+      ld_coef(pcoef + 4 * off, f + 1);
+      if (NF == 6) f[5] = __ldcs(fx + off);
+    }
+  };
+
+  R pre[kPre][NF];
+  u64 epa[kPre][EW], epc[kPre][EW];
+#pragma unroll
+  for (int v = 0; v < kPre; ++v) {
+    if (v < NR) load(off0 + v * RS, pre[v]);
+    const bool lv = v < NR && live_at(v);
+    const int sv = s_at(v);
+#pragma unroll
+    for (int k = 0; k < EW; ++k) {
+      epa[v][k] = (lv && ea_src) ? ld_relaxed_u64(ea_src + sv * ES + k) : 0ull;
+      epc[v][k] = (lv && ec_src) ? ld_relaxed_u64(ec_src + sv * ES + k) : 0ull;
+    }
+  }
+  R carry[PW], prev_a[PW], prev_c[PW];
+#pragma unroll
+  for (int k = 0; k < PW; ++k) carry[k] = prev_a[k] = prev_c[k] = R(0);
+  R rmax = 0;
+  double dsum = 0;
+  bool gave_up = false;
+  // complete an edge entry: re-read words whose tag is stale (bounded)
+  auto ewait = [&](u64* wd, const u64* src) {
+#pragma unroll
+    for (int k = 0; k < EW; ++k) {
+      if ((unsigned)(wd[k] >> 32) == ep) continue;
+      long long it = 0;
+      do {
+        if (gave_up || ++it > kSpinLimit) {
+          if (!gave_up) record_error(A.err, kErrWaitTimeout);
+          gave_up = true;
+          wd[k] = (u64)ep << 32;
+          break;
+        }
+        wd[k] = ld_relaxed_u64(src + k);
+      } while ((unsigned)(wd[k] >> 32) != ep);
+    }
+  };
+
+  for (int ub = 0; ub < NR; ub += kPre) {
+#pragma unroll
+    for (int v = 0; v < kPre; ++v) {
+      const int u = ub + v;
+      if (u >= NR) break;  // uniform over the CTA
+      const int off = off0 + u * RS;
+      const int cur = u & 1, nxt = cur ^ 1;
+      // neighbour inputs of step u = outputs of step u - 1
+      R in_a[PW], in_c[PW];
+#pragma unroll
+      for (int k = 0; k < PW; ++k) {
+        in_a[k] = BWD ? __shfl_down_sync(0xffffffffu, prev_a[k], 1)
+                      : __shfl_up_sync(0xffffffffu, prev_a[k], 1);
+        in_c[k] = BWD ? __shfl_down_sync(0xffffffffu, prev_c[k], 16)
+                      : __shfl_up_sync(0xffffffffu, prev_c[k], 16);
+        if (a_edge) in_a[k] = R(0);
+        if (!c_prod) in_c[k] = has_wsrc ? xc[cur][w_src][al][k] : R(0);
+      }
+      const bool live = live_at(u);
+      const int s = s_at(u);
+      if (live && ea_src) {
+        ewait(epa[v], ea_src + s * ES);
+#pragma unroll
+        for (int k = 0; k < PW; ++k) in_a[k] = TagWords<R>::unpack(epa[v] + k * TW);
+      }
+      if (live && ec_src) {
+        ewait(epc[v], ec_src + s * ES);
+#pragma unroll
+        for (int k = 0; k < PW; ++k) in_c[k] = TagWords<R>::unpack(epc[v] + k * TW);
+      }
+      const R* f = pre[v];
+      R out_s[PW], out_a[PW], out_c[PW];
+      if (MODE == kFactor) {
+        const R ad = f[0];
+        R d = ad;
+        R iv = R(0);
+        if (ad != R(0)) {
+          d = d - in_c[0] * in_c[0];
+          d = d - (omega * in_c[0]) * in_c[1];
+          d = d - in_a[0] * in_a[0];
+          d = d - (omega * in_a[0]) * in_a[1];
+          d = d - carry[0] * carry[0];
+          d = d - (omega * carry[0]) * carry[1];
+          const R piv = d < min_ratio * ad ? ad : d;
+          iv = R(1) / sqrt(piv);
+        }
+        const R ss = f[1] * iv, sa = f[2] * iv, scv = f[3] * iv;
+        st_coef(pcoef + 4 * off, iv, ss, sa, scv);
+        out_s[0] = ss; out_s[1] = sa + scv;
+        out_a[0] = sa; out_a[1] = ss + scv;
+        out_c[0] = scv; out_c[1] = ss + sa;
+      } else if (MODE == kForward) {
+        R rv = f[0];
+        if (UPD) {
+          rv = rv - al_r * f[5];
+          o_r[off] = rv;
+          const R av = fabs(rv);
+          rmax = av > rmax ? av : rmax;
+        }
+        R vv = rv;
+        vv -= in_c[0];
+        vv -= in_a[0];
+        vv -= carry[0];
+        const R y = vv * f[1];
+        o_out[off] = y;
+        out_s[0] = f[2] * y;
+        out_a[0] = f[3] * y;
+        out_c[0] = f[4] * y;
+      } else {
+        R vv = f[0];
+        vv -= f[2] * carry[0];
+        vv -= f[3] * in_a[0];
+        vv -= f[4] * in_c[0];
+        const R z = vv * f[1];
+        o_out[off] = z;
+        dsum += (double)z * (double)f[5];
+        out_s[0] = out_a[0] = out_c[0] = z;
+      }
+      if (live && ea_dst) {
+        u64 wd[EW];
+#pragma unroll
+        for (int k = 0; k < PW; ++k) TagWords<R>::pack(out_a[k], ep, wd + k * TW);
+#pragma unroll
+        for (int k = 0; k < EW; ++k) st_relaxed_u64(ea_dst + s * ES + k, wd[k]);
+      }
+      if (live && ec_dst) {
+        u64 wd[EW];
+#pragma unroll
+        for (int k = 0; k < PW; ++k) TagWords<R>::pack(out_c[k], ep, wd + k * TW);
+#pragma unroll
+        for (int k = 0; k < EW; ++k) st_relaxed_u64(ec_dst + s * ES + k, wd[k]);
+      }
+#pragma unroll
+      for (int k = 0; k < PW; ++k) {
+        if (c_prod) xc[nxt][w][al][k] = out_c[k];
+        prev_a[k] = out_a[k];
+        prev_c[k] = out_c[k];
+        carry[k] = out_s[k];
+      }
+      // refill this register slot with step u + kPre
+      {
+        const int un = u + kPre;
+        if (un < NR) load(off + kPre * RS, pre[v]);
+        const bool lv = un < NR && live_at(un);
+        const int sn = s_at(un);
+#pragma unroll
+        for (int k = 0; k < EW; ++k) {
+          if (lv && ea_src) epa[v][k] = ld_relaxed_u64(ea_src + sn * ES + k);
+          if (lv && ec_src) epc[v][k] = ld_relaxed_u64(ec_src + sn * ES + k);
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if (MODE == kForward && UPD && A.part) {
+    const double m = block_max<double>((double)rmax, red);
+    if (tid == 0) A.part[p] = m;
+  }
+  if (MODE == kBackward && A.part) {
+    const double sm = block_sum<double>(dsum, red);
+    if (tid == 0) A.part[p] = sm;
+  }
+}
+
+// x += alpha s (the update of the last PCG iteration, which no SpMV follows)
+template <typename R>
+__global__ void k_pl_axpy(long long len, const double* __restrict__ sc, const R* __restrict__ s,
+                          R* __restrict__ x) {
+  const R al = (R)sc[S_ALPHA];
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < len;
+       e += (long long)gridDim.x * blockDim.x)
+    x[e] = x[e] + al * s[e];
+}
+
+// ---- streaming kernels over the pencil layout --------------------------------
+// Element e -> (patch, row, line) and the cell's position in the box.
+struct PlCell {
+  long long p;
+  int t, l, al, cl, PAi, PCi, s;
+  bool live;
+};
+
+__device__ inline PlCell pl_cell(const PencilGeom& G, long long e) {
+  PlCell c;
+  const long long per = (long long)G.R * kPatchLines;
+  c.p = e / per;
+  const int rem = (int)(e - c.p * per);
+  c.t = rem / kPatchLines;
+  c.l = rem - c.t * kPatchLines;
+  c.al = c.l & (kPatch - 1);
+  c.cl = c.l / kPatch;
+  c.PAi = (int)(c.p % G.nPA);
+  c.PCi = (int)(c.p / G.nPA);
+  c.s = c.t - c.al - c.cl;
+  c.live = c.s >= 0 && c.s < G.Ls && c.PAi * kPatch + c.al < G.NA &&
+           c.PCi * kPatch + c.cl < G.NC;
+  return c;
+}
+
+// Indices of the six neighbours of a live cell (-1 where the box ends).
+struct PlNbr {
+  long long ms, ps, ma, pa, mc, pc;
+};
+
+__device__ inline PlNbr pl_nbr(const PencilGeom& G, const PlCell& c, long long e) {
+  PlNbr n;
+  n.ms = c.s > 0 ? e - kPatchLines : -1;
+  n.ps = c.s + 1 < G.Ls ? e + kPatchLines : -1;
+  if (c.al > 0) n.ma = e - kPatchLines - 1;
+  else n.ma = c.PAi > 0 ? pl_index(G, c.p - 1, c.t + kPatch - 1, c.l + kPatch - 1) : -1;
+  if (c.al < kPatch - 1) n.pa = e + kPatchLines + 1;
+  else n.pa = c.PAi + 1 < G.nPA ? pl_index(G, c.p + 1, c.t - (kPatch - 1), c.l - (kPatch - 1)) : -1;
+  if (c.cl > 0) n.mc = e - kPatchLines - kPatch;
+  else n.mc = c.PCi > 0 ? pl_index(G, c.p - G.nPA, c.t + kPatch - 1,
+                                    c.l + kPatch * (kPatch - 1)) : -1;
+  if (c.cl < kPatch - 1) n.pc = e + kPatchLines + kPatch;
+  else n.pc = c.PCi + 1 < G.nPC ? pl_index(G, c.p + G.nPA, c.t - (kPatch - 1),
+                                            c.l - kPatch * (kPatch - 1)) : -1;
+  return n;
+}
+
+// s_new = z + beta s_old (at all 7 stencil points), q = A s_new,
+// partial[block] = sum s_new.q.  Row order of the reference's sorted row for
+// interior cells: -c, -a, -s, diagonal, +s, +a, +c.
+//
+// The previous iteration's x += alpha s_old is applied here too (alpha is
+// still the previous iteration's when this kernel runs; 0 before the first).
+template <typename R>
+__global__ void __launch_bounds__(kRedThreads)
+    k_pl_spmv_s(PencilGeom G, const R* __restrict__ AD, const R* __restrict__ AS,
+                const R* __restrict__ AA, const R* __restrict__ AC, const R* __restrict__ z,
+                const R* __restrict__ sold, R* __restrict__ snew, R* __restrict__ q,
+                R* __restrict__ x, const double* __restrict__ sc,
+                double* __restrict__ partial) {
+  __shared__ double sm[kRedThreads];
+  if (*(const int*)(sc + S_DONE)) return;
+  const R be = (R)sc[S_BETA];
+  const R al = (R)sc[S_ALPHA];
+  double acc = 0;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < G.len;
+       e += (long long)gridDim.x * blockDim.x) {
+    const PlCell c = pl_cell(G, e);
+    if (!c.live) continue;
+    const PlNbr n = pl_nbr(G, c, e);
+    R r = 0;
+    if (n.mc >= 0) r += AC[n.mc] * (z[n.mc] + be * sold[n.mc]);
+    if (n.ma >= 0) r += AA[n.ma] * (z[n.ma] + be * sold[n.ma]);
+    if (n.ms >= 0) r += AS[n.ms] * (z[n.ms] + be * sold[n.ms]);
+    const R so = sold[e];
+    x[e] = x[e] + al * so;
+    const R sn = z[e] + be * so;
+    r += AD[e] * sn;
+    if (n.ps >= 0) r += AS[e] * (z[n.ps] + be * sold[n.ps]);
+    if (n.pa >= 0) r += AA[e] * (z[n.pa] + be * sold[n.pa]);
+    if (n.pc >= 0) r += AC[e] * (z[n.pc] + be * sold[n.pc]);
+    snew[e] = sn;
+    q[e] = r;
+    acc += (double)sn * (double)r;
+  }
+  acc = block_sum<double>(acc, sm);
+  if (threadIdx.x == 0) partial[blockIdx.x] = acc;
+}
+
+// FP64 residual r64 = b - A x64 with the coefficients promoted; partial max|r64|
+template <typename R>
+__global__ void __launch_bounds__(kRedThreads)
+    k_pl_residual64(PencilGeom G, const R* __restrict__ AD, const R* __restrict__ AS,
+                    const R* __restrict__ AA, const R* __restrict__ AC,
+                    const R* __restrict__ b, const double* __restrict__ x,
+                    double* __restrict__ r, double* __restrict__ partial) {
+  __shared__ double sm[kRedThreads];
+  double m = 0;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < G.len;
+       e += (long long)gridDim.x * blockDim.x) {
+    const PlCell c = pl_cell(G, e);
+    if (!c.live) continue;
+    const PlNbr n = pl_nbr(G, c, e);
+    double acc = (double)AD[e] * x[e];
+    if (n.ms >= 0) acc += (double)AS[n.ms] * x[n.ms];
+    if (n.ma >= 0) acc += (double)AA[n.ma] * x[n.ma];
+    if (n.mc >= 0) acc += (double)AC[n.mc] * x[n.mc];
+    if (n.ps >= 0) acc += (double)AS[e] * x[n.ps];
+    if (n.pa >= 0) acc += (double)AA[e] * x[n.pa];
+    if (n.pc >= 0) acc += (double)AC[e] * x[n.pc];
+    const double rv = (double)b[e] - acc;
+    r[e] = rv;
+    const double av = fabs(rv);
+    m = av > m ? av : m;
+  }
+  m = block_max<double>(m, sm);
+  if (threadIdx.x == 0) partial[blockIdx.x] = m;
+}
+
+// r32 = r64 / res, x32 = 0 (inner solve of one refinement)
+template <typename R>
+__global__ void k_pl_demote(long long len, const double* __restrict__ r64,
+                            const double* __restrict__ sc, R* __restrict__ r,
+                            R* __restrict__ x) {
+  const double scale = 1.0 / sc[0];
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < len;
+       e += (long long)gridDim.x * blockDim.x) {
+    r[e] = (R)(r64[e] * scale);
+    x[e] = R(0);
+  }
+}
+
+// x64 += x32 * res
+template <typename R>
+__global__ void k_pl_accumulate(long long len, const R* __restrict__ x,
+                                const double* __restrict__ sc, double* __restrict__ x64) {
+  const double s = sc[0];
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < len;
+       e += (long long)gridDim.x * blockDim.x)
+    x64[e] += (double)x[e] * s;
+}
+
+// r64 = b (promoted)
+template <typename R>
+__global__ void k_pl_promote(long long len, const R* __restrict__ b, double* __restrict__ o) {
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < len;
+       e += (long long)gridDim.x * blockDim.x)
+    o[e] = (double)b[e];
+}
+
+// The DOF box: block-reduced min/max of the DOF cell coordinates into
+// bbox[0..5] (min x,y,z, max x,y,z) and the DOF count into partial[block].
+__global__ void __launch_bounds__(kRedThreads)
+    k_dof_box(GridDesc g, const int* __restrict__ active_list, long long nent,
+              const unsigned char* __restrict__ dof, int* __restrict__ bbox,
+              double* __restrict__ partial) {
+  __shared__ int smn[3][kRedThreads / 32], smx[3][kRedThreads / 32];
+  __shared__ double sm[kRedThreads];
+  int mn[3] = {1 << 30, 1 << 30, 1 << 30}, mx[3] = {-1, -1, -1};
+  double cnt = 0;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nent;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long n = active_node(active_list, e);
+    if (!(dof[n] & 1)) continue;
+    int I, J, K;
+    node_ijk(g, n, I, J, K);
+    const int v[3] = {I, J, K};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      mn[a] = v[a] < mn[a] ? v[a] : mn[a];
+      mx[a] = v[a] > mx[a] ? v[a] : mx[a];
+    }
+    cnt += 1.0;
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int wmn = __reduce_min_sync(0xffffffffu, mn[a]);
+    const int wmx = __reduce_max_sync(0xffffffffu, mx[a]);
+    if (lane == 0) { smn[a][wid] = wmn; smx[a][wid] = wmx; }
+  }
+  cnt = block_sum<double>(cnt, sm);  // contains __syncthreads
+  if (threadIdx.x == 0) {
+    partial[blockIdx.x] = cnt;
+    for (int a = 0; a < 3; ++a) {
+      int bmn = 1 << 30, bmx = -1;
+      for (int w = 0; w < kRedThreads / 32; ++w) {
+        bmn = smn[a][w] < bmn ? smn[a][w] : bmn;
+        bmx = smx[a][w] > bmx ? smx[a][w] : bmx;
+      }
+      if (bmx >= 0) {
+        atomicMin(bbox + a, bmn);
+        atomicMax(bbox + 3 + a, bmx);
+      }
+    }
+  }
+}
+
+// Gather the assembled system into the pencil layout.  Couplings are kept
+// only between two DOF cells (the reference's matrix has no other entries).
+template <typename R>
+__global__ void __launch_bounds__(kRedThreads)
+    k_pl_gather(PencilGeom G, GridDesc g, const unsigned char* __restrict__ active,
+                const unsigned char* __restrict__ dof, const R* __restrict__ F,
+                long long fs, R* __restrict__ AD, R* __restrict__ AS, R* __restrict__ AA,
+                R* __restrict__ AC, R* __restrict__ B) {
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < G.len;
+       e += (long long)gridDim.x * blockDim.x) {
+    const PlCell c = pl_cell(G, e);
+    R ad = 0, as = 0, aa = 0, ac = 0, bv = 0;
+    if (c.live) {
+      int P[3];
+      P[G.ax_s] = G.lo[G.ax_s] + c.s;
+      P[G.ax_a] = G.lo[G.ax_a] + c.PAi * kPatch + c.al;
+      P[G.ax_c] = G.lo[G.ax_c] + c.PCi * kPatch + c.cl;
+      if (in_grid(g, P[0], P[1], P[2]) && active[bucket_of(g, P[0], P[1], P[2])]) {
+        const long long n = node_linear(g, P[0], P[1], P[2]);
+        if (dof[n] & 1) {
+          ad = F[G_ADIAG * fs + n];
+          bv = F[G_B * fs + n];
+          const int axes[3] = {G.ax_s, G.ax_a, G.ax_c};
+          R cpl[3];
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            int Q[3] = {P[0], P[1], P[2]};
+            Q[axes[k]] += 1;
+            cpl[k] = R(0);
+            if (in_grid(g, Q[0], Q[1], Q[2]) && active[bucket_of(g, Q[0], Q[1], Q[2])] &&
+                (dof[node_linear(g, Q[0], Q[1], Q[2])] & 1))
+              cpl[k] = F[(G_AX + axes[k]) * fs + n];
+          }
+          as = cpl[0]; aa = cpl[1]; ac = cpl[2];
+        }
+      }
+    }
+    AD[e] = ad; AS[e] = as; AA[e] = aa; AC[e] = ac; B[e] = bv;
+  }
+}
+
+// pressure of every active node from the pencil solution (0 off the DOFs)
+template <typename R>
+__global__ void k_pl_scatter_pressure(PencilGeom G, GridDesc g, const int* __restrict__ active_list,
+                                      long long nent, const unsigned char* __restrict__ dof,
+                                      const R* __restrict__ x32, const double* __restrict__ x64,
+                                      R* __restrict__ p) {
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nent;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long n = active_node(active_list, e);
+    R v = R(0);
+    if (dof[n] & 1) {
+      int P[3];
+      node_ijk(g, n, P[0], P[1], P[2]);
+      const int s = P[G.ax_s] - G.lo[G.ax_s];
+      const int a = P[G.ax_a] - G.lo[G.ax_a];
+      const int c = P[G.ax_c] - G.lo[G.ax_c];
+      const int PAi = a / kPatch, al = a - PAi * kPatch;
+      const int PCi = c / kPatch, cl = c - PCi * kPatch;
+      const long long idx = pl_index(G, (long long)PCi * G.nPA + PAi, s + al + cl, al + kPatch * cl);
+      v = x64 ? (R)x64[idx] : x32[idx];
+    }
+    p[n] = v;
+  }
+}
+
+}  // namespace wcg

@@ -11,6 +11,7 @@
 #include "wcg_kernels.cuh"
 #include "wcg_pcg.cuh"
 #include "wcg_wsweep.cuh"
+#include "wcg_pencil.cuh"
 #include "wcg_scan.cuh"
 
 namespace wcg {
@@ -59,6 +60,7 @@ void ctx_free(Context& c) {
                     &c.active_pre, &c.active, &c.cell_start, &c.cell_cursor,
                     &c.gfield, &c.gvalid, &c.gdof, &c.wave_list, &c.wave_count,
                     &c.tile_flag, &c.active_list, &c.rx64, &c.rr64, &c.rb64,
+                    &c.pl, &c.pl64, &c.pl_edge, &c.pl_order, &c.pl_part,
                     &c.scratch, &c.dscalars, &c.derr, &c.ticket};
   for (DevBuf* b : bufs) b->release();
   if (c.hscalars) cudaFreeHost(c.hscalars);
@@ -757,6 +759,281 @@ __global__ void k_store_pressure(const int* __restrict__ active_list, long long 
   }
 }
 
+// ---------------------------------------------------------------------------
+// Pressure solve in the pencil layout (wcg_pencil.cuh)
+
+// Lay out the DOF box [lo, hi] (grid cells, inclusive) and allocate the arrays.
+template <typename R>
+static cudaError_t pl_setup(Context& c, const int* lo, const int* hi) {
+  PencilGeom G{};
+  int ext[3];
+  for (int a = 0; a < 3; ++a) {
+    G.lo[a] = lo[a];
+    ext[a] = hi[a] - lo[a] + 1;
+  }
+  G.ax_s = 0;
+  for (int a = 1; a < 3; ++a)
+    if (ext[a] > ext[G.ax_s]) G.ax_s = a;
+  G.ax_a = G.ax_s == 0 ? 1 : 0;
+  G.ax_c = G.ax_s == 2 ? 1 : 2;
+  G.Ls = ext[G.ax_s];
+  G.NA = ext[G.ax_a];
+  G.NC = ext[G.ax_c];
+  G.nPA = (G.NA + kPatch - 1) / kPatch;
+  G.nPC = (G.NC + kPatch - 1) / kPatch;
+  G.R = G.Ls + 2 * (kPatch - 1);
+  G.npatch = (long long)G.nPA * G.nPC;
+  G.len = G.npatch * G.R * kPatchLines;
+  const bool same_shape = c.plg.npatch == G.npatch && c.plg.nPA == G.nPA;
+  c.plg = G;
+  if (G.len > c.pl_cap) {
+    c.pl_cap = G.len;
+    WCG_TRY(c.pl.ensure((size_t)kNumPlFields * G.len * sizeof(R)));
+    if (c.prm.precision != 0) WCG_TRY(c.pl64.ensure((size_t)kNumPl64Fields * G.len * sizeof(double)));
+  }
+  // edge words: 2 faces x Ls x 16 entries x (2 values x words per value)
+  const size_t edge_bytes = (size_t)G.npatch * 2 * G.Ls * kPatch * 2 * (sizeof(R) / 4) * 8;
+  if (edge_bytes > c.pl_edge.bytes) {
+    WCG_TRY(c.pl_edge.ensure(edge_bytes));
+    // tags of a fresh buffer must not match any epoch (epochs start at 1)
+    WCG_TRY(cudaMemsetAsync(c.pl_edge.p, 0, c.pl_edge.bytes, c.stream));
+  }
+  WCG_TRY(c.pl_part.ensure((size_t)std::max<long long>(G.npatch, kPlBlocks) * sizeof(double)));
+  if (!same_shape || c.pl_order_h.size() != (size_t)G.npatch) {
+    // patches in wave order PAi + PCi
+    c.pl_order_h.resize(G.npatch);
+    int k = 0;
+    for (int w = 0; w <= G.nPA + G.nPC - 2; ++w)
+      for (int pc = 0; pc < G.nPC; ++pc) {
+        const int pa = w - pc;
+        if (pa >= 0 && pa < G.nPA) c.pl_order_h[k++] = pc * G.nPA + pa;
+      }
+    WCG_TRY(c.pl_order.ensure((size_t)G.npatch * sizeof(int)));
+    WCG_TRY(cudaMemcpyAsync(c.pl_order.p, c.pl_order_h.data(), G.npatch * sizeof(int),
+                            cudaMemcpyHostToDevice, c.stream));
+  }
+  // every array starts at zero (rows and lines outside the box stay zero)
+  WCG_TRY(cudaMemsetAsync(c.pl.p, 0, (size_t)kNumPlFields * G.len * sizeof(R), c.stream));
+  c.pl_tickets = 0;
+  WCG_TRY(cudaMemsetAsync(c.ticket.as<int>() + 1, 0, sizeof(int), c.stream));
+  return cudaSuccess;
+}
+
+template <typename R>
+static R* pl_field(Context& c, int f) {
+  return c.pl.as<R>() + (size_t)f * c.plg.len;
+}
+
+template <typename R>
+static PencilSweepArgs<R> pl_args(Context& c) {
+  PencilSweepArgs<R> a{};
+  a.G = c.plg;
+  a.order = c.pl_order.as<int>();
+  a.ticket = c.ticket.as<int>() + 1;
+  a.edge = c.pl_edge.as<u64>();
+  a.AD = pl_field<R>(c, PL_AD);
+  a.AS = pl_field<R>(c, PL_AS);
+  a.AA = pl_field<R>(c, PL_AA);
+  a.AC = pl_field<R>(c, PL_AC);
+  a.coef = pl_field<R>(c, PL_COEF);
+  a.sc = c.dscalars.as<double>();
+  a.omega = (R)0.97;
+  a.min_ratio = (R)0.25;
+  a.err = c.derr.as<int>();
+  return a;
+}
+
+template <typename R, int MODE, bool UPD>
+static cudaError_t pl_sweep(Context& c, PencilSweepArgs<R> a) {
+  ProfScope prof(c, MODE == kFactor ? P_MICFACTOR : P_MICSWEEP);
+  a.epoch = (unsigned)(++c.tile_epoch);
+  a.ticket_base = c.pl_tickets;
+  c.pl_tickets += (int)c.plg.npatch;
+  ++c.launches, k_pencil_sweep<R, MODE, UPD><<<(unsigned)c.plg.npatch, kPatchLines, 0, c.stream>>>(a);
+  return cudaGetLastError();
+}
+
+// PCGSolver<T>::solve (PCGSolver.h:260-308) in the pencil layout on the
+// factored system: A x = r from x = 0; r is overwritten with the residual.
+template <typename R>
+static cudaError_t pl_pcg(Context& c, R* r, R* x, double tol_abs, int maxiters, int* iters,
+                          int* conv, double* res) {
+  const PencilGeom& G = c.plg;
+  R* z = pl_field<R>(c, PL_Z);
+  R* s0 = pl_field<R>(c, PL_S0);
+  R* s1 = pl_field<R>(c, PL_S1);
+  R* q = pl_field<R>(c, PL_Q);
+  R* y = pl_field<R>(c, PL_Y);
+  double* sc = c.dscalars.as<double>();
+  double* part = c.scratch.as<double>();
+  double* ppart = c.pl_part.as<double>();
+  const int np = (int)G.npatch;
+  *iters = 0;
+  *conv = 0;
+  *res = 0;
+  if (maxiters <= 0) return cudaSuccess;
+  {
+    const double init[9] = {0.0, 0.0, 0.0, 0.0, 0.0, tol_abs, 0.0, (double)maxiters, 0.0};
+    WCG_TRY(set_scalars(c, S_RHO, init, 9));  // clears S_DONE too
+  }
+  WCG_TRY(cudaMemsetAsync(s0, 0, G.len * sizeof(R), c.stream));
+  // z = M^-1 r, rho = z.r
+  PencilSweepArgs<R> fa = pl_args<R>(c);
+  fa.in = r;
+  fa.out = y;
+  WCG_TRY((pl_sweep<R, kForward, false>(c, fa)));
+  PencilSweepArgs<R> ba = pl_args<R>(c);
+  ba.in = y;
+  ba.out = z;
+  ba.r = r;
+  ba.part = ppart;
+  WCG_TRY((pl_sweep<R, kBackward, false>(c, ba)));
+  {
+    ProfScope prof(c, P_PCGVEC);
+    ++c.launches, k_red_beta<<<1, kRedThreads, 0, c.stream>>>(ppart, np, sc, 1);
+  }
+  double h[9];
+  WCG_TRY(fetch(c, sc + S_RHO, 1, h));
+  if (h[0] == 0 || h[0] != h[0]) return cudaSuccess;  // PCGSolver.h:276-279
+  fa.r = r;
+  fa.q = q;
+  fa.part = ppart;
+  R* sold = s0;
+  R* snew = s1;
+  const R* AD = pl_field<R>(c, PL_AD);
+  const R* AS = pl_field<R>(c, PL_AS);
+  const R* AA = pl_field<R>(c, PL_AA);
+  const R* AC = pl_field<R>(c, PL_AC);
+  for (;;) {
+    for (int b = 0; b < kPcgBatch; ++b) {
+      {
+        ProfScope prof(c, P_PCGVEC);
+        ++c.launches, k_pl_spmv_s<R><<<kPlBlocks, kRedThreads, 0, c.stream>>>(
+            G, AD, AS, AA, AC, z, sold, snew, q, x, sc, part);
+        ++c.launches, k_red_alpha<<<1, kRedThreads, 0, c.stream>>>(part, kPlBlocks, sc);
+      }
+      WCG_TRY((pl_sweep<R, kForward, true>(c, fa)));
+      {
+        ProfScope prof(c, P_PCGVEC);
+        ++c.launches, k_red_conv<<<1, kRedThreads, 0, c.stream>>>(ppart, np, sc);
+      }
+      WCG_TRY((pl_sweep<R, kBackward, false>(c, ba)));
+      {
+        ProfScope prof(c, P_PCGVEC);
+        ++c.launches, k_red_beta<<<1, kRedThreads, 0, c.stream>>>(ppart, np, sc, 0);
+      }
+      R* t = sold;
+      sold = snew;
+      snew = t;
+    }
+    WCG_TRY(fetch(c, sc + S_RES, 6, h));  // res, beta, tol, iter, maxit, done
+    const int done = *(const int*)&h[5];
+    *res = h[0];
+    *iters = (int)h[3];
+    if (done) {
+      *conv = done == 1 ? 1 : 0;
+      break;
+    }
+  }
+  // x += alpha s of the last iteration (iteration i searched along s1 for even
+  // i, s0 for odd i; later launches of the batch returned early)
+  if (*iters > 0) {
+    ProfScope prof(c, P_PCGVEC);
+    const R* slast = ((*iters - 1) & 1) == 0 ? s1 : s0;
+    ++c.launches, k_pl_axpy<R><<<kPlBlocks, kRedThreads, 0, c.stream>>>(G.len, sc, slast, x);
+  }
+  return cudaGetLastError();
+}
+
+// project_fine's solve in the pencil layout, from the assembled bucket-major
+// system to the bucket-major pressure field.
+template <typename R>
+static cudaError_t pl_project(Context& c, double bnorm, const int* lo, const int* hi) {
+  R* F = c.gfield.as<R>();
+  const int* al = c.active_list.as<int>();
+  const unsigned char* act = c.active.as<unsigned char>();
+  const unsigned char* dof = c.gdof.as<unsigned char>();
+  const long long nent = c.n_active * 64;
+  double* dsc = c.dscalars.as<double>();
+  double* part = c.scratch.as<double>();
+  const double tol = c.prm.criterion * bnorm;
+  WCG_TRY(pl_setup<R>(c, lo, hi));
+  const PencilGeom& G = c.plg;
+  {
+    ProfScope prof(c, P_PCGVEC);
+    ++c.launches, k_pl_gather<R><<<kPlBlocks, kRedThreads, 0, c.stream>>>(
+        G, c.g, act, dof, F, c.gcap, pl_field<R>(c, PL_AD), pl_field<R>(c, PL_AS),
+        pl_field<R>(c, PL_AA), pl_field<R>(c, PL_AC), pl_field<R>(c, PL_B));
+  }
+  WCG_TRY(cudaGetLastError());
+  // MIC(0) factor (PCGSolver::form_preconditioner)
+  {
+    const double zero = 0.0;
+    WCG_TRY(set_scalars(c, S_DONE, &zero, 1));
+  }
+  WCG_TRY((pl_sweep<R, kFactor, false>(c, pl_args<R>(c))));
+  R* r = pl_field<R>(c, PL_R);
+  R* x = pl_field<R>(c, PL_X);
+  const R* b = pl_field<R>(c, PL_B);
+  R* pressure = F + G_PRESSURE * c.gcap;
+  if (c.prm.precision == 0) {
+    WCG_TRY(cudaMemcpyAsync(r, b, G.len * sizeof(R), cudaMemcpyDeviceToDevice, c.stream));
+    int iters = 0, conv = 0;
+    double res = bnorm;
+    WCG_TRY(pl_pcg<R>(c, r, x, tol, c.prm.maxiters, &iters, &conv, &res));
+    c.stats.pcg_iters = iters;
+    c.stats.converged = conv;
+    c.stats.residual = res;
+    ++c.launches, k_pl_scatter_pressure<R><<<kRedBlocks, kRedThreads, 0, c.stream>>>(
+        G, c.g, al, nent, dof, x, nullptr, pressure);
+    return cudaGetLastError();
+  }
+  // mixed precision: FP32 inner PCG, FP64 residual and solution
+  double* x64 = c.pl64.as<double>() + (size_t)PL64_X * G.len;
+  double* r64 = c.pl64.as<double>() + (size_t)PL64_R * G.len;
+  WCG_TRY(cudaMemsetAsync(x64, 0, G.len * sizeof(double), c.stream));
+  ++c.launches, k_pl_promote<R><<<kPlBlocks, kRedThreads, 0, c.stream>>>(G.len, b, r64);
+  double res = bnorm;
+  double h[1];
+  int total = 0, k = 0;
+  bool conv = false;
+  const double inner_rel = c.prm.refine_inner_tol > 0 ? c.prm.refine_inner_tol : 0.0;
+  for (k = 0; k <= c.prm.max_refinements; ++k) {
+    if (res <= tol) {
+      conv = true;
+      break;
+    }
+    if (total >= c.prm.maxiters || k == c.prm.max_refinements) break;
+    // scaled residual (||r32||_inf == 1) into r, x = 0
+    WCG_TRY(cudaMemcpyAsync(dsc + 5, &res, sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    {
+      ProfScope prof(c, P_REFINE);
+      ++c.launches, k_pl_demote<R><<<kPlBlocks, kRedThreads, 0, c.stream>>>(G.len, r64, dsc + 5, r, x);
+    }
+    const double want = std::max(inner_rel, 0.5 * tol / res);
+    int iters = 0, ic = 0;
+    double ires = 0;
+    WCG_TRY(pl_pcg<R>(c, r, x, want, c.prm.maxiters - total, &iters, &ic, &ires));
+    total += iters;
+    ProfScope prof3(c, P_REFINE);
+    ++c.launches, k_pl_accumulate<R><<<kPlBlocks, kRedThreads, 0, c.stream>>>(G.len, x, dsc + 5, x64);
+    ++c.launches, k_pl_residual64<R><<<kPlBlocks, kRedThreads, 0, c.stream>>>(
+        G, pl_field<R>(c, PL_AD), pl_field<R>(c, PL_AS), pl_field<R>(c, PL_AA),
+        pl_field<R>(c, PL_AC), b, x64, r64, part);
+    ++c.launches, k_reduce_max<<<1, kRedThreads, 0, c.stream>>>(part, kPlBlocks, dsc + 6);
+    WCG_TRY(fetch(c, dsc + 6, 1, h));
+    res = h[0];
+    if (iters == 0) break;
+  }
+  c.stats.pcg_iters = total;
+  c.stats.refinements = k;
+  c.stats.converged = conv ? 1 : 0;
+  c.stats.residual = res;
+  ++c.launches, k_pl_scatter_pressure<R><<<kRedBlocks, kRedThreads, 0, c.stream>>>(
+      G, c.g, al, nent, dof, x, x64, pressure);
+  return cudaGetLastError();
+}
+
 template <typename R>
 static cudaError_t project_fine_t(Context& c, double dt) {
   c.stats.pcg_iters = 0;
@@ -781,14 +1058,23 @@ static cudaError_t project_fine_t(Context& c, double dt) {
   R* x = F + G_X * c.gcap;
   const R* b = F + G_B * c.gcap;
   double h[4];
-  // ||b||_inf and the number of DOFs
+  // ||b||_inf, the number of DOFs and their bounding box
   absmax<R>(c, b, dsc + 4);
+  int* dbox = (int*)(dsc + 32);
   {
     ProfScope prof(c, P_PCGVEC);
-    ++c.launches, k_count_dof<<<kRedBlocks, kRedThreads, 0, c.stream>>>(al, nent, dof, part);
+    const int init[6] = {1 << 30, 1 << 30, 1 << 30, -1, -1, -1};
+    WCG_TRY(cudaMemcpyAsync(dbox, init, sizeof(init), cudaMemcpyHostToDevice, c.stream));
+    ++c.launches, k_dof_box<<<kRedBlocks, kRedThreads, 0, c.stream>>>(c.g, al, nent, dof, dbox, part);
     ++c.launches, k_reduce_sum<<<1, kRedThreads, 0, c.stream>>>(part, kRedBlocks, dsc + 5);
   }
-  WCG_TRY(fetch(c, dsc + 4, 2, h));
+  WCG_TRY(cudaMemcpyAsync(c.hscalars + 4, dsc + 4, 31 * sizeof(double), cudaMemcpyDeviceToHost,
+                          c.stream));
+  WCG_TRY(cudaStreamSynchronize(c.stream));
+  h[0] = c.hscalars[4];
+  h[1] = c.hscalars[5];
+  int box[6];
+  std::memcpy(box, c.hscalars + 32, sizeof(box));
   const double bnorm = h[0];
   c.stats.rhs_norm = bnorm;
   c.stats.ndof = (long long)h[1];
@@ -797,6 +1083,7 @@ static cudaError_t project_fine_t(Context& c, double dt) {
     WCG_TRY(cudaMemsetAsync(F + G_PRESSURE * c.gcap, 0, c.gcap * sizeof(R), c.stream));
     return cudaGetLastError();
   }
+  if (c.pcg_layout == 0) return pl_project<R>(c, bnorm, box, box + 3);
   const double tol = c.prm.criterion * bnorm;
   // MIC(0) factor (PCGSolver::form_preconditioner)
   {
