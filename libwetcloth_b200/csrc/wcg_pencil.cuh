@@ -45,7 +45,7 @@ namespace wcg {
 
 constexpr int kPatch = 16;                    // lines per patch edge
 constexpr int kPatchLines = kPatch * kPatch;  // threads of a sweep CTA
-constexpr int kPre = 4;                       // rows prefetched ahead
+constexpr int kPre = 4;                       // rows of edge words prefetched ahead
 constexpr int kPlBlocks = 592;                // streaming kernels: 4 x 148 SMs
 
 __host__ __device__ inline long long pl_index(const PencilGeom& G, long long p, int t, int l) {
@@ -87,6 +87,57 @@ struct TagWords<double> {
     return __longlong_as_double((long long)((w[1] << 32) | (w[0] & 0xffffffffull)));
   }
 };
+
+// ---- bulk row copies into shared memory (cp.async.bulk + mbarrier) ---------
+__device__ inline unsigned smem_u32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ inline void mbar_init(unsigned bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+__device__ inline void mbar_expect_tx(unsigned bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+__device__ inline bool mbar_try_wait(unsigned bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// global -> shared, 16-byte aligned addresses, bytes a multiple of 16
+__device__ inline void bulk_g2s(unsigned dst, const void* src, unsigned bytes, unsigned bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+      "l"(src), "r"(bytes), "r"(bar)
+      : "memory");
+}
+__device__ inline unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+constexpr unsigned long long kWaitNs = 2000000000ull;  // bound of an mbarrier wait (2 s)
+
+// Stages of the shared-memory row ring of a sweep.
+template <typename R>
+struct SweepStages {
+  static constexpr int D = sizeof(R) == 4 ? 8 : 6;
+};
+// Arrays staged per row: factor A_d, A_s, A_a, A_c; forward r, coef x4 (, q);
+// backward y, coef x4, r.
+__host__ __device__ constexpr int sweep_nf(int mode, bool upd) {
+  return mode == 0 ? 4 : (mode == 1 ? (upd ? 6 : 5) : 6);
+}
+template <typename R>
+__host__ __device__ constexpr size_t sweep_dyn_smem(int mode, bool upd) {
+  return (size_t)SweepStages<R>::D * sweep_nf(mode, upd) * 256 * sizeof(R) +
+         (size_t)SweepStages<R>::D * 8;
+}
 
 // Words of the edge buffer: entry (producer patch, side, s, k), EW words each.
 // side 0: the a-face (k = cl), side 1: the c-face (k = al).
@@ -156,12 +207,18 @@ __global__ void __launch_bounds__(kPatchLines, 1)
   constexpr int EW = PW * TW;
   // prefetched per cell: factor A_d, A_s, A_a, A_c; forward in, coef[4] (, q);
   // backward in, coef[4], r
-  constexpr int NF = MODE == kFactor ? 4 : (MODE == kForward ? (UPD ? 6 : 5) : 6);
+  constexpr int NF = sweep_nf(MODE, UPD);
+  static_assert(kFactor == 0 && kForward == 1 && kBackward == 2, "mode numbering");
   constexpr int RS = BWD ? -kPatchLines : kPatchLines;  // element step per row
   constexpr int NW = kPatchLines / 32;
+  constexpr int D = SweepStages<R>::D;             // rows in flight
+  constexpr int SLOT = NF * kPatchLines;            // Reals per staged row
   __shared__ int s_ticket;
   __shared__ R xc[2][NW][kPatch][PW];
   __shared__ double red[kPatchLines];
+  extern __shared__ __align__(128) unsigned char dsm[];  // D slots, then D mbarriers
+  R* const ring = reinterpret_cast<R*>(dsm);
+  const unsigned bar0 = smem_u32(dsm + (size_t)D * SLOT * sizeof(R));
   const PencilGeom& G = A.G;
   const int tid = threadIdx.x;
   const int lane = tid & 31, w = tid >> 5;
@@ -209,37 +266,61 @@ __global__ void __launch_bounds__(kPatchLines, 1)
   const R omega = A.omega, min_ratio = A.min_ratio;
   // per-thread base pointers (patch and line applied); rows by 32-bit offset
   const long long pb = (long long)p * NR * kPatchLines + tid;
-  const R* __restrict__ f0 = MODE == kFactor ? A.AD + pb : A.in + pb;
-  const R* __restrict__ f1 = MODE == kFactor ? A.AS + pb : nullptr;
-  const R* __restrict__ f2 = MODE == kFactor ? A.AA + pb : nullptr;
-  const R* __restrict__ f3 = MODE == kFactor ? A.AC + pb : nullptr;
   R* __restrict__ pcoef = A.coef + 4 * pb;
-  const R* __restrict__ fx = MODE == kForward ? (UPD ? A.q + pb : nullptr)
-                                              : (BWD ? A.r + pb : nullptr);
   R* __restrict__ o_out = MODE == kFactor ? nullptr : A.out + pb;
   R* __restrict__ o_r = (MODE == kForward && UPD) ? A.r + pb : nullptr;
   const int off0 = BWD ? (NR - 1) * kPatchLines : 0;
   auto s_at = [&](int u) { return BWD ? (NR - 1 - u) - dl : u - dl; };
   auto live_at = [&](int u) { return line && (unsigned)(u - u0) < (unsigned)Ls; };
-  // rows outside a line's range hold zeros, so whole rows are read and every
-  // cell is computed (zeros stay zeros); only the edge words need liveness
-  auto load = [&](int off, R* f) {
-    f[0] = __ldcs(f0 + off);
+  // Rows outside a line's range hold zeros, so whole rows are staged and every
+  // cell is computed (zeros stay zeros); only the edge words need liveness.
+  // Thread 0 copies whole rows (one bulk copy per array) D rows ahead into a
+  // ring slot; the slot layout is [first array][coef x4 or A_s, A_a, A_c][q/r].
+  const long long pbase = (long long)p * NR * kPatchLines;
+  auto issue = [&](int u) {
+    const int j = u % D;
+    const unsigned bar = bar0 + 8 * j;
+    const unsigned dst = smem_u32(ring + (size_t)j * SLOT);
+    const long long rb = pbase + (long long)(BWD ? NR - 1 - u : u) * kPatchLines;
+    constexpr unsigned RB = kPatchLines * sizeof(R);
+    mbar_expect_tx(bar, NF * RB);
     if (MODE == kFactor) {
-      f[1] = __ldcs(f1 + off);
-      f[2] = __ldcs(f2 + off);
-      f[3] = __ldcs(f3 + off);
+      bulk_g2s(dst, A.AD + rb, RB, bar);
+      bulk_g2s(dst + RB, A.AS + rb, RB, bar);
+      bulk_g2s(dst + 2 * RB, A.AA + rb, RB, bar);
+      bulk_g2s(dst + 3 * RB, A.AC + rb, RB, bar);
     } else {
-      ld_coef(pcoef + 4 * off, f + 1);
-      if (NF == 6) f[5] = __ldcs(fx + off);
+      bulk_g2s(dst, A.in + rb, RB, bar);
+      bulk_g2s(dst + RB, A.coef + 4 * rb, 4 * RB, bar);
+      if (NF == 6) bulk_g2s(dst + 5 * RB, (MODE == kForward ? A.q : A.r) + rb, RB, bar);
     }
   };
+  bool gave_up = false;
+  auto mwait = [&](int u) {
+    const unsigned bar = bar0 + 8 * (u % D);
+    const unsigned par = (unsigned)(u / D) & 1u;
+    if (mbar_try_wait(bar, par)) return;
+    const unsigned long long t0 = global_ns();
+    while (!mbar_try_wait(bar, par)) {
+      if (gave_up || global_ns() - t0 > kWaitNs) {
+        if (!gave_up) record_error(A.err, kErrWaitTimeout);
+        gave_up = true;
+        return;
+      }
+    }
+  };
+  if (tid == 0) {
+    for (int j = 0; j < D; ++j) mbar_init(bar0 + 8 * j, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+  if (tid == 0)
+    for (int u = 0; u < D && u < NR; ++u) issue(u);
 
-  R pre[kPre][NF];
   u64 epa[kPre][EW], epc[kPre][EW];
 #pragma unroll
   for (int v = 0; v < kPre; ++v) {
-    if (v < NR) load(off0 + v * RS, pre[v]);
     const bool lv = v < NR && live_at(v);
     const int sv = s_at(v);
 #pragma unroll
@@ -253,7 +334,6 @@ __global__ void __launch_bounds__(kPatchLines, 1)
   for (int k = 0; k < PW; ++k) carry[k] = prev_a[k] = prev_c[k] = R(0);
   R rmax = 0;
   double dsum = 0;
-  bool gave_up = false;
   // complete an edge entry: re-read words whose tag is stale (bounded)
   auto ewait = [&](u64* wd, const u64* src) {
 #pragma unroll
@@ -302,7 +382,22 @@ __global__ void __launch_bounds__(kPatchLines, 1)
 #pragma unroll
         for (int k = 0; k < PW; ++k) in_c[k] = TagWords<R>::unpack(epc[v] + k * TW);
       }
-      const R* f = pre[v];
+      // this row's inputs from the ring
+      R f[NF];
+      mwait(u);
+      {
+        const R* S = ring + (size_t)(u % D) * SLOT;
+        f[0] = S[tid];
+        if (MODE == kFactor) {
+          f[1] = S[kPatchLines + tid];
+          f[2] = S[2 * kPatchLines + tid];
+          f[3] = S[3 * kPatchLines + tid];
+        } else {
+          const R* cf = S + kPatchLines + 4 * tid;
+          f[1] = cf[0]; f[2] = cf[1]; f[3] = cf[2]; f[4] = cf[3];
+          if (NF == 6) f[5] = S[5 * kPatchLines + tid];
+        }
+      }
       R out_s[PW], out_a[PW], out_c[PW];
       if (MODE == kFactor) {
         const R ad = f[0];
@@ -371,10 +466,9 @@ __global__ void __launch_bounds__(kPatchLines, 1)
         prev_c[k] = out_c[k];
         carry[k] = out_s[k];
       }
-      // refill this register slot with step u + kPre
+      // edge words of step u + kPre
       {
         const int un = u + kPre;
-        if (un < NR) load(off + kPre * RS, pre[v]);
         const bool lv = un < NR && live_at(un);
         const int sn = s_at(un);
 #pragma unroll
@@ -384,6 +478,19 @@ __global__ void __launch_bounds__(kPatchLines, 1)
         }
       }
       __syncthreads();
+      // every thread is done with slot u % D: refill it with row u + D
+      if (tid == 0 && u + D < NR) issue(u + D);
+    }
+  }
+  if (gave_up) {
+    // a wait gave up: give the copies still in flight into the ring time to
+    // land (bounded) before the CTA exits
+    for (int u = NR - D > 0 ? NR - D : 0; u < NR; ++u) {
+      const unsigned bar = bar0 + 8 * (u % D);
+      const unsigned par = (unsigned)(u / D) & 1u;
+      const unsigned long long t0 = global_ns();
+      while (!mbar_try_wait(bar, par) && global_ns() - t0 < kWaitNs) {
+      }
     }
   }
   if (MODE == kForward && UPD && A.part) {

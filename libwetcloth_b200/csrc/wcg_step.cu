@@ -849,7 +849,14 @@ static cudaError_t pl_sweep(Context& c, PencilSweepArgs<R> a) {
   a.epoch = (unsigned)(++c.tile_epoch);
   a.ticket_base = c.pl_tickets;
   c.pl_tickets += (int)c.plg.npatch;
-  ++c.launches, k_pencil_sweep<R, MODE, UPD><<<(unsigned)c.plg.npatch, kPatchLines, 0, c.stream>>>(a);
+  constexpr size_t smem = sweep_dyn_smem<R>(MODE, UPD);
+  static bool attr_set = false;  // per instantiation, once per process
+  if (!attr_set) {
+    WCG_TRY(cudaFuncSetAttribute(k_pencil_sweep<R, MODE, UPD>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_set = true;
+  }
+  ++c.launches, k_pencil_sweep<R, MODE, UPD><<<(unsigned)c.plg.npatch, kPatchLines, smem, c.stream>>>(a);
   return cudaGetLastError();
 }
 
