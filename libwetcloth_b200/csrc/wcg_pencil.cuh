@@ -47,6 +47,7 @@ constexpr int kPatch = 16;                    // lines per patch edge
 constexpr int kPatchLines = kPatch * kPatch;  // threads of a sweep CTA
 constexpr int kPre = 4;                       // rows of edge words prefetched ahead
 constexpr int kPlBlocks = 592;                // streaming kernels: 4 x 148 SMs
+static_assert(kRedThreads == kPatchLines, "streaming kernels walk one row per block");
 
 __host__ __device__ inline long long pl_index(const PencilGeom& G, long long p, int t, int l) {
   return (p * G.R + t) * kPatchLines + l;
@@ -521,17 +522,18 @@ struct PlCell {
   bool live;
 };
 
-__device__ inline PlCell pl_cell(const PencilGeom& G, long long e) {
+// Cell of line l in row `row` (= patch * R + t) of the layout; 32-bit math
+// (npatch * R stays far below 2^31).
+__device__ inline PlCell pl_cell(const PencilGeom& G, int row, int l) {
   PlCell c;
-  const long long per = (long long)G.R * kPatchLines;
-  c.p = e / per;
-  const int rem = (int)(e - c.p * per);
-  c.t = rem / kPatchLines;
-  c.l = rem - c.t * kPatchLines;
-  c.al = c.l & (kPatch - 1);
-  c.cl = c.l / kPatch;
-  c.PAi = (int)(c.p % G.nPA);
-  c.PCi = (int)(c.p / G.nPA);
+  const int p = row / G.R;
+  c.p = p;
+  c.t = row - p * G.R;
+  c.l = l;
+  c.al = l & (kPatch - 1);
+  c.cl = l / kPatch;
+  c.PAi = p % G.nPA;
+  c.PCi = p / G.nPA;
   c.s = c.t - c.al - c.cl;
   c.live = c.s >= 0 && c.s < G.Ls && c.PAi * kPatch + c.al < G.NA &&
            c.PCi * kPatch + c.cl < G.NC;
@@ -578,9 +580,10 @@ __global__ void __launch_bounds__(kRedThreads)
   const R be = (R)sc[S_BETA];
   const R al = (R)sc[S_ALPHA];
   double acc = 0;
-  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < G.len;
-       e += (long long)gridDim.x * blockDim.x) {
-    const PlCell c = pl_cell(G, e);
+  const int nrow = (int)(G.npatch * G.R);
+  for (int row = blockIdx.x; row < nrow; row += gridDim.x) {
+    const long long e = (long long)row * kPatchLines + threadIdx.x;
+    const PlCell c = pl_cell(G, row, threadIdx.x);
     if (!c.live) continue;
     const PlNbr n = pl_nbr(G, c, e);
     R r = 0;
@@ -611,9 +614,10 @@ __global__ void __launch_bounds__(kRedThreads)
                     double* __restrict__ r, double* __restrict__ partial) {
   __shared__ double sm[kRedThreads];
   double m = 0;
-  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < G.len;
-       e += (long long)gridDim.x * blockDim.x) {
-    const PlCell c = pl_cell(G, e);
+  const int nrow = (int)(G.npatch * G.R);
+  for (int row = blockIdx.x; row < nrow; row += gridDim.x) {
+    const long long e = (long long)row * kPatchLines + threadIdx.x;
+    const PlCell c = pl_cell(G, row, threadIdx.x);
     if (!c.live) continue;
     const PlNbr n = pl_nbr(G, c, e);
     double acc = (double)AD[e] * x[e];
@@ -719,9 +723,10 @@ __global__ void __launch_bounds__(kRedThreads)
                 const unsigned char* __restrict__ dof, const R* __restrict__ F,
                 long long fs, R* __restrict__ AD, R* __restrict__ AS, R* __restrict__ AA,
                 R* __restrict__ AC, R* __restrict__ B) {
-  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < G.len;
-       e += (long long)gridDim.x * blockDim.x) {
-    const PlCell c = pl_cell(G, e);
+  const int nrow = (int)(G.npatch * G.R);
+  for (int row = blockIdx.x; row < nrow; row += gridDim.x) {
+    const long long e = (long long)row * kPatchLines + threadIdx.x;
+    const PlCell c = pl_cell(G, row, threadIdx.x);
     R ad = 0, as = 0, aa = 0, ac = 0, bv = 0;
     if (c.live) {
       int P[3];
