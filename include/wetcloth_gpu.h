@@ -35,6 +35,11 @@ enum {
 
 enum { WCG_FP64 = 0, WCG_FP32_REFINE = 1 };
 
+/* Pressure solver: MIC(0)-PCG (robertbridson::PCGSolver, PCGSolver.h:245-330;
+ * the default) or the reference's own default, multigrid-PCG
+ * (AMGPCGSolveSparse, AlgebraicMultigrid.h:248-361). */
+enum { WCG_SOLVER_MIC0 = 0, WCG_SOLVER_MG = 1 };
+
 /* Scene parameters: the liquid subset of LiquidInfo
  * (libWetCloth/Core/TwoDScene.h:35-91) plus bucket info (numcells fixed at 4,
  * kernel order 2) and one solid box whose inside holds the fluid
@@ -54,6 +59,7 @@ typedef struct wcg_params {
   int precision;                   /* WCG_FP64 or WCG_FP32_REFINE */
   double refine_inner_tol;         /* FP32 inner-solve relative tolerance (0: aim at criterion) */
   int max_refinements;             /* FP64 refinement sweeps (0: 20) */
+  int solver;                      /* WCG_SOLVER_MIC0 or WCG_SOLVER_MG */
 } wcg_params;
 
 typedef struct wcg_ctx wcg_ctx;

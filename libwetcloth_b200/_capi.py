@@ -25,6 +25,8 @@ WCG_ERR_DEVICE = 4
 WCG_ERR_STATE = 5
 WCG_FP64 = 0
 WCG_FP32_REFINE = 1
+WCG_SOLVER_MIC0 = 0
+WCG_SOLVER_MG = 1
 
 
 class WcgParams(ctypes.Structure):
@@ -43,6 +45,7 @@ class WcgParams(ctypes.Structure):
         ("precision", ctypes.c_int),
         ("refine_inner_tol", ctypes.c_double),
         ("max_refinements", ctypes.c_int),
+        ("solver", ctypes.c_int),
     ]
 
 

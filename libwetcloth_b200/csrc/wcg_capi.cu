@@ -162,6 +162,7 @@ void wcg_default_params(wcg_params* p) {
   p->precision = WCG_FP64;
   p->refine_inner_tol = 0.0;
   p->max_refinements = 20;
+  p->solver = WCG_SOLVER_MIC0;
 }
 
 int wcg_create(const wcg_params* params, wcg_ctx** out) {
@@ -191,6 +192,9 @@ int wcg_create(const wcg_params* params, wcg_ctx** out) {
   p.precision = params->precision;
   p.refine_inner_tol = params->refine_inner_tol > 0 ? params->refine_inner_tol : 0.0;
   p.max_refinements = params->max_refinements > 0 ? params->max_refinements : 20;
+  if (params->solver != WCG_SOLVER_MIC0 && params->solver != WCG_SOLVER_MG)
+    return fail(WCG_ERR_ARG, "solver must be WCG_SOLVER_MIC0 or WCG_SOLVER_MG");
+  p.solver = params->solver;
   // wavefront tile shape (performance knob; both compute identical results)
   if (const char* v = getenv("WCG_SWEEP_TILE")) ctx->c.sweep_variant = !strcmp(v, "warp") ? 1 : 0;
   // layout of the pressure solve (performance knob; same arithmetic)

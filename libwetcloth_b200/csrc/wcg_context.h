@@ -28,6 +28,7 @@ struct Params {
   int precision;  // 0: FP64, 1: FP32 transfers + FP32 PCG with FP64 refinement
   double refine_inner_tol;  // relative tolerance of each FP32 inner solve
   int max_refinements;
+  int solver;     // 0: MIC(0)-PCG, 1: multigrid-PCG (AMGPCGSolveSparse)
 };
 
 // A device allocation that grows and never shrinks.
@@ -170,6 +171,12 @@ struct Context {
   long long pl_cap = 0;
   int pl_tickets = 0;            // sweep tickets handed out in this solve
   std::vector<int> pl_order_h;
+
+  // multigrid-PCG: dense levels (d, ax, ay, az, x, b per cell; masks) and the
+  // level-0 PCG vectors
+  DevBuf mg, mg_mask, mg_vec;
+  struct MgDims { int ni, nj, nk, n; long long off; };
+  std::vector<MgDims> mg_dims;     // levels of the last solve
 
   // FP64 refinement vectors (precision 1)
   DevBuf rx64, rr64, rb64;       // nnode doubles each

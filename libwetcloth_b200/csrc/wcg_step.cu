@@ -12,6 +12,7 @@
 #include "wcg_pcg.cuh"
 #include "wcg_wsweep.cuh"
 #include "wcg_pencil.cuh"
+#include "wcg_mg.cuh"
 #include "wcg_scan.cuh"
 
 namespace wcg {
@@ -61,6 +62,7 @@ void ctx_free(Context& c) {
                     &c.gfield, &c.gvalid, &c.gdof, &c.wave_list, &c.wave_count,
                     &c.tile_flag, &c.active_list, &c.rx64, &c.rr64, &c.rb64,
                     &c.pl, &c.pl64, &c.pl_edge, &c.pl_order, &c.pl_part,
+                    &c.mg, &c.mg_mask, &c.mg_vec,
                     &c.scratch, &c.dscalars, &c.derr, &c.ticket};
   for (DevBuf* b : bufs) b->release();
   if (c.hscalars) cudaFreeHost(c.hscalars);
@@ -1041,6 +1043,253 @@ static cudaError_t pl_project(Context& c, double bnorm, const int* lo, const int
   return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Multigrid-PCG (wcg_mg.cuh): AMGPCGSolveSparse, AlgebraicMultigrid.h:248-361
+
+constexpr int kMgMaxLevels = 24;
+constexpr int kMgPreSweeps = 4;      // amgVCycleCompressed: RBGS(.., 4)
+constexpr int kMgCoarseSweeps = 200; // RBGS(.., 200) on the coarsest level
+constexpr int kMgMaxCoarseDofs = 4096;
+
+static int mg_blocks(long long n) {
+  const long long b = (n + kMgThreads - 1) / kMgThreads;
+  return (int)std::max<long long>(1, std::min<long long>(b, kMgBlocks));
+}
+
+template <typename R>
+static MgLevel<R> mg_level(Context& c, int l) {
+  const Context::MgDims& d = c.mg_dims[l];
+  R* base = c.mg.as<R>() + d.off * 6;
+  MgLevel<R> L;
+  L.ni = d.ni; L.nj = d.nj; L.nk = d.nk; L.n = d.n;
+  L.d = base;
+  L.ax = base + d.n;
+  L.ay = base + 2 * (long long)d.n;
+  L.az = base + 3 * (long long)d.n;
+  L.x = base + 4 * (long long)d.n;
+  L.b = base + 5 * (long long)d.n;
+  L.m = c.mg_mask.as<unsigned char>() + d.off;
+  return L;
+}
+
+// Level 0 over the grid of cells; coarse levels while a level has more than
+// 4096 DOFs (generateLevelsGalerkinCoarseningSparse, GeometricLevelGen.h:192-236).
+// rhs receives the assembled rhs in the level-0 layout.
+template <typename R>
+static cudaError_t mg_setup(Context& c, long long ndof0) {
+  const GridDesc& g = c.g;
+  // dims of every possible level, then the allocation
+  std::vector<Context::MgDims> dims;
+  long long off = 0;
+  int ni = g.NI, nj = g.NJ, nk = g.NK;
+  for (int l = 0; l < kMgMaxLevels; ++l) {
+    Context::MgDims d{ni, nj, nk, ni * nj * nk, off};
+    dims.push_back(d);
+    off += d.n;
+    if (ni == 1 && nj == 1 && nk == 1) break;
+    ni = (ni + 1) / 2; nj = (nj + 1) / 2; nk = (nk + 1) / 2;
+  }
+  WCG_TRY(c.mg.ensure((size_t)off * 6 * sizeof(R)));
+  WCG_TRY(c.mg_mask.ensure((size_t)off));
+  const long long n0 = dims[0].n;
+  WCG_TRY(c.mg_vec.ensure((size_t)n0 * 5 * sizeof(R)));
+  c.mg_dims = dims;
+  R* F = c.gfield.as<R>();
+  R* rhs = c.mg_vec.as<R>();
+  MgLevel<R> L0 = mg_level<R>(c, 0);
+  {
+    ProfScope prof(c, P_PCGVEC);
+    ++c.launches, k_mg_gather0<R><<<mg_blocks(n0), kMgThreads, 0, c.stream>>>(
+        g, c.active.as<unsigned char>(), c.gdof.as<unsigned char>(), F, c.gcap, L0, rhs);
+  }
+  long long unknowns = ndof0;
+  int nlev = 1;
+  double* part = c.scratch.as<double>();
+  double* dsc = c.dscalars.as<double>();
+  while (unknowns > kMgMaxCoarseDofs && nlev < (int)dims.size()) {
+    MgLevel<R> f = mg_level<R>(c, nlev - 1), cl = mg_level<R>(c, nlev);
+    const int nb = std::min(mg_blocks(cl.n), kRedBlocks);
+    {
+      ProfScope prof(c, P_PCGVEC);
+      ++c.launches, k_mg_coarsen<R><<<nb, kMgThreads, 0, c.stream>>>(f, cl, part);
+      ++c.launches, k_reduce_sum<<<1, kRedThreads, 0, c.stream>>>(part, nb, dsc + 7);
+    }
+    double h = 0;
+    WCG_TRY(fetch(c, dsc + 7, 1, &h));
+    unknowns = (long long)h;
+    ++nlev;
+    if (cl.ni == 1 && cl.nj == 1 && cl.nk == 1) break;
+  }
+  c.mg_dims.resize(nlev);
+  return cudaGetLastError();
+}
+
+// z = one V-cycle from z = 0 on A z = r (amgPrecondCompressed /
+// amgVCycleCompressed); r and z are level-0 vectors
+template <typename R>
+static cudaError_t mg_vcycle(Context& c, R* z, R* r) {
+  ProfScope prof(c, P_MICSWEEP);
+  const int nlev = (int)c.mg_dims.size();
+  MgLevel<R> L[kMgMaxLevels];
+  for (int l = 0; l < nlev; ++l) L[l] = mg_level<R>(c, l);
+  L[0].x = z;
+  L[0].b = r;
+  WCG_TRY(cudaMemsetAsync(z, 0, (size_t)L[0].n * sizeof(R), c.stream));
+  auto smooth = [&](int l, int sweeps) {
+    const int nb = mg_blocks(L[l].n);
+    for (int it = 0; it < sweeps; ++it) {
+      ++c.launches, k_mg_smooth<R><<<nb, kMgThreads, 0, c.stream>>>(L[l], 1);
+      ++c.launches, k_mg_smooth<R><<<nb, kMgThreads, 0, c.stream>>>(L[l], 0);
+    }
+  };
+  for (int l = 0; l + 1 < nlev; ++l) {
+    smooth(l, kMgPreSweeps);
+    ++c.launches, k_mg_restrict<R><<<mg_blocks(L[l + 1].n), kMgThreads, 0, c.stream>>>(L[l], L[l + 1]);
+  }
+  ++c.launches, k_mg_coarsest<R><<<1, kMgCoarseThreads, 0, c.stream>>>(L[nlev - 1], kMgCoarseSweeps);
+  for (int l = nlev - 2; l >= 0; --l) {
+    ++c.launches, k_mg_prolong<R><<<mg_blocks(L[l].n), kMgThreads, 0, c.stream>>>(L[l + 1], L[l]);
+    smooth(l, kMgPreSweeps);
+  }
+  return cudaGetLastError();
+}
+
+// AMGPCGSolveSparse's CG loop on level 0: A x = r from x = 0 (r is overwritten
+// with the residual); stops when ||r||_inf <= tol_abs
+template <typename R>
+static cudaError_t mg_pcg(Context& c, R* r, R* x, double tol_abs, int maxiters, int* iters,
+                          int* conv, double* res) {
+  MgLevel<R> L0 = mg_level<R>(c, 0);
+  const int n = L0.n;
+  R* base = c.mg_vec.as<R>();
+  R* s = base + 2 * (long long)n;
+  R* q = base + 3 * (long long)n;
+  R* z = base + 4 * (long long)n;
+  double* sc = c.dscalars.as<double>();
+  double* part = c.scratch.as<double>();
+  const int nb = std::min(mg_blocks(n), kRedBlocks);
+  *iters = 0;
+  *conv = 0;
+  *res = 0;
+  if (maxiters <= 0) return cudaSuccess;
+  {
+    const double init[9] = {0.0, 0.0, 0.0, 0.0, 0.0, tol_abs, 0.0, (double)maxiters, 0.0};
+    WCG_TRY(set_scalars(c, S_RHO, init, 9));
+  }
+  WCG_TRY(cudaMemsetAsync(x, 0, (size_t)n * sizeof(R), c.stream));
+  WCG_TRY(mg_vcycle<R>(c, z, r));
+  {
+    ProfScope prof(c, P_PCGVEC);
+    ++c.launches, k_mg_dot<R><<<nb, kMgThreads, 0, c.stream>>>(n, z, r, part);
+    ++c.launches, k_red_beta<<<1, kRedThreads, 0, c.stream>>>(part, nb, sc, 1);
+  }
+  double h[6];
+  WCG_TRY(fetch(c, sc + S_RHO, 1, h));
+  if (h[0] == 0 || h[0] != h[0]) return cudaSuccess;  // AlgebraicMultigrid.h:301-314
+  WCG_TRY(cudaMemcpyAsync(s, z, (size_t)n * sizeof(R), cudaMemcpyDeviceToDevice, c.stream));
+  for (;;) {
+    {
+      ProfScope prof(c, P_PCGVEC);
+      ++c.launches, k_mg_spmv<R><<<nb, kMgThreads, 0, c.stream>>>(L0, s, q, sc, part);
+      ++c.launches, k_red_alpha<<<1, kRedThreads, 0, c.stream>>>(part, nb, sc);
+      ++c.launches, k_mg_update<R><<<nb, kMgThreads, 0, c.stream>>>(n, s, q, x, r, sc, part);
+      ++c.launches, k_red_conv<<<1, kRedThreads, 0, c.stream>>>(part, nb, sc);
+    }
+    WCG_TRY(fetch(c, sc + S_RES, 6, h));  // res, beta, tol, iter, maxit, done
+    const int done = *(const int*)&h[5];
+    *res = h[0];
+    *iters = (int)h[3];
+    if (done) {
+      *conv = done == 1 ? 1 : 0;
+      break;
+    }
+    WCG_TRY(mg_vcycle<R>(c, z, r));
+    ProfScope prof(c, P_PCGVEC);
+    ++c.launches, k_mg_dot<R><<<nb, kMgThreads, 0, c.stream>>>(n, z, r, part);
+    ++c.launches, k_red_beta<<<1, kRedThreads, 0, c.stream>>>(part, nb, sc, 0);
+    ++c.launches, k_mg_direction<R><<<nb, kMgThreads, 0, c.stream>>>(n, z, s, sc);
+  }
+  return cudaGetLastError();
+}
+
+// project_fine's solve with multigrid-PCG, from the assembled bucket-major
+// system to the bucket-major pressure field
+template <typename R>
+static cudaError_t mg_project(Context& c, double bnorm) {
+  R* F = c.gfield.as<R>();
+  const int* al = c.active_list.as<int>();
+  const unsigned char* dof = c.gdof.as<unsigned char>();
+  const long long nent = c.n_active * 64;
+  double* dsc = c.dscalars.as<double>();
+  double* part = c.scratch.as<double>();
+  const double tol = c.prm.criterion * bnorm;
+  WCG_TRY(mg_setup<R>(c, c.stats.ndof));
+  MgLevel<R> L0 = mg_level<R>(c, 0);
+  const int n = L0.n;
+  // level-0 vectors in mg_vec: rhs, r, s, q, z; the solution x takes the
+  // level-0 b array, which the V-cycle does not use (its level-0 rhs is r)
+  R* rhs = c.mg_vec.as<R>();
+  R* r = rhs + n;
+  R* x = L0.b;
+  R* pressure = F + G_PRESSURE * c.gcap;
+  const int nb = std::min(mg_blocks(n), kRedBlocks);
+  if (c.prm.precision == 0) {
+    WCG_TRY(cudaMemcpyAsync(r, rhs, (size_t)n * sizeof(R), cudaMemcpyDeviceToDevice, c.stream));
+    int iters = 0, conv = 0;
+    double res = bnorm;
+    WCG_TRY(mg_pcg<R>(c, r, x, tol, c.prm.maxiters, &iters, &conv, &res));
+    c.stats.pcg_iters = iters;
+    c.stats.converged = conv;
+    c.stats.residual = res;
+    ++c.launches, k_mg_scatter_pressure<R><<<kRedBlocks, kRedThreads, 0, c.stream>>>(
+        c.g, al, nent, dof, x, nullptr, pressure);
+    return cudaGetLastError();
+  }
+  // mixed precision: FP32 multigrid-PCG, FP64 residual and solution
+  WCG_TRY(c.rx64.ensure((size_t)n * sizeof(double)));
+  WCG_TRY(c.rr64.ensure((size_t)n * sizeof(double)));
+  double* x64 = c.rx64.as<double>();
+  double* r64 = c.rr64.as<double>();
+  WCG_TRY(cudaMemsetAsync(x64, 0, (size_t)n * sizeof(double), c.stream));
+  ++c.launches, k_pl_promote<R><<<nb, kMgThreads, 0, c.stream>>>(n, rhs, r64);
+  double res = bnorm;
+  double h[1];
+  int total = 0, k = 0;
+  bool conv = false;
+  const double inner_rel = c.prm.refine_inner_tol > 0 ? c.prm.refine_inner_tol : 0.0;
+  for (k = 0; k <= c.prm.max_refinements; ++k) {
+    if (res <= tol) {
+      conv = true;
+      break;
+    }
+    if (total >= c.prm.maxiters || k == c.prm.max_refinements) break;
+    WCG_TRY(cudaMemcpyAsync(dsc + 5, &res, sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    {
+      ProfScope prof(c, P_REFINE);
+      ++c.launches, k_pl_demote<R><<<nb, kMgThreads, 0, c.stream>>>(n, r64, dsc + 5, r, x);
+    }
+    const double want = std::max(inner_rel, 0.5 * tol / res);
+    int iters = 0, ic = 0;
+    double ires = 0;
+    WCG_TRY(mg_pcg<R>(c, r, x, want, c.prm.maxiters - total, &iters, &ic, &ires));
+    total += iters;
+    ProfScope prof3(c, P_REFINE);
+    ++c.launches, k_pl_accumulate<R><<<nb, kMgThreads, 0, c.stream>>>(n, x, dsc + 5, x64);
+    ++c.launches, k_mg_residual64<R><<<nb, kMgThreads, 0, c.stream>>>(L0, rhs, x64, r64, part);
+    ++c.launches, k_reduce_max<<<1, kRedThreads, 0, c.stream>>>(part, nb, dsc + 6);
+    WCG_TRY(fetch(c, dsc + 6, 1, h));
+    res = h[0];
+    if (iters == 0) break;
+  }
+  c.stats.pcg_iters = total;
+  c.stats.refinements = k;
+  c.stats.converged = conv ? 1 : 0;
+  c.stats.residual = res;
+  ++c.launches, k_mg_scatter_pressure<R><<<kRedBlocks, kRedThreads, 0, c.stream>>>(
+      c.g, al, nent, dof, x, x64, pressure);
+  return cudaGetLastError();
+}
+
 template <typename R>
 static cudaError_t project_fine_t(Context& c, double dt) {
   c.stats.pcg_iters = 0;
@@ -1090,6 +1339,7 @@ static cudaError_t project_fine_t(Context& c, double dt) {
     WCG_TRY(cudaMemsetAsync(F + G_PRESSURE * c.gcap, 0, c.gcap * sizeof(R), c.stream));
     return cudaGetLastError();
   }
+  if (c.prm.solver == 1) return mg_project<R>(c, bnorm);
   if (c.pcg_layout == 0) return pl_project<R>(c, bnorm, box, box + 3);
   const double tol = c.prm.criterion * bnorm;
   // MIC(0) factor (PCGSolver::form_preconditioner)

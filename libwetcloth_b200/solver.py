@@ -16,7 +16,7 @@ from ._capi import check, _dp
 
 
 def make_params(p, precision=_capi.WCG_FP64, refine_inner_tol=0.0,
-                max_refinements=20) -> _capi.WcgParams:
+                max_refinements=20, solver=_capi.WCG_SOLVER_MIC0) -> _capi.WcgParams:
     prm = _capi.WcgParams()
     _capi.load().wcg_default_params(ctypes.byref(prm))
     prm.dx = p.dx
@@ -34,6 +34,7 @@ def make_params(p, precision=_capi.WCG_FP64, refine_inner_tol=0.0,
     prm.precision = precision
     prm.refine_inner_tol = refine_inner_tol
     prm.max_refinements = max_refinements
+    prm.solver = solver
     return prm
 
 

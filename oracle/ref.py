@@ -47,6 +47,7 @@ def _lib(omp: bool):
         L.wcref_solver_stats.argtypes = [ctypes.c_void_p,
                                          ctypes.POINTER(ctypes.c_int), _D]
         L.wcref_timers.argtypes = [ctypes.c_void_p, _D]
+        L.wcref_amg_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), _D]
         _libs[omp] = L
     return _libs[omp]
 
@@ -105,6 +106,14 @@ class RefScene:
         it = ctypes.c_int(0)
         res = ctypes.c_double(0)
         self.L.wcref_solver_stats(self.h, ctypes.byref(it), ctypes.byref(res))
+        return it.value, res.value
+
+    def amg_stats(self):
+        """(iterations, residual) of the reference's default multigrid-PCG
+        (AMGPCGSolveSparse) on the system of the last snapshot step."""
+        it = ctypes.c_int(0)
+        res = ctypes.c_double(0)
+        self.L.wcref_amg_stats(self.h, ctypes.byref(it), ctypes.byref(res))
         return it.value, res.value
 
     def timers(self) -> np.ndarray:

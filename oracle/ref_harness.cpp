@@ -45,6 +45,7 @@
 #include <unordered_map>
 #include <unordered_set>
 #include <vector>
+#include "AlgebraicMultigrid.h"
 #include "MathDefs.h"
 #include <Eigen/Geometry>
 #define private public
@@ -471,6 +472,33 @@ int wcref_substep(void* hp, double sub_dt, int snapshot) {
   if (snapshot) {
     snap_system(*h);
     dense(*h, "pressure_amg", s.m_node_pressure);
+    // iteration count of the reference's default solve (printed, not kept, by
+    // pressure::solveNodePressure): the same AMGPCGSolveSparse call on the
+    // same system (Pressure.cpp:402-436, :797)
+    const unsigned n = e.m_fine_pressure_matrix.n;
+    if (n > 0 && e.m_fine_pressure_rhs.size() >= n) {
+      const Sorter& bk = s.getParticleBuckets();
+      const int nc = s.getDefaultNumNodes();
+      std::vector<Vector3i> dof_ijk(n);
+      const int nb = s.getNumBuckets();
+      for (int b = 0; b < nb; ++b) {
+        const VectorXi& gi = e.m_fine_global_indices[b];
+        const Vector3i hnd = bk.bucket_handle(b);
+        for (int i = 0; i < (int)gi.size(); ++i)
+          if (gi[i] >= 0) {
+            const Vector3i lh = s.getNodeHandle(i);
+            dof_ijk[gi[i]] = Vector3i(hnd(0) * nc + lh(0), hnd(1) * nc + lh(1), hnd(2) * nc + lh(2));
+          }
+      }
+      std::vector<double> rhs(e.m_fine_pressure_rhs.begin(), e.m_fine_pressure_rhs.begin() + n);
+      std::vector<double> result(n, 0.0);
+      double res = 0;
+      int iters = 0;
+      AMGPCGSolveSparse(e.m_fine_pressure_matrix, rhs, result, dof_ijk, h->p.criterion,
+                        h->p.maxiters, res, iters, bk.ni * nc, bk.nj * nc, bk.nk * nc);
+      h->last_iters_amg = iters;
+      h->last_res_amg = res;
+    }
   }
   if (h->p.mic) {
     const unsigned n = e.m_fine_pressure_matrix.n;
@@ -563,6 +591,13 @@ void wcref_solver_stats(void* hp, int* iters_mic, double* res_mic) {
   Harness* h = (Harness*)hp;
   *iters_mic = h->last_iters_mic;
   *res_mic = h->last_res_mic;
+}
+
+// AMGPCGSolveSparse iterations and residual of the last snapshot step
+void wcref_amg_stats(void* hp, int* iters, double* res) {
+  Harness* h = (Harness*)hp;
+  *iters = h->last_iters_amg;
+  *res = h->last_res_amg;
 }
 
 // cumulative phase timers (seconds), slots as WetClothCore timing_buffer
