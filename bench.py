@@ -40,6 +40,8 @@ def parse():
                     help="timed steps of the FP64 arm (default: --steps)")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-mg", action="store_true",
+                    help="skip the multigrid-PCG arms (the reference's default solver)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-n", type=int, default=64,
                     help="grid of the bounded CPU-baseline sample")
@@ -164,7 +166,8 @@ def run_ours(args, rank, world, dev):
     import numpy as np
     import torch
     from libwetcloth_b200 import scenes
-    from libwetcloth_b200._capi import WCG_FP32_REFINE, WCG_FP64
+    from libwetcloth_b200._capi import (WCG_FP32_REFINE, WCG_FP64, WCG_SOLVER_MG,
+                                        WCG_SOLVER_MIC0)
     from libwetcloth_b200.solver import FluidScene
 
     def barrier():
@@ -179,8 +182,8 @@ def run_ours(args, rank, world, dev):
     gen_s = time.time() - t0
     np_ = sc.x.shape[0]
 
-    def timed(precision, steps, warmup, sample_clocks=False):
-        sim = FluidScene(sc, precision=precision)
+    def timed(precision, steps, warmup, sample_clocks=False, solver=WCG_SOLVER_MIC0):
+        sim = FluidScene(sc, precision=precision, solver=solver)
         for _ in range(warmup):
             sim.step(DT)
         stream = torch.cuda.ExternalStream(sim.stream_ptr, device=f"cuda:{dev}")
@@ -266,6 +269,16 @@ def run_ours(args, rank, world, dev):
         sim64, info64 = timed(WCG_FP64, k64, args.warmup)
         sim64.close()
         fp64 = info64
+    # the reference's default solver (multigrid-PCG) on the same workload
+    mg = None
+    if not args.no_mg:
+        mg = {}
+        for name, prec in (("fp32_refine", WCG_FP32_REFINE), ("fp64", WCG_FP64)):
+            k_mg = max(1, min(args.steps, 5))
+            sim_mg, info_mg = timed(prec, k_mg, args.warmup, solver=WCG_SOLVER_MG)
+            sim_mg.close()
+            mg[name] = {"ms_per_step": round(info_mg["ms"], 3), "steps": k_mg,
+                        "pcg_iters_per_step": info_mg["iters"]}
     # roofline of the dominant phase
     peak, peak_kind = measured_peaks()
     w = 4
@@ -331,6 +344,9 @@ def run_ours(args, rank, world, dev):
     if fp64:
         out["fp64"] = {"ms_per_step": round(fp64["ms"], 3), "pcg_iters_per_step": fp64["iters"],
                        "speedup_fp32_refine_vs_fp64": round(fp64["ms"] / main["ms"], 3)}
+    if mg:
+        out["multigrid_pcg"] = dict(mg, note="same step with the reference's default "
+                                              "pressure solver (AMGPCGSolveSparse restated)")
     return out
 
 
