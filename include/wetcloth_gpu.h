@@ -100,6 +100,19 @@ int wcg_download_liquid_device(wcg_ctx* ctx, double* x3, double* v3,
                                double* C9);
 long long wcg_num_particles(const wcg_ctx* ctx);
 
+/* ---- state I/O in the reference's file formats ---- */
+/* TwoDSceneSerializer::serializePositionOnly (App/TwoDSceneSerializer.cpp:161):
+ * binary, int byte count + m_x (x, y, z, twist = 0 per particle, doubles,
+ * original particle order) + int byte count (0: no cloth Gauss points). */
+int wcg_save_positions(wcg_ctx* ctx, const char* path);
+/* TwoDSceneSerializer::loadPosOnly (App/TwoDSceneSerializer.cpp:172): replaces
+ * the particle positions; the file's particle count must match.  Call
+ * wcg_rebucketize_and_resample (or wcg_step) afterwards. */
+int wcg_load_positions(wcg_ctx* ctx, const char* path);
+/* The fluid OBJ of TwoDSceneSerializer (App/TwoDSceneSerializer.cpp:40-47,
+ * updateFluid :242): one "v x y z radius" line per particle, 8 digits. */
+int wcg_write_fluid_obj(wcg_ctx* ctx, const char* path);
+
 /* ---- the reference call sequence (WetClothCore::stepSystem order) ---- */
 /* updateParticleBoundingBox + rebucketizeParticles + resampleNodes
  * (TwoDScene.cpp:1588, :1657, :5069): grid, particle sort, bucket activation */

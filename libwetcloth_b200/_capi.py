@@ -76,6 +76,9 @@ SIGNATURES = {
     "wcg_download_liquid_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p,
                                                   ctypes.c_void_p, ctypes.c_void_p]),
     "wcg_num_particles": (ctypes.c_longlong, [ctypes.c_void_p]),
+    "wcg_save_positions": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
+    "wcg_load_positions": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
+    "wcg_write_fluid_obj": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
     "wcg_rebucketize_and_resample": (ctypes.c_int, [ctypes.c_void_p]),
     "wcg_map_particle_nodes": (ctypes.c_int, [ctypes.c_void_p]),
     "wcg_step_velocity": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),

@@ -1,5 +1,6 @@
 // extern "C" surface of libwcgpu (declared in include/wetcloth_gpu.h).
 #include <cuda_runtime.h>
+#include <fstream>
 
 #include <algorithm>
 #include <cmath>
@@ -264,6 +265,72 @@ int wcg_download_liquid_device(wcg_ctx* ctx, double* x3, double* v3, double* C9)
 }
 
 long long wcg_num_particles(const wcg_ctx* ctx) { return ctx ? ctx->c.np : -1; }
+
+// ---- state I/O in the reference's file formats ------------------------------
+// TwoDSceneSerializer::serializePositionOnly / serialize_pos_subprog
+// (App/TwoDSceneSerializer.cpp:20-32, :161-170): an int byte count and m_x
+// (x, y, z, twist per particle, doubles), then an int byte count and the
+// Gauss-point matrix of the cloth (empty here).
+int wcg_save_positions(wcg_ctx* ctx, const char* path) {
+  WCG_CHECK_CTX(ctx);
+  if (!path) return fail(WCG_ERR_ARG, "null path");
+  const long long n = ctx->c.np;
+  if (n * 4 * (long long)sizeof(double) > 2147483647ll)
+    return fail(WCG_ERR_ARG, "too many particles for the position file's int byte count");
+  std::vector<double> x4((size_t)n * 4);
+  if (n > 0) WCG_CALL(ctx, wcg::download_positions(ctx->c, x4.data(), nullptr), "save positions");
+  std::ofstream f(path, std::ios::binary);
+  if (!f) return fail(WCG_ERR_ARG, std::string("cannot open ") + path);
+  const int bytes = (int)(n * 4 * sizeof(double));
+  const int gauss_bytes = 0;
+  f.write((const char*)&bytes, sizeof(int));
+  f.write((const char*)x4.data(), bytes);
+  f.write((const char*)&gauss_bytes, sizeof(int));
+  if (!f) return fail(WCG_ERR_ARG, std::string("write failed: ") + path);
+  return WCG_OK;
+}
+
+// TwoDSceneSerializer::loadPosOnly (App/TwoDSceneSerializer.cpp:172-182): the
+// particle count of the file must equal the context's.
+int wcg_load_positions(wcg_ctx* ctx, const char* path) {
+  WCG_CHECK_CTX(ctx);
+  if (!path) return fail(WCG_ERR_ARG, "null path");
+  std::ifstream f(path, std::ios::binary);
+  if (!f) return fail(WCG_ERR_ARG, std::string("cannot open ") + path);
+  int bytes = -1;
+  f.read((char*)&bytes, sizeof(int));
+  const long long n = ctx->c.np;
+  if (!f || bytes != n * 4 * (long long)sizeof(double))
+    return fail(WCG_ERR_ARG, "position file holds " + std::to_string(bytes) +
+                                 " bytes, the scene needs " +
+                                 std::to_string(n * 4 * (long long)sizeof(double)));
+  std::vector<double> x4((size_t)n * 4);
+  f.read((char*)x4.data(), bytes);
+  int gauss_bytes = 0;
+  f.read((char*)&gauss_bytes, sizeof(int));
+  if (!f) return fail(WCG_ERR_ARG, std::string("truncated position file: ") + path);
+  for (double v : x4)
+    if (!std::isfinite(v)) return fail(WCG_ERR_ARG, "non-finite position in file");
+  if (n > 0) WCG_CALL(ctx, wcg::upload_positions(ctx->c, x4.data()), "load positions");
+  return WCG_OK;
+}
+
+// The fluid OBJ of serialize_subprog (App/TwoDSceneSerializer.cpp:40-47;
+// updateFluid :242-255): "v x y z r" per fluid particle, 8 significant digits.
+int wcg_write_fluid_obj(wcg_ctx* ctx, const char* path) {
+  WCG_CHECK_CTX(ctx);
+  if (!path) return fail(WCG_ERR_ARG, "null path");
+  const long long n = ctx->c.np;
+  std::vector<double> x4((size_t)n * 4), r((size_t)n);
+  if (n > 0) WCG_CALL(ctx, wcg::download_positions(ctx->c, x4.data(), r.data()), "fluid obj");
+  FILE* f = fopen(path, "w");
+  if (!f) return fail(WCG_ERR_ARG, std::string("cannot open ") + path);
+  for (long long i = 0; i < n; ++i)
+    fprintf(f, "v %.8g %.8g %.8g %.8g\n", x4[i * 4], x4[i * 4 + 1], x4[i * 4 + 2], r[i]);
+  const bool ok = fclose(f) == 0;
+  if (!ok) return fail(WCG_ERR_ARG, std::string("write failed: ") + path);
+  return WCG_OK;
+}
 
 int wcg_rebucketize_and_resample(wcg_ctx* ctx) {
   WCG_CHECK_CTX(ctx);

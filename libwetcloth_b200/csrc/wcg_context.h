@@ -237,6 +237,10 @@ cudaError_t upload_particles(Context& c, long long n, const double* x3,
                              const double* radius, bool device_ptrs);
 cudaError_t download_particles(Context& c, double* x3, double* v3, double* C9,
                                bool device_ptrs);
+// positions in the reference's m_x layout (x, y, z, 0 per particle) and radii,
+// original order, host buffers
+cudaError_t download_positions(Context& c, double* x4, double* radius);
+cudaError_t upload_positions(Context& c, const double* x4);
 
 // reference call sequence
 cudaError_t build_grid(Context& c);                 // bbox + rebucketize + resampleNodes

@@ -116,19 +116,43 @@ __global__ void k_load_particles(long long n, long long pcap, const double* x3,
   pid[i] = (int)i;
 }
 
-// scatter sorted state back to original particle order (x3, v3, C9 AoS)
+// scatter sorted state back to original particle order: x3 at out[0, 3n),
+// v3 at out[3n, 6n), C9 at out[6n, 15n), each in the caller's layout so the
+// copies out are contiguous
 template <typename R>
 __global__ void k_store_particles(long long n, long long pcap, const R* P,
                                   const int* pid, double* out) {
   const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   const long long i = pid[s];
-  double* o = out + i * 15;
   for (int a = 0; a < 3; ++a) {
-    o[a] = (double)P[(PX + a) * pcap + s];
-    o[3 + a] = (double)P[(VX + a) * pcap + s];
+    out[i * 3 + a] = (double)P[(PX + a) * pcap + s];
+    out[3 * n + i * 3 + a] = (double)P[(VX + a) * pcap + s];
   }
-  for (int q = 0; q < 9; ++q) o[6 + q] = (double)P[(C00 + q) * pcap + s];
+  for (int q = 0; q < 9; ++q) out[6 * n + i * 9 + q] = (double)P[(C00 + q) * pcap + s];
+}
+
+// positions in the reference's m_x layout (x, y, z, twist = 0 per particle) and
+// radii, original particle order
+template <typename R>
+__global__ void k_store_positions(long long n, long long pcap, const R* P, const int* pid,
+                                  double* x4, double* rad) {
+  const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const long long i = pid[s];
+  for (int a = 0; a < 3; ++a) x4[i * 4 + a] = (double)P[(PX + a) * pcap + s];
+  x4[i * 4 + 3] = 0.0;
+  rad[i] = (double)P[PR * pcap + s];
+}
+
+// replace positions (reference m_x layout, original order) of the sorted state
+template <typename R>
+__global__ void k_set_positions(long long n, long long pcap, R* P, const int* pid,
+                                const double* x4) {
+  const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const long long i = pid[s];
+  for (int a = 0; a < 3; ++a) P[(PX + a) * pcap + s] = (R)x4[i * 4 + a];
 }
 
 cudaError_t upload_particles(Context& c, long long n, const double* x3,
@@ -207,16 +231,47 @@ cudaError_t download_particles(Context& c, double* x3, double* v3, double* C9,
   WCG_TRY(cudaGetLastError());
   const cudaMemcpyKind kind =
       device_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
-  // AoS 15-wide -> three strided copies
   if (x3)
-    WCG_TRY(cudaMemcpy2DAsync(x3, 3 * sizeof(double), st, 15 * sizeof(double),
-                              3 * sizeof(double), n, kind, c.stream));
+    WCG_TRY(cudaMemcpyAsync(x3, st, n * 3 * sizeof(double), kind, c.stream));
   if (v3)
-    WCG_TRY(cudaMemcpy2DAsync(v3, 3 * sizeof(double), st + 3, 15 * sizeof(double),
-                              3 * sizeof(double), n, kind, c.stream));
+    WCG_TRY(cudaMemcpyAsync(v3, st + 3 * n, n * 3 * sizeof(double), kind, c.stream));
   if (C9)
-    WCG_TRY(cudaMemcpy2DAsync(C9, 9 * sizeof(double), st + 6, 15 * sizeof(double),
-                              9 * sizeof(double), n, kind, c.stream));
+    WCG_TRY(cudaMemcpyAsync(C9, st + 6 * n, n * 9 * sizeof(double), kind, c.stream));
+  return cudaStreamSynchronize(c.stream);
+}
+
+cudaError_t download_positions(Context& c, double* x4, double* radius) {
+  const long long n = c.np;
+  if (n == 0) return cudaSuccess;
+  double* st = c.hostorder.as<double>();
+  if (c.prm.precision == 0)
+    ++c.launches, k_store_positions<double><<<nblk(n, 256), 256, 0, c.stream>>>(
+        n, c.pcap, c.pbuf[c.cur].as<double>(), c.pid[c.cur].as<int>(), st, st + 4 * n);
+  else
+    ++c.launches, k_store_positions<float><<<nblk(n, 256), 256, 0, c.stream>>>(
+        n, c.pcap, c.pbuf[c.cur].as<float>(), c.pid[c.cur].as<int>(), st, st + 4 * n);
+  WCG_TRY(cudaGetLastError());
+  WCG_TRY(cudaMemcpyAsync(x4, st, n * 4 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  if (radius)
+    WCG_TRY(cudaMemcpyAsync(radius, st + 4 * n, n * sizeof(double), cudaMemcpyDeviceToHost,
+                            c.stream));
+  return cudaStreamSynchronize(c.stream);
+}
+
+cudaError_t upload_positions(Context& c, const double* x4) {
+  const long long n = c.np;
+  if (n == 0) return cudaSuccess;
+  double* st = c.hostorder.as<double>();
+  WCG_TRY(cudaMemcpyAsync(st, x4, n * 4 * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+  if (c.prm.precision == 0)
+    ++c.launches, k_set_positions<double><<<nblk(n, 256), 256, 0, c.stream>>>(
+        n, c.pcap, c.pbuf[c.cur].as<double>(), c.pid[c.cur].as<int>(), st);
+  else
+    ++c.launches, k_set_positions<float><<<nblk(n, 256), 256, 0, c.stream>>>(
+        n, c.pcap, c.pbuf[c.cur].as<float>(), c.pid[c.cur].as<int>(), st);
+  WCG_TRY(cudaGetLastError());
+  // positions changed: the grid of the old positions no longer applies
+  c.have_grid = false;
   return cudaStreamSynchronize(c.stream);
 }
 

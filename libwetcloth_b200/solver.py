@@ -8,6 +8,7 @@ libwcgpu.so on the GPU.
 from __future__ import annotations
 
 import ctypes
+import os
 
 import numpy as np
 
@@ -83,6 +84,19 @@ class FluidScene:
         C = np.empty((n, 9))
         check(self.L.wcg_download_liquid(self.h, _dp(x), _dp(v), _dp(C)))
         return x, v, C
+
+    # ---- state I/O (TwoDSceneSerializer formats) ----
+    def save_positions(self, path):
+        """serializePositionOnly's binary position file."""
+        check(self.L.wcg_save_positions(self.h, os.fsencode(path)))
+
+    def load_positions(self, path):
+        """loadPosOnly: replace the positions from a position file."""
+        check(self.L.wcg_load_positions(self.h, os.fsencode(path)))
+
+    def write_fluid_obj(self, path):
+        """The fluid OBJ dump: "v x y z radius" per particle."""
+        check(self.L.wcg_write_fluid_obj(self.h, os.fsencode(path)))
 
     # ---- reference call sequence ----
     def rebucketize_and_resample(self):
