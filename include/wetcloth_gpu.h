@@ -60,6 +60,8 @@ typedef struct wcg_params {
   double refine_inner_tol;         /* FP32 inner-solve relative tolerance (0: aim at criterion) */
   int max_refinements;             /* FP64 refinement sweeps (0: 20) */
   int solver;                      /* WCG_SOLVER_MIC0 or WCG_SOLVER_MG */
+  double viscosity;                /* LiquidInfo::viscosity; 0: no viscosity */
+  int viscosity_substeps;          /* explicit viscosity sub-steps (0: 1) */
 } wcg_params;
 
 typedef struct wcg_ctx wcg_ctx;
@@ -123,7 +125,9 @@ int wcg_rebucketize_and_resample(wcg_ctx* ctx);
  * :5952, :5933) */
 int wcg_map_particle_nodes(wcg_ctx* ctx);
 /* LinearizedImplicitEuler::stepVelocity (+acceptVelocity of u*),
- * LinearizedImplicitEuler.cpp:224 */
+ * LinearizedImplicitEuler.cpp:224, with the explicit viscosity sub-steps of
+ * :272-306 (viscosity::applyNodeViscosityExplicit, Viscosity.cpp:1780) when
+ * wcg_params.viscosity > 0 */
 int wcg_step_velocity(wcg_ctx* ctx, double dt);
 /* LinearizedImplicitEuler::projectFine -> pressure::solveNodePressure
  * (Pressure.cpp:285) with MIC(0)-PCG */

@@ -46,6 +46,8 @@ class WcgParams(ctypes.Structure):
         ("refine_inner_tol", ctypes.c_double),
         ("max_refinements", ctypes.c_int),
         ("solver", ctypes.c_int),
+        ("viscosity", ctypes.c_double),
+        ("viscosity_substeps", ctypes.c_int),
     ]
 
 

@@ -95,6 +95,8 @@ const FieldName kFields[] = {
     {"pressure", wcg::G_PRESSURE}, {"A_diag", wcg::G_ADIAG},
     {"A_x", wcg::G_AX}, {"A_y", wcg::G_AY}, {"A_z", wcg::G_AZ},
     {"b_dense", wcg::G_B}, {"mic_invdiag", wcg::G_INVDIAG},
+    {"liquid_c_vf", wcg::G_VFC}, {"liquid_ex_vf", wcg::G_VFEX},
+    {"liquid_ey_vf", wcg::G_VFEY}, {"liquid_ez_vf", wcg::G_VFEZ},
 };
 
 int lookup_field(const char* name) {
@@ -164,6 +166,8 @@ void wcg_default_params(wcg_params* p) {
   p->refine_inner_tol = 0.0;
   p->max_refinements = 20;
   p->solver = WCG_SOLVER_MIC0;
+  p->viscosity = 0.0;
+  p->viscosity_substeps = 1;
 }
 
 int wcg_create(const wcg_params* params, wcg_ctx** out) {
@@ -196,6 +200,10 @@ int wcg_create(const wcg_params* params, wcg_ctx** out) {
   if (params->solver != WCG_SOLVER_MIC0 && params->solver != WCG_SOLVER_MG)
     return fail(WCG_ERR_ARG, "solver must be WCG_SOLVER_MIC0 or WCG_SOLVER_MG");
   p.solver = params->solver;
+  if (!(params->viscosity >= 0.0) || !std::isfinite(params->viscosity))
+    return fail(WCG_ERR_ARG, "viscosity must be finite and >= 0");
+  p.viscosity = params->viscosity;
+  p.viscosity_substeps = params->viscosity_substeps > 0 ? params->viscosity_substeps : 1;
   // wavefront tile shape (performance knob; both compute identical results)
   if (const char* v = getenv("WCG_SWEEP_TILE")) ctx->c.sweep_variant = !strcmp(v, "warp") ? 1 : 0;
   // layout of the pressure solve (performance knob; same arithmetic)

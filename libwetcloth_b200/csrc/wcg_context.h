@@ -29,6 +29,8 @@ struct Params {
   double refine_inner_tol;  // relative tolerance of each FP32 inner solve
   int max_refinements;
   int solver;     // 0: MIC(0)-PCG, 1: multigrid-PCG (AMGPCGSolveSparse)
+  double viscosity;        // LiquidInfo::viscosity (0: compute_viscosity off)
+  int viscosity_substeps;  // explicit viscosity sub-steps per step_velocity
 };
 
 // A device allocation that grows and never shrinks.
@@ -92,7 +94,11 @@ enum GField : int {
   G_SX = 50,           // MIC(0) scaled couplings S_a = A_a * invdiag
   G_SY = 51,
   G_SZ = 52,
-  kNumGFields = 53
+  G_VFC = 53,          // liquid volume fraction at cell centres (viscosity)
+  G_VFEX = 54,         // ... at x-, y-, z-edge nodes
+  G_VFEY = 55,
+  G_VFEZ = 56,
+  kNumGFields = 57
 };
 
 // Geometry of the pencil layout of one pressure solve (wcg_pencil.cuh).

@@ -13,6 +13,7 @@
 #include "wcg_wsweep.cuh"
 #include "wcg_pencil.cuh"
 #include "wcg_mg.cuh"
+#include "wcg_visc.cuh"
 #include "wcg_scan.cuh"
 
 namespace wcg {
@@ -533,6 +534,10 @@ static cudaError_t map_particles_to_grid_t(Context& c) {
       c.pcap, c.cell_start.as<int>(), c.pdelta.as<int>() + c.cur * c.pcap, dr, F, c.gcap, w);
   ++c.launches, k_solid_weights<R><<<(unsigned)c.n_active, 192, 0, c.stream>>>(
       c.g, c.active_list.as<int>(), c.active.as<unsigned char>(), F, c.gcap, w);
+  // liquid volume fractions for the viscosity (updateLiquidPhi :3353-3367)
+  if (c.prm.viscosity > 0.0)
+    ++c.launches, k_volume_fractions<R><<<(unsigned)c.n_active, 64, 0, c.stream>>>(
+        c.g, c.active_list.as<int>(), c.active.as<unsigned char>(), F, c.gcap);
   return cudaGetLastError();
 }
 
@@ -548,6 +553,22 @@ static cudaError_t step_velocity_t(Context& c, double dt) {
   ++c.launches, k_predict<R><<<(unsigned)c.n_active, 192, 0, c.stream>>>(
       c.g, c.active_list.as<int>(), c.gfield.as<R>(), c.gcap, (R)c.prm.gravity[0],
       (R)c.prm.gravity[1], (R)c.prm.gravity[2], (R)dt);
+  // explicit viscosity sub-steps, then rhs = v * m (stepVelocity :272-306)
+  if (c.prm.viscosity > 0.0) {
+    R* F = c.gfield.as<R>();
+    const int ns = c.prm.viscosity_substeps > 0 ? c.prm.viscosity_substeps : 1;
+    const double sub_dt = dt / (double)ns;
+    const double dx = c.prm.dx;
+    const R factor = (R)(sub_dt / (dx * dx) * c.prm.viscosity / c.prm.liquid_density);
+    for (int it = 0; it < ns; ++it) {
+      WCG_TRY(cudaMemcpyAsync(F + G_UTMP * c.gcap, F + G_VSTAR * c.gcap,
+                              3 * c.gcap * sizeof(R), cudaMemcpyDeviceToDevice, c.stream));
+      ++c.launches, k_viscosity_explicit<R><<<(unsigned)c.n_active, 192, 0, c.stream>>>(
+          c.g, c.active_list.as<int>(), c.active.as<unsigned char>(), F, c.gcap, factor);
+    }
+    ++c.launches, k_rhs_from_vstar<R><<<(unsigned)c.n_active, 192, 0, c.stream>>>(
+        c.active_list.as<int>(), F, c.gcap);
+  }
   return cudaGetLastError();
 }
 

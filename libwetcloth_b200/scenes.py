@@ -32,6 +32,8 @@ class SceneParams:
     box_radius: float = 0.0
     criterion: float = 1e-6
     maxiters: int = 1000
+    viscosity: float = 0.0        # LiquidInfo::viscosity; 0 = compute_viscosity off
+    viscosity_substeps: int = 1   # LinearizedImplicitEuler viscosity sub-steps
 
 
 def particle_radius(dx: float, ppc: int) -> float:

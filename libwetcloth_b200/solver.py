@@ -36,6 +36,8 @@ def make_params(p, precision=_capi.WCG_FP64, refine_inner_tol=0.0,
     prm.refine_inner_tol = refine_inner_tol
     prm.max_refinements = max_refinements
     prm.solver = solver
+    prm.viscosity = getattr(p, "viscosity", 0.0)
+    prm.viscosity_substeps = getattr(p, "viscosity_substeps", 1)
     return prm
 
 

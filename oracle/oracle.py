@@ -32,6 +32,7 @@ def lib():
                                  ctypes.c_double, _D, _D, ctypes.c_double, ctypes.c_double,
                                  ctypes.c_int, ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _D, _D]
         L.wco_destroy.argtypes = [ctypes.c_void_p]
+        L.wco_set_viscosity.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
         L.wco_step.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
         L.wco_step.restype = ctypes.c_int
         L.wco_substep.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
@@ -71,6 +72,9 @@ class OracleScene:
                               arr(scene.x), arr(scene.v), C, arr(scene.mass), arr(scene.vol),
                               arr(scene.radius))
         self.L = L
+        mu = getattr(p, "viscosity", 0.0)
+        if mu > 0.0:
+            L.wco_set_viscosity(self.h, mu, getattr(p, "viscosity_substeps", 1))
 
     def close(self):
         if self.h:

@@ -48,6 +48,7 @@ def _lib(omp: bool):
                                          ctypes.POINTER(ctypes.c_int), _D]
         L.wcref_timers.argtypes = [ctypes.c_void_p, _D]
         L.wcref_amg_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), _D]
+        L.wcref_set_viscosity.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
         _libs[omp] = L
     return _libs[omp]
 
@@ -76,6 +77,9 @@ class RefScene:
             p.box_radius, p.criterion, p.maxiters, 1 if mic else 0,
             scene.x.shape[0], arr(scene.x.reshape(-1)), arr(scene.v.reshape(-1)),
             C, arr(scene.mass), arr(scene.vol), arr(scene.radius))
+        mu = getattr(p, "viscosity", 0.0)
+        if mu > 0.0:
+            self.L.wcref_set_viscosity(self.h, mu, getattr(p, "viscosity_substeps", 1))
 
     def close(self):
         if self.h:

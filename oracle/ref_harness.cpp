@@ -223,6 +223,12 @@ void snap_p2g(Harness& h) {
   dense(h, "psi_p", s.m_node_psi_p);
   dense(h, "pore_pressure_p", s.m_node_pore_pressure_p);
   dense(h, "liquid_phi", s.m_node_liquid_phi);
+  if (s.getLiquidInfo().compute_viscosity) {
+    dense(h, "liquid_c_vf", s.m_node_liquid_c_vf);
+    dense(h, "liquid_ex_vf", s.m_node_liquid_ex_vf);
+    dense(h, "liquid_ey_vf", s.m_node_liquid_ey_vf);
+    dense(h, "liquid_ez_vf", s.m_node_liquid_ez_vf);
+  }
   dense(h, "solid_phi", s.m_node_solid_phi);
   dense(h, "solid_weight_x", s.m_node_solid_weight_x);
   dense(h, "solid_weight_y", s.m_node_solid_weight_y);
@@ -591,6 +597,21 @@ void wcref_solver_stats(void* hp, int* iters_mic, double* res_mic) {
   Harness* h = (Harness*)hp;
   *iters_mic = h->last_iters_mic;
   *res_mic = h->last_res_mic;
+}
+
+// explicit liquid viscosity: LiquidInfo::compute_viscosity on, implicit off,
+// viscosity mu, LinearizedImplicitEuler's viscosity sub-steps (call before
+// the first step; mu = 0 turns it off)
+void wcref_set_viscosity(void* hp, double mu, int substeps) {
+  Harness* h = (Harness*)hp;
+  LiquidInfo& li = h->scene->getLiquidInfo();
+  li.compute_viscosity = mu > 0.0;
+  li.implicit_viscosity = false;
+  li.viscosity = mu;
+  // the sub-step count is a constructor argument of the stepper
+  h->stepper = std::make_shared<LinearizedImplicitEuler>(
+      1e-6, h->p.criterion, 1e-6, 1e-6, h->p.maxiters, 1, substeps > 0 ? substeps : 1, 1);
+  h->stepper->setUseApic(true);
 }
 
 // AMGPCGSolveSparse iterations and residual of the last snapshot step

@@ -26,6 +26,8 @@
 typedef struct {
   double dx, g[3], rho, flip, friction, bc[3], bh[3], br, criterion;
   int maxiters, mic;
+  double visc;       /* LiquidInfo::viscosity; 0: compute_viscosity off */
+  int visc_substeps; /* LinearizedImplicitEuler::m_viscosity_substeps */
 } Params;
 
 typedef struct {
@@ -61,6 +63,7 @@ typedef struct {
   /* node fields */
   double *mass[3], *vel[3], *vol_f[3], *sat[3], *psi[3], *wgt[3], *svel[3];
   double *sat_p, *psi_p, *pore_p, *lphi, *sphi, *pressure;
+  double *vf_c, *vf_e[3];  /* liquid volume fractions: cell centres, x/y/z edges */
   double *rhs[3], *vstar[3], *invC[3], *psifs[3], *psisf[3], *mshdvm[3], *mfhdvm[3];
   unsigned char* valid[3];
   /* pressure system */
@@ -617,6 +620,181 @@ static void sat_psi_p(Scene* s) {
  * constructHDV (:846-965, no drag), constructInvMDV (:1109-1148),
  * performLocalSolve (:128-170), acceptVelocity (:2176-2212),
  * constructPsiSF (:1052-1107). */
+/* ---- explicit viscosity ------------------------------------------------ */
+/* mathutils::sort of four values (MathUtilities.h:959-965) */
+static void sort4(double* a, double* b, double* c, double* d) {
+  double t;
+#define SWP(u, v) if (*u > *v) { t = *u; *u = *v; *v = t; }
+  SWP(a, b) SWP(c, d) SWP(a, c) SWP(b, d) SWP(b, c)
+#undef SWP
+}
+
+/* volume_fraction of a tetrahedron (VolumeFractions.cpp:101-127): the
+ * fraction with phi <= 0 by the sorted tet/prism cases */
+static double vf_tet(double p0, double p1, double p2, double p3) {
+  sort4(&p0, &p1, &p2, &p3);
+  if (p3 <= 0) return 1;
+  if (p2 <= 0) return 1 - p3 * p3 * p3 / ((p3 - p2) * (p3 - p1) * (p3 - p0));
+  if (p1 <= 0) {
+    const double a = p0 / (p0 - p2), b = p0 / (p0 - p3), c = p1 / (p1 - p3), d = p1 / (p1 - p2);
+    return a * b * (1 - d) + b * (1 - c) * d + c * d;
+  }
+  if (p0 <= 0) return p0 * p0 * p0 / ((p0 - p1) * (p0 - p2) * (p0 - p3));
+  return 0;
+}
+
+/* volume_fraction of a cube from its corner values, as twelve tetrahedra
+ * (two of them counted twice) (VolumeFractions.cpp:129-162) */
+static double vf_cube(double p000, double p100, double p010, double p110, double p001,
+                      double p101, double p011, double p111) {
+  return (vf_tet(p000, p001, p101, p011) + vf_tet(p000, p101, p100, p110) +
+          vf_tet(p000, p010, p011, p110) + vf_tet(p101, p011, p111, p110) +
+          2 * vf_tet(p000, p011, p101, p110) + vf_tet(p100, p101, p001, p111) +
+          vf_tet(p100, p001, p000, p010) + vf_tet(p100, p110, p111, p010) +
+          vf_tet(p001, p111, p011, p010) + 2 * vf_tet(p100, p111, p001, p010)) /
+         12;
+}
+
+/* TwoDScene::interpolateValue (TwoDScene.cpp:3586-3621) of the cell-centred
+ * liquid phi, default dx outside the grid or in inactive buckets */
+static double interp_lphi(const Scene* s, const double* pos) {
+  const double dx = s->p.dx;
+  double bp[3], fr[3], buf[8];
+  int bi[3];
+  for (int a = 0; a < 3; ++a) {
+    const double ori = s->org[a] + 0.5 * dx;
+    bp[a] = (pos[a] - ori) / dx;
+    bi[a] = (int)floor(bp[a]);
+  }
+  for (int t = 0; t < 2; ++t)
+    for (int u = 0; u < 2; ++u)
+      for (int r = 0; r < 2; ++r) {
+        const int q[3] = {bi[0] + r, bi[1] + u, bi[2] + t};
+        const int h[3] = {q[0] / NN, q[1] / NN, q[2] / NN};
+        double v = dx;
+        if (h[0] >= 0 && h[0] < s->ni && h[1] >= 0 && h[1] < s->nj && h[2] >= 0 && h[2] < s->nk) {
+          const long long b = bucket_index(s, h[0], h[1], h[2]);
+          if (s->act[b]) {
+            const int l = (q[2] - h[2] * NN) * NN * NN + (q[1] - h[1] * NN) * NN + (q[0] - h[0] * NN);
+            v = s->lphi[b * NPB + l];
+          }
+        }
+        buf[t * 4 + u * 2 + r] = v;
+      }
+  for (int a = 0; a < 3; ++a) fr[a] = bp[a] - (double)bi[a];
+#define LERP(v0, v1, f) ((1 - (f)) * (v0) + (f) * (v1))
+  const double b0 = LERP(LERP(buf[0], buf[1], fr[0]), LERP(buf[2], buf[3], fr[0]), fr[1]);
+  const double b1 = LERP(LERP(buf[4], buf[5], fr[0]), LERP(buf[6], buf[7], fr[0]), fr[1]);
+  return LERP(b0, b1, fr[2]);
+#undef LERP
+}
+
+/* TwoDScene::estimateVolumeFractions (TwoDScene.cpp:3535-3584) for the node
+ * offsets of updateLiquidPhi (:3353-3367).  The reference adds the offset to
+ * the node position in world units, not cells, and so does this. */
+static void volume_fractions(Scene* s) {
+  const double dx = s->p.dx;
+  const double offs[4][3] = {{0.5, 0.5, 0.5}, {0.5, 0.0, 0.0}, {0.0, 0.5, 0.0}, {0.0, 0.0, 0.5}};
+  double* out[4] = {s->vf_c, s->vf_e[0], s->vf_e[1], s->vf_e[2]};
+  for (long long n = 0; n < s->nnode; ++n) {
+    for (int f = 0; f < 4; ++f) out[f][n] = 0.0;
+    if (!s->act[n >> 6]) continue;
+    int I, J, K;
+    node_ijk(s, n, &I, &J, &K);
+    const double corner[3] = {node_coord(s, 0, I, 0.0), node_coord(s, 1, J, 0.0),
+                              node_coord(s, 2, K, 0.0)};
+    const double o = 0.5 * dx;
+    for (int f = 0; f < 4; ++f) {
+      const double c[3] = {corner[0] + offs[f][0], corner[1] + offs[f][1], corner[2] + offs[f][2]};
+      double ph[8];
+      for (int z = 0; z < 2; ++z)
+        for (int y = 0; y < 2; ++y)
+          for (int x = 0; x < 2; ++x) {
+            const double pos[3] = {c[0] + (x ? o : -o), c[1] + (y ? o : -o), c[2] + (z ? o : -o)};
+            ph[x * 4 + y * 2 + z] = interp_lphi(s, pos);
+          }
+      /* ph index x*4 + y*2 + z holds phi_xyz */
+      out[f][n] = vf_cube(ph[0], ph[4], ph[2], ph[6], ph[1], ph[5], ph[3], ph[7]);
+    }
+  }
+}
+
+/* viscosity::get_value (Viscosity.cpp:27-55): node value of a field at global
+ * node (I, J, K), default outside the grid or in an inactive bucket */
+static double vget(const Scene* s, const double* f, int I, int J, int K, double def) {
+  const long long n = node_of(s, I, J, K);
+  if (!node_active(s, n)) return def;
+  return f[n];
+}
+
+/* applyNodeViscosityExplicit (Viscosity.cpp:1780-2107): one explicit step of
+ * the liquid-volume-weighted viscous stress divergence on the face
+ * velocities, src -> dst, in the reference's order of terms. */
+static void viscosity_explicit(Scene* s, double* const* src, double* const* dst, double dt) {
+  const double dx = s->p.dx;
+  const double factor = dt / (dx * dx) * s->p.visc / s->p.rho;
+  const double* cvf = s->vf_c;
+  const double* const* evf = (const double* const*)s->vf_e;
+  for (long long n = 0; n < s->nnode; ++n) {
+    if (!s->act[n >> 6]) continue;
+    int I, J, K;
+    node_ijk(s, n, &I, &J, &K);
+    for (int a = 0; a < 3; ++a) {
+      /* axes: a (normal), and for the cross terms the reference's naming */
+      double v = src[a][n];
+      const double cv = v;
+#define VN(fld, di, dj, dk, def) vget(s, src[fld], I + (di), J + (dj), K + (dk), def)
+#define VF(arr, di, dj, dk) vget(s, arr, I + (di), J + (dj), K + (dk), 0.0)
+      if (a == 0) {
+        const double vol_left = VF(cvf, -1, 0, 0), vol_right = VF(cvf, 0, 0, 0);
+        const double vol_back = VF(evf[1], 0, 0, 0), vol_front = VF(evf[1], 0, 0, 1);
+        const double vol_bottom = VF(evf[2], 0, 0, 0), vol_top = VF(evf[2], 0, 1, 0);
+        v += 2.0 * factor * vol_right * (VN(0, 1, 0, 0, cv) - cv);
+        v += 2.0 * factor * vol_left * (VN(0, -1, 0, 0, cv) - cv);
+        v += factor * vol_top * (VN(0, 0, 1, 0, cv) - cv);
+        v += factor * vol_bottom * (VN(0, 0, -1, 0, cv) - cv);
+        v += factor * vol_front * (VN(0, 0, 0, 1, cv) - cv);
+        v += factor * vol_back * (VN(0, 0, 0, -1, cv) - cv);
+        v += factor * vol_top * (VN(1, 0, 1, 0, 0.0) - VN(1, -1, 1, 0, 0.0));
+        v += factor * vol_bottom * (VN(1, -1, 0, 0, 0.0) - VN(1, 0, 0, 0, 0.0));
+        v += factor * vol_front * (VN(2, 0, 0, 1, 0.0) - VN(2, -1, 0, 1, 0.0));
+        v += factor * vol_back * (VN(2, -1, 0, 0, 0.0) - VN(2, 0, 0, 0, 0.0));
+      } else if (a == 1) {
+        const double vol_bottom = VF(cvf, 0, -1, 0), vol_top = VF(cvf, 0, 0, 0);
+        const double vol_back = VF(evf[0], 0, 0, 0), vol_front = VF(evf[0], 0, 0, 1);
+        const double vol_left = VF(evf[2], 0, 0, 0), vol_right = VF(evf[2], 1, 0, 0);
+        v += factor * vol_right * (VN(1, 1, 0, 0, cv) - cv);
+        v += factor * vol_left * (VN(1, -1, 0, 0, cv) - cv);
+        v += 2.0 * factor * vol_top * (VN(1, 0, 1, 0, cv) - cv);
+        v += 2.0 * factor * vol_bottom * (VN(1, 0, -1, 0, cv) - cv);
+        v += factor * vol_front * (VN(1, 0, 0, 1, cv) - cv);
+        v += factor * vol_back * (VN(1, 0, 0, -1, cv) - cv);
+        v += factor * vol_right * (VN(0, 1, 0, 0, 0.0) - VN(0, 1, -1, 0, 0.0));
+        v += factor * vol_left * (VN(0, 0, -1, 0, 0.0) - VN(0, 0, 0, 0, 0.0));
+        v += factor * vol_front * (VN(2, 0, 0, 1, 0.0) - VN(2, 0, -1, 1, 0.0));
+        v += factor * vol_back * (VN(2, 0, -1, 0, 0.0) - VN(2, 0, 0, 0, 0.0));
+      } else {
+        const double vol_back = VF(cvf, 0, 0, -1), vol_front = VF(cvf, 0, 0, 0);
+        const double vol_bottom = VF(evf[0], 0, 0, 0), vol_top = VF(evf[0], 0, 1, 0);
+        const double vol_left = VF(evf[1], 0, 0, 0), vol_right = VF(evf[1], 1, 0, 0);
+        v += factor * vol_right * (VN(2, 1, 0, 0, cv) - cv);
+        v += factor * vol_left * (VN(2, -1, 0, 0, cv) - cv);
+        v += factor * vol_top * (VN(2, 0, 1, 0, cv) - cv);
+        v += factor * vol_bottom * (VN(2, 0, -1, 0, cv) - cv);
+        v += 2.0 * factor * vol_front * (VN(2, 0, 0, 1, cv) - cv);
+        v += 2.0 * factor * vol_back * (VN(2, 0, 0, -1, cv) - cv);
+        v += factor * vol_right * (VN(0, 1, 0, 0, 0.0) - VN(0, 1, 0, -1, 0.0));
+        v += factor * vol_left * (VN(0, 0, 0, -1, 0.0) - VN(0, 0, 0, 0, 0.0));
+        v += factor * vol_top * (VN(1, 0, 1, 0, 0.0) - VN(1, 0, 1, -1, 0.0));
+        v += factor * vol_bottom * (VN(1, 0, 0, -1, 0.0) - VN(1, 0, 0, 0, 0.0));
+      }
+#undef VN
+#undef VF
+      dst[a][n] = v;
+    }
+  }
+}
+
 static void step_velocity(Scene* s, double dt) {
   for (int a = 0; a < 3; ++a)
     for (long long n = 0; n < s->nnode; ++n) {
@@ -650,6 +828,23 @@ static void step_velocity(Scene* s, double dt) {
       s->psifs[a][n] = ((1.0 - psi) * s->invC[a][n] + psi * invCs * s->mfhdvm[a][n]) * m;
       s->psisf[a][n] = (psi * invCs + (1.0 - psi) * s->invC[a][n] * s->mshdvm[a][n]) * 0.0;
     }
+  /* explicit viscosity sub-steps, then the rhs from the new velocity
+   * (LinearizedImplicitEuler::stepVelocity, LinearizedImplicitEuler.cpp:272-306) */
+  if (s->p.visc > 0.0) {
+    const int ns = s->p.visc_substeps > 0 ? s->p.visc_substeps : 1;
+    const double sub_dt = dt / (double)ns;
+    double* tmp[3];
+    for (int a = 0; a < 3; ++a) tmp[a] = (double*)malloc(sizeof(double) * (size_t)s->nnode);
+    for (int it = 0; it < ns; ++it) {
+      for (int a = 0; a < 3; ++a) memcpy(tmp[a], s->vstar[a], sizeof(double) * (size_t)s->nnode);
+      viscosity_explicit(s, tmp, s->vstar, sub_dt);
+    }
+    for (int a = 0; a < 3; ++a) {
+      free(tmp[a]);
+      for (long long n = 0; n < s->nnode; ++n)
+        if (s->act[n >> 6]) s->rhs[a][n] = s->vstar[a][n] * s->mass[a][n];
+    }
+  }
 }
 
 /* robertbridson::SparseMatrix::add_to_element (SparseMatrix.h:64-80) on a
@@ -1063,7 +1258,8 @@ static void alloc_nodes(Scene* s) {
     free(s->valid[a]);
     s->valid[a] = (unsigned char*)calloc(n, 1);
   }
-  double** G[] = {&s->sat_p, &s->psi_p, &s->pore_p, &s->lphi, &s->sphi, &s->pressure};
+  double** G[] = {&s->sat_p, &s->psi_p, &s->pore_p, &s->lphi, &s->sphi, &s->pressure,
+                  &s->vf_c, &s->vf_e[0], &s->vf_e[1], &s->vf_e[2]};
   for (size_t k = 0; k < sizeof(G) / sizeof(G[0]); ++k) {
     free(*G[k]);
     *G[k] = (double*)calloc(n, sizeof(double));
@@ -1118,6 +1314,7 @@ int wco_substep(Scene* s, double dt, int snapshot) {
   build_pairs(s, &s->pw, s->ww, 2);
   build_pairs(s, &s->pp, s->wp, 4);
   liquid_phi(s);
+  if (s->p.visc > 0.0) volume_fractions(s);
   solid_phi_and_weights(s);
   p2g(s);
   sat_psi_p(s);
@@ -1128,6 +1325,9 @@ int wco_substep(Scene* s, double dt, int snapshot) {
       snprintf(nm, sizeof nm, "mass_fluid_%c", xyz[a]); snap_node(s, nm, s->mass[a]);
       snprintf(nm, sizeof nm, "vel_fluid_%c", xyz[a]); snap_node(s, nm, s->vel[a]);
       snprintf(nm, sizeof nm, "vol_fluid_%c", xyz[a]); snap_node(s, nm, s->vol_f[a]);
+      if (s->p.visc > 0.0) {
+        snprintf(nm, sizeof nm, "liquid_e%c_vf", xyz[a]); snap_node(s, nm, s->vf_e[a]);
+      }
       snprintf(nm, sizeof nm, "sat_%c", xyz[a]); snap_node(s, nm, s->sat[a]);
       snprintf(nm, sizeof nm, "psi_%c", xyz[a]); snap_node(s, nm, s->psi[a]);
       snprintf(nm, sizeof nm, "solid_weight_%c", xyz[a]); snap_node(s, nm, s->wgt[a]);
@@ -1137,6 +1337,7 @@ int wco_substep(Scene* s, double dt, int snapshot) {
     snap_node(s, "psi_p", s->psi_p);
     snap_node(s, "pore_pressure_p", s->pore_p);
     snap_node(s, "liquid_phi", s->lphi);
+    if (s->p.visc > 0.0) snap_node(s, "liquid_c_vf", s->vf_c);
     snap_node(s, "solid_phi", s->sphi);
   }
   step_velocity(s, dt);
@@ -1232,6 +1433,13 @@ int wco_step(Scene* s, double dt, int snapshot) {
   const int n = wco_num_substeps(s, dt);
   for (int k = 0; k < n; ++k) wco_substep(s, dt / (double)n, snapshot);
   return n;
+}
+
+/* liquid viscosity (LiquidInfo::viscosity with compute_viscosity on, explicit)
+ * and LinearizedImplicitEuler's viscosity sub-steps; mu = 0 turns it off */
+void wco_set_viscosity(Scene* s, double mu, int substeps) {
+  s->p.visc = mu;
+  s->p.visc_substeps = substeps > 0 ? substeps : 1;
 }
 
 Scene* wco_create(double dx, const double* g, double rho, double flip, double friction,

@@ -77,3 +77,28 @@ def test_mic0_pcg_on_reference_matrix():
     for i in range(len(b)):
         Ax[i] = np.dot(val[rs[i]:rs[i + 1]], x[col[rs[i]:rs[i + 1]]])
     assert np.abs(b - Ax).max() <= sc.params.criterion * np.abs(b).max() * 1.0001
+
+
+VISC = ["liquid_c_vf", "liquid_ex_vf", "liquid_ey_vf", "liquid_ez_vf", "v_star_x",
+        "v_star_y", "v_star_z", "rhs_fluid_x", "rhs_fluid_z", "pressure", "g2p_v", "adv_x"]
+
+
+@pytest.mark.parametrize("kind,mu", [("dam16", 5.0), ("curl16", 8.9e-3), ("curl16", 5.0)])
+def test_explicit_viscosity_step(kind, mu):
+    """Explicit viscosity (estimateVolumeFractions + applyNodeViscosityExplicit,
+    two sub-steps): volume fractions, the viscous face velocities and the rest
+    of the step against the reference."""
+    sc = _scene(kind)
+    sc.params.viscosity = mu
+    sc.params.viscosity_substeps = 2
+    r = oref.RefScene(sc, mic=True)
+    o = oo.OracleScene(sc)
+    r.step(DT, snapshot=True)
+    o.step(DT, snapshot=True)
+    for k in VISC:
+        a, b = r.get(k), o.get(k)
+        m = ~np.isnan(a)
+        assert np.array_equal(m, ~np.isnan(b)), k
+        if m.any():
+            assert np.abs(a[m] - b[m]).max() <= 1e-12 * max(np.abs(a[m]).max(), 1e-300), k
+    assert (r.get("liquid_c_vf")[~np.isnan(r.get("liquid_c_vf"))] > 0).any()
