@@ -30,7 +30,9 @@ enum {
   WCG_ERR_CUDA = 2,       /* CUDA runtime error (message has the details) */
   WCG_ERR_NOT_CONVERGED = 3, /* pressure solve hit maxiters or rho was 0/NaN */
   WCG_ERR_DEVICE = 4,     /* a kernel recorded an error (wait limit, index) */
-  WCG_ERR_STATE = 5       /* call out of order (e.g. no grid built yet) */
+  WCG_ERR_STATE = 5,      /* call out of order (e.g. no grid built yet) */
+  WCG_ERR_UNSUPPORTED = 6 /* the call needs a part of the reference not built
+                             here (the elasto coupling of the solve) */
 };
 
 enum { WCG_FP64 = 0, WCG_FP32_REFINE = 1 };
@@ -62,6 +64,9 @@ typedef struct wcg_params {
   int solver;                      /* WCG_SOLVER_MIC0 or WCG_SOLVER_MG */
   double viscosity;                /* LiquidInfo::viscosity; 0: no viscosity */
   int viscosity_substeps;          /* explicit viscosity sub-steps (0: 1) */
+  double elasto_flip_coeff;        /* LiquidInfo::elasto_flip_coeff (0.95) */
+  double elasto_flip_asym_coeff;   /* LiquidInfo::elasto_flip_asym_coeff (1.0) */
+  double elasto_advect_coeff;      /* LiquidInfo::elasto_advect_coeff (1.0) */
 } wcg_params;
 
 typedef struct wcg_ctx wcg_ctx;
@@ -101,6 +106,26 @@ int wcg_download_liquid(wcg_ctx* ctx, double* x3, double* v3, double* C9);
 int wcg_download_liquid_device(wcg_ctx* ctx, double* x3, double* v3,
                                double* C9);
 long long wcg_num_particles(const wcg_ctx* ctx);
+
+/* Elasto (cloth / yarn) particles, the reference's particles [0, n) ahead of
+ * the liquid ones (TwoDScene::isFluid, TwoDScene.cpp:6921;
+ * getNumElastoParticles :5212).  Arrays in the reference's layouts: x4/v4 =
+ * m_x/m_v (x, y, z, twist; 4n), B9 = m_B rows (9n row-major), m4/fm4 = m_m and
+ * m_fluid_m (4n; P2G adds the first three componentwise), m_rest_vol,
+ * m_rest_volume_fraction, m_fluid_vol, m_shape_factor (n each), m_orientation
+ * (3n), surfel (n; nonzero where m_particle_to_surfel >= 0).  Host pointers.
+ * They take part in the grid build, the transfers (mapParticleNodesAPIC
+ * :6609-6919, mapParticleSaturationPsiNodes :5952, updatePorePressureNodes
+ * :5933, mapNodeParticlesAPIC :6936-7090) and advection (SceneStepper.cpp:17);
+ * the solve calls return WCG_ERR_UNSUPPORTED while any are present. */
+int wcg_upload_elasto(wcg_ctx* ctx, long long n, const double* x4, const double* v4,
+                      const double* B9, const double* m4, const double* fm4,
+                      const double* rest_vol, const double* rest_vf,
+                      const double* fluid_vol, const double* shape_factor,
+                      const double* orient3, const int* surfel);
+/* Elasto state (m_x, m_v with twists; m_B rows) in the original order. */
+int wcg_download_elasto(wcg_ctx* ctx, double* x4, double* v4, double* B9);
+long long wcg_num_elasto(const wcg_ctx* ctx);
 
 /* ---- state I/O in the reference's file formats ---- */
 /* TwoDSceneSerializer::serializePositionOnly (App/TwoDSceneSerializer.cpp:161):
@@ -154,8 +179,15 @@ int wcg_get_stats(const wcg_ctx* ctx, wcg_stats* out);
 int wcg_grid_info(const wcg_ctx* ctx, int* dims, double* origin, double* bbx);
 /* number of values of a named field (-1 if unknown) */
 long long wcg_field_size(wcg_ctx* ctx, const char* name);
-/* double field by name, nb*64 values, NaN in inactive buckets */
+/* double field by name, nb*64 values (orientation_*: 3 per node,
+ * interleaved), NaN in inactive buckets */
 int wcg_download_field(wcg_ctx* ctx, const char* name, double* out, long long n);
+/* Set a node velocity field between calls: "u_x/y/z" (the liquid face
+ * velocity mapNodeParticlesAPIC reads, m_node_vel_fluid_*) or "vel_x/y/z"
+ * (the solid-phase m_node_vel_*, with elasto particles) -- the seam where a
+ * caller's own solve (e.g. LinearizedImplicitEuler's solid phase) hands its
+ * result back.  n >= number of nodes; inactive buckets are ignored. */
+int wcg_upload_field(wcg_ctx* ctx, const char* name, const double* in, long long n);
 /* integer field by name ("active", "dof_index", "valid_x", "array_idx",
  * "array_sup", "stencil_base", "grid_dims") */
 int wcg_download_ifield(wcg_ctx* ctx, const char* name, long long* out, long long n);

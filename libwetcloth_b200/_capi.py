@@ -23,6 +23,7 @@ WCG_ERR_CUDA = 2
 WCG_ERR_NOT_CONVERGED = 3
 WCG_ERR_DEVICE = 4
 WCG_ERR_STATE = 5
+WCG_ERR_UNSUPPORTED = 6
 WCG_FP64 = 0
 WCG_FP32_REFINE = 1
 WCG_SOLVER_MIC0 = 0
@@ -48,6 +49,9 @@ class WcgParams(ctypes.Structure):
         ("solver", ctypes.c_int),
         ("viscosity", ctypes.c_double),
         ("viscosity_substeps", ctypes.c_int),
+        ("elasto_flip_coeff", ctypes.c_double),
+        ("elasto_flip_asym_coeff", ctypes.c_double),
+        ("elasto_advect_coeff", ctypes.c_double),
     ]
 
 
@@ -78,6 +82,10 @@ SIGNATURES = {
     "wcg_download_liquid_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p,
                                                   ctypes.c_void_p, ctypes.c_void_p]),
     "wcg_num_particles": (ctypes.c_longlong, [ctypes.c_void_p]),
+    "wcg_upload_elasto": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong] + [_D] * 10 + [_I]),
+    "wcg_download_elasto": (ctypes.c_int, [ctypes.c_void_p, _D, _D, _D]),
+    "wcg_num_elasto": (ctypes.c_longlong, [ctypes.c_void_p]),
+    "wcg_upload_field": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, _D, ctypes.c_longlong]),
     "wcg_save_positions": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
     "wcg_load_positions": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
     "wcg_write_fluid_obj": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),

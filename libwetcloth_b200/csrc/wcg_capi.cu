@@ -66,8 +66,12 @@ int device_status(wcg::Context& c, const char* what) {
 
 struct FieldName {
   const char* name;
-  int field;  // wcg::GField, or -1 for an all-zero field
+  int field;      // wcg::GField, kEBase + wcg::EField, or -1 for an all-zero field
+  int ncomp = 1;  // values per node
 };
+
+// elasto node fields are numbered after the GField ones
+constexpr int kEBase = 1000;
 
 // P2G/step outputs that are identically zero for liquid-only scenes (no
 // elasto particles, static walls): solid volume fraction psi, solid velocity,
@@ -79,7 +83,16 @@ const FieldName kFields[] = {
     {"vol_fluid_x", wcg::G_VOL}, {"vol_fluid_y", wcg::G_VOL + 1},
     {"vol_fluid_z", wcg::G_VOL + 2}, {"sat_x", wcg::G_SAT},
     {"sat_y", wcg::G_SAT + 1}, {"sat_z", wcg::G_SAT + 2},
-    {"psi_x", -1}, {"psi_y", -1}, {"psi_z", -1},
+    {"psi_x", kEBase + wcg::E_PSI}, {"psi_y", kEBase + wcg::E_PSI + 1},
+    {"psi_z", kEBase + wcg::E_PSI + 2},
+    {"mass_x", kEBase + wcg::E_MASS}, {"mass_y", kEBase + wcg::E_MASS + 1},
+    {"mass_z", kEBase + wcg::E_MASS + 2}, {"vel_x", kEBase + wcg::E_VEL},
+    {"vel_y", kEBase + wcg::E_VEL + 1}, {"vel_z", kEBase + wcg::E_VEL + 2},
+    {"vol_x", kEBase + wcg::E_VOL}, {"vol_y", kEBase + wcg::E_VOL + 1},
+    {"vol_z", kEBase + wcg::E_VOL + 2}, {"shape_factor_x", kEBase + wcg::E_SF},
+    {"shape_factor_y", kEBase + wcg::E_SF + 1}, {"shape_factor_z", kEBase + wcg::E_SF + 2},
+    {"orientation_x", kEBase + wcg::E_ORI, 3}, {"orientation_y", kEBase + wcg::E_ORI + 3, 3},
+    {"orientation_z", kEBase + wcg::E_ORI + 6, 3},
     {"solid_weight_x", wcg::G_WEIGHT}, {"solid_weight_y", wcg::G_WEIGHT + 1},
     {"solid_weight_z", wcg::G_WEIGHT + 2}, {"solid_vel_x", -1},
     {"solid_vel_y", -1}, {"solid_vel_z", -1},
@@ -90,8 +103,8 @@ const FieldName kFields[] = {
     {"inv_C_z", wcg::G_INVC + 2}, {"psi_fs_x", wcg::G_PSIFS},
     {"psi_fs_y", wcg::G_PSIFS + 1}, {"psi_fs_z", wcg::G_PSIFS + 2},
     {"u_x", wcg::G_U}, {"u_y", wcg::G_U + 1}, {"u_z", wcg::G_U + 2},
-    {"liquid_phi", wcg::G_LPHI}, {"sat_p", wcg::G_SATP}, {"psi_p", -1},
-    {"pore_pressure_p", -1}, {"solid_phi", wcg::G_SPHI},
+    {"liquid_phi", wcg::G_LPHI}, {"sat_p", wcg::G_SATP}, {"psi_p", kEBase + wcg::E_PSIP},
+    {"pore_pressure_p", kEBase + wcg::E_PORE}, {"solid_phi", wcg::G_SPHI},
     {"pressure", wcg::G_PRESSURE}, {"A_diag", wcg::G_ADIAG},
     {"A_x", wcg::G_AX}, {"A_y", wcg::G_AY}, {"A_z", wcg::G_AZ},
     {"b_dense", wcg::G_B}, {"mic_invdiag", wcg::G_INVDIAG},
@@ -99,9 +112,12 @@ const FieldName kFields[] = {
     {"liquid_ey_vf", wcg::G_VFEY}, {"liquid_ez_vf", wcg::G_VFEZ},
 };
 
-int lookup_field(const char* name) {
+int lookup_field(const char* name, int* ncomp = nullptr) {
   for (const FieldName& f : kFields)
-    if (!strcmp(f.name, name)) return f.field;
+    if (!strcmp(f.name, name)) {
+      if (ncomp) *ncomp = f.ncomp;
+      return f.field;
+    }
   return -2;
 }
 
@@ -112,18 +128,21 @@ std::vector<unsigned char> host_active(wcg::Context& c) {
   return a;
 }
 
-// raw field (converted to double) over all nodes
+// raw field (converted to double) over all nodes; elasto fields are zero
+// while the scene has no elasto particles
 std::vector<double> host_field(wcg::Context& c, int field) {
   const long long nn = c.g.nnode;
   std::vector<double> out((size_t)nn, 0.0);
   if (field < 0 || nn == 0) return out;
+  const bool ef = field >= kEBase;
+  if (ef && (c.ne == 0 || c.efcap < c.gcap)) return out;
+  const wcg::DevBuf& buf = ef ? c.efield : c.gfield;
+  const size_t off = (size_t)(ef ? field - kEBase : field) * c.gcap;
   if (c.prm.precision == 0) {
-    cudaMemcpy(out.data(), c.gfield.as<double>() + (size_t)field * c.gcap,
-               nn * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaMemcpy(out.data(), buf.as<double>() + off, nn * sizeof(double), cudaMemcpyDeviceToHost);
   } else {
     std::vector<float> f((size_t)nn);
-    cudaMemcpy(f.data(), c.gfield.as<float>() + (size_t)field * c.gcap,
-               nn * sizeof(float), cudaMemcpyDeviceToHost);
+    cudaMemcpy(f.data(), buf.as<float>() + off, nn * sizeof(float), cudaMemcpyDeviceToHost);
     for (long long i = 0; i < nn; ++i) out[i] = f[i];
   }
   return out;
@@ -168,6 +187,9 @@ void wcg_default_params(wcg_params* p) {
   p->solver = WCG_SOLVER_MIC0;
   p->viscosity = 0.0;
   p->viscosity_substeps = 1;
+  p->elasto_flip_coeff = 0.95;
+  p->elasto_flip_asym_coeff = 1.0;
+  p->elasto_advect_coeff = 1.0;
 }
 
 int wcg_create(const wcg_params* params, wcg_ctx** out) {
@@ -176,6 +198,13 @@ int wcg_create(const wcg_params* params, wcg_ctx** out) {
   if (params->precision != WCG_FP64 && params->precision != WCG_FP32_REFINE)
     return fail(WCG_ERR_ARG, "precision must be WCG_FP64 or WCG_FP32_REFINE");
   if (params->maxiters < 0) return fail(WCG_ERR_ARG, "maxiters must be >= 0");
+  if (params->solver != WCG_SOLVER_MIC0 && params->solver != WCG_SOLVER_MG)
+    return fail(WCG_ERR_ARG, "solver must be WCG_SOLVER_MIC0 or WCG_SOLVER_MG");
+  if (!(params->viscosity >= 0.0) || !std::isfinite(params->viscosity))
+    return fail(WCG_ERR_ARG, "viscosity must be finite and >= 0");
+  if (!std::isfinite(params->elasto_flip_coeff) || !std::isfinite(params->elasto_flip_asym_coeff) ||
+      !std::isfinite(params->elasto_advect_coeff))
+    return fail(WCG_ERR_ARG, "elasto coefficients must be finite");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return fail(WCG_ERR_CUDA, "no CUDA device available");
@@ -197,13 +226,12 @@ int wcg_create(const wcg_params* params, wcg_ctx** out) {
   p.precision = params->precision;
   p.refine_inner_tol = params->refine_inner_tol > 0 ? params->refine_inner_tol : 0.0;
   p.max_refinements = params->max_refinements > 0 ? params->max_refinements : 20;
-  if (params->solver != WCG_SOLVER_MIC0 && params->solver != WCG_SOLVER_MG)
-    return fail(WCG_ERR_ARG, "solver must be WCG_SOLVER_MIC0 or WCG_SOLVER_MG");
   p.solver = params->solver;
-  if (!(params->viscosity >= 0.0) || !std::isfinite(params->viscosity))
-    return fail(WCG_ERR_ARG, "viscosity must be finite and >= 0");
   p.viscosity = params->viscosity;
   p.viscosity_substeps = params->viscosity_substeps > 0 ? params->viscosity_substeps : 1;
+  p.elasto_flip = params->elasto_flip_coeff;
+  p.elasto_flip_asym = params->elasto_flip_asym_coeff;
+  p.elasto_advect = params->elasto_advect_coeff;
   // wavefront tile shape (performance knob; both compute identical results)
   if (const char* v = getenv("WCG_SWEEP_TILE")) ctx->c.sweep_variant = !strcmp(v, "warp") ? 1 : 0;
   // layout of the pressure solve (performance knob; same arithmetic)
@@ -274,6 +302,44 @@ int wcg_download_liquid_device(wcg_ctx* ctx, double* x3, double* v3, double* C9)
 
 long long wcg_num_particles(const wcg_ctx* ctx) { return ctx ? ctx->c.np : -1; }
 
+int wcg_upload_elasto(wcg_ctx* ctx, long long n, const double* x4, const double* v4,
+                      const double* B9, const double* m4, const double* fm4,
+                      const double* rest_vol, const double* rest_vf, const double* fluid_vol,
+                      const double* shape_factor, const double* orient3, const int* surfel) {
+  WCG_CHECK_CTX(ctx);
+  if (n < 0 || n > 2000000000ll) return fail(WCG_ERR_ARG, "particle count out of range");
+  if (n > 0 && (!x4 || !v4 || !B9 || !m4 || !fm4 || !rest_vol || !rest_vf || !fluid_vol ||
+                !shape_factor || !orient3 || !surfel))
+    return fail(WCG_ERR_ARG, "null elasto particle array");
+  for (long long i = 0; i < 4 * n; ++i)
+    if (!std::isfinite(x4[i]) || !std::isfinite(v4[i]) || !std::isfinite(m4[i]) ||
+        !std::isfinite(fm4[i]))
+      return fail(WCG_ERR_ARG, "non-finite elasto position, velocity or mass");
+  for (long long i = 0; i < 9 * n; ++i)
+    if (!std::isfinite(B9[i])) return fail(WCG_ERR_ARG, "non-finite elasto affine matrix");
+  for (long long i = 0; i < n; ++i) {
+    if (!(rest_vol[i] >= 0) || !(fluid_vol[i] >= 0) || !(rest_vf[i] >= 0) ||
+        !std::isfinite(rest_vol[i]) || !std::isfinite(fluid_vol[i]) ||
+        !std::isfinite(rest_vf[i]) || !std::isfinite(shape_factor[i]))
+      return fail(WCG_ERR_ARG, "negative or non-finite elasto volume attribute");
+    for (int a = 0; a < 3; ++a)
+      if (!std::isfinite(orient3[i * 3 + a]))
+        return fail(WCG_ERR_ARG, "non-finite elasto orientation");
+  }
+  WCG_CALL(ctx, wcg::upload_elasto(ctx->c, n, x4, v4, B9, m4, fm4, rest_vol, rest_vf, fluid_vol,
+                                   shape_factor, orient3, surfel),
+           "upload elasto");
+  return WCG_OK;
+}
+
+int wcg_download_elasto(wcg_ctx* ctx, double* x4, double* v4, double* B9) {
+  WCG_CHECK_CTX(ctx);
+  WCG_CALL(ctx, wcg::download_elasto(ctx->c, x4, v4, B9), "download elasto");
+  return WCG_OK;
+}
+
+long long wcg_num_elasto(const wcg_ctx* ctx) { return ctx ? ctx->c.ne : -1; }
+
 // ---- state I/O in the reference's file formats ------------------------------
 // TwoDSceneSerializer::serializePositionOnly / serialize_pos_subprog
 // (App/TwoDSceneSerializer.cpp:20-32, :161-170): an int byte count and m_x
@@ -282,11 +348,15 @@ long long wcg_num_particles(const wcg_ctx* ctx) { return ctx ? ctx->c.np : -1; }
 int wcg_save_positions(wcg_ctx* ctx, const char* path) {
   WCG_CHECK_CTX(ctx);
   if (!path) return fail(WCG_ERR_ARG, "null path");
-  const long long n = ctx->c.np;
+  // elasto particles first, as the reference numbers them
+  const long long ne = ctx->c.ne, n = ne + ctx->c.np;
   if (n * 4 * (long long)sizeof(double) > 2147483647ll)
     return fail(WCG_ERR_ARG, "too many particles for the position file's int byte count");
   std::vector<double> x4((size_t)n * 4);
-  if (n > 0) WCG_CALL(ctx, wcg::download_positions(ctx->c, x4.data(), nullptr), "save positions");
+  if (ne > 0) WCG_CALL(ctx, wcg::download_elasto(ctx->c, x4.data(), nullptr, nullptr),
+                       "save positions");
+  if (ctx->c.np > 0)
+    WCG_CALL(ctx, wcg::download_positions(ctx->c, x4.data() + 4 * ne, nullptr), "save positions");
   std::ofstream f(path, std::ios::binary);
   if (!f) return fail(WCG_ERR_ARG, std::string("cannot open ") + path);
   const int bytes = (int)(n * 4 * sizeof(double));
@@ -307,7 +377,7 @@ int wcg_load_positions(wcg_ctx* ctx, const char* path) {
   if (!f) return fail(WCG_ERR_ARG, std::string("cannot open ") + path);
   int bytes = -1;
   f.read((char*)&bytes, sizeof(int));
-  const long long n = ctx->c.np;
+  const long long ne = ctx->c.ne, n = ne + ctx->c.np;
   if (!f || bytes != n * 4 * (long long)sizeof(double))
     return fail(WCG_ERR_ARG, "position file holds " + std::to_string(bytes) +
                                  " bytes, the scene needs " +
@@ -319,7 +389,10 @@ int wcg_load_positions(wcg_ctx* ctx, const char* path) {
   if (!f) return fail(WCG_ERR_ARG, std::string("truncated position file: ") + path);
   for (double v : x4)
     if (!std::isfinite(v)) return fail(WCG_ERR_ARG, "non-finite position in file");
-  if (n > 0) WCG_CALL(ctx, wcg::upload_positions(ctx->c, x4.data()), "load positions");
+  if (ne > 0)
+    WCG_CALL(ctx, wcg::upload_elasto_positions(ctx->c, x4.data()), "load positions");
+  if (ctx->c.np > 0)
+    WCG_CALL(ctx, wcg::upload_positions(ctx->c, x4.data() + 4 * ne), "load positions");
   return WCG_OK;
 }
 
@@ -352,6 +425,17 @@ int wcg_rebucketize_and_resample(wcg_ctx* ctx) {
       return fail(WCG_ERR_STATE, "no grid: call wcg_rebucketize_and_resample"); \
   } while (0)
 
+// The elasto coupling terms of the solve (drag arrays of constructHDV, the
+// solid volume fraction in the pressure system, applyPressureDragElasto) are
+// not built: calls that need them refuse scenes with elasto particles.
+#define WCG_NO_ELASTO(ctx, what)                                              \
+  do {                                                                       \
+    if ((ctx)->c.ne > 0)                                                     \
+      return fail(WCG_ERR_UNSUPPORTED, std::string(what) +                   \
+                                           ": the elasto coupling of the solve is not built " \
+                                           "(transfers only for elasto particles)"); \
+  } while (0)
+
 int wcg_map_particle_nodes(wcg_ctx* ctx) {
   WCG_CHECK_CTX(ctx);
   WCG_NEED_GRID(ctx);
@@ -361,6 +445,7 @@ int wcg_map_particle_nodes(wcg_ctx* ctx) {
 
 int wcg_step_velocity(wcg_ctx* ctx, double dt) {
   WCG_CHECK_CTX(ctx);
+  WCG_NO_ELASTO(ctx, "stepVelocity");
   WCG_NEED_GRID(ctx);
   if (!(dt > 0)) return fail(WCG_ERR_ARG, "dt must be positive");
   WCG_CALL(ctx, wcg::step_velocity(ctx->c, dt), "stepVelocity");
@@ -369,6 +454,7 @@ int wcg_step_velocity(wcg_ctx* ctx, double dt) {
 
 int wcg_project_fine(wcg_ctx* ctx, double dt) {
   WCG_CHECK_CTX(ctx);
+  WCG_NO_ELASTO(ctx, "projectFine");
   WCG_NEED_GRID(ctx);
   if (!(dt > 0)) return fail(WCG_ERR_ARG, "dt must be positive");
   WCG_CALL(ctx, wcg::project_fine(ctx->c, dt), "projectFine");
@@ -384,6 +470,7 @@ int wcg_project_fine(wcg_ctx* ctx, double dt) {
 
 int wcg_apply_pressure_drag_fluid(wcg_ctx* ctx, double dt) {
   WCG_CHECK_CTX(ctx);
+  WCG_NO_ELASTO(ctx, "applyPressureDragFluid");
   WCG_NEED_GRID(ctx);
   WCG_CALL(ctx, wcg::apply_pressure_and_extrapolate(ctx->c, dt), "applyPressureDragFluid");
   return device_status(ctx->c, "applyPressureDragFluid");
@@ -413,6 +500,7 @@ int wcg_advect(wcg_ctx* ctx, double dt) {
 
 int wcg_substep(wcg_ctx* ctx, double dt) {
   WCG_CHECK_CTX(ctx);
+  WCG_NO_ELASTO(ctx, "substep");
   if (!(dt > 0)) return fail(WCG_ERR_ARG, "dt must be positive");
   WCG_CALL(ctx, wcg::substep(ctx->c, dt), "substep");
   int s = device_status(ctx->c, "substep");
@@ -432,6 +520,7 @@ int wcg_num_substeps(wcg_ctx* ctx, double dt, int* n_out) {
 
 int wcg_step(wcg_ctx* ctx, double dt, int* substeps_out) {
   WCG_CHECK_CTX(ctx);
+  WCG_NO_ELASTO(ctx, "step");
   if (!(dt > 0)) return fail(WCG_ERR_ARG, "dt must be positive");
   int n = 1;
   WCG_CALL(ctx, wcg::num_substeps(ctx->c, dt, &n), "num_substeps");
@@ -489,14 +578,15 @@ int wcg_grid_info(const wcg_ctx* ctx, int* dims, double* origin, double* bbx) {
 long long wcg_field_size(wcg_ctx* ctx, const char* name) {
   if (!ctx || !name) return -1;
   const wcg::Context& c = ctx->c;
-  if (lookup_field(name) >= -1) return c.g.nnode;
+  int ncomp = 1;
+  if (lookup_field(name, &ncomp) >= -1) return ncomp * c.g.nnode;
   if (!strcmp(name, "active")) return c.g.nb;
   if (!strcmp(name, "dof_index") || !strcmp(name, "valid_x") ||
       !strcmp(name, "valid_y") || !strcmp(name, "valid_z"))
     return c.g.nnode;
-  if (!strcmp(name, "array_idx")) return c.np;
+  if (!strcmp(name, "array_idx")) return c.np + c.ne;
   if (!strcmp(name, "array_sup")) return 2 * c.g.nb;
-  if (!strcmp(name, "stencil_base")) return 15 * c.np;
+  if (!strcmp(name, "stencil_base")) return 15 * (c.np + c.ne);
   if (!strcmp(name, "grid_dims")) return 3;
   return -1;
 }
@@ -505,16 +595,54 @@ int wcg_download_field(wcg_ctx* ctx, const char* name, double* out, long long n)
   WCG_CHECK_CTX(ctx);
   if (!name || !out) return fail(WCG_ERR_ARG, "null argument");
   wcg::Context& c = ctx->c;
-  const int f = lookup_field(name);
+  int ncomp = 1;
+  const int f = lookup_field(name, &ncomp);
   if (f < -1) return fail(WCG_ERR_ARG, std::string("unknown field ") + name);
-  if (n < c.g.nnode) return fail(WCG_ERR_ARG, "output buffer too small");
+  if (n < ncomp * c.g.nnode) return fail(WCG_ERR_ARG, "output buffer too small");
+  cudaStreamSynchronize(c.stream);
+  std::vector<unsigned char> act = host_active(c);
+  const double nan = std::numeric_limits<double>::quiet_NaN();
+  // a multi-component field (orientation) interleaves its components per node
+  for (int q = 0; q < ncomp; ++q) {
+    std::vector<double> v = host_field(c, f < 0 ? f : f + q);
+    for (long long i = 0; i < c.g.nnode; ++i) out[i * ncomp + q] = act[i >> 6] ? v[i] : nan;
+  }
+  cudaError_t e = cudaGetLastError();
+  return cuda_status(c, e, "download_field");
+}
+
+// Node velocities a caller may set between the reference's calls (the
+// host-side seam for work not done here, e.g. a solid solve): the liquid face
+// velocity G2P reads ("u_*") and the solid-phase face velocity ("vel_*", with
+// elasto particles).  Values of nodes in inactive buckets are ignored.
+int wcg_upload_field(wcg_ctx* ctx, const char* name, const double* in, long long n) {
+  WCG_CHECK_CTX(ctx);
+  WCG_NEED_GRID(ctx);
+  if (!name || !in) return fail(WCG_ERR_ARG, "null argument");
+  wcg::Context& c = ctx->c;
+  int f = -2;
+  for (const char* w : {"u_x", "u_y", "u_z", "vel_x", "vel_y", "vel_z"})
+    if (!strcmp(name, w)) f = lookup_field(name);
+  if (f < 0) return fail(WCG_ERR_ARG, std::string("field is not writable: ") + name);
+  const bool ef = f >= kEBase;
+  if (ef && c.ne == 0) return fail(WCG_ERR_STATE, "solid-phase fields need elasto particles");
+  const long long nn = c.g.nnode;
+  if (n < nn) return fail(WCG_ERR_ARG, "input buffer too small");
   cudaStreamSynchronize(c.stream);
   std::vector<double> v = host_field(c, f);
   std::vector<unsigned char> act = host_active(c);
-  const double nan = std::numeric_limits<double>::quiet_NaN();
-  for (long long i = 0; i < c.g.nnode; ++i) out[i] = act[i >> 6] ? v[i] : nan;
-  cudaError_t e = cudaGetLastError();
-  return cuda_status(c, e, "download_field");
+  for (long long i = 0; i < nn; ++i)
+    if (act[i >> 6]) v[i] = in[i];
+  wcg::DevBuf& buf = ef ? c.efield : c.gfield;
+  const size_t off = (size_t)(ef ? f - kEBase : f) * c.gcap;
+  cudaError_t e;
+  if (c.prm.precision == 0) {
+    e = cudaMemcpy(buf.as<double>() + off, v.data(), nn * sizeof(double), cudaMemcpyHostToDevice);
+  } else {
+    std::vector<float> h(v.begin(), v.end());
+    e = cudaMemcpy(buf.as<float>() + off, h.data(), nn * sizeof(float), cudaMemcpyHostToDevice);
+  }
+  return cuda_status(c, e, "upload_field");
 }
 
 int wcg_download_ifield(wcg_ctx* ctx, const char* name, long long* out, long long n) {
@@ -555,17 +683,28 @@ int wcg_download_ifield(wcg_ctx* ctx, const char* name, long long* out, long lon
     for (long long i = 0; i < g.nnode; ++i) out[i] = a[i >> 6] ? v[i] : -1;
     return WCG_OK;
   }
-  const long long np = c.np;
+  // all particles in the reference's numbering: elasto [0, ne), liquid after
+  const long long ne = c.ne, nl = c.np, np = ne + nl;
   std::vector<int> pid(np), pb(np), dl(np);
   std::vector<long long> key(np);
-  if (np) {
-    cudaMemcpy(pid.data(), c.pid[c.cur].p, np * sizeof(int), cudaMemcpyDeviceToHost);
-    cudaMemcpy(pb.data(), c.pbucket.as<int>() + c.cur * c.pcap, np * sizeof(int),
+  if (ne) {
+    cudaMemcpy(pid.data(), c.epid[c.ecur].p, ne * sizeof(int), cudaMemcpyDeviceToHost);
+    cudaMemcpy(pb.data(), c.ebucket.as<int>() + c.ecur * c.ecap, ne * sizeof(int),
                cudaMemcpyDeviceToHost);
-    cudaMemcpy(dl.data(), c.pdelta.as<int>() + c.cur * c.pcap, np * sizeof(int),
+    cudaMemcpy(dl.data(), c.edelta.as<int>() + c.ecur * c.ecap, ne * sizeof(int),
                cudaMemcpyDeviceToHost);
-    cudaMemcpy(key.data(), c.pkey.as<long long>() + c.cur * c.pcap, np * sizeof(long long),
+    cudaMemcpy(key.data(), c.ekey.as<long long>() + c.ecur * c.ecap, ne * sizeof(long long),
                cudaMemcpyDeviceToHost);
+  }
+  if (nl) {
+    cudaMemcpy(pid.data() + ne, c.pid[c.cur].p, nl * sizeof(int), cudaMemcpyDeviceToHost);
+    cudaMemcpy(pb.data() + ne, c.pbucket.as<int>() + c.cur * c.pcap, nl * sizeof(int),
+               cudaMemcpyDeviceToHost);
+    cudaMemcpy(dl.data() + ne, c.pdelta.as<int>() + c.cur * c.pcap, nl * sizeof(int),
+               cudaMemcpyDeviceToHost);
+    cudaMemcpy(key.data() + ne, c.pkey.as<long long>() + c.cur * c.pcap, nl * sizeof(long long),
+               cudaMemcpyDeviceToHost);
+    for (long long s = ne; s < np; ++s) pid[s] += (int)ne;
   }
   if (!strcmp(name, "array_idx") || !strcmp(name, "array_sup")) {
     // Sorter::sort keys (bucket << 32 | particle), sorted

@@ -31,6 +31,9 @@ struct Params {
   int solver;     // 0: MIC(0)-PCG, 1: multigrid-PCG (AMGPCGSolveSparse)
   double viscosity;        // LiquidInfo::viscosity (0: compute_viscosity off)
   int viscosity_substeps;  // explicit viscosity sub-steps per step_velocity
+  double elasto_flip;      // LiquidInfo::elasto_flip_coeff
+  double elasto_flip_asym; // LiquidInfo::elasto_flip_asym_coeff
+  double elasto_advect;    // LiquidInfo::elasto_advect_coeff
 };
 
 // A device allocation that grows and never shrinks.
@@ -101,6 +104,28 @@ enum GField : int {
   kNumGFields = 57
 };
 
+// Columns of the elasto (cloth / yarn) particle SoA.  Positions come first so
+// the bounding-box and particle-pass kernels read them as they read liquid
+// particles.  EM* = m(a) + m_fluid(a), ERV/ERF = m_rest_vol and
+// m_rest_volume_fraction, EFV = m_fluid_vol, ESF = m_shape_factor, EO* =
+// m_orientation, ESURF = 1 for surfels (m_particle_to_surfel >= 0).
+enum ECol : int {
+  EX = 0, EY, EZ, ETH, EVX, EVY, EVZ, EVT,
+  EB00, EB01, EB02, EB10, EB11, EB12, EB20, EB21, EB22,
+  EM0, EM1, EM2, ERV, ERF, EFV, ESF, EOX, EOY, EOZ, ESURF,
+  kNumECols
+};
+
+// Node fields that only elasto particles make nonzero (m_node_mass_*,
+// m_node_vel_*, m_node_vol_*, m_node_psi_*, m_node_shape_factor_*,
+// m_node_orientation_* (3 per face axis), m_node_psi_p, pore pressure).
+enum EField : int {
+  E_MASS = 0, E_VEL = 3, E_VOL = 6, E_PSI = 9, E_SF = 12,
+  E_ORI = 15,  // E_ORI + 3 * axis + component
+  E_PSIP = 24, E_PORE = 25,
+  kNumEFields = 26
+};
+
 // Geometry of the pencil layout of one pressure solve (wcg_pencil.cuh).
 struct PencilGeom {
   int ax_s, ax_a, ax_c;  // physical axis (0 x, 1 y, 2 z) of s, a, c
@@ -140,6 +165,19 @@ struct Context {
   DevBuf pbucket;          // reference bucket index, int32
   DevBuf perm;             // sorted slot -> source slot, int32
   DevBuf hostorder;        // scratch for downloads in original order
+
+  // elasto particles: same sorted ping-pong scheme as the liquid ones
+  long long ne = 0;
+  long long ecap = 0;
+  DevBuf ebuf[2];          // kNumECols * ecap Reals each
+  int ecur = 0;
+  DevBuf epid[2];          // original elasto index, int32
+  DevBuf ekey, edelta, ebucket;  // as pkey/pdelta/pbucket, 2 * ecap each
+  DevBuf eperm;
+  DevBuf estage;           // upload/download staging (doubles)
+  DevBuf ecell_start;      // int32 per node + 1 (elasto particles per key cell)
+  DevBuf efield;           // kNumEFields * gcap Reals (allocated with elasto)
+  long long efcap = 0;
 
   // grid
   GridDesc g{};
@@ -247,6 +285,15 @@ cudaError_t download_particles(Context& c, double* x3, double* v3, double* C9,
 // original order, host buffers
 cudaError_t download_positions(Context& c, double* x4, double* radius);
 cudaError_t upload_positions(Context& c, const double* x4);
+// elasto particles in the reference's layouts (x4/v4/m4/fm4 stride 4, B9
+// row-major, orient3 stride 3), host buffers
+cudaError_t upload_elasto(Context& c, long long n, const double* x4, const double* v4,
+                          const double* B9, const double* m4, const double* fm4,
+                          const double* rest_vol, const double* rest_vf,
+                          const double* fluid_vol, const double* shape_factor,
+                          const double* orient3, const int* surfel);
+cudaError_t download_elasto(Context& c, double* x4, double* v4, double* B9);
+cudaError_t upload_elasto_positions(Context& c, const double* x4);
 
 // reference call sequence
 cudaError_t build_grid(Context& c);                 // bbox + rebucketize + resampleNodes

@@ -67,7 +67,8 @@ __global__ void k_particle_prepass(GridDesc g, const R* __restrict__ P,
                                    int* __restrict__ pbucket,
                                    unsigned char* __restrict__ active_pre,
                                    int* __restrict__ cell_count,
-                                   int* __restrict__ drange, int* err) {
+                                   int* __restrict__ drange, int* err,
+                                   const R* __restrict__ surf = nullptr) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = i < np;
   int d[3] = {0, 0, 0};
@@ -103,8 +104,10 @@ __global__ void k_particle_prepass(GridDesc g, const R* __restrict__ P,
       key[i] = k;
       atomicAdd(&cell_count[k], 1);
     }
-    // activation of the buckets under the five 3x3x3 stencils
-    for (int t = 0; t < 5; ++t) {
+    // activation of the buckets under the five 3x3x3 stencils, by soft
+    // particles only (isSoft :697: surfels activate nothing)
+    const int nt = (surf == nullptr || surf[i] == R(0)) ? 5 : 0;
+    for (int t = 0; t < nt; ++t) {
       // offsets: u(0,.5,.5) v(.5,0,.5) w(.5,.5,0) solid-phi(0,0,0) p(.5,.5,.5)
       int lo[3];
       for (int a = 0; a < 3; ++a) {
@@ -271,7 +274,7 @@ __global__ void __launch_bounds__(256)
           const unsigned char* __restrict__ active, const R* __restrict__ P,
           long long pcap, const int* __restrict__ start,
           const int* __restrict__ delta, DeltaRange dr, R* __restrict__ F,
-          long long fstride, Walls walls) {
+          long long fstride, Walls walls, int raw_satp, int have_liquid) {
   const int b = active_list[blockIdx.x];
   const int type = threadIdx.x >> 6;
   const int l = threadIdx.x & 63;
@@ -376,10 +379,13 @@ __global__ void __launch_bounds__(256)
     const double three_bs = 3.0 * g.bs;
     const double sphi_c = wall_phi(walls, (double)np_[0], (double)np_[1],
                                    (double)np_[2], three_bs);
-    if (sphi_c < 0.0) phi = R(-0.5) * dx;
+    // updateLiquidPhi returns before the wall rule when there is no liquid
+    // particle (TwoDScene.cpp:3303)
+    if (have_liquid && sphi_c < 0.0) phi = R(-0.5) * dx;
     F[G_LPHI * fstride + n] = phi;
     const R den = dV > R(1e-20) ? dV : R(1e-20);
-    F[G_SATP * fstride + n] = clamp01<R>(vliq / den);
+    // with elasto particles k_p2g_elasto completes sat_p from the raw sum
+    F[G_SATP * fstride + n] = raw_satp ? vliq : clamp01<R>(vliq / den);
     // solid phi at the corner node (TwoDScene::updateSolidPhi :7940-7960)
     const double cx = (double)coord<R>(org[0], bs, dx, I, R(0));
     const double cy = (double)coord<R>(org[1], bs, dx, J, R(0));

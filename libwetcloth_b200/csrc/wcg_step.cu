@@ -14,6 +14,7 @@
 #include "wcg_pencil.cuh"
 #include "wcg_mg.cuh"
 #include "wcg_visc.cuh"
+#include "wcg_elasto.cuh"
 #include "wcg_scan.cuh"
 
 namespace wcg {
@@ -276,6 +277,102 @@ cudaError_t upload_positions(Context& c, const double* x4) {
   return cudaStreamSynchronize(c.stream);
 }
 
+// Elasto particles: the host packs the reference's per-particle members into
+// kNumECols double columns (m(a) + m_fluid(a) summed in double, as the
+// reference's P2G does), one copy, one conversion kernel.
+cudaError_t upload_elasto(Context& c, long long n, const double* x4, const double* v4,
+                          const double* B9, const double* m4, const double* fm4,
+                          const double* rest_vol, const double* rest_vf,
+                          const double* fluid_vol, const double* shape_factor,
+                          const double* orient3, const int* surfel) {
+  const int rb = c.real_bytes();
+  if (n > c.ecap) {
+    const long long cap = n;
+    for (int k = 0; k < 2; ++k) {
+      WCG_TRY(c.ebuf[k].ensure((size_t)kNumECols * cap * rb));
+      WCG_TRY(c.epid[k].ensure((size_t)cap * sizeof(int)));
+    }
+    WCG_TRY(c.ekey.ensure((size_t)2 * cap * sizeof(long long)));
+    WCG_TRY(c.edelta.ensure((size_t)2 * cap * sizeof(int)));
+    WCG_TRY(c.ebucket.ensure((size_t)2 * cap * sizeof(int)));
+    WCG_TRY(c.eperm.ensure((size_t)cap * sizeof(int)));
+    WCG_TRY(c.estage.ensure((size_t)kNumECols * cap * sizeof(double)));
+    c.ecap = cap;
+  }
+  c.ne = n;
+  c.ecur = 0;
+  c.have_grid = false;
+  if (n == 0) return cudaSuccess;
+  std::vector<double> h((size_t)kNumECols * n);
+  auto col = [&](int k) { return h.data() + (size_t)k * n; };
+  for (long long i = 0; i < n; ++i) {
+    for (int a = 0; a < 4; ++a) {
+      col(EX + a)[i] = x4[i * 4 + a];
+      col(EVX + a)[i] = v4[i * 4 + a];
+    }
+    for (int q = 0; q < 9; ++q) col(EB00 + q)[i] = B9[i * 9 + q];
+    for (int a = 0; a < 3; ++a) {
+      col(EM0 + a)[i] = m4[i * 4 + a] + fm4[i * 4 + a];
+      col(EOX + a)[i] = orient3[i * 3 + a];
+    }
+    col(ERV)[i] = rest_vol[i];
+    col(ERF)[i] = rest_vf[i];
+    col(EFV)[i] = fluid_vol[i];
+    col(ESF)[i] = shape_factor[i];
+    col(ESURF)[i] = surfel[i] ? 1.0 : 0.0;
+  }
+  double* st = c.estage.as<double>();
+  WCG_TRY(cudaMemcpyAsync(st, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice,
+                          c.stream));
+  if (c.prm.precision == 0)
+    ++c.launches, k_load_elasto<double><<<nblk(n, 256), 256, 0, c.stream>>>(
+        n, c.ecap, st, c.ebuf[0].as<double>(), c.epid[0].as<int>());
+  else
+    ++c.launches, k_load_elasto<float><<<nblk(n, 256), 256, 0, c.stream>>>(
+        n, c.ecap, st, c.ebuf[0].as<float>(), c.epid[0].as<int>());
+  WCG_TRY(cudaGetLastError());
+  return cudaStreamSynchronize(c.stream);
+}
+
+cudaError_t download_elasto(Context& c, double* x4, double* v4, double* B9) {
+  const long long n = c.ne;
+  if (n == 0) return cudaSuccess;
+  double* st = c.estage.as<double>();
+  if (c.prm.precision == 0)
+    ++c.launches, k_store_elasto<double><<<nblk(n, 256), 256, 0, c.stream>>>(
+        n, c.ecap, c.ebuf[c.ecur].as<double>(), c.epid[c.ecur].as<int>(), st, st + 4 * n,
+        st + 8 * n);
+  else
+    ++c.launches, k_store_elasto<float><<<nblk(n, 256), 256, 0, c.stream>>>(
+        n, c.ecap, c.ebuf[c.ecur].as<float>(), c.epid[c.ecur].as<int>(), st, st + 4 * n,
+        st + 8 * n);
+  WCG_TRY(cudaGetLastError());
+  if (x4) WCG_TRY(cudaMemcpyAsync(x4, st, n * 4 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  if (v4)
+    WCG_TRY(cudaMemcpyAsync(v4, st + 4 * n, n * 4 * sizeof(double), cudaMemcpyDeviceToHost,
+                            c.stream));
+  if (B9)
+    WCG_TRY(cudaMemcpyAsync(B9, st + 8 * n, n * 9 * sizeof(double), cudaMemcpyDeviceToHost,
+                            c.stream));
+  return cudaStreamSynchronize(c.stream);
+}
+
+cudaError_t upload_elasto_positions(Context& c, const double* x4) {
+  const long long n = c.ne;
+  if (n == 0) return cudaSuccess;
+  double* st = c.estage.as<double>();
+  WCG_TRY(cudaMemcpyAsync(st, x4, n * 4 * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+  if (c.prm.precision == 0)
+    ++c.launches, k_set_elasto_positions<double><<<nblk(n, 256), 256, 0, c.stream>>>(
+        n, c.ecap, c.ebuf[c.ecur].as<double>(), c.epid[c.ecur].as<int>(), st);
+  else
+    ++c.launches, k_set_elasto_positions<float><<<nblk(n, 256), 256, 0, c.stream>>>(
+        n, c.ecap, c.ebuf[c.ecur].as<float>(), c.epid[c.ecur].as<int>(), st);
+  WCG_TRY(cudaGetLastError());
+  c.have_grid = false;
+  return cudaStreamSynchronize(c.stream);
+}
+
 // ---------------------------------------------------------------------------
 // bounding box
 template <typename R>
@@ -337,16 +434,23 @@ static cudaError_t build_grid_t(Context& c) {
   ProfScope prof(c, P_GRID);
   const long long n = c.np;
   R* P = c.pbuf[c.cur].as<R>();
-  WCG_TRY(ensure_scratch(c, 0));
+  WCG_TRY(ensure_scratch(c, (size_t)kRedBlocks * 12 * sizeof(double)));
   double* part = c.scratch.as<double>();
   double* dsc = c.dscalars.as<double>();
-  // 1. bounding box (TwoDScene::updateParticleBoundingBox :1588-1612)
+  const long long ne = c.ne;
+  R* EP = ne > 0 ? c.ebuf[c.ecur].as<R>() : nullptr;
+  // 1. bounding box over all particles, elasto included
+  //    (TwoDScene::updateParticleBoundingBox :1588-1612)
   ++c.launches, k_minmax<R><<<kRedBlocks, kRedThreads, 0, c.stream>>>(P, c.pcap, n, part);
-  ++c.launches, k_minmax_final<<<1, 32, 0, c.stream>>>(part, kRedBlocks, dsc);
+  if (ne > 0)
+    ++c.launches, k_minmax<R><<<kRedBlocks, kRedThreads, 0, c.stream>>>(EP, c.ecap, ne,
+                                                                      part + kRedBlocks * 6);
+  ++c.launches, k_minmax_final<<<1, 32, 0, c.stream>>>(part, ne > 0 ? 2 * kRedBlocks : kRedBlocks,
+                                                        dsc);
   WCG_TRY(cudaMemcpyAsync(c.hscalars, dsc, 6 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
   WCG_TRY(cudaStreamSynchronize(c.stream));
   double bbmin[3] = {1e20, 1e20, 1e20}, bbmax[3] = {-1e20, -1e20, -1e20};
-  if (n > 0)
+  if (n + ne > 0)
     for (int a = 0; a < 3; ++a) {
       bbmin[a] = c.hscalars[a];
       bbmax[a] = c.hscalars[3 + a];
@@ -394,6 +498,11 @@ static cudaError_t build_grid_t(Context& c) {
     }
     c.gcap = cap;
   }
+  if (ne > 0 && c.efcap < c.gcap) {
+    WCG_TRY(c.efield.ensure((size_t)kNumEFields * c.gcap * rb));
+    WCG_TRY(c.ecell_start.ensure((size_t)(c.gcap + 1) * sizeof(int)));
+    c.efcap = c.gcap;
+  }
   const long long bcap = c.gcap / 64 + 1;
   if ((size_t)bcap > c.active.bytes) {
     WCG_TRY(c.active_pre.ensure((size_t)bcap));
@@ -435,6 +544,15 @@ static cudaError_t build_grid_t(Context& c) {
     ++c.launches, k_particle_prepass<R><<<nblk(n, 256), 256, 0, c.stream>>>(
         g, P, c.pcap, n, key_cur, delta_cur, pb_cur, c.active_pre.as<unsigned char>(),
         cstart, drange, c.derr.as<int>());
+  int* ecstart = c.ecell_start.as<int>();
+  long long* ekey_cur = c.ekey.as<long long>() + c.ecur * c.ecap;
+  int* edelta_cur = c.edelta.as<int>() + c.ecur * c.ecap;
+  if (ne > 0) {
+    WCG_TRY(cudaMemsetAsync(ecstart, 0, (g.nnode + 1) * sizeof(int), c.stream));
+    ++c.launches, k_particle_prepass<R><<<nblk(ne, 256), 256, 0, c.stream>>>(
+        g, EP, c.ecap, ne, ekey_cur, edelta_cur, c.ebucket.as<int>() + c.ecur * c.ecap,
+        c.active_pre.as<unsigned char>(), ecstart, drange, c.derr.as<int>(), EP + ESURF * c.ecap);
+  }
   WCG_TRY(cudaGetLastError());
   // 5. dilation
   ++c.launches, k_dilate<<<nblk(g.nb, 256), 256, 0, c.stream>>>(g, c.active_pre.as<unsigned char>(),
@@ -467,7 +585,7 @@ static cudaError_t build_grid_t(Context& c) {
     c.n_active = *(const int*)(c.hscalars + 16);
     c.n_tiles = *((const int*)(c.hscalars + 16) + 1);
     c.stats.nactive = c.n_active;
-    for (int k = 0; k < 6; ++k) c.drange_h[k] = n > 0 ? hr[k] : (k < 3 ? 0 : 1);
+    for (int k = 0; k < 6; ++k) c.drange_h[k] = n + ne > 0 ? hr[k] : (k < 3 ? 0 : 1);
   }
   // 7. wave ordering of the active tiles (ti+tj+tk)
   int* wcount = c.wave_count.as<int>();
@@ -500,6 +618,25 @@ static cudaError_t build_grid_t(Context& c) {
         c.pdelta.as<int>() + nxt * c.pcap, pb_cur, c.pbucket.as<int>() + nxt * c.pcap);
     c.cur = nxt;
   }
+  // the same counting sort for the elasto particles
+  if (ne > 0) {
+    exclusive_scan<int, int>(ecstart, g.nnode, ecstart, (int*)part, ecstart + g.nnode, c.stream);
+    WCG_TRY(cudaMemsetAsync(tmpi, 0, g.nnode * sizeof(int), c.stream));
+    ++c.launches, k_sort_scatter<<<nblk(ne, 256), 256, 0, c.stream>>>(ekey_cur, ne, ecstart, tmpi,
+                                                                     c.eperm.as<int>());
+    ++c.launches, k_sort_cells<<<nblk(g.nnode, 256), 256, 0, c.stream>>>(
+        ecstart, g.nnode, c.epid[c.ecur].as<int>(), c.eperm.as<int>());
+    const int nxt = c.ecur ^ 1;
+    ++c.launches, k_gather_elasto<R><<<nblk(ne, 256), 256, 0, c.stream>>>(
+        c.eperm.as<int>(), ne, c.ecap, EP, c.ebuf[nxt].as<R>(), c.epid[c.ecur].as<int>(),
+        c.epid[nxt].as<int>(), ekey_cur, c.ekey.as<long long>() + nxt * c.ecap, edelta_cur,
+        c.edelta.as<int>() + nxt * c.ecap);
+    // bucket indices move with their particles (host-side key listings)
+    ++c.launches, k_permute_int<<<nblk(ne, 256), 256, 0, c.stream>>>(
+        c.eperm.as<int>(), ne, c.ebucket.as<int>() + c.ecur * c.ecap,
+        c.ebucket.as<int>() + nxt * c.ecap);
+    c.ecur = nxt;
+  }
   WCG_TRY(cudaGetLastError());
   return cudaSuccess;
 }
@@ -529,13 +666,23 @@ static cudaError_t map_particles_to_grid_t(Context& c) {
   }
   R* F = c.gfield.as<R>();
   const Walls w = make_walls(c);
+  const bool elasto = c.ne > 0;
   ++c.launches, k_p2g<R><<<(unsigned)c.n_active, 256, 0, c.stream>>>(
       c.g, c.active_list.as<int>(), c.active.as<unsigned char>(), c.pbuf[c.cur].as<R>(),
-      c.pcap, c.cell_start.as<int>(), c.pdelta.as<int>() + c.cur * c.pcap, dr, F, c.gcap, w);
+      c.pcap, c.cell_start.as<int>(), c.pdelta.as<int>() + c.cur * c.pcap, dr, F, c.gcap, w,
+      elasto ? 1 : 0, c.np > 0 ? 1 : 0);
+  // solid phase of the same P2G, sat/psi/pore pressure with elasto volumes;
+  // LiquidInfo surf_tension_coeff 72.8, rest_contact_angle 40.8 deg,
+  // pore_radius 0.005 (App/TwoDSceneXMLParser.cpp:1851-1904 defaults)
+  if (elasto)
+    ++c.launches, k_p2g_elasto<R><<<(unsigned)c.n_active, 256, 0, c.stream>>>(
+        c.g, c.active_list.as<int>(), c.ebuf[c.ecur].as<R>(), c.ecap,
+        c.ecell_start.as<int>(), c.edelta.as<int>() + c.ecur * c.ecap, dr, F, c.gcap,
+        c.efield.as<R>(), 72.8, std::cos(40.8 / 180.0 * M_PI), 0.005);
   ++c.launches, k_solid_weights<R><<<(unsigned)c.n_active, 192, 0, c.stream>>>(
       c.g, c.active_list.as<int>(), c.active.as<unsigned char>(), F, c.gcap, w);
   // liquid volume fractions for the viscosity (updateLiquidPhi :3353-3367)
-  if (c.prm.viscosity > 0.0)
+  if (c.prm.viscosity > 0.0 && c.np > 0)
     ++c.launches, k_volume_fractions<R><<<(unsigned)c.n_active, 64, 0, c.stream>>>(
         c.g, c.active_list.as<int>(), c.active.as<unsigned char>(), F, c.gcap);
   return cudaGetLastError();
@@ -1533,13 +1680,24 @@ cudaError_t constrain_liquid_velocity(Context& c) {
 }
 
 template <typename R>
+static void elasto_g2p_t(Context& c, double dt, bool g2p, bool advect) {
+  ++c.launches, k_g2p_elasto<R><<<nblk(c.ne, 128), 128, 0, c.stream>>>(
+      c.g, c.active.as<unsigned char>(), c.ebuf[c.ecur].as<R>(), c.ecap, c.ne,
+      c.ekey.as<long long>() + c.ecur * c.ecap, c.edelta.as<int>() + c.ecur * c.ecap,
+      c.efield.as<R>(), c.gcap, (R)c.prm.elasto_flip, (R)c.prm.elasto_flip_asym,
+      (R)c.prm.elasto_advect, (R)dt, g2p ? 1 : 0, advect ? 1 : 0);
+}
+
+template <typename R>
 static cudaError_t g2p_t(Context& c, double dt, bool advect) {
-  if (c.np == 0) return cudaSuccess;
+  if (c.np + c.ne == 0) return cudaSuccess;
   ProfScope prof(c, P_G2P);
-  ++c.launches, k_g2p<R><<<nblk(c.np, 128), 128, 0, c.stream>>>(
-      c.g, c.active.as<unsigned char>(), c.pbuf[c.cur].as<R>(), c.pcap, c.np,
-      c.pkey.as<long long>() + c.cur * c.pcap, c.pdelta.as<int>() + c.cur * c.pcap,
-      c.gfield.as<R>(), c.gcap, (R)c.prm.flip_coeff, (R)dt, advect ? 1 : 0);
+  if (c.np > 0)
+    ++c.launches, k_g2p<R><<<nblk(c.np, 128), 128, 0, c.stream>>>(
+        c.g, c.active.as<unsigned char>(), c.pbuf[c.cur].as<R>(), c.pcap, c.np,
+        c.pkey.as<long long>() + c.cur * c.pcap, c.pdelta.as<int>() + c.cur * c.pcap,
+        c.gfield.as<R>(), c.gcap, (R)c.prm.flip_coeff, (R)dt, advect ? 1 : 0);
+  if (c.ne > 0) elasto_g2p_t<R>(c, dt, true, advect);
   return cudaGetLastError();
 }
 
@@ -1548,14 +1706,22 @@ cudaError_t map_grid_to_particles_and_advect(Context& c, double dt, bool advect)
 }
 
 cudaError_t advect_only(Context& c, double dt) {
-  if (c.np == 0) return cudaSuccess;
+  if (c.np + c.ne == 0) return cudaSuccess;
   ProfScope prof(c, P_G2P);
-  if (c.prm.precision == 0)
-    ++c.launches, k_advect<double><<<nblk(c.np, 256), 256, 0, c.stream>>>(c.pbuf[c.cur].as<double>(), c.pcap,
-                                                            c.np, dt);
-  else
-    ++c.launches, k_advect<float><<<nblk(c.np, 256), 256, 0, c.stream>>>(c.pbuf[c.cur].as<float>(), c.pcap,
-                                                           c.np, (float)dt);
+  if (c.np > 0) {
+    if (c.prm.precision == 0)
+      ++c.launches, k_advect<double><<<nblk(c.np, 256), 256, 0, c.stream>>>(
+          c.pbuf[c.cur].as<double>(), c.pcap, c.np, dt);
+    else
+      ++c.launches, k_advect<float><<<nblk(c.np, 256), 256, 0, c.stream>>>(
+          c.pbuf[c.cur].as<float>(), c.pcap, c.np, (float)dt);
+  }
+  if (c.ne > 0) {
+    if (c.prm.precision == 0)
+      elasto_g2p_t<double>(c, dt, false, true);
+    else
+      elasto_g2p_t<float>(c, dt, false, true);
+  }
   return cudaGetLastError();
 }
 
@@ -1579,7 +1745,18 @@ cudaError_t num_substeps(Context& c, double dt, int* n) {
   double h;
   WCG_TRY(fetch(c, dsc + 7, 1, &h));
   const double max_fluid_vel = std::sqrt(h);
-  const double max_elasto_vel = 0.0;
+  double he = 0.0;
+  if (c.ne > 0) {
+    if (c.prm.precision == 0)
+      ++c.launches, k_maxvel2_elasto<double><<<kRedBlocks, kRedThreads, 0, c.stream>>>(
+          c.ebuf[c.ecur].as<double>(), c.ecap, c.ne, part);
+    else
+      ++c.launches, k_maxvel2_elasto<float><<<kRedBlocks, kRedThreads, 0, c.stream>>>(
+          c.ebuf[c.ecur].as<float>(), c.ecap, c.ne, part);
+    ++c.launches, k_reduce_max<<<1, kRedThreads, 0, c.stream>>>(part, kRedBlocks, dsc + 7);
+    WCG_TRY(fetch(c, dsc + 7, 1, &he));
+  }
+  const double max_elasto_vel = std::sqrt(he);
   const double cell = c.prm.dx;
   const double max_elasto_dt = std::min(cell / std::max(1e-63, max_elasto_vel) / 3.0, 1.0 / 30.0);
   const double max_fluid_dt = std::min(cell / std::max(1e-63, max_fluid_vel) * 3.0, 1.0 / 30.0);

@@ -34,6 +34,9 @@ class SceneParams:
     maxiters: int = 1000
     viscosity: float = 0.0        # LiquidInfo::viscosity; 0 = compute_viscosity off
     viscosity_substeps: int = 1   # LinearizedImplicitEuler viscosity sub-steps
+    elasto_flip_coeff: float = 0.95       # LiquidInfo elasto_flip_coeff
+    elasto_flip_asym_coeff: float = 1.0   # LiquidInfo elasto_flip_asym_coeff
+    elasto_advect_coeff: float = 1.0      # LiquidInfo elasto_advect_coeff
 
 
 def particle_radius(dx: float, ppc: int) -> float:
@@ -121,6 +124,35 @@ def curl_noise_velocity(x: np.ndarray, n: int, sigma_cells: float,
 
 
 @dataclasses.dataclass
+class ElastoSet:
+    """Elasto (cloth / yarn) particles, which the reference stores ahead of
+    the liquid ones (TwoDScene::isFluid, libWetCloth/Core/TwoDScene.cpp:6921).
+    Arrays follow the reference's per-particle members: x4 / v4 = m_x / m_v
+    (position or velocity plus the twist component), B = m_B (row-major 3x3),
+    m4 / fm4 = m_m / m_fluid_m, rest_vol = m_rest_vol, rest_vf =
+    m_rest_volume_fraction, fluid_vol = m_fluid_vol (liquid held in the
+    cloth), shape_factor, orientation = m_orientation, surfel != 0 where
+    m_particle_to_surfel >= 0, radius."""
+
+    x4: np.ndarray
+    v4: np.ndarray
+    B: np.ndarray
+    m4: np.ndarray
+    fm4: np.ndarray
+    rest_vol: np.ndarray
+    rest_vf: np.ndarray
+    fluid_vol: np.ndarray
+    shape_factor: np.ndarray
+    orientation: np.ndarray
+    surfel: np.ndarray
+    radius: np.ndarray
+
+    @property
+    def n(self) -> int:
+        return self.x4.shape[0]
+
+
+@dataclasses.dataclass
 class Scene:
     params: SceneParams
     x: np.ndarray
@@ -130,6 +162,74 @@ class Scene:
     radius: np.ndarray
     C: np.ndarray | None = None
     name: str = ""
+    elasto: ElastoSet | None = None
+
+
+def cloth_sheet(lo, hi, y: float, spacing: float, seed: int, thickness: float = 0.004,
+                density: float = 1320.0, rest_vf: float = 0.5, wetness: float = 0.3,
+                liquid_density: float = 1000.0, speed: float = 0.5,
+                surfel_every: int = 0) -> ElastoSet:
+    """A seeded cloth sheet of vertices on a regular grid in the plane y,
+    spanning [lo, hi] in x and z, with the per-vertex attributes of
+    TwoDSceneXMLParser::loadClothes (App/TwoDSceneXMLParser.cpp:1455-1470):
+    volume = rest area x thickness, mass = density x volume x rest volume
+    fraction.  Each vertex holds liquid of volume wetness x (1 - rest_vf) x
+    volume; velocities, affine matrices, twists, shape factors and normal tilts
+    are seeded random.  surfel_every = k > 0 marks every k-th vertex a
+    surfel."""
+    rng = np.random.default_rng(seed)
+    xs = np.arange(lo[0], hi[0] + 0.5 * spacing, spacing)
+    zs = np.arange(lo[1], hi[1] + 0.5 * spacing, spacing)
+    X, Z = np.meshgrid(xs, zs, indexing="ij")
+    n = X.size
+    x4 = np.zeros((n, 4))
+    x4[:, 0] = X.reshape(-1) + rng.uniform(-0.1, 0.1, n) * spacing
+    x4[:, 1] = y + rng.uniform(-0.1, 0.1, n) * spacing
+    x4[:, 2] = Z.reshape(-1) + rng.uniform(-0.1, 0.1, n) * spacing
+    x4[:, 3] = rng.uniform(-0.5, 0.5, n)
+    v4 = np.zeros((n, 4))
+    v4[:, :3] = rng.normal(0.0, 0.1 * speed, (n, 3))
+    v4[:, 1] -= speed
+    v4[:, 3] = rng.normal(0.0, 1.0, n)
+    B = rng.normal(0.0, 1.0, (n, 9))
+    vol = spacing * spacing * thickness
+    mass = density * vol * rest_vf
+    m4 = np.zeros((n, 4))
+    m4[:, :3] = mass
+    m4[:, 3] = mass * thickness * thickness * 0.25
+    fvol = wetness * (1.0 - rest_vf) * vol
+    fm4 = np.zeros((n, 4))
+    fm4[:, :3] = liquid_density * fvol
+    tilt = rng.normal(0.0, 0.2, (n, 3))
+    tilt[:, 1] = 1.0
+    orientation = tilt / np.linalg.norm(tilt, axis=1, keepdims=True)
+    surfel = np.zeros(n, dtype=np.int32)
+    if surfel_every > 0:
+        surfel[::surfel_every] = 1
+        v4[surfel != 0] = 0.0
+    return ElastoSet(x4=x4, v4=v4, B=B, m4=m4, fm4=fm4, rest_vol=np.full(n, vol),
+                     rest_vf=np.full(n, rest_vf), fluid_vol=np.full(n, fvol),
+                     shape_factor=rng.uniform(0.2, 0.8, n), orientation=orientation,
+                     surfel=surfel, radius=np.full(n, 0.5 * thickness))
+
+
+def liquid_on_sheet(n_cells: int = 32, ppc: int = 8, seed: int = 3, sheet_spacing=None,
+                    surfel_every: int = 0) -> Scene:
+    """A falling liquid sphere (r 0.15 at (0.5, 0.75, 0.5), v = (0, -1, 0)
+    plus a spin of 3 rad/s about y) above a cloth sheet at y = 0.4 spanning
+    [0.1, 0.9] in x and z."""
+    dx = 1.0 / n_cells
+    prm = SceneParams(dx=dx)
+    x = liquid_block(dx, (0.35, 0.6, 0.35), (0.65, 0.9, 0.65), ppc, seed)
+    c = np.array([0.5, 0.75, 0.5])
+    x = x[np.linalg.norm(x - c, axis=1) <= 0.15]
+    v = np.cross(np.array([0.0, 3.0, 0.0]), x - c)
+    v[:, 1] = -1.0
+    m, vol, r = attributes(x.shape[0], dx, ppc, prm.liquid_density)
+    h = sheet_spacing if sheet_spacing is not None else 0.5 * dx
+    sheet = cloth_sheet((0.1, 0.1), (0.9, 0.9), 0.4, h, seed + 1, surfel_every=surfel_every)
+    return Scene(prm, x, v, m, vol, r, elasto=sheet,
+                 name=f"liquid_on_sheet_{n_cells}^3_{ppc}ppc_{sheet.n}v")
 
 
 def dam_break(n_cells: int = 64, ppc: int = 8, seed: int = 0,

@@ -38,6 +38,9 @@ def make_params(p, precision=_capi.WCG_FP64, refine_inner_tol=0.0,
     prm.solver = solver
     prm.viscosity = getattr(p, "viscosity", 0.0)
     prm.viscosity_substeps = getattr(p, "viscosity_substeps", 1)
+    prm.elasto_flip_coeff = getattr(p, "elasto_flip_coeff", 0.95)
+    prm.elasto_flip_asym_coeff = getattr(p, "elasto_flip_asym_coeff", 1.0)
+    prm.elasto_advect_coeff = getattr(p, "elasto_advect_coeff", 1.0)
     return prm
 
 
@@ -51,6 +54,8 @@ class FluidScene:
         self.precision = prm.precision
         if scene is not None:
             self.upload(scene.x, scene.v, scene.C, scene.mass, scene.vol, scene.radius)
+            if getattr(scene, "elasto", None) is not None:
+                self.upload_elasto(scene.elasto)
 
     def close(self):
         if getattr(self, "h", None):
@@ -78,6 +83,35 @@ class FluidScene:
     @property
     def num_particles(self):
         return self.L.wcg_num_particles(self.h)
+
+    def upload_elasto(self, e):
+        """Elasto particles (a scenes.ElastoSet): the reference's particles
+        [0, n) ahead of the liquid ones."""
+        arr = lambda a: np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+        cols = [arr(a) for a in (e.x4, e.v4, e.B, e.m4, e.fm4, e.rest_vol, e.rest_vf,
+                                 e.fluid_vol, e.shape_factor, e.orientation)]
+        surf = np.ascontiguousarray(e.surfel, dtype=np.int32)
+        check(self.L.wcg_upload_elasto(self.h, e.n, *[_dp(c) for c in cols],
+                                       surf.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
+
+    @property
+    def num_elasto(self):
+        return self.L.wcg_num_elasto(self.h)
+
+    def download_elasto(self):
+        """(x4, v4, B9) of the elasto particles in their original order."""
+        n = self.num_elasto
+        x4 = np.empty((n, 4))
+        v4 = np.empty((n, 4))
+        B = np.empty((n, 9))
+        check(self.L.wcg_download_elasto(self.h, _dp(x4), _dp(v4), _dp(B)))
+        return x4, v4, B
+
+    def upload_field(self, name, values):
+        """Set "u_x/y/z" or "vel_x/y/z" node velocities (inactive buckets
+        ignored)."""
+        v = np.ascontiguousarray(values, dtype=np.float64).reshape(-1)
+        check(self.L.wcg_upload_field(self.h, name.encode(), _dp(v), v.shape[0]))
 
     def download(self):
         n = self.num_particles

@@ -33,9 +33,14 @@ def lib():
                                  ctypes.c_int, ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _D, _D]
         L.wco_destroy.argtypes = [ctypes.c_void_p]
         L.wco_set_viscosity.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
+        L.wco_set_elasto.argtypes = [ctypes.c_void_p, ctypes.c_int] + [_D] * 10 + [_I, _D]
+        L.wco_set_elasto_coeffs.argtypes = [ctypes.c_void_p] + [ctypes.c_double] * 3
+        L.wco_transfer.argtypes = [ctypes.c_void_p, ctypes.c_double]
         L.wco_step.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
         L.wco_step.restype = ctypes.c_int
         L.wco_substep.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
+        L.wco_num_substeps.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        L.wco_num_substeps.restype = ctypes.c_int
         L.wco_size.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
         L.wco_size.restype = ctypes.c_longlong
         L.wco_get_f.argtypes = [ctypes.c_void_p, ctypes.c_char_p, _D]
@@ -50,6 +55,28 @@ def lib():
 
 def _dp(a):
     return a.ctypes.data_as(_D)
+
+
+def set_elasto(fn_set, fn_coeffs, h, scene, keep):
+    """Pass a scene's elasto particles and elasto coefficients to a created
+    scene handle (no-op for liquid-only scenes)."""
+    p = scene.params
+    fn_coeffs(h, getattr(p, "elasto_flip_coeff", 0.95), getattr(p, "elasto_flip_asym_coeff", 1.0),
+              getattr(p, "elasto_advect_coeff", 1.0))
+    e = getattr(scene, "elasto", None)
+    if e is None or e.n == 0:
+        return
+
+    def arr(a):
+        a = np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+        keep.append(a)
+        return _dp(a)
+
+    surf = np.ascontiguousarray(e.surfel, dtype=np.int32)
+    keep.append(surf)
+    fn_set(h, e.n, arr(e.x4), arr(e.v4), arr(e.B), arr(e.m4), arr(e.fm4), arr(e.rest_vol),
+           arr(e.rest_vf), arr(e.fluid_vol), arr(e.shape_factor), arr(e.orientation),
+           surf.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), arr(e.radius))
 
 
 class OracleScene:
@@ -75,6 +102,7 @@ class OracleScene:
         mu = getattr(p, "viscosity", 0.0)
         if mu > 0.0:
             L.wco_set_viscosity(self.h, mu, getattr(p, "viscosity_substeps", 1))
+        set_elasto(L.wco_set_elasto, L.wco_set_elasto_coeffs, self.h, scene, self._keep)
 
     def close(self):
         if self.h:
@@ -89,6 +117,15 @@ class OracleScene:
 
     def step(self, dt, snapshot=True):
         return self.L.wco_step(self.h, dt, 1 if snapshot else 0)
+
+    def num_substeps(self, dt):
+        """CFL sub-step count of WetClothCore::stepSystem for dt."""
+        return self.L.wco_num_substeps(self.h, dt)
+
+    def transfer(self, dt):
+        """Grid, P2G, then G2P from the P2G velocities and advection (no
+        solve); snapshots as in a step."""
+        self.L.wco_transfer(self.h, dt)
 
     def get(self, name):
         n = self.L.wco_size(self.h, name.encode())

@@ -49,12 +49,38 @@ def _lib(omp: bool):
         L.wcref_timers.argtypes = [ctypes.c_void_p, _D]
         L.wcref_amg_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), _D]
         L.wcref_set_viscosity.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
+        _I = ctypes.POINTER(ctypes.c_int)
+        L.wcref_set_elasto.argtypes = [ctypes.c_void_p, ctypes.c_int] + [_D] * 10 + [_I, _D]
+        L.wcref_set_elasto_coeffs.argtypes = [ctypes.c_void_p] + [ctypes.c_double] * 3
+        L.wcref_transfer.argtypes = [ctypes.c_void_p, ctypes.c_double]
         _libs[omp] = L
     return _libs[omp]
 
 
 def _dp(a):
     return a.ctypes.data_as(_D)
+
+
+def set_elasto(fn_set, fn_coeffs, h, scene, keep):
+    """Pass a scene's elasto particles and elasto coefficients to a created
+    scene handle (no-op for liquid-only scenes)."""
+    p = scene.params
+    fn_coeffs(h, getattr(p, "elasto_flip_coeff", 0.95), getattr(p, "elasto_flip_asym_coeff", 1.0),
+              getattr(p, "elasto_advect_coeff", 1.0))
+    e = getattr(scene, "elasto", None)
+    if e is None or e.n == 0:
+        return
+
+    def arr(a):
+        a = np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+        keep.append(a)
+        return _dp(a)
+
+    surf = np.ascontiguousarray(e.surfel, dtype=np.int32)
+    keep.append(surf)
+    fn_set(h, e.n, arr(e.x4), arr(e.v4), arr(e.B), arr(e.m4), arr(e.fm4), arr(e.rest_vol),
+           arr(e.rest_vf), arr(e.fluid_vol), arr(e.shape_factor), arr(e.orientation),
+           surf.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), arr(e.radius))
 
 
 class RefScene:
@@ -80,6 +106,8 @@ class RefScene:
         mu = getattr(p, "viscosity", 0.0)
         if mu > 0.0:
             self.L.wcref_set_viscosity(self.h, mu, getattr(p, "viscosity_substeps", 1))
+        set_elasto(self.L.wcref_set_elasto, self.L.wcref_set_elasto_coeffs, self.h, scene,
+                   self._keep)
 
     def close(self):
         if self.h:
@@ -94,6 +122,11 @@ class RefScene:
 
     def step(self, dt: float, snapshot: bool = True) -> int:
         return self.L.wcref_step(self.h, dt, 1 if snapshot else 0)
+
+    def transfer(self, dt: float) -> None:
+        """Grid, P2G, then G2P from the P2G velocities and advection (no
+        solve); snapshots as in a step."""
+        self.L.wcref_transfer(self.h, dt)
 
     def get(self, name: str) -> np.ndarray:
         n = self.L.wcref_size(self.h, name.encode())

@@ -146,14 +146,27 @@ void snap_particles(Harness& h, const std::string& tag) {
   std::vector<double>& x = h.f[tag + "x"];
   std::vector<double>& v = h.f[tag + "v"];
   std::vector<double>& c = h.f[tag + "C"];
+  std::vector<double>& x4 = h.f[tag + "x4"];
+  std::vector<double>& ev = h.f[tag + "ev4"];
+  std::vector<double>& eb = h.f[tag + "eB"];
   x.resize((size_t)np * 3);
   v.resize((size_t)np * 3);
   c.resize((size_t)np * 9);
+  x4.resize((size_t)np * 4);
+  ev.resize((size_t)np * 4);
+  eb.resize((size_t)np * 9);
   for (int i = 0; i < np; ++i) {
     for (int r = 0; r < 3; ++r) {
       x[i * 3 + r] = s.m_x(i * 4 + r);
       v[i * 3 + r] = s.m_fluid_v(i * 4 + r);
-      for (int q = 0; q < 3; ++q) c[i * 9 + r * 3 + q] = s.m_fB(i * 3 + r, q);
+      for (int q = 0; q < 3; ++q) {
+        c[i * 9 + r * 3 + q] = s.m_fB(i * 3 + r, q);
+        eb[i * 9 + r * 3 + q] = s.m_B(i * 3 + r, q);
+      }
+    }
+    for (int r = 0; r < 4; ++r) {
+      x4[i * 4 + r] = s.m_x(i * 4 + r);
+      ev[i * 4 + r] = s.m_v(i * 4 + r);
     }
   }
 }
@@ -213,6 +226,15 @@ void snap_p2g(Harness& h) {
   dense(h, "vol_x", s.m_node_vol_x);
   dense(h, "vol_y", s.m_node_vol_y);
   dense(h, "vol_z", s.m_node_vol_z);
+  dense(h, "vel_x", s.m_node_vel_x);
+  dense(h, "vel_y", s.m_node_vel_y);
+  dense(h, "vel_z", s.m_node_vel_z);
+  dense(h, "shape_factor_x", s.m_node_shape_factor_x);
+  dense(h, "shape_factor_y", s.m_node_shape_factor_y);
+  dense(h, "shape_factor_z", s.m_node_shape_factor_z);
+  dense(h, "orientation_x", s.m_node_orientation_x, 3);
+  dense(h, "orientation_y", s.m_node_orientation_y, 3);
+  dense(h, "orientation_z", s.m_node_orientation_z, 3);
   dense(h, "psi_x", s.m_node_psi_x);
   dense(h, "psi_y", s.m_node_psi_y);
   dense(h, "psi_z", s.m_node_psi_z);
@@ -273,6 +295,41 @@ void snap_system(Harness& h) {
   h.f["b"] = e.m_fine_pressure_rhs;
   h.f["b"].resize(A.n);
   dense_vi(h, "dof_index", e.m_fine_global_indices);
+}
+
+// One liquid particle, attribute set of TwoDScene::sampleLiquidDistanceFields
+// (Core/TwoDScene.cpp:5564-5605).
+void set_liquid_particle(TwoDScene& s, int i, const double* x3, const double* v3,
+                         const double* C9, double fmass, double fvol, double radius) {
+  s.m_x.segment<4>(i * 4) = Vector4s(x3[0], x3[1], x3[2], 0.0);
+  s.m_rest_x.segment<4>(i * 4) = s.m_x.segment<4>(i * 4);
+  s.m_v.segment<4>(i * 4).setZero();
+  s.m_dv.segment<4>(i * 4).setZero();
+  s.m_fluid_v.segment<4>(i * 4) = Vector4s(v3[0], v3[1], v3[2], 0.0);
+  s.m_m.segment<4>(i * 4).setZero();
+  s.m_fluid_m.segment<3>(i * 4).setConstant(fmass);
+  s.m_fluid_m(i * 4 + 3) = fmass * radius * radius * 0.4;
+  s.m_fluid_vol(i) = fvol;
+  s.m_vol(i) = 0.0;
+  s.m_rest_vol(i) = 0.0;
+  s.m_shape_factor(i) = 0.0;
+  s.m_radius(i * 2 + 0) = s.m_radius(i * 2 + 1) = radius;
+  s.m_volume_fraction(i) = 0.0;
+  s.m_rest_volume_fraction(i) = 0.0;
+  s.m_fixed[i] = 0U;
+  s.m_twist[i] = false;
+  s.m_particle_rest_length(i) = radius * 2.0;
+  s.m_particle_rest_area(i) = M_PI * radius * radius;
+  s.m_particle_group[i] = 0;
+  for (int r = 0; r < 3; ++r)
+    for (int q = 0; q < 3; ++q) s.m_fB(i * 3 + r, q) = C9 ? C9[r * 3 + q] : 0.0;
+  s.m_B.block<3, 3>(i * 3, 0).setZero();
+  s.m_is_strand_tip[i] = false;
+  s.m_div[i].resize(0);
+  s.m_particle_to_surfel[i] = -1;
+  s.m_inside[i] = 0U;
+  s.m_classifier[i] = PC_o;
+  s.m_orientation.segment<3>(i * 3).setZero();
 }
 
 }  // namespace
@@ -380,37 +437,8 @@ void* wcref_create(double dx, const double* g, double rho, double flip,
   s.resizeParticleSystem(np);
   s.m_fluids.resize(np);
   for (int i = 0; i < np; ++i) {
-    s.m_x.segment<4>(i * 4) = Vector4s(x3[i * 3], x3[i * 3 + 1], x3[i * 3 + 2], 0.0);
-    s.m_rest_x.segment<4>(i * 4) = s.m_x.segment<4>(i * 4);
-    s.m_v.segment<4>(i * 4).setZero();
-    s.m_dv.segment<4>(i * 4).setZero();
-    s.m_fluid_v.segment<4>(i * 4) =
-        Vector4s(v3[i * 3], v3[i * 3 + 1], v3[i * 3 + 2], 0.0);
-    s.m_m.segment<4>(i * 4).setZero();
-    s.m_fluid_m.segment<3>(i * 4).setConstant(fmass[i]);
-    s.m_fluid_m(i * 4 + 3) = fmass[i] * radius[i] * radius[i] * 0.4;
-    s.m_fluid_vol(i) = fvol[i];
-    s.m_vol(i) = 0.0;
-    s.m_rest_vol(i) = 0.0;
-    s.m_shape_factor(i) = 0.0;
-    s.m_radius(i * 2 + 0) = s.m_radius(i * 2 + 1) = radius[i];
-    s.m_volume_fraction(i) = 0.0;
-    s.m_rest_volume_fraction(i) = 0.0;
-    s.m_fixed[i] = 0U;
-    s.m_twist[i] = false;
-    s.m_particle_rest_length(i) = radius[i] * 2.0;
-    s.m_particle_rest_area(i) = M_PI * radius[i] * radius[i];
-    s.m_particle_group[i] = 0;
-    for (int r = 0; r < 3; ++r)
-      for (int q = 0; q < 3; ++q)
-        s.m_fB(i * 3 + r, q) = C9 ? C9[i * 9 + r * 3 + q] : 0.0;
-    s.m_B.block<3, 3>(i * 3, 0).setZero();
-    s.m_is_strand_tip[i] = false;
-    s.m_div[i].resize(0);
-    s.m_particle_to_surfel[i] = -1;
-    s.m_inside[i] = 0U;
-    s.m_classifier[i] = PC_o;
-    s.m_orientation.segment<3>(i * 3).setZero();
+    set_liquid_particle(s, i, x3 + i * 3, v3 + i * 3, C9 ? C9 + i * 9 : nullptr, fmass[i],
+                        fvol[i], radius[i]);
     s.m_fluids[i] = i;
   }
   s.updateRestPos();
@@ -612,6 +640,110 @@ void wcref_set_viscosity(void* hp, double mu, int substeps) {
   h->stepper = std::make_shared<LinearizedImplicitEuler>(
       1e-6, h->p.criterion, 1e-6, 1e-6, h->p.maxiters, 1, substeps > 0 ? substeps : 1, 1);
   h->stepper->setUseApic(true);
+}
+
+// Elasto (cloth/yarn) particles: the scene's particles become [0, ne) elasto
+// followed by the current liquid particles (TwoDScene::isFluid :6921,
+// getNumElastoParticles :5212-5217).  Per particle: x4/v4 (position, velocity
+// and twist), B9 (row-major affine matrix m_B), m4/fm4 (m_m, m_fluid_m),
+// m_rest_vol, m_rest_volume_fraction, m_fluid_vol, m_shape_factor,
+// m_orientation (3), surfel (m_particle_to_surfel >= 0 when nonzero; only its
+// sign is read on the hot path), radius.  Call before the first step.
+void wcref_set_elasto(void* hp, int ne, const double* x4, const double* v4, const double* B9,
+                      const double* m4, const double* fm4, const double* rest_vol,
+                      const double* rest_vf, const double* fluid_vol, const double* shape_factor,
+                      const double* orient3, const int* surfel, const double* radius) {
+  Harness* h = (Harness*)hp;
+  TwoDScene& s = *h->scene;
+  const int nl = (int)s.m_fluids.size();
+  std::vector<double> lx(nl * 3), lv(nl * 3), lC(nl * 9), lm(nl), lvol(nl), lr(nl);
+  for (int k = 0; k < nl; ++k) {
+    const int i = s.m_fluids[k];
+    for (int r = 0; r < 3; ++r) {
+      lx[k * 3 + r] = s.m_x(i * 4 + r);
+      lv[k * 3 + r] = s.m_fluid_v(i * 4 + r);
+      for (int q = 0; q < 3; ++q) lC[k * 9 + r * 3 + q] = s.m_fB(i * 3 + r, q);
+    }
+    lm[k] = s.m_fluid_m(i * 4);
+    lvol[k] = s.m_fluid_vol(i);
+    lr[k] = s.m_radius(i * 2);
+  }
+  s.resizeParticleSystem(ne + nl);
+  s.m_fluids.resize(nl);
+  for (int i = 0; i < ne; ++i) {
+    s.m_x.segment<4>(i * 4) = Vector4s(x4[i * 4], x4[i * 4 + 1], x4[i * 4 + 2], x4[i * 4 + 3]);
+    s.m_rest_x.segment<4>(i * 4) = s.m_x.segment<4>(i * 4);
+    s.m_v.segment<4>(i * 4) = Vector4s(v4[i * 4], v4[i * 4 + 1], v4[i * 4 + 2], v4[i * 4 + 3]);
+    s.m_dv.segment<4>(i * 4).setZero();
+    s.m_fluid_v.segment<4>(i * 4).setZero();
+    s.m_m.segment<4>(i * 4) = Vector4s(m4[i * 4], m4[i * 4 + 1], m4[i * 4 + 2], m4[i * 4 + 3]);
+    s.m_fluid_m.segment<4>(i * 4) =
+        Vector4s(fm4[i * 4], fm4[i * 4 + 1], fm4[i * 4 + 2], fm4[i * 4 + 3]);
+    s.m_vol(i) = rest_vol[i];
+    s.m_rest_vol(i) = rest_vol[i];
+    s.m_fluid_vol(i) = fluid_vol[i];
+    s.m_shape_factor(i) = shape_factor[i];
+    s.m_radius(i * 2 + 0) = s.m_radius(i * 2 + 1) = radius[i];
+    s.m_volume_fraction(i) = rest_vf[i];
+    s.m_rest_volume_fraction(i) = rest_vf[i];
+    s.m_fixed[i] = 0U;
+    s.m_twist[i] = false;
+    s.m_particle_rest_length(i) = radius[i] * 2.0;
+    s.m_particle_rest_area(i) = M_PI * radius[i] * radius[i];
+    s.m_particle_group[i] = 0;
+    for (int r = 0; r < 3; ++r)
+      for (int q = 0; q < 3; ++q) s.m_B(i * 3 + r, q) = B9[i * 9 + r * 3 + q];
+    s.m_fB.block<3, 3>(i * 3, 0).setZero();
+    s.m_is_strand_tip[i] = false;
+    s.m_div[i].resize(0);
+    s.m_particle_to_surfel[i] = surfel[i] ? i : -1;
+    s.m_inside[i] = 0U;
+    s.m_classifier[i] = PC_NONE;
+    s.m_orientation.segment<3>(i * 3) =
+        Vector3s(orient3[i * 3], orient3[i * 3 + 1], orient3[i * 3 + 2]);
+  }
+  for (int k = 0; k < nl; ++k) {
+    set_liquid_particle(s, ne + k, &lx[k * 3], &lv[k * 3], &lC[k * 9], lm[k], lvol[k], lr[k]);
+    s.m_fluids[k] = ne + k;
+  }
+  s.updateRestPos();
+}
+
+// LiquidInfo::elasto_flip_coeff, elasto_flip_asym_coeff, elasto_advect_coeff
+void wcref_set_elasto_coeffs(void* hp, double flip, double asym, double advect) {
+  LiquidInfo& li = ((Harness*)hp)->scene->getLiquidInfo();
+  li.elasto_flip_coeff = flip;
+  li.elasto_flip_asym_coeff = asym;
+  li.elasto_advect_coeff = advect;
+}
+
+// The transfers alone, in WetClothCore::stepSystem order with the solve left
+// out: grid, weights, APIC P2G (+ saturation/psi/pore pressure), then G2P
+// straight from the P2G node velocities and advection.  Snapshots as in a
+// step ("g2p_" / "adv_" particle tags).
+int wcref_transfer(void* hp, double dt) {
+  Harness* h = (Harness*)hp;
+  TwoDScene& s = *h->scene;
+  LinearizedImplicitEuler& e = *h->stepper;
+  s.updateParticleBoundingBox();
+  s.rebucketizeParticles();
+  s.resampleNodes();
+  snap_grid(*h);
+  s.computeWeights(dt);
+  s.updateLiquidPhi(dt);
+  s.updateSolidPhi();
+  s.updateSolidWeights();
+  s.saveParticleVelocity();
+  s.mapParticleNodesAPIC();
+  s.saveFluidVelocity();
+  s.mapParticleSaturationPsiNodes();
+  s.updatePorePressureNodes();
+  snap_p2g(*h);
+  s.mapNodeParticlesAPIC();
+  snap_particles(*h, "g2p_");
+  e.advectScene(s, dt);
+  snap_particles(*h, "adv_");
+  return 0;
 }
 
 // AMGPCGSolveSparse iterations and residual of the last snapshot step

@@ -28,6 +28,7 @@ typedef struct {
   int maxiters, mic;
   double visc;       /* LiquidInfo::viscosity; 0: compute_viscosity off */
   int visc_substeps; /* LinearizedImplicitEuler::m_viscosity_substeps */
+  double e_flip, e_asym, e_advect; /* elasto_flip_coeff, _asym_coeff, elasto_advect_coeff */
 } Params;
 
 typedef struct {
@@ -47,8 +48,14 @@ typedef struct {
 
 typedef struct {
   Params p;
-  int np;
+  int np;  /* all particles: [0, ne) elasto, then liquid (TwoDScene::isFluid :6921) */
+  int ne;
   double *x, *v, *C, *m, *vol, *rad;  /* particle state (x3, v3, C9) */
+  /* elasto particles only (liquid entries are 0): m(a) + m_fluid(a) per axis,
+   * m_rest_vol, m_rest_volume_fraction, m_shape_factor, m_orientation (3),
+   * twist angle and twist velocity (4th components of m_x, m_v), surfel flag */
+  double *em, *rvol, *rvf, *sf, *ori, *xt, *vt;
+  unsigned char* surf;
   /* grid */
   double bbmin[3], bbmax[3], org[3], bs;
   int ni, nj, nk;
@@ -62,6 +69,9 @@ typedef struct {
   Pairs pu, pv, pw, pp;
   /* node fields */
   double *mass[3], *vel[3], *vol_f[3], *sat[3], *psi[3], *wgt[3], *svel[3];
+  /* elasto P2G: m_node_mass, m_node_vel, m_node_vol, m_node_shape_factor,
+   * m_node_orientation (3 per node) */
+  double *emass[3], *evel[3], *evol[3], *esf[3], *eori[3];
   double *sat_p, *psi_p, *pore_p, *lphi, *sphi, *pressure;
   double *vf_c, *vf_e[3];  /* liquid volume fractions: cell centres, x/y/z edges */
   double *rhs[3], *vstar[3], *invC[3], *psifs[3], *psisf[3], *mshdvm[3], *mfhdvm[3];
@@ -75,7 +85,7 @@ typedef struct {
   int last_iters;
   double last_res;
   double timers[12];
-  Snap snaps[160];
+  Snap snaps[256];
   int nsnaps;
 } Scene;
 
@@ -337,7 +347,8 @@ static void resample_nodes(Scene* s) {
             const int I = lo[0] + i, J = lo[1] + j, K = lo[2] + k;
             const int hi = I >= 0 ? I / NN : -1, hj = J >= 0 ? J / NN : -1, hk = K >= 0 ? K / NN : -1;
             if (hi < 0 || hj < 0 || hk < 0 || hi >= s->ni || hj >= s->nj || hk >= s->nk) continue;
-            s->act[bucket_index(s, hi, hj, hk)] = 1;  /* liquid particles are soft */
+            /* only soft particles (not surfels) activate (isSoft :697) */
+            if (!s->surf[p]) s->act[bucket_index(s, hi, hj, hk)] = 1;
           }
     }
   }
@@ -460,7 +471,11 @@ static void build_pairs(Scene* s, Pairs* P, const double* W, int t) {
   free(cursor);
 }
 
-/* TwoDScene::mapParticleNodesAPIC liquid branch (TwoDScene.cpp:6609-6919) */
+/* TwoDScene::mapParticleNodesAPIC (TwoDScene.cpp:6609-6919), both branches:
+ * elasto particles (p < ne) add (m + m_fluid) and their momentum to the solid
+ * phase and, unless surfels, their solid volume (m_rest_vol x rest volume
+ * fraction), held liquid volume, shape factor and orientation; liquid
+ * particles add to the liquid phase. */
 static void p2g(Scene* s) {
   const double dV = s->p.dx * s->p.dx * s->p.dx;
   Pairs* PP[3] = {&s->pu, &s->pv, &s->pw};
@@ -469,6 +484,8 @@ static void p2g(Scene* s) {
     for (long long n = 0; n < s->nnode; ++n) {
       s->mass[a][n] = s->vel[a][n] = s->vol_f[a][n] = 0;
       s->psi[a][n] = s->sat[a][n] = 0;
+      s->emass[a][n] = s->evel[a][n] = s->evol[a][n] = s->esf[a][n] = 0;
+      s->eori[a][n * 3] = s->eori[a][n * 3 + 1] = s->eori[a][n * 3 + 2] = 0;
       if (!s->act[n >> 6]) continue;
       const int I = (int)((n >> 6) % s->ni) * NN + (int)(n & 3);
       const long long bb = n >> 6;
@@ -478,7 +495,8 @@ static void p2g(Scene* s) {
       const double off[3] = {a == 0 ? 0.0 : 0.5, a == 1 ? 0.0 : 0.5, a == 2 ? 0.0 : 0.5};
       const double np[3] = {node_coord(s, 0, I, off[0]), node_coord(s, 1, J, off[1]),
                             node_coord(s, 2, K, off[2])};
-      double pf = 0, mf = 0, vf = 0, vs = 0, vfe = 0;
+      double ps = 0, ms = 0, vs = 0, pf = 0, mf = 0, vf = 0, vfe = 0, shp = 0, shw = 0;
+      double o[3] = {0, 0, 0};
       for (int e = PP[a]->start[n]; e < PP[a]->start[n + 1]; ++e) {
         const int p = PP[a]->pid[e];
         const double w = W[a][p * 27 + PP[a]->slot[e]];
@@ -486,15 +504,38 @@ static void p2g(Scene* s) {
         const double dot = (C[0] * (np[0] - s->x[p * 3]) + C[1] * (np[1] - s->x[p * 3 + 1])) +
                            C[2] * (np[2] - s->x[p * 3 + 2]);
         const double vel = s->v[p * 3 + a] + dot;
-        pf += vel * s->m[p] * w;
-        mf += s->m[p] * w;
-        vf += s->vol[p] * w;
+        if (p < s->ne) {
+          const double mm = s->em[p * 3 + a];
+          ps += vel * mm * w;
+          ms += mm * w;
+          if (!s->surf[p]) {
+            vs += s->rvol[p] * s->rvf[p] * w;
+            vfe += s->vol[p] * w;
+            shp += s->sf[p] * w;
+            shw += w;
+            for (int q = 0; q < 3; ++q) o[q] += s->ori[p * 3 + q] * w;
+          }
+        } else {
+          pf += vel * s->m[p] * w;
+          mf += s->m[p] * w;
+          vf += s->vol[p] * w;
+        }
       }
+      if (ms > 1e-20) s->evel[a][n] = ps / ms;
       if (mf > 1e-20) s->vel[a][n] = pf / mf;
+      if (shw > 1e-20) shp /= shw;
+      s->emass[a][n] = ms;
+      s->evol[a][n] = vs + vfe;
       s->mass[a][n] = mf;
       s->vol_f[a][n] = vf;
       s->psi[a][n] = clampd(vs / dV, 0.0, 1.0);
       s->sat[a][n] = clampd((vf + vfe) / fmax(1e-20, dV - vs), 0.0, 1.0);
+      /* Vector3s::norm, then orientation /= norm (Eigen: per component) */
+      const double lo = sqrt(o[0] * o[0] + o[1] * o[1] + o[2] * o[2]);
+      if (lo > 1e-20)
+        for (int q = 0; q < 3; ++q) o[q] /= lo;
+      for (int q = 0; q < 3; ++q) s->eori[a][n * 3 + q] = o[q];
+      s->esf[a][n] = shp;
     }
   }
 }
@@ -506,6 +547,7 @@ static void liquid_phi(Scene* s) {
     s->lphi[n] = 3.0 * s->bs;
     s->pressure[n] = 0.0;
   }
+  if (s->np == s->ne) return;  /* no liquid particles: nothing else (:3303) */
   const int nc = 3;
   const int sni = (s->ni + nc - 1) / nc, snj = (s->nj + nc - 1) / nc, snk = (s->nk + nc - 1) / nc;
   const double off[3] = {0.5, 0.5, 0.5};
@@ -521,6 +563,7 @@ static void liquid_phi(Scene* s) {
           const long long b = bucket_index(s, i, j, k);
           for (int q = s->sup[b * 2]; q < s->sup[b * 2 + 1]; ++q) {
             const int p = (int)(s->keys[q] & 0xffffffffu);
+            if (p < s->ne) continue;  /* liquid particles only (:3309) */
             const int* lo = &s->base[p * 15 + 12];
             for (int sl = 0; sl < 27; ++sl) {
               const int I = lo[0] + sl % 3, J = lo[1] + (sl / 3) % 3, K = lo[2] + sl / 9;
@@ -599,9 +642,10 @@ static void sat_psi_p(Scene* s) {
     double vl = 0, vs = 0;
     for (int e = s->pp.start[n]; e < s->pp.start[n + 1]; ++e) {
       const int p = s->pp.pid[e];
+      if (s->surf[p]) continue;
       const double w = s->wp[p * 27 + s->pp.slot[e]];
       vl += s->vol[p] * w;
-      vs += 0.0 * w * 0.0;  /* rest volume x rest fraction of liquid particles */
+      vs += s->rvol[p] * w * s->rvf[p];  /* 0 for liquid particles */
     }
     s->psi_p[n] = clampd(vs / dV, 0.0, 1.0);
     s->sat_p[n] = clampd(vl / fmax(1e-20, dV - vs), 0.0, 1.0);
@@ -1217,30 +1261,59 @@ static void constrain(Scene* s) {
     }
 }
 
-/* mapNodeParticlesAPIC liquid branch (TwoDScene.cpp:6936-7000) */
+/* mapNodeParticlesAPIC (TwoDScene.cpp:6936-7090): liquid particles gather the
+ * liquid face velocities into v and C (x flip_coeff); elasto particles other
+ * than surfels gather the solid-phase velocities into v and B, then
+ * v (twist included) *= elasto_advect_coeff and
+ * B = ((f + g) B + (f - g) B^T) / 2 with f = elasto_flip_coeff,
+ * g = elasto_flip_asym_coeff. */
 static void g2p(Scene* s) {
   const double invD = 4.0 / (s->p.dx * s->p.dx);
   double* W[3] = {s->wu, s->wv, s->ww};
   for (int p = 0; p < s->np; ++p) {
-    if (s->inside[p] == 0) continue;
+    const int elasto = p < s->ne;
+    if (elasto ? s->surf[p] : s->inside[p] == 0) continue;
     double fv[3] = {0, 0, 0}, B[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     for (int a = 0; a < 3; ++a) {
       const int* lo = &s->base[p * 15 + a * 3];
       const double off[3] = {a == 0 ? 0.0 : 0.5, a == 1 ? 0.0 : 0.5, a == 2 ? 0.0 : 0.5};
+      const double* U = elasto ? s->evel[a] : s->vel[a];
       for (int sl = 0; sl < 27; ++sl) {
         const int I = lo[0] + sl % 3, J = lo[1] + (sl / 3) % 3, K = lo[2] + sl / 9;
         const long long n = node_of(s, I, J, K);
         if (!node_active(s, n)) continue;
         double np[3];
         stencil_node_pos(s, I, J, K, off, np);
-        const double fnv = s->vel[a][n];
+        const double fnv = U[n];
         const double w = W[a][p * 27 + sl];
         fv[a] += fnv * w;
         for (int q = 0; q < 3; ++q) B[a * 3 + q] += fnv * w * (np[q] - s->x[p * 3 + q]) * invD;
       }
     }
-    for (int a = 0; a < 3; ++a) s->v[p * 3 + a] = fv[a];
-    for (int q = 0; q < 9; ++q) s->C[p * 9 + q] = B[q] * s->p.flip;
+    if (!elasto) {
+      for (int a = 0; a < 3; ++a) s->v[p * 3 + a] = fv[a];
+      for (int q = 0; q < 9; ++q) s->C[p * 9 + q] = B[q] * s->p.flip;
+      continue;
+    }
+    const double ac = s->p.e_advect;
+    for (int a = 0; a < 3; ++a) s->v[p * 3 + a] = fv[a] * ac;
+    s->vt[p] *= ac;
+    const double c1 = s->p.e_flip + s->p.e_asym, c2 = s->p.e_flip - s->p.e_asym;
+    /* the reference assigns the blend into m_B's own block: Eigen evaluates
+     * it coefficient by coefficient in column-major order, so entries above
+     * the diagonal read the already blended entries below it */
+    for (int j = 0; j < 3; ++j)
+      for (int i = 0; i < 3; ++i) B[i * 3 + j] = (c1 * B[i * 3 + j] + c2 * B[j * 3 + i]) * 0.5;
+    for (int q = 0; q < 9; ++q) s->C[p * 9 + q] = B[q];
+  }
+}
+
+/* SceneStepper::advectScene (SceneStepper.cpp:17-41): liquid x += v dt,
+ * elasto x += v dt including the twist */
+static void advect(Scene* s, double dt) {
+  for (int p = 0; p < s->np; ++p) {
+    for (int a = 0; a < 3; ++a) s->x[p * 3 + a] += s->v[p * 3 + a] * dt;
+    if (p < s->ne) s->xt[p] += s->vt[p] * dt;
   }
 }
 
@@ -1250,11 +1323,14 @@ static void alloc_nodes(Scene* s) {
   for (int a = 0; a < 3; ++a) {
     double** F[] = {&s->mass[a], &s->vel[a], &s->vol_f[a], &s->sat[a], &s->psi[a], &s->wgt[a],
                     &s->svel[a], &s->rhs[a], &s->vstar[a], &s->invC[a], &s->psifs[a],
-                    &s->psisf[a], &s->mshdvm[a], &s->mfhdvm[a]};
+                    &s->psisf[a], &s->mshdvm[a], &s->mfhdvm[a], &s->emass[a], &s->evel[a],
+                    &s->evol[a], &s->esf[a]};
     for (size_t k = 0; k < sizeof(F) / sizeof(F[0]); ++k) {
       free(*F[k]);
       *F[k] = (double*)calloc(n, sizeof(double));
     }
+    free(s->eori[a]);
+    s->eori[a] = (double*)calloc(3 * n, sizeof(double));
     free(s->valid[a]);
     s->valid[a] = (unsigned char*)calloc(n, 1);
   }
@@ -1276,14 +1352,46 @@ static void snap_particles(Scene* s, const char* tag) {
   char nm[32];
   snprintf(nm, sizeof nm, "%sx", tag);
   snap_put_f(s, nm, s->x, (long long)s->np * 3);
+  /* m_fluid_v and m_fB: liquid entries, zeros for elasto particles */
+  double* fv = (double*)malloc(sizeof(double) * 3 * (size_t)(s->np > 0 ? s->np : 1));
+  double* fb = (double*)malloc(sizeof(double) * 9 * (size_t)(s->np > 0 ? s->np : 1));
+  for (int p = 0; p < s->np; ++p) {
+    for (int a = 0; a < 3; ++a) fv[p * 3 + a] = p < s->ne ? 0.0 : s->v[p * 3 + a];
+    for (int q = 0; q < 9; ++q) fb[p * 9 + q] = p < s->ne ? 0.0 : s->C[p * 9 + q];
+  }
   snprintf(nm, sizeof nm, "%sv", tag);
-  snap_put_f(s, nm, s->v, (long long)s->np * 3);
+  snap_put_f(s, nm, fv, (long long)s->np * 3);
   snprintf(nm, sizeof nm, "%sC", tag);
-  snap_put_f(s, nm, s->C, (long long)s->np * 9);
+  snap_put_f(s, nm, fb, (long long)s->np * 9);
+  free(fv);
+  free(fb);
+  /* m_x and m_v with their 4th (twist) components, m_B: elasto entries,
+   * zeros for liquid particles */
+  const size_t n = (size_t)(s->np > 0 ? s->np : 1);
+  double* x4 = (double*)calloc(4 * n, sizeof(double));
+  double* v4 = (double*)calloc(4 * n, sizeof(double));
+  double* b9 = (double*)calloc(9 * n, sizeof(double));
+  for (int p = 0; p < s->np; ++p) {
+    for (int a = 0; a < 3; ++a) x4[p * 4 + a] = s->x[p * 3 + a];
+    if (p >= s->ne) continue;
+    x4[p * 4 + 3] = s->xt[p];
+    for (int a = 0; a < 3; ++a) v4[p * 4 + a] = s->v[p * 3 + a];
+    v4[p * 4 + 3] = s->vt[p];
+    for (int q = 0; q < 9; ++q) b9[p * 9 + q] = s->C[p * 9 + q];
+  }
+  snprintf(nm, sizeof nm, "%sx4", tag);
+  snap_put_f(s, nm, x4, (long long)s->np * 4);
+  snprintf(nm, sizeof nm, "%sev4", tag);
+  snap_put_f(s, nm, v4, (long long)s->np * 4);
+  snprintf(nm, sizeof nm, "%seB", tag);
+  snap_put_f(s, nm, b9, (long long)s->np * 9);
+  free(x4);
+  free(v4);
+  free(b9);
 }
 
-/* one sub-step in WetClothCore::stepSystem order (WetClothCore.cpp:115-258) */
-int wco_substep(Scene* s, double dt, int snapshot) {
+/* grid, weights and P2G of a sub-step (WetClothCore.cpp:115-160) */
+static void transfer_in(Scene* s, int snapshot) {
   build_grid(s);
   sort_particles(s);
   resample_nodes(s);
@@ -1332,6 +1440,16 @@ int wco_substep(Scene* s, double dt, int snapshot) {
       snprintf(nm, sizeof nm, "psi_%c", xyz[a]); snap_node(s, nm, s->psi[a]);
       snprintf(nm, sizeof nm, "solid_weight_%c", xyz[a]); snap_node(s, nm, s->wgt[a]);
       snprintf(nm, sizeof nm, "solid_vel_%c", xyz[a]); snap_node(s, nm, s->svel[a]);
+      snprintf(nm, sizeof nm, "mass_%c", xyz[a]); snap_node(s, nm, s->emass[a]);
+      snprintf(nm, sizeof nm, "vel_%c", xyz[a]); snap_node(s, nm, s->evel[a]);
+      snprintf(nm, sizeof nm, "vol_%c", xyz[a]); snap_node(s, nm, s->evol[a]);
+      snprintf(nm, sizeof nm, "shape_factor_%c", xyz[a]); snap_node(s, nm, s->esf[a]);
+      snprintf(nm, sizeof nm, "orientation_%c", xyz[a]);
+      double* t = (double*)malloc(sizeof(double) * 3 * (size_t)s->nnode);
+      for (long long n = 0; n < s->nnode; ++n)
+        for (int q = 0; q < 3; ++q) t[n * 3 + q] = s->act[n >> 6] ? s->eori[a][n * 3 + q] : NAN;
+      snap_put_f(s, nm, t, 3 * s->nnode);
+      free(t);
     }
     snap_node(s, "sat_p", s->sat_p);
     snap_node(s, "psi_p", s->psi_p);
@@ -1340,6 +1458,22 @@ int wco_substep(Scene* s, double dt, int snapshot) {
     if (s->p.visc > 0.0) snap_node(s, "liquid_c_vf", s->vf_c);
     snap_node(s, "solid_phi", s->sphi);
   }
+}
+
+/* G2P and advection of a sub-step (WetClothCore.cpp:228-236) */
+static void transfer_out(Scene* s, double dt, int snapshot) {
+  g2p(s);
+  if (snapshot) snap_particles(s, "g2p_");
+  advect(s, dt);
+  if (snapshot) snap_particles(s, "adv_");
+}
+
+/* one sub-step in WetClothCore::stepSystem order (WetClothCore.cpp:115-258) */
+int wco_substep(Scene* s, double dt, int snapshot) {
+  /* the elasto coupling terms of stepVelocity/projectFine (drag, solid volume
+   * fraction in the pressure system) are not restated: transfers only */
+  if (s->ne > 0) return -1;
+  transfer_in(s, snapshot);
   step_velocity(s, dt);
   if (snapshot) {
     static const char* xyz = "xyz";
@@ -1401,26 +1535,38 @@ int wco_substep(Scene* s, double dt, int snapshot) {
       snap_node(s, nm, s->vel[a]);
     }
   }
-  g2p(s);
-  if (snapshot) snap_particles(s, "g2p_");
-  /* SceneStepper::advectScene (SceneStepper.cpp:17-41) */
-  for (int p = 0; p < s->np; ++p)
-    for (int a = 0; a < 3; ++a) s->x[p * 3 + a] += s->v[p * 3 + a] * dt;
-  if (snapshot) snap_particles(s, "adv_");
+  transfer_out(s, dt, snapshot);
+  return 0;
+}
+
+/* the transfers alone: grid, P2G, then G2P straight from the P2G node
+ * velocities and advection (no solve), snapshots as in a step */
+int wco_transfer(Scene* s, double dt) {
+  transfer_in(s, 1);
+  transfer_out(s, dt, 1);
   return 0;
 }
 
 /* WetClothCore::stepSystem CFL sub-stepping (WetClothCore.cpp:50-62) */
 int wco_num_substeps(Scene* s, double dt) {
   double mv = 0.0;
-  for (int p = 0; p < s->np; ++p) {
+  for (int p = s->ne; p < s->np; ++p) {
     const double q = s->v[p * 3] * s->v[p * 3] + s->v[p * 3 + 1] * s->v[p * 3 + 1] +
                      s->v[p * 3 + 2] * s->v[p * 3 + 2];
     if (q > mv) mv = q;
   }
   mv = sqrt(mv);
+  /* getMaxVelocity (TwoDScene.cpp:4171-4178): soft elasto particles */
+  double ev = 0.0;
+  for (int p = 0; p < s->ne; ++p) {
+    if (s->surf[p]) continue;
+    const double q = s->v[p * 3] * s->v[p * 3] + s->v[p * 3 + 1] * s->v[p * 3 + 1] +
+                     s->v[p * 3 + 2] * s->v[p * 3 + 2];
+    if (q > ev) ev = q;
+  }
+  ev = sqrt(ev);
   const double dx = s->p.dx;
-  double me = dx / 1e-63 / 3.0;
+  double me = dx / (ev > 1e-63 ? ev : 1e-63) / 3.0;
   if (me > 1.0 / 30.0) me = 1.0 / 30.0;
   double mf = dx / (mv > 1e-63 ? mv : 1e-63) * 3.0;
   if (mf > 1.0 / 30.0) mf = 1.0 / 30.0;
@@ -1437,6 +1583,13 @@ int wco_step(Scene* s, double dt, int snapshot) {
 
 /* liquid viscosity (LiquidInfo::viscosity with compute_viscosity on, explicit)
  * and LinearizedImplicitEuler's viscosity sub-steps; mu = 0 turns it off */
+/* LiquidInfo elasto_flip_coeff, elasto_flip_asym_coeff, elasto_advect_coeff */
+void wco_set_elasto_coeffs(Scene* s, double flip, double asym, double advect) {
+  s->p.e_flip = flip;
+  s->p.e_asym = asym;
+  s->p.e_advect = advect;
+}
+
 void wco_set_viscosity(Scene* s, double mu, int substeps) {
   s->p.visc = mu;
   s->p.visc_substeps = substeps > 0 ? substeps : 1;
@@ -1460,6 +1613,9 @@ Scene* wco_create(double dx, const double* g, double rho, double flip, double fr
   s->p.criterion = criterion;
   s->p.maxiters = maxiters;
   s->p.mic = mic;
+  s->p.e_flip = 0.95;
+  s->p.e_asym = 1.0;
+  s->p.e_advect = 1.0;
   s->bs = dx * 4.0;
   s->np = np;
   const size_t n = (size_t)(np > 0 ? np : 1);
@@ -1475,7 +1631,74 @@ Scene* wco_create(double dx, const double* g, double rho, double flip, double fr
   memcpy(s->m, mass, sizeof(double) * np);
   memcpy(s->vol, vol, sizeof(double) * np);
   memcpy(s->rad, radius, sizeof(double) * np);
+  s->ne = 0;
+  s->em = (double*)calloc(3 * n, sizeof(double));
+  s->rvol = (double*)calloc(n, sizeof(double));
+  s->rvf = (double*)calloc(n, sizeof(double));
+  s->sf = (double*)calloc(n, sizeof(double));
+  s->ori = (double*)calloc(3 * n, sizeof(double));
+  s->xt = (double*)calloc(n, sizeof(double));
+  s->vt = (double*)calloc(n, sizeof(double));
+  s->surf = (unsigned char*)calloc(n, 1);
   return s;
+}
+
+/* grow a per-particle array of k values to ne + np particles, the old
+ * (liquid) values moving behind ne zeroed elasto slots */
+static double* prepend(double* a, int k, int ne, int np) {
+  double* b = (double*)calloc((size_t)k * (ne + np > 0 ? ne + np : 1), sizeof(double));
+  memcpy(b + (size_t)k * ne, a, sizeof(double) * k * np);
+  free(a);
+  return b;
+}
+
+/* Elasto (cloth/yarn) particles become particles [0, ne) ahead of the liquid
+ * ones (TwoDScene::getNumElastoParticles :5212-5217).  Per particle: x4/v4
+ * (position/velocity with the twist as 4th component), B9 (row-major m_B),
+ * m4/fm4 (m_m, m_fluid_m; P2G uses m(a) + m_fluid(a)), m_rest_vol,
+ * m_rest_volume_fraction, m_fluid_vol, m_shape_factor, m_orientation (3),
+ * surfel flag (m_particle_to_surfel >= 0), radius. */
+void wco_set_elasto(Scene* s, int ne, const double* x4, const double* v4, const double* B9,
+                    const double* m4, const double* fm4, const double* rest_vol,
+                    const double* rest_vf, const double* fluid_vol, const double* shape_factor,
+                    const double* orient3, const int* surfel, const double* radius) {
+  const int nl = s->np;
+  s->x = prepend(s->x, 3, ne, nl);
+  s->v = prepend(s->v, 3, ne, nl);
+  s->C = prepend(s->C, 9, ne, nl);
+  s->m = prepend(s->m, 1, ne, nl);
+  s->vol = prepend(s->vol, 1, ne, nl);
+  s->rad = prepend(s->rad, 1, ne, nl);
+  s->em = prepend(s->em, 3, ne, nl);
+  s->rvol = prepend(s->rvol, 1, ne, nl);
+  s->rvf = prepend(s->rvf, 1, ne, nl);
+  s->sf = prepend(s->sf, 1, ne, nl);
+  s->ori = prepend(s->ori, 3, ne, nl);
+  s->xt = prepend(s->xt, 1, ne, nl);
+  s->vt = prepend(s->vt, 1, ne, nl);
+  unsigned char* su = (unsigned char*)calloc((size_t)(ne + nl > 0 ? ne + nl : 1), 1);
+  free(s->surf);
+  s->surf = su;
+  for (int p = 0; p < ne; ++p) {
+    for (int a = 0; a < 3; ++a) {
+      s->x[p * 3 + a] = x4[p * 4 + a];
+      s->v[p * 3 + a] = v4[p * 4 + a];
+      s->em[p * 3 + a] = m4[p * 4 + a] + fm4[p * 4 + a];
+      s->ori[p * 3 + a] = orient3[p * 3 + a];
+    }
+    for (int q = 0; q < 9; ++q) s->C[p * 9 + q] = B9[p * 9 + q];
+    s->xt[p] = x4[p * 4 + 3];
+    s->vt[p] = v4[p * 4 + 3];
+    s->m[p] = 0.0;
+    s->vol[p] = fluid_vol[p];
+    s->rad[p] = radius[p];
+    s->rvol[p] = rest_vol[p];
+    s->rvf[p] = rest_vf[p];
+    s->sf[p] = shape_factor[p];
+    s->surf[p] = surfel[p] ? 1 : 0;
+  }
+  s->ne = ne;
+  s->np = ne + nl;
 }
 
 void wco_destroy(Scene* s) {
@@ -1484,7 +1707,8 @@ void wco_destroy(Scene* s) {
     free(s->snaps[k].f);
     free(s->snaps[k].i);
   }
-  void* ptrs[] = {s->x, s->v, s->C, s->m, s->vol, s->rad, s->keys, s->sup, s->act, s->base,
+  void* ptrs[] = {s->x, s->v, s->C, s->m, s->vol, s->rad, s->em, s->rvol, s->rvf, s->sf,
+                  s->ori, s->xt, s->vt, s->surf, s->keys, s->sup, s->act, s->base,
                   s->inside, s->wu, s->wv, s->ww, s->wp, s->pu.start, s->pu.pid, s->pu.slot,
                   s->pv.start, s->pv.pid, s->pv.slot, s->pw.start, s->pw.pid, s->pw.slot,
                   s->pp.start, s->pp.pid, s->pp.slot, s->sat_p, s->psi_p, s->pore_p, s->lphi,
@@ -1493,7 +1717,8 @@ void wco_destroy(Scene* s) {
   for (int a = 0; a < 3; ++a) {
     void* q[] = {s->mass[a], s->vel[a], s->vol_f[a], s->sat[a], s->psi[a], s->wgt[a], s->svel[a],
                  s->rhs[a], s->vstar[a], s->invC[a], s->psifs[a], s->psisf[a], s->mshdvm[a],
-                 s->mfhdvm[a], s->valid[a]};
+                 s->mfhdvm[a], s->valid[a], s->emass[a], s->evel[a], s->evol[a], s->esf[a],
+                 s->eori[a]};
     for (size_t k = 0; k < sizeof(q) / sizeof(q[0]); ++k) free(q[k]);
   }
   free(s);

@@ -102,3 +102,60 @@ def test_explicit_viscosity_step(kind, mu):
         if m.any():
             assert np.abs(a[m] - b[m]).max() <= 1e-12 * max(np.abs(a[m]).max(), 1e-300), k
     assert (r.get("liquid_c_vf")[~np.isnan(r.get("liquid_c_vf"))] > 0).any()
+
+
+ELASTO_EXACT = ["grid_dims", "grid_origin", "bbx", "array_idx", "array_sup", "active",
+                "stencil_base", "inside"]
+ELASTO_CLOSE = ([f"{f}_{c}" for f in ("mass_fluid", "vel_fluid", "vol_fluid", "mass", "vel",
+                                      "vol", "psi", "sat", "shape_factor", "orientation")
+                 for c in "xyz"] +
+                ["sat_p", "psi_p", "pore_pressure_p", "liquid_phi"] +
+                [t + q for t in ("g2p_", "adv_") for q in ("x", "v", "C", "x4", "ev4", "eB")])
+
+
+@pytest.mark.parametrize("surfel_every,flip,asym", [(0, 0.95, 1.0), (5, 0.9, 0.3)])
+def test_elasto_transfers(surfel_every, flip, asym):
+    """P2G with both particle kinds (solid mass/velocity/volume, psi,
+    saturation, shape factor, orientation, cell-centre psi/saturation/pore
+    pressure), then G2P from the P2G velocities (the elasto B blend included)
+    and advection, on a liquid sphere over a cloth sheet."""
+    sc = scenes.liquid_on_sheet(16, 8, 3, surfel_every=surfel_every)
+    sc.params.elasto_flip_coeff = flip
+    sc.params.elasto_flip_asym_coeff = asym
+    sc.params.elasto_advect_coeff = 0.97
+    r = oref.RefScene(sc, mic=True)
+    o = oo.OracleScene(sc)
+    r.transfer(DT)
+    o.transfer(DT)
+    for k in ELASTO_EXACT:
+        assert np.array_equal(r.get(k), o.get(k)), k
+    psi = r.get("psi_x")
+    assert np.nanmax(psi) > 0.0            # the sheet shows up as solid
+    for k in ELASTO_CLOSE:
+        a, b = r.get(k), o.get(k)
+        m = ~np.isnan(a)
+        assert np.array_equal(m, ~np.isnan(b)), k
+        if m.any():
+            assert np.abs(a[m] - b[m]).max() <= 1e-12 * max(np.abs(a[m]).max(), 1e-300), k
+
+
+def test_elasto_only_scene():
+    """No liquid particle: every particle is elasto and the liquid level set
+    keeps its initial value (updateLiquidPhi returns early)."""
+    sc = scenes.liquid_on_sheet(16, 8, 3)
+    sc.x, sc.v = sc.x[:0], sc.v[:0]
+    sc.mass, sc.vol, sc.radius = sc.mass[:0], sc.vol[:0], sc.radius[:0]
+    r = oref.RefScene(sc, mic=True)
+    o = oo.OracleScene(sc)
+    r.transfer(DT)
+    o.transfer(DT)
+    for k in ELASTO_EXACT:
+        assert np.array_equal(r.get(k), o.get(k)), k
+    lp = r.get("liquid_phi")
+    assert np.all(lp[~np.isnan(lp)] == 3.0 * 4 * sc.params.dx)
+    for k in ("mass_x", "vel_y", "psi_z", "sat_p", "psi_p", "liquid_phi", "g2p_ev4", "g2p_eB",
+              "adv_x4"):
+        a, b = r.get(k), o.get(k)
+        m = ~np.isnan(a)
+        assert np.array_equal(m, ~np.isnan(b)), k
+        assert np.abs(a[m] - b[m]).max() <= 1e-12 * max(np.abs(a[m]).max(), 1e-300), k
