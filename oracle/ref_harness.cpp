@@ -3,7 +3,7 @@
 // pins the C restatement (oracle/wc_oracle.c) and the timed CPU baseline; no
 // product code links it.
 //
-// It builds a liquid-only TwoDScene programmatically (the XML parser TU needs
+// It builds a TwoDScene programmatically (the XML parser TU needs
 // GL headers), replays the fluid hot path in WetClothCore::stepSystem order
 // (libWetCloth/Core/WetClothCore.cpp:115-258, minus the particle maintenance,
 // elasto and surface-tension calls which are no-ops or out of scope for a
