@@ -236,6 +236,12 @@ int wcg_create(const wcg_params* params, wcg_ctx** out) {
   if (const char* v = getenv("WCG_SWEEP_TILE")) ctx->c.sweep_variant = !strcmp(v, "warp") ? 1 : 0;
   // layout of the pressure solve (performance knob; same arithmetic)
   if (const char* v = getenv("WCG_PCG_LAYOUT")) ctx->c.pcg_layout = !strcmp(v, "tiles") ? 1 : 0;
+  // CTAs per thread-block cluster along c in the MIC(0) sweeps (1, 2, 4 or 8;
+  // performance knob, identical results)
+  if (const char* v = getenv("WCG_SWEEP_CLUSTER")) {
+    const int k = atoi(v);
+    ctx->c.sweep_cluster = (k == 2 || k == 4 || k == 8) ? k : 1;
+  }
   cudaError_t e = wcg::ctx_init(ctx->c);
   if (e != cudaSuccess) {
     std::string m = std::string("context init: ") + cudaGetErrorString(e);

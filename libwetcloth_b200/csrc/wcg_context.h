@@ -211,6 +211,8 @@ struct Context {
   DevBuf pl64;                   // kNumPl64Fields * pl_cap doubles
   DevBuf pl_edge;                // tagged edge words
   DevBuf pl_order;               // patches in wave order (int32)
+  DevBuf pl_corder;              // cluster columns in wave order (sweep_cluster > 1)
+  int sweep_cluster = 1;         // CTAs per cluster along c in the MIC(0) sweeps
   DevBuf pl_part;                // per-patch partials (double)
   long long pl_cap = 0;
   int pl_tickets = 0;            // sweep tickets handed out in this solve

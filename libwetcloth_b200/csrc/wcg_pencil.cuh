@@ -124,6 +124,39 @@ __device__ inline unsigned long long global_ns() {
 }
 constexpr unsigned long long kWaitNs = 2000000000ull;  // bound of an mbarrier wait (2 s)
 
+// ---- thread-block clusters: distributed shared memory -----------------------
+__device__ inline unsigned cluster_rank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+// every thread of every CTA of the cluster; release/acquire orders the shared
+// memory each CTA wrote before it against the reads after it
+__device__ inline void cluster_sync() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n"
+               "barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// address of the same shared variable in CTA `rank` of the cluster
+__device__ inline unsigned cluster_map(unsigned local, unsigned rank) {
+  unsigned r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(local), "r"(rank));
+  return r;
+}
+__device__ inline unsigned ld_cluster_u32(unsigned addr) {
+  unsigned v;
+  asm volatile("ld.relaxed.cluster.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(addr) : "memory");
+  return v;
+}
+__device__ inline void st_cluster_u64(unsigned addr, u64 v) {
+  asm volatile("st.relaxed.cluster.shared::cluster.u64 [%0], %1;" ::"r"(addr), "l"(v) : "memory");
+}
+// a word of this CTA's shared memory that peers of the cluster write
+__device__ inline u64 ld_own_u64(unsigned addr) {
+  u64 v;
+  asm volatile("ld.relaxed.cluster.shared::cta.u64 %0, [%1];" : "=l"(v) : "r"(addr) : "memory");
+  return v;
+}
+
 // Stages of the shared-memory row ring of a sweep.
 template <typename R>
 struct SweepStages {
@@ -138,6 +171,17 @@ template <typename R>
 __host__ __device__ constexpr size_t sweep_dyn_smem(int mode, bool upd) {
   return (size_t)SweepStages<R>::D * sweep_nf(mode, upd) * 256 * sizeof(R) +
          (size_t)SweepStages<R>::D * 8;
+}
+// With clusters the c-face edge words of the patch upstream in the same
+// cluster land in this CTA's shared memory: Ls x 16 entries, 16-byte aligned
+// after the ring and its mbarriers.
+template <typename R>
+__host__ __device__ constexpr size_t sweep_cedge_off(int mode, bool upd) {
+  return (sweep_dyn_smem<R>(mode, upd) + 15) / 16 * 16;
+}
+template <typename R>
+__host__ __device__ constexpr size_t sweep_cedge_bytes(int mode, int Ls) {
+  return (size_t)Ls * 16 * (mode == 0 ? 2 : 1) * (sizeof(R) / 4) * 8;
 }
 
 // Words of the edge buffer: entry (producer patch, side, s, k), EW words each.
@@ -199,7 +243,16 @@ struct PencilSweepArgs {
 // c-neighbour inside the warp come by shuffle of the previous step's outputs,
 // the c-neighbour in the adjacent warp through shared memory, and values across
 // the patch faces through the tagged edge words.
-template <typename R, int MODE, bool UPD>
+//
+// CL > 1: launched in clusters of CL CTAs along c.  The patches of a cluster
+// are one cluster column of CL consecutive c-patches; a c-face neighbour in
+// the same cluster writes its tagged words straight into this CTA's shared
+// memory (st.shared::cluster), which takes the global round trip off those
+// hops.  Tickets are handed out per cluster in wave order, so every upstream
+// cluster started earlier.  The cluster syncs after the edge buffers are
+// cleared and before any CTA exits, so no CTA writes into a peer that has not
+// started or has already left.
+template <typename R, int MODE, bool UPD, int CL>
 __global__ void __launch_bounds__(kPatchLines, 1)
     k_pencil_sweep(const PencilSweepArgs<R> A) {
   constexpr bool BWD = MODE == kBackward;
@@ -223,17 +276,37 @@ __global__ void __launch_bounds__(kPatchLines, 1)
   const PencilGeom& G = A.G;
   const int tid = threadIdx.x;
   const int lane = tid & 31, w = tid >> 5;
-  if (tid == 0) s_ticket = atomicAdd(A.ticket, 1) - A.ticket_base;
-  for (int i = tid; i < 2 * NW * kPatch * PW; i += kPatchLines) (&xc[0][0][0][0])[i] = R(0);
-  __syncthreads();
+  // one ticket per patch (per cluster with CL > 1), taken even by a launch
+  // that returns at once, so the counter stays in step with the host's base
+  const int crank = CL > 1 ? (int)cluster_rank() : 0;
+  if (tid == 0 && crank == 0) s_ticket = atomicAdd(A.ticket, 1) - A.ticket_base;
+  // set by an earlier launch, so uniform: the whole cluster returns before
+  // any cross-CTA access
   if (*(const int*)(A.sc + S_DONE)) return;
-  const int tk = s_ticket;
-  if (tk < 0 || tk >= (int)G.npatch) {
+  for (int i = tid; i < 2 * NW * kPatch * PW; i += kPatchLines) (&xc[0][0][0][0])[i] = R(0);
+  u64* const cedge = CL > 1 ? reinterpret_cast<u64*>(dsm + sweep_cedge_off<R>(MODE, UPD)) : nullptr;
+  if (CL > 1)
+    for (int i = tid; i < G.Ls * kPatch * EW; i += kPatchLines) cedge[i] = 0ull;
+  if (CL > 1)
+    cluster_sync();
+  else
+    __syncthreads();
+  const int tk = CL > 1 ? (int)ld_cluster_u32(cluster_map(smem_u32(&s_ticket), 0)) : s_ticket;
+  const int nunits = CL > 1 ? G.nPA * ((G.nPC + CL - 1) / CL) : (int)G.npatch;
+  bool run = true;
+  if (tk < 0 || tk >= nunits) {
     if (tid == 0) record_error(A.err, kErrIndex);
-    return;
+    run = false;
   }
-  const int p = BWD ? A.order[G.npatch - 1 - tk] : A.order[tk];
-  const int PAi = p % G.nPA, PCi = p / G.nPA;
+  int p = 0, PAi = 0, PCi = 0;
+  if (run) {
+    const int unit = BWD ? A.order[nunits - 1 - tk] : A.order[tk];
+    PAi = unit % G.nPA;
+    PCi = CL > 1 ? (unit / G.nPA) * CL + crank : unit / G.nPA;
+    run = PCi < G.nPC;  // the last cluster column may reach past the box
+    p = PCi * G.nPA + PAi;
+  }
+  if (run) {
   const int al = tid & (kPatch - 1), cl = tid / kPatch;
   const bool line = PAi * kPatch + al < G.NA && PCi * kPatch + cl < G.NC;
   const int dl = al + cl;
@@ -253,6 +326,13 @@ __global__ void __launch_bounds__(kPatchLines, 1)
     pub_c = cl == 0 && PCi > 0;
   }
   if (!line) up_a = up_c = -1;
+  // c-face neighbours in the same cluster exchange through shared memory
+  const bool c_loc = CL > 1 && up_c >= 0 && (BWD ? (PCi + 1) % CL != 0 : PCi % CL != 0);
+  const bool c_rem = CL > 1 && pub_c && (BWD ? PCi % CL != 0 : (PCi + 1) % CL != 0);
+  if (c_loc) up_c = -1;
+  if (c_rem) pub_c = false;
+  const unsigned cedge_own = CL > 1 ? smem_u32(cedge) : 0u;
+  const unsigned cedge_dst = c_rem ? cluster_map(cedge_own, BWD ? crank - 1 : crank + 1) : 0u;
   const bool a_edge = al == (BWD ? kPatch - 1 : 0);  // no in-warp a source
   const bool c_prod = BWD ? lane < 16 : lane >= 16;  // half read by the next warp
   const int w_src = BWD ? w + 1 : w - 1;
@@ -383,6 +463,25 @@ __global__ void __launch_bounds__(kPatchLines, 1)
 #pragma unroll
         for (int k = 0; k < PW; ++k) in_c[k] = TagWords<R>::unpack(epc[v] + k * TW);
       }
+      if (CL > 1 && live && c_loc) {
+        u64 wd[EW];
+        const unsigned a0 = cedge_own + (unsigned)((s * kPatch + al) * EW) * 8u;
+#pragma unroll
+        for (int k = 0; k < EW; ++k) {
+          wd[k] = ld_own_u64(a0 + 8u * k);
+          long long it = 0;
+          while ((unsigned)(wd[k] >> 32) != ep) {
+            if (gave_up || ++it > kSpinLimit) {
+              if (!gave_up) record_error(A.err, kErrWaitTimeout);
+              gave_up = true;
+              break;
+            }
+            wd[k] = ld_own_u64(a0 + 8u * k);
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < PW; ++k) in_c[k] = TagWords<R>::unpack(wd + k * TW);
+      }
       // this row's inputs from the ring
       R f[NF];
       mwait(u);
@@ -460,6 +559,14 @@ __global__ void __launch_bounds__(kPatchLines, 1)
 #pragma unroll
         for (int k = 0; k < EW; ++k) st_relaxed_u64(ec_dst + s * ES + k, wd[k]);
       }
+      if (CL > 1 && live && c_rem) {
+        u64 wd[EW];
+#pragma unroll
+        for (int k = 0; k < PW; ++k) TagWords<R>::pack(out_c[k], ep, wd + k * TW);
+        const unsigned a0 = cedge_dst + (unsigned)((s * kPatch + al) * EW) * 8u;
+#pragma unroll
+        for (int k = 0; k < EW; ++k) st_cluster_u64(a0 + 8u * k, wd[k]);
+      }
 #pragma unroll
       for (int k = 0; k < PW; ++k) {
         if (c_prod) xc[nxt][w][al][k] = out_c[k];
@@ -502,6 +609,8 @@ __global__ void __launch_bounds__(kPatchLines, 1)
     const double sm = block_sum<double>(dsum, red);
     if (tid == 0) A.part[p] = sm;
   }
+  }  // run
+  if (CL > 1) cluster_sync();
 }
 
 // x += alpha s (the update of the last PCG iteration, which no SpMV follows)

@@ -1037,6 +1037,22 @@ static cudaError_t pl_setup(Context& c, const int* lo, const int* hi) {
     WCG_TRY(cudaMemcpyAsync(c.pl_order.p, c.pl_order_h.data(), G.npatch * sizeof(int),
                             cudaMemcpyHostToDevice, c.stream));
   }
+  if (c.sweep_cluster > 1) {
+    // cluster columns (PAi, PCc) of sweep_cluster c-patches, in wave order
+    const int CL = c.sweep_cluster;
+    const int nPCc = (G.nPC + CL - 1) / CL;
+    std::vector<int> co;
+    co.reserve((size_t)G.nPA * nPCc);
+    for (int w = 0; w <= G.nPA + nPCc - 2; ++w)
+      for (int pc = 0; pc < nPCc; ++pc) {
+        const int pa = w - pc;
+        if (pa >= 0 && pa < G.nPA) co.push_back(pc * G.nPA + pa);
+      }
+    WCG_TRY(c.pl_corder.ensure(co.size() * sizeof(int)));
+    WCG_TRY(cudaMemcpyAsync(c.pl_corder.p, co.data(), co.size() * sizeof(int),
+                            cudaMemcpyHostToDevice, c.stream));
+    WCG_TRY(cudaStreamSynchronize(c.stream));  // co is a host temporary
+  }
   // every array starts at zero (rows and lines outside the box stay zero)
   WCG_TRY(cudaMemsetAsync(c.pl.p, 0, (size_t)kNumPlFields * G.len * sizeof(R), c.stream));
   c.pl_tickets = 0;
@@ -1068,21 +1084,60 @@ static PencilSweepArgs<R> pl_args(Context& c) {
   return a;
 }
 
-template <typename R, int MODE, bool UPD>
-static cudaError_t pl_sweep(Context& c, PencilSweepArgs<R> a) {
+// dynamic shared memory a cluster sweep may use (the kernel's static
+// arrays take under 8 KB of the 227 KB per CTA)
+constexpr size_t kSweepSmemMax = 200 * 1024;
+
+template <typename R, int MODE, bool UPD, int CL>
+static cudaError_t pl_sweep_cl(Context& c, PencilSweepArgs<R> a) {
   ProfScope prof(c, MODE == kFactor ? P_MICFACTOR : P_MICSWEEP);
+  const PencilGeom& G = c.plg;
+  const int nunits = CL > 1 ? G.nPA * ((G.nPC + CL - 1) / CL) : (int)G.npatch;
   a.epoch = (unsigned)(++c.tile_epoch);
   a.ticket_base = c.pl_tickets;
-  c.pl_tickets += (int)c.plg.npatch;
-  constexpr size_t smem = sweep_dyn_smem<R>(MODE, UPD);
+  c.pl_tickets += nunits;
+  const size_t smem = CL > 1 ? sweep_cedge_off<R>(MODE, UPD) + sweep_cedge_bytes<R>(MODE, G.Ls)
+                             : sweep_dyn_smem<R>(MODE, UPD);
   static bool attr_set = false;  // per instantiation, once per process
   if (!attr_set) {
-    WCG_TRY(cudaFuncSetAttribute(k_pencil_sweep<R, MODE, UPD>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    WCG_TRY(cudaFuncSetAttribute(k_pencil_sweep<R, MODE, UPD, CL>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(CL > 1 ? kSweepSmemMax : smem)));
     attr_set = true;
   }
-  ++c.launches, k_pencil_sweep<R, MODE, UPD><<<(unsigned)c.plg.npatch, kPatchLines, smem, c.stream>>>(a);
-  return cudaGetLastError();
+  if (CL == 1) {
+    ++c.launches, k_pencil_sweep<R, MODE, UPD, 1><<<(unsigned)G.npatch, kPatchLines, smem, c.stream>>>(a);
+    return cudaGetLastError();
+  }
+  a.order = c.pl_corder.as<int>();
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(nunits * CL));
+  cfg.blockDim = dim3(kPatchLines);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = c.stream;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = CL;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  ++c.launches;
+  return cudaLaunchKernelEx(&cfg, k_pencil_sweep<R, MODE, UPD, CL>, a);
+}
+
+// The cluster form needs the c-edge buffer of a patch (Ls x 16 tagged
+// entries) in shared memory; longer boxes use the plain form.
+template <typename R, int MODE, bool UPD>
+static cudaError_t pl_sweep(Context& c, PencilSweepArgs<R> a) {
+  const int CL = c.sweep_cluster;
+  if (CL > 1 &&
+      sweep_cedge_off<R>(MODE, UPD) + sweep_cedge_bytes<R>(MODE, c.plg.Ls) <= kSweepSmemMax) {
+    if (CL == 2) return pl_sweep_cl<R, MODE, UPD, 2>(c, a);
+    if (CL == 4) return pl_sweep_cl<R, MODE, UPD, 4>(c, a);
+    if (CL == 8) return pl_sweep_cl<R, MODE, UPD, 8>(c, a);
+  }
+  return pl_sweep_cl<R, MODE, UPD, 1>(c, a);
 }
 
 // PCGSolver<T>::solve (PCGSolver.h:260-308) in the pencil layout on the

@@ -27,19 +27,23 @@ def _scene(kind):
         return scenes.dam_break(48, 2, 4, block_hi=(0.5, 0.3, 0.95))
     if kind == "curl48":
         return scenes.half_box(48, 2, 5, amplitude=0.5, sigma_cells=2.0)
+    if kind == "curl96":  # 6 patches along c: several cluster columns
+        return scenes.half_box(96, 2, 6, amplitude=0.5, sigma_cells=3.0)
     raise ValueError(kind)
 
 
-def _solve(sc, layout, precision):
-    old = os.environ.get("WCG_PCG_LAYOUT")
-    os.environ["WCG_PCG_LAYOUT"] = layout
+def _solve(sc, layout, precision, cluster=1):
+    env = {"WCG_PCG_LAYOUT": layout, "WCG_SWEEP_CLUSTER": str(cluster)}
+    old = {k: os.environ.get(k) for k in env}
+    os.environ.update(env)
     try:
         g = FluidScene(sc, precision=precision)
     finally:
-        if old is None:
-            del os.environ["WCG_PCG_LAYOUT"]
-        else:
-            os.environ["WCG_PCG_LAYOUT"] = old
+        for k, v in old.items():
+            if v is None:
+                del os.environ[k]
+            else:
+                os.environ[k] = v
     g.rebucketize_and_resample()
     g.map_particle_nodes()
     g.step_velocity(DT)
@@ -82,4 +86,24 @@ def test_pencil_deterministic(wcg):
     b, sb = _solve(sc, "pencil", _capi.WCG_FP32_REFINE)
     assert sa["pcg_iters"] == sb["pcg_iters"]
     m = ~np.isnan(a)
+    assert np.array_equal(a[m], b[m])
+
+
+@pytest.mark.parametrize("cluster", [2, 4, 8])
+@pytest.mark.parametrize("kind,precision", [("curl48", _capi.WCG_FP64),
+                                            ("slab64_x", _capi.WCG_FP64),
+                                            ("curl96", _capi.WCG_FP64),
+                                            ("curl48", _capi.WCG_FP32_REFINE)])
+def test_pencil_cluster_sweeps_bit_identical(kind, precision, cluster, wcg):
+    """Clusters only change how c-face edge values travel (shared memory of
+    the neighbouring CTA instead of a global round trip): the arithmetic is
+    the same, so pressures and iteration counts are bit-identical, also when
+    the patch count along c is not a multiple of the cluster size."""
+    sc = _scene(kind)
+    a, sa = _solve(sc, "pencil", precision, 1)
+    b, sb = _solve(sc, "pencil", precision, cluster)
+    assert sb["converged"] == 1
+    assert sa["pcg_iters"] == sb["pcg_iters"] and sa["refinements"] == sb["refinements"]
+    m = ~np.isnan(a)
+    assert np.array_equal(m, ~np.isnan(b))
     assert np.array_equal(a[m], b[m])
