@@ -198,6 +198,26 @@ int wcg_export_pressure_system(wcg_ctx* ctx, long long* ndof, long long* nnz,
                                long long* rowstart, long long* col,
                                double* val, double* rhs);
 
+/* ---- many scenes at once (config 4 of the benchmark plan) ---- */
+/* A batch steps independent scenes (each created, uploaded and owned by the
+ * caller) from a pool of host threads, largest scene first; every scene keeps
+ * its own stream, so the kernels of different scenes overlap on the GPU.
+ * Each scene's result is what wcg_step on it alone gives.  No reference
+ * counterpart: the reference steps one TwoDScene per process. */
+typedef struct wcg_batch wcg_batch;
+int wcg_batch_create(int n, wcg_ctx* const* scenes, wcg_batch** out);
+int wcg_batch_destroy(wcg_batch* b);
+/* nsteps wcg_step calls per scene with its own dt[i]; status[i] (may be NULL)
+ * receives each scene's last status.  Returns the first hard error, else
+ * WCG_ERR_NOT_CONVERGED if any scene's solve did not converge, else WCG_OK. */
+int wcg_batch_step(wcg_batch* b, const double* dt, int nsteps, int* status);
+int wcg_batch_set_threads(wcg_batch* b, int nthreads);
+int wcg_batch_threads(const wcg_batch* b);
+/* Times one batch step per candidate thread count (each trial advances every
+ * scene by one step), keeps the fastest; ms[k] (may be NULL) gets the times. */
+int wcg_batch_autotune(wcg_batch* b, const double* dt, const int* candidates, int ncand,
+                       double* ms);
+
 /* ---- instrumentation ---- */
 /* the cudaStream_t all of this context's kernels run on */
 void* wcg_stream(const wcg_ctx* ctx);

@@ -86,6 +86,13 @@ SIGNATURES = {
     "wcg_download_elasto": (ctypes.c_int, [ctypes.c_void_p, _D, _D, _D]),
     "wcg_num_elasto": (ctypes.c_longlong, [ctypes.c_void_p]),
     "wcg_upload_field": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, _D, ctypes.c_longlong]),
+    "wcg_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
+                                        ctypes.POINTER(ctypes.c_void_p)]),
+    "wcg_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "wcg_batch_step": (ctypes.c_int, [ctypes.c_void_p, _D, ctypes.c_int, _I]),
+    "wcg_batch_set_threads": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "wcg_batch_threads": (ctypes.c_int, [ctypes.c_void_p]),
+    "wcg_batch_autotune": (ctypes.c_int, [ctypes.c_void_p, _D, _I, ctypes.c_int, _D]),
     "wcg_save_positions": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
     "wcg_load_positions": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
     "wcg_write_fluid_obj": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),

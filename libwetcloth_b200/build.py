@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libwcgpu.so")
-SOURCES = ["wcg_step.cu", "wcg_capi.cu", "wcg_noalloc.cu"]
+SOURCES = ["wcg_step.cu", "wcg_capi.cu", "wcg_noalloc.cu", "wcg_batch.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3",
               "-std=c++17", "-Xcompiler", "-fPIC", "-shared"]
 

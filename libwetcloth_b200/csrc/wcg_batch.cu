@@ -1,0 +1,150 @@
+// Many independent scenes stepped together.
+//
+// Each scene is its own wcg_ctx with its own stream; a batch steps them from a
+// small pool of host threads that take scenes from a shared queue, largest
+// first.  The kernels of different scenes then overlap on the GPU: small
+// scenes leave most SMs idle and their launches are short, so running several
+// at once fills the machine.  The thread count is chosen by
+// wcg_batch_autotune, which times one batch step per candidate.  Results are
+// those of stepping each scene alone (the same kernels on the same data).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "wcg_context.h"
+#include "../../include/wetcloth_gpu.h"
+
+struct wcg_batch {
+  std::vector<wcg_ctx*> scenes;
+  std::vector<int> order;  // largest particle count first
+  int nthreads = 1;
+};
+
+namespace {
+
+int fail(int code, const std::string& msg) { return wcg::set_last_error(code, msg); }
+
+// One batch step: every scene takes nsteps calls of wcg_step with its dt.
+// Returns the first hard error; WCG_ERR_NOT_CONVERGED (which the reference
+// treats as a warning) only if no hard error occurred.
+int run_batch(wcg_batch* b, const double* dt, int nsteps, int nthreads, int* status) {
+  const int n = (int)b->scenes.size();
+  std::atomic<int> next(0);
+  std::vector<int> st((size_t)n, WCG_OK);
+  std::vector<std::string> msg((size_t)n);
+  auto worker = [&]() {
+    int dev = -1;
+    for (;;) {
+      const int k = next.fetch_add(1);
+      if (k >= n) break;
+      const int i = b->order[k];
+      wcg_ctx* ctx = b->scenes[i];
+      if (ctx->c.device != dev) {
+        cudaSetDevice(ctx->c.device);
+        dev = ctx->c.device;
+      }
+      for (int s = 0; s < nsteps; ++s) {
+        int sub = 0;
+        const int r = wcg_step(ctx, dt[i], &sub);
+        if (r == WCG_OK) continue;
+        if (r == WCG_ERR_NOT_CONVERGED) {
+          st[i] = r;
+          continue;
+        }
+        st[i] = r;
+        msg[i] = wcg_last_error();
+        break;
+      }
+    }
+  };
+  const int nt = std::max(1, std::min(nthreads, n));
+  std::vector<std::thread> pool;
+  pool.reserve((size_t)nt - 1);
+  for (int t = 1; t < nt; ++t) pool.emplace_back(worker);
+  worker();
+  for (std::thread& t : pool) t.join();
+  int first = WCG_OK;
+  for (int i = 0; i < n; ++i) {
+    if (status) status[i] = st[i];
+    if (st[i] != WCG_OK && st[i] != WCG_ERR_NOT_CONVERGED && first == WCG_OK) {
+      first = st[i];
+      fail(st[i], "scene " + std::to_string(i) + ": " + msg[i]);
+    }
+  }
+  if (first != WCG_OK) return first;
+  for (int i = 0; i < n; ++i)
+    if (st[i] == WCG_ERR_NOT_CONVERGED)
+      return fail(WCG_ERR_NOT_CONVERGED, "scene " + std::to_string(i) + " did not converge");
+  return WCG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int wcg_batch_create(int n, wcg_ctx* const* scenes, wcg_batch** out) {
+  if (!out || n <= 0 || !scenes) return fail(WCG_ERR_ARG, "need scenes and an output pointer");
+  for (int i = 0; i < n; ++i)
+    if (!scenes[i]) return fail(WCG_ERR_ARG, "null scene in batch");
+  wcg_batch* b = new wcg_batch();
+  b->scenes.assign(scenes, scenes + n);
+  b->order.resize((size_t)n);
+  for (int i = 0; i < n; ++i) b->order[i] = i;
+  std::stable_sort(b->order.begin(), b->order.end(), [&](int x, int y) {
+    return b->scenes[x]->c.np + b->scenes[x]->c.ne > b->scenes[y]->c.np + b->scenes[y]->c.ne;
+  });
+  b->nthreads = std::min(n, 8);
+  *out = b;
+  return WCG_OK;
+}
+
+int wcg_batch_destroy(wcg_batch* b) {
+  delete b;
+  return WCG_OK;
+}
+
+int wcg_batch_step(wcg_batch* b, const double* dt, int nsteps, int* status) {
+  if (!b || !dt || nsteps < 0) return fail(WCG_ERR_ARG, "bad batch step arguments");
+  for (size_t i = 0; i < b->scenes.size(); ++i)
+    if (!(dt[i] > 0)) return fail(WCG_ERR_ARG, "dt must be positive");
+  return run_batch(b, dt, nsteps, b->nthreads, status);
+}
+
+int wcg_batch_set_threads(wcg_batch* b, int nthreads) {
+  if (!b || nthreads < 1) return fail(WCG_ERR_ARG, "thread count must be >= 1");
+  b->nthreads = nthreads;
+  return WCG_OK;
+}
+
+int wcg_batch_threads(const wcg_batch* b) { return b ? b->nthreads : -1; }
+
+// Times one batch step for each candidate thread count (each trial advances
+// every scene by one step) and keeps the fastest.
+int wcg_batch_autotune(wcg_batch* b, const double* dt, const int* candidates, int ncand,
+                       double* ms_out) {
+  if (!b || !dt || !candidates || ncand <= 0) return fail(WCG_ERR_ARG, "bad autotune arguments");
+  double best = 1e300;
+  int best_t = b->nthreads;
+  for (int k = 0; k < ncand; ++k) {
+    if (candidates[k] < 1) return fail(WCG_ERR_ARG, "thread count must be >= 1");
+    const auto t0 = std::chrono::steady_clock::now();
+    const int r = run_batch(b, dt, 1, candidates[k], nullptr);
+    const double ms =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    if (r != WCG_OK && r != WCG_ERR_NOT_CONVERGED) return r;
+    if (ms_out) ms_out[k] = ms;
+    if (ms < best) {
+      best = ms;
+      best_t = candidates[k];
+    }
+  }
+  b->nthreads = best_t;
+  return WCG_OK;
+}
+
+}  // extern "C"

@@ -14,10 +14,6 @@
 #include "../../include/wetcloth_gpu.h"
 #include "wcg_context.h"
 
-struct wcg_ctx {
-  wcg::Context c;
-};
-
 namespace {
 
 thread_local std::string g_err;

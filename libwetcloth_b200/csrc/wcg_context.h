@@ -316,3 +316,8 @@ cudaError_t prepared_solve_fp64(Context& c, double* out, int* iters, double* res
                                 int* converged, double* rhs_norm);
 
 }  // namespace wcg
+
+// The C-ABI's opaque scene handle (include/wetcloth_gpu.h).
+struct wcg_ctx {
+  wcg::Context c;
+};

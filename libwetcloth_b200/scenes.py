@@ -255,3 +255,28 @@ def half_box(n_cells: int = 256, ppc: int = 2, seed: int = 1,
     m, vol, r = attributes(x.shape[0], dx, ppc, prm.liquid_density)
     return Scene(prm, x, v, m, vol, r,
                  name=f"half_box_{n_cells}^3_{ppc}ppc")
+
+
+def batch_scenes(count: int = 256, seed: int = 4, n_range=(32, 96), np_range=(10_000, 1_000_000),
+                 ppc: int = 8):
+    """Seeded independent scenes of uneven size: grid n ~ U{n_range}^3, a
+    liquid block of about N_p ~ U[np_range] particles (capped by the box) at a
+    seeded position, viscosity log-uniform in [1e-3, 1], density U[800, 1300]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        n = int(rng.integers(n_range[0], n_range[1] + 1))
+        dx = 1.0 / n
+        target = float(rng.uniform(np_range[0], np_range[1]))
+        cells = min(target / ppc, 0.6 * n ** 3)
+        # block with aspect (1, 2, 1) scaled to the cell count, inside the box
+        side = (cells / 2.0) ** (1.0 / 3.0) * dx
+        size = np.minimum(np.array([side, 2.0 * side, side]), 0.9)
+        lo = rng.uniform(0.0, 1.0 - size)
+        lo[1] = 0.0
+        prm = SceneParams(dx=dx, liquid_density=float(rng.uniform(800.0, 1300.0)),
+                          viscosity=float(10.0 ** rng.uniform(-3.0, 0.0)))
+        x = liquid_block(dx, lo, lo + size, ppc, seed * 1000 + k)
+        m, vol, r = attributes(x.shape[0], dx, ppc, prm.liquid_density)
+        out.append(Scene(prm, x, np.zeros_like(x), m, vol, r, name=f"batch{k}_{n}^3_{x.shape[0]}p"))
+    return out

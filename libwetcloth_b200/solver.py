@@ -236,3 +236,57 @@ class FluidScene:
         names = [self.L.wcg_profile_phase_name(i).decode() for i in range(n)]
         return {names[i]: (float(ms[i]), int(cnt[i])) for i in range(n)}
 
+
+
+class FluidBatch:
+    """Independent scenes stepped together (wcg_batch_*): each scene is a
+    FluidScene with its own stream; a pool of host threads steps them largest
+    first so their kernels overlap on the GPU."""
+
+    def __init__(self, scenes):
+        self.L = _capi.load()
+        self.scenes = list(scenes)
+        arr = (ctypes.c_void_p * len(self.scenes))(*[s.h.value for s in self.scenes])
+        h = ctypes.c_void_p()
+        check(self.L.wcg_batch_create(len(self.scenes), arr, ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.wcg_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, dt, nsteps=1):
+        """nsteps steps of every scene; dt is a scalar or one value per
+        scene.  Returns the per-scene status codes."""
+        d = np.ascontiguousarray(np.broadcast_to(np.asarray(dt, dtype=np.float64),
+                                                 (len(self.scenes),)))
+        st = (ctypes.c_int * len(self.scenes))()
+        rc = self.L.wcg_batch_step(self.h, _dp(d), nsteps, st)
+        if rc not in (_capi.WCG_OK, _capi.WCG_ERR_NOT_CONVERGED):
+            check(rc)
+        return list(st)
+
+    @property
+    def threads(self):
+        return self.L.wcg_batch_threads(self.h)
+
+    @threads.setter
+    def threads(self, n):
+        check(self.L.wcg_batch_set_threads(self.h, int(n)))
+
+    def autotune(self, dt, candidates=(1, 2, 4, 8, 16)):
+        """Time one batch step per candidate thread count (each advances every
+        scene by one step) and keep the fastest; returns {threads: ms}."""
+        d = np.ascontiguousarray(np.broadcast_to(np.asarray(dt, dtype=np.float64),
+                                                 (len(self.scenes),)))
+        c = (ctypes.c_int * len(candidates))(*candidates)
+        ms = (ctypes.c_double * len(candidates))()
+        check(self.L.wcg_batch_autotune(self.h, _dp(d), c, len(candidates), ms))
+        return dict(zip(candidates, list(ms)))
