@@ -171,6 +171,17 @@ int wcg_substep(wcg_ctx* ctx, double dt);
 /* WetClothCore::stepSystem (WetClothCore.cpp:45): CFL sub-stepping + sub-steps */
 int wcg_step(wcg_ctx* ctx, double dt, int* substeps_out);
 int wcg_num_substeps(wcg_ctx* ctx, double dt, int* n_out);
+/* Reverse mode of wcg_substep (no reference counterpart: the reference has
+ * no derivatives).  Call with the context holding the particle state before
+ * the sub-step; it recomputes the forward grid fields there and leaves the
+ * particles unchanged.  In: cotangents of the sub-step's outputs v' (3n),
+ * C' (9n, rows as in wcg_download_liquid) and x' (3n).  Out: cotangents of
+ * the inputs v (3n) and C (9n); xbar0 = xbar3 (positions are held fixed: the
+ * weights' dependence on x is not differentiated).  Liquid scenes without
+ * viscosity; the solve is the forward's solver on the same (symmetric)
+ * matrix. */
+int wcg_substep_vjp(wcg_ctx* ctx, double dt, const double* vbar3, const double* Cbar9,
+                    const double* xbar3, double* vbar0, double* Cbar0, double* xbar0);
 
 int wcg_get_stats(const wcg_ctx* ctx, wcg_stats* out);
 

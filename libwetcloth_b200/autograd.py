@@ -1,0 +1,49 @@
+"""torch.autograd binding of one liquid sub-step (the C-ABI's wcg_substep and
+wcg_substep_vjp); the arithmetic is all in libwcgpu.so.
+
+``substep(scene, x, v, C, dt)`` returns (x', v', C') as float64 tensors and
+records a node whose backward restores the checkpoint (x, v, C) in the scene,
+recomputes the forward grid there and runs the reverse-mode kernels.  The
+positions are held fixed in the derivative: d(x')/d(x) is the identity and the
+weights' dependence on x is not differentiated, so gradients through several
+chained sub-steps omit that term.  The scene's particle state after backward is
+the checkpoint of the last node differentiated.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+
+class _Substep(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, x, v, C, scene, dt):
+        xs, vs, Cs = (t.detach().cpu().numpy().astype(np.float64) for t in (x, v, C))
+        scene.set_state(xs, vs, Cs)
+        scene.substep(dt)
+        x1, v1, C1 = scene.download()
+        ctx.scene = scene
+        ctx.dt = dt
+        ctx.state = (xs, vs, Cs)
+        dev = v.device
+        return (torch.from_numpy(x1).to(dev), torch.from_numpy(v1).to(dev),
+                torch.from_numpy(C1).to(dev))
+
+    @staticmethod
+    def backward(ctx, gx1, gv1, gC1):
+        n = ctx.state[0].shape[0]
+        dev = gv1.device if gv1 is not None else gx1.device
+
+        def host(g, k):
+            return np.zeros((n, k)) if g is None else g.detach().cpu().numpy().astype(np.float64)
+
+        scene = ctx.scene
+        scene.set_state(*ctx.state)
+        vb, Cb, xb = scene.substep_vjp(ctx.dt, host(gv1, 3), host(gC1, 9), host(gx1, 3))
+        return (torch.from_numpy(xb).to(dev), torch.from_numpy(vb).to(dev),
+                torch.from_numpy(Cb).to(dev), None, None)
+
+
+def substep(scene, x, v, C, dt: float):
+    """One differentiable sub-step of a FluidScene (liquid, no viscosity)."""
+    return _Substep.apply(x, v, C, scene, dt)

@@ -1,0 +1,329 @@
+// Reverse mode of one liquid sub-step with the particle positions held fixed.
+//
+// With x fixed, the grid (activation, weights, liquid phi, DOFs, solid
+// weights, the matrix) is fixed too, and the sub-step is affine in the
+// particles' velocities v and affine matrices C:
+//   P2G          mom = sum m w (v + C d),  u_f = mom / m_node   (m_node > 1e-20)
+//   stepVelocity v* = u_f + g dt           (heavy nodes; light nodes constant)
+//   assembly     b(c) = sum_faces +-(v* psi_fs w) / dx
+//   solve        A p = b
+//   apply        u = v* - s (p_r - p_l),   s = dt V_f inv_C / (dx theta) on valid faces
+//   extrapolate  two layers of neighbour means into invalid faces
+//   constrain    u *= (1 - friction) on faces with solid weight 0
+//   G2P          v' = sum u w,  C' = flip sum u w d 4/h^2,  x' = x + v' dt
+// (d = x_node - x_particle).  The kernels below apply the transposes in reverse
+// order; A is symmetric, so the adjoint solve reuses the forward solver on the
+// same matrix.  Gradients through the weights' dependence on x are not formed
+// (x-bar passes straight through).  Every sum is a gather in fixed order.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "wcg_common.cuh"
+#include "wcg_context.h"
+#include "wcg_kernels.cuh"
+
+namespace wcg {
+
+// Adjoint grid fields (adj buffer, gcap each).
+enum AdjField : int { A_UBAR = 0, A_UTMP = 3, A_VSBAR = 6, kNumAdjFields = 9 };
+
+// Original-order cotangents of (v', C', x') into sorted-order columns:
+// vb = v-bar + dt x-bar (x' = x + v' dt), Cb = C-bar.
+template <typename R>
+__global__ void k_adj_load(long long np, long long pcap, const int* __restrict__ pid,
+                           const double* __restrict__ vbar, const double* __restrict__ Cbar,
+                           const double* __restrict__ xbar, double dt, R* __restrict__ B) {
+  const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= np) return;
+  const long long i = pid[s];
+  for (int a = 0; a < 3; ++a)
+    B[a * pcap + s] = (R)(vbar[i * 3 + a] + dt * xbar[i * 3 + a]);
+  for (int q = 0; q < 9; ++q) B[(3 + q) * pcap + s] = (R)Cbar[i * 9 + q];
+}
+
+// G2P^T and constrain^T: per face node, over the particles whose stencil
+// holds it (the k_p2g neighbourhood),
+//   u-bar = sum w (vb_a + flip 4/h^2 sum_q Cb_aq d_q),
+// then u-bar *= 1 - friction where the solid weight is 0.
+template <typename R>
+__global__ void __launch_bounds__(192)
+    k_adj_g2p(GridDesc g, const int* __restrict__ active_list, const R* __restrict__ P,
+              long long pcap, const int* __restrict__ start, const int* __restrict__ delta,
+              DeltaRange dr, const R* __restrict__ B, const R* __restrict__ F, long long fstride,
+              R* __restrict__ AG, R flip, R friction) {
+  const int b = active_list[blockIdx.x];
+  const int a = threadIdx.x >> 6;
+  const int l = threadIdx.x & 63;
+  const int bk = b / (g.ni * g.nj);
+  const int rem = b - bk * g.ni * g.nj;
+  const int bj = rem / g.ni;
+  const int bi = rem - bj * g.ni;
+  const int I = bi * 4 + (l & 3), J = bj * 4 + ((l >> 2) & 3), K = bk * 4 + (l >> 4);
+  const long long n = (long long)b * 64 + l;
+  const R org[3] = {(R)g.ox, (R)g.oy, (R)g.oz};
+  const R bs = (R)g.bs, dx = (R)g.dx;
+  const R invh = R(1) / dx;
+  const R invD = R(4) / (dx * dx);
+  const int IJK[3] = {I, J, K};
+  R np_[3];
+  for (int q = 0; q < 3; ++q) np_[q] = coord<R>(org[q], bs, dx, IJK[q], q == a ? R(0) : R(0.5));
+  int lo[3], hi[3];
+  for (int q = 0; q < 3; ++q) {
+    lo[q] = q == a ? IJK[q] - 1 - dr.hi[q] : IJK[q] - 1;
+    hi[q] = q == a ? IJK[q] + 1 - dr.lo[q] : IJK[q] + 1;
+    lo[q] = lo[q] < 0 ? 0 : lo[q];
+  }
+  hi[0] = hi[0] > g.NI - 1 ? g.NI - 1 : hi[0];
+  hi[1] = hi[1] > g.NJ - 1 ? g.NJ - 1 : hi[1];
+  hi[2] = hi[2] > g.NK - 1 ? g.NK - 1 : hi[2];
+  const R* px = P + PX * pcap;
+  const R* py = P + PY * pcap;
+  const R* pz = P + PZ * pcap;
+  const R* vb = B + a * pcap;
+  const R* c0 = B + (3 + 3 * a) * pcap;
+  const R* c1 = B + (3 + 3 * a + 1) * pcap;
+  const R* c2 = B + (3 + 3 * a + 2) * pcap;
+  const R fi = flip * invD;
+  R acc = 0;
+  for (int KZ = lo[2]; KZ <= hi[2]; ++KZ)
+    for (int KY = lo[1]; KY <= hi[1]; ++KY)
+      for (int KX = lo[0]; KX <= hi[0]; ++KX) {
+        const long long c = node_linear(g, KX, KY, KZ);
+        const int s1 = start[c + 1];
+        const int Ka = a == 0 ? KX : (a == 1 ? KY : KZ);
+        for (int s = start[c]; s < s1; ++s) {
+          const int base = Ka - 1 + unpack_delta(delta[s], a);
+          const int off = IJK[a] - base;
+          if (off < 0 || off > 2) continue;
+          const R x = px[s], y = py[s], z = pz[s];
+          const R w = quad_kernel<R>((x - np_[0]) * invh) * quad_kernel<R>((y - np_[1]) * invh) *
+                      quad_kernel<R>((z - np_[2]) * invh);
+          const R cd = (c0[s] * (np_[0] - x) + c1[s] * (np_[1] - y)) + c2[s] * (np_[2] - z);
+          acc += w * (vb[s] + fi * cd);
+        }
+      }
+  if (F[(G_WEIGHT + a) * fstride + n] == R(0)) acc *= R(1) - friction;
+  AG[(A_UBAR + a) * fstride + n] = acc;
+}
+
+// Validity after applyPressureGradsFluidRHS (k_apply_pressure): solid weight
+// > 0 and a liquid cell on either side.
+template <typename R>
+__device__ inline bool adj_face_valid(const GridDesc& g, const unsigned char* active,
+                                      const R* F, long long fstride, int a, int I, int J, int K,
+                                      long long n, R* theta) {
+  if (!(F[(G_WEIGHT + a) * fstride + n] > R(0))) return false;
+  const int lI = I - (a == 0), lJ = J - (a == 1), lK = K - (a == 2);
+  const bool hl = in_grid(g, lI, lJ, lK) && active[bucket_of(g, lI, lJ, lK)];
+  const R phil = hl ? F[G_LPHI * fstride + node_linear(g, lI, lJ, lK)] : R(0);
+  const R phir = F[G_LPHI * fstride + n];
+  if (!(phil < R(0) || phir < R(0))) return false;
+  R t = 1;
+  if (phir >= R(0) || phil >= R(0)) {
+    t = fraction_inside2<R>(phil, phir);
+    t = t > R(kThetaCriterion) ? t : R(kThetaCriterion);
+  }
+  *theta = t;
+  return true;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(192)
+    k_adj_valid0(GridDesc g, const int* __restrict__ active_list,
+                 const unsigned char* __restrict__ active, const R* __restrict__ F,
+                 long long fstride, unsigned char* __restrict__ mask) {
+  const int b = active_list[blockIdx.x];
+  const int a = threadIdx.x >> 6;
+  const int l = threadIdx.x & 63;
+  const int bk = b / (g.ni * g.nj);
+  const int rem = b - bk * g.ni * g.nj;
+  const int bj = rem / g.ni;
+  const int bi = rem - bj * g.ni;
+  const int I = bi * 4 + (l & 3), J = bj * 4 + ((l >> 2) & 3), K = bk * 4 + (l >> 4);
+  const long long n = (long long)b * 64 + l;
+  R t;
+  mask[a * fstride + n] = adj_face_valid<R>(g, active, F, fstride, a, I, J, K, n, &t) ? 1 : 0;
+}
+
+// extrapolate^T for one layer whose input validity is vin:
+//   in-bar(q) = out-bar(q)             if q valid or q had no valid neighbour
+//             + sum over invalid neighbours n of q with count(n) > 0 of
+//               out-bar(n) / count(n)  (q valid)
+template <typename R>
+__global__ void __launch_bounds__(192)
+    k_adj_extrapolate(GridDesc g, const int* __restrict__ active_list,
+                      const unsigned char* __restrict__ active, const R* __restrict__ obar,
+                      R* __restrict__ ibar, const unsigned char* __restrict__ vin,
+                      long long fstride) {
+  const int b = active_list[blockIdx.x];
+  const int a = threadIdx.x >> 6;
+  const int l = threadIdx.x & 63;
+  const int bk = b / (g.ni * g.nj);
+  const int rem = b - bk * g.ni * g.nj;
+  const int bj = rem / g.ni;
+  const int bi = rem - bj * g.ni;
+  const int I = bi * 4 + (l & 3), J = bj * 4 + ((l >> 2) & 3), K = bk * 4 + (l >> 4);
+  const long long n = (long long)b * 64 + l;
+  const R* ob = obar + a * fstride;
+  const unsigned char* vi = vin + a * fstride;
+  const int dI[6] = {-1, 1, 0, 0, 0, 0};
+  const int dJ[6] = {0, 0, -1, 1, 0, 0};
+  const int dK[6] = {0, 0, 0, 0, -1, 1};
+  // number of valid neighbours of the face (I, J, K) as the forward layer counts them
+  auto count_at = [&](int x0, int y0, int z0) {
+    int cnt = 0;
+    for (int r = 0; r < 6; ++r) {
+      const int x = x0 + dI[r], y = y0 + dJ[r], z = z0 + dK[r];
+      if (!in_grid(g, x, y, z) || !active[bucket_of(g, x, y, z)]) continue;
+      if (vi[node_linear(g, x, y, z)]) ++cnt;
+    }
+    return cnt;
+  };
+  R acc = 0;
+  if (vi[n] || count_at(I, J, K) == 0) acc = ob[n];
+  if (vi[n]) {
+    for (int r = 0; r < 6; ++r) {
+      const int x = I + dI[r], y = J + dJ[r], z = K + dK[r];
+      if (!in_grid(g, x, y, z) || !active[bucket_of(g, x, y, z)]) continue;
+      const long long q = node_linear(g, x, y, z);
+      if (vi[q]) continue;
+      const int cnt = count_at(x, y, z);
+      if (cnt > 0) acc += ob[q] / (R)cnt;
+    }
+  }
+  ibar[a * fstride + n] = acc;
+}
+
+// apply^T to the cells: p-bar(c) = sum over valid faces f of c of -+ s_f u-bar_f
+// (the face above c along an axis has c as its left cell: +s; the face at c
+// has c as its right cell: -s), kept on the DOFs; written to G_B as the rhs
+// of the adjoint solve.
+template <typename R>
+__global__ void __launch_bounds__(64)
+    k_adj_apply(GridDesc g, const int* __restrict__ active_list,
+                const unsigned char* __restrict__ active, const unsigned char* __restrict__ dof,
+                const R* __restrict__ AG, R* __restrict__ F, long long fstride, R dt) {
+  const int b = active_list[blockIdx.x];
+  const int l = threadIdx.x;
+  const int bk = b / (g.ni * g.nj);
+  const int rem = b - bk * g.ni * g.nj;
+  const int bj = rem / g.ni;
+  const int bi = rem - bj * g.ni;
+  const int I = bi * 4 + (l & 3), J = bj * 4 + ((l >> 2) & 3), K = bk * 4 + (l >> 4);
+  const long long n = (long long)b * 64 + l;
+  const R dx = (R)g.dx;
+  R acc = 0;
+  if (dof[n] & 1) {
+    for (int a = 0; a < 3; ++a) {
+      // face at the cell (the cell is its right side)
+      R t;
+      if (adj_face_valid<R>(g, active, F, fstride, a, I, J, K, n, &t)) {
+        const R s = ((dt * F[(G_VOL + a) * fstride + n]) * F[(G_INVC + a) * fstride + n]) / (dx * t);
+        acc -= s * AG[(A_UBAR + a) * fstride + n];
+      }
+      // face above the cell (the cell is its left side)
+      const int uI = I + (a == 0), uJ = J + (a == 1), uK = K + (a == 2);
+      if (in_grid(g, uI, uJ, uK) && active[bucket_of(g, uI, uJ, uK)]) {
+        const long long u = node_linear(g, uI, uJ, uK);
+        if (adj_face_valid<R>(g, active, F, fstride, a, uI, uJ, uK, u, &t)) {
+          const R s = ((dt * F[(G_VOL + a) * fstride + u]) * F[(G_INVC + a) * fstride + u]) / (dx * t);
+          acc += s * AG[(A_UBAR + a) * fstride + u];
+        }
+      }
+    }
+  }
+  F[G_B * fstride + n] = acc;
+}
+
+// assembly^T plus the identity part of apply: per face,
+//   v*-bar = u-bar + (psi_fs w / dx) (lambda(cell at the face) - lambda(cell below))
+// over the DOF cells (lambda = the adjoint solve's solution in G_PRESSURE).
+template <typename R>
+__global__ void __launch_bounds__(192)
+    k_adj_div(GridDesc g, const int* __restrict__ active_list,
+              const unsigned char* __restrict__ active, const unsigned char* __restrict__ dof,
+              const R* __restrict__ F, long long fstride, R* __restrict__ AG) {
+  const int b = active_list[blockIdx.x];
+  const int a = threadIdx.x >> 6;
+  const int l = threadIdx.x & 63;
+  const int bk = b / (g.ni * g.nj);
+  const int rem = b - bk * g.ni * g.nj;
+  const int bj = rem / g.ni;
+  const int bi = rem - bj * g.ni;
+  const int I = bi * 4 + (l & 3), J = bj * 4 + ((l >> 2) & 3), K = bk * 4 + (l >> 4);
+  const long long n = (long long)b * 64 + l;
+  const R dx = (R)g.dx;
+  R lam = 0;
+  if (dof[n] & 1) lam += F[G_PRESSURE * fstride + n];
+  const int lI = I - (a == 0), lJ = J - (a == 1), lK = K - (a == 2);
+  if (in_grid(g, lI, lJ, lK) && active[bucket_of(g, lI, lJ, lK)]) {
+    const long long c = node_linear(g, lI, lJ, lK);
+    if (dof[c] & 1) lam -= F[G_PRESSURE * fstride + c];
+  }
+  const R k = (F[(G_PSIFS + a) * fstride + n] * F[(G_WEIGHT + a) * fstride + n]) / dx;
+  AG[(A_VSBAR + a) * fstride + n] = AG[(A_UBAR + a) * fstride + n] + k * lam;
+}
+
+// stepVelocity^T and P2G^T per particle over its own face stencils (nodes of
+// inactive buckets skipped): mom-bar = v*-bar / m_node on heavy nodes,
+//   v-bar_a = sum m w mom-bar,  C-bar_aq = sum m w mom-bar d_q;
+// results in original particle order.
+template <typename R>
+__global__ void __launch_bounds__(128)
+    k_adj_p2g(GridDesc g, const unsigned char* __restrict__ active, const R* __restrict__ P,
+              long long pcap, long long np, const int* __restrict__ pid,
+              const long long* __restrict__ key, const int* __restrict__ delta,
+              const R* __restrict__ F, const R* __restrict__ AG, long long fstride,
+              double* __restrict__ vbar0, double* __restrict__ Cbar0) {
+  const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= np) return;
+  const long long i = pid[s];
+  const long long kn = key[s];
+  if (kn < 0) return;
+  const R org[3] = {(R)g.ox, (R)g.oy, (R)g.oz};
+  const R bs = (R)g.bs, dx = (R)g.dx;
+  const R invh = R(1) / dx;
+  const R x = P[PX * pcap + s], y = P[PY * pcap + s], z = P[PZ * pcap + s];
+  const R m = P[PM * pcap + s];
+  int KI, KJ, KK;
+  node_ijk(g, kn, KI, KJ, KK);
+  const int kp[3] = {KI - 1, KJ - 1, KK - 1};
+  const int dl = delta[s];
+  for (int a = 0; a < 3; ++a) {
+    int base[3];
+    for (int q = 0; q < 3; ++q) base[q] = kp[q] + (q == a ? unpack_delta(dl, a) : 0);
+    R cx[3], cy[3], cz[3], wx[3], wy[3], wz[3];
+    for (int t = 0; t < 3; ++t) {
+      cx[t] = coord<R>(org[0], bs, dx, base[0] + t, a == 0 ? R(0) : R(0.5));
+      cy[t] = coord<R>(org[1], bs, dx, base[1] + t, a == 1 ? R(0) : R(0.5));
+      cz[t] = coord<R>(org[2], bs, dx, base[2] + t, a == 2 ? R(0) : R(0.5));
+      wx[t] = quad_kernel<R>((x - cx[t]) * invh);
+      wy[t] = quad_kernel<R>((y - cy[t]) * invh);
+      wz[t] = quad_kernel<R>((z - cz[t]) * invh);
+    }
+    const R* VS = AG + (A_VSBAR + a) * fstride;
+    const R* MS = F + (G_MASS + a) * fstride;
+    R vb = 0, b0 = 0, b1 = 0, b2 = 0;
+    for (int k = 0; k < 3; ++k)
+      for (int j = 0; j < 3; ++j)
+        for (int ii = 0; ii < 3; ++ii) {
+          const int NI_ = base[0] + ii, NJ_ = base[1] + j, NK_ = base[2] + k;
+          if (!in_grid(g, NI_, NJ_, NK_) || !active[bucket_of(g, NI_, NJ_, NK_)]) continue;
+          const long long nn = node_linear(g, NI_, NJ_, NK_);
+          const R mn = MS[nn];
+          if (!(mn > R(1e-20))) continue;
+          const R mw = (m * (wx[ii] * wy[j] * wz[k])) * (VS[nn] / mn);
+          vb += mw;
+          b0 += mw * (cx[ii] - x);
+          b1 += mw * (cy[j] - y);
+          b2 += mw * (cz[k] - z);
+        }
+    vbar0[i * 3 + a] = (double)vb;
+    Cbar0[i * 9 + a * 3 + 0] = (double)b0;
+    Cbar0[i * 9 + a * 3 + 1] = (double)b1;
+    Cbar0[i * 9 + a * 3 + 2] = (double)b2;
+  }
+}
+
+}  // namespace wcg

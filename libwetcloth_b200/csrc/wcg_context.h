@@ -224,6 +224,11 @@ struct Context {
   struct MgDims { int ni, nj, nk, n; long long off; };
   std::vector<MgDims> mg_dims;     // levels of the last solve
 
+  // reverse mode of a sub-step (wcg_adjoint.cuh): grid cotangents, particle
+  // cotangents (sorted order), the first extrapolation layer's input mask,
+  // host staging
+  DevBuf adj, adjp, adjmask, adjstage;
+
   // FP64 refinement vectors (precision 1)
   DevBuf rx64, rr64, rb64;       // nnode doubles each
 
@@ -308,6 +313,11 @@ cudaError_t map_grid_to_particles_and_advect(Context& c, double dt, bool advect)
 cudaError_t advect_only(Context& c, double dt);
 cudaError_t num_substeps(Context& c, double dt, int* n);
 cudaError_t substep(Context& c, double dt);
+// Reverse mode of substep at the current (pre-step) particle state with the
+// positions held fixed: cotangents of (v', C', x') in, of (v, C) out (host
+// arrays, original order; x-bar passes through unchanged).
+cudaError_t substep_vjp(Context& c, double dt, const double* vbar, const double* Cbar,
+                        const double* xbar, double* vbar0, double* Cbar0);
 // record the message returned by wcg_last_error() on this thread; returns code
 int set_last_error(int code, const std::string& msg);
 // FP64 MIC(0)-PCG on a system already placed in the context's fields

@@ -15,6 +15,7 @@
 #include "wcg_mg.cuh"
 #include "wcg_visc.cuh"
 #include "wcg_elasto.cuh"
+#include "wcg_adjoint.cuh"
 #include "wcg_scan.cuh"
 
 namespace wcg {
@@ -1569,6 +1570,9 @@ static cudaError_t mg_project(Context& c, double bnorm) {
 }
 
 template <typename R>
+static cudaError_t solve_assembled_t(Context& c);
+
+template <typename R>
 static cudaError_t project_fine_t(Context& c, double dt) {
   c.stats.pcg_iters = 0;
   c.stats.refinements = 0;
@@ -1580,12 +1584,30 @@ static cudaError_t project_fine_t(Context& c, double dt) {
   const int* al = c.active_list.as<int>();
   const unsigned char* act = c.active.as<unsigned char>();
   unsigned char* dof = c.gdof.as<unsigned char>();
-  const long long nent = c.n_active * 64;
   {
     ProfScope prof(c, P_GRIDOPS);
     ++c.launches, k_assemble<R><<<(unsigned)c.n_active, 64, 0, c.stream>>>(c.g, al, act, F, c.gcap, dof, (R)dt);
   }
   WCG_TRY(cudaGetLastError());
+  return solve_assembled_t<R>(c);
+}
+
+// The pressure solve of projectFine on the system in the context's fields
+// (G_ADIAG, G_AX/AY/AZ, DOF flags, rhs G_B, zero off the DOFs); the solution
+// goes to G_PRESSURE.
+template <typename R>
+static cudaError_t solve_assembled_t(Context& c) {
+  c.stats.pcg_iters = 0;
+  c.stats.refinements = 0;
+  c.stats.residual = 0;
+  c.stats.rhs_norm = 0;
+  c.stats.converged = 1;
+  if (c.n_active == 0) return cudaSuccess;
+  R* F = c.gfield.as<R>();
+  const int* al = c.active_list.as<int>();
+  const unsigned char* act = c.active.as<unsigned char>();
+  unsigned char* dof = c.gdof.as<unsigned char>();
+  const long long nent = c.n_active * 64;
   double* dsc = c.dscalars.as<double>();
   double* part = c.scratch.as<double>();
   R* r = F + G_R * c.gcap;
@@ -1901,6 +1923,81 @@ cudaError_t prepared_solve_fp64(Context& c, double* out, int* iters, double* res
   ++c.launches, k_copy_dof<double><<<kRedBlocks, kRedThreads, 0, c.stream>>>(al, nent, dof, x, out);
   WCG_TRY(cudaGetLastError());
   return cudaStreamSynchronize(c.stream);
+}
+
+template <typename R>
+static cudaError_t substep_vjp_t(Context& c, double dt, const double* vbar, const double* Cbar,
+                                 const double* xbar, double* vbar0, double* Cbar0) {
+  const long long np = c.np;
+  // forward recompute at the checkpoint: grid, fields, matrix, masks (the
+  // particle state is not touched)
+  WCG_TRY(build_grid(c));
+  WCG_TRY(map_particles_to_grid(c));
+  WCG_TRY(step_velocity(c, dt));
+  WCG_TRY(project_fine(c, dt));
+  WCG_TRY(apply_pressure_and_extrapolate(c, dt));
+  if (np == 0 || c.n_active == 0) {
+    std::fill(vbar0, vbar0 + 3 * np, 0.0);
+    std::fill(Cbar0, Cbar0 + 9 * np, 0.0);
+    return cudaSuccess;
+  }
+  const int rb = c.real_bytes();
+  WCG_TRY(c.adj.ensure((size_t)kNumAdjFields * c.gcap * rb));
+  WCG_TRY(c.adjmask.ensure((size_t)3 * c.gcap));
+  WCG_TRY(c.adjp.ensure((size_t)12 * c.pcap * rb));
+  WCG_TRY(c.adjstage.ensure((size_t)15 * np * sizeof(double)));
+  double* st = c.adjstage.as<double>();
+  WCG_TRY(cudaMemcpyAsync(st, vbar, 3 * np * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+  WCG_TRY(cudaMemcpyAsync(st + 3 * np, Cbar, 9 * np * sizeof(double), cudaMemcpyHostToDevice,
+                          c.stream));
+  WCG_TRY(cudaMemcpyAsync(st + 12 * np, xbar, 3 * np * sizeof(double), cudaMemcpyHostToDevice,
+                          c.stream));
+  R* F = c.gfield.as<R>();
+  R* AG = c.adj.as<R>();
+  R* B = c.adjp.as<R>();
+  const int* al = c.active_list.as<int>();
+  const unsigned char* act = c.active.as<unsigned char>();
+  const unsigned char* dof = c.gdof.as<unsigned char>();
+  unsigned char* vtmp = c.gvalid.as<unsigned char>() + 3 * c.gcap;  // layer-1 output mask
+  unsigned char* v0 = c.adjmask.as<unsigned char>();
+  const unsigned nb = (unsigned)c.n_active;
+  DeltaRange dr;
+  for (int a = 0; a < 3; ++a) {
+    dr.lo[a] = c.drange_h[a];
+    dr.hi[a] = c.drange_h[3 + a];
+  }
+  ++c.launches, k_adj_load<R><<<nblk(np, 256), 256, 0, c.stream>>>(
+      np, c.pcap, c.pid[c.cur].as<int>(), st, st + 3 * np, st + 12 * np, dt, B);
+  ++c.launches, k_adj_g2p<R><<<nb, 192, 0, c.stream>>>(
+      c.g, al, c.pbuf[c.cur].as<R>(), c.pcap, c.cell_start.as<int>(),
+      c.pdelta.as<int>() + c.cur * c.pcap, dr, B, F, c.gcap, AG, (R)c.prm.flip_coeff,
+      (R)c.prm.liquid_boundary_friction);
+  // extrapolation layers in reverse: layer 2 read the layer-1 output mask,
+  // layer 1 the validity after the pressure gradient
+  ++c.launches, k_adj_extrapolate<R><<<nb, 192, 0, c.stream>>>(
+      c.g, al, act, AG + A_UBAR * c.gcap, AG + A_UTMP * c.gcap, vtmp, c.gcap);
+  ++c.launches, k_adj_valid0<R><<<nb, 192, 0, c.stream>>>(c.g, al, act, F, c.gcap, v0);
+  ++c.launches, k_adj_extrapolate<R><<<nb, 192, 0, c.stream>>>(
+      c.g, al, act, AG + A_UTMP * c.gcap, AG + A_UBAR * c.gcap, v0, c.gcap);
+  ++c.launches, k_adj_apply<R><<<nb, 64, 0, c.stream>>>(c.g, al, act, dof, AG, F, c.gcap, (R)dt);
+  WCG_TRY(cudaGetLastError());
+  WCG_TRY(solve_assembled_t<R>(c));  // A lambda = p-bar, A symmetric
+  ++c.launches, k_adj_div<R><<<nb, 192, 0, c.stream>>>(c.g, al, act, dof, F, c.gcap, AG);
+  ++c.launches, k_adj_p2g<R><<<nblk(np, 128), 128, 0, c.stream>>>(
+      c.g, act, c.pbuf[c.cur].as<R>(), c.pcap, np, c.pid[c.cur].as<int>(),
+      c.pkey.as<long long>() + c.cur * c.pcap, c.pdelta.as<int>() + c.cur * c.pcap, F, AG,
+      c.gcap, st, st + 3 * np);
+  WCG_TRY(cudaGetLastError());
+  WCG_TRY(cudaMemcpyAsync(vbar0, st, 3 * np * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  WCG_TRY(cudaMemcpyAsync(Cbar0, st + 3 * np, 9 * np * sizeof(double), cudaMemcpyDeviceToHost,
+                          c.stream));
+  return cudaStreamSynchronize(c.stream);
+}
+
+cudaError_t substep_vjp(Context& c, double dt, const double* vbar, const double* Cbar,
+                        const double* xbar, double* vbar0, double* Cbar0) {
+  return c.prm.precision == 0 ? substep_vjp_t<double>(c, dt, vbar, Cbar, xbar, vbar0, Cbar0)
+                              : substep_vjp_t<float>(c, dt, vbar, Cbar, xbar, vbar0, Cbar0);
 }
 
 cudaError_t substep(Context& c, double dt) {

@@ -73,8 +73,27 @@ class FluidScene:
         arr = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
         x, v, C, mass, vol, radius = map(arr, (x, v, C, mass, vol, radius))
         n = mass.shape[0]
+        self._attrs = (mass, vol, radius)
         check(self.L.wcg_upload_liquid(self.h, n, _dp(x), _dp(v), _dp(C), _dp(mass),
                                        _dp(vol), _dp(radius)))
+
+    def set_state(self, x, v, C):
+        """Replace the liquid particles' positions, velocities and affine
+        matrices (mass, volume and radius as last uploaded)."""
+        self.upload(x, v, C, *self._attrs)
+
+    def substep_vjp(self, dt, vbar, Cbar, xbar):
+        """Reverse mode of substep(dt) at the current (pre-step) state with the
+        positions held fixed: cotangents of (v', C', x') -> of (v, C, x)."""
+        n = self.num_particles
+        arr = lambda a, k: np.ascontiguousarray(a, dtype=np.float64).reshape(n * k)
+        vb, Cb, xb = arr(vbar, 3), arr(Cbar, 9), arr(xbar, 3)
+        v0 = np.empty(n * 3)
+        C0 = np.empty(n * 9)
+        x0 = np.empty(n * 3)
+        check(self.L.wcg_substep_vjp(self.h, dt, _dp(vb), _dp(Cb), _dp(xb), _dp(v0), _dp(C0),
+                                     _dp(x0)))
+        return v0.reshape(n, 3), C0.reshape(n, 9), x0.reshape(n, 3)
 
     def upload_device(self, n, x, v, C, mass, vol, radius):
         """Arguments are device pointers (ints) to contiguous float64 arrays."""

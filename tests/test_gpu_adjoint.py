@@ -1,0 +1,164 @@
+"""Reverse mode of one liquid sub-step (wcg_substep_vjp, libwetcloth_b200.autograd).
+
+With the positions fixed the sub-step is affine in the particles' velocities
+v and affine matrices C, so central differences of the forward are exact up
+to rounding and the solver tolerance.  Checks, at a 1e-12 pressure criterion:
+- the adjoint identity <y, J d> = <J^T y, d> for random d and y, with J d from
+  central differences of the GPU forward (FP64: 1e-9 relative; FP32 with FP64
+  refinement: 1e-4);
+- the same with J d from central differences of the FP64 oracle, the C
+  restatement pinned to the reference (an FP64 reference gradient: 1e-6);
+- torch.autograd gradients of a scalar loss against per-entry central
+  differences (1e-4 relative, the tolerance the plan states)."""
+import numpy as np
+import pytest
+
+from libwetcloth_b200 import _capi, scenes
+from libwetcloth_b200.solver import FluidScene
+from oracle import oracle as oo
+
+pytestmark = pytest.mark.gpu
+DT = 1e-3
+
+
+def _scene(kind):
+    if kind == "dam16":
+        sc = scenes.dam_break(16, 8, 0)
+    else:
+        sc = scenes.half_box(24, 2, 7, amplitude=1.0, sigma_cells=1.5)
+    sc.params.criterion = 1e-12
+    rng = np.random.default_rng(11)
+    sc.C = rng.normal(0.0, 2.0, (sc.x.shape[0], 9))
+    return sc
+
+
+def _forward(g, x, v, C):
+    g.set_state(x, v, C)
+    g.substep(DT)
+    x1, v1, C1 = g.download()
+    return np.concatenate([v1.ravel(), C1.ravel(), x1.ravel()])
+
+
+def _oracle_forward(sc, v, C):
+    s2 = scenes.Scene(sc.params, sc.x.copy(), v.copy(), sc.mass, sc.vol, sc.radius, C=C.copy())
+    o = oo.OracleScene(s2)
+    o.L.wco_substep(o.h, DT, 1)
+    n = sc.x.shape[0]
+    out = np.concatenate([o.get("g2p_v"), o.get("g2p_C"), o.get("adv_x")])
+    o.close()
+    assert out.shape[0] == 15 * n
+    return out
+
+
+def _directions(n, seed):
+    rng = np.random.default_rng(seed)
+    dv = rng.normal(size=(n, 3))
+    dC = rng.normal(size=(n, 9)) * 10.0
+    y = rng.normal(size=15 * n)
+    return dv, dC, y
+
+
+def _vjp(g, sc, y):
+    n = sc.x.shape[0]
+    g.set_state(sc.x, sc.v, sc.C)
+    vb, Cb, xb = g.substep_vjp(DT, y[:3 * n].reshape(n, 3), y[3 * n:12 * n].reshape(n, 9),
+                               y[12 * n:].reshape(n, 3))
+    assert np.array_equal(xb.ravel(), y[12 * n:])
+    return vb, Cb
+
+
+@pytest.mark.parametrize("kind", ["dam16", "curl24"])
+def test_adjoint_identity_fp64(kind, wcg):
+    sc = _scene(kind)
+    n = sc.x.shape[0]
+    g = FluidScene(sc)
+    dv, dC, y = _directions(n, 3)
+    h = 1e-2
+    Jd = (_forward(g, sc.x, sc.v + h * dv, sc.C + h * dC) -
+          _forward(g, sc.x, sc.v - h * dv, sc.C - h * dC)) / (2 * h)
+    vb, Cb = _vjp(g, sc, y)
+    lhs = float(y @ Jd)
+    rhs = float((vb * dv).sum() + (Cb * dC).sum())
+    assert abs(lhs - rhs) <= 1e-9 * max(abs(lhs), np.abs(y).sum() * 1e-12), (lhs, rhs)
+    g.close()
+
+
+def test_adjoint_identity_fp32_refine(wcg):
+    sc = _scene("curl24")
+    n = sc.x.shape[0]
+    g = FluidScene(sc, precision=_capi.WCG_FP32_REFINE)
+    dv, dC, y = _directions(n, 5)
+    h = 1e-1
+    Jd = (_forward(g, sc.x, sc.v + h * dv, sc.C + h * dC) -
+          _forward(g, sc.x, sc.v - h * dv, sc.C - h * dC)) / (2 * h)
+    vb, Cb = _vjp(g, sc, y)
+    lhs = float(y @ Jd)
+    rhs = float((vb * dv).sum() + (Cb * dC).sum())
+    assert abs(lhs - rhs) <= 1e-4 * abs(lhs), (lhs, rhs)
+    g.close()
+
+
+def test_adjoint_against_fp64_oracle(wcg):
+    """J d from the C restatement (pinned to the reference), J^T y from the
+    GPU reverse mode."""
+    sc = _scene("dam16")
+    n = sc.x.shape[0]
+    dv, dC, y = _directions(n, 9)
+    h = 1e-2
+    Jd = (_oracle_forward(sc, sc.v + h * dv, sc.C + h * dC) -
+          _oracle_forward(sc, sc.v - h * dv, sc.C - h * dC)) / (2 * h)
+    g = FluidScene(sc)
+    vb, Cb = _vjp(g, sc, y)
+    lhs = float(y @ Jd)
+    rhs = float((vb * dv).sum() + (Cb * dC).sum())
+    assert abs(lhs - rhs) <= 1e-6 * abs(lhs), (lhs, rhs)
+    g.close()
+
+
+def test_autograd_against_central_differences(wcg):
+    torch = pytest.importorskip("torch")
+    from libwetcloth_b200.autograd import substep
+    sc = _scene("curl24")
+    n = sc.x.shape[0]
+    g = FluidScene(sc)
+    rng = np.random.default_rng(2)
+    wx = torch.from_numpy(rng.normal(size=(n, 3)))
+    target = torch.from_numpy(rng.normal(size=(n, 3)))
+
+    def loss_of(v, C):
+        x1, v1, C1 = substep(g, torch.from_numpy(sc.x), v, C, DT)
+        return ((v1 - target) ** 2).sum() + (x1 * wx).sum() + 1e-3 * (C1 ** 2).sum()
+
+    v = torch.from_numpy(sc.v.copy()).requires_grad_(True)
+    C = torch.from_numpy(sc.C.copy()).requires_grad_(True)
+    L = loss_of(v, C)
+    L.backward()
+    gv, gC = v.grad.numpy().copy(), C.grad.numpy().copy()
+    h = 1e-3
+    for (arr, grad, name) in ((sc.v, gv, "v"), (sc.C, gC, "C")):
+        for idx in rng.choice(arr.size, 6, replace=False):
+            p = arr.copy().ravel()
+            p[idx] += h
+            m = arr.copy().ravel()
+            m[idx] -= h
+            if name == "v":
+                lp = loss_of(torch.from_numpy(p.reshape(arr.shape)), torch.from_numpy(sc.C)).item()
+                lm = loss_of(torch.from_numpy(m.reshape(arr.shape)), torch.from_numpy(sc.C)).item()
+            else:
+                lp = loss_of(torch.from_numpy(sc.v), torch.from_numpy(p.reshape(arr.shape))).item()
+                lm = loss_of(torch.from_numpy(sc.v), torch.from_numpy(m.reshape(arr.shape))).item()
+            fd = (lp - lm) / (2 * h)
+            gr = grad.ravel()[idx]
+            assert abs(fd - gr) <= 1e-4 * max(abs(fd), np.abs(grad).max() * 1e-3), (name, idx, fd, gr)
+    g.close()
+
+
+def test_adjoint_refuses_viscosity(wcg):
+    sc = _scene("dam16")
+    sc.params.viscosity = 1.0
+    g = FluidScene(sc)
+    n = sc.x.shape[0]
+    with pytest.raises(_capi.WcgError) as e:
+        g.substep_vjp(DT, np.zeros((n, 3)), np.zeros((n, 9)), np.zeros((n, 3)))
+    assert e.value.code == _capi.WCG_ERR_UNSUPPORTED
+    g.close()
