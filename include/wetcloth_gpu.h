@@ -176,12 +176,16 @@ int wcg_num_substeps(wcg_ctx* ctx, double dt, int* n_out);
  * the sub-step; it recomputes the forward grid fields there and leaves the
  * particles unchanged.  In: cotangents of the sub-step's outputs v' (3n),
  * C' (9n, rows as in wcg_download_liquid) and x' (3n).  Out: cotangents of
- * the inputs v (3n) and C (9n); xbar0 = xbar3 (positions are held fixed: the
- * weights' dependence on x is not differentiated).  Liquid scenes without
- * viscosity; the solve is the forward's solver on the same (symmetric)
- * matrix. */
+ * the inputs v (3n) and C (9n), of the liquid viscosity (viscosity_bar, may be
+ * NULL; 0 when the viscosity is off); xbar0 = xbar3 (positions are held
+ * fixed: the weights' dependence on x is not differentiated).  Liquid scenes;
+ * the solve is the forward's solver on the same (symmetric) matrix. */
 int wcg_substep_vjp(wcg_ctx* ctx, double dt, const double* vbar3, const double* Cbar9,
-                    const double* xbar3, double* vbar0, double* Cbar0, double* xbar0);
+                    const double* xbar3, double* vbar0, double* Cbar0, double* xbar0,
+                    double* viscosity_bar);
+/* LiquidInfo::viscosity and the explicit viscosity sub-steps of a context
+ * (0: off), as wcg_params sets them at creation. */
+int wcg_set_viscosity(wcg_ctx* ctx, double viscosity, int substeps);
 
 int wcg_get_stats(const wcg_ctx* ctx, wcg_stats* out);
 

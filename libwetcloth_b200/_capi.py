@@ -107,7 +107,9 @@ SIGNATURES = {
     "wcg_substep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "wcg_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _I]),
     "wcg_num_substeps": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _I]),
-    "wcg_substep_vjp": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _D, _D, _D, _D, _D, _D]),
+    "wcg_substep_vjp": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _D, _D, _D, _D, _D, _D,
+                                       _D]),
+    "wcg_set_viscosity": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]),
     "wcg_get_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(WcgStats)]),
     "wcg_grid_info": (ctypes.c_int, [ctypes.c_void_p, _I, _D, _D]),
     "wcg_field_size": (ctypes.c_longlong, [ctypes.c_void_p, ctypes.c_char_p]),

@@ -1,9 +1,10 @@
 """torch.autograd binding of one liquid sub-step (the C-ABI's wcg_substep and
 wcg_substep_vjp); the arithmetic is all in libwcgpu.so.
 
-``substep(scene, x, v, C, dt)`` returns (x', v', C') as float64 tensors and
-records a node whose backward restores the checkpoint (x, v, C) in the scene,
-recomputes the forward grid there and runs the reverse-mode kernels.  The
+``substep(scene, x, v, C, dt, viscosity)`` returns (x', v', C') as float64
+tensors and records a node whose backward restores the checkpoint (x, v, C)
+in the scene, recomputes the forward grid there and runs the reverse-mode
+kernels; an optional 0-d ``viscosity`` tensor gets its gradient too.  The
 positions are held fixed in the derivative: d(x')/d(x) is the identity and the
 weights' dependence on x is not differentiated, so gradients through several
 chained sub-steps omit that term.  The scene's particle state after backward is
@@ -17,13 +18,17 @@ import torch
 
 class _Substep(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, x, v, C, scene, dt):
+    def forward(ctx, x, v, C, mu, scene, dt, substeps):
         xs, vs, Cs = (t.detach().cpu().numpy().astype(np.float64) for t in (x, v, C))
+        m = float(mu.detach().cpu().item()) if mu is not None else None
+        if m is not None:
+            scene.set_viscosity(m, substeps)
         scene.set_state(xs, vs, Cs)
         scene.substep(dt)
         x1, v1, C1 = scene.download()
         ctx.scene = scene
         ctx.dt = dt
+        ctx.mu = (m, substeps)
         ctx.state = (xs, vs, Cs)
         dev = v.device
         return (torch.from_numpy(x1).to(dev), torch.from_numpy(v1).to(dev),
@@ -38,12 +43,18 @@ class _Substep(torch.autograd.Function):
             return np.zeros((n, k)) if g is None else g.detach().cpu().numpy().astype(np.float64)
 
         scene = ctx.scene
+        m, substeps = ctx.mu
+        if m is not None:
+            scene.set_viscosity(m, substeps)
         scene.set_state(*ctx.state)
-        vb, Cb, xb = scene.substep_vjp(ctx.dt, host(gv1, 3), host(gC1, 9), host(gx1, 3))
+        vb, Cb, xb, mub = scene.substep_vjp(ctx.dt, host(gv1, 3), host(gC1, 9), host(gx1, 3),
+                                            with_viscosity=True)
+        gmu = None if m is None else torch.tensor(mub, dtype=torch.float64, device=dev)
         return (torch.from_numpy(xb).to(dev), torch.from_numpy(vb).to(dev),
-                torch.from_numpy(Cb).to(dev), None, None)
+                torch.from_numpy(Cb).to(dev), gmu, None, None, None)
 
 
-def substep(scene, x, v, C, dt: float):
-    """One differentiable sub-step of a FluidScene (liquid, no viscosity)."""
-    return _Substep.apply(x, v, C, scene, dt)
+def substep(scene, x, v, C, dt: float, viscosity=None, viscosity_substeps: int = 1):
+    """One differentiable sub-step of a FluidScene (liquid).  viscosity: an
+    optional 0-d tensor (LiquidInfo::viscosity) that receives a gradient."""
+    return _Substep.apply(x, v, C, viscosity, scene, dt, viscosity_substeps)

@@ -239,11 +239,15 @@ __global__ void __launch_bounds__(64)
 // assembly^T plus the identity part of apply: per face,
 //   v*-bar = u-bar + (psi_fs w / dx) (lambda(cell at the face) - lambda(cell below))
 // over the DOF cells (lambda = the adjoint solve's solution in G_PRESSURE).
+// With the viscosity on, the rhs the pressure step starts from is v* m (not
+// the predictor's rhs), so u depends on v* through m inv_C (1 on heavy nodes,
+// m on light ones): rhs_from_vstar scales the identity part by it.
 template <typename R>
 __global__ void __launch_bounds__(192)
     k_adj_div(GridDesc g, const int* __restrict__ active_list,
               const unsigned char* __restrict__ active, const unsigned char* __restrict__ dof,
-              const R* __restrict__ F, long long fstride, R* __restrict__ AG) {
+              const R* __restrict__ F, long long fstride, R* __restrict__ AG,
+              int rhs_from_vstar) {
   const int b = active_list[blockIdx.x];
   const int a = threadIdx.x >> 6;
   const int l = threadIdx.x & 63;
@@ -262,7 +266,9 @@ __global__ void __launch_bounds__(192)
     if (dof[c] & 1) lam -= F[G_PRESSURE * fstride + c];
   }
   const R k = (F[(G_PSIFS + a) * fstride + n] * F[(G_WEIGHT + a) * fstride + n]) / dx;
-  AG[(A_VSBAR + a) * fstride + n] = AG[(A_UBAR + a) * fstride + n] + k * lam;
+  R ub = AG[(A_UBAR + a) * fstride + n];
+  if (rhs_from_vstar) ub *= F[(G_MASS + a) * fstride + n] * F[(G_INVC + a) * fstride + n];
+  AG[(A_VSBAR + a) * fstride + n] = ub + k * lam;
 }
 
 // stepVelocity^T and P2G^T per particle over its own face stencils (nodes of
@@ -323,6 +329,110 @@ __global__ void __launch_bounds__(128)
     Cbar0[i * 9 + a * 3 + 0] = (double)b0;
     Cbar0[i * 9 + a * 3 + 1] = (double)b1;
     Cbar0[i * 9 + a * 3 + 2] = (double)b2;
+  }
+}
+
+// ---- explicit viscosity (k_viscosity_explicit) ------------------------------
+// One explicit step is v_out = v_in + f K v_in with f = sub_dt mu / (rho dx^2).
+// Per output component a, K has six same-component neighbour terms
+// c_t (v_a(n + o_t) - v_a(n)) (present when n + o_t is in an active bucket)
+// and eight cross terms +-c (v_b(n + o)) (zero outside active buckets).  The
+// coefficients c are volume fractions at fixed offsets from n (times 2 on the
+// component's own axis).  The table below lists, per component: the six
+// coefficient sources {field, offset} in the order (+x, -x, +y, -y, +z, -z)
+// with their multipliers, and the cross terms {component, offset, sign,
+// coefficient}; it restates k_viscosity_explicit term by term.
+struct VCoef { signed char field, di, dj, dk; };   // field 0 centre, 1..3 x/y/z edge
+struct VCross { signed char comp, di, dj, dk, sign, coef; };
+__constant__ VCoef kVCoef[3][6] = {
+    {{0, 0, 0, 0}, {0, -1, 0, 0}, {3, 0, 1, 0}, {3, 0, 0, 0}, {2, 0, 0, 1}, {2, 0, 0, 0}},
+    {{3, 1, 0, 0}, {3, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, -1, 0}, {1, 0, 0, 1}, {1, 0, 0, 0}},
+    {{2, 1, 0, 0}, {2, 0, 0, 0}, {1, 0, 1, 0}, {1, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, -1}}};
+__constant__ signed char kVMult[3][6] = {{2, 2, 1, 1, 1, 1}, {1, 1, 2, 2, 1, 1}, {1, 1, 1, 1, 2, 2}};
+__constant__ VCross kVCross[3][8] = {
+    {{1, 0, 1, 0, 1, 2}, {1, -1, 1, 0, -1, 2}, {1, -1, 0, 0, 1, 3}, {1, 0, 0, 0, -1, 3},
+     {2, 0, 0, 1, 1, 4}, {2, -1, 0, 1, -1, 4}, {2, -1, 0, 0, 1, 5}, {2, 0, 0, 0, -1, 5}},
+    {{0, 1, 0, 0, 1, 0}, {0, 1, -1, 0, -1, 0}, {0, 0, -1, 0, 1, 1}, {0, 0, 0, 0, -1, 1},
+     {2, 0, 0, 1, 1, 4}, {2, 0, -1, 1, -1, 4}, {2, 0, -1, 0, 1, 5}, {2, 0, 0, 0, -1, 5}},
+    {{0, 1, 0, 0, 1, 0}, {0, 1, 0, -1, -1, 0}, {0, 0, 0, -1, 1, 1}, {0, 0, 0, 0, -1, 1},
+     {1, 0, 1, 0, 1, 2}, {1, 0, 1, -1, -1, 2}, {1, 0, 0, -1, 1, 3}, {1, 0, 0, 0, -1, 3}}};
+__constant__ signed char kVDir[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0},
+                                        {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+
+template <typename R>
+__device__ inline R v_coef(const GridDesc& g, const unsigned char* active, const R* F,
+                           long long fs, int a, int t, int I, int J, int K) {
+  const VCoef c = kVCoef[a][t];
+  const int fld = c.field == 0 ? G_VFC : G_VFEX + c.field - 1;
+  return (R)kVMult[a][t] *
+         v_get<R>(g, active, F + (long long)fld * fs, I + c.di, J + c.dj, K + c.dk, R(0));
+}
+
+template <typename R>
+__device__ inline bool v_live(const GridDesc& g, const unsigned char* active, int I, int J, int K) {
+  return in_grid(g, I, J, K) && active[bucket_of(g, I, J, K)];
+}
+
+// K^T: in-bar(a, m) = out-bar(a, m) + f [sum of the terms of every output
+// (b, n) that read (a, m)]; written to ib (3 fields).
+template <typename R>
+__global__ void __launch_bounds__(192)
+    k_adj_viscosity(GridDesc g, const int* __restrict__ active_list,
+                    const unsigned char* __restrict__ active, const R* __restrict__ F,
+                    long long fs, const R* __restrict__ ob, R* __restrict__ ib, R factor) {
+  const int b = active_list[blockIdx.x];
+  const int a = threadIdx.x >> 6;
+  const int l = threadIdx.x & 63;
+  const int bk = b / (g.ni * g.nj);
+  const int rem = b - bk * g.ni * g.nj;
+  const int bj = rem / g.ni;
+  const int bi = rem - bj * g.ni;
+  const int I = bi * 4 + (l & 3), J = bj * 4 + ((l >> 2) & 3), K = bk * 4 + (l >> 4);
+  const long long m = (long long)b * 64 + l;
+  const R* oa = ob + a * fs;
+  R acc = 0;
+  for (int t = 0; t < 6; ++t) {
+    const int di = kVDir[t][0], dj = kVDir[t][1], dk = kVDir[t][2];
+    // the output at m itself: its own part of the term toward m + o_t
+    if (v_live<R>(g, active, I + di, J + dj, K + dk))
+      acc -= v_coef<R>(g, active, F, fs, a, t, I, J, K) * oa[m];
+    // the output at n = m - o_t whose term reads m
+    const int nI = I - di, nJ = J - dj, nK = K - dk;
+    if (v_live<R>(g, active, nI, nJ, nK))
+      acc += v_coef<R>(g, active, F, fs, a, t, nI, nJ, nK) * oa[node_linear(g, nI, nJ, nK)];
+  }
+  for (int c = 0; c < 3; ++c) {
+    if (c == a) continue;
+    for (int t = 0; t < 8; ++t) {
+      const VCross x = kVCross[c][t];
+      if (x.comp != a) continue;
+      // output (c, n) reads (a, n + o) = (a, m)
+      const int nI = I - x.di, nJ = J - x.dj, nK = K - x.dk;
+      if (!v_live<R>(g, active, nI, nJ, nK)) continue;
+      const R cf = v_coef<R>(g, active, F, fs, c, x.coef, nI, nJ, nK) / (R)kVMult[c][x.coef];
+      acc += (R)x.sign * cf * ob[c * fs + node_linear(g, nI, nJ, nK)];
+    }
+  }
+  ib[a * fs + m] = oa[m] + factor * acc;
+}
+
+// <out-bar, v_out - v_in> over the faces of the active buckets, per block
+// (the viscosity cotangent: each explicit step's increment is linear in mu)
+template <typename R>
+__global__ void __launch_bounds__(192)
+    k_adj_mu_dot(const int* __restrict__ active_list, const R* __restrict__ ob,
+                 const R* __restrict__ vout, const R* __restrict__ vin, long long fs,
+                 double* __restrict__ part) {
+  __shared__ double sm[192];
+  const int b = active_list[blockIdx.x];
+  const int a = threadIdx.x >> 6;
+  const long long n = (long long)b * 64 + (threadIdx.x & 63);
+  sm[threadIdx.x] = (double)ob[a * fs + n] * ((double)vout[a * fs + n] - (double)vin[a * fs + n]);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0;
+    for (int k = 0; k < 192; ++k) s += sm[k];
+    part[blockIdx.x] = s;
   }
 }
 

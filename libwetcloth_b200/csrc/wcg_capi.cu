@@ -514,22 +514,31 @@ int wcg_substep(wcg_ctx* ctx, double dt) {
 }
 
 int wcg_substep_vjp(wcg_ctx* ctx, double dt, const double* vbar3, const double* Cbar9,
-                    const double* xbar3, double* vbar0, double* Cbar0, double* xbar0) {
+                    const double* xbar3, double* vbar0, double* Cbar0, double* xbar0,
+                    double* viscosity_bar) {
   WCG_CHECK_CTX(ctx);
   if (!(dt > 0)) return fail(WCG_ERR_ARG, "dt must be positive");
   WCG_NO_ELASTO(ctx, "substep_vjp");
-  if (ctx->c.prm.viscosity > 0.0)
-    return fail(WCG_ERR_UNSUPPORTED, "substep_vjp: the viscosity term has no reverse mode here");
   const long long n = ctx->c.np;
   if (n > 0 && (!vbar3 || !Cbar9 || !xbar3 || !vbar0 || !Cbar0 || !xbar0))
     return fail(WCG_ERR_ARG, "null cotangent array");
-  WCG_CALL(ctx, wcg::substep_vjp(ctx->c, dt, vbar3, Cbar9, xbar3, vbar0, Cbar0), "substep_vjp");
+  WCG_CALL(ctx, wcg::substep_vjp(ctx->c, dt, vbar3, Cbar9, xbar3, vbar0, Cbar0, viscosity_bar),
+           "substep_vjp");
   int st = device_status(ctx->c, "substep_vjp");
   if (st) return st;
   for (long long i = 0; i < 3 * n; ++i) xbar0[i] = xbar3[i];
   ctx->c.have_grid = true;
   if (!ctx->c.stats.converged)
     return fail(WCG_ERR_NOT_CONVERGED, "adjoint pressure solve did not converge");
+  return WCG_OK;
+}
+
+int wcg_set_viscosity(wcg_ctx* ctx, double viscosity, int substeps) {
+  WCG_CHECK_CTX(ctx);
+  if (!(viscosity >= 0.0) || !std::isfinite(viscosity))
+    return fail(WCG_ERR_ARG, "viscosity must be finite and >= 0");
+  ctx->c.prm.viscosity = viscosity;
+  ctx->c.prm.viscosity_substeps = substeps > 0 ? substeps : 1;
   return WCG_OK;
 }
 

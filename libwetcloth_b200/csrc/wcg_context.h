@@ -227,7 +227,7 @@ struct Context {
   // reverse mode of a sub-step (wcg_adjoint.cuh): grid cotangents, particle
   // cotangents (sorted order), the first extrapolation layer's input mask,
   // host staging
-  DevBuf adj, adjp, adjmask, adjstage;
+  DevBuf adj, adjp, adjmask, adjstage, adjvisc;
 
   // FP64 refinement vectors (precision 1)
   DevBuf rx64, rr64, rb64;       // nnode doubles each
@@ -314,10 +314,11 @@ cudaError_t advect_only(Context& c, double dt);
 cudaError_t num_substeps(Context& c, double dt, int* n);
 cudaError_t substep(Context& c, double dt);
 // Reverse mode of substep at the current (pre-step) particle state with the
-// positions held fixed: cotangents of (v', C', x') in, of (v, C) out (host
-// arrays, original order; x-bar passes through unchanged).
+// positions held fixed: cotangents of (v', C', x') in, of (v, C) and of the
+// viscosity (mubar, may be null) out (host arrays, original order; x-bar
+// passes through unchanged).
 cudaError_t substep_vjp(Context& c, double dt, const double* vbar, const double* Cbar,
-                        const double* xbar, double* vbar0, double* Cbar0);
+                        const double* xbar, double* vbar0, double* Cbar0, double* mubar);
 // record the message returned by wcg_last_error() on this thread; returns code
 int set_last_error(int code, const std::string& msg);
 // FP64 MIC(0)-PCG on a system already placed in the context's fields

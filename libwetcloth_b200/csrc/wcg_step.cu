@@ -1927,13 +1927,43 @@ cudaError_t prepared_solve_fp64(Context& c, double* out, int* iters, double* res
 
 template <typename R>
 static cudaError_t substep_vjp_t(Context& c, double dt, const double* vbar, const double* Cbar,
-                                 const double* xbar, double* vbar0, double* Cbar0) {
+                                 const double* xbar, double* vbar0, double* Cbar0,
+                                 double* mubar) {
   const long long np = c.np;
+  const int rb = c.real_bytes();
+  const bool visc = c.prm.viscosity > 0.0;
+  const int ns = visc ? std::max(1, c.prm.viscosity_substeps) : 0;
+  if (mubar) *mubar = 0.0;
   // forward recompute at the checkpoint: grid, fields, matrix, masks (the
-  // particle state is not touched)
+  // particle state is not touched); with the viscosity, the velocity before
+  // each explicit sub-step is kept for the reverse pass
   WCG_TRY(build_grid(c));
   WCG_TRY(map_particles_to_grid(c));
-  WCG_TRY(step_velocity(c, dt));
+  const R factor = visc ? (R)(dt / ns / (c.prm.dx * c.prm.dx) * c.prm.viscosity /
+                              c.prm.liquid_density)
+                        : R(0);
+  if (!visc) {
+    WCG_TRY(step_velocity(c, dt));
+  } else if (c.n_active > 0) {
+    R* F = c.gfield.as<R>();
+    WCG_TRY(c.adjvisc.ensure((size_t)(ns + 1) * 3 * c.gcap * rb));
+    R* VK = c.adjvisc.as<R>();
+    ++c.launches, k_predict<R><<<(unsigned)c.n_active, 192, 0, c.stream>>>(
+        c.g, c.active_list.as<int>(), F, c.gcap, (R)c.prm.gravity[0], (R)c.prm.gravity[1],
+        (R)c.prm.gravity[2], (R)dt);
+    for (int it = 0; it < ns; ++it) {
+      WCG_TRY(cudaMemcpyAsync(VK + (size_t)it * 3 * c.gcap, F + G_VSTAR * c.gcap,
+                              3 * c.gcap * sizeof(R), cudaMemcpyDeviceToDevice, c.stream));
+      WCG_TRY(cudaMemcpyAsync(F + G_UTMP * c.gcap, F + G_VSTAR * c.gcap, 3 * c.gcap * sizeof(R),
+                              cudaMemcpyDeviceToDevice, c.stream));
+      ++c.launches, k_viscosity_explicit<R><<<(unsigned)c.n_active, 192, 0, c.stream>>>(
+          c.g, c.active_list.as<int>(), c.active.as<unsigned char>(), F, c.gcap, factor);
+    }
+    WCG_TRY(cudaMemcpyAsync(VK + (size_t)ns * 3 * c.gcap, F + G_VSTAR * c.gcap,
+                            3 * c.gcap * sizeof(R), cudaMemcpyDeviceToDevice, c.stream));
+    ++c.launches, k_rhs_from_vstar<R><<<(unsigned)c.n_active, 192, 0, c.stream>>>(
+        c.active_list.as<int>(), F, c.gcap);
+  }
   WCG_TRY(project_fine(c, dt));
   WCG_TRY(apply_pressure_and_extrapolate(c, dt));
   if (np == 0 || c.n_active == 0) {
@@ -1941,7 +1971,6 @@ static cudaError_t substep_vjp_t(Context& c, double dt, const double* vbar, cons
     std::fill(Cbar0, Cbar0 + 9 * np, 0.0);
     return cudaSuccess;
   }
-  const int rb = c.real_bytes();
   WCG_TRY(c.adj.ensure((size_t)kNumAdjFields * c.gcap * rb));
   WCG_TRY(c.adjmask.ensure((size_t)3 * c.gcap));
   WCG_TRY(c.adjp.ensure((size_t)12 * c.pcap * rb));
@@ -1982,7 +2011,34 @@ static cudaError_t substep_vjp_t(Context& c, double dt, const double* vbar, cons
   ++c.launches, k_adj_apply<R><<<nb, 64, 0, c.stream>>>(c.g, al, act, dof, AG, F, c.gcap, (R)dt);
   WCG_TRY(cudaGetLastError());
   WCG_TRY(solve_assembled_t<R>(c));  // A lambda = p-bar, A symmetric
-  ++c.launches, k_adj_div<R><<<nb, 192, 0, c.stream>>>(c.g, al, act, dof, F, c.gcap, AG);
+  ++c.launches, k_adj_div<R><<<nb, 192, 0, c.stream>>>(c.g, al, act, dof, F, c.gcap, AG,
+                                                        visc ? 1 : 0);
+  if (visc) {
+    // explicit viscosity steps in reverse: mu-bar += <v-bar_{k+1}, v_{k+1} - v_k> / mu,
+    // v-bar_k = v-bar_{k+1} + f K^T v-bar_{k+1}
+    const R* VK = c.adjvisc.as<R>();
+    WCG_TRY(ensure_scratch(c, (size_t)c.n_active * sizeof(double) + 64));
+    double* part = c.scratch.as<double>();
+    double* dsc = c.dscalars.as<double>();
+    double musum = 0.0;
+    R* cur = AG + A_VSBAR * c.gcap;
+    R* tmp = AG + A_UTMP * c.gcap;
+    for (int it = ns - 1; it >= 0; --it) {
+      ++c.launches, k_adj_mu_dot<R><<<nb, 192, 0, c.stream>>>(
+          al, cur, VK + (size_t)(it + 1) * 3 * c.gcap, VK + (size_t)it * 3 * c.gcap, c.gcap, part);
+      ++c.launches, k_reduce_sum<<<1, kRedThreads, 0, c.stream>>>(part, (int)c.n_active, dsc + 7);
+      double h = 0;
+      WCG_TRY(fetch(c, dsc + 7, 1, &h));
+      musum += h;
+      ++c.launches, k_adj_viscosity<R><<<nb, 192, 0, c.stream>>>(c.g, al, act, F, c.gcap, cur, tmp,
+                                                                  factor);
+      std::swap(cur, tmp);
+    }
+    if (cur != AG + A_VSBAR * c.gcap)
+      WCG_TRY(cudaMemcpyAsync(AG + A_VSBAR * c.gcap, cur, 3 * c.gcap * sizeof(R),
+                              cudaMemcpyDeviceToDevice, c.stream));
+    if (mubar) *mubar = musum / c.prm.viscosity;
+  }
   ++c.launches, k_adj_p2g<R><<<nblk(np, 128), 128, 0, c.stream>>>(
       c.g, act, c.pbuf[c.cur].as<R>(), c.pcap, np, c.pid[c.cur].as<int>(),
       c.pkey.as<long long>() + c.cur * c.pcap, c.pdelta.as<int>() + c.cur * c.pcap, F, AG,
@@ -1995,9 +2051,10 @@ static cudaError_t substep_vjp_t(Context& c, double dt, const double* vbar, cons
 }
 
 cudaError_t substep_vjp(Context& c, double dt, const double* vbar, const double* Cbar,
-                        const double* xbar, double* vbar0, double* Cbar0) {
-  return c.prm.precision == 0 ? substep_vjp_t<double>(c, dt, vbar, Cbar, xbar, vbar0, Cbar0)
-                              : substep_vjp_t<float>(c, dt, vbar, Cbar, xbar, vbar0, Cbar0);
+                        const double* xbar, double* vbar0, double* Cbar0, double* mubar) {
+  return c.prm.precision == 0
+             ? substep_vjp_t<double>(c, dt, vbar, Cbar, xbar, vbar0, Cbar0, mubar)
+             : substep_vjp_t<float>(c, dt, vbar, Cbar, xbar, vbar0, Cbar0, mubar);
 }
 
 cudaError_t substep(Context& c, double dt) {

@@ -82,18 +82,25 @@ class FluidScene:
         matrices (mass, volume and radius as last uploaded)."""
         self.upload(x, v, C, *self._attrs)
 
-    def substep_vjp(self, dt, vbar, Cbar, xbar):
+    def substep_vjp(self, dt, vbar, Cbar, xbar, with_viscosity=False):
         """Reverse mode of substep(dt) at the current (pre-step) state with the
-        positions held fixed: cotangents of (v', C', x') -> of (v, C, x)."""
+        positions held fixed: cotangents of (v', C', x') -> of (v, C, x), and of
+        the viscosity when with_viscosity."""
         n = self.num_particles
         arr = lambda a, k: np.ascontiguousarray(a, dtype=np.float64).reshape(n * k)
         vb, Cb, xb = arr(vbar, 3), arr(Cbar, 9), arr(xbar, 3)
         v0 = np.empty(n * 3)
         C0 = np.empty(n * 9)
         x0 = np.empty(n * 3)
+        mu = ctypes.c_double(0.0)
         check(self.L.wcg_substep_vjp(self.h, dt, _dp(vb), _dp(Cb), _dp(xb), _dp(v0), _dp(C0),
-                                     _dp(x0)))
-        return v0.reshape(n, 3), C0.reshape(n, 9), x0.reshape(n, 3)
+                                     _dp(x0), ctypes.byref(mu)))
+        out = (v0.reshape(n, 3), C0.reshape(n, 9), x0.reshape(n, 3))
+        return out + (mu.value,) if with_viscosity else out
+
+    def set_viscosity(self, mu, substeps=1):
+        """LiquidInfo::viscosity and its explicit sub-steps (0: off)."""
+        check(self.L.wcg_set_viscosity(self.h, float(mu), int(substeps)))
 
     def upload_device(self, n, x, v, C, mass, vol, radius):
         """Arguments are device pointers (ints) to contiguous float64 arrays."""

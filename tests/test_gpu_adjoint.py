@@ -9,7 +9,9 @@ to rounding and the solver tolerance.  Checks, at a 1e-12 pressure criterion:
 - the same with J d from central differences of the FP64 oracle, the C
   restatement pinned to the reference (an FP64 reference gradient: 1e-6);
 - torch.autograd gradients of a scalar loss against per-entry central
-  differences (1e-4 relative, the tolerance the plan states)."""
+  differences (1e-4 relative, the tolerance the plan states);
+- with the explicit viscosity on: the same identity, and the viscosity's
+  cotangent against a central difference in mu."""
 import numpy as np
 import pytest
 
@@ -153,12 +155,54 @@ def test_autograd_against_central_differences(wcg):
     g.close()
 
 
-def test_adjoint_refuses_viscosity(wcg):
-    sc = _scene("dam16")
-    sc.params.viscosity = 1.0
-    g = FluidScene(sc)
+@pytest.mark.parametrize("substeps", [1, 3])
+def test_adjoint_identity_with_viscosity(substeps, wcg):
+    """The explicit viscosity steps are linear in v*, so the identity holds
+    with them on; the viscosity cotangent matches a central difference in mu
+    (the step is a polynomial of degree `substeps` in mu)."""
+    sc = _scene("curl24")
+    mu = 0.5
+    sc.params.viscosity = mu
+    sc.params.viscosity_substeps = substeps
     n = sc.x.shape[0]
-    with pytest.raises(_capi.WcgError) as e:
-        g.substep_vjp(DT, np.zeros((n, 3)), np.zeros((n, 9)), np.zeros((n, 3)))
-    assert e.value.code == _capi.WCG_ERR_UNSUPPORTED
+    g = FluidScene(sc)
+    dv, dC, y = _directions(n, 13)
+    h = 1e-2
+    Jd = (_forward(g, sc.x, sc.v + h * dv, sc.C + h * dC) -
+          _forward(g, sc.x, sc.v - h * dv, sc.C - h * dC)) / (2 * h)
+    g.set_state(sc.x, sc.v, sc.C)
+    vb, Cb, xb, mub = g.substep_vjp(DT, y[:3 * n].reshape(n, 3), y[3 * n:12 * n].reshape(n, 9),
+                                    y[12 * n:].reshape(n, 3), with_viscosity=True)
+    lhs = float(y @ Jd)
+    rhs = float((vb * dv).sum() + (Cb * dC).sum())
+    assert abs(lhs - rhs) <= 1e-9 * abs(lhs), (lhs, rhs)
+    hm = 1e-3 * mu
+    g.set_viscosity(mu + hm, substeps)
+    fp = _forward(g, sc.x, sc.v, sc.C)
+    g.set_viscosity(mu - hm, substeps)
+    fm = _forward(g, sc.x, sc.v, sc.C)
+    fd = float(y @ ((fp - fm) / (2 * hm)))
+    assert abs(fd - mub) <= 1e-5 * abs(fd), (fd, mub)
+    g.close()
+
+
+def test_autograd_viscosity_gradient(wcg):
+    torch = pytest.importorskip("torch")
+    from libwetcloth_b200.autograd import substep
+    sc = _scene("dam16")
+    sc.params.viscosity = 0.2
+    g = FluidScene(sc)
+    mu = torch.tensor(0.2, dtype=torch.float64, requires_grad=True)
+
+    def loss_of(m):
+        x1, v1, C1 = substep(g, torch.from_numpy(sc.x), torch.from_numpy(sc.v),
+                             torch.from_numpy(sc.C), DT, viscosity=m, viscosity_substeps=2)
+        return (v1 ** 2).sum() + (C1 ** 2).sum() * 1e-4
+
+    L = loss_of(mu)
+    L.backward()
+    h = 1e-4
+    fd = (loss_of(torch.tensor(0.2 + h, dtype=torch.float64)).item() -
+          loss_of(torch.tensor(0.2 - h, dtype=torch.float64)).item()) / (2 * h)
+    assert abs(fd - mu.grad.item()) <= 1e-4 * abs(fd), (fd, mu.grad.item())
     g.close()
