@@ -409,6 +409,25 @@ def run_batch(args, steps=3):
 
 
 # ---------------------------------------------------------------------------
+class _quiet_stdout:
+    """Send file descriptor 1 to /dev/null (the reference Core prints solver
+    progress with std::cout) so the JSON line stays the only stdout output."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        self.null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.null, 1)
+        return self
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        os.close(self.null)
+        return False
+
+
 def run_reference_cpu(args, sample_n, steps=2, warmup=1):
     """The reference Core (oracle/_ref, OpenMP stand-in for TBB, all host
     threads) on a bounded sample: the same scene type at sample_n^3, ms/step
@@ -421,14 +440,15 @@ def run_reference_cpu(args, sample_n, steps=2, warmup=1):
     os.environ.setdefault("OMP_NUM_THREADS", str(cores))
     sc = scenes.half_box(sample_n, args.ppc, seed=1)
     full_np = None
-    r = oref.RefScene(sc, mic=False, omp=True)
-    for _ in range(warmup):
-        r.step(DT, snapshot=False)
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        r.step(DT, snapshot=False)
-    dt = (time.perf_counter() - t0) / steps
-    r.close()
+    with _quiet_stdout():
+        r = oref.RefScene(sc, mic=False, omp=True)
+        for _ in range(warmup):
+            r.step(DT, snapshot=False)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            r.step(DT, snapshot=False)
+        dt = (time.perf_counter() - t0) / steps
+        r.close()
     n_sample = sc.x.shape[0]
     # full-workload particle count of the same generator
     full_np = args.ppc * args.n * (args.n // 2) * args.n
