@@ -214,14 +214,14 @@ def cloth_sheet(lo, hi, y: float, spacing: float, seed: int, thickness: float = 
 
 
 def liquid_on_sheet(n_cells: int = 32, ppc: int = 8, seed: int = 3, sheet_spacing=None,
-                    surfel_every: int = 0) -> Scene:
-    """A falling liquid sphere (r 0.15 at (0.5, 0.75, 0.5), v = (0, -1, 0)
-    plus a spin of 3 rad/s about y) above a cloth sheet at y = 0.4 spanning
-    [0.1, 0.9] in x and z."""
+                    surfel_every: int = 0, center=(0.5, 0.75, 0.5)) -> Scene:
+    """A falling liquid sphere (r 0.15 at `center`, v = (0, -1, 0) plus a
+    spin of 3 rad/s about y) and a cloth sheet at y = 0.4 spanning [0.1, 0.9]
+    in x and z; with the centre at y = 0.45 the sphere straddles the sheet."""
     dx = 1.0 / n_cells
     prm = SceneParams(dx=dx)
-    x = liquid_block(dx, (0.35, 0.6, 0.35), (0.65, 0.9, 0.65), ppc, seed)
-    c = np.array([0.5, 0.75, 0.5])
+    c = np.array(center, dtype=np.float64)
+    x = liquid_block(dx, tuple(c - 0.15), tuple(c + 0.15), ppc, seed)
     x = x[np.linalg.norm(x - c, axis=1) <= 0.15]
     v = np.cross(np.array([0.0, 3.0, 0.0]), x - c)
     v[:, 1] = -1.0

@@ -29,6 +29,7 @@ typedef struct {
   double visc;       /* LiquidInfo::viscosity; 0: compute_viscosity off */
   int visc_substeps; /* LinearizedImplicitEuler::m_viscosity_substeps */
   double e_flip, e_asym, e_advect; /* elasto_flip_coeff, _asym_coeff, elasto_advect_coeff */
+  double drag_mu;  /* LiquidInfo::viscosity as the drag reads it (also when compute_viscosity is off) */
 } Params;
 
 typedef struct {
@@ -657,6 +658,46 @@ static void sat_psi_p(Scene* s) {
   }
 }
 
+/* mathutils::get_rotated_pore_coeff_{x,y,z} (MathUtilities.h:792-818): the
+ * row sum along `axis` of (2 - sf) I + (2 sf - 1) n n^T, n = o/|o|, written in
+ * closed form; 0 when the orientation is zero, as the reference's quotient by
+ * max(1e-63, |o|^2) gives. */
+static double pore_coeff(const double* o, double sf, int axis) {
+  const double n2 = (o[0] * o[0] + o[1] * o[1]) + o[2] * o[2];
+  if (!(n2 > 0.0)) return 0.0;
+  return (2.0 - sf) + (2.0 * sf - 1.0) * o[axis] * ((o[0] + o[1]) + o[2]) / n2;
+}
+
+/* TwoDScene::getDragCoeffWithOrientation (TwoDScene.cpp:4042-4097) for the
+ * liquid (material 0) with use_drag and use_nonlinear_drag on: permeabilities
+ * k_a, k_b of the yarn packing at solid fraction psi, the Ergun/Yazdchi
+ * coefficients c_a, c_b, the transversely isotropic tensor (c_xy, c_xy, c_z)
+ * about the node orientation, and its row sum along `axis`
+ * (mathutils::get_rotated_drag_*, MathUtilities.h:819-878), written as
+ * c_xy + (c_z - c_xy) n_axis (n_x + n_y + n_z).  Yarn diameter 0.01,
+ * Yazdchi power 1.6 (the LiquidInfo defaults of loadLiquidInfo). */
+static double drag_coeff(const Scene* s, double psi, double sat, double dv, const double* o,
+                         double sf, int axis) {
+  const double n2 = (o[0] * o[0] + o[1] * o[1]) + o[2] * o[2];
+  if (psi == 0.0 || sat == 0.0 || n2 < 1e-20) return 0.0;
+  const double ergun = 0.1428869017, di = 0.01, yp = 1.6;
+  const double mu = s->p.drag_mu, rho = s->p.rho;
+  const double lp = -log(psi);
+  double ka = (lp - 1.476 + 2.0 * psi - 0.5 * psi * psi) / (16.0 * psi) * di * di;
+  double kb = (lp - 1.476 + 2.0 * psi - 1.774 * psi * psi + 4.078 * pow(psi, 3.0)) /
+              (32.0 * psi) * di * di;
+  ka = fmax(1e-20, ka);
+  kb = fmax(1e-20, kb);
+  const double inertial = ergun * pow(di, yp - 1.0) * pow(mu, 1.0 - yp);
+  const double flow = pow(rho * fabs(dv), yp);
+  const double den = pow(1.0 - psi, 1.5);
+  const double ca = fmin(1e63, mu / ka + inertial / (den * sqrt(ka)) * flow);
+  const double cb = fmin(1e63, mu / kb + inertial / (den * sqrt(kb)) * flow);
+  const double cxy = ca * (1.0 - sf) + cb * sf;
+  const double cz = ca * sf + cb * (1.0 - sf);
+  return cxy + (cz - cxy) * o[axis] * ((o[0] + o[1]) + o[2]) / n2;
+}
+
 /* LinearizedImplicitEuler::stepVelocity for liquid nodes
  * (LinearizedImplicitEuler.cpp:224-337): constructNodeForce (:548-667),
  * SimpleGravityForce::addLiquidGradEToNode (SimpleGravityForce.cpp:25-52),
@@ -848,6 +889,7 @@ static void step_velocity(Scene* s, double dt) {
       const double m = s->mass[a][n];
       double r = 0.0;
       r -= m * s->p.g[a] * (-dt);
+      const double* ori = &s->eori[a][n * 3];
       if (s->vol_f[a][n] > 0.0 && s->wgt[a][n] > 0.0) {
         int I, J, K;
         node_ijk(s, n, &I, &J, &K);
@@ -855,22 +897,27 @@ static void step_velocity(Scene* s, double dt) {
         const double pp0 = node_active(s, l) ? s->pore_p[l] : 0.0;
         const double pp1 = s->pore_p[n];
         const double grad = (pp1 - pp0) / s->p.dx;
-        /* get_rotated_pore_coeff_* with a zero orientation (MathUtilities.h:792-818) */
-        const double coeff = 0.0 / fmax(1e-63, 0.0);
+        const double coeff = pore_coeff(ori, s->esf[a][n], a);
         r += grad * s->vol_f[a][n] * dt * s->sat[a][n] * s->wgt[a][n] * coeff;
       }
       r += m * s->vel[a][n];
-      const double hdV = dt * 0.0 * (0.0 + s->vol_f[a][n]);
-      const double mf = m + hdV, ms = 0.0 + hdV;
+      /* constructHDV (:846-1000, drag_by_air off: damped mass = solid mass) with
+       * the P2G liquid and solid velocities; constructInvMDV (:1109-1148) */
+      const double ms = s->emass[a][n], vs = s->evol[a][n], psi = s->psi[a][n];
+      const double dc = drag_coeff(s, psi, s->sat[a][n], s->vel[a][n] - s->evel[a][n], ori,
+                                   s->esf[a][n], a);
+      const double hdV = dt * dc * (vs + s->vol_f[a][n]);
+      const double mf = m + hdV, msh = ms + hdV;
       s->mfhdvm[a][n] = mf > 1e-20 ? hdV / mf : 1.0;
-      s->mshdvm[a][n] = ms > 1e-20 ? hdV / ms : 1.0;
-      const double C = m + s->mshdvm[a][n] * 0.0;
+      s->mshdvm[a][n] = msh > 1e-20 ? hdV / msh : 1.0;
+      const double C = m + s->mshdvm[a][n] * ms;
       s->invC[a][n] = C > 1e-20 ? 1.0 / C : 1.0;
       s->rhs[a][n] = r;
       s->vstar[a][n] = m > 1e-20 ? r / m : r;
-      const double psi = s->psi[a][n], invCs = 0.0;
+      /* constructPsiSF (:1052-1107); inv_Cs stays 0 without the solid solve */
+      const double invCs = 0.0;
       s->psifs[a][n] = ((1.0 - psi) * s->invC[a][n] + psi * invCs * s->mfhdvm[a][n]) * m;
-      s->psisf[a][n] = (psi * invCs + (1.0 - psi) * s->invC[a][n] * s->mshdvm[a][n]) * 0.0;
+      s->psisf[a][n] = (psi * invCs + (1.0 - psi) * s->invC[a][n] * s->mshdvm[a][n]) * ms;
     }
   /* explicit viscosity sub-steps, then the rhs from the new velocity
    * (LinearizedImplicitEuler::stepVelocity, LinearizedImplicitEuler.cpp:272-306) */
@@ -956,14 +1003,18 @@ static void assemble(Scene* s, double dt) {
       const long long f = up ? node_of(s, I + (a == 0), J + (a == 1), K + (a == 2)) : n;
       if (!node_active(s, f)) continue;
       const double w = s->wgt[a][f];
-      const double t = ((s->vstar[a][f] * s->psifs[a][f] + 0.0 * s->psisf[a][f]) * w +
+      /* the elasto velocity projectFine passes is m_node_v_plus, which stays
+       * zero without the solid solve (LinearizedImplicitEuler.cpp:2511-2522) */
+      const double ue = 0.0;
+      const double t = ((s->vstar[a][f] * s->psifs[a][f] + ue * s->psisf[a][f]) * w +
                         s->svel[a][f] * (1.0 - w)) / dx;
       if (up) s->b[d] -= t; else s->b[d] += t;
       if (w > 0.0) {
         double term = w * coeff;
         const double psi = s->psi[a][f];
-        term *= (1.0 - psi) * s->invC[a][f] * (s->vol_f[a][f] + 0.0 * s->mshdvm[a][f]) +
-                psi * 0.0 * (0.0 + s->vol_f[a][f] * s->mfhdvm[a][f]);
+        const double invCs = 0.0, vs = s->evol[a][f];
+        term *= (1.0 - psi) * s->invC[a][f] * (s->vol_f[a][f] + vs * s->mshdvm[a][f]) +
+                psi * invCs * (vs + s->vol_f[a][f] * s->mfhdvm[a][f]);
         const long long c = up ? f : node_of(s, I - (a == 0), J - (a == 1), K - (a == 2));
         if (!node_active(s, c)) continue;
         const double nphi = s->lphi[c];
@@ -1197,8 +1248,8 @@ static void apply_pressure(Scene* s, double dt) {
     for (long long n = 0; n < s->nnode; ++n) {
       s->valid[a][n] = 0;
       if (!s->act[n >> 6]) continue;
-      /* addSolidDragRHS (LinearizedImplicitEuler.cpp:713-739): + 1 * 0 * 0 */
-      s->rhs[a][n] += s->mshdvm[a][n] * 0.0 * 0.0;
+      /* addSolidDragRHS (LinearizedImplicitEuler.cpp:689-717) */
+      s->rhs[a][n] += s->mshdvm[a][n] * s->emass[a][n] * s->evel[a][n];
       if (s->wgt[a][n] > 0.) {
         int I, J, K;
         node_ijk(s, n, &I, &J, &K);
@@ -1215,7 +1266,7 @@ static void apply_pressure(Scene* s, double dt) {
           if (hl) pg -= s->pressure[l];
           pg += s->pressure[n];
           pg /= (dx * theta);
-          const double term = pg * dt * (s->vol_f[a][n] + 0.0 * s->mshdvm[a][n]);
+          const double term = pg * dt * (s->vol_f[a][n] + s->evol[a][n] * s->mshdvm[a][n]);
           s->rhs[a][n] -= term;
           s->valid[a][n] = 1;
         }
@@ -1470,9 +1521,6 @@ static void transfer_out(Scene* s, double dt, int snapshot) {
 
 /* one sub-step in WetClothCore::stepSystem order (WetClothCore.cpp:115-258) */
 int wco_substep(Scene* s, double dt, int snapshot) {
-  /* the elasto coupling terms of stepVelocity/projectFine (drag, solid volume
-   * fraction in the pressure system) are not restated: transfers only */
-  if (s->ne > 0) return -1;
   transfer_in(s, snapshot);
   step_velocity(s, dt);
   if (snapshot) {
@@ -1593,6 +1641,7 @@ void wco_set_elasto_coeffs(Scene* s, double flip, double asym, double advect) {
 void wco_set_viscosity(Scene* s, double mu, int substeps) {
   s->p.visc = mu;
   s->p.visc_substeps = substeps > 0 ? substeps : 1;
+  s->p.drag_mu = mu > 0.0 ? mu : 8.9e-3;
 }
 
 Scene* wco_create(double dx, const double* g, double rho, double flip, double friction,
@@ -1616,6 +1665,7 @@ Scene* wco_create(double dx, const double* g, double rho, double flip, double fr
   s->p.e_flip = 0.95;
   s->p.e_asym = 1.0;
   s->p.e_advect = 1.0;
+  s->p.drag_mu = 8.9e-3;
   s->bs = dx * 4.0;
   s->np = np;
   const size_t n = (size_t)(np > 0 ? np : 1);

@@ -159,3 +159,32 @@ def test_elasto_only_scene():
         m = ~np.isnan(a)
         assert np.array_equal(m, ~np.isnan(b)), k
         assert np.abs(a[m] - b[m]).max() <= 1e-12 * max(np.abs(a[m]).max(), 1e-300), k
+
+
+@pytest.mark.parametrize("surfel_every", [0, 5])
+def test_elasto_coupled_step(surfel_every):
+    """A full step with a liquid sphere straddling a cloth sheet: the drag of
+    constructHDV, the pore-pressure gradient with the node orientation, the
+    solid volume in the pressure system and applyPressureDragFluid's solid
+    drag, the solid solve off (LiquidInfo::solve_solid false)."""
+    sc = scenes.liquid_on_sheet(16, 8, 3, center=(0.5, 0.45, 0.5), surfel_every=surfel_every)
+    r = oref.RefScene(sc, mic=True)
+    o = oo.OracleScene(sc)
+    assert r.step(DT, snapshot=True) == o.step(DT, snapshot=True)
+    assert r.solver_stats()[0] == o.solver_stats()[0]
+    for k in ("array_idx", "active", "dof_index", "A_rowstart", "A_col", "valid_x"):
+        assert np.array_equal(r.get(k), o.get(k)), k
+    for k in ("v_star_y", "rhs_fluid_x", "inv_C_z", "psi_fs_y", "A_val", "b", "pressure",
+              "u_proj_x", "u_final_y", "g2p_v", "g2p_C", "adv_x", "g2p_ev4", "g2p_eB", "adv_x4"):
+        a, b = r.get(k), o.get(k)
+        m = ~np.isnan(a)
+        assert np.array_equal(m, ~np.isnan(b)), k
+        if m.any():
+            assert np.abs(a[m] - b[m]).max() <= 1e-12 * max(np.abs(a[m]).max(), 1e-300), k
+    # the coupling is active: the same liquid without the sheet steps differently
+    sc2 = scenes.liquid_on_sheet(16, 8, 3, center=(0.5, 0.45, 0.5))
+    sc2.elasto = None
+    o2 = oo.OracleScene(sc2)
+    o2.step(DT, snapshot=True)
+    a, b = o.get("g2p_v")[-3 * sc.x.shape[0]:], o2.get("g2p_v")
+    assert np.abs(a - b).max() > 1e-3 * np.abs(b).max()
