@@ -67,6 +67,8 @@ typedef struct wcg_params {
   double elasto_flip_coeff;        /* LiquidInfo::elasto_flip_coeff (0.95) */
   double elasto_flip_asym_coeff;   /* LiquidInfo::elasto_flip_asym_coeff (1.0) */
   double elasto_advect_coeff;      /* LiquidInfo::elasto_advect_coeff (1.0) */
+  double drag_viscosity;           /* LiquidInfo::viscosity as the liquid-solid drag reads it
+                                      while the viscosity term is off (8.9e-3) */
 } wcg_params;
 
 typedef struct wcg_ctx wcg_ctx;
@@ -116,8 +118,12 @@ long long wcg_num_particles(const wcg_ctx* ctx);
  * (3n), surfel (n; nonzero where m_particle_to_surfel >= 0).  Host pointers.
  * They take part in the grid build, the transfers (mapParticleNodesAPIC
  * :6609-6919, mapParticleSaturationPsiNodes :5952, updatePorePressureNodes
- * :5933, mapNodeParticlesAPIC :6936-7090) and advection (SceneStepper.cpp:17);
- * the solve calls return WCG_ERR_UNSUPPORTED while any are present. */
+ * :5933, mapNodeParticlesAPIC :6936-7090), the liquid step's coupling to them
+ * (constructHDV drag, pore-pressure gradients, the solid volume in the
+ * pressure system, applyPressureDragFluid's solid drag) and advection
+ * (SceneStepper.cpp:17).  The solid phase itself is not solved
+ * (LiquidInfo::solve_solid off): its node velocity is the P2G one, or what
+ * wcg_upload_field("vel_*") sets. */
 int wcg_upload_elasto(wcg_ctx* ctx, long long n, const double* x4, const double* v4,
                       const double* B9, const double* m4, const double* fm4,
                       const double* rest_vol, const double* rest_vf,

@@ -52,6 +52,7 @@ class WcgParams(ctypes.Structure):
         ("elasto_flip_coeff", ctypes.c_double),
         ("elasto_flip_asym_coeff", ctypes.c_double),
         ("elasto_advect_coeff", ctypes.c_double),
+        ("drag_viscosity", ctypes.c_double),
     ]
 
 

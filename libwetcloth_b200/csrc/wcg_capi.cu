@@ -186,6 +186,7 @@ void wcg_default_params(wcg_params* p) {
   p->elasto_flip_coeff = 0.95;
   p->elasto_flip_asym_coeff = 1.0;
   p->elasto_advect_coeff = 1.0;
+  p->drag_viscosity = 8.9e-3;
 }
 
 int wcg_create(const wcg_params* params, wcg_ctx** out) {
@@ -201,6 +202,8 @@ int wcg_create(const wcg_params* params, wcg_ctx** out) {
   if (!std::isfinite(params->elasto_flip_coeff) || !std::isfinite(params->elasto_flip_asym_coeff) ||
       !std::isfinite(params->elasto_advect_coeff))
     return fail(WCG_ERR_ARG, "elasto coefficients must be finite");
+  if (!(params->drag_viscosity > 0.0) || !std::isfinite(params->drag_viscosity))
+    return fail(WCG_ERR_ARG, "drag_viscosity must be finite and > 0");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return fail(WCG_ERR_CUDA, "no CUDA device available");
@@ -228,6 +231,7 @@ int wcg_create(const wcg_params* params, wcg_ctx** out) {
   p.elasto_flip = params->elasto_flip_coeff;
   p.elasto_flip_asym = params->elasto_flip_asym_coeff;
   p.elasto_advect = params->elasto_advect_coeff;
+  p.drag_viscosity = params->drag_viscosity;
   // wavefront tile shape (performance knob; both compute identical results)
   if (const char* v = getenv("WCG_SWEEP_TILE")) ctx->c.sweep_variant = !strcmp(v, "warp") ? 1 : 0;
   // layout of the pressure solve (performance knob; same arithmetic)
@@ -427,15 +431,12 @@ int wcg_rebucketize_and_resample(wcg_ctx* ctx) {
       return fail(WCG_ERR_STATE, "no grid: call wcg_rebucketize_and_resample"); \
   } while (0)
 
-// The elasto coupling terms of the solve (drag arrays of constructHDV, the
-// solid volume fraction in the pressure system, applyPressureDragElasto) are
-// not built: calls that need them refuse scenes with elasto particles.
+// Calls without an elasto form refuse scenes with elasto particles.
 #define WCG_NO_ELASTO(ctx, what)                                              \
   do {                                                                       \
     if ((ctx)->c.ne > 0)                                                     \
       return fail(WCG_ERR_UNSUPPORTED, std::string(what) +                   \
-                                           ": the elasto coupling of the solve is not built " \
-                                           "(transfers only for elasto particles)"); \
+                                           ": not available with elasto particles"); \
   } while (0)
 
 int wcg_map_particle_nodes(wcg_ctx* ctx) {
@@ -447,7 +448,6 @@ int wcg_map_particle_nodes(wcg_ctx* ctx) {
 
 int wcg_step_velocity(wcg_ctx* ctx, double dt) {
   WCG_CHECK_CTX(ctx);
-  WCG_NO_ELASTO(ctx, "stepVelocity");
   WCG_NEED_GRID(ctx);
   if (!(dt > 0)) return fail(WCG_ERR_ARG, "dt must be positive");
   WCG_CALL(ctx, wcg::step_velocity(ctx->c, dt), "stepVelocity");
@@ -456,7 +456,6 @@ int wcg_step_velocity(wcg_ctx* ctx, double dt) {
 
 int wcg_project_fine(wcg_ctx* ctx, double dt) {
   WCG_CHECK_CTX(ctx);
-  WCG_NO_ELASTO(ctx, "projectFine");
   WCG_NEED_GRID(ctx);
   if (!(dt > 0)) return fail(WCG_ERR_ARG, "dt must be positive");
   WCG_CALL(ctx, wcg::project_fine(ctx->c, dt), "projectFine");
@@ -472,7 +471,6 @@ int wcg_project_fine(wcg_ctx* ctx, double dt) {
 
 int wcg_apply_pressure_drag_fluid(wcg_ctx* ctx, double dt) {
   WCG_CHECK_CTX(ctx);
-  WCG_NO_ELASTO(ctx, "applyPressureDragFluid");
   WCG_NEED_GRID(ctx);
   WCG_CALL(ctx, wcg::apply_pressure_and_extrapolate(ctx->c, dt), "applyPressureDragFluid");
   return device_status(ctx->c, "applyPressureDragFluid");
@@ -502,7 +500,6 @@ int wcg_advect(wcg_ctx* ctx, double dt) {
 
 int wcg_substep(wcg_ctx* ctx, double dt) {
   WCG_CHECK_CTX(ctx);
-  WCG_NO_ELASTO(ctx, "substep");
   if (!(dt > 0)) return fail(WCG_ERR_ARG, "dt must be positive");
   WCG_CALL(ctx, wcg::substep(ctx->c, dt), "substep");
   int s = device_status(ctx->c, "substep");
@@ -551,7 +548,6 @@ int wcg_num_substeps(wcg_ctx* ctx, double dt, int* n_out) {
 
 int wcg_step(wcg_ctx* ctx, double dt, int* substeps_out) {
   WCG_CHECK_CTX(ctx);
-  WCG_NO_ELASTO(ctx, "step");
   if (!(dt > 0)) return fail(WCG_ERR_ARG, "dt must be positive");
   int n = 1;
   WCG_CALL(ctx, wcg::num_substeps(ctx->c, dt, &n), "num_substeps");

@@ -34,6 +34,7 @@ struct Params {
   double elasto_flip;      // LiquidInfo::elasto_flip_coeff
   double elasto_flip_asym; // LiquidInfo::elasto_flip_asym_coeff
   double elasto_advect;    // LiquidInfo::elasto_advect_coeff
+  double drag_viscosity;   // LiquidInfo::viscosity as the drag reads it when viscosity == 0
 };
 
 // A device allocation that grows and never shrinks.
@@ -123,7 +124,8 @@ enum EField : int {
   E_MASS = 0, E_VEL = 3, E_VOL = 6, E_PSI = 9, E_SF = 12,
   E_ORI = 15,  // E_ORI + 3 * axis + component
   E_PSIP = 24, E_PORE = 25,
-  kNumEFields = 26
+  E_Q = 26,    // mshdvm_hdvm: hdV / (m_solid + hdV) of constructHDV, per face axis
+  kNumEFields = 29
 };
 
 // Geometry of the pencil layout of one pressure solve (wcg_pencil.cuh).

@@ -439,24 +439,108 @@ __global__ void __launch_bounds__(192)
 // (SimpleGravityForce.cpp:25-52, coeff -dt) and the node momentum;
 // constructHDV/constructInvMDV/constructPsiSF (:846-1149) with no solid
 // (drag 0, Q_s = 1, inv_C = 1/m_f or 1); performLocalSolve (:128-170).
+// mathutils::get_rotated_pore_coeff_* (MathUtilities.h:792-818) in closed
+// form: the row sum along `axis` of (2 - sf) I + (2 sf - 1) n n^T, n = o/|o|;
+// 0 for a zero orientation.
+__device__ inline double pore_coeff(double o0, double o1, double o2, double sf, int axis) {
+  const double n2 = (o0 * o0 + o1 * o1) + o2 * o2;
+  if (!(n2 > 0.0)) return 0.0;
+  const double oa = axis == 0 ? o0 : (axis == 1 ? o1 : o2);
+  return (2.0 - sf) + (2.0 * sf - 1.0) * oa * ((o0 + o1) + o2) / n2;
+}
+
+// TwoDScene::getDragCoeffWithOrientation (TwoDScene.cpp:4042-4097), liquid,
+// use_drag and use_nonlinear_drag on, yarn diameter 0.01, Yazdchi power 1.6;
+// the rotated coefficient (mathutils::get_rotated_drag_*) is the row sum
+// c_xy + (c_z - c_xy) n_axis (n_x + n_y + n_z).
+__device__ inline double drag_coeff(double psi, double sat, double dv, double o0, double o1,
+                                    double o2, double sf, int axis, double mu, double rho) {
+  const double n2 = (o0 * o0 + o1 * o1) + o2 * o2;
+  if (psi == 0.0 || sat == 0.0 || n2 < 1e-20) return 0.0;
+  const double ergun = 0.1428869017, di = 0.01, yp = 1.6;
+  const double lp = -log(psi);
+  double ka = (lp - 1.476 + 2.0 * psi - 0.5 * psi * psi) / (16.0 * psi) * di * di;
+  double kb = (lp - 1.476 + 2.0 * psi - 1.774 * psi * psi + 4.078 * pow(psi, 3.0)) /
+              (32.0 * psi) * di * di;
+  ka = fmax(1e-20, ka);
+  kb = fmax(1e-20, kb);
+  const double inertial = ergun * pow(di, yp - 1.0) * pow(mu, 1.0 - yp);
+  const double flow = pow(rho * fabs(dv), yp);
+  const double den = pow(1.0 - psi, 1.5);
+  const double ca = fmin(1e63, mu / ka + inertial / (den * sqrt(ka)) * flow);
+  const double cb = fmin(1e63, mu / kb + inertial / (den * sqrt(kb)) * flow);
+  const double cxy = ca * (1.0 - sf) + cb * sf;
+  const double cz = ca * sf + cb * (1.0 - sf);
+  const double oa = axis == 0 ? o0 : (axis == 1 ? o1 : o2);
+  return cxy + (cz - cxy) * oa * ((o0 + o1) + o2) / n2;
+}
+
+// With elasto particles (EF != null): the pore-pressure gradient term of
+// pressure::computePorePressureGrads (Pressure.cpp:26-110) on the liquid rhs,
+// constructHDV's drag between the P2G liquid and solid velocities
+// (drag_by_air off: damped mass = solid mass), Q = hdV/(m_s + hdV), inv_C =
+// 1/(m_f + Q m_s), psi_fs = (1 - psi) inv_C m_f (inv_Cs = 0 without the solid
+// solve); Q goes to EF[E_Q].
 template <typename R>
 __global__ void __launch_bounds__(192)
     k_predict(GridDesc g, const int* __restrict__ active_list, R* __restrict__ F,
-              long long fstride, R gx, R gy, R gz, R dt) {
+              long long fstride, R gx, R gy, R gz, R dt, R* __restrict__ EF,
+              const unsigned char* __restrict__ active, double drag_mu, double rho) {
   const int b = active_list[blockIdx.x];
   const int a = threadIdx.x >> 6;
-  const long long n = (long long)b * 64 + (threadIdx.x & 63);
+  const int l = threadIdx.x & 63;
+  const long long n = (long long)b * 64 + l;
   const R grav = a == 0 ? gx : (a == 1 ? gy : gz);
   const R m = F[(G_MASS + a) * fstride + n];
   const R u = F[(G_VEL + a) * fstride + n];
   R rhs = R(0) - (m * grav) * (-dt);
+  if (EF) {
+    const R vf = F[(G_VOL + a) * fstride + n];
+    const R w = F[(G_WEIGHT + a) * fstride + n];
+    if (vf > R(0) && w > R(0)) {
+      const int bk = b / (g.ni * g.nj);
+      const int rem = b - bk * g.ni * g.nj;
+      const int bj = rem / g.ni;
+      const int bi = rem - bj * g.ni;
+      const int I = bi * 4 + (l & 3), J = bj * 4 + ((l >> 2) & 3), K = bk * 4 + (l >> 4);
+      const int lI = I - (a == 0), lJ = J - (a == 1), lK = K - (a == 2);
+      const R pp0 = in_grid(g, lI, lJ, lK) && active[bucket_of(g, lI, lJ, lK)]
+                        ? EF[E_PORE * fstride + node_linear(g, lI, lJ, lK)]
+                        : R(0);
+      const R pp1 = EF[E_PORE * fstride + n];
+      const R grad = (pp1 - pp0) / (R)g.dx;
+      const R coeff = (R)pore_coeff((double)EF[(E_ORI + 3 * a) * fstride + n],
+                                    (double)EF[(E_ORI + 3 * a + 1) * fstride + n],
+                                    (double)EF[(E_ORI + 3 * a + 2) * fstride + n],
+                                    (double)EF[(E_SF + a) * fstride + n], a);
+      rhs += grad * vf * dt * F[(G_SAT + a) * fstride + n] * w * coeff;
+    }
+  }
   rhs += m * u;
   const bool heavy = m > R(1e-20);
-  const R invC = heavy ? R(1) / m : R(1);
+  R invC = heavy ? R(1) / m : R(1);
+  R psifs = invC * m;
+  if (EF) {
+    const R ms = EF[(E_MASS + a) * fstride + n], vs = EF[(E_VOL + a) * fstride + n];
+    const R psi = EF[(E_PSI + a) * fstride + n];
+    const double dc = drag_coeff(
+        (double)psi, (double)F[(G_SAT + a) * fstride + n],
+        (double)(u - EF[(E_VEL + a) * fstride + n]), (double)EF[(E_ORI + 3 * a) * fstride + n],
+        (double)EF[(E_ORI + 3 * a + 1) * fstride + n],
+        (double)EF[(E_ORI + 3 * a + 2) * fstride + n], (double)EF[(E_SF + a) * fstride + n], a,
+        drag_mu, rho);
+    const R hdV = dt * (R)dc * (vs + F[(G_VOL + a) * fstride + n]);
+    const R msh = ms + hdV;
+    const R Q = msh > R(1e-20) ? hdV / msh : R(1);
+    const R C = m + Q * ms;
+    invC = C > R(1e-20) ? R(1) / C : R(1);
+    psifs = ((R(1) - psi) * invC + psi * R(0) * Q) * m;
+    EF[(E_Q + a) * fstride + n] = Q;
+  }
   F[(G_RHS + a) * fstride + n] = rhs;
   F[(G_INVC + a) * fstride + n] = invC;
   F[(G_VSTAR + a) * fstride + n] = heavy ? rhs / m : rhs;
-  F[(G_PSIFS + a) * fstride + n] = invC * m;
+  F[(G_PSIFS + a) * fstride + n] = psifs;
 }
 
 // Pressure system (pressure::solveNodePressure, Core/Pressure.cpp:350-791):
@@ -470,7 +554,8 @@ template <typename R>
 __global__ void __launch_bounds__(64)
     k_assemble(GridDesc g, const int* __restrict__ active_list,
                const unsigned char* __restrict__ active, R* __restrict__ F,
-               long long fstride, unsigned char* __restrict__ dof, R dt) {
+               long long fstride, unsigned char* __restrict__ dof, R dt,
+               const R* __restrict__ EF) {
   const int b = active_list[blockIdx.x];
   const int l = threadIdx.x;
   const int bk = b / (g.ni * g.nj);
@@ -513,7 +598,12 @@ __global__ void __launch_bounds__(64)
       const R t = ((F[(G_VSTAR + a) * fstride + q] * F[(G_PSIFS + a) * fstride + q]) * w) / dx;
       if (f & 1) rhs -= t; else rhs += t;
       if (w > R(0)) {
-        const R term = (w * coeff) * (F[(G_INVC + a) * fstride + q] * F[(G_VOL + a) * fstride + q]);
+        // with elasto: (1 - psi) inv_C (V_f + V_s Q) (+ psi inv_Cs (...), inv_Cs = 0)
+        const R term =
+            EF ? (w * coeff) * ((R(1) - EF[(E_PSI + a) * fstride + q]) * F[(G_INVC + a) * fstride + q] *
+                                (F[(G_VOL + a) * fstride + q] +
+                                 EF[(E_VOL + a) * fstride + q] * EF[(E_Q + a) * fstride + q]))
+               : (w * coeff) * (F[(G_INVC + a) * fstride + q] * F[(G_VOL + a) * fstride + q]);
         if (in_grid(g, cI[f], cJ[f], cK[f]) &&
             active[bucket_of(g, cI[f], cJ[f], cK[f])]) {
           const R phin = F[G_LPHI * fstride + node_linear(g, cI[f], cJ[f], cK[f])];
@@ -548,7 +638,8 @@ template <typename R>
 __global__ void __launch_bounds__(192)
     k_apply_pressure(GridDesc g, const int* __restrict__ active_list,
                      const unsigned char* __restrict__ active, R* __restrict__ F,
-                     long long fstride, unsigned char* __restrict__ valid, R dt) {
+                     long long fstride, unsigned char* __restrict__ valid, R dt,
+                     const R* __restrict__ EF) {
   const int b = active_list[blockIdx.x];
   const int a = threadIdx.x >> 6;
   const int l = threadIdx.x & 63;
@@ -560,6 +651,9 @@ __global__ void __launch_bounds__(192)
   const long long n = (long long)b * 64 + l;
   const R dx = (R)g.dx;
   R rhs = F[(G_RHS + a) * fstride + n];
+  // addSolidDragRHS (LinearizedImplicitEuler.cpp:689-717) with the P2G solid velocity
+  const R Q = EF ? EF[(E_Q + a) * fstride + n] : R(0);
+  if (EF) rhs += Q * EF[(E_MASS + a) * fstride + n] * EF[(E_VEL + a) * fstride + n];
   unsigned char v = 0;
   const R w = F[(G_WEIGHT + a) * fstride + n];
   if (w > R(0)) {
@@ -579,7 +673,8 @@ __global__ void __launch_bounds__(192)
       if (hl) pg -= F[G_PRESSURE * fstride + nl];
       if (hr) pg += F[G_PRESSURE * fstride + n];
       pg /= (dx * theta);
-      const R term = pg * dt * F[(G_VOL + a) * fstride + n];
+      const R term = EF ? pg * dt * (F[(G_VOL + a) * fstride + n] + EF[(E_VOL + a) * fstride + n] * Q)
+                        : pg * dt * F[(G_VOL + a) * fstride + n];
       rhs -= term;
       v = 1;
     }

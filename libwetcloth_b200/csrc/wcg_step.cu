@@ -646,6 +646,18 @@ cudaError_t build_grid(Context& c) {
   return c.prm.precision == 0 ? build_grid_t<double>(c) : build_grid_t<float>(c);
 }
 
+// node fields of the elasto particles, or null for a liquid-only scene
+template <typename R>
+static R* elasto_fields(Context& c) {
+  return c.ne > 0 && c.efcap >= c.gcap ? c.efield.as<R>() : nullptr;
+}
+
+// LiquidInfo::viscosity as the drag reads it: the liquid viscosity when the
+// viscosity term is on, else the scene's drag viscosity (8.9e-3 by default)
+static double drag_viscosity(const Context& c) {
+  return c.prm.viscosity > 0.0 ? c.prm.viscosity : c.prm.drag_viscosity;
+}
+
 static Walls make_walls(const Context& c) {
   Walls w;
   w.cx = c.prm.box_center[0]; w.cy = c.prm.box_center[1]; w.cz = c.prm.box_center[2];
@@ -700,7 +712,8 @@ static cudaError_t step_velocity_t(Context& c, double dt) {
   ProfScope prof(c, P_GRIDOPS);
   ++c.launches, k_predict<R><<<(unsigned)c.n_active, 192, 0, c.stream>>>(
       c.g, c.active_list.as<int>(), c.gfield.as<R>(), c.gcap, (R)c.prm.gravity[0],
-      (R)c.prm.gravity[1], (R)c.prm.gravity[2], (R)dt);
+      (R)c.prm.gravity[1], (R)c.prm.gravity[2], (R)dt, elasto_fields<R>(c),
+      c.active.as<unsigned char>(), drag_viscosity(c), c.prm.liquid_density);
   // explicit viscosity sub-steps, then rhs = v * m (stepVelocity :272-306)
   if (c.prm.viscosity > 0.0) {
     R* F = c.gfield.as<R>();
@@ -1586,7 +1599,8 @@ static cudaError_t project_fine_t(Context& c, double dt) {
   unsigned char* dof = c.gdof.as<unsigned char>();
   {
     ProfScope prof(c, P_GRIDOPS);
-    ++c.launches, k_assemble<R><<<(unsigned)c.n_active, 64, 0, c.stream>>>(c.g, al, act, F, c.gcap, dof, (R)dt);
+    ++c.launches, k_assemble<R><<<(unsigned)c.n_active, 64, 0, c.stream>>>(c.g, al, act, F, c.gcap, dof, (R)dt,
+                                                                            elasto_fields<R>(c));
   }
   WCG_TRY(cudaGetLastError());
   return solve_assembled_t<R>(c);
@@ -1727,7 +1741,7 @@ static cudaError_t apply_pressure_t(Context& c, double dt) {
   unsigned char* valid = c.gvalid.as<unsigned char>();
   unsigned char* vtmp = valid + 3 * c.gcap;
   ++c.launches, k_apply_pressure<R><<<(unsigned)c.n_active, 192, 0, c.stream>>>(c.g, al, act, F, c.gcap,
-                                                                  valid, (R)dt);
+                                                                  valid, (R)dt, elasto_fields<R>(c));
   R* U = F + G_U * c.gcap;
   R* UT = F + G_UTMP * c.gcap;
   ++c.launches, k_extrapolate<R><<<(unsigned)c.n_active, 192, 0, c.stream>>>(c.g, al, act, U, UT, valid,
@@ -1950,7 +1964,8 @@ static cudaError_t substep_vjp_t(Context& c, double dt, const double* vbar, cons
     R* VK = c.adjvisc.as<R>();
     ++c.launches, k_predict<R><<<(unsigned)c.n_active, 192, 0, c.stream>>>(
         c.g, c.active_list.as<int>(), F, c.gcap, (R)c.prm.gravity[0], (R)c.prm.gravity[1],
-        (R)c.prm.gravity[2], (R)dt);
+        (R)c.prm.gravity[2], (R)dt, elasto_fields<R>(c), c.active.as<unsigned char>(),
+        drag_viscosity(c), c.prm.liquid_density);
     for (int it = 0; it < ns; ++it) {
       WCG_TRY(cudaMemcpyAsync(VK + (size_t)it * 3 * c.gcap, F + G_VSTAR * c.gcap,
                               3 * c.gcap * sizeof(R), cudaMemcpyDeviceToDevice, c.stream));

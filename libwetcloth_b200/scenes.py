@@ -37,6 +37,7 @@ class SceneParams:
     elasto_flip_coeff: float = 0.95       # LiquidInfo elasto_flip_coeff
     elasto_flip_asym_coeff: float = 1.0   # LiquidInfo elasto_flip_asym_coeff
     elasto_advect_coeff: float = 1.0      # LiquidInfo elasto_advect_coeff
+    drag_viscosity: float = 8.9e-3        # LiquidInfo viscosity as the drag reads it
 
 
 def particle_radius(dx: float, ppc: int) -> float:

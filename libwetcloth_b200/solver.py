@@ -41,6 +41,7 @@ def make_params(p, precision=_capi.WCG_FP64, refine_inner_tol=0.0,
     prm.elasto_flip_coeff = getattr(p, "elasto_flip_coeff", 0.95)
     prm.elasto_flip_asym_coeff = getattr(p, "elasto_flip_asym_coeff", 1.0)
     prm.elasto_advect_coeff = getattr(p, "elasto_advect_coeff", 1.0)
+    prm.drag_viscosity = getattr(p, "drag_viscosity", 8.9e-3)
     return prm
 
 

@@ -109,23 +109,60 @@ def test_elasto_transfer_fp32(wcg):
     g.close()
 
 
-def test_elasto_solve_refused_and_cfl(wcg):
-    """The solve's elasto coupling is not built: step/stepVelocity/projectFine
-    refuse with WCG_ERR_UNSUPPORTED; the CFL sub-step count includes the
-    elasto velocities (getMaxVelocity)."""
-    sc = _scene()
+@pytest.mark.parametrize("surfel_every", [0, 5])
+def test_elasto_coupled_step_fp64(surfel_every, wcg):
+    """A full step with a liquid sphere straddling the sheet: the drag, the
+    pore-pressure gradient, the solid volume in the pressure system and the
+    solid drag on the liquid (pinned to the reference in
+    test_oracle_vs_reference.py::test_elasto_coupled_step), stage by stage."""
+    sc = scenes.liquid_on_sheet(16, 8, 3, center=(0.5, 0.45, 0.5), surfel_every=surfel_every)
+    o = oo.OracleScene(sc)
+    o.step(DT, snapshot=True)
     g = FluidScene(sc)
-    with pytest.raises(_capi.WcgError) as e:
-        g.step(DT)
-    assert e.value.code == _capi.WCG_ERR_UNSUPPORTED
     g.rebucketize_and_resample()
     g.map_particle_nodes()
-    with pytest.raises(_capi.WcgError) as e:
-        g.step_velocity(DT)
-    assert e.value.code == _capi.WCG_ERR_UNSUPPORTED
+    g.step_velocity(DT)
+    for f in ("v_star_x", "v_star_y", "v_star_z", "rhs_fluid_y", "psi_fs_y"):
+        _close(g.field(f), o.get(f), 1e-10, f)
+    g.project_fine(DT)
+    _close(g.field("pressure"), o.get("pressure"), 1e-10, "pressure")
+    g.apply_pressure_drag_fluid(DT)
+    g.constrain_liquid_velocity()
+    g.map_node_particles()
+    g.advect(DT)
+    ne = sc.elasto.n
+    x, v, C = g.download()
+    _close(v, o.get("g2p_v").reshape(-1, 3)[ne:], 1e-10, "g2p_v")
+    _close(x, o.get("adv_x").reshape(-1, 3)[ne:], 1e-12, "adv_x")
+    x4, v4, B = g.download_elasto()
+    _close(x4, o.get("adv_x4").reshape(-1, 4)[:ne], 1e-12, "adv_x4")
+    _close(B, o.get("adv_eB").reshape(-1, 9)[:ne], 1e-10, "adv_eB", np.abs(v4).max() * 64)
+    g.close()
+
+
+def test_elasto_coupled_steps_fp32_and_cfl(wcg):
+    sc = scenes.liquid_on_sheet(24, 8, 3, center=(0.5, 0.45, 0.5))
     o = oo.OracleScene(sc)
+    g = FluidScene(sc, precision=_capi.WCG_FP32_REFINE)
     for dt in (1e-3, 2e-2, 0.2):
         assert g.num_substeps(dt) == o.num_substeps(dt), dt
+    o.step(DT, snapshot=True)
+    g.step(DT)
+    assert g.stats()["converged"] == 1
+    ne = sc.elasto.n
+    x, v, C = g.download()
+    _close(v, o.get("g2p_v").reshape(-1, 3)[ne:], 1e-5, "g2p_v")
+    _close(x, o.get("adv_x").reshape(-1, 3)[ne:], 1e-6, "adv_x")
+    g.close()
+
+
+def test_elasto_vjp_refused(wcg):
+    sc = _scene()
+    g = FluidScene(sc)
+    n = sc.x.shape[0]
+    with pytest.raises(_capi.WcgError) as e:
+        g.substep_vjp(DT, np.zeros((n, 3)), np.zeros((n, 9)), np.zeros((n, 3)))
+    assert e.value.code == _capi.WCG_ERR_UNSUPPORTED
     g.close()
 
 
