@@ -38,6 +38,13 @@ class SceneParams:
     elasto_flip_asym_coeff: float = 1.0   # LiquidInfo elasto_flip_asym_coeff
     elasto_advect_coeff: float = 1.0      # LiquidInfo elasto_advect_coeff
     drag_viscosity: float = 8.9e-3        # LiquidInfo viscosity as the drag reads it
+    # correctLiquidParticles (TwoDScene.cpp:1967): LiquidInfo correction_strength
+    # (0 turns it off), correction_step, correction_multiplier, and the seed of
+    # the stream that picks each sub-step's particle subset
+    correction_strength: float = 0.0
+    correction_step: int = 8
+    correction_multiplier: float = 2.0
+    correction_seed: int = 0
 
 
 def particle_radius(dx: float, ppc: int) -> float:

@@ -36,6 +36,12 @@ def lib():
         L.wco_set_elasto.argtypes = [ctypes.c_void_p, ctypes.c_int] + [_D] * 10 + [_I, _D]
         L.wco_set_elasto_coeffs.argtypes = [ctypes.c_void_p] + [ctypes.c_double] * 3
         L.wco_transfer.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        L.wco_set_correction.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int,
+                                         ctypes.c_double, ctypes.c_uint64]
+        L.wco_set_correction_selector.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.wco_correct_liquid.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
+        L.wco_correction_selector.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int]
+        L.wco_correction_selector.restype = ctypes.c_int
         L.wco_step.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
         L.wco_step.restype = ctypes.c_int
         L.wco_substep.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
@@ -103,6 +109,9 @@ class OracleScene:
         if mu > 0.0:
             L.wco_set_viscosity(self.h, mu, getattr(p, "viscosity_substeps", 1))
         set_elasto(L.wco_set_elasto, L.wco_set_elasto_coeffs, self.h, scene, self._keep)
+        if getattr(p, "correction_strength", 0.0) > 0.0:
+            L.wco_set_correction(self.h, p.correction_strength, p.correction_step,
+                                 p.correction_multiplier, p.correction_seed)
 
     def close(self):
         if self.h:
@@ -126,6 +135,10 @@ class OracleScene:
         """Grid, P2G, then G2P from the P2G velocities and advection (no
         solve); snapshots as in a step."""
         self.L.wco_transfer(self.h, dt)
+
+    def set_correction_selector(self, selector):
+        """Particle subset (fluid index % step) of the next correction."""
+        self.L.wco_set_correction_selector(self.h, int(selector))
 
     def get(self, name):
         n = self.L.wco_size(self.h, name.encode())

@@ -53,6 +53,8 @@ def _lib(omp: bool):
         L.wcref_set_elasto.argtypes = [ctypes.c_void_p, ctypes.c_int] + [_D] * 10 + [_I, _D]
         L.wcref_set_elasto_coeffs.argtypes = [ctypes.c_void_p] + [ctypes.c_double] * 3
         L.wcref_transfer.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        L.wcref_set_correction.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int,
+                                           ctypes.c_double, ctypes.c_uint]
         _libs[omp] = L
     return _libs[omp]
 
@@ -108,6 +110,9 @@ class RefScene:
             self.L.wcref_set_viscosity(self.h, mu, getattr(p, "viscosity_substeps", 1))
         set_elasto(self.L.wcref_set_elasto, self.L.wcref_set_elasto_coeffs, self.h, scene,
                    self._keep)
+        if getattr(p, "correction_strength", 0.0) > 0.0:
+            self.L.wcref_set_correction(self.h, p.correction_strength, p.correction_step,
+                                        p.correction_multiplier, p.correction_seed)
 
     def close(self):
         if self.h:

@@ -29,6 +29,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <cstdlib>
 #include <fstream>
 #include <functional>
 #include <iostream>
@@ -92,6 +93,8 @@ struct Harness {
   double timers[12];
   int last_iters_amg = 0, last_iters_mic = 0;
   double last_res_amg = 0, last_res_mic = 0;
+  bool corr_on = false;       // correctLiquidParticles before G2P (WetClothCore.cpp:242)
+  unsigned corr_seed = 0, corr_count = 0;
 };
 
 double now() {
@@ -578,11 +581,24 @@ int wcref_substep(void* hp, double sub_dt, int snapshot) {
     dense(*h, "u_final_z", s.m_node_vel_fluid_z);
   }
 
+  if (h->corr_on) {
+    // the correction draws its particle subset with one rand(): seed it and
+    // record the value it will draw
+    const unsigned seed = h->corr_seed + h->corr_count++;
+    srand(seed);
+    const int sel = rand() % s.getLiquidInfo().correction_step;
+    srand(seed);
+    s.correctLiquidParticles(sub_dt);
+    h->ii["correction_selector"] = {sel};
+    if (snapshot) snap_particles(*h, "corr_");
+  }
+
   s.mapNodeParticlesAPIC();
   t1 = now(); h->timers[9] += t1 - t0; t0 = t1;
   if (snapshot) snap_particles(*h, "g2p_");
 
   e.advectScene(s, sub_dt);
+  s.solidProjection(sub_dt);
   t1 = now(); h->timers[10] += t1 - t0; t0 = t1;
   if (snapshot) snap_particles(*h, "adv_");
   return 0;
@@ -742,8 +758,25 @@ int wcref_transfer(void* hp, double dt) {
   s.mapNodeParticlesAPIC();
   snap_particles(*h, "g2p_");
   e.advectScene(s, dt);
+  s.solidProjection(dt);
   snap_particles(*h, "adv_");
   return 0;
+}
+
+// TwoDScene::correctLiquidParticles between constrainLiquidVelocity and G2P,
+// as WetClothCore::stepSystem runs it, with LiquidInfo correction_strength,
+// correction_step and correction_multiplier; srand(seed + k) before the k-th
+// call fixes the subset it corrects (strength 0: off)
+void wcref_set_correction(void* hp, double strength, int step, double multiplier,
+                          unsigned seed) {
+  Harness* h = (Harness*)hp;
+  LiquidInfo& li = h->scene->getLiquidInfo();
+  li.correction_strength = strength;
+  li.correction_step = step > 0 ? step : 1;
+  li.correction_multiplier = multiplier;
+  h->corr_on = strength > 0.0;
+  h->corr_seed = seed;
+  h->corr_count = 0;
 }
 
 // AMGPCGSolveSparse iterations and residual of the last snapshot step

@@ -30,6 +30,10 @@ typedef struct {
   int visc_substeps; /* LinearizedImplicitEuler::m_viscosity_substeps */
   double e_flip, e_asym, e_advect; /* elasto_flip_coeff, _asym_coeff, elasto_advect_coeff */
   double drag_mu;  /* LiquidInfo::viscosity as the drag reads it (also when compute_viscosity is off) */
+  /* LiquidInfo correction_strength (0: correctLiquidParticles off),
+   * correction_step, correction_multiplier */
+  double corr_strength, corr_mult;
+  int corr_step;
 } Params;
 
 typedef struct {
@@ -86,6 +90,9 @@ typedef struct {
   int last_iters;
   double last_res;
   double timers[12];
+  double* xw;  /* positions the sub-step's stencil weights were taken at (x3) */
+  uint64_t corr_seed, corr_count; /* selector stream of the particle correction */
+  int corr_sel_once;              /* >= 0: selector of the next correction */
   Snap snaps[256];
   int nsnaps;
 } Scene;
@@ -402,6 +409,9 @@ static void compute_weights(Scene* s) {
   static const double offs[4][3] = {{0.0, 0.5, 0.5}, {0.5, 0.0, 0.5}, {0.5, 0.5, 0.0},
                                     {0.5, 0.5, 0.5}};
   double* W[4] = {s->wu, s->wv, s->ww, s->wp};
+  free(s->xw);
+  s->xw = (double*)malloc(sizeof(double) * 3 * (size_t)(s->np > 0 ? s->np : 1));
+  memcpy(s->xw, s->x, sizeof(double) * 3 * (size_t)s->np);
   const int tmap[4] = {0, 1, 2, 4};
   const double h = s->p.dx;
   for (int p = 0; p < s->np; ++p) {
@@ -1361,12 +1371,206 @@ static void g2p(Scene* s) {
 
 /* SceneStepper::advectScene (SceneStepper.cpp:17-41): liquid x += v dt,
  * elasto x += v dt including the twist */
+/* The solid phi seen by liquid particle p through its solid-phi stencil
+ * (offset 0) with the weights m_particle_weights(., 3) of updateParticleWeights
+ * (TwoDScene.cpp:2113-2127), i.e. taken at the position xw the sub-step's
+ * weights were computed at:
+ *   phi = sum phi_n w_n,  grad = sum phi_n iD w_n (x_n - pos),
+ * grad normalised when its norm exceeds 1e-20; nodes of inactive buckets read
+ * 3 dx (solidProjection :1786-1811, correctLiquidParticles :2030-2050). */
+static void solid_sample(const Scene* s, int p, const double* xw, const double* pos,
+                         double* phi_out, double* grad) {
+  static const double off0[3] = {0.0, 0.0, 0.0};
+  const double h = s->p.dx;
+  const double iD = 4.0 / (h * h);
+  const int* lo = &s->base[p * 15 + 9];
+  double phi_ori = 0.0, g[3] = {0.0, 0.0, 0.0};
+  for (int k = 0; k < 3; ++k)
+    for (int j = 0; j < 3; ++j)
+      for (int i = 0; i < 3; ++i) {
+        const int I = lo[0] + i, J = lo[1] + j, K = lo[2] + k;
+        double np[3];
+        stencil_node_pos(s, I, J, K, off0, np);
+        const double w = quad_kernel((xw[0] - np[0]) / h) * quad_kernel((xw[1] - np[1]) / h) *
+                         quad_kernel((xw[2] - np[2]) / h);
+        const long long n = node_of(s, I, J, K);
+        const double phi = node_active(s, n) ? s->sphi[n] : 3.0 * h;
+        phi_ori += phi * w;
+        const double c = phi * iD * w;
+        for (int q = 0; q < 3; ++q) g[q] += c * (np[q] - pos[q]);
+      }
+  const double nrm = sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
+  if (nrm > 1e-20)
+    for (int q = 0; q < 3; ++q) g[q] /= nrm;
+  *phi_out = phi_ori;
+  for (int q = 0; q < 3; ++q) grad[q] = g[q];
+}
+
+/* SceneStepper::advectScene (SceneStepper.cpp:17-41), then
+ * TwoDScene::solidProjection (TwoDScene.cpp:1776-1821) of the liquid
+ * particles: the solid phi extrapolated by the step just taken,
+ * phi + grad . v dt, pushes a particle that ends inside back out along grad */
 static void advect(Scene* s, double dt) {
   for (int p = 0; p < s->np; ++p) {
     for (int a = 0; a < 3; ++a) s->x[p * 3 + a] += s->v[p * 3 + a] * dt;
     if (p < s->ne) s->xt[p] += s->vt[p] * dt;
   }
+  int projected = 0;
+  for (int p = s->ne; p < s->np; ++p) {
+    double* pos = &s->x[p * 3];
+    double phi, g[3];
+    solid_sample(s, p, &s->xw[p * 3], pos, &phi, g);
+    const double d[3] = {s->v[p * 3] * dt, s->v[p * 3 + 1] * dt, s->v[p * 3 + 2] * dt};
+    const double phi_now = phi + (g[0] * d[0] + g[1] * d[1] + g[2] * d[2]);
+    if (phi_now < 0.0) {
+      for (int q = 0; q < 3; ++q) pos[q] -= phi_now * g[q];
+      ++projected;
+    }
+  }
+  const long long pc = projected;
+  snap_put_i(s, "projected", &pc, 1);
 }
+
+/* SplitMix64 (Steele, Lea and Flood, OOPSLA 2014): the deterministic
+ * stream that stands in for the reference's rand() and scalarRand */
+static uint64_t splitmix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+/* correction selector of call k of a seeded stream */
+int wco_correction_selector(uint64_t seed, uint64_t k, int step) {
+  return (int)(splitmix64(seed ^ splitmix64(k)) % (uint64_t)(step > 0 ? step : 1));
+}
+
+/* uniform [0, 1) for the coincident-pair push of particles i, j (fluid
+ * indices), component c */
+static double pair_unit(int i, int j, int c) {
+  const uint64_t key = ((uint64_t)(uint32_t)i << 34) ^ ((uint64_t)(uint32_t)j << 2) ^ (uint64_t)c;
+  return (double)(splitmix64(key) >> 11) * (1.0 / 9007199254740992.0);
+}
+
+/* TwoDScene::correctLiquidParticles (TwoDScene.cpp:1967-2061): Ando-style
+ * relaxation of the liquid particles with fluid index i % step == selector.
+ * Particles are sorted into the grid cells of rebucketizeParticles
+ * (grid_num_cells :1662-1669; key cell floor((x - origin)/dx), clamped) and
+ * visited in the 8-colour order of Sorter::for_each_bucket_particles_colored
+ * (Sorter.h:403-437), each cell's particles in index order, reading the
+ * positions as they are being moved.  Each pulls away from the neighbours of
+ * the 27 cells around (Sorter.h:352-371 order: x outermost) within
+ * re = sqrt(r_i r_j) * multiplier:
+ *   spring += (strength/dt) smooth_kernel(d^2, re) (x_i - x_j) / d * re,
+ * moves by spring dt and is projected out of the solid along the gradient of
+ * the solid phi when phi + grad . (spring dt) < 0.  Pairs closer than
+ * 1e-4 re get a push re * u with u uniform in [0, 1) per component: from
+ * pair_unit here (scalarRand in the reference). */
+static void correct_liquid(Scene* s, double dt, int selector) {
+  const int nf = s->np - s->ne;
+  if (nf == 0) return;
+  const double dx = s->p.dx;
+  const int step = s->p.corr_step > 0 ? s->p.corr_step : 1;
+  int nc[3];
+  for (int a = 0; a < 3; ++a) {
+    const double content = (s->bbmax[a] - s->bbmin[a]) + s->bs * 3.0 * 2.0;
+    nc[a] = (int)ceil(content / dx);
+    if (nc[a] < 1) nc[a] = 1;
+  }
+  const long long ncell = (long long)nc[0] * nc[1] * nc[2];
+  uint64_t* key = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)nf);
+  for (int i = 0; i < nf; ++i) {
+    const double* x = &s->x[(s->ne + i) * 3];
+    int c[3];
+    for (int a = 0; a < 3; ++a) {
+      c[a] = (int)floor((x[a] - s->org[a]) / dx);
+      if (c[a] < 0) c[a] = 0;
+      if (c[a] > nc[a] - 1) c[a] = nc[a] - 1;
+    }
+    const uint64_t cell = ((uint64_t)c[2] * nc[1] + c[1]) * nc[0] + c[0];
+    key[i] = (cell << 32) | (uint64_t)i;
+  }
+  qsort(key, nf, sizeof(uint64_t), cmp_u64);
+  int* cs = (int*)calloc((size_t)ncell * 2, sizeof(int));
+  for (int q = 0; q < nf; ++q) {
+    const uint64_t b = key[q] >> 32;
+    if (q == 0 || (key[q - 1] >> 32) != b) cs[b * 2] = q;
+    if (q + 1 == nf || (key[q + 1] >> 32) != b) cs[b * 2 + 1] = q + 1;
+  }
+  const double coeff = s->p.corr_strength / dt;
+  const int sn[3] = {(nc[0] + 1) / 2, (nc[1] + 1) / 2, (nc[2] + 1) / 2};
+  for (int t = 0; t < 2; ++t)
+    for (int u = 0; u < 2; ++u)
+      for (int r = 0; r < 2; ++r)
+        for (long long sb = 0; sb < (long long)sn[0] * sn[1] * sn[2]; ++sb) {
+          const int sk = (int)(sb / ((long long)sn[0] * sn[1]));
+          const int sj = (int)((sb - (long long)sk * sn[0] * sn[1]) / sn[0]);
+          const int si = (int)(sb - (long long)sk * sn[0] * sn[1] - (long long)sj * sn[0]);
+          const int ck = sk * 2 + t, cj = sj * 2 + u, ci = si * 2 + r;
+          if (ck >= nc[2] || cj >= nc[1] || ci >= nc[0]) continue;
+          const long long cell = ((long long)ck * nc[1] + cj) * nc[0] + ci;
+          for (int q = cs[cell * 2]; q < cs[cell * 2 + 1]; ++q) {
+            const int i = (int)(key[q] & 0xffffffffu);
+            if (i % step != selector) continue;
+            const int p = s->ne + i;
+            double* pos = &s->x[p * 3];
+            const double ri = s->rad[p];
+            double spring[3] = {0.0, 0.0, 0.0};
+            for (int x = ci - 1; x <= ci + 1; ++x)
+              for (int y = cj - 1; y <= cj + 1; ++y)
+                for (int z = ck - 1; z <= ck + 1; ++z) {
+                  if (x < 0 || x > nc[0] - 1 || y < 0 || y > nc[1] - 1 || z < 0 || z > nc[2] - 1)
+                    continue;
+                  const long long nb = ((long long)z * nc[1] + y) * nc[0] + x;
+                  for (int q2 = cs[nb * 2]; q2 < cs[nb * 2 + 1]; ++q2) {
+                    const int j = (int)(key[q2] & 0xffffffffu);
+                    if (j == i) continue;
+                    const double* xn = &s->x[(s->ne + j) * 3];
+                    const double re = sqrt(ri * s->rad[s->ne + j]) * s->p.corr_mult;
+                    const double d[3] = {pos[0] - xn[0], pos[1] - xn[1], pos[2] - xn[2]};
+                    const double dist = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+                    if (dist > re) continue;
+                    const double sk3 = pow(1.0 - dist * dist / (re * re), 3.0);
+                    const double w = coeff * (sk3 > 0.0 ? sk3 : 0.0);
+                    if (w == 0.0) continue;
+                    if (dist > 1e-4 * re) {
+                      for (int a = 0; a < 3; ++a) spring[a] += w * d[a] / dist * re;
+                    } else {
+                      for (int a = 0; a < 3; ++a) spring[a] += re * pair_unit(i, j, a);
+                    }
+                  }
+                }
+            double buf[3];
+            for (int a = 0; a < 3; ++a) buf[a] = pos[a] + spring[a] * dt;
+            double phi, g[3];
+            solid_sample(s, p, &s->xw[p * 3], pos, &phi, g);
+            const double dp[3] = {spring[0] * dt, spring[1] * dt, spring[2] * dt};
+            const double phi_now = phi + (g[0] * dp[0] + g[1] * dp[1] + g[2] * dp[2]);
+            if (phi_now < 0.0)
+              for (int a = 0; a < 3; ++a) buf[a] -= phi_now * g[a];
+            for (int a = 0; a < 3; ++a) pos[a] = buf[a];
+          }
+        }
+  free(cs);
+  free(key);
+}
+
+/* correctLiquidParticles with an explicit particle subset, outside a step */
+void wco_correct_liquid(Scene* s, double dt, int selector) { correct_liquid(s, dt, selector); }
+
+/* LiquidInfo correction_strength / _step / _multiplier and the seed of the
+ * selector stream (strength 0: off) */
+void wco_set_correction(Scene* s, double strength, int step, double mult, uint64_t seed) {
+  s->p.corr_strength = strength;
+  s->p.corr_step = step > 0 ? step : 1;
+  s->p.corr_mult = mult;
+  s->corr_seed = seed;
+  s->corr_count = 0;
+  s->corr_sel_once = -1;
+}
+
+/* the selector the next correction uses instead of the seeded stream's */
+void wco_set_correction_selector(Scene* s, int selector) { s->corr_sel_once = selector; }
 
 /* ---------------------------------------------------------------------- */
 static void alloc_nodes(Scene* s) {
@@ -1511,8 +1715,20 @@ static void transfer_in(Scene* s, int snapshot) {
   }
 }
 
-/* G2P and advection of a sub-step (WetClothCore.cpp:228-236) */
+/* particle correction, G2P and advection of a sub-step
+ * (WetClothCore.cpp:241-262); G2P keeps the weights of the positions before
+ * the correction and measures x_n - x_p from the corrected ones */
 static void transfer_out(Scene* s, double dt, int snapshot) {
+  if (s->p.corr_strength > 0.0 && s->np > s->ne) {
+    int sel = s->corr_sel_once;
+    if (sel < 0) sel = wco_correction_selector(s->corr_seed, s->corr_count, s->p.corr_step);
+    s->corr_sel_once = -1;
+    ++s->corr_count;
+    correct_liquid(s, dt, sel);
+    const long long sl = sel;
+    snap_put_i(s, "correction_selector", &sl, 1);
+    if (snapshot) snap_particles(s, "corr_");
+  }
   g2p(s);
   if (snapshot) snap_particles(s, "g2p_");
   advect(s, dt);
@@ -1666,6 +1882,9 @@ Scene* wco_create(double dx, const double* g, double rho, double flip, double fr
   s->p.e_asym = 1.0;
   s->p.e_advect = 1.0;
   s->p.drag_mu = 8.9e-3;
+  s->p.corr_step = 8;
+  s->p.corr_mult = 2.0;
+  s->corr_sel_once = -1;
   s->bs = dx * 4.0;
   s->np = np;
   const size_t n = (size_t)(np > 0 ? np : 1);
@@ -1762,7 +1981,7 @@ void wco_destroy(Scene* s) {
                   s->inside, s->wu, s->wv, s->ww, s->wp, s->pu.start, s->pu.pid, s->pu.slot,
                   s->pv.start, s->pv.pid, s->pv.slot, s->pw.start, s->pw.pid, s->pw.slot,
                   s->pp.start, s->pp.pid, s->pp.slot, s->sat_p, s->psi_p, s->pore_p, s->lphi,
-                  s->sphi, s->pressure, s->dofidx, s->rowstart, s->col, s->val, s->b};
+                  s->sphi, s->pressure, s->dofidx, s->rowstart, s->col, s->val, s->b, s->xw};
   for (size_t k = 0; k < sizeof(ptrs) / sizeof(ptrs[0]); ++k) free(ptrs[k]);
   for (int a = 0; a < 3; ++a) {
     void* q[] = {s->mass[a], s->vel[a], s->vol_f[a], s->sat[a], s->psi[a], s->wgt[a], s->svel[a],

@@ -188,3 +188,57 @@ def test_elasto_coupled_step(surfel_every):
     o2.step(DT, snapshot=True)
     a, b = o.get("g2p_v")[-3 * sc.x.shape[0]:], o2.get("g2p_v")
     assert np.abs(a - b).max() > 1e-3 * np.abs(b).max()
+
+
+def _fall(n=16, vy=-3.0):
+    """A dam-break block thrown at the floor: many liquid particles end a
+    sub-step inside the wall and are pushed back out by solidProjection."""
+    sc = scenes.dam_break(n, 8, 0)
+    sc.v[:, 1] = vy
+    return sc
+
+
+@pytest.mark.parametrize("dt", [1e-3, 2e-2])
+def test_solid_projection(dt):
+    """advectScene + solidProjection (TwoDScene.cpp:1776-1821) of the liquid
+    particles at the end of each sub-step."""
+    sc = _fall()
+    r = oref.RefScene(sc, mic=True)
+    o = oo.OracleScene(sc)
+    n = r.step(dt, snapshot=True)
+    assert o.step(dt, snapshot=True) == n
+    assert o.get("projected")[0] > 0
+    for k in ("g2p_v", "adv_x"):
+        a, b = r.get(k), o.get(k)
+        assert np.abs(a - b).max() <= 1e-12 * np.abs(a).max(), k
+
+
+@pytest.mark.parametrize("kind,seed", [("dam16", 3), ("curl16", 11), ("fall", 5)])
+def test_particle_correction(kind, seed):
+    """correctLiquidParticles (TwoDScene.cpp:1967-2061) at the scene parser's
+    defaults (strength 0.2, step 8, multiplier 2): the reference draws its
+    subset with rand() after srand(seed), the oracle is handed the same subset;
+    positions after the correction, G2P (weights of the uncorrected positions,
+    x_n - x_p of the corrected ones) and advection agree."""
+    sc = _fall() if kind == "fall" else _scene(kind)
+    sc.params.correction_strength = 0.2
+    sc.params.correction_seed = seed
+    r = oref.RefScene(sc, mic=True)
+    r.step(DT, snapshot=True)
+    sel = int(r.get("correction_selector")[0])
+    o = oo.OracleScene(sc)
+    o.set_correction_selector(sel)
+    o.step(DT, snapshot=True)
+    assert int(o.get("correction_selector")[0]) == sel
+    moved = np.abs(r.get("corr_x") - r.get("adv_x")).max()
+    assert moved > 0
+    x0 = sc.x.reshape(-1)
+    dx_ref = r.get("corr_x") - x0
+    assert np.abs(dx_ref).max() > 0.0
+    for k in ("corr_x", "g2p_v", "g2p_C", "adv_x"):
+        a, b = r.get(k), o.get(k)
+        assert np.abs(a - b).max() <= 1e-12 * np.abs(a).max(), k
+    # only the chosen subset moved
+    idx = np.arange(sc.x.shape[0])
+    still = (idx % sc.params.correction_step) != sel
+    assert np.array_equal(r.get("corr_x").reshape(-1, 3)[still], sc.x[still])
