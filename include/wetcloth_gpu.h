@@ -69,6 +69,13 @@ typedef struct wcg_params {
   double elasto_advect_coeff;      /* LiquidInfo::elasto_advect_coeff (1.0) */
   double drag_viscosity;           /* LiquidInfo::viscosity as the liquid-solid drag reads it
                                       while the viscosity term is off (8.9e-3) */
+  double correction_strength;      /* LiquidInfo::correction_strength; 0 (default here) turns
+                                      correctLiquidParticles off, the reference's scene
+                                      parser defaults it to 0.2 */
+  int correction_step;             /* LiquidInfo::correction_step (8) */
+  double correction_multiplier;    /* LiquidInfo::correction_multiplier (2.0) */
+  unsigned long long correction_seed; /* seed of the stream that picks each sub-step's
+                                         particle subset (rand() in the reference) */
 } wcg_params;
 
 typedef struct wcg_ctx wcg_ctx;
@@ -168,9 +175,23 @@ int wcg_project_fine(wcg_ctx* ctx, double dt);
 int wcg_apply_pressure_drag_fluid(wcg_ctx* ctx, double dt);
 /* TwoDScene::constrainLiquidVelocity (TwoDScene.cpp:1827) */
 int wcg_constrain_liquid_velocity(wcg_ctx* ctx);
+/* TwoDScene::correctLiquidParticles (TwoDScene.cpp:1967-2061) for the liquid
+ * particles with index % correction_step == selector (the reference draws the
+ * selector with rand(); wcg_substep draws it from wcg_correction_selector).
+ * Runs between wcg_constrain_liquid_velocity and wcg_map_node_particles, as
+ * WetClothCore::stepSystem does (WetClothCore.cpp:242); G2P then keeps the
+ * weights of the positions before the correction.  Coincident pairs (closer
+ * than 1e-4 re) are pushed by a SplitMix64 hash of their indices instead of
+ * scalarRand. */
+int wcg_correct_liquid_particles(wcg_ctx* ctx, double dt, int selector);
+/* the subset wcg_substep corrects in its k-th call: SplitMix64 of the seed and
+ * k, modulo step */
+int wcg_correction_selector(unsigned long long seed, unsigned long long k, int step);
 /* TwoDScene::mapNodeParticlesAPIC (TwoDScene.cpp:6936) */
 int wcg_map_node_particles(wcg_ctx* ctx);
-/* SceneStepper::advectScene (SceneStepper.cpp:17) */
+/* SceneStepper::advectScene (SceneStepper.cpp:17) followed by
+ * TwoDScene::solidProjection (TwoDScene.cpp:1776-1821) of the liquid
+ * particles, as WetClothCore::stepSystem runs them (WetClothCore.cpp:258-262) */
 int wcg_advect(wcg_ctx* ctx, double dt);
 /* One CFL sub-step of everything above (G2P and advection fused). */
 int wcg_substep(wcg_ctx* ctx, double dt);

@@ -53,6 +53,10 @@ class WcgParams(ctypes.Structure):
         ("elasto_flip_asym_coeff", ctypes.c_double),
         ("elasto_advect_coeff", ctypes.c_double),
         ("drag_viscosity", ctypes.c_double),
+        ("correction_strength", ctypes.c_double),
+        ("correction_step", ctypes.c_int),
+        ("correction_multiplier", ctypes.c_double),
+        ("correction_seed", ctypes.c_ulonglong),
     ]
 
 
@@ -104,6 +108,8 @@ SIGNATURES = {
     "wcg_apply_pressure_drag_fluid": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "wcg_constrain_liquid_velocity": (ctypes.c_int, [ctypes.c_void_p]),
     "wcg_map_node_particles": (ctypes.c_int, [ctypes.c_void_p]),
+    "wcg_correct_liquid_particles": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]),
+    "wcg_correction_selector": (ctypes.c_int, [ctypes.c_ulonglong, ctypes.c_ulonglong, ctypes.c_int]),
     "wcg_advect": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "wcg_substep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "wcg_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _I]),

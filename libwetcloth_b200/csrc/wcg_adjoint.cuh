@@ -13,8 +13,10 @@
 //   G2P          v' = sum u w,  C' = flip sum u w d 4/h^2,  x' = x + v' dt
 // (d = x_node - x_particle).  The kernels below apply the transposes in reverse
 // order; A is symmetric, so the adjoint solve reuses the forward solver on the
-// same matrix.  Gradients through the weights' dependence on x are not formed
-// (x-bar passes straight through).  Every sum is a gather in fixed order.
+// same matrix.  After G2P come advection and the solid projection of the
+// particles that end inside the solid (piecewise smooth in v'; k_adj_load).
+// Gradients through the weights' dependence on x are not formed (x-bar
+// passes straight through).  Every sum is a gather in fixed order.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -29,16 +31,62 @@ namespace wcg {
 enum AdjField : int { A_UBAR = 0, A_UTMP = 3, A_VSBAR = 6, kNumAdjFields = 9 };
 
 // Original-order cotangents of (v', C', x') into sorted-order columns:
-// vb = v-bar + dt x-bar (x' = x + v' dt), Cb = C-bar.
+// Cb = C-bar, vb = v-bar + dt d-bar, where d-bar is the cotangent of the step
+// d = v' dt through advection and TwoDScene::solidProjection
+// (TwoDScene.cpp:1776-1821).  A projected particle (phi_now < 0) ends at
+//   x' = x + d - phi_now g,  phi_now = phi + g . d,  g = G / |G|,
+//   G = sum phi_n iD w_n (x_n - x - d),  dG/dd = -iD phi I,
+// so with M = I - g g^T and s = -iD phi / |G| (M = I, s = -iD phi when |G|
+// is at most 1e-20 and G is used unnormalised)
+//   d-bar = x-bar - (g + s M d)(g . x-bar) - phi_now s M x-bar;
+// any other particle has d-bar = x-bar.  v' is recomputed by G2P from the
+// face velocities with constrainLiquidVelocity applied on the fly (friction).
 template <typename R>
-__global__ void k_adj_load(long long np, long long pcap, const int* __restrict__ pid,
-                           const double* __restrict__ vbar, const double* __restrict__ Cbar,
-                           const double* __restrict__ xbar, double dt, R* __restrict__ B) {
+__global__ void __launch_bounds__(128)
+    k_adj_load(GridDesc g, const unsigned char* __restrict__ active, const R* __restrict__ P,
+               long long pcap, long long np, const long long* __restrict__ key,
+               const int* __restrict__ delta, const R* __restrict__ F, long long fstride,
+               R flip, R friction, const int* __restrict__ pid,
+               const double* __restrict__ vbar, const double* __restrict__ Cbar,
+               const double* __restrict__ xbar, double dt, R* __restrict__ B) {
   const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= np) return;
   const long long i = pid[s];
-  for (int a = 0; a < 3; ++a)
-    B[a * pcap + s] = (R)(vbar[i * 3 + a] + dt * xbar[i * 3 + a]);
+  double db[3] = {xbar[i * 3 + 0], xbar[i * 3 + 1], xbar[i * 3 + 2]};
+  const long long kn = key[s];
+  if (kn >= 0) {
+    const R x[3] = {P[PX * pcap + s], P[PY * pcap + s], P[PZ * pcap + s]};
+    int KI, KJ, KK;
+    node_ijk(g, kn, KI, KJ, KK);
+    const int kp[3] = {KI - 1, KJ - 1, KK - 1};
+    const int dl = delta[s];
+    R v[3], C[9];
+    g2p_gather<R>(g, active, F, fstride, kp, dl, x, x, flip, friction, v, C);
+    R d[3], pos[3];
+    for (int q = 0; q < 3; ++q) {
+      d[q] = v[q] * (R)dt;
+      pos[q] = x[q] + d[q];
+    }
+    R phi, gr[3];
+    const R nrm = solid_sample<R>(g, active, F, fstride, kp, dl, x, pos, phi, gr);
+    const double phi_now = (double)phi + ((double)gr[0] * d[0] + (double)gr[1] * d[1] +
+                                          (double)gr[2] * d[2]);
+    if (phi_now < 0.0) {
+      const double iD = 4.0 / (g.dx * g.dx);
+      const bool unit = nrm > R(1e-20);
+      const double sc = unit ? -iD * (double)phi / (double)nrm : -iD * (double)phi;
+      const double gx = gr[0] * db[0] + gr[1] * db[1] + gr[2] * db[2];
+      const double gd = gr[0] * (double)d[0] + gr[1] * (double)d[1] + gr[2] * (double)d[2];
+      double out[3];
+      for (int q = 0; q < 3; ++q) {
+        const double Md = unit ? (double)d[q] - gr[q] * gd : (double)d[q];
+        const double Mx = unit ? db[q] - gr[q] * gx : db[q];
+        out[q] = db[q] - ((double)gr[q] + sc * Md) * gx - phi_now * sc * Mx;
+      }
+      for (int q = 0; q < 3; ++q) db[q] = out[q];
+    }
+  }
+  for (int a = 0; a < 3; ++a) B[a * pcap + s] = (R)(vbar[i * 3 + a] + dt * db[a]);
   for (int q = 0; q < 9; ++q) B[(3 + q) * pcap + s] = (R)Cbar[i * 9 + q];
 }
 

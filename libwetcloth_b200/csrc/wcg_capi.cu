@@ -187,6 +187,10 @@ void wcg_default_params(wcg_params* p) {
   p->elasto_flip_asym_coeff = 1.0;
   p->elasto_advect_coeff = 1.0;
   p->drag_viscosity = 8.9e-3;
+  p->correction_strength = 0.0;
+  p->correction_step = 8;
+  p->correction_multiplier = 2.0;
+  p->correction_seed = 0;
 }
 
 int wcg_create(const wcg_params* params, wcg_ctx** out) {
@@ -204,6 +208,11 @@ int wcg_create(const wcg_params* params, wcg_ctx** out) {
     return fail(WCG_ERR_ARG, "elasto coefficients must be finite");
   if (!(params->drag_viscosity > 0.0) || !std::isfinite(params->drag_viscosity))
     return fail(WCG_ERR_ARG, "drag_viscosity must be finite and > 0");
+  if (!(params->correction_strength >= 0.0) || !std::isfinite(params->correction_strength) ||
+      !std::isfinite(params->correction_multiplier) || params->correction_step < 1)
+    return fail(WCG_ERR_ARG,
+                "correction_strength must be finite and >= 0, correction_step >= 1, "
+                "correction_multiplier finite");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return fail(WCG_ERR_CUDA, "no CUDA device available");
@@ -232,6 +241,10 @@ int wcg_create(const wcg_params* params, wcg_ctx** out) {
   p.elasto_flip_asym = params->elasto_flip_asym_coeff;
   p.elasto_advect = params->elasto_advect_coeff;
   p.drag_viscosity = params->drag_viscosity;
+  p.correction_strength = params->correction_strength;
+  p.correction_step = params->correction_step;
+  p.correction_multiplier = params->correction_multiplier;
+  p.correction_seed = params->correction_seed;
   // wavefront tile shape (performance knob; both compute identical results)
   if (const char* v = getenv("WCG_SWEEP_TILE")) ctx->c.sweep_variant = !strcmp(v, "warp") ? 1 : 0;
   // layout of the pressure solve (performance knob; same arithmetic)
@@ -491,6 +504,20 @@ int wcg_map_node_particles(wcg_ctx* ctx) {
   return device_status(ctx->c, "mapNodeParticlesAPIC");
 }
 
+int wcg_correct_liquid_particles(wcg_ctx* ctx, double dt, int selector) {
+  WCG_CHECK_CTX(ctx);
+  WCG_NEED_GRID(ctx);
+  if (!(dt > 0)) return fail(WCG_ERR_ARG, "dt must be positive");
+  if (selector < 0 || selector >= ctx->c.prm.correction_step)
+    return fail(WCG_ERR_ARG, "selector must lie in [0, correction_step)");
+  WCG_CALL(ctx, wcg::correct_liquid_particles(ctx->c, dt, selector), "correctLiquidParticles");
+  return device_status(ctx->c, "correctLiquidParticles");
+}
+
+int wcg_correction_selector(unsigned long long seed, unsigned long long k, int step) {
+  return wcg::correction_selector(seed, k, step);
+}
+
 int wcg_advect(wcg_ctx* ctx, double dt) {
   WCG_CHECK_CTX(ctx);
   WCG_CALL(ctx, wcg::advect_only(ctx->c, dt), "advectScene");
@@ -516,6 +543,8 @@ int wcg_substep_vjp(wcg_ctx* ctx, double dt, const double* vbar3, const double* 
   WCG_CHECK_CTX(ctx);
   if (!(dt > 0)) return fail(WCG_ERR_ARG, "dt must be positive");
   WCG_NO_ELASTO(ctx, "substep_vjp");
+  if (ctx->c.prm.correction_strength > 0.0)
+    return fail(WCG_ERR_UNSUPPORTED, "substep_vjp: not available with the particle correction on");
   const long long n = ctx->c.np;
   if (n > 0 && (!vbar3 || !Cbar9 || !xbar3 || !vbar0 || !Cbar0 || !xbar0))
     return fail(WCG_ERR_ARG, "null cotangent array");

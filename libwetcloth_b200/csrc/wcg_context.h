@@ -35,6 +35,10 @@ struct Params {
   double elasto_flip_asym; // LiquidInfo::elasto_flip_asym_coeff
   double elasto_advect;    // LiquidInfo::elasto_advect_coeff
   double drag_viscosity;   // LiquidInfo::viscosity as the drag reads it when viscosity == 0
+  double correction_strength;    // LiquidInfo::correction_strength (0: no correction)
+  int correction_step;           // LiquidInfo::correction_step
+  double correction_multiplier;  // LiquidInfo::correction_multiplier
+  unsigned long long correction_seed;  // seed of the per-sub-step subset stream
 };
 
 // A device allocation that grows and never shrinks.
@@ -226,6 +230,14 @@ struct Context {
   struct MgDims { int ni, nj, nk, n; long long off; };
   std::vector<MgDims> mg_dims;     // levels of the last solve
 
+  // particle correction (wcg_correct.cuh): positions before the correction
+  // (3 Reals per particle; valid from the correction to the next grid build),
+  // the cell lists of correctLiquidParticles' own sort, the subset stream
+  DevBuf xw;
+  bool xw_valid = false;
+  DevBuf corr_start, corr_cursor, corr_list;
+  unsigned long long corr_count = 0;
+
   // reverse mode of a sub-step (wcg_adjoint.cuh): grid cotangents, particle
   // cotangents (sorted order), the first extrapolation layer's input mask,
   // host staging
@@ -315,6 +327,11 @@ cudaError_t map_grid_to_particles_and_advect(Context& c, double dt, bool advect)
 cudaError_t advect_only(Context& c, double dt);
 cudaError_t num_substeps(Context& c, double dt, int* n);
 cudaError_t substep(Context& c, double dt);
+// TwoDScene::correctLiquidParticles for the liquid particles with original
+// index % correction_step == selector
+cudaError_t correct_liquid_particles(Context& c, double dt, int selector);
+// subset of call k of the seeded correction stream
+int correction_selector(unsigned long long seed, unsigned long long k, int step);
 // Reverse mode of substep at the current (pre-step) particle state with the
 // positions held fixed: cotangents of (v', C', x') in, of (v, C) and of the
 // viscosity (mubar, may be null) out (host arrays, original order; x-bar

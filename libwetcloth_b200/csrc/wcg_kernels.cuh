@@ -746,30 +746,98 @@ __global__ void __launch_bounds__(192)
   }
 }
 
-// G2P + advection (mapNodeParticlesAPIC TwoDScene.cpp:6936-7000 liquid branch,
-// SceneStepper::advectScene SceneStepper.cpp:17-41): over the particle's own
-// 27-node stencils (nodes of inactive buckets skipped),
-//   v_a = sum u w;  C.row(a) = flip * sum u w (x_n - x_p) 4/h^2;  x += v dt.
+// The solid phi a liquid particle sees through its solid-phi stencil (offset
+// 0 on every axis: base = key node - 1 + stencil offset), with the weights
+// m_particle_weights(., 3) of updateParticleWeights (TwoDScene.cpp:2113-2127)
+// taken at xw, the position the sub-step's weights were computed at:
+//   phi = sum phi_n w_n,   grad = sum phi_n iD w_n (x_n - pos),   iD = 4/h^2,
+// grad normalised when its norm exceeds 1e-20 (solidProjection :1786-1811,
+// correctLiquidParticles :2030-2050); nodes of inactive buckets read 3 dx.
+// Returns the norm of the unnormalised gradient.
 template <typename R>
-__global__ void __launch_bounds__(128)
-    k_g2p(GridDesc g, const unsigned char* __restrict__ active, R* __restrict__ P,
-          long long pcap, long long np, const long long* __restrict__ key,
-          const int* __restrict__ delta, const R* __restrict__ F,
-          long long fstride, R flip, R dt, int advect) {
-  const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= np) return;
+__device__ inline R solid_sample(const GridDesc& g, const unsigned char* __restrict__ active,
+                                 const R* __restrict__ F, long long fstride, const int kp[3],
+                                 int dl, const R xw[3], const R pos[3], R& phi_out, R grad[3]) {
+  const R org[3] = {(R)g.ox, (R)g.oy, (R)g.oz};
+  const R bs = (R)g.bs, dx = (R)g.dx;
+  const R invh = R(1) / dx;
+  const R iD = R(4) / (dx * dx);
+  int base[3];
+  R c[3][3], w[3][3];
+  for (int q = 0; q < 3; ++q) {
+    base[q] = kp[q] + unpack_delta(dl, q);
+    for (int t = 0; t < 3; ++t) {
+      c[q][t] = coord<R>(org[q], bs, dx, base[q] + t, R(0));
+      w[q][t] = quad_kernel<R>((xw[q] - c[q][t]) * invh);
+    }
+  }
+  const R* S = F + G_SPHI * fstride;
+  R phi = 0, g0 = 0, g1 = 0, g2 = 0;
+  for (int k = 0; k < 3; ++k)
+    for (int j = 0; j < 3; ++j)
+      for (int i = 0; i < 3; ++i) {
+        const int NI_ = base[0] + i, NJ_ = base[1] + j, NK_ = base[2] + k;
+        const bool on = in_grid(g, NI_, NJ_, NK_) && active[bucket_of(g, NI_, NJ_, NK_)];
+        const R ph = on ? S[node_linear(g, NI_, NJ_, NK_)] : R(3) * dx;
+        const R wn = w[0][i] * w[1][j] * w[2][k];
+        phi += ph * wn;
+        const R cc = ph * iD * wn;
+        g0 += cc * (c[0][i] - pos[0]);
+        g1 += cc * (c[1][j] - pos[1]);
+        g2 += cc * (c[2][k] - pos[2]);
+      }
+  const R nrm = sqrt(g0 * g0 + g1 * g1 + g2 * g2);
+  if (nrm > R(1e-20)) {
+    g0 /= nrm;
+    g1 /= nrm;
+    g2 /= nrm;
+  }
+  phi_out = phi;
+  grad[0] = g0;
+  grad[1] = g1;
+  grad[2] = g2;
+  return nrm;
+}
+
+// x += v dt followed by TwoDScene::solidProjection (TwoDScene.cpp:1776-1821)
+// of a liquid particle: with the solid phi extrapolated by the step,
+// phi_now = phi + grad . v dt, a particle with phi_now < 0 moves by
+// -phi_now grad.  xw: the position the sub-step's weights were taken at.
+template <typename R>
+__device__ inline void advect_project(const GridDesc& g, const unsigned char* __restrict__ active,
+                                      const R* __restrict__ F, long long fstride,
+                                      const int kp[3], int dl, const R xw[3], const R x[3],
+                                      const R v[3], R dt, R out[3]) {
+  R pos[3], d[3];
+  for (int q = 0; q < 3; ++q) {
+    d[q] = v[q] * dt;
+    pos[q] = x[q] + d[q];
+  }
+  R phi, gr[3];
+  solid_sample<R>(g, active, F, fstride, kp, dl, xw, pos, phi, gr);
+  const R phi_now = phi + (gr[0] * d[0] + gr[1] * d[1] + gr[2] * d[2]);
+  if (phi_now < R(0))
+    for (int q = 0; q < 3; ++q) pos[q] -= phi_now * gr[q];
+  for (int q = 0; q < 3; ++q) out[q] = pos[q];
+}
+
+// G2P of one liquid particle (mapNodeParticlesAPIC TwoDScene.cpp:6936-7000
+// liquid branch) over its own 27-node face stencils, nodes of inactive
+// buckets skipped:
+//   v_a = sum u w;  C.row(a) = flip * sum u w (x_n - x_p) 4/h^2.
+// The weights are taken at xw (the positions the sub-step's weights were
+// computed at, before any particle correction), x_n - x_p from the current
+// position x.  friction >= 0 applies constrainLiquidVelocity to each face
+// value read (u (1 - friction) where the solid weight is 0); -1 reads U as is.
+template <typename R>
+__device__ inline void g2p_gather(const GridDesc& g, const unsigned char* __restrict__ active,
+                                  const R* __restrict__ F, long long fstride, const int kp[3],
+                                  int dl, const R xw[3], const R x[3], R flip, R friction,
+                                  R v[3], R C[9]) {
   const R org[3] = {(R)g.ox, (R)g.oy, (R)g.oz};
   const R bs = (R)g.bs, dx = (R)g.dx;
   const R invh = R(1) / dx;
   const R invD = R(4) / (dx * dx);
-  const R x = P[PX * pcap + s], y = P[PY * pcap + s], z = P[PZ * pcap + s];
-  const long long kn = key[s];
-  if (kn < 0) return;
-  int KI, KJ, KK;
-  node_ijk(g, kn, KI, KJ, KK);
-  const int kp[3] = {KI - 1, KJ - 1, KK - 1};
-  const int dl = delta[s];
-  R v[3], C[9];
   for (int a = 0; a < 3; ++a) {
     int base[3];
     for (int q = 0; q < 3; ++q) base[q] = kp[q] + (q == a ? unpack_delta(dl, a) : 0);
@@ -779,46 +847,93 @@ __global__ void __launch_bounds__(128)
       cx[t] = coord<R>(org[0], bs, dx, base[0] + t, a == 0 ? R(0) : R(0.5));
       cy[t] = coord<R>(org[1], bs, dx, base[1] + t, a == 1 ? R(0) : R(0.5));
       cz[t] = coord<R>(org[2], bs, dx, base[2] + t, a == 2 ? R(0) : R(0.5));
-      wx[t] = quad_kernel<R>((x - cx[t]) * invh);
-      wy[t] = quad_kernel<R>((y - cy[t]) * invh);
-      wz[t] = quad_kernel<R>((z - cz[t]) * invh);
+      wx[t] = quad_kernel<R>((xw[0] - cx[t]) * invh);
+      wy[t] = quad_kernel<R>((xw[1] - cy[t]) * invh);
+      wz[t] = quad_kernel<R>((xw[2] - cz[t]) * invh);
     }
     R fv = 0, b0 = 0, b1 = 0, b2 = 0;
     const R* U = F + (G_U + a) * fstride;
+    const R* W = F + (G_WEIGHT + a) * fstride;
     for (int k = 0; k < 3; ++k)
       for (int j = 0; j < 3; ++j)
         for (int i = 0; i < 3; ++i) {
           const int NI_ = base[0] + i, NJ_ = base[1] + j, NK_ = base[2] + k;
           if (!in_grid(g, NI_, NJ_, NK_) || !active[bucket_of(g, NI_, NJ_, NK_)])
             continue;
-          const R un = U[node_linear(g, NI_, NJ_, NK_)];
+          const long long nn = node_linear(g, NI_, NJ_, NK_);
+          R un = U[nn];
+          if (friction >= R(0) && W[nn] == R(0)) un = (R(1) - friction) * un + friction * R(0);
           const R w = wx[i] * wy[j] * wz[k];
           const R uw = un * w;
           fv += uw;
-          b0 += uw * (cx[i] - x) * invD;
-          b1 += uw * (cy[j] - y) * invD;
-          b2 += uw * (cz[k] - z) * invD;
+          b0 += uw * (cx[i] - x[0]) * invD;
+          b1 += uw * (cy[j] - x[1]) * invD;
+          b2 += uw * (cz[k] - x[2]) * invD;
         }
     v[a] = fv;
     C[a * 3 + 0] = b0 * flip;
     C[a * 3 + 1] = b1 * flip;
     C[a * 3 + 2] = b2 * flip;
   }
+}
+
+// G2P + advection + solid projection (mapNodeParticlesAPIC, then
+// SceneStepper::advectScene SceneStepper.cpp:17-41 and
+// TwoDScene::solidProjection :1776-1821).  XW: positions before the particle
+// correction (3 columns, stride pcap), or null when no correction ran.
+template <typename R>
+__global__ void __launch_bounds__(128)
+    k_g2p(GridDesc g, const unsigned char* __restrict__ active, R* __restrict__ P,
+          long long pcap, long long np, const long long* __restrict__ key,
+          const int* __restrict__ delta, const R* __restrict__ F,
+          long long fstride, R flip, R dt, int advect, const R* __restrict__ XW) {
+  const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= np) return;
+  const R x[3] = {P[PX * pcap + s], P[PY * pcap + s], P[PZ * pcap + s]};
+  R xw[3] = {x[0], x[1], x[2]};
+  if (XW)
+    for (int q = 0; q < 3; ++q) xw[q] = XW[q * pcap + s];
+  const long long kn = key[s];
+  if (kn < 0) return;
+  int KI, KJ, KK;
+  node_ijk(g, kn, KI, KJ, KK);
+  const int kp[3] = {KI - 1, KJ - 1, KK - 1};
+  const int dl = delta[s];
+  R v[3], C[9];
+  g2p_gather<R>(g, active, F, fstride, kp, dl, xw, x, flip, R(-1), v, C);
   for (int a = 0; a < 3; ++a) P[(VX + a) * pcap + s] = v[a];
   for (int q = 0; q < 9; ++q) P[(C00 + q) * pcap + s] = C[q];
   if (advect) {
-    P[PX * pcap + s] = x + v[0] * dt;
-    P[PY * pcap + s] = y + v[1] * dt;
-    P[PZ * pcap + s] = z + v[2] * dt;
+    R xn[3];
+    advect_project<R>(g, active, F, fstride, kp, dl, xw, x, v, dt, xn);
+    for (int q = 0; q < 3; ++q) P[(PX + q) * pcap + s] = xn[q];
   }
 }
 
+// advection + solid projection alone (after a separate G2P)
 template <typename R>
-__global__ void k_advect(R* __restrict__ P, long long pcap, long long np, R dt) {
+__global__ void k_advect(GridDesc g, const unsigned char* __restrict__ active, R* __restrict__ P,
+                         long long pcap, long long np, const long long* __restrict__ key,
+                         const int* __restrict__ delta, const R* __restrict__ F,
+                         long long fstride, R dt, const R* __restrict__ XW) {
   const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= np) return;
-  for (int a = 0; a < 3; ++a)
-    P[(PX + a) * pcap + s] = P[(PX + a) * pcap + s] + P[(VX + a) * pcap + s] * dt;
+  const R x[3] = {P[PX * pcap + s], P[PY * pcap + s], P[PZ * pcap + s]};
+  const R v[3] = {P[VX * pcap + s], P[VY * pcap + s], P[VZ * pcap + s]};
+  R xw[3] = {x[0], x[1], x[2]};
+  if (XW)
+    for (int q = 0; q < 3; ++q) xw[q] = XW[q * pcap + s];
+  const long long kn = key[s];
+  if (kn < 0) {
+    for (int q = 0; q < 3; ++q) P[(PX + q) * pcap + s] = x[q] + v[q] * dt;
+    return;
+  }
+  int KI, KJ, KK;
+  node_ijk(g, kn, KI, KJ, KK);
+  const int kp[3] = {KI - 1, KJ - 1, KK - 1};
+  R xn[3];
+  advect_project<R>(g, active, F, fstride, kp, delta[s], xw, x, v, dt, xn);
+  for (int q = 0; q < 3; ++q) P[(PX + q) * pcap + s] = xn[q];
 }
 
 }  // namespace wcg

@@ -16,6 +16,7 @@
 #include "wcg_visc.cuh"
 #include "wcg_elasto.cuh"
 #include "wcg_adjoint.cuh"
+#include "wcg_correct.cuh"
 #include "wcg_scan.cuh"
 
 namespace wcg {
@@ -61,15 +62,27 @@ cudaError_t ctx_init(Context& c) {
 void ctx_free(Context& c) {
   DevBuf* bufs[] = {&c.pbuf[0], &c.pbuf[1], &c.pid[0], &c.pid[1], &c.pkey,
                     &c.pdelta, &c.pbucket, &c.perm, &c.hostorder,
+                    &c.ebuf[0], &c.ebuf[1], &c.epid[0], &c.epid[1], &c.ekey, &c.edelta,
+                    &c.ebucket, &c.eperm, &c.estage, &c.ecell_start, &c.efield,
                     &c.active_pre, &c.active, &c.cell_start, &c.cell_cursor,
                     &c.gfield, &c.gvalid, &c.gdof, &c.wave_list, &c.wave_count,
-                    &c.tile_flag, &c.active_list, &c.rx64, &c.rr64, &c.rb64,
-                    &c.pl, &c.pl64, &c.pl_edge, &c.pl_order, &c.pl_part,
+                    &c.tile_flag, &c.tile_active, &c.tile_part, &c.active_list,
+                    &c.rx64, &c.rr64, &c.rb64,
+                    &c.pl, &c.pl64, &c.pl_edge, &c.pl_order, &c.pl_corder, &c.pl_part,
                     &c.mg, &c.mg_mask, &c.mg_vec,
+                    &c.adj, &c.adjp, &c.adjmask, &c.adjstage, &c.adjvisc,
+                    &c.xw, &c.corr_start, &c.corr_cursor, &c.corr_list,
                     &c.scratch, &c.dscalars, &c.derr, &c.ticket};
   for (DevBuf* b : bufs) b->release();
   if (c.hscalars) cudaFreeHost(c.hscalars);
   c.hscalars = nullptr;
+  for (Context::ProfRec& r : c.prof_recs) {
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  c.prof_recs.clear();
+  for (cudaEvent_t e : c.prof_pool) cudaEventDestroy(e);
+  c.prof_pool.clear();
   if (c.stream) cudaStreamDestroy(c.stream);
   c.stream = nullptr;
 }
@@ -433,6 +446,7 @@ static cudaError_t ensure_scratch(Context& c, size_t bytes) {
 template <typename R>
 static cudaError_t build_grid_t(Context& c) {
   ProfScope prof(c, P_GRID);
+  c.xw_valid = false;  // the weights now follow the current positions
   const long long n = c.np;
   R* P = c.pbuf[c.cur].as<R>();
   WCG_TRY(ensure_scratch(c, (size_t)kRedBlocks * 12 * sizeof(double)));
@@ -1787,7 +1801,8 @@ static cudaError_t g2p_t(Context& c, double dt, bool advect) {
     ++c.launches, k_g2p<R><<<nblk(c.np, 128), 128, 0, c.stream>>>(
         c.g, c.active.as<unsigned char>(), c.pbuf[c.cur].as<R>(), c.pcap, c.np,
         c.pkey.as<long long>() + c.cur * c.pcap, c.pdelta.as<int>() + c.cur * c.pcap,
-        c.gfield.as<R>(), c.gcap, (R)c.prm.flip_coeff, (R)dt, advect ? 1 : 0);
+        c.gfield.as<R>(), c.gcap, (R)c.prm.flip_coeff, (R)dt, advect ? 1 : 0,
+        c.xw_valid ? c.xw.as<R>() : nullptr);
   if (c.ne > 0) elasto_g2p_t<R>(c, dt, true, advect);
   return cudaGetLastError();
 }
@@ -1796,16 +1811,22 @@ cudaError_t map_grid_to_particles_and_advect(Context& c, double dt, bool advect)
   return c.prm.precision == 0 ? g2p_t<double>(c, dt, advect) : g2p_t<float>(c, dt, advect);
 }
 
+template <typename R>
+static void advect_liquid_t(Context& c, double dt) {
+  ++c.launches, k_advect<R><<<nblk(c.np, 128), 128, 0, c.stream>>>(
+      c.g, c.active.as<unsigned char>(), c.pbuf[c.cur].as<R>(), c.pcap, c.np,
+      c.pkey.as<long long>() + c.cur * c.pcap, c.pdelta.as<int>() + c.cur * c.pcap,
+      c.gfield.as<R>(), c.gcap, (R)dt, c.xw_valid ? c.xw.as<R>() : nullptr);
+}
+
 cudaError_t advect_only(Context& c, double dt) {
   if (c.np + c.ne == 0) return cudaSuccess;
   ProfScope prof(c, P_G2P);
   if (c.np > 0) {
     if (c.prm.precision == 0)
-      ++c.launches, k_advect<double><<<nblk(c.np, 256), 256, 0, c.stream>>>(
-          c.pbuf[c.cur].as<double>(), c.pcap, c.np, dt);
+      advect_liquid_t<double>(c, dt);
     else
-      ++c.launches, k_advect<float><<<nblk(c.np, 256), 256, 0, c.stream>>>(
-          c.pbuf[c.cur].as<float>(), c.pcap, c.np, (float)dt);
+      advect_liquid_t<float>(c, dt);
   }
   if (c.ne > 0) {
     if (c.prm.precision == 0)
@@ -2010,8 +2031,11 @@ static cudaError_t substep_vjp_t(Context& c, double dt, const double* vbar, cons
     dr.lo[a] = c.drange_h[a];
     dr.hi[a] = c.drange_h[3 + a];
   }
-  ++c.launches, k_adj_load<R><<<nblk(np, 256), 256, 0, c.stream>>>(
-      np, c.pcap, c.pid[c.cur].as<int>(), st, st + 3 * np, st + 12 * np, dt, B);
+  ++c.launches, k_adj_load<R><<<nblk(np, 128), 128, 0, c.stream>>>(
+      c.g, act, c.pbuf[c.cur].as<R>(), c.pcap, np, c.pkey.as<long long>() + c.cur * c.pcap,
+      c.pdelta.as<int>() + c.cur * c.pcap, F, c.gcap, (R)c.prm.flip_coeff,
+      (R)c.prm.liquid_boundary_friction, c.pid[c.cur].as<int>(), st, st + 3 * np,
+      st + 12 * np, dt, B);
   ++c.launches, k_adj_g2p<R><<<nb, 192, 0, c.stream>>>(
       c.g, al, c.pbuf[c.cur].as<R>(), c.pcap, c.cell_start.as<int>(),
       c.pdelta.as<int>() + c.cur * c.pcap, dr, B, F, c.gcap, AG, (R)c.prm.flip_coeff,
@@ -2072,6 +2096,66 @@ cudaError_t substep_vjp(Context& c, double dt, const double* vbar, const double*
              : substep_vjp_t<float>(c, dt, vbar, Cbar, xbar, vbar0, Cbar0, mubar);
 }
 
+int correction_selector(unsigned long long seed, unsigned long long k, int step) {
+  return (int)(splitmix64(seed ^ splitmix64(k)) % (unsigned long long)(step > 0 ? step : 1));
+}
+
+template <typename R>
+static cudaError_t correct_liquid_t(Context& c, double dt, int selector) {
+  const long long n = c.np;
+  if (n == 0 || c.n_active == 0 || !(c.prm.correction_strength > 0.0)) return cudaSuccess;
+  ProfScope prof(c, P_OTHER);
+  R* P = c.pbuf[c.cur].as<R>();
+  // positions before the correction: G2P keeps their weights
+  WCG_TRY(c.xw.ensure((size_t)3 * c.pcap * sizeof(R)));
+  WCG_TRY(cudaMemcpyAsync(c.xw.p, P + PX * c.pcap, 3 * c.pcap * sizeof(R),
+                          cudaMemcpyDeviceToDevice, c.stream));
+  c.xw_valid = true;
+  // the cells of rebucketizeParticles (grid_num_cells, TwoDScene.cpp:1662-1669)
+  CellGrid cg;
+  const double org[3] = {c.g.ox, c.g.oy, c.g.oz};
+  long long ncell = 1;
+  for (int a = 0; a < 3; ++a) {
+    const double content = (c.bbx_max[a] - c.bbx_min[a]) + c.g.bs * 3.0 * 2.0;
+    cg.n[a] = std::max(1, (int)std::ceil(content / c.prm.dx));
+    cg.org[a] = org[a];
+    ncell *= cg.n[a];
+  }
+  cg.dx = c.prm.dx;
+  WCG_TRY(c.corr_start.ensure((size_t)(ncell + 1) * sizeof(int)));
+  WCG_TRY(c.corr_cursor.ensure((size_t)ncell * sizeof(int)));
+  WCG_TRY(c.corr_list.ensure((size_t)n * sizeof(int)));
+  const long long scan_tiles = (std::max(ncell + 1, n) + kScanTile - 1) / kScanTile + 1;
+  WCG_TRY(ensure_scratch(c, (size_t)scan_tiles * sizeof(long long) + 64));
+  int* start = c.corr_start.as<int>();
+  int* cursor = c.corr_cursor.as<int>();
+  int* list = c.corr_list.as<int>();
+  long long* cell = c.pkey.as<long long>() + (c.cur ^ 1) * c.pcap;  // free half
+  const int* pid = c.pid[c.cur].as<int>();
+  WCG_TRY(cudaMemsetAsync(start, 0, (size_t)(ncell + 1) * sizeof(int), c.stream));
+  WCG_TRY(cudaMemsetAsync(cursor, 0, (size_t)ncell * sizeof(int), c.stream));
+  ++c.launches, k_corr_cells<R><<<nblk(n, 256), 256, 0, c.stream>>>(P, c.pcap, n, cg, cell, start);
+  exclusive_scan<int, int>(start, ncell, start, c.scratch.as<int>(), start + ncell, c.stream);
+  ++c.launches, k_sort_scatter<<<nblk(n, 256), 256, 0, c.stream>>>(cell, n, start, cursor, list);
+  ++c.launches, k_sort_cells<<<nblk(ncell, 256), 256, 0, c.stream>>>(start, ncell, pid, list);
+  const long long ncol = (long long)((cg.n[0] + 1) / 2) * ((cg.n[1] + 1) / 2) * ((cg.n[2] + 1) / 2);
+  const int step = c.prm.correction_step > 0 ? c.prm.correction_step : 1;
+  for (int t = 0; t < 2; ++t)
+    for (int u = 0; u < 2; ++u)
+      for (int r = 0; r < 2; ++r)
+        ++c.launches, k_correct<R><<<nblk(ncol, 128), 128, 0, c.stream>>>(
+            c.g, cg, r, u, t, P, c.pcap, pid, list, start,
+            c.pkey.as<long long>() + c.cur * c.pcap, c.pdelta.as<int>() + c.cur * c.pcap,
+            c.active.as<unsigned char>(), c.gfield.as<R>(), c.gcap, c.xw.as<R>(), selector, step,
+            (R)(c.prm.correction_strength / dt), (R)c.prm.correction_multiplier, (R)dt);
+  return cudaGetLastError();
+}
+
+cudaError_t correct_liquid_particles(Context& c, double dt, int selector) {
+  return c.prm.precision == 0 ? correct_liquid_t<double>(c, dt, selector)
+                              : correct_liquid_t<float>(c, dt, selector);
+}
+
 cudaError_t substep(Context& c, double dt) {
   WCG_TRY(build_grid(c));
   WCG_TRY(map_particles_to_grid(c));
@@ -2079,6 +2163,12 @@ cudaError_t substep(Context& c, double dt) {
   WCG_TRY(project_fine(c, dt));
   WCG_TRY(apply_pressure_and_extrapolate(c, dt));
   WCG_TRY(constrain_liquid_velocity(c));
+  // correctLiquidParticles (WetClothCore.cpp:242), subset from the seeded stream
+  if (c.prm.correction_strength > 0.0 && c.np > 0) {
+    const int sel = correction_selector(c.prm.correction_seed, c.corr_count++,
+                                        c.prm.correction_step);
+    WCG_TRY(correct_liquid_particles(c, dt, sel));
+  }
   WCG_TRY(map_grid_to_particles_and_advect(c, dt, true));
   return cudaSuccess;
 }

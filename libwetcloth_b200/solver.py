@@ -42,6 +42,10 @@ def make_params(p, precision=_capi.WCG_FP64, refine_inner_tol=0.0,
     prm.elasto_flip_asym_coeff = getattr(p, "elasto_flip_asym_coeff", 1.0)
     prm.elasto_advect_coeff = getattr(p, "elasto_advect_coeff", 1.0)
     prm.drag_viscosity = getattr(p, "drag_viscosity", 8.9e-3)
+    prm.correction_strength = getattr(p, "correction_strength", 0.0)
+    prm.correction_step = getattr(p, "correction_step", 8)
+    prm.correction_multiplier = getattr(p, "correction_multiplier", 2.0)
+    prm.correction_seed = getattr(p, "correction_seed", 0)
     return prm
 
 
@@ -179,6 +183,10 @@ class FluidScene:
 
     def constrain_liquid_velocity(self):
         check(self.L.wcg_constrain_liquid_velocity(self.h))
+
+    def correct_liquid_particles(self, dt, selector):
+        """correctLiquidParticles for the particles with index % step == selector."""
+        check(self.L.wcg_correct_liquid_particles(self.h, dt, int(selector)))
 
     def map_node_particles(self):
         check(self.L.wcg_map_node_particles(self.h))

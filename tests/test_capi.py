@@ -66,3 +66,35 @@ def test_noalloc_size_limit_checked_before_device_work():
     rc = L.wcg_pressure_solve_noalloc(0, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1e-6, 10, None,
                                       ctypes.byref(it), ctypes.byref(res))
     assert rc == _capi.WCG_ERR_ARG
+
+
+def test_correction_params_and_selector_stream():
+    """Correction defaults and checks; the subset stream of wcg_step is the
+    oracle's (host code, no device needed)."""
+    L = _capi.load()
+    p = _capi.WcgParams()
+    L.wcg_default_params(ctypes.byref(p))
+    assert p.correction_strength == 0.0 and p.correction_step == 8
+    assert p.correction_multiplier == 2.0 and p.correction_seed == 0
+    h = ctypes.c_void_p()
+    p.correction_step = 0
+    assert L.wcg_create(ctypes.byref(p), ctypes.byref(h)) == _capi.WCG_ERR_ARG
+    assert b"correction" in L.wcg_last_error()
+    p.correction_step = 8
+    p.correction_strength = -0.1
+    assert L.wcg_create(ctypes.byref(p), ctypes.byref(h)) == _capi.WCG_ERR_ARG
+    assert L.wcg_correct_liquid_particles(None, 1e-3, 0) == _capi.WCG_ERR_ARG
+    from oracle import oracle as oo
+    if not oo.available():
+        pytest.skip("oracle not built")
+    O = oo.lib()
+    seen = set()
+    for seed in (0, 1, 7, 2**40 + 3):
+        for k in range(50):
+            for step in (1, 3, 8):
+                s = L.wcg_correction_selector(seed, k, step)
+                assert s == O.wco_correction_selector(seed, k, step)
+                assert 0 <= s < step
+                if step == 8:
+                    seen.add(s)
+    assert seen == set(range(8))
