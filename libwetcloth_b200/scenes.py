@@ -38,6 +38,10 @@ class SceneParams:
     elasto_flip_asym_coeff: float = 1.0   # LiquidInfo elasto_flip_asym_coeff
     elasto_advect_coeff: float = 1.0      # LiquidInfo elasto_advect_coeff
     drag_viscosity: float = 8.9e-3        # LiquidInfo viscosity as the drag reads it
+    # LiquidInfo::implicit_viscosity (stepImplicitViscosityDiagonalPCG) and the
+    # stepper's viscous criterion
+    viscosity_implicit: bool = False
+    viscosity_criterion: float = 1e-6
     # correctLiquidParticles (TwoDScene.cpp:1967): LiquidInfo correction_strength
     # (0 turns it off), correction_step, correction_multiplier, and the seed of
     # the stream that picks each sub-step's particle subset

@@ -33,6 +33,10 @@ def lib():
                                  ctypes.c_int, ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _D, _D]
         L.wco_destroy.argtypes = [ctypes.c_void_p]
         L.wco_set_viscosity.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
+        L.wco_set_viscosity_implicit.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double]
+        L.wco_viscosity_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                                          ctypes.POINTER(ctypes.c_double),
+                                          ctypes.POINTER(ctypes.c_int)]
         L.wco_set_elasto.argtypes = [ctypes.c_void_p, ctypes.c_int] + [_D] * 10 + [_I, _D]
         L.wco_set_elasto_coeffs.argtypes = [ctypes.c_void_p] + [ctypes.c_double] * 3
         L.wco_transfer.argtypes = [ctypes.c_void_p, ctypes.c_double]
@@ -108,6 +112,8 @@ class OracleScene:
         mu = getattr(p, "viscosity", 0.0)
         if mu > 0.0:
             L.wco_set_viscosity(self.h, mu, getattr(p, "viscosity_substeps", 1))
+        if mu > 0.0 and getattr(p, "viscosity_implicit", False):
+            L.wco_set_viscosity_implicit(self.h, 1, getattr(p, "viscosity_criterion", 1e-6))
         set_elasto(L.wco_set_elasto, L.wco_set_elasto_coeffs, self.h, scene, self._keep)
         if getattr(p, "correction_strength", 0.0) > 0.0:
             L.wco_set_correction(self.h, p.correction_strength, p.correction_step,
@@ -150,6 +156,13 @@ class OracleScene:
         out = np.empty(n, dtype=np.int64)
         self.L.wco_get_i(self.h, name.encode(), out.ctypes.data_as(_L))
         return out
+
+    def viscosity_stats(self):
+        """(iterations, residual, unknowns) of the last implicit viscosity solve"""
+        it, nd = ctypes.c_int(0), ctypes.c_int(0)
+        res = ctypes.c_double(0)
+        self.L.wco_viscosity_stats(self.h, ctypes.byref(it), ctypes.byref(res), ctypes.byref(nd))
+        return it.value, res.value, nd.value
 
     def solver_stats(self):
         it = ctypes.c_int(0)

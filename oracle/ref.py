@@ -49,6 +49,8 @@ def _lib(omp: bool):
         L.wcref_timers.argtypes = [ctypes.c_void_p, _D]
         L.wcref_amg_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), _D]
         L.wcref_set_viscosity.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
+        L.wcref_set_viscosity_implicit.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int,
+                                                   ctypes.c_double]
         _I = ctypes.POINTER(ctypes.c_int)
         L.wcref_set_elasto.argtypes = [ctypes.c_void_p, ctypes.c_int] + [_D] * 10 + [_I, _D]
         L.wcref_set_elasto_coeffs.argtypes = [ctypes.c_void_p] + [ctypes.c_double] * 3
@@ -106,7 +108,10 @@ class RefScene:
             scene.x.shape[0], arr(scene.x.reshape(-1)), arr(scene.v.reshape(-1)),
             C, arr(scene.mass), arr(scene.vol), arr(scene.radius))
         mu = getattr(p, "viscosity", 0.0)
-        if mu > 0.0:
+        if mu > 0.0 and getattr(p, "viscosity_implicit", False):
+            self.L.wcref_set_viscosity_implicit(self.h, mu, getattr(p, "viscosity_substeps", 1),
+                                                getattr(p, "viscosity_criterion", 1e-6))
+        elif mu > 0.0:
             self.L.wcref_set_viscosity(self.h, mu, getattr(p, "viscosity_substeps", 1))
         set_elasto(self.L.wcref_set_elasto, self.L.wcref_set_elasto_coeffs, self.h, scene,
                    self._keep)

@@ -253,6 +253,11 @@ void snap_p2g(Harness& h) {
     dense(h, "liquid_ex_vf", s.m_node_liquid_ex_vf);
     dense(h, "liquid_ey_vf", s.m_node_liquid_ey_vf);
     dense(h, "liquid_ez_vf", s.m_node_liquid_ez_vf);
+    if (s.getLiquidInfo().implicit_viscosity) {
+      dense(h, "liquid_u_vf", s.m_node_liquid_u_vf);
+      dense(h, "liquid_v_vf", s.m_node_liquid_v_vf);
+      dense(h, "liquid_w_vf", s.m_node_liquid_w_vf);
+    }
   }
   dense(h, "solid_phi", s.m_node_solid_phi);
   dense(h, "solid_weight_x", s.m_node_solid_weight_x);
@@ -268,6 +273,28 @@ void snap_predict(Harness& h) {
   dense(h, "v_star_x", e.m_node_v_fluid_plus_x);
   dense(h, "v_star_y", e.m_node_v_fluid_plus_y);
   dense(h, "v_star_z", e.m_node_v_fluid_plus_z);
+  const LiquidInfo& li = h.scene->getLiquidInfo();
+  if (li.compute_viscosity && li.implicit_viscosity) {
+    // the last implicit viscosity sub-step's system (Viscosity.cpp:789-1779)
+    const robertbridson::SparseMatrix<scalar>& A = e.m_visc_matrix;
+    std::vector<long long>& rs = h.ii["V_rowstart"];
+    std::vector<long long>& ci = h.ii["V_col"];
+    std::vector<double>& va = h.f["V_val"];
+    rs.assign(1, 0);
+    ci.clear();
+    va.clear();
+    for (unsigned i = 0; i < A.n; ++i) {
+      for (size_t k = 0; k < A.index[i].size(); ++k) {
+        ci.push_back(A.index[i][k]);
+        va.push_back(A.value[i][k]);
+      }
+      rs.push_back((long long)ci.size());
+    }
+    h.f["V_rhs"] = e.m_visc_rhs;
+    h.f["V_rhs"].resize(A.n);
+    h.f["V_soln"] = e.m_visc_solution;
+    h.f["V_soln"].resize(A.n);
+  }
   dense(h, "rhs_fluid_x", e.m_node_rhs_fluid_x);
   dense(h, "rhs_fluid_y", e.m_node_rhs_fluid_y);
   dense(h, "rhs_fluid_z", e.m_node_rhs_fluid_z);
@@ -655,6 +682,20 @@ void wcref_set_viscosity(void* hp, double mu, int substeps) {
   // the sub-step count is a constructor argument of the stepper
   h->stepper = std::make_shared<LinearizedImplicitEuler>(
       1e-6, h->p.criterion, 1e-6, 1e-6, h->p.maxiters, 1, substeps > 0 ? substeps : 1, 1);
+  h->stepper->setUseApic(true);
+}
+
+// implicit liquid viscosity: LiquidInfo::compute_viscosity and
+// implicit_viscosity on, viscosity mu, the stepper's viscosity sub-steps and
+// viscous criterion (call before the first step)
+void wcref_set_viscosity_implicit(void* hp, double mu, int substeps, double criterion) {
+  Harness* h = (Harness*)hp;
+  LiquidInfo& li = h->scene->getLiquidInfo();
+  li.compute_viscosity = mu > 0.0;
+  li.implicit_viscosity = true;
+  li.viscosity = mu;
+  h->stepper = std::make_shared<LinearizedImplicitEuler>(
+      1e-6, h->p.criterion, 1e-6, criterion, h->p.maxiters, 1, substeps > 0 ? substeps : 1, 1);
   h->stepper->setUseApic(true);
 }
 

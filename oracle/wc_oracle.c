@@ -28,6 +28,8 @@ typedef struct {
   int maxiters, mic;
   double visc;       /* LiquidInfo::viscosity; 0: compute_viscosity off */
   int visc_substeps; /* LinearizedImplicitEuler::m_viscosity_substeps */
+  int visc_implicit; /* LiquidInfo::implicit_viscosity */
+  double visc_criterion; /* LinearizedImplicitEuler::m_viscous_criterion */
   double e_flip, e_asym, e_advect; /* elasto_flip_coeff, _asym_coeff, elasto_advect_coeff */
   double drag_mu;  /* LiquidInfo::viscosity as the drag reads it (also when compute_viscosity is off) */
   /* LiquidInfo correction_strength (0: correctLiquidParticles off),
@@ -79,6 +81,9 @@ typedef struct {
   double *emass[3], *evel[3], *evol[3], *esf[3], *eori[3];
   double *sat_p, *psi_p, *pore_p, *lphi, *sphi, *pressure;
   double *vf_c, *vf_e[3];  /* liquid volume fractions: cell centres, x/y/z edges */
+  double* vf_f[3];         /* ... at x/y/z faces (implicit viscosity) */
+  int visc_iters, visc_ndof; /* last implicit viscosity solve */
+  double visc_res;
   double *rhs[3], *vstar[3], *invC[3], *psifs[3], *psisf[3], *mshdvm[3], *mfhdvm[3];
   unsigned char* valid[3];
   /* pressure system */
@@ -789,17 +794,19 @@ static double interp_lphi(const Scene* s, const double* pos) {
  * the node position in world units, not cells, and so does this. */
 static void volume_fractions(Scene* s) {
   const double dx = s->p.dx;
-  const double offs[4][3] = {{0.5, 0.5, 0.5}, {0.5, 0.0, 0.0}, {0.0, 0.5, 0.0}, {0.0, 0.0, 0.5}};
-  double* out[4] = {s->vf_c, s->vf_e[0], s->vf_e[1], s->vf_e[2]};
+  const double offs[7][3] = {{0.5, 0.5, 0.5}, {0.5, 0.0, 0.0}, {0.0, 0.5, 0.0}, {0.0, 0.0, 0.5},
+                             {0.0, 0.5, 0.5}, {0.5, 0.0, 0.5}, {0.5, 0.5, 0.0}};
+  double* out[7] = {s->vf_c, s->vf_e[0], s->vf_e[1], s->vf_e[2], s->vf_f[0], s->vf_f[1], s->vf_f[2]};
+  const int nf = s->p.visc_implicit ? 7 : 4;
   for (long long n = 0; n < s->nnode; ++n) {
-    for (int f = 0; f < 4; ++f) out[f][n] = 0.0;
+    for (int f = 0; f < nf; ++f) out[f][n] = 0.0;
     if (!s->act[n >> 6]) continue;
     int I, J, K;
     node_ijk(s, n, &I, &J, &K);
     const double corner[3] = {node_coord(s, 0, I, 0.0), node_coord(s, 1, J, 0.0),
                               node_coord(s, 2, K, 0.0)};
     const double o = 0.5 * dx;
-    for (int f = 0; f < 4; ++f) {
+    for (int f = 0; f < nf; ++f) {
       const double c[3] = {corner[0] + offs[f][0], corner[1] + offs[f][1], corner[2] + offs[f][2]};
       double ph[8];
       for (int z = 0; z < 2; ++z)
@@ -890,6 +897,206 @@ static void viscosity_explicit(Scene* s, double* const* src, double* const* dst,
   }
 }
 
+int wco_pcg_solve(int n, const int* rs, const int* col, const double* val, const double* rhs,
+                  double* result, double tol_factor, int maxiters, double omega,
+                  double min_ratio, double* residual_out, int* iters_out);
+
+/* node state of a face for the viscosity (updateSolidPhi, TwoDScene.cpp:7972-8056):
+ * solid when the solid phi at the centres of its two cells (those in active
+ * buckets) sums below zero, fluid otherwise */
+static int face_is_fluid(const Scene* s, int a, int I, int J, int K) {
+  double sphi = 0.0;
+  for (int t = 0; t < 2; ++t) {
+    const int ci = I - (a == 0 && t == 0), cj = J - (a == 1 && t == 0), ck = K - (a == 2 && t == 0);
+    if (!node_active(s, node_of(s, ci, cj, ck))) continue;
+    sphi += wall_phi(s, node_coord(s, 0, ci, 0.5), node_coord(s, 1, cj, 0.5), node_coord(s, 2, ck, 0.5));
+  }
+  return !(sphi < 0.0);
+}
+
+/* the liquid volume weights around a face of axis a, in the reference's
+ * order right, left, top, bottom, front, back (+x, -x, +y, -y, +z, -z): the
+ * cell centres along a, the edges across the other two axes
+ * (constructViscosityMatrixRHS :1130-1151 and its y/z counterparts) */
+static void face_vols(const Scene* s, int a, int I, int J, int K, double vol[6]) {
+  for (int d = 0; d < 6; ++d) {
+    const int ax = d >> 1, up = !(d & 1);
+    int o[3] = {0, 0, 0};
+    const double* f;
+    if (ax == a) {
+      f = s->vf_c;
+      if (!up) o[a] = -1;
+    } else {
+      f = s->vf_e[3 - a - ax];
+      if (up) o[ax] = 1;
+    }
+    vol[d] = vget(s, f, I + o[0], J + o[1], K + o[2], 0.0);
+  }
+}
+
+typedef struct {
+  int n;
+  int col[16];
+  double val[16];
+} VRow;
+
+static void vrow_add(VRow* r, int j, double v) {
+  int k = 0;
+  while (k < r->n && r->col[k] < j) ++k;
+  if (k < r->n && r->col[k] == j) {
+    r->val[k] += v;
+    return;
+  }
+  for (int q = r->n; q > k; --q) {
+    r->col[q] = r->col[q - 1];
+    r->val[q] = r->val[q - 1];
+  }
+  r->col[k] = j;
+  r->val[k] = v;
+  ++r->n;
+}
+
+/* One implicit viscosity sub-step (constructViscosityMatrixRHS /
+ * updateViscosityRHS Viscosity.cpp:169-1779, applyNodeViscosityImplicit
+ * :101-167): the faces of axis x, then y, then z, bucket by bucket, that are
+ * fluid and touch liquid (own, cell or edge volume fraction > 0) become
+ * unknowns;
+ *   (V_f + f sum_d w_d V_d) u - f sum_d w_d V_d u_d - f sum (cross terms) = V_f u_src,
+ * f = dt mu / (rho dx^2), w_d = 2 along the face's own axis, 1 across;
+ * neighbours that are solid faces move to the rhs with their source values.
+ * Solved with robertbridson::PCGSolver (MIC(0) 0.97, minimum diagonal ratio
+ * 0.1); fluid faces that are no unknown keep their value, other faces take
+ * the solid velocity. */
+static void viscosity_implicit(Scene* s, double* const* vel, double dt) {
+  const double dx = s->p.dx;
+  const double factor = dt / (dx * dx) * s->p.visc / s->p.rho;
+  const long long nn = s->nnode;
+  int* idx = (int*)malloc(sizeof(int) * 3 * (size_t)nn);
+  unsigned char* fl = (unsigned char*)calloc(3 * (size_t)nn, 1);
+  int ndof = 0;
+  for (int a = 0; a < 3; ++a)
+    for (long long n = 0; n < nn; ++n) {
+      idx[a * nn + n] = -1;
+      if (!s->act[n >> 6]) continue;
+      int I, J, K;
+      node_ijk(s, n, &I, &J, &K);
+      fl[a * nn + n] = (unsigned char)face_is_fluid(s, a, I, J, K);
+      if (!fl[a * nn + n]) continue;
+      double vol[6];
+      face_vols(s, a, I, J, K, vol);
+      int any = s->vf_f[a][n] > 0.0;
+      for (int d = 0; d < 6; ++d) any |= vol[d] > 0.0;
+      if (any) idx[a * nn + n] = ndof++;
+    }
+  s->visc_ndof = ndof;
+  s->visc_iters = 0;
+  s->visc_res = 0.0;
+  if (ndof == 0) {
+    free(idx);
+    free(fl);
+    return;
+  }
+  VRow* rows = (VRow*)calloc((size_t)ndof, sizeof(VRow));
+  double* rhs = (double*)malloc(sizeof(double) * (size_t)ndof);
+  for (int a = 0; a < 3; ++a)
+    for (long long n = 0; n < nn; ++n) {
+      const int row = idx[a * nn + n];
+      if (row < 0) continue;
+      int I, J, K;
+      node_ijk(s, n, &I, &J, &K);
+      VRow* R = &rows[row];
+      rhs[row] = s->vf_f[a][n] * vel[a][n];
+      vrow_add(R, row, s->vf_f[a][n]);
+      double vol[6];
+      face_vols(s, a, I, J, K, vol);
+      /* same-axis neighbours */
+      for (int d = 0; d < 6; ++d) {
+        if (!(vol[d] > 0.0)) continue;
+        const int ax = d >> 1, sg = (d & 1) ? -1 : 1;
+        const int q[3] = {I + (ax == 0) * sg, J + (ax == 1) * sg, K + (ax == 2) * sg};
+        const long long m = node_of(s, q[0], q[1], q[2]);
+        if (!node_active(s, m)) continue;
+        const double w = ax == a ? 2.0 : 1.0;
+        vrow_add(R, row, w * factor * vol[d]);
+        if (fl[a * nn + m])
+          vrow_add(R, idx[a * nn + m], -w * factor * vol[d]);
+        else
+          rhs[row] -= -w * vel[a][m] * factor * vol[d];
+      }
+      /* cross terms: the two faces of axis ax on the edge across direction d */
+      for (int d = 0; d < 6; ++d) {
+        const int ax = d >> 1, sg = (d & 1) ? -1 : 1;
+        if (ax == a || !(vol[d] > 0.0)) continue;
+        for (int t = 0; t < 2; ++t) {
+          int q[3] = {I, J, K};
+          if (sg > 0) q[ax] += 1;
+          if (t == 1) q[a] -= 1;
+          const long long m = node_of(s, q[0], q[1], q[2]);
+          if (!node_active(s, m)) continue;
+          const double c = (t == 0 ? -1.0 : 1.0) * (double)sg;
+          if (fl[ax * nn + m])
+            vrow_add(R, idx[ax * nn + m], c * factor * vol[d]);
+          else
+            rhs[row] -= c * vel[ax][m] * factor * vol[d];
+        }
+      }
+    }
+  int* rs = (int*)malloc(sizeof(int) * ((size_t)ndof + 1));
+  rs[0] = 0;
+  for (int r = 0; r < ndof; ++r) rs[r + 1] = rs[r] + rows[r].n;
+  int* col = (int*)malloc(sizeof(int) * (size_t)rs[ndof]);
+  double* val = (double*)malloc(sizeof(double) * (size_t)rs[ndof]);
+  for (int r = 0; r < ndof; ++r)
+    for (int k = 0; k < rows[r].n; ++k) {
+      col[rs[r] + k] = rows[r].col[k];
+      val[rs[r] + k] = rows[r].val[k];
+    }
+  double* soln = (double*)malloc(sizeof(double) * (size_t)ndof);
+  wco_pcg_solve(ndof, rs, col, val, rhs, soln, s->p.visc_criterion, s->p.maxiters, 0.97, 0.1,
+                &s->visc_res, &s->visc_iters);
+  for (int a = 0; a < 3; ++a)
+    for (long long n = 0; n < nn; ++n) {
+      if (!s->act[n >> 6]) continue;
+      if (fl[a * nn + n]) {
+        if (idx[a * nn + n] >= 0) vel[a][n] = soln[idx[a * nn + n]];
+      } else {
+        vel[a][n] = s->svel[a][n];
+      }
+    }
+  /* the system of this sub-step, in the reference's CSR order */
+  {
+    long long* t = (long long*)malloc(sizeof(long long) * ((size_t)rs[ndof] + (size_t)ndof + 1));
+    for (int r = 0; r <= ndof; ++r) t[r] = rs[r];
+    snap_put_i(s, "V_rowstart", t, ndof + 1);
+    for (int k = 0; k < rs[ndof]; ++k) t[k] = col[k];
+    snap_put_i(s, "V_col", t, rs[ndof]);
+    free(t);
+    snap_put_f(s, "V_val", val, rs[ndof]);
+    snap_put_f(s, "V_rhs", rhs, ndof);
+    snap_put_f(s, "V_soln", soln, ndof);
+    double* vu = (double*)malloc(sizeof(double) * (size_t)ndof);
+    for (int a = 0; a < 3; ++a)
+      for (long long n = 0; n < nn; ++n)
+        if (idx[a * nn + n] >= 0) vu[idx[a * nn + n]] = s->vf_f[a][n];
+    snap_put_f(s, "V_volu", vu, ndof);
+    free(vu);
+    long long* vf = (long long*)malloc(sizeof(long long) * (size_t)ndof);
+    for (int a = 0; a < 3; ++a)
+      for (long long n = 0; n < nn; ++n)
+        if (idx[a * nn + n] >= 0) vf[idx[a * nn + n]] = a * nn + n;
+    snap_put_i(s, "V_face", vf, ndof);
+    free(vf);
+  }
+  free(soln);
+  free(val);
+  free(col);
+  free(rs);
+  free(rhs);
+  free(rows);
+  free(idx);
+  free(fl);
+}
+
 static void step_velocity(Scene* s, double dt) {
   for (int a = 0; a < 3; ++a)
     for (long long n = 0; n < s->nnode; ++n) {
@@ -937,6 +1144,11 @@ static void step_velocity(Scene* s, double dt) {
     double* tmp[3];
     for (int a = 0; a < 3; ++a) tmp[a] = (double*)malloc(sizeof(double) * (size_t)s->nnode);
     for (int it = 0; it < ns; ++it) {
+      if (s->p.visc_implicit) {
+        /* stepImplicitViscosityDiagonalPCG (LinearizedImplicitEuler.cpp:2127-2172) */
+        viscosity_implicit(s, s->vstar, sub_dt);
+        continue;
+      }
       for (int a = 0; a < 3; ++a) memcpy(tmp[a], s->vstar[a], sizeof(double) * (size_t)s->nnode);
       viscosity_explicit(s, tmp, s->vstar, sub_dt);
     }
@@ -1590,7 +1802,8 @@ static void alloc_nodes(Scene* s) {
     s->valid[a] = (unsigned char*)calloc(n, 1);
   }
   double** G[] = {&s->sat_p, &s->psi_p, &s->pore_p, &s->lphi, &s->sphi, &s->pressure,
-                  &s->vf_c, &s->vf_e[0], &s->vf_e[1], &s->vf_e[2]};
+                  &s->vf_c, &s->vf_e[0], &s->vf_e[1], &s->vf_e[2], &s->vf_f[0],
+                  &s->vf_f[1], &s->vf_f[2]};
   for (size_t k = 0; k < sizeof(G) / sizeof(G[0]); ++k) {
     free(*G[k]);
     *G[k] = (double*)calloc(n, sizeof(double));
@@ -1690,6 +1903,9 @@ static void transfer_in(Scene* s, int snapshot) {
       snprintf(nm, sizeof nm, "vol_fluid_%c", xyz[a]); snap_node(s, nm, s->vol_f[a]);
       if (s->p.visc > 0.0) {
         snprintf(nm, sizeof nm, "liquid_e%c_vf", xyz[a]); snap_node(s, nm, s->vf_e[a]);
+        if (s->p.visc_implicit) {
+          snprintf(nm, sizeof nm, "liquid_%c_vf", "uvw"[a]); snap_node(s, nm, s->vf_f[a]);
+        }
       }
       snprintf(nm, sizeof nm, "sat_%c", xyz[a]); snap_node(s, nm, s->sat[a]);
       snprintf(nm, sizeof nm, "psi_%c", xyz[a]); snap_node(s, nm, s->psi[a]);
@@ -1860,6 +2076,19 @@ void wco_set_viscosity(Scene* s, double mu, int substeps) {
   s->p.drag_mu = mu > 0.0 ? mu : 8.9e-3;
 }
 
+/* LiquidInfo::implicit_viscosity and the stepper's viscous criterion */
+void wco_set_viscosity_implicit(Scene* s, int implicit, double criterion) {
+  s->p.visc_implicit = implicit;
+  s->p.visc_criterion = criterion;
+}
+
+/* iterations, residual and unknowns of the last implicit viscosity solve */
+void wco_viscosity_stats(Scene* s, int* iters, double* res, int* ndof) {
+  *iters = s->visc_iters;
+  *res = s->visc_res;
+  *ndof = s->visc_ndof;
+}
+
 Scene* wco_create(double dx, const double* g, double rho, double flip, double friction,
                   const double* bc, const double* bh, double br, double criterion,
                   int maxiters, int mic, int np, const double* x3, const double* v3,
@@ -1884,6 +2113,7 @@ Scene* wco_create(double dx, const double* g, double rho, double flip, double fr
   s->p.drag_mu = 8.9e-3;
   s->p.corr_step = 8;
   s->p.corr_mult = 2.0;
+  s->p.visc_criterion = 1e-6;
   s->corr_sel_once = -1;
   s->bs = dx * 4.0;
   s->np = np;
@@ -1981,7 +2211,8 @@ void wco_destroy(Scene* s) {
                   s->inside, s->wu, s->wv, s->ww, s->wp, s->pu.start, s->pu.pid, s->pu.slot,
                   s->pv.start, s->pv.pid, s->pv.slot, s->pw.start, s->pw.pid, s->pw.slot,
                   s->pp.start, s->pp.pid, s->pp.slot, s->sat_p, s->psi_p, s->pore_p, s->lphi,
-                  s->sphi, s->pressure, s->dofidx, s->rowstart, s->col, s->val, s->b, s->xw};
+                  s->sphi, s->pressure, s->dofidx, s->rowstart, s->col, s->val, s->b, s->xw,
+                  s->vf_c, s->vf_e[0], s->vf_e[1], s->vf_e[2], s->vf_f[0], s->vf_f[1], s->vf_f[2]};
   for (size_t k = 0; k < sizeof(ptrs) / sizeof(ptrs[0]); ++k) free(ptrs[k]);
   for (int a = 0; a < 3; ++a) {
     void* q[] = {s->mass[a], s->vel[a], s->vol_f[a], s->sat[a], s->psi[a], s->wgt[a], s->svel[a],

@@ -83,3 +83,82 @@ def test_viscosity_changes_the_flow_and_fp32(wcg):
     assert g32.stats()["converged"] == 1
     assert np.abs(v32 - v1).max() <= 1e-5 * np.abs(v1).max()
     g32.close()
+
+
+def _implicit(kind, mu, ns, criterion):
+    sc = _scene(kind, mu)
+    sc.params.viscosity_substeps = ns
+    sc.params.viscosity_implicit = True
+    sc.params.viscosity_criterion = criterion
+    sc.params.maxiters = 5000
+    return sc
+
+
+@pytest.mark.parametrize("kind,mu,ns", [("dam16", 0.5, 1), ("curl16", 2.0, 2), ("dam16", 50.0, 1),
+                                        ("curl32", 1.0, 1)])
+def test_implicit_viscosity_fp64(kind, mu, ns, wcg):
+    """Implicit viscosity (stepImplicitViscosityDiagonalPCG), pinned to the
+    reference through the oracle (test_oracle_vs_reference.py::
+    test_implicit_viscosity).  The GPU solves the same system matrix-free with
+    the diagonal as preconditioner: face volume fractions to 1e-10; on the last
+    sub-step the GPU's velocities solve the oracle's assembled system to the
+    criterion; the velocities agree on every face with liquid volume (where
+    the system's null space vanishes) to 1e-8."""
+    sc = _implicit(kind, mu, ns, 1e-13)
+    o = oo.OracleScene(sc)
+    o.step(DT, snapshot=True)
+    g = FluidScene(sc)
+    g.rebucketize_and_resample()
+    g.map_particle_nodes()
+    for k in ("liquid_u_vf", "liquid_v_vf", "liquid_w_vf", "liquid_c_vf", "liquid_ey_vf"):
+        _close(g.field(k), o.get(k), 1e-10, k)
+    g.step_velocity(DT)
+    st = g.stats()
+    assert st["visc_converged"] == 1 and st["visc_iters"] > 0
+    vs = [g.field("v_star_" + c) for c in "xyz"]
+    rs, ci, va, b = o.get("V_rowstart"), o.get("V_col"), o.get("V_val"), o.get("V_rhs")
+    face = o.get("V_face")
+    nn = vs[0].size
+    x = np.array([vs[f // nn][f % nn] for f in face])
+    import scipy.sparse as sps
+    A = sps.csr_matrix((va, ci, rs), shape=(rs.size - 1, rs.size - 1))
+    if ns == 1:
+        assert np.abs(b - A @ x).max() <= 1e-11 * np.abs(b).max()
+    errs, scale = [], 0.0
+    for a, c in enumerate("xyz"):
+        m = np.nan_to_num(o.get("liquid_" + "uvw"[a] + "_vf"), nan=0.0) > 0.0
+        ov = o.get("v_star_" + c)
+        errs.append(np.abs(vs[a][m] - ov[m]).max())
+        scale = max(scale, np.abs(ov[m]).max())
+    assert max(errs) <= 1e-8 * scale, errs
+    g.close()
+
+
+def test_implicit_viscosity_steps_and_fp32(wcg):
+    """Whole steps with the implicit viscosity converge in both precisions;
+    FP32 (criterion 1e-5) agrees with the FP64 oracle to 1e-4 on faces with
+    liquid volume."""
+    sc = _implicit("curl16", 2.0, 1, 1e-5)
+    o = oo.OracleScene(sc)
+    o.step(DT, snapshot=True)
+    g = FluidScene(sc, precision=_capi.WCG_FP32_REFINE)
+    g.rebucketize_and_resample()
+    g.map_particle_nodes()
+    g.step_velocity(DT)
+    errs, scale = [], 0.0
+    for a, c in enumerate("xyz"):
+        m = np.nan_to_num(o.get("liquid_" + "uvw"[a] + "_vf"), nan=0.0) > 0.0
+        ov = o.get("v_star_" + c)
+        errs.append(np.abs(g.field("v_star_" + c)[m] - ov[m]).max())
+        scale = max(scale, np.abs(ov[m]).max())
+    assert max(errs) <= 1e-4 * scale, errs
+    g.close()
+    for prec in (_capi.WCG_FP64, _capi.WCG_FP32_REFINE):
+        g = FluidScene(_implicit("dam16", 0.5, 2, 1e-6), precision=prec)
+        for _ in range(3):
+            g.step(DT)
+        st = g.stats()
+        assert st["converged"] == 1 and st["visc_converged"] == 1 and st["visc_iters"] > 0
+        x, v, C = g.download()
+        assert np.all(np.isfinite(v))
+        g.close()

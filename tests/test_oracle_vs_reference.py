@@ -242,3 +242,58 @@ def test_particle_correction(kind, seed):
     idx = np.arange(sc.x.shape[0])
     still = (idx % sc.params.correction_step) != sel
     assert np.array_equal(r.get("corr_x").reshape(-1, 3)[still], sc.x[still])
+
+
+@pytest.mark.parametrize("kind,mu,ns", [("dam16", 0.5, 1), ("curl16", 2.0, 2), ("dam16", 50.0, 1)])
+def test_implicit_viscosity(kind, mu, ns):
+    """stepImplicitViscosityDiagonalPCG (LinearizedImplicitEuler.cpp:2127) with
+    constructViscosityMatrixRHS / updateViscosityRHS (Viscosity.cpp:169-1779):
+    face volume fractions, the unknowns and the last sub-step's system (CSR
+    structure exact, values and rhs to 1e-12; 1e-9 for the rhs of a later
+    sub-step, which carries the earlier solution).  Unknowns without liquid
+    volume of their own that touch liquid only across edges make the matrix
+    singular, and the solution there is whatever the solver's Krylov path
+    leaves, on either side; the solution is compared on the unknowns with
+    their own liquid volume (the null space vanishes there; 1e-8, as the
+    system is ill-conditioned next to it), and the reference's solution
+    solves the oracle's system to the criterion."""
+    sc = _scene(kind)
+    sc.params.viscosity = mu
+    sc.params.viscosity_substeps = ns
+    sc.params.viscosity_implicit = True
+    sc.params.viscosity_criterion = 1e-13
+    sc.params.maxiters = 5000
+    r = oref.RefScene(sc, mic=True)
+    o = oo.OracleScene(sc)
+    r.step(DT, snapshot=True)
+    o.step(DT, snapshot=True)
+    for k in ("V_rowstart", "V_col"):
+        assert np.array_equal(r.get(k), o.get(k)), k
+    for k in ("liquid_u_vf", "liquid_v_vf", "liquid_w_vf"):
+        a, b = r.get(k), o.get(k)
+        m = ~np.isnan(a)
+        assert np.array_equal(m, ~np.isnan(b)), k
+        assert np.abs(a[m] - b[m]).max() <= 1e-12, k
+    va, vb = r.get("V_val"), o.get("V_val")
+    assert np.abs(va - vb).max() <= 1e-12 * np.abs(va).max()
+    ba, bb = r.get("V_rhs"), o.get("V_rhs")
+    assert np.abs(ba - bb).max() <= (1e-12 if ns == 1 else 1e-9) * np.abs(ba).max()
+    import scipy.sparse as sps
+    rs, ci = o.get("V_rowstart"), o.get("V_col")
+    n = rs.size - 1
+    A = sps.csr_matrix((vb, ci, rs), shape=(n, n))
+    xr, xo = r.get("V_soln"), o.get("V_soln")
+    assert np.abs(bb - A @ xr).max() <= 1e-11 * np.abs(bb).max()
+    own = o.get("V_volu") > 0.0
+    assert own.sum() > 0 and (~own).sum() > 0
+    assert np.abs(xr[own] - xo[own]).max() <= 1e-8 * np.abs(xr).max()
+    it, res, nd = o.viscosity_stats()
+    assert nd == n and it > 0
+    errs, scale = [], 0.0
+    for k in ("v_star_x", "v_star_y", "v_star_z"):
+        f = r.get("liquid_" + "uvw"["xyz".index(k[-1])] + "_vf")
+        m = np.nan_to_num(f, nan=0.0) > 0.0
+        a, b = r.get(k), o.get(k)
+        errs.append(np.abs(a[m] - b[m]).max())
+        scale = max(scale, np.abs(a[m]).max())
+    assert max(errs) <= 1e-8 * scale, errs
