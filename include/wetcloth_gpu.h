@@ -76,6 +76,13 @@ typedef struct wcg_params {
   double correction_multiplier;    /* LiquidInfo::correction_multiplier (2.0) */
   unsigned long long correction_seed; /* seed of the stream that picks each sub-step's
                                          particle subset (rand() in the reference) */
+  int viscosity_implicit;          /* LiquidInfo::implicit_viscosity: each viscosity sub-step
+                                      solves the implicit system
+                                      (stepImplicitViscosityDiagonalPCG,
+                                      LinearizedImplicitEuler.cpp:2127) with PCG
+                                      preconditioned by its diagonal */
+  double viscosity_criterion;      /* LinearizedImplicitEuler::m_viscous_criterion (1e-6):
+                                      ||r||_inf <= criterion ||b||_inf */
 } wcg_params;
 
 typedef struct wcg_ctx wcg_ctx;
@@ -89,6 +96,9 @@ typedef struct wcg_stats {
   double rhs_norm;   /* ||b||_inf */
   long long ndof;
   long long nactive_buckets;
+  int visc_iters;        /* iterations of the last implicit viscosity solve */
+  int visc_converged;    /* every implicit viscosity solve of the last step converged */
+  double visc_residual;  /* its final ||b - A u||_inf */
 } wcg_stats;
 
 const char* wcg_last_error(void);

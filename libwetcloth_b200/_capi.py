@@ -57,6 +57,8 @@ class WcgParams(ctypes.Structure):
         ("correction_step", ctypes.c_int),
         ("correction_multiplier", ctypes.c_double),
         ("correction_seed", ctypes.c_ulonglong),
+        ("viscosity_implicit", ctypes.c_int),
+        ("viscosity_criterion", ctypes.c_double),
     ]
 
 
@@ -70,6 +72,9 @@ class WcgStats(ctypes.Structure):
         ("rhs_norm", ctypes.c_double),
         ("ndof", ctypes.c_longlong),
         ("nactive_buckets", ctypes.c_longlong),
+        ("visc_iters", ctypes.c_int),
+        ("visc_converged", ctypes.c_int),
+        ("visc_residual", ctypes.c_double),
     ]
 
 

@@ -106,6 +106,7 @@ const FieldName kFields[] = {
     {"b_dense", wcg::G_B}, {"mic_invdiag", wcg::G_INVDIAG},
     {"liquid_c_vf", wcg::G_VFC}, {"liquid_ex_vf", wcg::G_VFEX},
     {"liquid_ey_vf", wcg::G_VFEY}, {"liquid_ez_vf", wcg::G_VFEZ},
+    {"liquid_u_vf", wcg::G_VFU}, {"liquid_v_vf", wcg::G_VFV}, {"liquid_w_vf", wcg::G_VFW},
 };
 
 int lookup_field(const char* name, int* ncomp = nullptr) {
@@ -191,6 +192,8 @@ void wcg_default_params(wcg_params* p) {
   p->correction_step = 8;
   p->correction_multiplier = 2.0;
   p->correction_seed = 0;
+  p->viscosity_implicit = 0;
+  p->viscosity_criterion = 1e-6;
 }
 
 int wcg_create(const wcg_params* params, wcg_ctx** out) {
@@ -208,6 +211,8 @@ int wcg_create(const wcg_params* params, wcg_ctx** out) {
     return fail(WCG_ERR_ARG, "elasto coefficients must be finite");
   if (!(params->drag_viscosity > 0.0) || !std::isfinite(params->drag_viscosity))
     return fail(WCG_ERR_ARG, "drag_viscosity must be finite and > 0");
+  if (!(params->viscosity_criterion > 0.0) || !std::isfinite(params->viscosity_criterion))
+    return fail(WCG_ERR_ARG, "viscosity_criterion must be finite and > 0");
   if (!(params->correction_strength >= 0.0) || !std::isfinite(params->correction_strength) ||
       !std::isfinite(params->correction_multiplier) || params->correction_step < 1)
     return fail(WCG_ERR_ARG,
@@ -245,6 +250,8 @@ int wcg_create(const wcg_params* params, wcg_ctx** out) {
   p.correction_step = params->correction_step;
   p.correction_multiplier = params->correction_multiplier;
   p.correction_seed = params->correction_seed;
+  p.viscosity_implicit = params->viscosity_implicit ? 1 : 0;
+  p.viscosity_criterion = params->viscosity_criterion;
   // wavefront tile shape (performance knob; both compute identical results)
   if (const char* v = getenv("WCG_SWEEP_TILE")) ctx->c.sweep_variant = !strcmp(v, "warp") ? 1 : 0;
   // layout of the pressure solve (performance knob; same arithmetic)
@@ -464,7 +471,12 @@ int wcg_step_velocity(wcg_ctx* ctx, double dt) {
   WCG_NEED_GRID(ctx);
   if (!(dt > 0)) return fail(WCG_ERR_ARG, "dt must be positive");
   WCG_CALL(ctx, wcg::step_velocity(ctx->c, dt), "stepVelocity");
-  return device_status(ctx->c, "stepVelocity");
+  int s = device_status(ctx->c, "stepVelocity");
+  if (s) return s;
+  if (!ctx->c.stats.visc_converged)
+    return fail(WCG_ERR_NOT_CONVERGED, "implicit viscosity PCG did not converge (residual " +
+                                           std::to_string(ctx->c.stats.visc_residual) + ")");
+  return WCG_OK;
 }
 
 int wcg_project_fine(wcg_ctx* ctx, double dt) {
@@ -534,6 +546,8 @@ int wcg_substep(wcg_ctx* ctx, double dt) {
   ctx->c.have_grid = false;
   if (!ctx->c.stats.converged)
     return fail(WCG_ERR_NOT_CONVERGED, "pressure PCG did not converge");
+  if (!ctx->c.stats.visc_converged)
+    return fail(WCG_ERR_NOT_CONVERGED, "implicit viscosity PCG did not converge");
   return WCG_OK;
 }
 
@@ -545,6 +559,8 @@ int wcg_substep_vjp(wcg_ctx* ctx, double dt, const double* vbar3, const double* 
   WCG_NO_ELASTO(ctx, "substep_vjp");
   if (ctx->c.prm.correction_strength > 0.0)
     return fail(WCG_ERR_UNSUPPORTED, "substep_vjp: not available with the particle correction on");
+  if (ctx->c.prm.viscosity > 0.0 && ctx->c.prm.viscosity_implicit)
+    return fail(WCG_ERR_UNSUPPORTED, "substep_vjp: not available with the implicit viscosity");
   const long long n = ctx->c.np;
   if (n > 0 && (!vbar3 || !Cbar9 || !xbar3 || !vbar0 || !Cbar0 || !xbar0))
     return fail(WCG_ERR_ARG, "null cotangent array");
@@ -606,6 +622,9 @@ int wcg_get_stats(const wcg_ctx* ctx, wcg_stats* out) {
   out->rhs_norm = s.rhs_norm;
   out->ndof = s.ndof;
   out->nactive_buckets = s.nactive;
+  out->visc_iters = s.visc_iters;
+  out->visc_converged = s.visc_converged;
+  out->visc_residual = s.visc_residual;
   return WCG_OK;
 }
 

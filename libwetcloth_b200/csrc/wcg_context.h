@@ -30,7 +30,9 @@ struct Params {
   int max_refinements;
   int solver;     // 0: MIC(0)-PCG, 1: multigrid-PCG (AMGPCGSolveSparse)
   double viscosity;        // LiquidInfo::viscosity (0: compute_viscosity off)
-  int viscosity_substeps;  // explicit viscosity sub-steps per step_velocity
+  int viscosity_substeps;  // viscosity sub-steps per step_velocity
+  int viscosity_implicit;  // LiquidInfo::implicit_viscosity
+  double viscosity_criterion;  // LinearizedImplicitEuler::m_viscous_criterion
   double elasto_flip;      // LiquidInfo::elasto_flip_coeff
   double elasto_flip_asym; // LiquidInfo::elasto_flip_asym_coeff
   double elasto_advect;    // LiquidInfo::elasto_advect_coeff
@@ -57,6 +59,9 @@ struct Stats {
   int pcg_iters = 0;          // total inner PCG iterations of the last solve
   int refinements = 0;        // FP64 outer iterations of the last solve
   double residual = 0;        // final ||b - A p||_inf of the last solve
+  int visc_iters = 0;         // iterations of the last implicit viscosity solve
+  double visc_residual = 0;   // its final ||b - A u||_inf
+  int visc_converged = 1;     // every implicit viscosity solve of the step converged
   double rhs_norm = 0;        // ||b||_inf of the last solve
   int converged = 1;
   long long ndof = 0;
@@ -106,7 +111,10 @@ enum GField : int {
   G_VFEX = 54,         // ... at x-, y-, z-edge nodes
   G_VFEY = 55,
   G_VFEZ = 56,
-  kNumGFields = 57
+  G_VFU = 57,          // ... at x-, y-, z-faces (implicit viscosity)
+  G_VFV = 58,
+  G_VFW = 59,
+  kNumGFields = 60
 };
 
 // Columns of the elasto (cloth / yarn) particle SoA.  Positions come first so
@@ -242,6 +250,10 @@ struct Context {
   // cotangents (sorted order), the first extrapolation layer's input mask,
   // host staging
   DevBuf adj, adjp, adjmask, adjstage, adjvisc;
+
+  // implicit viscosity (wcg_visc.cuh): PCG vectors x, r, p, q and the
+  // diagonal (3 face fields each), face flags
+  DevBuf visc, viscflag;
 
   // FP64 refinement vectors (precision 1)
   DevBuf rx64, rr64, rb64;       // nnode doubles each

@@ -71,6 +71,7 @@ void ctx_free(Context& c) {
                     &c.pl, &c.pl64, &c.pl_edge, &c.pl_order, &c.pl_corder, &c.pl_part,
                     &c.mg, &c.mg_mask, &c.mg_vec,
                     &c.adj, &c.adjp, &c.adjmask, &c.adjstage, &c.adjvisc,
+                    &c.visc, &c.viscflag,
                     &c.xw, &c.corr_start, &c.corr_cursor, &c.corr_list,
                     &c.scratch, &c.dscalars, &c.derr, &c.ticket};
   for (DevBuf* b : bufs) b->release();
@@ -711,13 +712,87 @@ static cudaError_t map_particles_to_grid_t(Context& c) {
   // liquid volume fractions for the viscosity (updateLiquidPhi :3353-3367)
   if (c.prm.viscosity > 0.0 && c.np > 0)
     ++c.launches, k_volume_fractions<R><<<(unsigned)c.n_active, 64, 0, c.stream>>>(
-        c.g, c.active_list.as<int>(), c.active.as<unsigned char>(), F, c.gcap);
+        c.g, c.active_list.as<int>(), c.active.as<unsigned char>(), F, c.gcap,
+        c.prm.viscosity_implicit ? 7 : 4);
   return cudaGetLastError();
 }
 
 cudaError_t map_particles_to_grid(Context& c) {
   return c.prm.precision == 0 ? map_particles_to_grid_t<double>(c)
                               : map_particles_to_grid_t<float>(c);
+}
+
+static cudaError_t fetch(Context& c, const double* d, int k, double* h);
+
+// One implicit viscosity sub-step on G_VSTAR (stepImplicitViscosityDiagonalPCG
+// LinearizedImplicitEuler.cpp:2127-2172 with the PCG stop rule of
+// robertbridson::PCGSolver::solve PCGSolver.h:261-330: ||r||_inf <=
+// criterion ||b||_inf; the diagonal preconditions).  Device scalars 40-43:
+// max |r|, p.q and rho (two slots).
+template <typename R>
+static cudaError_t viscosity_implicit_t(Context& c, double dt) {
+  const unsigned nb = (unsigned)c.n_active;
+  const int* al = c.active_list.as<int>();
+  const unsigned char* act = c.active.as<unsigned char>();
+  R* F = c.gfield.as<R>();
+  WCG_TRY(c.visc.ensure((size_t)kNumViscFields * c.gcap * sizeof(R)));
+  WCG_TRY(c.viscflag.ensure((size_t)3 * c.gcap));
+  WCG_TRY(ensure_scratch(c, (size_t)c.n_active * sizeof(double) + 64));
+  double* part = c.scratch.as<double>();
+  double* dsc = c.dscalars.as<double>();
+  R* V = c.visc.as<R>();
+  unsigned char* fl = c.viscflag.as<unsigned char>();
+  const double dx = c.prm.dx;
+  const R factor = (R)(dt / (dx * dx) * c.prm.viscosity / c.prm.liquid_density);
+  const int kRmax = 40, kPq = 41, kRho0 = 42;
+  ++c.launches, k_visc_flags<R><<<nb, 192, 0, c.stream>>>(c.g, al, act, F, c.gcap, make_walls(c), fl);
+  ++c.launches, k_visc_rhs<R><<<nb, 192, 0, c.stream>>>(c.g, al, act, F, c.gcap, fl, factor, V, part);
+  ++c.launches, k_reduce_max<<<1, kRedThreads, 0, c.stream>>>(part, (int)nb, dsc + kRmax);
+  double bmax = 0;
+  WCG_TRY(fetch(c, dsc + kRmax, 1, &bmax));
+  c.stats.visc_iters = 0;
+  c.stats.visc_residual = bmax;
+  if (bmax < 1e-30) {
+    ++c.launches, k_visc_writeback<R><<<nb, 192, 0, c.stream>>>(al, c.gcap, fl, V, F, 1);
+    return cudaGetLastError();
+  }
+  const double tol = std::max(c.prm.viscosity_criterion, 1e-30) * bmax;
+  int cur = 0;
+  ++c.launches, k_visc_zdot<R><<<nb, 192, 0, c.stream>>>(al, c.gcap, fl, V, part);
+  ++c.launches, k_reduce_sum<<<1, kRedThreads, 0, c.stream>>>(part, (int)nb, dsc + kRho0);
+  double rho = 0;
+  WCG_TRY(fetch(c, dsc + kRho0, 1, &rho));
+  if (rho == 0.0 || rho != rho) {
+    c.stats.visc_converged = 0;
+    return cudaSuccess;  // the reference stops the program here
+  }
+  ++c.launches, k_visc_dir<R><<<nb, 192, 0, c.stream>>>(al, c.gcap, fl, V, dsc, kRho0, kRho0, 1);
+  bool done = false;
+  double rmax = bmax;
+  for (int it = 0; it < c.prm.maxiters && !done; ++it) {
+    ++c.launches, k_visc_apply<R><<<nb, 192, 0, c.stream>>>(c.g, al, act, F, c.gcap, fl, factor,
+                                                             V, part);
+    ++c.launches, k_reduce_sum<<<1, kRedThreads, 0, c.stream>>>(part, (int)nb, dsc + kPq);
+    ++c.launches, k_visc_update<R><<<nb, 192, 0, c.stream>>>(al, c.gcap, fl, V, dsc,
+                                                              kRho0 + cur, kPq, part);
+    ++c.launches, k_reduce_max<<<1, kRedThreads, 0, c.stream>>>(part, (int)nb, dsc + kRmax);
+    WCG_TRY(fetch(c, dsc + kRmax, 1, &rmax));
+    c.stats.visc_iters = it + 1;
+    if (rmax <= tol) {
+      done = true;
+      break;
+    }
+    const int nxt = cur ^ 1;
+    ++c.launches, k_visc_zdot<R><<<nb, 192, 0, c.stream>>>(al, c.gcap, fl, V, part);
+    ++c.launches, k_reduce_sum<<<1, kRedThreads, 0, c.stream>>>(part, (int)nb, dsc + kRho0 + nxt);
+    ++c.launches, k_visc_dir<R><<<nb, 192, 0, c.stream>>>(al, c.gcap, fl, V, dsc, kRho0 + nxt,
+                                                           kRho0 + cur, 0);
+    cur = nxt;
+  }
+  c.stats.visc_residual = rmax;
+  if (!done) c.stats.visc_converged = 0;
+  ++c.launches, k_visc_writeback<R><<<nb, 192, 0, c.stream>>>(al, c.gcap, fl, V, F, 0);
+  return cudaGetLastError();
 }
 
 template <typename R>
@@ -728,14 +803,20 @@ static cudaError_t step_velocity_t(Context& c, double dt) {
       c.g, c.active_list.as<int>(), c.gfield.as<R>(), c.gcap, (R)c.prm.gravity[0],
       (R)c.prm.gravity[1], (R)c.prm.gravity[2], (R)dt, elasto_fields<R>(c),
       c.active.as<unsigned char>(), drag_viscosity(c), c.prm.liquid_density);
-  // explicit viscosity sub-steps, then rhs = v * m (stepVelocity :272-306)
+  // viscosity sub-steps (explicit, or implicit solves), then rhs = v * m
+  // (stepVelocity :272-306)
   if (c.prm.viscosity > 0.0) {
     R* F = c.gfield.as<R>();
     const int ns = c.prm.viscosity_substeps > 0 ? c.prm.viscosity_substeps : 1;
     const double sub_dt = dt / (double)ns;
     const double dx = c.prm.dx;
     const R factor = (R)(sub_dt / (dx * dx) * c.prm.viscosity / c.prm.liquid_density);
+    c.stats.visc_converged = 1;
     for (int it = 0; it < ns; ++it) {
+      if (c.prm.viscosity_implicit) {
+        WCG_TRY(viscosity_implicit_t<R>(c, sub_dt));
+        continue;
+      }
       WCG_TRY(cudaMemcpyAsync(F + G_UTMP * c.gcap, F + G_VSTAR * c.gcap,
                               3 * c.gcap * sizeof(R), cudaMemcpyDeviceToDevice, c.stream));
       ++c.launches, k_viscosity_explicit<R><<<(unsigned)c.n_active, 192, 0, c.stream>>>(

@@ -42,6 +42,8 @@ def make_params(p, precision=_capi.WCG_FP64, refine_inner_tol=0.0,
     prm.elasto_flip_asym_coeff = getattr(p, "elasto_flip_asym_coeff", 1.0)
     prm.elasto_advect_coeff = getattr(p, "elasto_advect_coeff", 1.0)
     prm.drag_viscosity = getattr(p, "drag_viscosity", 8.9e-3)
+    prm.viscosity_implicit = 1 if getattr(p, "viscosity_implicit", False) else 0
+    prm.viscosity_criterion = getattr(p, "viscosity_criterion", 1e-6)
     prm.correction_strength = getattr(p, "correction_strength", 0.0)
     prm.correction_step = getattr(p, "correction_step", 8)
     prm.correction_multiplier = getattr(p, "correction_multiplier", 2.0)

@@ -135,9 +135,10 @@ def test_implicit_viscosity_fp64(kind, mu, ns, wcg):
 
 
 def test_implicit_viscosity_steps_and_fp32(wcg):
-    """Whole steps with the implicit viscosity converge in both precisions;
-    FP32 (criterion 1e-5) agrees with the FP64 oracle to 1e-4 on faces with
-    liquid volume."""
+    """FP32 (criterion 1e-5): the velocities solve the oracle's FP64 system to
+    2e-5 of its rhs (the solution itself is only as determined as the
+    ill-conditioned system and the criterion allow); whole steps with the
+    implicit viscosity converge in both precisions."""
     sc = _implicit("curl16", 2.0, 1, 1e-5)
     o = oo.OracleScene(sc)
     o.step(DT, snapshot=True)
@@ -145,13 +146,14 @@ def test_implicit_viscosity_steps_and_fp32(wcg):
     g.rebucketize_and_resample()
     g.map_particle_nodes()
     g.step_velocity(DT)
-    errs, scale = [], 0.0
-    for a, c in enumerate("xyz"):
-        m = np.nan_to_num(o.get("liquid_" + "uvw"[a] + "_vf"), nan=0.0) > 0.0
-        ov = o.get("v_star_" + c)
-        errs.append(np.abs(g.field("v_star_" + c)[m] - ov[m]).max())
-        scale = max(scale, np.abs(ov[m]).max())
-    assert max(errs) <= 1e-4 * scale, errs
+    vs = [g.field("v_star_" + c) for c in "xyz"]
+    rs, ci, va, b = o.get("V_rowstart"), o.get("V_col"), o.get("V_val"), o.get("V_rhs")
+    face = o.get("V_face")
+    nn = vs[0].size
+    x = np.array([vs[f // nn][f % nn] for f in face])
+    import scipy.sparse as sps
+    A = sps.csr_matrix((va, ci, rs), shape=(rs.size - 1, rs.size - 1))
+    assert np.abs(b - A @ x).max() <= 2e-5 * np.abs(b).max()
     g.close()
     for prec in (_capi.WCG_FP64, _capi.WCG_FP32_REFINE):
         g = FluidScene(_implicit("dam16", 0.5, 2, 1e-6), precision=prec)
