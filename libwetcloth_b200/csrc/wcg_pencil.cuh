@@ -47,6 +47,9 @@ constexpr int kPatch = 16;                    // lines per patch edge
 constexpr int kPatchLines = kPatch * kPatch;  // threads of a sweep CTA
 constexpr int kPre = 4;                       // rows of edge words prefetched ahead
 constexpr int kPlBlocks = 592;                // streaming kernels: 4 x 148 SMs
+// the fused SpMV in FP32 (32 registers): 8 resident CTAs per SM, so twice the
+// loads in flight of the other streaming kernels
+constexpr int kPlSpmvBlocks32 = 1184;
 static_assert(kRedThreads == kPatchLines, "streaming kernels walk one row per block");
 
 __host__ __device__ inline long long pl_index(const PencilGeom& G, long long p, int t, int l) {
@@ -678,7 +681,7 @@ __device__ inline PlNbr pl_nbr(const PencilGeom& G, const PlCell& c, long long e
 // The previous iteration's x += alpha s_old is applied here too (alpha is
 // still the previous iteration's when this kernel runs; 0 before the first).
 template <typename R>
-__global__ void __launch_bounds__(kRedThreads)
+__global__ void __launch_bounds__(kRedThreads, sizeof(R) == 4 ? 8 : 4)
     k_pl_spmv_s(PencilGeom G, const R* __restrict__ AD, const R* __restrict__ AS,
                 const R* __restrict__ AA, const R* __restrict__ AC, const R* __restrict__ z,
                 const R* __restrict__ sold, R* __restrict__ snew, R* __restrict__ q,

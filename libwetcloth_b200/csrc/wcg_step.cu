@@ -1132,7 +1132,8 @@ static cudaError_t pl_setup(Context& c, const int* lo, const int* hi) {
     // tags of a fresh buffer must not match any epoch (epochs start at 1)
     WCG_TRY(cudaMemsetAsync(c.pl_edge.p, 0, c.pl_edge.bytes, c.stream));
   }
-  WCG_TRY(c.pl_part.ensure((size_t)std::max<long long>(G.npatch, kPlBlocks) * sizeof(double)));
+  WCG_TRY(c.pl_part.ensure(
+      (size_t)std::max<long long>(G.npatch, std::max(kPlBlocks, kPlSpmvBlocks32)) * sizeof(double)));
   if (!same_shape || c.pl_order_h.size() != (size_t)G.npatch) {
     // patches in wave order PAi + PCi
     c.pl_order_h.resize(G.npatch);
@@ -1300,13 +1301,14 @@ static cudaError_t pl_pcg(Context& c, R* r, R* x, double tol_abs, int maxiters, 
   const R* AS = pl_field<R>(c, PL_AS);
   const R* AA = pl_field<R>(c, PL_AA);
   const R* AC = pl_field<R>(c, PL_AC);
+  const int spmv_blocks = sizeof(R) == 4 ? kPlSpmvBlocks32 : kPlBlocks;
   for (;;) {
     for (int b = 0; b < kPcgBatch; ++b) {
       {
         ProfScope prof(c, P_PCGVEC);
-        ++c.launches, k_pl_spmv_s<R><<<kPlBlocks, kRedThreads, 0, c.stream>>>(
+        ++c.launches, k_pl_spmv_s<R><<<spmv_blocks, kRedThreads, 0, c.stream>>>(
             G, AD, AS, AA, AC, z, sold, snew, q, x, sc, part);
-        ++c.launches, k_red_alpha<<<1, kRedThreads, 0, c.stream>>>(part, kPlBlocks, sc);
+        ++c.launches, k_red_alpha<<<1, kRedThreads, 0, c.stream>>>(part, spmv_blocks, sc);
       }
       WCG_TRY((pl_sweep<R, kForward, true>(c, fa)));
       {
