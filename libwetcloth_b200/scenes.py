@@ -256,6 +256,26 @@ def dam_break(n_cells: int = 64, ppc: int = 8, seed: int = 0,
                  name=f"dam_break_{n_cells}^3_{ppc}ppc")
 
 
+def fine_volume(dx: float, cell_multiplier: float = 0.3535533906) -> float:
+    """V_fine of relabelLiquidParticles (TwoDScene.cpp:2484-2489): the
+    volume of a sphere of radius dx * cell_multiplier / sqrt(3)."""
+    r = 1.0 / np.sqrt(3.0) * dx * cell_multiplier
+    return 4.0 / 3.0 * np.pi * r * r * r
+
+
+def mixed_volumes(sc: Scene, seed: int = 0, mrel=(0.3, 0.7, 1.0, 1.5, 2.5)) -> Scene:
+    """The scene with every liquid particle's volume set to V_fine times a
+    seeded choice from mrel (radius and mass to match), so that the merge and
+    split classes S, s, o, l and L all occur."""
+    rng = np.random.default_rng(seed)
+    vf = fine_volume(sc.params.dx)
+    vol = vf * rng.choice(np.asarray(mrel, dtype=np.float64), size=sc.x.shape[0])
+    sc.vol = vol
+    sc.mass = vol * sc.params.liquid_density
+    sc.radius = np.cbrt(vol * 0.75 / np.pi)
+    return sc
+
+
 def half_box(n_cells: int = 256, ppc: int = 2, seed: int = 1,
              amplitude: float = 0.5, sigma_cells: float = 4.0) -> Scene:
     """Half-filled unit box (y < 0.5) at ppc particles per cell with a random

@@ -44,6 +44,8 @@ def lib():
                                          ctypes.c_double, ctypes.c_uint64]
         L.wco_set_correction_selector.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.wco_correct_liquid.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
+        L.wco_merge_liquid.argtypes = [ctypes.c_void_p, ctypes.c_int, _I, _I, _I]
+        L.wco_merge_liquid.restype = ctypes.c_int
         L.wco_correction_selector.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int]
         L.wco_correction_selector.restype = ctypes.c_int
         L.wco_step.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
@@ -141,6 +143,14 @@ class OracleScene:
         """Grid, P2G, then G2P from the P2G velocities and advection (no
         solve); snapshots as in a step."""
         self.L.wco_transfer(self.h, dt)
+
+    def merge(self, selector, perm):
+        """mergeLiquidParticles with the given subset and colour permutations
+        (perm: 9 ints, t then s then r); returns the particles removed."""
+        pm = np.ascontiguousarray(perm, dtype=np.int32).reshape(3, 3)
+        rows = [np.ascontiguousarray(pm[k]) for k in range(3)]
+        ip = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+        return self.L.wco_merge_liquid(self.h, int(selector), ip(rows[0]), ip(rows[1]), ip(rows[2]))
 
     def set_correction_selector(self, selector):
         """Particle subset (fluid index % step) of the next correction."""

@@ -57,6 +57,8 @@ def _lib(omp: bool):
         L.wcref_transfer.argtypes = [ctypes.c_void_p, ctypes.c_double]
         L.wcref_set_correction.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int,
                                            ctypes.c_double, ctypes.c_uint]
+        L.wcref_merge.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_int]
+        L.wcref_merge.restype = ctypes.c_int
         _libs[omp] = L
     return _libs[omp]
 
@@ -132,6 +134,11 @@ class RefScene:
 
     def step(self, dt: float, snapshot: bool = True) -> int:
         return self.L.wcref_step(self.h, dt, 1 if snapshot else 0)
+
+    def merge(self, seed: int, step: int) -> int:
+        """updateOptiVolume + mergeLiquidParticles after srand(seed); returns
+        the particles removed (draws in "merge_selector", "merge_perm")."""
+        return self.L.wcref_merge(self.h, seed, step)
 
     def transfer(self, dt: float) -> None:
         """Grid, P2G, then G2P from the P2G velocities and advection (no

@@ -685,6 +685,47 @@ void wcref_set_viscosity(void* hp, double mu, int substeps) {
   h->stepper->setUseApic(true);
 }
 
+// TwoDScene::updateOptiVolume and mergeLiquidParticles, as
+// WetClothCore::stepSystem runs them before a step's grid build (the bucket
+// lists are the last step's), with LiquidInfo correction_step = step.
+// srand(seed) fixes the merge's rand() draws (the subset selector, then three
+// Fisher-Yates colour permutations), which are replayed and recorded
+// ("merge_selector", "merge_perm" t, s, r).  Returns the particles removed.
+int wcref_merge(void* hp, unsigned seed, int step) {
+  Harness* h = (Harness*)hp;
+  TwoDScene& s = *h->scene;
+  s.getLiquidInfo().correction_step = step > 0 ? step : 1;
+  s.updateOptiVolume();
+  srand(seed);
+  const int sel = rand() % s.getLiquidInfo().correction_step;
+  std::vector<int> pt, ps, pr;
+  mathutils::fisherYates(3, pt);
+  mathutils::fisherYates(3, ps);
+  mathutils::fisherYates(3, pr);
+  srand(seed);
+  const int before = s.getNumParticles();
+  s.mergeLiquidParticles();
+  h->ii["merge_selector"] = {sel};
+  h->ii["merge_perm"] = {pt[0], pt[1], pt[2], ps[0], ps[1], ps[2], pr[0], pr[1], pr[2]};
+  snap_particles(*h, "merge_");
+  const int np = s.getNumParticles();
+  std::vector<double>& vol = h->f["merge_vol"];
+  std::vector<double>& mass = h->f["merge_mass"];
+  std::vector<double>& rad = h->f["merge_radius"];
+  std::vector<long long>& cls = h->ii["merge_class"];
+  vol.assign(np, 0.0);
+  mass.assign(np, 0.0);
+  rad.assign(np, 0.0);
+  cls.assign(np, 0);
+  for (int i = 0; i < np; ++i) {
+    vol[i] = s.m_fluid_vol(i);
+    mass[i] = s.m_fluid_m(i * 4);
+    rad[i] = s.m_radius(i * 2);
+    cls[i] = (long long)s.m_classifier[i];
+  }
+  return before - np;
+}
+
 // implicit liquid viscosity: LiquidInfo::compute_viscosity and
 // implicit_viscosity on, viscosity mu, the stepper's viscosity sub-steps and
 // viscous criterion (call before the first step)

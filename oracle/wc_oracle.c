@@ -36,6 +36,7 @@ typedef struct {
    * correction_step, correction_multiplier */
   double corr_strength, corr_mult;
   int corr_step;
+  double cell_mult; /* LiquidInfo::particle_cell_multiplier */
 } Params;
 
 typedef struct {
@@ -98,6 +99,7 @@ typedef struct {
   double* xw;  /* positions the sub-step's stencil weights were taken at (x3) */
   uint64_t corr_seed, corr_count; /* selector stream of the particle correction */
   int corr_sel_once;              /* >= 0: selector of the next correction */
+  unsigned char* cls;             /* m_classifier of the liquid particles */
   Snap snaps[256];
   int nsnaps;
 } Scene;
@@ -1767,6 +1769,224 @@ static void correct_liquid(Scene* s, double dt, int selector) {
   free(key);
 }
 
+static void snap_particles(Scene* s, const char* tag);
+
+/* particle classes of relabelLiquidParticles (TwoDScene.h:31) */
+enum { PCL_NONE = 0, PCL_S, PCL_s, PCL_o, PCL_l, PCL_L };
+
+/* V_fine of relabelLiquidParticles / mergeLiquidParticles
+ * (TwoDScene.cpp:2484-2489, 2518-2520) */
+static double fine_volume(const Scene* s) {
+  const double rad_fine = 1.0 / sqrt(3.0) * s->p.dx * s->p.cell_mult;
+  return 4.0 / 3.0 * M_PI * rad_fine * rad_fine * rad_fine;
+}
+
+/* TwoDScene::relabelLiquidParticles (TwoDScene.cpp:2484-2505) */
+static void relabel(Scene* s) {
+  const double vf = fine_volume(s);
+  free(s->cls);
+  s->cls = (unsigned char*)calloc((size_t)(s->np > 0 ? s->np : 1), 1);
+  for (int p = s->ne; p < s->np; ++p) {
+    const double mrel = s->vol[p] / vf;
+    s->cls[p] = mrel < 0.5 ? PCL_S : mrel <= 0.9 ? PCL_s : mrel <= 1.1 ? PCL_o
+              : mrel <= 2.0 ? PCL_l : PCL_L;
+  }
+}
+
+static void swap_d(double* a, int i, int j, int w) {
+  for (int k = 0; k < w; ++k) {
+    const double t = a[i * w + k];
+    a[i * w + k] = a[j * w + k];
+    a[j * w + k] = t;
+  }
+}
+
+/* TwoDScene::removeEmptyParticles (TwoDScene.cpp:1713-1745): a liquid
+ * particle with fluid volume below 1e-20 is swapped with the last one and
+ * the count shrinks (swapParticles :176-208 on the liquid attributes) */
+static int remove_empty(Scene* s) {
+  int n = s->np;
+  for (int i = s->ne; i < n;) {
+    if (s->vol[i] < 1e-20) {
+      --n;
+      swap_d(s->x, i, n, 3);
+      swap_d(s->v, i, n, 3);
+      swap_d(s->C, i, n, 9);
+      swap_d(s->m, i, n, 1);
+      swap_d(s->vol, i, n, 1);
+      swap_d(s->rad, i, n, 1);
+      const unsigned char t = s->cls[i];
+      s->cls[i] = s->cls[n];
+      s->cls[n] = t;
+    } else {
+      ++i;
+    }
+  }
+  const int removed = s->np - n;
+  s->np = n;
+  return removed;
+}
+
+/* TwoDScene::mergeLiquidParticles (TwoDScene.cpp:2510-2666) after
+ * updateOptiVolume's relabelling: the small (S) and the large-ish (l) liquid
+ * particles of the subset index % step == selector, visited bucket by bucket
+ * in the 27 colours of Sorter::for_each_bucket_particles_colored_randomized
+ * (Sorter.h:439-480, numcolors 3, colour order perm_t x perm_s x perm_r), hand
+ * their volume (S: all of it, then they are removed; l: the part above V_fine,
+ * then they shrink to V_fine) and the matching momentum in equal parts to the
+ * neighbours within 2 r_fine in the 27 buckets around (S: to S, s and o
+ * particles; l: to s particles) holding no more than V_fine; then every
+ * particle that gathered volume takes the volume-weighted mean velocity and
+ * the radius of its new volume, empty particles are removed and all are
+ * relabelled.  The bucket lists are those of the last grid build (the
+ * reference merges before the step's rebucketizeParticles).  The reference
+ * draws the selector and the three colour permutations with rand(); here
+ * they are arguments. */
+int wco_merge_liquid(Scene* s, int selector, const int* perm_t, const int* perm_s,
+                     const int* perm_r) {
+  if (!s->keys || s->np == s->ne) return 0;
+  relabel(s);
+  const double vf = fine_volume(s);
+  const double rad_fine = 1.0 / sqrt(3.0) * s->p.dx * s->p.cell_mult;
+  const double should_rad = rad_fine * 2.0;
+  const int step = s->p.corr_step > 0 ? s->p.corr_step : 1;
+  const int np = s->np;
+  unsigned char* removed = (unsigned char*)calloc((size_t)np, 1);
+  double* gvol = (double*)calloc((size_t)np, sizeof(double));
+  double* gmom = (double*)calloc((size_t)np * 3, sizeof(double));
+  const int nc = 3;
+  const int sn[3] = {(s->ni + nc - 1) / nc, (s->nj + nc - 1) / nc, (s->nk + nc - 1) / nc};
+  for (int a = 0; a < nc; ++a)
+    for (int b = 0; b < nc; ++b)
+      for (int c = 0; c < nc; ++c) {
+        const int t = perm_t[a], u = perm_s[b], r = perm_r[c];
+        for (long long sb = 0; sb < (long long)sn[0] * sn[1] * sn[2]; ++sb) {
+          const int sk = (int)(sb / ((long long)sn[0] * sn[1]));
+          const int sj = (int)((sb - (long long)sk * sn[0] * sn[1]) / sn[0]);
+          const int si = (int)(sb - (long long)sk * sn[0] * sn[1] - (long long)sj * sn[0]);
+          const int k = sk * nc + t, j = sj * nc + u, i = si * nc + r;
+          if (k >= s->nk || j >= s->nj || i >= s->ni) continue;
+          const long long bkt = bucket_index(s, i, j, k);
+          for (int q = s->sup[bkt * 2]; q < s->sup[bkt * 2 + 1]; ++q) {
+            const int p = (int)(s->keys[q] & 0xffffffffu);
+            if (p < s->ne || (s->cls[p] != PCL_S && s->cls[p] != PCL_l)) continue;
+            if (p % step != selector) continue;
+            const int small = s->cls[p] == PCL_S;
+            const double full_vol = s->vol[p] + gvol[p];
+            if (!small && full_vol < 1e-20) continue;
+            const double mrel = full_vol / vf;
+            if (small && mrel >= 0.5) {
+              s->cls[p] = PCL_s;
+              continue;
+            }
+            if (!small && mrel > 2.0) {
+              s->cls[p] = PCL_L;
+              continue;
+            }
+            /* partners in the 27 buckets around, x outermost (Sorter.h:352-371);
+             * counted first, then served, both with the same test */
+            int npart = 0;
+            for (int pass = 0; pass < 2; ++pass) {
+              double dvol = 0.0, dmom[3] = {0.0, 0.0, 0.0};
+              if (pass == 1) {
+                if (npart == 0) break;
+                const double invN = 1.0 / (double)npart;
+                if (small) {
+                  dvol = full_vol * invN;
+                  for (int a2 = 0; a2 < 3; ++a2)
+                    dmom[a2] = (s->v[p * 3 + a2] * s->vol[p] + gmom[p * 3 + a2]) * invN;
+                } else {
+                  const double ex_vol = full_vol - vf;
+                  dvol = ex_vol * invN;
+                  const double coeff = dvol / full_vol;
+                  for (int a2 = 0; a2 < 3; ++a2)
+                    dmom[a2] = (s->v[p * 3 + a2] * s->vol[p] + gmom[p * 3 + a2]) * coeff;
+                }
+              }
+              for (int x = i - 1; x <= i + 1; ++x)
+                for (int y = j - 1; y <= j + 1; ++y)
+                  for (int z = k - 1; z <= k + 1; ++z) {
+                    if (x < 0 || x > s->ni - 1 || y < 0 || y > s->nj - 1 || z < 0 ||
+                        z > s->nk - 1)
+                      continue;
+                    const long long nb = bucket_index(s, x, y, z);
+                    for (int q2 = s->sup[nb * 2]; q2 < s->sup[nb * 2 + 1]; ++q2) {
+                      const int n = (int)(s->keys[q2] & 0xffffffffu);
+                      if (n == p || n < s->ne || removed[n]) continue;
+                      const int c2 = s->cls[n];
+                      if (small ? !(c2 == PCL_S || c2 == PCL_s || c2 == PCL_o) : c2 != PCL_s)
+                        continue;
+                      const double neigh_vol = s->vol[n] + gvol[n];
+                      if (neigh_vol > vf) continue;
+                      const double d[3] = {s->x[p * 3] - s->x[n * 3], s->x[p * 3 + 1] - s->x[n * 3 + 1],
+                                           s->x[p * 3 + 2] - s->x[n * 3 + 2]};
+                      const double dist = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+                      if (!(dist < should_rad)) continue;
+                      if (pass == 0) {
+                        ++npart;
+                      } else {
+                        gvol[n] += dvol;
+                        for (int a2 = 0; a2 < 3; ++a2) gmom[n * 3 + a2] += dmom[a2];
+                      }
+                    }
+                  }
+            }
+            if (npart == 0) continue;
+            if (small) {
+              removed[p] = 1;
+              s->vol[p] = 0.0;
+              gvol[p] = 0.0;
+              for (int a2 = 0; a2 < 3; ++a2) gmom[p * 3 + a2] = 0.0;
+            } else {
+              const double scaling = vf / full_vol;
+              const double rad_scaling = pow(scaling, 1.0 / 3.0);
+              s->vol[p] *= scaling;
+              s->m[p] *= scaling;
+              s->rad[p] *= rad_scaling;
+              s->cls[p] = PCL_o;
+            }
+          }
+        }
+      }
+  /* gather and update (:2649-2666) */
+  for (int p = s->ne; p < np; ++p) {
+    if (removed[p] || gvol[p] == 0.0) continue;
+    double fm[3];
+    for (int a2 = 0; a2 < 3; ++a2) fm[a2] = s->v[p * 3 + a2] * s->vol[p] + gmom[p * 3 + a2];
+    const double full_vol = s->vol[p] + gvol[p];
+    const double full_rad = pow(full_vol * 0.75 / M_PI, 1.0 / 3.0);
+    const double inv = 1.0 / full_vol;
+    s->vol[p] = full_vol;
+    for (int a2 = 0; a2 < 3; ++a2) s->v[p * 3 + a2] = fm[a2] * inv;
+    s->m[p] = full_vol * s->p.rho;
+    s->rad[p] = full_rad;
+  }
+  free(removed);
+  free(gvol);
+  free(gmom);
+  const int nrem = remove_empty(s);
+  relabel(s);
+  {
+    const int n = s->np;
+    double* t = (double*)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+    long long* c = (long long*)malloc(sizeof(long long) * (size_t)(n > 0 ? n : 1));
+    snap_particles(s, "merge_");
+    memcpy(t, s->vol, sizeof(double) * (size_t)n);
+    snap_put_f(s, "merge_vol", t, n);
+    memcpy(t, s->m, sizeof(double) * (size_t)n);
+    snap_put_f(s, "merge_mass", t, n);
+    memcpy(t, s->rad, sizeof(double) * (size_t)n);
+    snap_put_f(s, "merge_radius", t, n);
+    for (int p = 0; p < n; ++p) c[p] = s->cls[p];
+    snap_put_i(s, "merge_class", c, n);
+    free(t);
+    free(c);
+  }
+  free(s->keys);
+  s->keys = NULL;  /* the bucket lists no longer match the particles */
+  return nrem;
+}
+
 /* correctLiquidParticles with an explicit particle subset, outside a step */
 void wco_correct_liquid(Scene* s, double dt, int selector) { correct_liquid(s, dt, selector); }
 
@@ -2114,6 +2334,7 @@ Scene* wco_create(double dx, const double* g, double rho, double flip, double fr
   s->p.corr_step = 8;
   s->p.corr_mult = 2.0;
   s->p.visc_criterion = 1e-6;
+  s->p.cell_mult = 0.3535533906;
   s->corr_sel_once = -1;
   s->bs = dx * 4.0;
   s->np = np;
@@ -2212,7 +2433,8 @@ void wco_destroy(Scene* s) {
                   s->pv.start, s->pv.pid, s->pv.slot, s->pw.start, s->pw.pid, s->pw.slot,
                   s->pp.start, s->pp.pid, s->pp.slot, s->sat_p, s->psi_p, s->pore_p, s->lphi,
                   s->sphi, s->pressure, s->dofidx, s->rowstart, s->col, s->val, s->b, s->xw,
-                  s->vf_c, s->vf_e[0], s->vf_e[1], s->vf_e[2], s->vf_f[0], s->vf_f[1], s->vf_f[2]};
+                  s->vf_c, s->vf_e[0], s->vf_e[1], s->vf_e[2], s->vf_f[0], s->vf_f[1], s->vf_f[2],
+                  s->cls};
   for (size_t k = 0; k < sizeof(ptrs) / sizeof(ptrs[0]); ++k) free(ptrs[k]);
   for (int a = 0; a < 3; ++a) {
     void* q[] = {s->mass[a], s->vel[a], s->vol_f[a], s->sat[a], s->psi[a], s->wgt[a], s->svel[a],

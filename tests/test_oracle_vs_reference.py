@@ -297,3 +297,30 @@ def test_implicit_viscosity(kind, mu, ns):
         errs.append(np.abs(a[m] - b[m]).max())
         scale = max(scale, np.abs(a[m]).max())
     assert max(errs) <= 1e-8 * scale, errs
+
+
+@pytest.mark.parametrize("kind,seed", [("dam16", 3), ("curl16", 5), ("fall", 8)])
+def test_particle_merge(kind, seed):
+    """updateOptiVolume + mergeLiquidParticles (TwoDScene.cpp:2484-2666) and
+    removeEmptyParticles (:1713) after a step, on particles of mixed volume
+    (classes S, s, o, l, L): the reference draws its subset and colour order
+    with rand() after srand(seed); the oracle is handed the same draws.  Same
+    particles removed, the same order after the swap-with-last removal, the
+    same classes; positions, velocities, volumes, masses and radii to 1e-12."""
+    sc = _fall() if kind == "fall" else _scene(kind)
+    scenes.mixed_volumes(sc, seed)
+    r = oref.RefScene(sc, mic=True)
+    o = oo.OracleScene(sc)
+    r.step(DT, snapshot=True)
+    o.step(DT, snapshot=True)
+    nr = r.merge(seed, 8)
+    sel = int(r.get("merge_selector")[0])
+    perm = r.get("merge_perm")
+    assert sorted(perm[:3]) == [0, 1, 2] and sorted(perm[6:]) == [0, 1, 2]
+    assert nr > 0
+    assert o.merge(sel, perm) == nr
+    assert np.array_equal(r.get("merge_class"), o.get("merge_class"))
+    for k in ("merge_x", "merge_v", "merge_C", "merge_vol", "merge_mass", "merge_radius"):
+        a, b = r.get(k), o.get(k)
+        assert a.shape == b.shape, k
+        assert np.abs(a - b).max() <= 1e-12 * np.abs(a).max(), k
