@@ -83,6 +83,13 @@ typedef struct wcg_params {
                                       preconditioned by its diagonal */
   double viscosity_criterion;      /* LinearizedImplicitEuler::m_viscous_criterion (1e-6):
                                       ||r||_inf <= criterion ||b||_inf */
+  int particle_merge;              /* relabelLiquidParticles + mergeLiquidParticles +
+                                      removeEmptyParticles before each sub-step
+                                      (WetClothCore.cpp:97-110); the subset uses
+                                      correction_step, as in the reference */
+  unsigned long long merge_seed;   /* seed of the merge's draws (rand() in the reference) */
+  double particle_cell_multiplier; /* LiquidInfo::particle_cell_multiplier (0.3535533906):
+                                      V_fine = 4/3 pi (dx m / sqrt 3)^3 */
 } wcg_params;
 
 typedef struct wcg_ctx wcg_ctx;
@@ -197,6 +204,19 @@ int wcg_correct_liquid_particles(wcg_ctx* ctx, double dt, int selector);
 /* the subset wcg_substep corrects in its k-th call: SplitMix64 of the seed and
  * k, modulo step */
 int wcg_correction_selector(unsigned long long seed, unsigned long long k, int step);
+/* TwoDScene::updateOptiVolume (relabelLiquidParticles TwoDScene.cpp:2484-2505),
+ * mergeLiquidParticles (:2510-2666) and removeEmptyParticles (:1713-1745) on
+ * the buckets of the last grid build, for the liquid particles with index %
+ * correction_step == selector, colours in the order perm9 (three permutations
+ * of {0, 1, 2}: z, y, x parities), as the reference draws them with rand().
+ * Removed particles leave the arrays with the reference's swap-with-last
+ * renumbering; *removed (may be NULL) receives their count. */
+int wcg_merge_liquid_particles(wcg_ctx* ctx, int selector, const int* perm9,
+                               long long* removed);
+/* the draws wcg_substep uses for its k-th merge: SplitMix64 of the seed and k
+ * for the selector, then three Fisher-Yates permutations of {0, 1, 2} */
+int wcg_merge_draws(unsigned long long seed, unsigned long long k, int step, int* selector,
+                    int* perm9);
 /* TwoDScene::mapNodeParticlesAPIC (TwoDScene.cpp:6936) */
 int wcg_map_node_particles(wcg_ctx* ctx);
 /* SceneStepper::advectScene (SceneStepper.cpp:17) followed by

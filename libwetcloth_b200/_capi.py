@@ -59,6 +59,9 @@ class WcgParams(ctypes.Structure):
         ("correction_seed", ctypes.c_ulonglong),
         ("viscosity_implicit", ctypes.c_int),
         ("viscosity_criterion", ctypes.c_double),
+        ("particle_merge", ctypes.c_int),
+        ("merge_seed", ctypes.c_ulonglong),
+        ("particle_cell_multiplier", ctypes.c_double),
     ]
 
 
@@ -113,6 +116,11 @@ SIGNATURES = {
     "wcg_apply_pressure_drag_fluid": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "wcg_constrain_liquid_velocity": (ctypes.c_int, [ctypes.c_void_p]),
     "wcg_map_node_particles": (ctypes.c_int, [ctypes.c_void_p]),
+    "wcg_merge_liquid_particles": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
+                                                  ctypes.POINTER(ctypes.c_int),
+                                                  ctypes.POINTER(ctypes.c_longlong)]),
+    "wcg_merge_draws": (ctypes.c_int, [ctypes.c_ulonglong, ctypes.c_ulonglong, ctypes.c_int,
+                                       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     "wcg_correct_liquid_particles": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]),
     "wcg_correction_selector": (ctypes.c_int, [ctypes.c_ulonglong, ctypes.c_ulonglong, ctypes.c_int]),
     "wcg_advect": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),

@@ -194,6 +194,9 @@ void wcg_default_params(wcg_params* p) {
   p->correction_seed = 0;
   p->viscosity_implicit = 0;
   p->viscosity_criterion = 1e-6;
+  p->particle_merge = 0;
+  p->merge_seed = 0;
+  p->particle_cell_multiplier = 0.3535533906;
 }
 
 int wcg_create(const wcg_params* params, wcg_ctx** out) {
@@ -211,6 +214,8 @@ int wcg_create(const wcg_params* params, wcg_ctx** out) {
     return fail(WCG_ERR_ARG, "elasto coefficients must be finite");
   if (!(params->drag_viscosity > 0.0) || !std::isfinite(params->drag_viscosity))
     return fail(WCG_ERR_ARG, "drag_viscosity must be finite and > 0");
+  if (!(params->particle_cell_multiplier > 0.0) || !std::isfinite(params->particle_cell_multiplier))
+    return fail(WCG_ERR_ARG, "particle_cell_multiplier must be finite and > 0");
   if (!(params->viscosity_criterion > 0.0) || !std::isfinite(params->viscosity_criterion))
     return fail(WCG_ERR_ARG, "viscosity_criterion must be finite and > 0");
   if (!(params->correction_strength >= 0.0) || !std::isfinite(params->correction_strength) ||
@@ -251,6 +256,9 @@ int wcg_create(const wcg_params* params, wcg_ctx** out) {
   p.correction_multiplier = params->correction_multiplier;
   p.correction_seed = params->correction_seed;
   p.viscosity_implicit = params->viscosity_implicit ? 1 : 0;
+  p.particle_merge = params->particle_merge ? 1 : 0;
+  p.merge_seed = params->merge_seed;
+  p.cell_multiplier = params->particle_cell_multiplier;
   p.viscosity_criterion = params->viscosity_criterion;
   // wavefront tile shape (performance knob; both compute identical results)
   if (const char* v = getenv("WCG_SWEEP_TILE")) ctx->c.sweep_variant = !strcmp(v, "warp") ? 1 : 0;
@@ -524,6 +532,35 @@ int wcg_correct_liquid_particles(wcg_ctx* ctx, double dt, int selector) {
     return fail(WCG_ERR_ARG, "selector must lie in [0, correction_step)");
   WCG_CALL(ctx, wcg::correct_liquid_particles(ctx->c, dt, selector), "correctLiquidParticles");
   return device_status(ctx->c, "correctLiquidParticles");
+}
+
+static bool valid_perm3(const int* p) {
+  return p[0] >= 0 && p[0] < 3 && p[1] >= 0 && p[1] < 3 && p[2] >= 0 && p[2] < 3 &&
+         p[0] != p[1] && p[0] != p[2] && p[1] != p[2];
+}
+
+int wcg_merge_liquid_particles(wcg_ctx* ctx, int selector, const int* perm9,
+                               long long* removed) {
+  WCG_CHECK_CTX(ctx);
+  if (!perm9) return fail(WCG_ERR_ARG, "null colour permutation");
+  if (selector < 0 || selector >= ctx->c.prm.correction_step)
+    return fail(WCG_ERR_ARG, "selector must lie in [0, correction_step)");
+  for (int q = 0; q < 3; ++q)
+    if (!valid_perm3(perm9 + 3 * q))
+      return fail(WCG_ERR_ARG, "perm9 must hold three permutations of {0, 1, 2}");
+  if (ctx->c.g.nb == 0) return fail(WCG_ERR_STATE, "no grid build to take the buckets from");
+  long long rem = 0;
+  WCG_CALL(ctx, wcg::merge_liquid_particles(ctx->c, selector, perm9, &rem),
+           "mergeLiquidParticles");
+  if (removed) *removed = rem;
+  return device_status(ctx->c, "mergeLiquidParticles");
+}
+
+int wcg_merge_draws(unsigned long long seed, unsigned long long k, int step, int* selector,
+                    int* perm9) {
+  if (!selector || !perm9 || step < 1) return fail(WCG_ERR_ARG, "bad merge draw arguments");
+  wcg::merge_draws(seed, k, step, selector, perm9);
+  return WCG_OK;
 }
 
 int wcg_correction_selector(unsigned long long seed, unsigned long long k, int step) {

@@ -41,6 +41,9 @@ struct Params {
   int correction_step;           // LiquidInfo::correction_step
   double correction_multiplier;  // LiquidInfo::correction_multiplier
   unsigned long long correction_seed;  // seed of the per-sub-step subset stream
+  int particle_merge;            // relabel + mergeLiquidParticles before each sub-step
+  unsigned long long merge_seed; // seed of the merge's draws
+  double cell_multiplier;        // LiquidInfo::particle_cell_multiplier (V_fine)
 };
 
 // A device allocation that grows and never shrinks.
@@ -245,6 +248,11 @@ struct Context {
   bool xw_valid = false;
   DevBuf corr_start, corr_cursor, corr_list;
   unsigned long long corr_count = 0;
+  // particle merge (wcg_merge.cuh): classes, flags, gathered volume and
+  // momentum, index maps; the merge's draw counter
+  DevBuf mwork;
+  unsigned long long merge_count = 0;
+  long long merged_removed = 0;  // particles the last merge removed
 
   // reverse mode of a sub-step (wcg_adjoint.cuh): grid cotangents, particle
   // cotangents (sorted order), the first extrapolation layer's input mask,
@@ -344,6 +352,13 @@ cudaError_t substep(Context& c, double dt);
 cudaError_t correct_liquid_particles(Context& c, double dt, int selector);
 // subset of call k of the seeded correction stream
 int correction_selector(unsigned long long seed, unsigned long long k, int step);
+// relabelLiquidParticles + mergeLiquidParticles + removeEmptyParticles on the
+// buckets of the last grid build, with the given subset and colour order
+// (perm: t, s, r permutations of {0, 1, 2}); *removed = particles removed
+cudaError_t merge_liquid_particles(Context& c, int selector, const int* perm, long long* removed);
+// draws of merge call k of a seeded stream: selector, then three Fisher-Yates
+// permutations of {0, 1, 2}
+void merge_draws(unsigned long long seed, unsigned long long k, int step, int* selector, int* perm);
 // Reverse mode of substep at the current (pre-step) particle state with the
 // positions held fixed: cotangents of (v', C', x') in, of (v, C) and of the
 // viscosity (mubar, may be null) out (host arrays, original order; x-bar

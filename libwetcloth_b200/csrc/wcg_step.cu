@@ -17,6 +17,7 @@
 #include "wcg_elasto.cuh"
 #include "wcg_adjoint.cuh"
 #include "wcg_correct.cuh"
+#include "wcg_merge.cuh"
 #include "wcg_scan.cuh"
 
 namespace wcg {
@@ -72,7 +73,7 @@ void ctx_free(Context& c) {
                     &c.mg, &c.mg_mask, &c.mg_vec,
                     &c.adj, &c.adjp, &c.adjmask, &c.adjstage, &c.adjvisc,
                     &c.visc, &c.viscflag,
-                    &c.xw, &c.corr_start, &c.corr_cursor, &c.corr_list,
+                    &c.xw, &c.corr_start, &c.corr_cursor, &c.corr_list, &c.mwork,
                     &c.scratch, &c.dscalars, &c.derr, &c.ticket};
   for (DevBuf* b : bufs) b->release();
   if (c.hscalars) cudaFreeHost(c.hscalars);
@@ -2239,7 +2240,144 @@ cudaError_t correct_liquid_particles(Context& c, double dt, int selector) {
                               : correct_liquid_t<float>(c, dt, selector);
 }
 
+void merge_draws(unsigned long long seed, unsigned long long k, int step, int* selector,
+                 int* perm) {
+  unsigned long long z = splitmix64(seed ^ splitmix64(k ^ 0x6d657267652d6b65ull));
+  *selector = (int)(z % (unsigned long long)(step > 0 ? step : 1));
+  for (int q = 0; q < 3; ++q) {
+    int* pq = perm + 3 * q;
+    pq[0] = 0;
+    pq[1] = 1;
+    pq[2] = 2;
+    for (int i = 2; i >= 1; --i) {  // mathutils::fisherYates (MathUtilities.h:238-245)
+      z = splitmix64(z);
+      const int j = (int)(z % (unsigned long long)(i + 1));
+      const int t = pq[i];
+      pq[i] = pq[j];
+      pq[j] = t;
+    }
+  }
+}
+
+template <typename R>
+static cudaError_t merge_liquid_t(Context& c, int selector, const int* perm, long long* removed) {
+  *removed = 0;
+  const long long n = c.np;
+  if (n == 0 || c.g.nb == 0) return cudaSuccess;
+  ProfScope prof(c, P_OTHER);
+  const int rb = c.real_bytes();
+  const long long cap = c.pcap;
+  // mwork: cls, removed (bytes), gvol, gmom (Reals), five int arrays
+  const size_t off_g = ((size_t)2 * cap + 15) / 16 * 16;
+  const size_t off_i = off_g + ((size_t)4 * cap * rb + 15) / 16 * 16;
+  WCG_TRY(c.mwork.ensure(off_i + (size_t)5 * cap * sizeof(int) + 64));
+  unsigned char* cls = c.mwork.as<unsigned char>();
+  unsigned char* rem = cls + cap;
+  R* gvol = (R*)(c.mwork.as<unsigned char>() + off_g);
+  R* gmom = gvol + cap;
+  int* iw = (int*)(c.mwork.as<unsigned char>() + off_i);
+  int* alive_slot = iw;
+  int* alive_pid = iw + cap;
+  int* hole_rank = iw + 2 * cap;
+  int* high_rank = iw + 3 * cap;
+  int* holes = iw + 4 * cap;
+  const long long nb = c.g.nb;
+  WCG_TRY(c.corr_start.ensure((size_t)(nb + 2) * sizeof(int)));
+  WCG_TRY(c.corr_cursor.ensure((size_t)std::max(nb, n) * sizeof(int)));
+  WCG_TRY(c.corr_list.ensure((size_t)n * sizeof(int)));
+  const long long scan_tiles = (std::max(nb + 1, n) + kScanTile - 1) / kScanTile + 1;
+  WCG_TRY(ensure_scratch(c, (size_t)scan_tiles * sizeof(long long) + 64));
+  int* start = c.corr_start.as<int>();
+  int* cursor = c.corr_cursor.as<int>();
+  int* list = c.corr_list.as<int>();
+  R* P = c.pbuf[c.cur].as<R>();
+  const int* pid = c.pid[c.cur].as<int>();
+  const int* pb = c.pbucket.as<int>() + c.cur * c.pcap;
+  long long* key = c.pkey.as<long long>() + (c.cur ^ 1) * c.pcap;  // free half
+  const double rad_fine = 1.0 / std::sqrt(3.0) * c.prm.dx * c.prm.cell_multiplier;
+  const double vf = 4.0 / 3.0 * M_PI * rad_fine * rad_fine * rad_fine;
+  // 1. classes and the bucket lists (index order inside a bucket)
+  WCG_TRY(cudaMemsetAsync(start, 0, (size_t)(nb + 1) * sizeof(int), c.stream));
+  WCG_TRY(cudaMemsetAsync(cursor, 0, (size_t)nb * sizeof(int), c.stream));
+  ++c.launches, k_merge_setup<R><<<nblk(n, 256), 256, 0, c.stream>>>(
+      P, cap, n, pb, nb, vf, cls, rem, gvol, gmom, key, start);
+  exclusive_scan<int, int>(start, nb, start, c.scratch.as<int>(), start + nb, c.stream);
+  ++c.launches, k_sort_scatter<<<nblk(n, 256), 256, 0, c.stream>>>(key, n, start, cursor, list);
+  ++c.launches, k_sort_cells<<<nblk(nb, 256), 256, 0, c.stream>>>(start, nb, pid, list);
+  // 2. the 27 colours in the drawn order
+  MergeArgs A;
+  A.g = c.g;
+  A.selector = selector;
+  A.step = c.prm.correction_step > 0 ? c.prm.correction_step : 1;
+  A.ne = (int)c.ne;
+  A.vf = vf;
+  A.should_rad = rad_fine * 2.0;
+  A.pid = pid;
+  A.list = list;
+  A.start = start;
+  const long long ncol = (long long)((c.g.ni + 2) / 3) * ((c.g.nj + 2) / 3) * ((c.g.nk + 2) / 3);
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b)
+      for (int d = 0; d < 3; ++d)
+        ++c.launches, k_merge<R><<<nblk(ncol, 128), 128, 0, c.stream>>>(
+            A, perm[6 + d], perm[3 + b], perm[a], P, cap, cls, rem, gvol, gmom);
+  // 3. gather and update, alive flags
+  ++c.launches, k_merge_gather<R><<<nblk(n, 256), 256, 0, c.stream>>>(
+      P, cap, n, pid, rem, gvol, gmom, c.prm.liquid_density, alive_slot, alive_pid);
+  int* dtot = (int*)(c.dscalars.as<double>() + 48);
+  exclusive_scan<int, int>(alive_slot, n, alive_slot, c.scratch.as<int>(), dtot, c.stream);
+  int K = 0;
+  WCG_TRY(cudaMemcpyAsync(&K, dtot, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  WCG_TRY(cudaStreamSynchronize(c.stream));
+  c.have_grid = false;  // volumes, masses and radii changed
+  c.xw_valid = false;
+  if (K == n) return cudaGetLastError();
+  // 4. removeEmptyParticles: the holes below K take the survivors above it
+  //    in descending order; compact the slots and renumber
+  ++c.launches, k_merge_flags<<<nblk(n, 256), 256, 0, c.stream>>>(n, K, alive_pid, hole_rank,
+                                                                   high_rank);
+  exclusive_scan<int, int>(hole_rank, n, hole_rank, c.scratch.as<int>(), dtot, c.stream);
+  exclusive_scan<int, int>(high_rank, n, high_rank, c.scratch.as<int>(), dtot + 1, c.stream);
+  ++c.launches, k_merge_holes<<<nblk(n, 256), 256, 0, c.stream>>>(n, K, alive_pid, hole_rank, holes);
+  int counts[2] = {0, 0};
+  WCG_TRY(cudaMemcpyAsync(counts, dtot, 2 * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  // surviving slots: alive_slot now holds their ranks; the flags come back
+  // from alive_pid through pid
+  ++c.launches, k_merge_alive_slots<<<nblk(n, 256), 256, 0, c.stream>>>(n, pid, alive_pid, cursor);
+  ++c.launches, k_merge_compact<<<nblk(n, 256), 256, 0, c.stream>>>(n, cursor, alive_slot, list);
+  WCG_TRY(cudaStreamSynchronize(c.stream));
+  const int nxt = c.cur ^ 1;
+  ++c.launches, k_gather_particles<R><<<nblk(K, 256), 256, 0, c.stream>>>(
+      list, K, cap, P, c.pbuf[nxt].as<R>(), pid, c.pid[nxt].as<int>(),
+      c.pkey.as<long long>() + c.cur * cap, c.pkey.as<long long>() + nxt * cap,
+      c.pdelta.as<int>() + c.cur * cap, c.pdelta.as<int>() + nxt * cap, pb,
+      c.pbucket.as<int>() + nxt * cap);
+  ++c.launches, k_merge_repid<<<nblk(K, 256), 256, 0, c.stream>>>(
+      K, list, pid, high_rank, holes, counts[1], c.pid[nxt].as<int>());
+  WCG_TRY(cudaGetLastError());
+  c.cur = nxt;
+  *removed = n - K;
+  c.np = K;
+  c.have_grid = false;
+  c.xw_valid = false;
+  return cudaStreamSynchronize(c.stream);
+}
+
+cudaError_t merge_liquid_particles(Context& c, int selector, const int* perm, long long* removed) {
+  return c.prm.precision == 0 ? merge_liquid_t<double>(c, selector, perm, removed)
+                              : merge_liquid_t<float>(c, selector, perm, removed);
+}
+
 cudaError_t substep(Context& c, double dt) {
+  // updateOptiVolume + mergeLiquidParticles (WetClothCore.cpp:97-110), on the
+  // buckets of the previous sub-step's grid build
+  if (c.prm.particle_merge && c.np > 0 && c.g.nb > 0) {
+    int sel = 0, perm[9];
+    merge_draws(c.prm.merge_seed, c.merge_count++, c.prm.correction_step, &sel, perm);
+    long long removed = 0;
+    WCG_TRY(merge_liquid_particles(c, sel, perm, &removed));
+    c.merged_removed = removed;
+  }
   WCG_TRY(build_grid(c));
   WCG_TRY(map_particles_to_grid(c));
   WCG_TRY(step_velocity(c, dt));

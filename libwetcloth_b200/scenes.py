@@ -49,6 +49,11 @@ class SceneParams:
     correction_step: int = 8
     correction_multiplier: float = 2.0
     correction_seed: int = 0
+    # relabel + mergeLiquidParticles before each sub-step, the seed of its
+    # draws, and LiquidInfo::particle_cell_multiplier (V_fine)
+    particle_merge: bool = False
+    merge_seed: int = 0
+    particle_cell_multiplier: float = 0.3535533906
 
 
 def particle_radius(dx: float, ppc: int) -> float:

@@ -44,6 +44,9 @@ def make_params(p, precision=_capi.WCG_FP64, refine_inner_tol=0.0,
     prm.drag_viscosity = getattr(p, "drag_viscosity", 8.9e-3)
     prm.viscosity_implicit = 1 if getattr(p, "viscosity_implicit", False) else 0
     prm.viscosity_criterion = getattr(p, "viscosity_criterion", 1e-6)
+    prm.particle_merge = 1 if getattr(p, "particle_merge", False) else 0
+    prm.merge_seed = getattr(p, "merge_seed", 0)
+    prm.particle_cell_multiplier = getattr(p, "particle_cell_multiplier", 0.3535533906)
     prm.correction_strength = getattr(p, "correction_strength", 0.0)
     prm.correction_step = getattr(p, "correction_step", 8)
     prm.correction_multiplier = getattr(p, "correction_multiplier", 2.0)
@@ -185,6 +188,15 @@ class FluidScene:
 
     def constrain_liquid_velocity(self):
         check(self.L.wcg_constrain_liquid_velocity(self.h))
+
+    def merge_liquid_particles(self, selector, perm):
+        """relabel + mergeLiquidParticles + removeEmptyParticles with the given
+        subset and colour order (9 ints: z, y, x permutations); returns the
+        number of particles removed."""
+        pm = (ctypes.c_int * 9)(*[int(v) for v in np.asarray(perm).reshape(-1)])
+        rem = ctypes.c_longlong(0)
+        check(self.L.wcg_merge_liquid_particles(self.h, int(selector), pm, ctypes.byref(rem)))
+        return rem.value
 
     def correct_liquid_particles(self, dt, selector):
         """correctLiquidParticles for the particles with index % step == selector."""

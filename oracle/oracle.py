@@ -46,6 +46,8 @@ def lib():
         L.wco_correct_liquid.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
         L.wco_merge_liquid.argtypes = [ctypes.c_void_p, ctypes.c_int, _I, _I, _I]
         L.wco_merge_liquid.restype = ctypes.c_int
+        L.wco_merge_draws.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, _I, _I]
+        L.wco_set_merge.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_uint64, ctypes.c_double]
         L.wco_correction_selector.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int]
         L.wco_correction_selector.restype = ctypes.c_int
         L.wco_step.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
@@ -117,6 +119,10 @@ class OracleScene:
         if mu > 0.0 and getattr(p, "viscosity_implicit", False):
             L.wco_set_viscosity_implicit(self.h, 1, getattr(p, "viscosity_criterion", 1e-6))
         set_elasto(L.wco_set_elasto, L.wco_set_elasto_coeffs, self.h, scene, self._keep)
+        if getattr(p, "particle_merge", False) or getattr(p, "particle_cell_multiplier", None):
+            L.wco_set_merge(self.h, 1 if getattr(p, "particle_merge", False) else 0,
+                            getattr(p, "merge_seed", 0),
+                            getattr(p, "particle_cell_multiplier", 0.3535533906))
         if getattr(p, "correction_strength", 0.0) > 0.0:
             L.wco_set_correction(self.h, p.correction_strength, p.correction_step,
                                  p.correction_multiplier, p.correction_seed)

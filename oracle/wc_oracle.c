@@ -37,6 +37,7 @@ typedef struct {
   double corr_strength, corr_mult;
   int corr_step;
   double cell_mult; /* LiquidInfo::particle_cell_multiplier */
+  int merge_on;     /* relabel + mergeLiquidParticles before each sub-step */
 } Params;
 
 typedef struct {
@@ -100,6 +101,7 @@ typedef struct {
   uint64_t corr_seed, corr_count; /* selector stream of the particle correction */
   int corr_sel_once;              /* >= 0: selector of the next correction */
   unsigned char* cls;             /* m_classifier of the liquid particles */
+  uint64_t merge_seed, merge_count; /* draw stream of the merge */
   Snap snaps[256];
   int nsnaps;
 } Scene;
@@ -1987,6 +1989,36 @@ int wco_merge_liquid(Scene* s, int selector, const int* perm_t, const int* perm_
   return nrem;
 }
 
+/* the draws of merge call k of a seeded stream: selector, then three
+ * Fisher-Yates permutations of {0, 1, 2} (mathutils::fisherYates,
+ * MathUtilities.h:238-245, on SplitMix64 draws) */
+void wco_merge_draws(uint64_t seed, uint64_t k, int step, int* selector, int* perm9) {
+  uint64_t z = splitmix64(seed ^ splitmix64(k ^ 0x6d657267652d6b65ull));
+  *selector = (int)(z % (uint64_t)(step > 0 ? step : 1));
+  for (int q = 0; q < 3; ++q) {
+    int* pq = perm9 + 3 * q;
+    pq[0] = 0;
+    pq[1] = 1;
+    pq[2] = 2;
+    for (int i = 2; i >= 1; --i) {
+      z = splitmix64(z);
+      const int j = (int)(z % (uint64_t)(i + 1));
+      const int t = pq[i];
+      pq[i] = pq[j];
+      pq[j] = t;
+    }
+  }
+}
+
+/* merge before each sub-step with the seeded draws; LiquidInfo
+ * particle_cell_multiplier */
+void wco_set_merge(Scene* s, int on, uint64_t seed, double cell_mult) {
+  s->p.merge_on = on;
+  s->merge_seed = seed;
+  s->merge_count = 0;
+  s->p.cell_mult = cell_mult;
+}
+
 /* correctLiquidParticles with an explicit particle subset, outside a step */
 void wco_correct_liquid(Scene* s, double dt, int selector) { correct_liquid(s, dt, selector); }
 
@@ -2171,8 +2203,14 @@ static void transfer_out(Scene* s, double dt, int snapshot) {
   if (snapshot) snap_particles(s, "adv_");
 }
 
-/* one sub-step in WetClothCore::stepSystem order (WetClothCore.cpp:115-258) */
+/* one sub-step in WetClothCore::stepSystem order (WetClothCore.cpp:97-258) */
 int wco_substep(Scene* s, double dt, int snapshot) {
+  if (s->p.merge_on && s->keys && s->np > s->ne) {
+    int sel, perm[9];
+    wco_merge_draws(s->merge_seed, s->merge_count++, s->p.corr_step, &sel, perm);
+    const long long nrem = wco_merge_liquid(s, sel, perm, perm + 3, perm + 6);
+    snap_put_i(s, "merge_removed", &nrem, 1);
+  }
   transfer_in(s, snapshot);
   step_velocity(s, dt);
   if (snapshot) {

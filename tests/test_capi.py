@@ -98,3 +98,24 @@ def test_correction_params_and_selector_stream():
                 if step == 8:
                     seen.add(s)
     assert seen == set(range(8))
+
+
+def test_merge_draw_stream():
+    """The merge draws of wcg_step (host code) are the oracle's."""
+    L = _capi.load()
+    from oracle import oracle as oo
+    if not oo.available():
+        pytest.skip("oracle not built")
+    O = oo.lib()
+    sel_g, sel_o = ctypes.c_int(0), ctypes.c_int(0)
+    pg, po = (ctypes.c_int * 9)(), (ctypes.c_int * 9)()
+    seen = set()
+    for seed in (0, 3, 2**33 + 1):
+        for k in range(40):
+            assert L.wcg_merge_draws(seed, k, 8, ctypes.byref(sel_g), pg) == 0
+            O.wco_merge_draws(seed, k, 8, ctypes.byref(sel_o), po)
+            assert sel_g.value == sel_o.value and list(pg) == list(po)
+            for q in range(3):
+                assert sorted(pg[3 * q:3 * q + 3]) == [0, 1, 2]
+            seen.add(tuple(pg[:3]))
+    assert len(seen) == 6
