@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the many-scenes measurement (batched vs sequential)")
     ap.add_argument("--batch-scenes", type=int, default=32)
+    ap.add_argument("--no-cloth", action="store_true",
+                    help="skip the liquid-on-cloth measurement (128^3 sphere on a sheet)")
     return ap.parse_args()
 
 
@@ -352,6 +354,58 @@ def run_ours(args, rank, world, dev):
                                               "pressure solver (AMGPCGSolveSparse restated)")
     if not args.no_batch:
         out["batch"] = run_batch(args)
+    if not args.no_cloth:
+        out["cloth"] = run_cloth(dev)
+    return out
+
+
+def run_cloth(dev, n=128, steps=5, warmup=2, dt=5e-4):
+    """The liquid-on-cloth configuration: at 128^3 a liquid sphere (r 0.15,
+    8 per cell, falling at 1 m/s) onto a 128 x 128-vertex cloth sheet at
+    y = 0.4 (porosity 0.5), dt 5e-4: ms per step of the liquid step with its
+    coupling to the sheet (transfers of both phases, drag, pore pressure, the
+    solid volume in the pressure system) in FP64 and FP32 + refinement; the
+    sheet keeps its transferred velocity (the cloth solve is not part of the
+    path).  Device time with CUDA events on the context's stream."""
+    import torch
+    from libwetcloth_b200 import scenes
+    from libwetcloth_b200._capi import WCG_FP32_REFINE, WCG_FP64
+    from libwetcloth_b200.solver import FluidScene
+    sc = scenes.liquid_on_sheet(n, 8, 3, sheet_spacing=0.8 / 127)
+    out = {"grid": n, "liquid_particles": int(sc.x.shape[0]),
+           "cloth_vertices": int(sc.elasto.n), "dt": dt, "steps": steps}
+    for name, prec in (("fp64", WCG_FP64), ("fp32_refine", WCG_FP32_REFINE)):
+        g = FluidScene(sc, precision=prec)
+        for _ in range(warmup):
+            g.step(dt)
+        stream = torch.cuda.ExternalStream(g.stream_ptr, device=f"cuda:{dev}")
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        iters = []
+        for _ in range(steps):
+            g.step(dt)
+            iters.append(g.stats()["pcg_iters"])
+        e1.record(stream)
+        e1.synchronize()
+        out[name] = {"ms_per_step": round(e0.elapsed_time(e1) / steps, 3),
+                     "pcg_iters_per_step": iters}
+        g.close()
+    # the reference Core on the same scene, one step after one warm-up
+    from oracle import ref as oref
+    if oref.available(omp=True):
+        os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+        with _quiet_stdout():
+            r = oref.RefScene(sc, mic=False, omp=True)
+            r.step(dt, snapshot=False)
+            t0 = time.perf_counter()
+            r.step(dt, snapshot=False)
+            ref_ms = (time.perf_counter() - t0) * 1000
+            r.close()
+        out["reference_cpu"] = {"ms_per_step": round(ref_ms, 1),
+                                "cores": int(os.environ["OMP_NUM_THREADS"]),
+                                "note": "reference Core (OpenMP stand-in for TBB), one step"}
     return out
 
 
