@@ -131,6 +131,24 @@ int wcg_upload_liquid_device(wcg_ctx* ctx, long long n, const double* x3,
 int wcg_download_liquid(wcg_ctx* ctx, double* x3, double* v3, double* C9);
 int wcg_download_liquid_device(wcg_ctx* ctx, double* x3, double* v3,
                                double* C9);
+/* wcg_download_liquid without waiting for the copies: the particle state is
+ * gathered at once, and its transfer to the host overlaps whatever the caller
+ * does next on this context (an upload, the next step).  The host buffers
+ * should be pinned (cudaHostAlloc) and must stay untouched until
+ * wcg_synchronize returns. */
+int wcg_download_liquid_async(wcg_ctx* ctx, double* x3, double* v3, double* C9);
+/* The upload of wcg_upload_liquid in two halves, so that the host-to-device
+ * copies of the next set overlap the current step: wcg_stage_liquid_async
+ * queues the copies into a staging buffer and returns (host buffers pinned
+ * and untouched until the set is loaded); wcg_upload_staged loads the staged
+ * set into the particle arrays after the work already queued on the context
+ * (a step in progress), as wcg_upload_liquid would. */
+int wcg_stage_liquid_async(wcg_ctx* ctx, long long n, const double* x3, const double* v3,
+                           const double* C9, const double* mass, const double* vol,
+                           const double* radius);
+int wcg_upload_staged(wcg_ctx* ctx);
+/* waits for every operation on the context, asynchronous copies included */
+int wcg_synchronize(wcg_ctx* ctx);
 long long wcg_num_particles(const wcg_ctx* ctx);
 
 /* Elasto (cloth / yarn) particles, the reference's particles [0, n) ahead of

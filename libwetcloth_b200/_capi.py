@@ -121,6 +121,11 @@ SIGNATURES = {
                                                   ctypes.POINTER(ctypes.c_longlong)]),
     "wcg_merge_draws": (ctypes.c_int, [ctypes.c_ulonglong, ctypes.c_ulonglong, ctypes.c_int,
                                        ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "wcg_download_liquid_async": (ctypes.c_int, [ctypes.c_void_p, _D, _D, _D]),
+    "wcg_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
+    "wcg_stage_liquid_async": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, _D, _D, _D, _D,
+                                              _D, _D]),
+    "wcg_upload_staged": (ctypes.c_int, [ctypes.c_void_p]),
     "wcg_correct_liquid_particles": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]),
     "wcg_correction_selector": (ctypes.c_int, [ctypes.c_ulonglong, ctypes.c_ulonglong, ctypes.c_int]),
     "wcg_advect": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),

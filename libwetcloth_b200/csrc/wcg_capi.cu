@@ -44,7 +44,10 @@ int device_status(wcg::Context& c, const char* what) {
                                     std::to_string(h) +
                                     (h == wcg::kErrWaitTimeout
                                          ? " (wavefront wait limit reached)"
-                                         : " (index out of range, access skipped)"));
+                                         : h == wcg::kErrInput
+                                               ? " (invalid particle input: non-finite position "
+                                                 "or velocity, or negative mass/volume/radius)"
+                                               : " (index out of range, access skipped)"));
   }
   return WCG_OK;
 }
@@ -325,6 +328,39 @@ int wcg_upload_liquid_device(wcg_ctx* ctx, long long n, const double* x3,
 int wcg_download_liquid(wcg_ctx* ctx, double* x3, double* v3, double* C9) {
   WCG_CHECK_CTX(ctx);
   WCG_CALL(ctx, wcg::download_particles(ctx->c, x3, v3, C9, false), "download");
+  return WCG_OK;
+}
+
+int wcg_download_liquid_async(wcg_ctx* ctx, double* x3, double* v3, double* C9) {
+  WCG_CHECK_CTX(ctx);
+  WCG_CALL(ctx, wcg::download_particles_async(ctx->c, x3, v3, C9), "download (asynchronous)");
+  return WCG_OK;
+}
+
+int wcg_stage_liquid_async(wcg_ctx* ctx, long long n, const double* x3, const double* v3,
+                           const double* C9, const double* mass, const double* vol,
+                           const double* radius) {
+  WCG_CHECK_CTX(ctx);
+  if (n < 0) return fail(WCG_ERR_ARG, "negative particle count");
+  if (n > 0 && (!x3 || !v3 || !mass || !vol || !radius))
+    return fail(WCG_ERR_ARG, "null particle array");
+  if (n > INT_MAX) return fail(WCG_ERR_ARG, "more than 2^31 - 1 particles");
+  WCG_CALL(ctx, wcg::stage_particles_async(ctx->c, n, x3, v3, C9, mass, vol, radius),
+           "stage (asynchronous)");
+  return WCG_OK;
+}
+
+int wcg_upload_staged(wcg_ctx* ctx) {
+  WCG_CHECK_CTX(ctx);
+  if (ctx->c.staged_n < 0) return fail(WCG_ERR_STATE, "no staged particle set");
+  WCG_CALL(ctx, wcg::load_staged(ctx->c), "upload staged");
+  ctx->c.have_grid = false;
+  return WCG_OK;
+}
+
+int wcg_synchronize(wcg_ctx* ctx) {
+  WCG_CHECK_CTX(ctx);
+  WCG_CALL(ctx, wcg::synchronize(ctx->c), "synchronize");
   return WCG_OK;
 }
 
@@ -633,6 +669,8 @@ int wcg_step(wcg_ctx* ctx, double dt, int* substeps_out) {
   if (!(dt > 0)) return fail(WCG_ERR_ARG, "dt must be positive");
   int n = 1;
   WCG_CALL(ctx, wcg::num_substeps(ctx->c, dt, &n), "num_substeps");
+  // a staged upload is checked on the device: stop before stepping bad input
+  if (int st = device_status(ctx->c, "particle upload")) return st;
   const double sub = dt / (double)n;
   int status = WCG_OK;
   for (int k = 0; k < n; ++k) {

@@ -35,6 +35,8 @@ enum DeviceError : int {
   kErrNone = 0,
   kErrWaitTimeout = 1,   // a wavefront dependency wait gave up
   kErrIndex = 2,         // an index fell outside its buffer (skipped)
+  kErrInput = 3,         // a staged particle had a non-finite position or velocity,
+                         // or a negative or NaN mass, volume or radius
 };
 
 __host__ __device__ inline long long node_linear(const GridDesc& g, int I,

@@ -168,6 +168,18 @@ enum Pl64Field : int { PL64_X = 0, PL64_R, kNumPl64Fields };
 struct Context {
   Params prm;
   cudaStream_t stream = nullptr;
+  // asynchronous downloads: the gather into dstage runs on `stream`, the
+  // device-to-host copies on copy_stream, ordered by the two events
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_store = nullptr, ev_d2h = nullptr;
+  DevBuf dstage;
+  // staged uploads: host-to-device copies into ustage on in_stream, loaded
+  // into the particle arrays later on `stream`
+  cudaStream_t in_stream = nullptr;
+  cudaEvent_t ev_staged = nullptr, ev_loaded = nullptr;
+  DevBuf ustage;
+  long long staged_n = -1;
+  bool staged_C = false;
   int device = 0;
   std::string last_error;
 
@@ -322,6 +334,18 @@ cudaError_t upload_particles(Context& c, long long n, const double* x3,
                              const double* radius, bool device_ptrs);
 cudaError_t download_particles(Context& c, double* x3, double* v3, double* C9,
                                bool device_ptrs);
+// the same into host buffers without waiting: the copies run on copy_stream
+// and overlap later work on `stream` (synchronize() waits for them)
+cudaError_t download_particles_async(Context& c, double* x3, double* v3, double* C9);
+cudaError_t synchronize(Context& c);
+// host-to-device copies of a liquid particle set into the staging buffer on
+// in_stream, without waiting (host buffers pinned and untouched until the
+// staged set is loaded); load_staged() puts it into the particle arrays on
+// `stream`, after whatever was queued there
+cudaError_t stage_particles_async(Context& c, long long n, const double* x3, const double* v3,
+                                  const double* C9, const double* mass, const double* vol,
+                                  const double* radius);
+cudaError_t load_staged(Context& c);
 // positions in the reference's m_x layout (x, y, z, 0 per particle) and radii,
 // original order, host buffers
 cudaError_t download_positions(Context& c, double* x4, double* radius);

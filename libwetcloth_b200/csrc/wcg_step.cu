@@ -52,6 +52,12 @@ static inline unsigned nblk(long long n, int t) {
 cudaError_t ctx_init(Context& c) {
   WCG_TRY(cudaGetDevice(&c.device));
   WCG_TRY(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+  WCG_TRY(cudaStreamCreateWithFlags(&c.copy_stream, cudaStreamNonBlocking));
+  WCG_TRY(cudaEventCreateWithFlags(&c.ev_store, cudaEventDisableTiming));
+  WCG_TRY(cudaEventCreateWithFlags(&c.ev_d2h, cudaEventDisableTiming));
+  WCG_TRY(cudaStreamCreateWithFlags(&c.in_stream, cudaStreamNonBlocking));
+  WCG_TRY(cudaEventCreateWithFlags(&c.ev_staged, cudaEventDisableTiming));
+  WCG_TRY(cudaEventCreateWithFlags(&c.ev_loaded, cudaEventDisableTiming));
   WCG_TRY(cudaMallocHost((void**)&c.hscalars, 64 * sizeof(double)));
   WCG_TRY(c.dscalars.ensure(64 * sizeof(double)));
   WCG_TRY(c.derr.ensure(sizeof(int)));
@@ -72,7 +78,7 @@ void ctx_free(Context& c) {
                     &c.pl, &c.pl64, &c.pl_edge, &c.pl_order, &c.pl_corder, &c.pl_part,
                     &c.mg, &c.mg_mask, &c.mg_vec,
                     &c.adj, &c.adjp, &c.adjmask, &c.adjstage, &c.adjvisc,
-                    &c.visc, &c.viscflag,
+                    &c.visc, &c.viscflag, &c.dstage, &c.ustage,
                     &c.xw, &c.corr_start, &c.corr_cursor, &c.corr_list, &c.mwork,
                     &c.scratch, &c.dscalars, &c.derr, &c.ticket};
   for (DevBuf* b : bufs) b->release();
@@ -85,6 +91,22 @@ void ctx_free(Context& c) {
   c.prof_recs.clear();
   for (cudaEvent_t e : c.prof_pool) cudaEventDestroy(e);
   c.prof_pool.clear();
+  if (c.copy_stream) {
+    cudaStreamSynchronize(c.copy_stream);
+    cudaStreamDestroy(c.copy_stream);
+  }
+  c.copy_stream = nullptr;
+  if (c.in_stream) {
+    cudaStreamSynchronize(c.in_stream);
+    cudaStreamDestroy(c.in_stream);
+  }
+  c.in_stream = nullptr;
+  if (c.ev_staged) cudaEventDestroy(c.ev_staged);
+  if (c.ev_loaded) cudaEventDestroy(c.ev_loaded);
+  c.ev_staged = c.ev_loaded = nullptr;
+  if (c.ev_store) cudaEventDestroy(c.ev_store);
+  if (c.ev_d2h) cudaEventDestroy(c.ev_d2h);
+  c.ev_store = c.ev_d2h = nullptr;
   if (c.stream) cudaStreamDestroy(c.stream);
   c.stream = nullptr;
 }
@@ -120,13 +142,17 @@ template <typename R>
 __global__ void k_load_particles(long long n, long long pcap, const double* x3,
                                  const double* v3, const double* C9,
                                  const double* m, const double* vol,
-                                 const double* rad, R* P, int* pid) {
+                                 const double* rad, R* P, int* pid, int* err) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  bool bad = !(m[i] >= 0.0) || !(vol[i] >= 0.0) || !(rad[i] >= 0.0);
   for (int a = 0; a < 3; ++a) {
-    P[(PX + a) * pcap + i] = (R)x3[i * 3 + a];
-    P[(VX + a) * pcap + i] = (R)v3[i * 3 + a];
+    const double x = x3[i * 3 + a], v = v3[i * 3 + a];
+    bad = bad || !isfinite(x) || !isfinite(v);
+    P[(PX + a) * pcap + i] = (R)x;
+    P[(VX + a) * pcap + i] = (R)v;
   }
+  if (bad && err) record_error(err, kErrInput);
   for (int q = 0; q < 9; ++q) P[(C00 + q) * pcap + i] = C9 ? (R)C9[i * 9 + q] : R(0);
   P[PM * pcap + i] = (R)m[i];
   P[PV * pcap + i] = (R)vol[i];
@@ -226,11 +252,11 @@ cudaError_t upload_particles(Context& c, long long n, const double* x3,
   if (c.prm.precision == 0)
     ++c.launches, k_load_particles<double><<<nblk(n, 256), 256, 0, c.stream>>>(
         n, c.pcap, dx3, dv3, dC9, dm, dvol, drad, c.pbuf[0].as<double>(),
-        c.pid[0].as<int>());
+        c.pid[0].as<int>(), c.derr.as<int>());
   else
     ++c.launches, k_load_particles<float><<<nblk(n, 256), 256, 0, c.stream>>>(
         n, c.pcap, dx3, dv3, dC9, dm, dvol, drad, c.pbuf[0].as<float>(),
-        c.pid[0].as<int>());
+        c.pid[0].as<int>(), c.derr.as<int>());
   WCG_TRY(cudaGetLastError());
   return cudaStreamSynchronize(c.stream);
 }
@@ -256,6 +282,71 @@ cudaError_t download_particles(Context& c, double* x3, double* v3, double* C9,
   if (C9)
     WCG_TRY(cudaMemcpyAsync(C9, st + 6 * n, n * 9 * sizeof(double), kind, c.stream));
   return cudaStreamSynchronize(c.stream);
+}
+
+cudaError_t download_particles_async(Context& c, double* x3, double* v3, double* C9) {
+  const long long n = c.np;
+  if (n == 0) return cudaSuccess;
+  WCG_TRY(c.dstage.ensure((size_t)15 * n * sizeof(double)));
+  double* st = c.dstage.as<double>();
+  // the previous asynchronous download must have read dstage out
+  WCG_TRY(cudaStreamWaitEvent(c.stream, c.ev_d2h, 0));
+  if (c.prm.precision == 0)
+    ++c.launches, k_store_particles<double><<<nblk(n, 256), 256, 0, c.stream>>>(
+        n, c.pcap, c.pbuf[c.cur].as<double>(), c.pid[c.cur].as<int>(), st);
+  else
+    ++c.launches, k_store_particles<float><<<nblk(n, 256), 256, 0, c.stream>>>(
+        n, c.pcap, c.pbuf[c.cur].as<float>(), c.pid[c.cur].as<int>(), st);
+  WCG_TRY(cudaGetLastError());
+  WCG_TRY(cudaEventRecord(c.ev_store, c.stream));
+  WCG_TRY(cudaStreamWaitEvent(c.copy_stream, c.ev_store, 0));
+  if (x3)
+    WCG_TRY(cudaMemcpyAsync(x3, st, n * 3 * sizeof(double), cudaMemcpyDeviceToHost, c.copy_stream));
+  if (v3)
+    WCG_TRY(cudaMemcpyAsync(v3, st + 3 * n, n * 3 * sizeof(double), cudaMemcpyDeviceToHost,
+                            c.copy_stream));
+  if (C9)
+    WCG_TRY(cudaMemcpyAsync(C9, st + 6 * n, n * 9 * sizeof(double), cudaMemcpyDeviceToHost,
+                            c.copy_stream));
+  return cudaEventRecord(c.ev_d2h, c.copy_stream);
+}
+
+cudaError_t synchronize(Context& c) {
+  WCG_TRY(cudaStreamSynchronize(c.stream));
+  WCG_TRY(cudaStreamSynchronize(c.in_stream));
+  return cudaStreamSynchronize(c.copy_stream);
+}
+
+cudaError_t stage_particles_async(Context& c, long long n, const double* x3, const double* v3,
+                                  const double* C9, const double* mass, const double* vol,
+                                  const double* radius) {
+  WCG_TRY(c.ustage.ensure((size_t)18 * std::max(n, 1LL) * sizeof(double)));
+  double* u = c.ustage.as<double>();
+  // the previously staged set must have been loaded
+  WCG_TRY(cudaStreamWaitEvent(c.in_stream, c.ev_loaded, 0));
+  const cudaMemcpyKind k = cudaMemcpyHostToDevice;
+  WCG_TRY(cudaMemcpyAsync(u, x3, n * 3 * sizeof(double), k, c.in_stream));
+  WCG_TRY(cudaMemcpyAsync(u + 3 * n, v3, n * 3 * sizeof(double), k, c.in_stream));
+  if (C9) WCG_TRY(cudaMemcpyAsync(u + 6 * n, C9, n * 9 * sizeof(double), k, c.in_stream));
+  WCG_TRY(cudaMemcpyAsync(u + 15 * n, mass, n * sizeof(double), k, c.in_stream));
+  WCG_TRY(cudaMemcpyAsync(u + 16 * n, vol, n * sizeof(double), k, c.in_stream));
+  WCG_TRY(cudaMemcpyAsync(u + 17 * n, radius, n * sizeof(double), k, c.in_stream));
+  WCG_TRY(cudaEventRecord(c.ev_staged, c.in_stream));
+  c.staged_n = n;
+  c.staged_C = C9 != nullptr;
+  return cudaSuccess;
+}
+
+cudaError_t load_staged(Context& c) {
+  const long long n = c.staged_n;
+  const double* u = c.ustage.as<double>();
+  WCG_TRY(cudaStreamWaitEvent(c.stream, c.ev_staged, 0));
+  // device-pointer upload from the staging buffer (grows the arrays as needed)
+  WCG_TRY(upload_particles(c, n, u, u + 3 * n, c.staged_C ? u + 6 * n : nullptr, u + 15 * n,
+                           u + 16 * n, u + 17 * n, true));
+  WCG_TRY(cudaEventRecord(c.ev_loaded, c.stream));
+  c.staged_n = -1;
+  return cudaSuccess;
 }
 
 cudaError_t download_positions(Context& c, double* x4, double* radius) {

@@ -84,3 +84,63 @@ def test_fluid_obj(tmp_path, wcg):
     assert np.allclose(vals[:, :3], x, rtol=1e-7, atol=1e-12)
     assert np.allclose(vals[:, 3], sc.radius, rtol=1e-7)
     g.close()
+
+
+def test_async_download_overlaps_and_matches(wcg):
+    """wcg_download_liquid_async: the read-back of step k, left running on the
+    copy stream while the next upload and step run, equals the synchronous
+    download of the same state."""
+    import ctypes
+    import torch
+    sc = scenes.dam_break(16, 8, 0)
+    g = FluidScene(sc)
+    n = sc.x.shape[0]
+    outs = [tuple(torch.empty(n * k, dtype=torch.float64).pin_memory() for k in (3, 3, 9))
+            for _ in range(2)]
+    ptr = lambda t: ctypes.cast(t.data_ptr(), ctypes.POINTER(ctypes.c_double))
+    ref = []
+    for k in range(4):
+        g.step(1e-3)
+        ref.append(g.download())
+        ox, ov, oC = outs[k % 2]
+        assert g.L.wcg_download_liquid_async(g.h, ptr(ox), ptr(ov), ptr(oC)) == 0
+        if k % 2 == 1:
+            assert g.L.wcg_synchronize(g.h) == 0
+            for j in (k - 1, k):
+                x, v, C = ref[j]
+                bx, bv, bC = outs[j % 2]
+                assert np.array_equal(bx.numpy().reshape(n, 3), x)
+                assert np.array_equal(bv.numpy().reshape(n, 3), v)
+                assert np.array_equal(bC.numpy().reshape(n, 9), C)
+    g.close()
+
+
+def test_staged_upload_matches_and_checks_input(wcg):
+    """wcg_stage_liquid_async + wcg_upload_staged load the same state as
+    wcg_upload_liquid, while a step is queued; bad input is caught on the
+    device and the next step stops before stepping it."""
+    import ctypes
+    import torch
+    sc = scenes.dam_break(16, 8, 0)
+    n = sc.x.shape[0]
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).pin_memory()
+    bufs = [pin(a) for a in (sc.x, sc.v, np.zeros((n, 9)), sc.mass, sc.vol, sc.radius)]
+    ptr = lambda t: ctypes.cast(t.data_ptr(), ctypes.POINTER(ctypes.c_double))
+    a = FluidScene(sc)
+    a.step(1e-3)
+    xa, va, Ca = a.download()
+    b = FluidScene(sc)
+    b.step(1e-3)  # other state first
+    assert b.L.wcg_stage_liquid_async(b.h, n, *[ptr(t) for t in bufs]) == 0
+    b.step(1e-3)  # runs while the copies are in flight; replaced by the staged set
+    assert b.L.wcg_upload_staged(b.h) == 0
+    b.step(1e-3)
+    xb, vb, Cb = b.download()
+    assert np.array_equal(xa, xb) and np.array_equal(va, vb) and np.array_equal(Ca, Cb)
+    bufs[1][5] = float("nan")
+    assert b.L.wcg_stage_liquid_async(b.h, n, *[ptr(t) for t in bufs]) == 0
+    assert b.L.wcg_upload_staged(b.h) == 0
+    assert b.L.wcg_step(b.h, 1e-3, None) == _capi.WCG_ERR_DEVICE
+    assert b"invalid particle input" in b.L.wcg_last_error()
+    a.close()
+    b.close()
