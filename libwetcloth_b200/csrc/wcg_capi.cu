@@ -634,6 +634,8 @@ int wcg_substep_vjp(wcg_ctx* ctx, double dt, const double* vbar3, const double* 
     return fail(WCG_ERR_UNSUPPORTED, "substep_vjp: not available with the particle correction on");
   if (ctx->c.prm.viscosity > 0.0 && ctx->c.prm.viscosity_implicit)
     return fail(WCG_ERR_UNSUPPORTED, "substep_vjp: not available with the implicit viscosity");
+  if (ctx->c.prm.particle_merge)
+    return fail(WCG_ERR_UNSUPPORTED, "substep_vjp: not available with the particle merge on");
   const long long n = ctx->c.np;
   if (n > 0 && (!vbar3 || !Cbar9 || !xbar3 || !vbar0 || !Cbar0 || !xbar0))
     return fail(WCG_ERR_ARG, "null cotangent array");
