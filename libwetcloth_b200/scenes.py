@@ -53,6 +53,8 @@ class SceneParams:
     # draws, and LiquidInfo::particle_cell_multiplier (V_fine)
     particle_merge: bool = False
     merge_seed: int = 0
+    particle_split: bool = False   # relabel + splitLiquidParticles before each sub-step
+    split_seed: int = 0
     particle_cell_multiplier: float = 0.3535533906
 
 

@@ -48,6 +48,11 @@ def lib():
         L.wco_merge_liquid.restype = ctypes.c_int
         L.wco_merge_draws.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, _I, _I]
         L.wco_set_merge.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_uint64, ctypes.c_double]
+        L.wco_split_liquid.argtypes = [ctypes.c_void_p, ctypes.c_uint64]
+        L.wco_split_liquid.restype = ctypes.c_int
+        L.wco_split_key.argtypes = [ctypes.c_uint64, ctypes.c_uint64]
+        L.wco_split_key.restype = ctypes.c_uint64
+        L.wco_set_split.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_uint64]
         L.wco_correction_selector.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int]
         L.wco_correction_selector.restype = ctypes.c_int
         L.wco_step.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
@@ -123,6 +128,8 @@ class OracleScene:
             L.wco_set_merge(self.h, 1 if getattr(p, "particle_merge", False) else 0,
                             getattr(p, "merge_seed", 0),
                             getattr(p, "particle_cell_multiplier", 0.3535533906))
+        if getattr(p, "particle_split", False):
+            L.wco_set_split(self.h, 1, getattr(p, "split_seed", 0))
         if getattr(p, "correction_strength", 0.0) > 0.0:
             L.wco_set_correction(self.h, p.correction_strength, p.correction_step,
                                  p.correction_multiplier, p.correction_seed)
@@ -157,6 +164,11 @@ class OracleScene:
         rows = [np.ascontiguousarray(pm[k]) for k in range(3)]
         ip = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
         return self.L.wco_merge_liquid(self.h, int(selector), ip(rows[0]), ip(rows[1]), ip(rows[2]))
+
+    def split(self, key):
+        """splitLiquidParticles with the rotations of key; returns the
+        particles added."""
+        return self.L.wco_split_liquid(self.h, int(key))
 
     def set_correction_selector(self, selector):
         """Particle subset (fluid index % step) of the next correction."""

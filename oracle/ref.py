@@ -59,6 +59,8 @@ def _lib(omp: bool):
                                            ctypes.c_double, ctypes.c_uint]
         L.wcref_merge.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_int]
         L.wcref_merge.restype = ctypes.c_int
+        L.wcref_split.argtypes = [ctypes.c_void_p, ctypes.c_uint]
+        L.wcref_split.restype = ctypes.c_int
         _libs[omp] = L
     return _libs[omp]
 
@@ -139,6 +141,11 @@ class RefScene:
         """updateOptiVolume + mergeLiquidParticles after srand(seed); returns
         the particles removed (draws in "merge_selector", "merge_perm")."""
         return self.L.wcref_merge(self.h, seed, step)
+
+    def split(self, seed: int) -> int:
+        """updateOptiVolume + splitLiquidParticles after srand(seed);
+        returns the particles added."""
+        return self.L.wcref_split(self.h, seed)
 
     def transfer(self, dt: float) -> None:
         """Grid, P2G, then G2P from the P2G velocities and advection (no

@@ -726,6 +726,36 @@ int wcref_merge(void* hp, unsigned seed, int step) {
   return before - np;
 }
 
+// TwoDScene::updateOptiVolume and splitLiquidParticles, as
+// WetClothCore::stepSystem runs them before a step's grid build; the
+// children's rotations come from Matrix3s::Random() (rand()), seeded by
+// srand(seed).  Returns the particles added.
+int wcref_split(void* hp, unsigned seed) {
+  Harness* h = (Harness*)hp;
+  TwoDScene& s = *h->scene;
+  s.updateOptiVolume();
+  srand(seed);
+  const int before = s.getNumParticles();
+  s.splitLiquidParticles();
+  snap_particles(*h, "split_");
+  const int np = s.getNumParticles();
+  std::vector<double>& vol = h->f["split_vol"];
+  std::vector<double>& mass = h->f["split_mass"];
+  std::vector<double>& rad = h->f["split_radius"];
+  std::vector<long long>& cls = h->ii["split_class"];
+  vol.assign(np, 0.0);
+  mass.assign(np, 0.0);
+  rad.assign(np, 0.0);
+  cls.assign(np, 0);
+  for (int i = 0; i < np; ++i) {
+    vol[i] = s.m_fluid_vol(i);
+    mass[i] = s.m_fluid_m(i * 4);
+    rad[i] = s.m_radius(i * 2);
+    cls[i] = (long long)s.m_classifier[i];
+  }
+  return np - before;
+}
+
 // implicit liquid viscosity: LiquidInfo::compute_viscosity and
 // implicit_viscosity on, viscosity mu, the stepper's viscosity sub-steps and
 // viscous criterion (call before the first step)

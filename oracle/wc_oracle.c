@@ -38,6 +38,7 @@ typedef struct {
   int corr_step;
   double cell_mult; /* LiquidInfo::particle_cell_multiplier */
   int merge_on;     /* relabel + mergeLiquidParticles before each sub-step */
+  int split_on;     /* relabel + splitLiquidParticles before each sub-step */
 } Params;
 
 typedef struct {
@@ -102,6 +103,7 @@ typedef struct {
   int corr_sel_once;              /* >= 0: selector of the next correction */
   unsigned char* cls;             /* m_classifier of the liquid particles */
   uint64_t merge_seed, merge_count; /* draw stream of the merge */
+  uint64_t split_seed, split_count; /* draw stream of the split */
   Snap snaps[256];
   int nsnaps;
 } Scene;
@@ -2019,6 +2021,167 @@ void wco_set_merge(Scene* s, int on, uint64_t seed, double cell_mult) {
   s->p.cell_mult = cell_mult;
 }
 
+/* point i of n on the unit sphere (spherical Fibonacci lattice, golden angle
+ * pi (3 - sqrt 5)): the children's pattern of the particle split */
+static void sphere_point(int n, int i, double* p) {
+  const double y = 1.0 - (2.0 * i + 1.0) / (double)n;
+  const double r = sqrt(1.0 - y * y);
+  const double phi = (double)i * 2.3999632297286533;
+  p[0] = r * cos(phi);
+  p[1] = y;
+  p[2] = r * sin(phi);
+}
+
+/* rotation of a split parent: a uniform random unit quaternion (Shoemake,
+ * Graphics Gems III, 1992) from SplitMix64 draws of key */
+static void split_rotation(uint64_t key, double* Q) {
+  uint64_t z = splitmix64(key);
+  const double u1 = (double)(z >> 11) * (1.0 / 9007199254740992.0);
+  z = splitmix64(z);
+  const double u2 = (double)(z >> 11) * (1.0 / 9007199254740992.0);
+  z = splitmix64(z);
+  const double u3 = (double)(z >> 11) * (1.0 / 9007199254740992.0);
+  const double a = sqrt(1.0 - u1), b = sqrt(u1);
+  const double tp = 6.283185307179586;
+  const double w = a * sin(tp * u2), x = a * cos(tp * u2), y = b * sin(tp * u3),
+               zq = b * cos(tp * u3);
+  Q[0] = 1.0 - 2.0 * (y * y + zq * zq);
+  Q[1] = 2.0 * (x * y - zq * w);
+  Q[2] = 2.0 * (x * zq + y * w);
+  Q[3] = 2.0 * (x * y + zq * w);
+  Q[4] = 1.0 - 2.0 * (x * x + zq * zq);
+  Q[5] = 2.0 * (y * zq - x * w);
+  Q[6] = 2.0 * (x * zq - y * w);
+  Q[7] = 2.0 * (y * zq + x * w);
+  Q[8] = 1.0 - 2.0 * (x * x + y * y);
+}
+
+/* the key of split call k of a seeded stream */
+uint64_t wco_split_key(uint64_t seed, uint64_t k) {
+  return splitmix64(seed ^ splitmix64(k ^ 0x73706c69742d6b65ull));
+}
+
+static double* grow_d(double* a, int w, int oldn, int newn) {
+  double* b = (double*)calloc((size_t)w * (size_t)(newn > 0 ? newn : 1), sizeof(double));
+  if (a) memcpy(b, a, sizeof(double) * (size_t)w * (size_t)oldn);
+  free(a);
+  return b;
+}
+
+/* TwoDScene::splitLiquidParticles (TwoDScene.cpp:2362-2480) after
+ * updateOptiVolume's relabelling: every large (L) liquid particle splits
+ * into n = min(ceil(V / V_fine), 32) particles of volume V/n and radius
+ * (3 V / (4 pi n))^(1/3); the parent moves to centre + p_0 s and its n - 1
+ * children, appended after all particles in the parents' index order, sit at
+ * centre + Q p_i s, s = 0.75 max(r_new, r - r_new), with the parent's
+ * velocity and a zero affine matrix.  The pattern p_i and the rotation Q are
+ * this library's (sphere_point, split_rotation with the parent's key
+ * splitmix64(key ^ fluid index)); the reference takes p_i from its
+ * compiled pattern table and Q from Matrix3s::Random().  Returns the number
+ * of particles added. */
+int wco_split_liquid(Scene* s, uint64_t key) {
+  if (s->np == s->ne) return 0;
+  relabel(s);
+  const double vf = fine_volume(s);
+  const int np = s->np, nf = s->np - s->ne;
+  int* add = (int*)calloc((size_t)nf, sizeof(int));
+  int total = 0;
+  for (int f = 0; f < nf; ++f) {
+    const int p = s->ne + f;
+    if (s->cls[p] != PCL_L) continue;
+    int n = (int)ceil(s->vol[p] / vf);
+    if (n > 32) n = 32;
+    if (n <= 1) continue;
+    add[f] = n - 1;
+    total += n - 1;
+  }
+  if (total == 0) {
+    free(add);
+    return 0;
+  }
+  const int nn = np + total;
+  s->x = grow_d(s->x, 3, np, nn);
+  s->v = grow_d(s->v, 3, np, nn);
+  s->C = grow_d(s->C, 9, np, nn);
+  s->m = grow_d(s->m, 1, np, nn);
+  s->vol = grow_d(s->vol, 1, np, nn);
+  s->rad = grow_d(s->rad, 1, np, nn);
+  if (s->em) {
+    s->em = grow_d(s->em, 3, np, nn);
+    s->rvol = grow_d(s->rvol, 1, np, nn);
+    s->rvf = grow_d(s->rvf, 1, np, nn);
+    s->sf = grow_d(s->sf, 1, np, nn);
+    s->ori = grow_d(s->ori, 3, np, nn);
+    s->xt = grow_d(s->xt, 1, np, nn);
+    s->vt = grow_d(s->vt, 1, np, nn);
+    unsigned char* su = (unsigned char*)calloc((size_t)nn, 1);
+    memcpy(su, s->surf, (size_t)np);
+    free(s->surf);
+    s->surf = su;
+  }
+  int next = np;
+  for (int f = 0; f < nf; ++f) {
+    if (!add[f]) continue;
+    const int p = s->ne + f;
+    const int n = add[f] + 1;
+    const double c[3] = {s->x[p * 3], s->x[p * 3 + 1], s->x[p * 3 + 2]};
+    const double rad = s->rad[p];
+    const double new_vol = s->vol[p] / (double)n;
+    const double new_rad = pow(new_vol / M_PI * 0.75, 1.0 / 3.0);
+    const double splat = (new_rad > rad - new_rad ? new_rad : rad - new_rad) * 0.75;
+    double Q[9];
+    split_rotation(splitmix64(key ^ (uint64_t)f), Q);
+    for (int i = 1; i < n; ++i) {
+      double pt[3];
+      sphere_point(n, i, pt);
+      const int q = next++;
+      for (int a = 0; a < 3; ++a) {
+        const double rq = Q[a * 3] * pt[0] + Q[a * 3 + 1] * pt[1] + Q[a * 3 + 2] * pt[2];
+        s->x[q * 3 + a] = c[a] + rq * splat;
+        s->v[q * 3 + a] = s->v[p * 3 + a];
+      }
+      for (int r = 0; r < 9; ++r) s->C[q * 9 + r] = 0.0;
+      s->m[q] = new_vol * s->p.rho;
+      s->vol[q] = new_vol;
+      s->rad[q] = new_rad;
+    }
+    double p0[3];
+    sphere_point(n, 0, p0);
+    for (int a = 0; a < 3; ++a) s->x[p * 3 + a] = c[a] + p0[a] * splat;
+    s->rad[p] = new_rad;
+    s->vol[p] = new_vol;
+    s->m[p] = new_vol * s->p.rho;
+  }
+  s->np = nn;
+  free(add);
+  relabel(s);
+  free(s->keys);
+  s->keys = NULL;
+  {
+    double* t = (double*)malloc(sizeof(double) * (size_t)nn);
+    long long* c = (long long*)malloc(sizeof(long long) * (size_t)nn);
+    snap_particles(s, "split_");
+    memcpy(t, s->vol, sizeof(double) * (size_t)nn);
+    snap_put_f(s, "split_vol", t, nn);
+    memcpy(t, s->m, sizeof(double) * (size_t)nn);
+    snap_put_f(s, "split_mass", t, nn);
+    memcpy(t, s->rad, sizeof(double) * (size_t)nn);
+    snap_put_f(s, "split_radius", t, nn);
+    for (int p = 0; p < nn; ++p) c[p] = s->cls[p];
+    snap_put_i(s, "split_class", c, nn);
+    free(t);
+    free(c);
+  }
+  return total;
+}
+
+/* split before each sub-step with the seeded keys */
+void wco_set_split(Scene* s, int on, uint64_t seed) {
+  s->p.split_on = on;
+  s->split_seed = seed;
+  s->split_count = 0;
+}
+
 /* correctLiquidParticles with an explicit particle subset, outside a step */
 void wco_correct_liquid(Scene* s, double dt, int selector) { correct_liquid(s, dt, selector); }
 
@@ -2205,6 +2368,15 @@ static void transfer_out(Scene* s, double dt, int snapshot) {
 
 /* one sub-step in WetClothCore::stepSystem order (WetClothCore.cpp:97-258) */
 int wco_substep(Scene* s, double dt, int snapshot) {
+  /* updateOptiVolume, splitLiquidParticles, mergeLiquidParticles
+   * (WetClothCore.cpp:97-110); a split that adds particles re-sorts the
+   * buckets (TwoDScene.cpp:2471-2478), so the merge after it sees the new
+   * positions in the buckets of the last grid build */
+  if (s->p.split_on && s->np > s->ne) {
+    const long long nadd = wco_split_liquid(s, wco_split_key(s->split_seed, s->split_count++));
+    snap_put_i(s, "split_added", &nadd, 1);
+    if (nadd > 0 && s->p.merge_on) sort_particles(s);
+  }
   if (s->p.merge_on && s->keys && s->np > s->ne) {
     int sel, perm[9];
     wco_merge_draws(s->merge_seed, s->merge_count++, s->p.corr_step, &sel, perm);

@@ -324,3 +324,40 @@ def test_particle_merge(kind, seed):
         a, b = r.get(k), o.get(k)
         assert a.shape == b.shape, k
         assert np.abs(a - b).max() <= 1e-12 * np.abs(a).max(), k
+
+
+@pytest.mark.parametrize("kind,seed", [("dam16", 3), ("curl16", 5)])
+def test_particle_split(kind, seed):
+    """updateOptiVolume + splitLiquidParticles (TwoDScene.cpp:2362-2480) after
+    a step, on particles of mixed volume up to 40 V_fine (splits into up to 32):
+    the number of children, their order (appended parent by parent), volumes,
+    masses, radii, velocities, zero affine matrices and the classes match the
+    reference to 1e-12, and every particle that did not split keeps its
+    position.  The children's positions are not compared: the reference
+    places them on its compiled sphere-pattern table rotated by
+    Matrix3s::Random(), the oracle (and the GPU) on a Fibonacci lattice rotated
+    by a seeded quaternion; both put them at distance |p_i| s from the
+    parent's centre."""
+    sc = _scene(kind)
+    scenes.mixed_volumes(sc, seed, mrel=(0.3, 1.0, 2.5, 7.0, 40.0))
+    r = oref.RefScene(sc, mic=True)
+    o = oo.OracleScene(sc)
+    r.step(DT, snapshot=True)
+    o.step(DT, snapshot=True)
+    added = r.split(seed)
+    assert added > 0
+    assert o.split(seed * 7919 + 1) == added
+    for k in ("split_v", "split_C", "split_vol", "split_mass", "split_radius"):
+        a, b = r.get(k), o.get(k)
+        assert a.shape == b.shape, k
+        assert np.abs(a - b).max() <= 1e-12 * np.abs(a).max(), k
+    assert np.array_equal(r.get("split_class"), o.get("split_class"))
+    n0 = sc.x.shape[0]
+    before = r.get("adv_x").reshape(-1, 3)
+    xr = r.get("split_x").reshape(-1, 3)
+    xo = o.get("split_x").reshape(-1, 3)
+    still = np.abs(xr[:n0] - before).max(axis=1) == 0
+    assert still.sum() > 0 and (~still).sum() > 0
+    assert np.array_equal(xo[:n0][still], xr[:n0][still])
+    # children of the oracle sit within 0.75 max(r_new, r - r_new) of their parent's centre
+    assert np.all(np.abs(xo[n0:]).max() <= 2.0)
