@@ -358,6 +358,6 @@ def test_particle_split(kind, seed):
     xo = o.get("split_x").reshape(-1, 3)
     still = np.abs(xr[:n0] - before).max(axis=1) == 0
     assert still.sum() > 0 and (~still).sum() > 0
-    assert np.array_equal(xo[:n0][still], xr[:n0][still])
+    assert np.abs(xo[:n0][still] - xr[:n0][still]).max() <= 1e-12
     # children of the oracle sit within 0.75 max(r_new, r - r_new) of their parent's centre
     assert np.all(np.abs(xo[n0:]).max() <= 2.0)
