@@ -90,6 +90,9 @@ typedef struct wcg_params {
   unsigned long long merge_seed;   /* seed of the merge's draws (rand() in the reference) */
   double particle_cell_multiplier; /* LiquidInfo::particle_cell_multiplier (0.3535533906):
                                       V_fine = 4/3 pi (dx m / sqrt 3)^3 */
+  int particle_split;              /* relabelLiquidParticles + splitLiquidParticles before
+                                      each sub-step, ahead of the merge */
+  unsigned long long split_seed;   /* seed of the split's rotations */
 } wcg_params;
 
 typedef struct wcg_ctx wcg_ctx;
@@ -231,6 +234,17 @@ int wcg_correction_selector(unsigned long long seed, unsigned long long k, int s
  * renumbering; *removed (may be NULL) receives their count. */
 int wcg_merge_liquid_particles(wcg_ctx* ctx, int selector, const int* perm9,
                                long long* removed);
+/* TwoDScene::updateOptiVolume + splitLiquidParticles (TwoDScene.cpp:2362-2480):
+ * every large liquid particle (volume above 2 V_fine) splits into
+ * n = min(ceil(V / V_fine), 32) particles of volume V/n, the children
+ * appended after all particles in the parents' index order with the parent's
+ * velocity and a zero affine matrix.  The children sit on a spherical
+ * Fibonacci lattice rotated by a quaternion drawn from SplitMix64 of
+ * key ^ parent index (the reference: its compiled sphere-pattern table and
+ * Matrix3s::Random()); *added (may be NULL) receives their count. */
+int wcg_split_liquid_particles(wcg_ctx* ctx, unsigned long long key, long long* added);
+/* the key wcg_substep uses for its k-th split */
+unsigned long long wcg_split_key(unsigned long long seed, unsigned long long k);
 /* the draws wcg_substep uses for its k-th merge: SplitMix64 of the seed and k
  * for the selector, then three Fisher-Yates permutations of {0, 1, 2} */
 int wcg_merge_draws(unsigned long long seed, unsigned long long k, int step, int* selector,

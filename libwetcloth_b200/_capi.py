@@ -62,6 +62,8 @@ class WcgParams(ctypes.Structure):
         ("particle_merge", ctypes.c_int),
         ("merge_seed", ctypes.c_ulonglong),
         ("particle_cell_multiplier", ctypes.c_double),
+        ("particle_split", ctypes.c_int),
+        ("split_seed", ctypes.c_ulonglong),
     ]
 
 
@@ -119,6 +121,9 @@ SIGNATURES = {
     "wcg_merge_liquid_particles": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
                                                   ctypes.POINTER(ctypes.c_int),
                                                   ctypes.POINTER(ctypes.c_longlong)]),
+    "wcg_split_liquid_particles": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_ulonglong,
+                                                  ctypes.POINTER(ctypes.c_longlong)]),
+    "wcg_split_key": (ctypes.c_ulonglong, [ctypes.c_ulonglong, ctypes.c_ulonglong]),
     "wcg_merge_draws": (ctypes.c_int, [ctypes.c_ulonglong, ctypes.c_ulonglong, ctypes.c_int,
                                        ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     "wcg_download_liquid_async": (ctypes.c_int, [ctypes.c_void_p, _D, _D, _D]),

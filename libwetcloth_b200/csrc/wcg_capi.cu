@@ -199,6 +199,8 @@ void wcg_default_params(wcg_params* p) {
   p->viscosity_criterion = 1e-6;
   p->particle_merge = 0;
   p->merge_seed = 0;
+  p->particle_split = 0;
+  p->split_seed = 0;
   p->particle_cell_multiplier = 0.3535533906;
 }
 
@@ -261,6 +263,8 @@ int wcg_create(const wcg_params* params, wcg_ctx** out) {
   p.viscosity_implicit = params->viscosity_implicit ? 1 : 0;
   p.particle_merge = params->particle_merge ? 1 : 0;
   p.merge_seed = params->merge_seed;
+  p.particle_split = params->particle_split ? 1 : 0;
+  p.split_seed = params->split_seed;
   p.cell_multiplier = params->particle_cell_multiplier;
   p.viscosity_criterion = params->viscosity_criterion;
   // wavefront tile shape (performance knob; both compute identical results)
@@ -592,6 +596,18 @@ int wcg_merge_liquid_particles(wcg_ctx* ctx, int selector, const int* perm9,
   return device_status(ctx->c, "mergeLiquidParticles");
 }
 
+int wcg_split_liquid_particles(wcg_ctx* ctx, unsigned long long key, long long* added) {
+  WCG_CHECK_CTX(ctx);
+  long long add = 0;
+  WCG_CALL(ctx, wcg::split_liquid_particles(ctx->c, key, &add), "splitLiquidParticles");
+  if (added) *added = add;
+  return device_status(ctx->c, "splitLiquidParticles");
+}
+
+unsigned long long wcg_split_key(unsigned long long seed, unsigned long long k) {
+  return wcg::split_key(seed, k);
+}
+
 int wcg_merge_draws(unsigned long long seed, unsigned long long k, int step, int* selector,
                     int* perm9) {
   if (!selector || !perm9 || step < 1) return fail(WCG_ERR_ARG, "bad merge draw arguments");
@@ -634,8 +650,9 @@ int wcg_substep_vjp(wcg_ctx* ctx, double dt, const double* vbar3, const double* 
     return fail(WCG_ERR_UNSUPPORTED, "substep_vjp: not available with the particle correction on");
   if (ctx->c.prm.viscosity > 0.0 && ctx->c.prm.viscosity_implicit)
     return fail(WCG_ERR_UNSUPPORTED, "substep_vjp: not available with the implicit viscosity");
-  if (ctx->c.prm.particle_merge)
-    return fail(WCG_ERR_UNSUPPORTED, "substep_vjp: not available with the particle merge on");
+  if (ctx->c.prm.particle_merge || ctx->c.prm.particle_split)
+    return fail(WCG_ERR_UNSUPPORTED,
+                "substep_vjp: not available with the particle merge or split on");
   const long long n = ctx->c.np;
   if (n > 0 && (!vbar3 || !Cbar9 || !xbar3 || !vbar0 || !Cbar0 || !xbar0))
     return fail(WCG_ERR_ARG, "null cotangent array");

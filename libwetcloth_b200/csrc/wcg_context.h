@@ -42,6 +42,8 @@ struct Params {
   double correction_multiplier;  // LiquidInfo::correction_multiplier
   unsigned long long correction_seed;  // seed of the per-sub-step subset stream
   int particle_merge;            // relabel + mergeLiquidParticles before each sub-step
+  int particle_split;            // relabel + splitLiquidParticles before each sub-step
+  unsigned long long split_seed; // seed of the split's rotations
   unsigned long long merge_seed; // seed of the merge's draws
   double cell_multiplier;        // LiquidInfo::particle_cell_multiplier (V_fine)
 };
@@ -264,6 +266,7 @@ struct Context {
   // momentum, index maps; the merge's draw counter
   DevBuf mwork;
   unsigned long long merge_count = 0;
+  unsigned long long split_count = 0;
   long long merged_removed = 0;  // particles the last merge removed
 
   // reverse mode of a sub-step (wcg_adjoint.cuh): grid cotangents, particle
@@ -380,6 +383,10 @@ int correction_selector(unsigned long long seed, unsigned long long k, int step)
 // buckets of the last grid build, with the given subset and colour order
 // (perm: t, s, r permutations of {0, 1, 2}); *removed = particles removed
 cudaError_t merge_liquid_particles(Context& c, int selector, const int* perm, long long* removed);
+// splitLiquidParticles with the rotations of key (after relabelling);
+// *added = particles appended
+cudaError_t split_liquid_particles(Context& c, unsigned long long key, long long* added);
+unsigned long long split_key(unsigned long long seed, unsigned long long k);
 // draws of merge call k of a seeded stream: selector, then three Fisher-Yates
 // permutations of {0, 1, 2}
 void merge_draws(unsigned long long seed, unsigned long long k, int step, int* selector, int* perm);

@@ -16,6 +16,8 @@
 
 #include "wcg_common.cuh"
 #include "wcg_context.h"
+#include "wcg_correct.cuh"
+#include "wcg_kernels.cuh"
 
 namespace wcg {
 
@@ -226,6 +228,122 @@ __global__ void k_merge_compact(long long np, const int* __restrict__ alive_slot
   const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= np || !alive_slot[s]) return;
   perm[rank[s]] = (int)s;
+}
+
+// ---- particle split: TwoDScene::splitLiquidParticles (TwoDScene.cpp:2362-2480)
+
+// point i of n on the unit sphere (spherical Fibonacci lattice)
+__host__ __device__ inline void sphere_point(int n, int i, double* p) {
+  const double y = 1.0 - (2.0 * i + 1.0) / (double)n;
+  const double r = sqrt(1.0 - y * y);
+  const double phi = (double)i * 2.3999632297286533;
+  p[0] = r * cos(phi);
+  p[1] = y;
+  p[2] = r * sin(phi);
+}
+
+// rotation of a split parent: a uniform random unit quaternion (Shoemake,
+// Graphics Gems III, 1992) from SplitMix64 draws of key
+__host__ __device__ inline void split_rotation(unsigned long long key, double* Q) {
+  unsigned long long z = splitmix64(key);
+  const double u1 = (double)(z >> 11) * (1.0 / 9007199254740992.0);
+  z = splitmix64(z);
+  const double u2 = (double)(z >> 11) * (1.0 / 9007199254740992.0);
+  z = splitmix64(z);
+  const double u3 = (double)(z >> 11) * (1.0 / 9007199254740992.0);
+  const double a = sqrt(1.0 - u1), b = sqrt(u1);
+  const double tp = 6.283185307179586;
+  const double w = a * sin(tp * u2), x = a * cos(tp * u2), y = b * sin(tp * u3),
+               zq = b * cos(tp * u3);
+  Q[0] = 1.0 - 2.0 * (y * y + zq * zq);
+  Q[1] = 2.0 * (x * y - zq * w);
+  Q[2] = 2.0 * (x * zq + y * w);
+  Q[3] = 2.0 * (x * y + zq * w);
+  Q[4] = 1.0 - 2.0 * (x * x + zq * zq);
+  Q[5] = 2.0 * (y * zq - x * w);
+  Q[6] = 2.0 * (x * zq - y * w);
+  Q[7] = 2.0 * (y * zq + x * w);
+  Q[8] = 1.0 - 2.0 * (x * x + y * y);
+}
+
+// children per large particle, n = min(ceil(V / V_fine), 32), by slot and by
+// original index
+template <typename R>
+__global__ void k_split_count(const R* __restrict__ P, long long pcap, long long np,
+                              const int* __restrict__ pid, double vf, int* __restrict__ add_slot,
+                              int* __restrict__ add_pid) {
+  const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= np) return;
+  const R vol = P[PV * pcap + s];
+  int add = 0;
+  if (particle_class<R>(vol, vf) == PCL_L) {
+    int n = (int)ceil((double)vol / vf);
+    n = n > 32 ? 32 : n;
+    add = n > 1 ? n - 1 : 0;
+  }
+  add_slot[s] = add;
+  add_pid[pid[s]] = add;
+}
+
+// the parent moves to centre + p_0 s and takes volume V/n; its children are
+// appended at np + (exclusive sum of the children of lower original index)
+template <typename R>
+__global__ void k_split(R* P, long long pcap, long long np, int* pid,
+                        const int* __restrict__ add_slot, const int* __restrict__ off_pid,
+                        unsigned long long key, double rho) {
+  const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= np) return;
+  const int add = add_slot[s];
+  if (add == 0) return;
+  const int f = pid[s];
+  const int n = add + 1;
+  const double c[3] = {(double)P[PX * pcap + s], (double)P[PY * pcap + s],
+                       (double)P[PZ * pcap + s]};
+  const double rad = (double)P[PR * pcap + s];
+  const double new_vol = (double)P[PV * pcap + s] / (double)n;
+  const double new_rad = pow(new_vol / M_PI * 0.75, 1.0 / 3.0);
+  const double splat = (new_rad > rad - new_rad ? new_rad : rad - new_rad) * 0.75;
+  double Q[9];
+  split_rotation(splitmix64(key ^ (unsigned long long)f), Q);
+  const long long base = np + off_pid[f];
+  for (int i = 1; i < n; ++i) {
+    double pt[3];
+    sphere_point(n, i, pt);
+    const long long q = base + i - 1;
+    for (int a = 0; a < 3; ++a) {
+      const double rq = Q[a * 3] * pt[0] + Q[a * 3 + 1] * pt[1] + Q[a * 3 + 2] * pt[2];
+      P[(PX + a) * pcap + q] = (R)(c[a] + rq * splat);
+      P[(VX + a) * pcap + q] = P[(VX + a) * pcap + s];
+    }
+    for (int r = 0; r < 9; ++r) P[(C00 + r) * pcap + q] = R(0);
+    P[PM * pcap + q] = (R)(new_vol * rho);
+    P[PV * pcap + q] = (R)new_vol;
+    P[PR * pcap + q] = (R)new_rad;
+    pid[q] = (int)q;
+  }
+  double p0[3];
+  sphere_point(n, 0, p0);
+  for (int a = 0; a < 3; ++a) P[(PX + a) * pcap + s] = (R)(c[a] + p0[a] * splat);
+  P[PR * pcap + s] = (R)new_rad;
+  P[PV * pcap + s] = (R)new_vol;
+  P[PM * pcap + s] = (R)(new_vol * rho);
+}
+
+// bucket of every particle's current position in the last build's bucket grid
+// (the re-sort at the end of splitLiquidParticles, TwoDScene.cpp:2471-2478)
+template <typename R>
+__global__ void k_rebucket(const R* __restrict__ P, long long pcap, long long np, GridDesc g,
+                           int* __restrict__ pbucket) {
+  const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= np) return;
+  const R org[3] = {(R)g.ox, (R)g.oy, (R)g.oz};
+  const int nbk[3] = {g.ni, g.nj, g.nk};
+  int h[3];
+  for (int a = 0; a < 3; ++a) {
+    int v = (int)floor(div_rn(sub_rn(P[(PX + a) * pcap + s], org[a]), (R)g.bs));
+    h[a] = v < 0 ? 0 : (v > nbk[a] - 1 ? nbk[a] - 1 : v);
+  }
+  pbucket[s] = (h[2] * g.nj + h[1]) * g.ni + h[0];
 }
 
 }  // namespace wcg

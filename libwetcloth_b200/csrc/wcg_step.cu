@@ -2454,14 +2454,99 @@ static cudaError_t merge_liquid_t(Context& c, int selector, const int* perm, lon
   return cudaStreamSynchronize(c.stream);
 }
 
+unsigned long long split_key(unsigned long long seed, unsigned long long k) {
+  return splitmix64(seed ^ splitmix64(k ^ 0x73706c69742d6b65ull));
+}
+
+// grows the particle capacity to cap, keeping the state of the current half
+// (columns, original indices); the other buffers are re-sized empty
+static cudaError_t grow_particles(Context& c, long long cap) {
+  if (cap <= c.pcap) return cudaSuccess;
+  const int rb = c.real_bytes();
+  const long long n = c.np;
+  DevBuf nb, np_;
+  WCG_TRY(nb.ensure((size_t)kNumPCols * cap * rb));
+  WCG_TRY(np_.ensure((size_t)cap * sizeof(int)));
+  for (int col = 0; col < kNumPCols; ++col)
+    WCG_TRY(cudaMemcpyAsync((char*)nb.p + (size_t)col * cap * rb,
+                            (const char*)c.pbuf[c.cur].p + (size_t)col * c.pcap * rb,
+                            (size_t)n * rb, cudaMemcpyDeviceToDevice, c.stream));
+  WCG_TRY(cudaMemcpyAsync(np_.p, c.pid[c.cur].p, (size_t)n * sizeof(int),
+                          cudaMemcpyDeviceToDevice, c.stream));
+  WCG_TRY(cudaStreamSynchronize(c.stream));
+  c.pbuf[c.cur].release();
+  c.pid[c.cur].release();
+  c.pbuf[c.cur] = nb;
+  c.pid[c.cur] = np_;
+  const int o = c.cur ^ 1;
+  WCG_TRY(c.pbuf[o].ensure((size_t)kNumPCols * cap * rb));
+  WCG_TRY(c.pid[o].ensure((size_t)cap * sizeof(int)));
+  // keys, offsets and buckets are rebuilt by the next grid build
+  WCG_TRY(c.pkey.ensure((size_t)2 * cap * sizeof(long long)));
+  WCG_TRY(c.pdelta.ensure((size_t)2 * cap * sizeof(int)));
+  WCG_TRY(c.pbucket.ensure((size_t)2 * cap * sizeof(int)));
+  WCG_TRY(c.perm.ensure((size_t)cap * sizeof(int)));
+  WCG_TRY(c.hostorder.ensure((size_t)cap * 15 * sizeof(double)));
+  c.pcap = cap;
+  return cudaSuccess;
+}
+
+template <typename R>
+static cudaError_t split_liquid_t(Context& c, unsigned long long key, long long* added) {
+  *added = 0;
+  const long long n = c.np;
+  if (n == 0) return cudaSuccess;
+  ProfScope prof(c, P_OTHER);
+  const double rad_fine = 1.0 / std::sqrt(3.0) * c.prm.dx * c.prm.cell_multiplier;
+  const double vf = 4.0 / 3.0 * M_PI * rad_fine * rad_fine * rad_fine;
+  WCG_TRY(c.corr_cursor.ensure((size_t)(n + 1) * sizeof(int)));
+  WCG_TRY(c.corr_list.ensure((size_t)(n + 1) * sizeof(int)));
+  const long long scan_tiles = (n + 1 + kScanTile - 1) / kScanTile + 1;
+  WCG_TRY(ensure_scratch(c, (size_t)scan_tiles * sizeof(long long) + 64));
+  int* add_slot = c.corr_cursor.as<int>();
+  int* off_pid = c.corr_list.as<int>();
+  ++c.launches, k_split_count<R><<<nblk(n, 256), 256, 0, c.stream>>>(
+      c.pbuf[c.cur].as<R>(), c.pcap, n, c.pid[c.cur].as<int>(), vf, add_slot, off_pid);
+  int* dtot = (int*)(c.dscalars.as<double>() + 50);
+  exclusive_scan<int, int>(off_pid, n, off_pid, c.scratch.as<int>(), dtot, c.stream);
+  int total = 0;
+  WCG_TRY(cudaMemcpyAsync(&total, dtot, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  WCG_TRY(cudaStreamSynchronize(c.stream));
+  if (total == 0) return cudaGetLastError();
+  if (n + total > 2000000000ll) return cudaErrorInvalidValue;
+  WCG_TRY(grow_particles(c, n + total));
+  ++c.launches, k_split<R><<<nblk(n, 128), 128, 0, c.stream>>>(
+      c.pbuf[c.cur].as<R>(), c.pcap, n, c.pid[c.cur].as<int>(), add_slot, off_pid, key,
+      c.prm.liquid_density);
+  c.np = n + total;
+  c.have_grid = false;
+  c.xw_valid = false;
+  if (c.g.nb > 0)
+    ++c.launches, k_rebucket<R><<<nblk(c.np, 256), 256, 0, c.stream>>>(
+        c.pbuf[c.cur].as<R>(), c.pcap, c.np, c.g, c.pbucket.as<int>() + c.cur * c.pcap);
+  *added = total;
+  WCG_TRY(cudaGetLastError());
+  return cudaStreamSynchronize(c.stream);
+}
+
+cudaError_t split_liquid_particles(Context& c, unsigned long long key, long long* added) {
+  return c.prm.precision == 0 ? split_liquid_t<double>(c, key, added)
+                              : split_liquid_t<float>(c, key, added);
+}
+
 cudaError_t merge_liquid_particles(Context& c, int selector, const int* perm, long long* removed) {
   return c.prm.precision == 0 ? merge_liquid_t<double>(c, selector, perm, removed)
                               : merge_liquid_t<float>(c, selector, perm, removed);
 }
 
 cudaError_t substep(Context& c, double dt) {
-  // updateOptiVolume + mergeLiquidParticles (WetClothCore.cpp:97-110), on the
-  // buckets of the previous sub-step's grid build
+  // updateOptiVolume, splitLiquidParticles, mergeLiquidParticles
+  // (WetClothCore.cpp:97-110): the merge works on the buckets of the previous
+  // sub-step's grid build, re-sorted by a split that added particles
+  if (c.prm.particle_split && c.np > 0) {
+    long long added = 0;
+    WCG_TRY(split_liquid_particles(c, split_key(c.prm.split_seed, c.split_count++), &added));
+  }
   if (c.prm.particle_merge && c.np > 0 && c.g.nb > 0) {
     int sel = 0, perm[9];
     merge_draws(c.prm.merge_seed, c.merge_count++, c.prm.correction_step, &sel, perm);

@@ -45,6 +45,8 @@ def make_params(p, precision=_capi.WCG_FP64, refine_inner_tol=0.0,
     prm.viscosity_implicit = 1 if getattr(p, "viscosity_implicit", False) else 0
     prm.viscosity_criterion = getattr(p, "viscosity_criterion", 1e-6)
     prm.particle_merge = 1 if getattr(p, "particle_merge", False) else 0
+    prm.particle_split = 1 if getattr(p, "particle_split", False) else 0
+    prm.split_seed = getattr(p, "split_seed", 0)
     prm.merge_seed = getattr(p, "merge_seed", 0)
     prm.particle_cell_multiplier = getattr(p, "particle_cell_multiplier", 0.3535533906)
     prm.correction_strength = getattr(p, "correction_strength", 0.0)
@@ -188,6 +190,13 @@ class FluidScene:
 
     def constrain_liquid_velocity(self):
         check(self.L.wcg_constrain_liquid_velocity(self.h))
+
+    def split_liquid_particles(self, key):
+        """relabel + splitLiquidParticles with the rotations of key; returns
+        the number of particles added."""
+        add = ctypes.c_longlong(0)
+        check(self.L.wcg_split_liquid_particles(self.h, int(key), ctypes.byref(add)))
+        return add.value
 
     def merge_liquid_particles(self, selector, perm):
         """relabel + mergeLiquidParticles + removeEmptyParticles with the given

@@ -2375,7 +2375,7 @@ int wco_substep(Scene* s, double dt, int snapshot) {
   if (s->p.split_on && s->np > s->ne) {
     const long long nadd = wco_split_liquid(s, wco_split_key(s->split_seed, s->split_count++));
     snap_put_i(s, "split_added", &nadd, 1);
-    if (nadd > 0 && s->p.merge_on) sort_particles(s);
+    if (nadd > 0 && s->p.merge_on && s->nb > 0) sort_particles(s);
   }
   if (s->p.merge_on && s->keys && s->np > s->ne) {
     int sel, perm[9];

@@ -119,3 +119,19 @@ def test_merge_draw_stream():
                 assert sorted(pg[3 * q:3 * q + 3]) == [0, 1, 2]
             seen.add(tuple(pg[:3]))
     assert len(seen) == 6
+
+
+def test_split_key_stream():
+    """The split keys of wcg_step (host code) are the oracle's."""
+    L = _capi.load()
+    from oracle import oracle as oo
+    if not oo.available():
+        pytest.skip("oracle not built")
+    O = oo.lib()
+    keys = set()
+    for seed in (0, 5, 2**40 + 7):
+        for k in range(30):
+            a = L.wcg_split_key(seed, k)
+            assert a == O.wco_split_key(seed, k)
+            keys.add(a)
+    assert len(keys) == 90

@@ -104,3 +104,63 @@ def test_merge_arguments(wcg):
             g.merge_liquid_particles(sel, perm)
         assert e.value.code == _capi.WCG_ERR_ARG
     g.close()
+
+
+@pytest.mark.parametrize("kind,seed", [("dam16", 3), ("curl16", 5)])
+def test_split_after_step_fp64(kind, seed, wcg):
+    """splitLiquidParticles (seeded pattern and rotations, the same on both
+    sides): the particles added, their order, positions, velocities and
+    affine matrices to 1e-12, then a step that reads their volumes, masses
+    and radii."""
+    sc = _scene(kind, seed)
+    scenes.mixed_volumes(sc, seed, mrel=(0.3, 1.0, 2.5, 7.0, 40.0))
+    key = 0x9E3779B97F4A7C15 ^ seed
+    o = oo.OracleScene(sc)
+    o.step(DT, snapshot=True)
+    g = FluidScene(sc)
+    g.step(DT)
+    n0 = g.num_particles
+    added = g.split_liquid_particles(key)
+    assert added == o.split(key) and added > 0
+    assert g.num_particles == n0 + added
+    x, v, C = g.download()
+    _close(x, o.get("split_x"), 1e-12, "x")
+    _close(v, o.get("split_v"), 1e-12, "v")
+    _close(C, o.get("split_C"), 1e-12, "C")
+    o.step(DT, snapshot=True)
+    g.step(DT)
+    x, v, C = g.download()
+    _close(v, o.get("g2p_v"), 1e-10, "g2p_v")
+    _close(x, o.get("adv_x"), 1e-12, "adv_x")
+    g.close()
+
+
+def test_split_and_merge_seeded_steps(wcg):
+    """wcg_step with the split and the merge on (split first, the merge on
+    the re-sorted buckets), both sides drawing from the same seeded streams,
+    in FP64 and FP32; the particle count grows past the first capacity."""
+    sc = _scene("dam16", 13)
+    scenes.mixed_volumes(sc, 13, mrel=(0.3, 0.7, 1.0, 2.5, 7.0))
+    sc.params.particle_split = True
+    sc.params.split_seed = 21
+    sc.params.particle_merge = True
+    sc.params.merge_seed = 4
+    o = oo.OracleScene(sc)
+    g = FluidScene(sc)
+    g32 = FluidScene(sc, precision=_capi.WCG_FP32_REFINE)
+    n0 = sc.x.shape[0]
+    for _ in range(3):
+        o.step(DT, snapshot=True)
+        g.step(DT)
+        g32.step(DT)
+    n = int(o.get("adv_x").size // 3)
+    assert n > n0
+    assert g.num_particles == n and g32.num_particles == n
+    x, v, C = g.download()
+    _close(v, o.get("g2p_v"), 1e-10, "g2p_v")
+    _close(x, o.get("adv_x"), 1e-12, "adv_x")
+    x, v, C = g32.download()
+    _close(v, o.get("g2p_v"), 1e-5, "g2p_v fp32")
+    _close(x, o.get("adv_x"), 1e-6, "adv_x fp32")
+    g.close()
+    g32.close()
