@@ -225,6 +225,9 @@ int wcg_correct_liquid_particles(wcg_ctx* ctx, double dt, int selector);
 /* the subset wcg_substep corrects in its k-th call: SplitMix64 of the seed and
  * k, modulo step */
 int wcg_correction_selector(unsigned long long seed, unsigned long long k, int step);
+/* sets the call count of the correction stream: the next sub-step (and the
+ * sub-step wcg_substep_vjp differentiates) corrects the subset of call k */
+int wcg_set_correction_count(wcg_ctx* ctx, unsigned long long k);
 /* TwoDScene::updateOptiVolume (relabelLiquidParticles TwoDScene.cpp:2484-2505),
  * mergeLiquidParticles (:2510-2666) and removeEmptyParticles (:1713-1745) on
  * the buckets of the last grid build, for the liquid particles with index %
@@ -268,7 +271,12 @@ int wcg_num_substeps(wcg_ctx* ctx, double dt, int* n_out);
  * the inputs v (3n) and C (9n), of the liquid viscosity (viscosity_bar, may be
  * NULL; 0 when the viscosity is off); xbar0 = xbar3 (positions are held
  * fixed: the weights' dependence on x is not differentiated).  Liquid scenes;
- * the solve is the forward's solver on the same (symmetric) matrix. */
+ * the solve is the forward's solver on the same (symmetric) matrix.  The
+ * advection's solid projection is differentiated; with the particle
+ * correction on, the sub-step differentiated corrects the subset of the
+ * correction stream's next call (wcg_set_correction_count).  Refused
+ * (WCG_ERR_UNSUPPORTED) with elasto particles, the implicit viscosity, or the
+ * particle split or merge on. */
 int wcg_substep_vjp(wcg_ctx* ctx, double dt, const double* vbar3, const double* Cbar9,
                     const double* xbar3, double* vbar0, double* Cbar0, double* xbar0,
                     double* viscosity_bar);

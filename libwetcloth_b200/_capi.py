@@ -121,6 +121,7 @@ SIGNATURES = {
     "wcg_merge_liquid_particles": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
                                                   ctypes.POINTER(ctypes.c_int),
                                                   ctypes.POINTER(ctypes.c_longlong)]),
+    "wcg_set_correction_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_ulonglong]),
     "wcg_split_liquid_particles": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_ulonglong,
                                                   ctypes.POINTER(ctypes.c_longlong)]),
     "wcg_split_key": (ctypes.c_ulonglong, [ctypes.c_ulonglong, ctypes.c_ulonglong]),

@@ -48,7 +48,8 @@ __global__ void __launch_bounds__(128)
                const int* __restrict__ delta, const R* __restrict__ F, long long fstride,
                R flip, R friction, const int* __restrict__ pid,
                const double* __restrict__ vbar, const double* __restrict__ Cbar,
-               const double* __restrict__ xbar, double dt, R* __restrict__ B) {
+               const double* __restrict__ xbar, double dt, R* __restrict__ B,
+               const R* __restrict__ XC) {
   const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= np) return;
   const long long i = pid[s];
@@ -56,16 +57,18 @@ __global__ void __launch_bounds__(128)
   const long long kn = key[s];
   if (kn >= 0) {
     const R x[3] = {P[PX * pcap + s], P[PY * pcap + s], P[PZ * pcap + s]};
+    // the corrected position (the particle correction ran before G2P), or x
+    const R xc[3] = {XC ? XC[s] : x[0], XC ? XC[pcap + s] : x[1], XC ? XC[2 * pcap + s] : x[2]};
     int KI, KJ, KK;
     node_ijk(g, kn, KI, KJ, KK);
     const int kp[3] = {KI - 1, KJ - 1, KK - 1};
     const int dl = delta[s];
     R v[3], C[9];
-    g2p_gather<R>(g, active, F, fstride, kp, dl, x, x, flip, friction, v, C);
+    g2p_gather<R>(g, active, F, fstride, kp, dl, x, xc, flip, friction, v, C);
     R d[3], pos[3];
     for (int q = 0; q < 3; ++q) {
       d[q] = v[q] * (R)dt;
-      pos[q] = x[q] + d[q];
+      pos[q] = xc[q] + d[q];
     }
     R phi, gr[3];
     const R nrm = solid_sample<R>(g, active, F, fstride, kp, dl, x, pos, phi, gr);
@@ -99,7 +102,7 @@ __global__ void __launch_bounds__(192)
     k_adj_g2p(GridDesc g, const int* __restrict__ active_list, const R* __restrict__ P,
               long long pcap, const int* __restrict__ start, const int* __restrict__ delta,
               DeltaRange dr, const R* __restrict__ B, const R* __restrict__ F, long long fstride,
-              R* __restrict__ AG, R flip, R friction) {
+              R* __restrict__ AG, R flip, R friction, const R* __restrict__ XC) {
   const int b = active_list[blockIdx.x];
   const int a = threadIdx.x >> 6;
   const int l = threadIdx.x & 63;
@@ -147,7 +150,9 @@ __global__ void __launch_bounds__(192)
           const R x = px[s], y = py[s], z = pz[s];
           const R w = quad_kernel<R>((x - np_[0]) * invh) * quad_kernel<R>((y - np_[1]) * invh) *
                       quad_kernel<R>((z - np_[2]) * invh);
-          const R cd = (c0[s] * (np_[0] - x) + c1[s] * (np_[1] - y)) + c2[s] * (np_[2] - z);
+          // x_n - x_p from the corrected position when the step corrects
+          const R xc = XC ? XC[s] : x, yc = XC ? XC[pcap + s] : y, zc = XC ? XC[2 * pcap + s] : z;
+          const R cd = (c0[s] * (np_[0] - xc) + c1[s] * (np_[1] - yc)) + c2[s] * (np_[2] - zc);
           acc += w * (vb[s] + fi * cd);
         }
       }

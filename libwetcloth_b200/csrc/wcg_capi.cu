@@ -604,6 +604,12 @@ int wcg_split_liquid_particles(wcg_ctx* ctx, unsigned long long key, long long* 
   return device_status(ctx->c, "splitLiquidParticles");
 }
 
+int wcg_set_correction_count(wcg_ctx* ctx, unsigned long long k) {
+  WCG_CHECK_CTX(ctx);
+  ctx->c.corr_count = k;
+  return WCG_OK;
+}
+
 unsigned long long wcg_split_key(unsigned long long seed, unsigned long long k) {
   return wcg::split_key(seed, k);
 }
@@ -646,8 +652,6 @@ int wcg_substep_vjp(wcg_ctx* ctx, double dt, const double* vbar3, const double* 
   WCG_CHECK_CTX(ctx);
   if (!(dt > 0)) return fail(WCG_ERR_ARG, "dt must be positive");
   WCG_NO_ELASTO(ctx, "substep_vjp");
-  if (ctx->c.prm.correction_strength > 0.0)
-    return fail(WCG_ERR_UNSUPPORTED, "substep_vjp: not available with the particle correction on");
   if (ctx->c.prm.viscosity > 0.0 && ctx->c.prm.viscosity_implicit)
     return fail(WCG_ERR_UNSUPPORTED, "substep_vjp: not available with the implicit viscosity");
   if (ctx->c.prm.particle_merge || ctx->c.prm.particle_split)

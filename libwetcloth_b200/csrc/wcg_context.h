@@ -273,6 +273,7 @@ struct Context {
   // cotangents (sorted order), the first extrapolation layer's input mask,
   // host staging
   DevBuf adj, adjp, adjmask, adjstage, adjvisc;
+  DevBuf adjxc;  // corrected positions of the sub-step (3 Reals per particle)
 
   // implicit viscosity (wcg_visc.cuh): PCG vectors x, r, p, q and the
   // diagonal (3 face fields each), face flags

@@ -77,7 +77,7 @@ void ctx_free(Context& c) {
                     &c.rx64, &c.rr64, &c.rb64,
                     &c.pl, &c.pl64, &c.pl_edge, &c.pl_order, &c.pl_corder, &c.pl_part,
                     &c.mg, &c.mg_mask, &c.mg_vec,
-                    &c.adj, &c.adjp, &c.adjmask, &c.adjstage, &c.adjvisc,
+                    &c.adj, &c.adjp, &c.adjmask, &c.adjstage, &c.adjvisc, &c.adjxc,
                     &c.visc, &c.viscflag, &c.dstage, &c.ustage,
                     &c.xw, &c.corr_start, &c.corr_cursor, &c.corr_list, &c.mwork,
                     &c.scratch, &c.dscalars, &c.derr, &c.ticket};
@@ -2206,15 +2206,32 @@ static cudaError_t substep_vjp_t(Context& c, double dt, const double* vbar, cons
     dr.lo[a] = c.drange_h[a];
     dr.hi[a] = c.drange_h[3 + a];
   }
+  // with the particle correction on, the positions G2P and the advection see:
+  // the correction of this sub-step (the next selector of the seeded stream)
+  // on the recomputed grid, into XC, the particle state restored after it
+  const R* XC = nullptr;
+  if (c.prm.correction_strength > 0.0) {
+    R* P = c.pbuf[c.cur].as<R>();
+    const int sel = correction_selector(c.prm.correction_seed, c.corr_count,
+                                        c.prm.correction_step);
+    WCG_TRY(correct_liquid_particles(c, dt, sel));  // x -> xw, P positions -> x_c
+    WCG_TRY(c.adjxc.ensure((size_t)3 * c.pcap * rb));
+    WCG_TRY(cudaMemcpyAsync(c.adjxc.p, P + PX * c.pcap, 3 * c.pcap * sizeof(R),
+                            cudaMemcpyDeviceToDevice, c.stream));
+    WCG_TRY(cudaMemcpyAsync(P + PX * c.pcap, c.xw.p, 3 * c.pcap * sizeof(R),
+                            cudaMemcpyDeviceToDevice, c.stream));
+    c.xw_valid = false;
+    XC = c.adjxc.as<R>();
+  }
   ++c.launches, k_adj_load<R><<<nblk(np, 128), 128, 0, c.stream>>>(
       c.g, act, c.pbuf[c.cur].as<R>(), c.pcap, np, c.pkey.as<long long>() + c.cur * c.pcap,
       c.pdelta.as<int>() + c.cur * c.pcap, F, c.gcap, (R)c.prm.flip_coeff,
       (R)c.prm.liquid_boundary_friction, c.pid[c.cur].as<int>(), st, st + 3 * np,
-      st + 12 * np, dt, B);
+      st + 12 * np, dt, B, XC);
   ++c.launches, k_adj_g2p<R><<<nb, 192, 0, c.stream>>>(
       c.g, al, c.pbuf[c.cur].as<R>(), c.pcap, c.cell_start.as<int>(),
       c.pdelta.as<int>() + c.cur * c.pcap, dr, B, F, c.gcap, AG, (R)c.prm.flip_coeff,
-      (R)c.prm.liquid_boundary_friction);
+      (R)c.prm.liquid_boundary_friction, XC);
   // extrapolation layers in reverse: layer 2 read the layer-1 output mask,
   // layer 1 the validity after the pressure gradient
   ++c.launches, k_adj_extrapolate<R><<<nb, 192, 0, c.stream>>>(

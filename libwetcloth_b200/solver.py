@@ -207,6 +207,11 @@ class FluidScene:
         check(self.L.wcg_merge_liquid_particles(self.h, int(selector), pm, ctypes.byref(rem)))
         return rem.value
 
+    def set_correction_count(self, k):
+        """Call count of the correction stream (the next sub-step corrects the
+        subset of call k)."""
+        check(self.L.wcg_set_correction_count(self.h, int(k)))
+
     def correct_liquid_particles(self, dt, selector):
         """correctLiquidParticles for the particles with index % step == selector."""
         check(self.L.wcg_correct_liquid_particles(self.h, dt, int(selector)))

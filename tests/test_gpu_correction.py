@@ -166,7 +166,7 @@ def test_correction_fp32(wcg):
     g.close()
 
 
-def test_correction_args_and_vjp_refused(wcg):
+def test_correction_args(wcg):
     sc = _scene("dam16")
     g = FluidScene(sc)
     g.rebucketize_and_resample()
@@ -174,8 +174,4 @@ def test_correction_args_and_vjp_refused(wcg):
     with pytest.raises(_capi.WcgError) as e:
         g.correct_liquid_particles(DT, 8)
     assert e.value.code == _capi.WCG_ERR_ARG
-    n = sc.x.shape[0]
-    with pytest.raises(_capi.WcgError) as e:
-        g.substep_vjp(DT, np.zeros((n, 3)), np.zeros((n, 9)), np.zeros((n, 3)))
-    assert e.value.code == _capi.WCG_ERR_UNSUPPORTED
     g.close()
