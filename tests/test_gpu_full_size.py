@@ -56,3 +56,23 @@ def test_full_size_step_fp32_refine(full_scene, wcg):
     # the solid projection puts a particle that ends inside a wall back on its
     # surface, up to rounding
     assert x0.min() > -1e-9 and x0.max() < 1.0 + 1e-9
+
+
+def test_full_size_fp32_refine_against_fp64(full_scene, wcg):
+    """The precision configuration at full size: three steps of the FP32 +
+    refinement form against the FP64 GPU form (the FP64 form is pinned to the
+    oracle at small sizes); velocities within 1e-4 of their largest value,
+    positions within 1e-6."""
+    sc = full_scene
+    out = {}
+    for prec in (_capi.WCG_FP64, _capi.WCG_FP32_REFINE):
+        g = FluidScene(sc, precision=prec)
+        for _ in range(3):
+            g.step(DT)
+        assert g.stats()["converged"] == 1
+        x, v, _ = g.download()
+        out[prec] = (x, v)
+        g.close()
+    (x64, v64), (x32, v32) = out[_capi.WCG_FP64], out[_capi.WCG_FP32_REFINE]
+    assert np.abs(v32 - v64).max() <= 1e-4 * np.abs(v64).max()
+    assert np.abs(x32 - x64).max() <= 1e-6
