@@ -266,6 +266,7 @@ struct Context {
   // momentum, index maps; the merge's draw counter
   DevBuf mwork;
   unsigned long long merge_count = 0;
+  bool buckets_valid = false;    // pbucket holds the bucket of every current particle
   unsigned long long split_count = 0;
   long long merged_removed = 0;  // particles the last merge removed
 

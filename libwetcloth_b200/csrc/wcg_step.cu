@@ -219,6 +219,7 @@ cudaError_t upload_particles(Context& c, long long n, const double* x3,
   }
   c.np = n;
   c.cur = 0;
+  c.buckets_valid = false;
   if (n == 0) return cudaSuccess;
   // stage host arrays into the scratch copy (device side, doubles)
   double* stage = c.hostorder.as<double>();
@@ -745,6 +746,7 @@ static cudaError_t build_grid_t(Context& c) {
         c.ebucket.as<int>() + nxt * c.ecap);
     c.ecur = nxt;
   }
+  c.buckets_valid = true;
   WCG_TRY(cudaGetLastError());
   return cudaSuccess;
 }
@@ -2402,6 +2404,13 @@ static cudaError_t merge_liquid_t(Context& c, int selector, const int* perm, lon
   const int* pid = c.pid[c.cur].as<int>();
   const int* pb = c.pbucket.as<int>() + c.cur * c.pcap;
   long long* key = c.pkey.as<long long>() + (c.cur ^ 1) * c.pcap;  // free half
+  // particles uploaded since the last grid build: their buckets in that
+  // build's bucket grid, from the current positions
+  if (!c.buckets_valid) {
+    ++c.launches, k_rebucket<R><<<nblk(n, 256), 256, 0, c.stream>>>(
+        P, c.pcap, n, c.g, c.pbucket.as<int>() + c.cur * c.pcap);
+    c.buckets_valid = true;
+  }
   const double rad_fine = 1.0 / std::sqrt(3.0) * c.prm.dx * c.prm.cell_multiplier;
   const double vf = 4.0 / 3.0 * M_PI * rad_fine * rad_fine * rad_fine;
   // 1. classes and the bucket lists (index order inside a bucket)
@@ -2538,9 +2547,11 @@ static cudaError_t split_liquid_t(Context& c, unsigned long long key, long long*
   c.np = n + total;
   c.have_grid = false;
   c.xw_valid = false;
-  if (c.g.nb > 0)
+  if (c.g.nb > 0) {
     ++c.launches, k_rebucket<R><<<nblk(c.np, 256), 256, 0, c.stream>>>(
         c.pbuf[c.cur].as<R>(), c.pcap, c.np, c.g, c.pbucket.as<int>() + c.cur * c.pcap);
+    c.buckets_valid = true;
+  }
   *added = total;
   WCG_TRY(cudaGetLastError());
   return cudaStreamSynchronize(c.stream);
