@@ -52,3 +52,37 @@ def test_batch_autotune_and_per_scene_dt(wcg):
         FluidBatch([])
     for g in gs:
         g.close()
+
+
+def test_batch_with_particle_maintenance_matches_alone(wcg):
+    """Scenes with the correction, split and merge on (each its own seeded
+    streams, particle counts changing between steps) step in a batch exactly
+    as they step alone."""
+    specs = scenes.batch_scenes(5, 9, (16, 32), (2000, 20000))
+    for k, sc in enumerate(specs):
+        scenes.mixed_volumes(sc, k, mrel=(0.3, 0.7, 1.0, 2.5, 5.0))
+        sc.params.correction_strength = 0.2
+        sc.params.correction_seed = k
+        sc.params.particle_split = True
+        sc.params.split_seed = 10 + k
+        sc.params.particle_merge = True
+        sc.params.merge_seed = 20 + k
+    alone = []
+    for sc in specs:
+        g = FluidScene(sc)
+        for _ in range(3):
+            g.step(DT)
+        alone.append(g.download())
+        g.close()
+    gs = [FluidScene(sc) for sc in specs]
+    b = FluidBatch(gs)
+    b.threads = 3
+    st = b.step(DT, nsteps=3)
+    assert all(s == _capi.WCG_OK for s in st), st
+    for g, ref, sc in zip(gs, alone, specs):
+        assert g.num_particles != sc.x.shape[0]
+        for a, r in zip(g.download(), ref):
+            assert np.array_equal(a, r)
+    b.close()
+    for g in gs:
+        g.close()
