@@ -199,3 +199,21 @@ def test_elasto_upload_field_and_positions(tmp_path, wcg):
     g.load_positions(path)
     assert np.array_equal(g.download_elasto()[0], x4)
     g.close()
+
+
+def test_elasto_coupled_four_steps_fp64(wcg):
+    """Four whole steps with the coupling against the oracle (pinned to the
+    reference over the same four steps)."""
+    sc = scenes.liquid_on_sheet(16, 8, 3, center=(0.5, 0.45, 0.5), surfel_every=5)
+    o = oo.OracleScene(sc)
+    g = FluidScene(sc)
+    for k in range(4):
+        o.step(DT, snapshot=(k == 3))
+        g.step(DT)
+    ne = sc.elasto.n
+    x, v, C = g.download()
+    _close(v, o.get("g2p_v").reshape(-1, 3)[ne:], 1e-9, "g2p_v")
+    _close(x, o.get("adv_x").reshape(-1, 3)[ne:], 1e-11, "adv_x")
+    x4, v4, B = g.download_elasto()
+    _close(x4, o.get("adv_x4").reshape(-1, 4)[:ne], 1e-11, "adv_x4")
+    g.close()

@@ -361,3 +361,16 @@ def test_particle_split(kind, seed):
     assert np.abs(xo[:n0][still] - xr[:n0][still]).max() <= 1e-12
     # children of the oracle sit within 0.75 max(r_new, r - r_new) of their parent's centre
     assert np.all(np.abs(xo[n0:]).max() <= 2.0)
+
+
+def test_elasto_coupled_four_steps():
+    """Four steps of the liquid sphere straddling the sheet (drag, pore
+    pressure, solid volume, the sheet carried by its transferred velocity)."""
+    sc = scenes.liquid_on_sheet(16, 8, 3, center=(0.5, 0.45, 0.5), surfel_every=5)
+    r = oref.RefScene(sc, mic=True)
+    o = oo.OracleScene(sc)
+    for k in range(4):
+        assert r.step(DT, snapshot=(k == 3)) == o.step(DT, snapshot=(k == 3))
+    for k in ("g2p_v", "adv_x", "adv_x4", "g2p_eB"):
+        a, b = r.get(k), o.get(k)
+        assert np.abs(a - b).max() <= 1e-10 * np.abs(a).max(), k
