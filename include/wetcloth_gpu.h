@@ -59,7 +59,8 @@ typedef struct wcg_params {
   double criterion;                /* pressure criterion: ||r||_inf <= c ||b||_inf */
   int maxiters;                    /* PCG iteration limit */
   int precision;                   /* WCG_FP64 or WCG_FP32_REFINE */
-  double refine_inner_tol;         /* FP32 inner-solve relative tolerance (0: aim at criterion) */
+  double refine_inner_tol;         /* FP32 inner-solve relative tolerance (default 1e-5;
+                                      0: aim each inner solve at the criterion) */
   int max_refinements;             /* FP64 refinement sweeps (0: 20) */
   int solver;                      /* WCG_SOLVER_MIC0 or WCG_SOLVER_MG */
   double viscosity;                /* LiquidInfo::viscosity; 0: no viscosity */

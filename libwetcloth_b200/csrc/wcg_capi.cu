@@ -182,7 +182,10 @@ void wcg_default_params(wcg_params* p) {
   p->criterion = 1e-6;
   p->maxiters = 1000;
   p->precision = WCG_FP64;
-  p->refine_inner_tol = 0.0;
+  // the first FP32 inner solve stops at 1e-5 and the FP64 refinement takes it
+  // the rest of the way: at 256^3 about 5 % fewer PCG iterations than aiming
+  // every inner solve at the criterion
+  p->refine_inner_tol = 1e-5;
   p->max_refinements = 20;
   p->solver = WCG_SOLVER_MIC0;
   p->viscosity = 0.0;

@@ -16,7 +16,7 @@ from . import _capi
 from ._capi import check, _dp
 
 
-def make_params(p, precision=_capi.WCG_FP64, refine_inner_tol=0.0,
+def make_params(p, precision=_capi.WCG_FP64, refine_inner_tol=1e-5,
                 max_refinements=20, solver=_capi.WCG_SOLVER_MIC0) -> _capi.WcgParams:
     prm = _capi.WcgParams()
     _capi.load().wcg_default_params(ctypes.byref(prm))
