@@ -94,6 +94,15 @@ typedef struct wcg_params {
   int particle_split;              /* relabelLiquidParticles + splitLiquidParticles before
                                       each sub-step, ahead of the merge */
   unsigned long long split_seed;   /* seed of the split's rotations */
+  int terminator;                  /* 1: one terminator box (a distance field with usage
+                                      DFU_TERMINATOR); each sub-step starts with
+                                      terminateParticles (TwoDScene.cpp:1756,
+                                      WetClothCore.cpp:97) */
+  double terminator_center[3];
+  double terminator_half[3];
+  double terminator_radius;
+  int terminator_inside;           /* the box's inside flag: 1 removes the liquid particles
+                                      that leave the box, 0 the ones that enter it */
 } wcg_params;
 
 typedef struct wcg_ctx wcg_ctx;
@@ -247,6 +256,14 @@ int wcg_merge_liquid_particles(wcg_ctx* ctx, int selector, const int* perm9,
  * key ^ parent index (the reference: its compiled sphere-pattern table and
  * Matrix3s::Random()); *added (may be NULL) receives their count. */
 int wcg_split_liquid_particles(wcg_ctx* ctx, unsigned long long key, long long* added);
+/* TwoDScene::terminateParticles (TwoDScene.cpp:1756-1771): the liquid
+ * particles where the terminator box's phi is negative (outside it for
+ * terminator_inside = 1) and every liquid particle without volume are
+ * removed as removeEmptyParticles does (each hole takes the last survivor);
+ * *removed (may be NULL) receives their count.  With params.terminator = 0
+ * only particles without volume are removed.  wcg_substep runs it first when
+ * params.terminator is set. */
+int wcg_terminate_liquid_particles(wcg_ctx* ctx, long long* removed);
 /* the key wcg_substep uses for its k-th split */
 unsigned long long wcg_split_key(unsigned long long seed, unsigned long long k);
 /* the draws wcg_substep uses for its k-th merge: SplitMix64 of the seed and k

@@ -64,6 +64,11 @@ class WcgParams(ctypes.Structure):
         ("particle_cell_multiplier", ctypes.c_double),
         ("particle_split", ctypes.c_int),
         ("split_seed", ctypes.c_ulonglong),
+        ("terminator", ctypes.c_int),
+        ("terminator_center", ctypes.c_double * 3),
+        ("terminator_half", ctypes.c_double * 3),
+        ("terminator_radius", ctypes.c_double),
+        ("terminator_inside", ctypes.c_int),
     ]
 
 
@@ -124,6 +129,8 @@ SIGNATURES = {
     "wcg_set_correction_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_ulonglong]),
     "wcg_split_liquid_particles": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_ulonglong,
                                                   ctypes.POINTER(ctypes.c_longlong)]),
+    "wcg_terminate_liquid_particles": (ctypes.c_int, [ctypes.c_void_p,
+                                                      ctypes.POINTER(ctypes.c_longlong)]),
     "wcg_split_key": (ctypes.c_ulonglong, [ctypes.c_ulonglong, ctypes.c_ulonglong]),
     "wcg_merge_draws": (ctypes.c_int, [ctypes.c_ulonglong, ctypes.c_ulonglong, ctypes.c_int,
                                        ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),

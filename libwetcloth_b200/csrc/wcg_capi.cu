@@ -204,6 +204,13 @@ void wcg_default_params(wcg_params* p) {
   p->merge_seed = 0;
   p->particle_split = 0;
   p->split_seed = 0;
+  p->terminator = 0;
+  for (int a = 0; a < 3; ++a) {
+    p->terminator_center[a] = 0.5;
+    p->terminator_half[a] = 0.5;
+  }
+  p->terminator_radius = 0.0;
+  p->terminator_inside = 1;
   p->particle_cell_multiplier = 0.3535533906;
 }
 
@@ -231,6 +238,15 @@ int wcg_create(const wcg_params* params, wcg_ctx** out) {
     return fail(WCG_ERR_ARG,
                 "correction_strength must be finite and >= 0, correction_step >= 1, "
                 "correction_multiplier finite");
+  if (params->terminator) {
+    bool ok = std::isfinite(params->terminator_radius) && params->terminator_radius >= 0.0;
+    for (int a = 0; a < 3; ++a)
+      ok = ok && std::isfinite(params->terminator_center[a]) &&
+           std::isfinite(params->terminator_half[a]) && params->terminator_half[a] >= 0.0;
+    if (!ok)
+      return fail(WCG_ERR_ARG,
+                  "terminator centre, half extents (>= 0) and radius (>= 0) must be finite");
+  }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return fail(WCG_ERR_CUDA, "no CUDA device available");
@@ -268,6 +284,13 @@ int wcg_create(const wcg_params* params, wcg_ctx** out) {
   p.merge_seed = params->merge_seed;
   p.particle_split = params->particle_split ? 1 : 0;
   p.split_seed = params->split_seed;
+  p.terminator = params->terminator ? 1 : 0;
+  for (int a = 0; a < 3; ++a) {
+    p.term_center[a] = params->terminator_center[a];
+    p.term_half[a] = params->terminator_half[a];
+  }
+  p.term_radius = params->terminator_radius;
+  p.term_inside = params->terminator_inside ? 1 : 0;
   p.cell_multiplier = params->particle_cell_multiplier;
   p.viscosity_criterion = params->viscosity_criterion;
   // wavefront tile shape (performance knob; both compute identical results)
@@ -607,6 +630,14 @@ int wcg_split_liquid_particles(wcg_ctx* ctx, unsigned long long key, long long* 
   return device_status(ctx->c, "splitLiquidParticles");
 }
 
+int wcg_terminate_liquid_particles(wcg_ctx* ctx, long long* removed) {
+  WCG_CHECK_CTX(ctx);
+  long long rem = 0;
+  WCG_CALL(ctx, wcg::terminate_liquid_particles(ctx->c, &rem), "terminateParticles");
+  if (removed) *removed = rem;
+  return device_status(ctx->c, "terminateParticles");
+}
+
 int wcg_set_correction_count(wcg_ctx* ctx, unsigned long long k) {
   WCG_CHECK_CTX(ctx);
   ctx->c.corr_count = k;
@@ -657,9 +688,9 @@ int wcg_substep_vjp(wcg_ctx* ctx, double dt, const double* vbar3, const double* 
   WCG_NO_ELASTO(ctx, "substep_vjp");
   if (ctx->c.prm.viscosity > 0.0 && ctx->c.prm.viscosity_implicit)
     return fail(WCG_ERR_UNSUPPORTED, "substep_vjp: not available with the implicit viscosity");
-  if (ctx->c.prm.particle_merge || ctx->c.prm.particle_split)
+  if (ctx->c.prm.particle_merge || ctx->c.prm.particle_split || ctx->c.prm.terminator)
     return fail(WCG_ERR_UNSUPPORTED,
-                "substep_vjp: not available with the particle merge or split on");
+                "substep_vjp: not available with the particle merge, split or terminator on");
   const long long n = ctx->c.np;
   if (n > 0 && (!vbar3 || !Cbar9 || !xbar3 || !vbar0 || !Cbar0 || !xbar0))
     return fail(WCG_ERR_ARG, "null cotangent array");

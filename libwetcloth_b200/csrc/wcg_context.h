@@ -46,6 +46,9 @@ struct Params {
   unsigned long long split_seed; // seed of the split's rotations
   unsigned long long merge_seed; // seed of the merge's draws
   double cell_multiplier;        // LiquidInfo::particle_cell_multiplier (V_fine)
+  int terminator;                // a terminator box: terminateParticles first in each sub-step
+  double term_center[3], term_half[3], term_radius;
+  int term_inside;               // the box's inside flag (sign -1)
 };
 
 // A device allocation that grows and never shrinks.
@@ -388,6 +391,7 @@ cudaError_t merge_liquid_particles(Context& c, int selector, const int* perm, lo
 // splitLiquidParticles with the rotations of key (after relabelling);
 // *added = particles appended
 cudaError_t split_liquid_particles(Context& c, unsigned long long key, long long* added);
+cudaError_t terminate_liquid_particles(Context& c, long long* removed);
 unsigned long long split_key(unsigned long long seed, unsigned long long k);
 // draws of merge call k of a seeded stream: selector, then three Fisher-Yates
 // permutations of {0, 1, 2}

@@ -2369,6 +2369,59 @@ void merge_draws(unsigned long long seed, unsigned long long k, int step, int* s
   }
 }
 
+// removeEmptyParticles (TwoDScene.cpp:1713-1745) on flagged slots: alive_slot
+// holds 0/1 per slot (scanned in place here), alive_pid the same per original
+// index; hole_rank, high_rank and holes take n ints each, corr_cursor and
+// corr_list n each.  The holes below K (the survivor count) take the
+// survivors at K and above in descending order; the slots are compacted and
+// the original indices renumbered.
+template <typename R>
+static cudaError_t remove_flagged_t(Context& c, long long n, int* alive_slot, int* alive_pid,
+                                    int* hole_rank, int* high_rank, int* holes,
+                                    long long* removed) {
+  const long long cap = c.pcap;
+  R* P = c.pbuf[c.cur].as<R>();
+  const int* pid = c.pid[c.cur].as<int>();
+  const int* pb = c.pbucket.as<int>() + c.cur * c.pcap;
+  int* cursor = c.corr_cursor.as<int>();
+  int* list = c.corr_list.as<int>();
+  int* dtot = (int*)(c.dscalars.as<double>() + 48);
+  exclusive_scan<int, int>(alive_slot, n, alive_slot, c.scratch.as<int>(), dtot, c.stream);
+  int K = 0;
+  WCG_TRY(cudaMemcpyAsync(&K, dtot, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  WCG_TRY(cudaStreamSynchronize(c.stream));
+  c.have_grid = false;  // volumes, masses and radii changed
+  c.xw_valid = false;
+  if (K == n) return cudaGetLastError();
+  ++c.launches, k_merge_flags<<<nblk(n, 256), 256, 0, c.stream>>>(n, K, alive_pid, hole_rank,
+                                                                   high_rank);
+  exclusive_scan<int, int>(hole_rank, n, hole_rank, c.scratch.as<int>(), dtot, c.stream);
+  exclusive_scan<int, int>(high_rank, n, high_rank, c.scratch.as<int>(), dtot + 1, c.stream);
+  ++c.launches, k_merge_holes<<<nblk(n, 256), 256, 0, c.stream>>>(n, K, alive_pid, hole_rank, holes);
+  int counts[2] = {0, 0};
+  WCG_TRY(cudaMemcpyAsync(counts, dtot, 2 * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  // surviving slots: alive_slot now holds their ranks; the flags come back
+  // from alive_pid through pid
+  ++c.launches, k_merge_alive_slots<<<nblk(n, 256), 256, 0, c.stream>>>(n, pid, alive_pid, cursor);
+  ++c.launches, k_merge_compact<<<nblk(n, 256), 256, 0, c.stream>>>(n, cursor, alive_slot, list);
+  WCG_TRY(cudaStreamSynchronize(c.stream));
+  const int nxt = c.cur ^ 1;
+  ++c.launches, k_gather_particles<R><<<nblk(K, 256), 256, 0, c.stream>>>(
+      list, K, cap, P, c.pbuf[nxt].as<R>(), pid, c.pid[nxt].as<int>(),
+      c.pkey.as<long long>() + c.cur * cap, c.pkey.as<long long>() + nxt * cap,
+      c.pdelta.as<int>() + c.cur * cap, c.pdelta.as<int>() + nxt * cap, pb,
+      c.pbucket.as<int>() + nxt * cap);
+  ++c.launches, k_merge_repid<<<nblk(K, 256), 256, 0, c.stream>>>(
+      K, list, pid, high_rank, holes, counts[1], c.pid[nxt].as<int>());
+  WCG_TRY(cudaGetLastError());
+  c.cur = nxt;
+  *removed = n - K;
+  c.np = K;
+  c.have_grid = false;
+  c.xw_valid = false;
+  return cudaStreamSynchronize(c.stream);
+}
+
 template <typename R>
 static cudaError_t merge_liquid_t(Context& c, int selector, const int* perm, long long* removed) {
   *removed = 0;
@@ -2441,43 +2494,38 @@ static cudaError_t merge_liquid_t(Context& c, int selector, const int* perm, lon
   // 3. gather and update, alive flags
   ++c.launches, k_merge_gather<R><<<nblk(n, 256), 256, 0, c.stream>>>(
       P, cap, n, pid, rem, gvol, gmom, c.prm.liquid_density, alive_slot, alive_pid);
-  int* dtot = (int*)(c.dscalars.as<double>() + 48);
-  exclusive_scan<int, int>(alive_slot, n, alive_slot, c.scratch.as<int>(), dtot, c.stream);
-  int K = 0;
-  WCG_TRY(cudaMemcpyAsync(&K, dtot, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
-  WCG_TRY(cudaStreamSynchronize(c.stream));
-  c.have_grid = false;  // volumes, masses and radii changed
-  c.xw_valid = false;
-  if (K == n) return cudaGetLastError();
-  // 4. removeEmptyParticles: the holes below K take the survivors above it
-  //    in descending order; compact the slots and renumber
-  ++c.launches, k_merge_flags<<<nblk(n, 256), 256, 0, c.stream>>>(n, K, alive_pid, hole_rank,
-                                                                   high_rank);
-  exclusive_scan<int, int>(hole_rank, n, hole_rank, c.scratch.as<int>(), dtot, c.stream);
-  exclusive_scan<int, int>(high_rank, n, high_rank, c.scratch.as<int>(), dtot + 1, c.stream);
-  ++c.launches, k_merge_holes<<<nblk(n, 256), 256, 0, c.stream>>>(n, K, alive_pid, hole_rank, holes);
-  int counts[2] = {0, 0};
-  WCG_TRY(cudaMemcpyAsync(counts, dtot, 2 * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
-  // surviving slots: alive_slot now holds their ranks; the flags come back
-  // from alive_pid through pid
-  ++c.launches, k_merge_alive_slots<<<nblk(n, 256), 256, 0, c.stream>>>(n, pid, alive_pid, cursor);
-  ++c.launches, k_merge_compact<<<nblk(n, 256), 256, 0, c.stream>>>(n, cursor, alive_slot, list);
-  WCG_TRY(cudaStreamSynchronize(c.stream));
-  const int nxt = c.cur ^ 1;
-  ++c.launches, k_gather_particles<R><<<nblk(K, 256), 256, 0, c.stream>>>(
-      list, K, cap, P, c.pbuf[nxt].as<R>(), pid, c.pid[nxt].as<int>(),
-      c.pkey.as<long long>() + c.cur * cap, c.pkey.as<long long>() + nxt * cap,
-      c.pdelta.as<int>() + c.cur * cap, c.pdelta.as<int>() + nxt * cap, pb,
-      c.pbucket.as<int>() + nxt * cap);
-  ++c.launches, k_merge_repid<<<nblk(K, 256), 256, 0, c.stream>>>(
-      K, list, pid, high_rank, holes, counts[1], c.pid[nxt].as<int>());
-  WCG_TRY(cudaGetLastError());
-  c.cur = nxt;
-  *removed = n - K;
-  c.np = K;
-  c.have_grid = false;
-  c.xw_valid = false;
-  return cudaStreamSynchronize(c.stream);
+  return remove_flagged_t<R>(c, n, alive_slot, alive_pid, hole_rank, high_rank, holes, removed);
+}
+
+template <typename R>
+static cudaError_t terminate_liquid_t(Context& c, long long* removed) {
+  *removed = 0;
+  const long long n = c.np;
+  if (n == 0) return cudaSuccess;
+  ProfScope prof(c, P_OTHER);
+  const long long cap = c.pcap;
+  WCG_TRY(c.mwork.ensure((size_t)5 * cap * sizeof(int) + 64));
+  int* iw = c.mwork.as<int>();
+  WCG_TRY(c.corr_cursor.ensure((size_t)n * sizeof(int)));
+  WCG_TRY(c.corr_list.ensure((size_t)n * sizeof(int)));
+  const long long scan_tiles = (n + kScanTile - 1) / kScanTile + 1;
+  WCG_TRY(ensure_scratch(c, (size_t)scan_tiles * sizeof(long long) + 64));
+  Walls t;
+  t.cx = c.prm.term_center[0]; t.cy = c.prm.term_center[1]; t.cz = c.prm.term_center[2];
+  t.ex = c.prm.term_half[0]; t.ey = c.prm.term_half[1]; t.ez = c.prm.term_half[2];
+  t.radius = c.prm.term_radius;
+  t.sign = c.prm.term_inside ? -1.0 : 1.0;
+  t.enabled = c.prm.terminator;
+  ++c.launches, k_terminate<R><<<nblk(n, 256), 256, 0, c.stream>>>(
+      c.pbuf[c.cur].as<R>(), cap, n, c.pid[c.cur].as<int>(), t, 3.0 * 4.0 * c.prm.dx, iw,
+      iw + cap);
+  return remove_flagged_t<R>(c, n, iw, iw + cap, iw + 2 * cap, iw + 3 * cap, iw + 4 * cap,
+                             removed);
+}
+
+cudaError_t terminate_liquid_particles(Context& c, long long* removed) {
+  return c.prm.precision == 0 ? terminate_liquid_t<double>(c, removed)
+                              : terminate_liquid_t<float>(c, removed);
 }
 
 unsigned long long split_key(unsigned long long seed, unsigned long long k) {
@@ -2568,6 +2616,11 @@ cudaError_t merge_liquid_particles(Context& c, int selector, const int* perm, lo
 }
 
 cudaError_t substep(Context& c, double dt) {
+  // terminateParticles (WetClothCore.cpp:97) ahead of the particle maintenance
+  if (c.prm.terminator && c.np > 0) {
+    long long rem = 0;
+    WCG_TRY(terminate_liquid_particles(c, &rem));
+  }
   // updateOptiVolume, splitLiquidParticles, mergeLiquidParticles
   // (WetClothCore.cpp:97-110): the merge works on the buckets of the previous
   // sub-step's grid build, re-sorted by a split that added particles

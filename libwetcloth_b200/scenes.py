@@ -56,6 +56,14 @@ class SceneParams:
     particle_split: bool = False   # relabel + splitLiquidParticles before each sub-step
     split_seed: int = 0
     particle_cell_multiplier: float = 0.3535533906
+    # terminateParticles (TwoDScene.cpp:1756): one terminator box (a distance
+    # field with usage "terminator"); inside=True removes the liquid particles
+    # that leave it, inside=False the ones that enter it
+    terminator: bool = False
+    terminator_center: tuple = (0.5, 0.5, 0.5)
+    terminator_half: tuple = (0.5, 0.5, 0.5)
+    terminator_radius: float = 0.0
+    terminator_inside: bool = True
 
 
 def particle_radius(dx: float, ppc: int) -> float:

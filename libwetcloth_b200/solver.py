@@ -47,6 +47,13 @@ def make_params(p, precision=_capi.WCG_FP64, refine_inner_tol=1e-5,
     prm.particle_merge = 1 if getattr(p, "particle_merge", False) else 0
     prm.particle_split = 1 if getattr(p, "particle_split", False) else 0
     prm.split_seed = getattr(p, "split_seed", 0)
+    if getattr(p, "terminator", False):
+        prm.terminator = 1
+        for a in range(3):
+            prm.terminator_center[a] = p.terminator_center[a]
+            prm.terminator_half[a] = p.terminator_half[a]
+        prm.terminator_radius = p.terminator_radius
+        prm.terminator_inside = 1 if p.terminator_inside else 0
     prm.merge_seed = getattr(p, "merge_seed", 0)
     prm.particle_cell_multiplier = getattr(p, "particle_cell_multiplier", 0.3535533906)
     prm.correction_strength = getattr(p, "correction_strength", 0.0)
@@ -197,6 +204,13 @@ class FluidScene:
         add = ctypes.c_longlong(0)
         check(self.L.wcg_split_liquid_particles(self.h, int(key), ctypes.byref(add)))
         return add.value
+
+    def terminate_liquid_particles(self):
+        """terminateParticles with the scene's terminator box; returns the
+        number of particles removed."""
+        rem = ctypes.c_longlong(0)
+        check(self.L.wcg_terminate_liquid_particles(self.h, ctypes.byref(rem)))
+        return rem.value
 
     def merge_liquid_particles(self, selector, perm):
         """relabel + mergeLiquidParticles + removeEmptyParticles with the given

@@ -53,6 +53,10 @@ def lib():
         L.wco_split_key.argtypes = [ctypes.c_uint64, ctypes.c_uint64]
         L.wco_split_key.restype = ctypes.c_uint64
         L.wco_set_split.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_uint64]
+        L.wco_terminate_liquid.argtypes = [ctypes.c_void_p]
+        L.wco_terminate_liquid.restype = ctypes.c_int
+        L.wco_set_terminator.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, _D, ctypes.c_double,
+                                         ctypes.c_int]
         L.wco_correction_selector.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int]
         L.wco_correction_selector.restype = ctypes.c_int
         L.wco_step.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
@@ -130,6 +134,9 @@ class OracleScene:
                             getattr(p, "particle_cell_multiplier", 0.3535533906))
         if getattr(p, "particle_split", False):
             L.wco_set_split(self.h, 1, getattr(p, "split_seed", 0))
+        if getattr(p, "terminator", False):
+            L.wco_set_terminator(self.h, 1, arr(p.terminator_center), arr(p.terminator_half),
+                                 p.terminator_radius, 1 if p.terminator_inside else 0)
         if getattr(p, "correction_strength", 0.0) > 0.0:
             L.wco_set_correction(self.h, p.correction_strength, p.correction_step,
                                  p.correction_multiplier, p.correction_seed)
@@ -169,6 +176,11 @@ class OracleScene:
         """splitLiquidParticles with the rotations of key; returns the
         particles added."""
         return self.L.wco_split_liquid(self.h, int(key))
+
+    def terminate(self):
+        """terminateParticles with the scene's terminator box; returns the
+        particles removed."""
+        return self.L.wco_terminate_liquid(self.h)
 
     def set_correction_selector(self, selector):
         """Particle subset (fluid index % step) of the next correction."""

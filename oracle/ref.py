@@ -61,6 +61,9 @@ def _lib(omp: bool):
         L.wcref_merge.restype = ctypes.c_int
         L.wcref_split.argtypes = [ctypes.c_void_p, ctypes.c_uint]
         L.wcref_split.restype = ctypes.c_int
+        L.wcref_set_terminator.argtypes = [ctypes.c_void_p, _D, _D, ctypes.c_double, ctypes.c_int]
+        L.wcref_terminate.argtypes = [ctypes.c_void_p]
+        L.wcref_terminate.restype = ctypes.c_int
         _libs[omp] = L
     return _libs[omp]
 
@@ -119,6 +122,9 @@ class RefScene:
             self.L.wcref_set_viscosity(self.h, mu, getattr(p, "viscosity_substeps", 1))
         set_elasto(self.L.wcref_set_elasto, self.L.wcref_set_elasto_coeffs, self.h, scene,
                    self._keep)
+        if getattr(p, "terminator", False):
+            self.L.wcref_set_terminator(self.h, arr(p.terminator_center), arr(p.terminator_half),
+                                        p.terminator_radius, 1 if p.terminator_inside else 0)
         if getattr(p, "correction_strength", 0.0) > 0.0:
             self.L.wcref_set_correction(self.h, p.correction_strength, p.correction_step,
                                         p.correction_multiplier, p.correction_seed)
@@ -141,6 +147,10 @@ class RefScene:
         """updateOptiVolume + mergeLiquidParticles after srand(seed); returns
         the particles removed (draws in "merge_selector", "merge_perm")."""
         return self.L.wcref_merge(self.h, seed, step)
+
+    def terminate(self) -> int:
+        """terminateParticles; returns the particles removed."""
+        return self.L.wcref_terminate(self.h)
 
     def split(self, seed: int) -> int:
         """updateOptiVolume + splitLiquidParticles after srand(seed);

@@ -95,6 +95,7 @@ struct Harness {
   double last_res_amg = 0, last_res_mic = 0;
   bool corr_on = false;       // correctLiquidParticles before G2P (WetClothCore.cpp:242)
   unsigned corr_seed = 0, corr_count = 0;
+  bool term_on = false;       // terminateParticles first (WetClothCore.cpp:97)
 };
 
 double now() {
@@ -508,6 +509,11 @@ int wcref_substep(void* hp, double sub_dt, int snapshot) {
   LinearizedImplicitEuler& e = *h->stepper;
   double t0 = now(), t1;
 
+  if (h->term_on) {
+    const int before = s.getNumParticles();
+    s.terminateParticles();
+    h->ii["terminate_removed"] = {(long long)(before - s.getNumParticles())};
+  }
   s.updateParticleBoundingBox();
   s.rebucketizeParticles();
   s.resampleNodes();
@@ -724,6 +730,44 @@ int wcref_merge(void* hp, unsigned seed, int step) {
     cls[i] = (long long)s.m_classifier[i];
   }
   return before - np;
+}
+
+// A terminator box (DFT_BOX, DFU_TERMINATOR) in a distance-field group of its
+// own (group 1: the group's union operator votes the terminator usage); the
+// groups are rebuilt around it (TwoDScene::resizeGroups, initGroupPos), and
+// each sub-step then starts with terminateParticles.
+void wcref_set_terminator(void* hp, const double* c, const double* half, double radius,
+                          int inside) {
+  Harness* h = (Harness*)hp;
+  TwoDScene& s = *h->scene;
+  VectorXs par(4);
+  par << half[0], half[1], half[2], radius;
+  std::vector<DF_SOURCE_DURATION> dur;
+  auto term = std::make_shared<DistanceFieldObject>(
+      Vector3s(c[0], c[1], c[2]), par, DFT_BOX, DFU_TERMINATOR, inside != 0,
+      Vector3s(0, 1, 0), 0.0, 1, 0, false, dur);
+  s.m_distance_fields.push_back(term);
+  for (auto& df : s.m_distance_fields) df->parent.reset();
+  s.resizeGroups(2);
+  s.initGroupPos();
+  // the scene parser builds the grid at load (App/TwoDSceneXMLParser.cpp:725-727),
+  // so the first terminateParticles re-sorts valid bucket lists
+  s.updateParticleBoundingBox();
+  s.rebucketizeParticles();
+  s.resampleNodes();
+  h->term_on = true;
+}
+
+// TwoDScene::terminateParticles: liquid particles inside the terminator's
+// negative region lose their volume and removeEmptyParticles drops them.
+// Returns the particles removed.
+int wcref_terminate(void* hp) {
+  Harness* h = (Harness*)hp;
+  TwoDScene& s = *h->scene;
+  const int before = s.getNumParticles();
+  s.terminateParticles();
+  snap_particles(*h, "term_");
+  return before - s.getNumParticles();
 }
 
 // TwoDScene::updateOptiVolume and splitLiquidParticles, as

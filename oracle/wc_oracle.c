@@ -39,6 +39,10 @@ typedef struct {
   double cell_mult; /* LiquidInfo::particle_cell_multiplier */
   int merge_on;     /* relabel + mergeLiquidParticles before each sub-step */
   int split_on;     /* relabel + splitLiquidParticles before each sub-step */
+  /* one terminator box (DFT_BOX, DFU_TERMINATOR, in a distance-field group of
+   * its own): centre, half extents, radius, sign (-1: inside=true) */
+  int term_on;
+  double tc[3], th[3], tr, tsign;
 } Params;
 
 typedef struct {
@@ -261,6 +265,30 @@ static double wall_phi(const Scene* s, double px, double py, double pz) {
   m = m < 0.0 ? m : 0.0;
   const double box = m + sqrt(da[0] * da[0] + da[1] * da[1] + da[2] * da[2]) - s->p.br;
   const double phi = -1.0 * box;
+  double u = 1e20;
+  if (phi < u) u = phi;
+  double r = 3.0 * s->bs;
+  if (u < r) r = u;
+  return r;
+}
+
+/* The terminator: the same box distance field with usage DFU_TERMINATOR in
+ * its own group, whose DFT_UNION operator votes the terminator usage
+ * (DistanceFieldOperator::vote_usage, DistanceFields.cpp:922-938), read by
+ * computePhiVel through the terminator selector (TwoDScene.cpp:1757-1759). */
+static double term_phi(const Scene* s, double px, double py, double pz) {
+  const double p[3] = {px, py, pz};
+  double d[3], da[3];
+  for (int a = 0; a < 3; ++a) {
+    const double rp = (p[a] - s->p.tc[a]) + s->p.tc[a];
+    d[a] = fabs(rp - s->p.tc[a]) - s->p.th[a];
+    da[a] = d[a] > 0.0 ? d[a] : 0.0;
+  }
+  double m = d[0] > d[1] ? d[0] : d[1];
+  m = m > d[2] ? m : d[2];
+  m = m < 0.0 ? m : 0.0;
+  const double box = m + sqrt(da[0] * da[0] + da[1] * da[1] + da[2] * da[2]) - s->p.tr;
+  const double phi = s->p.tsign * box;
   double u = 1e20;
   if (phi < u) u = phi;
   double r = 3.0 * s->bs;
@@ -1819,9 +1847,11 @@ static int remove_empty(Scene* s) {
       swap_d(s->m, i, n, 1);
       swap_d(s->vol, i, n, 1);
       swap_d(s->rad, i, n, 1);
-      const unsigned char t = s->cls[i];
-      s->cls[i] = s->cls[n];
-      s->cls[n] = t;
+      if (s->cls) {
+        const unsigned char t = s->cls[i];
+        s->cls[i] = s->cls[n];
+        s->cls[n] = t;
+      }
     } else {
       ++i;
     }
@@ -2175,6 +2205,36 @@ int wco_split_liquid(Scene* s, uint64_t key) {
   return total;
 }
 
+/* TwoDScene::terminateParticles (TwoDScene.cpp:1756-1771): a liquid particle
+ * where the terminator's phi is negative loses its fluid volume, then
+ * removeEmptyParticles drops every liquid particle without volume.  Returns
+ * the particles removed. */
+int wco_terminate_liquid(Scene* s) {
+  if (s->bs <= 0.0) s->bs = s->p.dx * NN;
+  for (int i = s->ne; i < s->np; ++i)
+    if (s->p.term_on && term_phi(s, s->x[i * 3], s->x[i * 3 + 1], s->x[i * 3 + 2]) < 0.0)
+      s->vol[i] = 0.0;
+  const int removed = remove_empty(s);
+  snap_particles(s, "term_");
+  /* removeEmptyParticles re-sorts the bucket lists after a removal
+   * (TwoDScene.cpp:1734-1743) */
+  if (removed > 0 && s->keys && s->nb > 0) sort_particles(s);
+  return removed;
+}
+
+/* the terminator box (inside: 1 removes the particles that leave it, 0 the
+ * ones that enter it) */
+void wco_set_terminator(Scene* s, int on, const double* c, const double* h, double r,
+                        int inside) {
+  s->p.term_on = on;
+  for (int a = 0; a < 3; ++a) {
+    s->p.tc[a] = c[a];
+    s->p.th[a] = h[a];
+  }
+  s->p.tr = r;
+  s->p.tsign = inside ? -1.0 : 1.0;
+}
+
 /* split before each sub-step with the seeded keys */
 void wco_set_split(Scene* s, int on, uint64_t seed) {
   s->p.split_on = on;
@@ -2372,6 +2432,10 @@ int wco_substep(Scene* s, double dt, int snapshot) {
    * (WetClothCore.cpp:97-110); a split that adds particles re-sorts the
    * buckets (TwoDScene.cpp:2471-2478), so the merge after it sees the new
    * positions in the buckets of the last grid build */
+  if (s->p.term_on) {
+    const long long nrem = wco_terminate_liquid(s);
+    snap_put_i(s, "terminate_removed", &nrem, 1);
+  }
   if (s->p.split_on && s->np > s->ne) {
     const long long nadd = wco_split_liquid(s, wco_split_key(s->split_seed, s->split_count++));
     snap_put_i(s, "split_added", &nadd, 1);

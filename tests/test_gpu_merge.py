@@ -164,3 +164,62 @@ def test_split_and_merge_seeded_steps(wcg):
     _close(x, o.get("adv_x"), 1e-6, "adv_x fp32")
     g.close()
     g32.close()
+
+
+def _terminator_scene(inside=True):
+    sc = scenes.half_box(16, 2, 7, amplitude=1.0, sigma_cells=1.5)
+    lo, hi = sc.x.min(axis=0), sc.x.max(axis=0)
+    p = sc.params
+    p.terminator = True
+    p.terminator_center = tuple(0.5 * (lo + hi))
+    p.terminator_half = tuple(0.3 * (hi - lo))
+    p.terminator_radius = 0.25 * p.dx
+    p.terminator_inside = inside
+    return sc
+
+
+@pytest.mark.parametrize("inside", [True, False])
+def test_terminate_call_fp64(inside, wcg):
+    """terminateParticles on its own (tests/test_oracle_vs_reference.py pins
+    the oracle's to the reference): the same particles removed, the survivors
+    in the same order, bit-exact (the removal only moves particles)."""
+    sc = _terminator_scene(inside)
+    o = oo.OracleScene(sc)
+    g = FluidScene(sc)
+    rem = g.terminate_liquid_particles()
+    assert 0 < rem < sc.x.shape[0]
+    assert o.terminate() == rem
+    x, v, C = g.download()
+    assert np.array_equal(x.reshape(-1), o.get("term_x").reshape(-1))
+    assert np.array_equal(v.reshape(-1), o.get("term_v").reshape(-1))
+    assert g.terminate_liquid_particles() == 0
+    g.close()
+
+
+@pytest.mark.parametrize("prec", [_capi.WCG_FP64, _capi.WCG_FP32_REFINE])
+def test_terminator_steps(prec, wcg):
+    """Three steps, each sub-step starting with terminateParticles: FP64 agrees
+    with the oracle on the removals (count and order) and the state to the
+    step tolerances; FP32 on the count (its positions are rounded, so a
+    particle on the box's surface may fall the other way) and, when the
+    counts match, the state to 1e-5 / 1e-6."""
+    sc = _terminator_scene(True)
+    o = oo.OracleScene(sc)
+    g = FluidScene(sc, precision=prec)
+    removed = 0
+    for _ in range(3):
+        o.step(DT, snapshot=True)
+        g.step(DT)
+        removed += int(o.get("terminate_removed")[0])
+    assert removed > 0
+    x, v, C = g.download()
+    ox = o.get("adv_x").reshape(-1, 3)
+    if prec == _capi.WCG_FP64:
+        _close(v, o.get("g2p_v"), 1e-10, "g2p_v")
+        _close(x, ox, 1e-12, "adv_x")
+    else:
+        assert abs(x.shape[0] - ox.shape[0]) <= 2
+        if x.shape[0] == ox.shape[0]:
+            _close(v, o.get("g2p_v"), 1e-5, "g2p_v")
+            _close(x, ox, 1e-6, "adv_x")
+    g.close()

@@ -374,3 +374,40 @@ def test_elasto_coupled_four_steps():
     for k in ("g2p_v", "adv_x", "adv_x4", "g2p_eB"):
         a, b = r.get(k), o.get(k)
         assert np.abs(a - b).max() <= 1e-10 * np.abs(a).max(), k
+
+
+@pytest.mark.parametrize("inside", [True, False])
+def test_terminate_particles(inside):
+    """terminateParticles (TwoDScene.cpp:1756-1771) with a terminator box in a
+    distance-field group of its own, after a step: the same particles are
+    removed, the survivors take the same slots (removeEmptyParticles' swap
+    with the last one) and keep their state to 1e-12; a second call removes
+    nothing."""
+    sc = _scene("curl16")
+    lo, hi = sc.x.min(axis=0), sc.x.max(axis=0)
+    p = sc.params
+    p.terminator = True
+    p.terminator_center = tuple(0.5 * (lo + hi))
+    p.terminator_half = tuple(0.3 * (hi - lo))
+    p.terminator_radius = 0.25 * p.dx
+    p.terminator_inside = inside
+    r = oref.RefScene(sc, mic=True)
+    o = oo.OracleScene(sc)
+    # the step's first stage is the terminator (WetClothCore.cpp:97)
+    r.step(DT, snapshot=True)
+    o.step(DT, snapshot=True)
+    removed = int(r.get("terminate_removed")[0])
+    assert 0 < removed < sc.x.shape[0]
+    assert int(o.get("terminate_removed")[0]) == removed
+    for k in ("adv_x", "adv_v", "g2p_C"):
+        a, b = r.get(k), o.get(k)
+        assert a.shape == b.shape, k
+        assert np.abs(a - b).max() <= 1e-10 * max(np.abs(a).max(), 1.0), k
+    # and a call on its own after the step: particles that moved out
+    n = r.terminate()
+    assert o.terminate() == n
+    for k in ("term_x", "term_v", "term_C"):
+        a, b = r.get(k), o.get(k)
+        assert a.shape == b.shape, k
+        assert np.abs(a - b).max() <= 1e-10 * max(np.abs(a).max(), 1.0), k
+    assert r.terminate() == 0 and o.terminate() == 0
