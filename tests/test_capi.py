@@ -36,6 +36,27 @@ def test_default_params():
     L.wcg_default_params(ctypes.byref(p))
     assert p.criterion == 1e-6 and p.maxiters == 1000 and p.walls == 1
     assert p.precision == _capi.WCG_FP64
+    assert p.refine_inner_tol == 1e-5
+    assert p.terminator == 0 and p.terminator_inside == 1
+    assert list(p.terminator_half) == [0.5, 0.5, 0.5]
+
+
+def test_terminator_params_checked_before_device_work():
+    """A terminator box with a negative or non-finite extent is refused
+    before any device is touched."""
+    L = _capi.load()
+    h = ctypes.c_void_p()
+    p = _capi.WcgParams()
+    L.wcg_default_params(ctypes.byref(p))
+    p.dx = 1.0 / 16
+    p.terminator = 1
+    p.terminator_half[1] = -0.1
+    assert L.wcg_create(ctypes.byref(p), ctypes.byref(h)) == _capi.WCG_ERR_ARG
+    assert b"terminator" in L.wcg_last_error()
+    p.terminator_half[1] = 0.5
+    p.terminator_radius = float("nan")
+    assert L.wcg_create(ctypes.byref(p), ctypes.byref(h)) == _capi.WCG_ERR_ARG
+    assert L.wcg_terminate_liquid_particles(None, None) == _capi.WCG_ERR_ARG
 
 
 def test_argument_errors_without_device():
