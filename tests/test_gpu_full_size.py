@@ -93,3 +93,40 @@ def test_full_size_fp32_refine_against_fp64(full_scene, wcg):
     assert np.mean(dv > 1e-4 * vmax) <= 1e-4
     assert dv.max() <= 1e-2 * vmax
     assert np.quantile(dx, 0.9999) <= 1e-6 and dx.max() <= 1e-4
+
+
+def test_full_size_terminator_fp64(full_scene, wcg):
+    """terminateParticles at full size against a NumPy restatement of the box
+    phi (the same operations in the same order, no fused multiply-adds) and of
+    removeEmptyParticles' swap with the last particle: the survivors and their
+    order are bit-exact."""
+    sc = full_scene
+    p = sc.params
+    saved = (p.terminator, p.terminator_center, p.terminator_half, p.terminator_radius,
+             p.terminator_inside)
+    p.terminator, p.terminator_center = True, (0.4, 0.3, 0.55)
+    p.terminator_half, p.terminator_radius, p.terminator_inside = (0.3, 0.2, 0.35), 0.01, True
+    try:
+        g = FluidScene(sc)
+        removed = g.terminate_liquid_particles()
+        x, v, _ = g.download()
+        g.close()
+    finally:
+        (p.terminator, p.terminator_center, p.terminator_half, p.terminator_radius,
+         p.terminator_inside) = saved
+    c = np.array((0.4, 0.3, 0.55))
+    e = np.array((0.3, 0.2, 0.35))
+    x0 = sc.x
+    d = np.abs(((x0 - c) + c) - c) - e
+    da = np.maximum(d, 0.0)
+    m = np.minimum(np.maximum(np.maximum(d[:, 0], d[:, 1]), d[:, 2]), 0.0)
+    box = (m + np.sqrt(da[:, 0] * da[:, 0] + da[:, 1] * da[:, 1] + da[:, 2] * da[:, 2])) - 0.01
+    alive = (-1.0 * box >= 0.0) & (sc.vol >= 1e-20)
+    K = int(alive.sum())
+    assert removed == x0.shape[0] - K and 0 < removed < x0.shape[0]
+    idx = np.arange(x0.shape[0])
+    holes = idx[:K][~alive[:K]]
+    highs = idx[K:][alive[K:]]
+    order = idx[:K].copy()
+    order[holes] = highs[::-1]
+    assert np.array_equal(x, x0[order]) and np.array_equal(v, sc.v[order])
