@@ -57,7 +57,13 @@ typedef struct wcg_params {
   double box_radius;
   int walls;                       /* 1: the box above is present */
   double criterion;                /* pressure criterion: ||r||_inf <= c ||b||_inf */
-  int maxiters;                    /* PCG iteration limit */
+  int maxiters;                    /* PCG iteration limit.  wcg_default_params sets 1000,
+                                      not the reference integrator's 100
+                                      (App/TwoDSceneXMLParser.cpp:3265): that limit is sized
+                                      for the reference's multigrid-PCG (6-8 iterations),
+                                      while MIC(0)-PCG, this library's default solver, takes
+                                      up to about 230 iterations at 256^3.  Pass 100 with
+                                      WCG_SOLVER_MG for the reference's exact behaviour. */
   int precision;                   /* WCG_FP64 or WCG_FP32_REFINE */
   double refine_inner_tol;         /* FP32 inner-solve relative tolerance (default 1e-5;
                                       0: aim each inner solve at the criterion) */
@@ -302,6 +308,17 @@ int wcg_substep_vjp(wcg_ctx* ctx, double dt, const double* vbar3, const double* 
  * (0: off), as wcg_params sets them at creation. */
 int wcg_set_viscosity(wcg_ctx* ctx, double viscosity, int substeps);
 
+/* Failure handling of the MIC(0) wavefront (no reference counterpart; the
+ * reference's triangular solves are serial and never wait).  Each poll of a
+ * wavefront edge word is bounded by spin_limit polls (default 2^20); a wait
+ * that reaches it records a device error, the sweep finishes with zeros in
+ * place of the missing values, and the call returns WCG_ERR_DEVICE -- the
+ * context stays usable.  stale_patch >= 0 makes that patch of the pencil
+ * layout (indices past the last patch mean the last one) wait for a tag that
+ * no producer writes, so a test can run the limit out on purpose; -1 turns
+ * it off. */
+int wcg_set_wait_limit(wcg_ctx* ctx, long long spin_limit, int stale_patch);
+
 int wcg_get_stats(const wcg_ctx* ctx, wcg_stats* out);
 
 /* ---- parity downloads in the reference's dense bucket-major layout ---- */
@@ -327,6 +344,23 @@ int wcg_download_ifield(wcg_ctx* ctx, const char* name, long long* out, long lon
 int wcg_export_pressure_system(wcg_ctx* ctx, long long* ndof, long long* nnz,
                                long long* rowstart, long long* col,
                                double* val, double* rhs);
+
+/* ---- a sparse solve with the reference's PCGSolver call shape ---- */
+/* robertbridson::PCGSolver<double>::solve(matrix, rhs, result, residual_out,
+ * iterations_out) after set_solver_parameters(tolerance_factor,
+ * max_iterations) (libWetCloth/Core/PCGSolver/PCGSolver.h:249-308): MIC(0)
+ * preconditioned CG (modification 0.97, pivot ratio 0.25, as
+ * form_preconditioner fixes them) on the symmetric matrix given in CSR form --
+ * rowstart[n + 1], col[] strictly ascending inside each row, val[] -- which is
+ * the layout of the reference's SparseMatrix / FixedSparseMatrix rows.  x[n]
+ * receives the solution from a zero start; the stop rule is the reference's:
+ * ||r||_inf <= tolerance_factor * ||rhs||_inf.  Host arrays.  Returns WCG_OK
+ * when converged (the reference's true) and WCG_ERR_NOT_CONVERGED at the
+ * iteration limit or a zero/NaN rho (its false), with x, *residual_out and
+ * *iterations_out filled either way; WCG_ERR_ARG for a malformed matrix. */
+int wcg_pcg_solve_csr(const int* rowstart, const int* col, const double* val, int n,
+                      const double* rhs, double* x, double tolerance_factor,
+                      int max_iterations, double* residual_out, int* iterations_out);
 
 /* ---- many scenes at once (config 4 of the benchmark plan) ---- */
 /* A batch steps independent scenes (each created, uploaded and owned by the

@@ -166,6 +166,9 @@ SIGNATURES = {
                                                   ctypes.c_void_p, ctypes.c_void_p,
                                                   ctypes.c_void_p, ctypes.c_double,
                                                   ctypes.c_int, ctypes.c_void_p, _I, _D]),
+    "wcg_set_wait_limit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_int]),
+    "wcg_pcg_solve_csr": (ctypes.c_int, [_I, _I, _D, ctypes.c_int, _D, _D, ctypes.c_double,
+                                         ctypes.c_int, _D, _I]),
 }
 
 _lib = None
@@ -200,3 +203,25 @@ def check(code):
 
 def _dp(a):
     return a.ctypes.data_as(_D) if a is not None else None
+
+
+def pcg_solve_csr(rowstart, col, val, rhs, tolerance_factor, max_iterations):
+    """robertbridson::PCGSolver<double>::solve on a CSR matrix (wcg_pcg_solve_csr).
+    Returns (x, residual, iterations, status); status is WCG_OK or
+    WCG_ERR_NOT_CONVERGED (any other code raises)."""
+    L = load()
+    rs = np.ascontiguousarray(rowstart, dtype=np.int32)
+    cl = np.ascontiguousarray(col, dtype=np.int32)
+    vl = np.ascontiguousarray(val, dtype=np.float64)
+    b = np.ascontiguousarray(rhs, dtype=np.float64)
+    n = rs.shape[0] - 1
+    x = np.zeros(n, dtype=np.float64)
+    res = ctypes.c_double(0.0)
+    it = ctypes.c_int(0)
+    st = L.wcg_pcg_solve_csr(rs.ctypes.data_as(_I), cl.ctypes.data_as(_I), vl.ctypes.data_as(_D),
+                             n, b.ctypes.data_as(_D), x.ctypes.data_as(_D),
+                             float(tolerance_factor), int(max_iterations), ctypes.byref(res),
+                             ctypes.byref(it))
+    if st not in (WCG_OK, WCG_ERR_NOT_CONVERGED):
+        check(st)
+    return x, res.value, it.value, st

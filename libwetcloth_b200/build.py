@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libwcgpu.so")
-SOURCES = ["wcg_step.cu", "wcg_capi.cu", "wcg_noalloc.cu", "wcg_batch.cu"]
+SOURCES = ["wcg_step.cu", "wcg_capi.cu", "wcg_noalloc.cu", "wcg_batch.cu", "wcg_csr.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3",
               "-std=c++17", "-Xcompiler", "-fPIC", "-shared"]
 
@@ -33,10 +33,27 @@ def newest_source_mtime() -> float:
     return t
 
 
+OBJDIR = os.path.join(os.path.dirname(HERE), "_build", "wcgpu")
+
+
 def build(force: bool = False, verbose: bool = True) -> str:
+    """Compiles every translation unit to an object in parallel, then links."""
     if not force and os.path.exists(OUT) and os.path.getmtime(OUT) >= newest_source_mtime():
         return OUT
-    cmd = [nvcc(), *NVCC_FLAGS, "-o", OUT] + [os.path.join(CSRC, s) for s in SOURCES]
+    os.makedirs(OBJDIR, exist_ok=True)
+    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
+    objs, procs = [], []
+    for src in SOURCES:
+        obj = os.path.join(OBJDIR, os.path.splitext(src)[0] + ".o")
+        cmd = [nvcc(), *compile_flags, "-c", os.path.join(CSRC, src), "-o", obj]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        procs.append((cmd, subprocess.Popen(cmd)))
+        objs.append(obj)
+    failed = [cmd for cmd, p in procs if p.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, failed[0])
+    cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", OUT, *objs]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)

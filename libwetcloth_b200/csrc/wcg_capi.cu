@@ -714,6 +714,15 @@ int wcg_set_viscosity(wcg_ctx* ctx, double viscosity, int substeps) {
   return WCG_OK;
 }
 
+int wcg_set_wait_limit(wcg_ctx* ctx, long long spin_limit, int stale_patch) {
+  WCG_CHECK_CTX(ctx);
+  if (spin_limit < 1 || spin_limit > (1ll << 40))
+    return fail(WCG_ERR_ARG, "spin_limit must lie in [1, 2^40]");
+  ctx->c.spin_limit = spin_limit;
+  ctx->c.stale_patch = stale_patch < 0 ? -1 : stale_patch;
+  return WCG_OK;
+}
+
 int wcg_num_substeps(wcg_ctx* ctx, double dt, int* n_out) {
   WCG_CHECK_CTX(ctx);
   if (!n_out || !(dt > 0)) return fail(WCG_ERR_ARG, "bad argument");

@@ -250,6 +250,8 @@ struct Context {
   DevBuf pl_part;                // per-patch partials (double)
   long long pl_cap = 0;
   int pl_tickets = 0;            // sweep tickets handed out in this solve
+  long long spin_limit = 1ll << 20;  // polls of a wavefront edge word before giving up
+  int stale_patch = -1;          // failure-path test: a patch whose waits cannot succeed
   std::vector<int> pl_order_h;
 
   // multigrid-PCG: dense levels (d, ax, ay, az, x, b per cell; masks) and the
@@ -270,6 +272,8 @@ struct Context {
   DevBuf mwork;
   unsigned long long merge_count = 0;
   bool buckets_valid = false;    // pbucket holds the bucket of every current particle
+  bool maybe_empty = false;      // an upload since the last sub-step may have brought
+                                 // liquid particles without fluid volume
   unsigned long long split_count = 0;
   long long merged_removed = 0;  // particles the last merge removed
 

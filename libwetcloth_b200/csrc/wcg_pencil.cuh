@@ -235,6 +235,9 @@ struct PencilSweepArgs {
   double* part;  // per-patch partial: forward max|r|, backward z.r
   R omega, min_ratio;
   int* err;
+  long long spin_limit;  // polls of an edge word before the wait gives up
+  int stale_patch;       // failure-path test: this patch waits for a tag nothing
+                         // writes (-1: none)
 };
 
 // MODE: kFactor, kForward, kBackward.  UPD: the forward sweep first applies
@@ -346,6 +349,10 @@ __global__ void __launch_bounds__(kPatchLines, 1)
   u64* ea_dst = pub_a ? A.edge + edge_word(G, p, 0, 0, cl, EW) : nullptr;
   u64* ec_dst = pub_c ? A.edge + edge_word(G, p, 1, 0, al, EW) : nullptr;
   const unsigned ep = A.epoch;
+  // the tag this patch waits for: the launch's, except on the patch a
+  // failure-path test marks, whose waits then run into their limit
+  const unsigned ep_want = p == A.stale_patch ? (ep ^ 0x80000000u) : ep;
+  const long long spin_limit = A.spin_limit;
   const R al_r = (MODE == kForward && UPD) ? (R)A.sc[S_ALPHA] : R(0);
   const R omega = A.omega, min_ratio = A.min_ratio;
   // per-thread base pointers (patch and line applied); rows by 32-bit offset
@@ -422,17 +429,17 @@ __global__ void __launch_bounds__(kPatchLines, 1)
   auto ewait = [&](u64* wd, const u64* src) {
 #pragma unroll
     for (int k = 0; k < EW; ++k) {
-      if ((unsigned)(wd[k] >> 32) == ep) continue;
+      if ((unsigned)(wd[k] >> 32) == ep_want) continue;
       long long it = 0;
       do {
-        if (gave_up || ++it > kSpinLimit) {
+        if (gave_up || ++it > spin_limit) {
           if (!gave_up) record_error(A.err, kErrWaitTimeout);
           gave_up = true;
           wd[k] = (u64)ep << 32;
           break;
         }
         wd[k] = ld_relaxed_u64(src + k);
-      } while ((unsigned)(wd[k] >> 32) != ep);
+      } while ((unsigned)(wd[k] >> 32) != ep_want);
     }
   };
 
@@ -473,8 +480,8 @@ __global__ void __launch_bounds__(kPatchLines, 1)
         for (int k = 0; k < EW; ++k) {
           wd[k] = ld_own_u64(a0 + 8u * k);
           long long it = 0;
-          while ((unsigned)(wd[k] >> 32) != ep) {
-            if (gave_up || ++it > kSpinLimit) {
+          while ((unsigned)(wd[k] >> 32) != ep_want) {
+            if (gave_up || ++it > spin_limit) {
               if (!gave_up) record_error(A.err, kErrWaitTimeout);
               gave_up = true;
               break;

@@ -63,6 +63,7 @@ cudaError_t ctx_init(Context& c) {
   WCG_TRY(c.derr.ensure(sizeof(int)));
   WCG_TRY(c.ticket.ensure(16 * sizeof(int)));
   WCG_TRY(cudaMemsetAsync(c.derr.p, 0, sizeof(int), c.stream));
+  WCG_TRY(cudaMemsetAsync(c.dscalars.p, 0, 64 * sizeof(double), c.stream));
   return cudaStreamSynchronize(c.stream);
 }
 
@@ -138,14 +139,23 @@ ProfScope::~ProfScope() {
 
 // ---------------------------------------------------------------------------
 // particles
+
+// device word set by an upload that brought a liquid particle without fluid
+// volume (cleared when the sub-step removes such particles)
+static int* empty_word(Context& c) { return (int*)(c.dscalars.as<double>() + 52); }
+
 template <typename R>
 __global__ void k_load_particles(long long n, long long pcap, const double* x3,
                                  const double* v3, const double* C9,
                                  const double* m, const double* vol,
-                                 const double* rad, R* P, int* pid, int* err) {
+                                 const double* rad, R* P, int* pid, int* err,
+                                 int* empty) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   bool bad = !(m[i] >= 0.0) || !(vol[i] >= 0.0) || !(rad[i] >= 0.0);
+  // removeEmptyParticles drops liquid particles below 1e-20 of fluid volume
+  // at the start of every sub-step (TwoDScene.cpp:1717-1721)
+  if (vol[i] < 1e-20) *empty = 1;
   for (int a = 0; a < 3; ++a) {
     const double x = x3[i * 3 + a], v = v3[i * 3 + a];
     bad = bad || !isfinite(x) || !isfinite(v);
@@ -253,11 +263,12 @@ cudaError_t upload_particles(Context& c, long long n, const double* x3,
   if (c.prm.precision == 0)
     ++c.launches, k_load_particles<double><<<nblk(n, 256), 256, 0, c.stream>>>(
         n, c.pcap, dx3, dv3, dC9, dm, dvol, drad, c.pbuf[0].as<double>(),
-        c.pid[0].as<int>(), c.derr.as<int>());
+        c.pid[0].as<int>(), c.derr.as<int>(), empty_word(c));
   else
     ++c.launches, k_load_particles<float><<<nblk(n, 256), 256, 0, c.stream>>>(
         n, c.pcap, dx3, dv3, dC9, dm, dvol, drad, c.pbuf[0].as<float>(),
-        c.pid[0].as<int>(), c.derr.as<int>());
+        c.pid[0].as<int>(), c.derr.as<int>(), empty_word(c));
+  c.maybe_empty = true;
   WCG_TRY(cudaGetLastError());
   return cudaStreamSynchronize(c.stream);
 }
@@ -1285,6 +1296,9 @@ static PencilSweepArgs<R> pl_args(Context& c) {
   a.omega = (R)0.97;
   a.min_ratio = (R)0.25;
   a.err = c.derr.as<int>();
+  a.spin_limit = c.spin_limit;
+  a.stale_patch = c.stale_patch < 0 ? -1 : (int)std::min<long long>(c.stale_patch,
+                                                                     c.plg.npatch - 1);
   return a;
 }
 
@@ -2419,6 +2433,10 @@ static cudaError_t remove_flagged_t(Context& c, long long n, int* alive_slot, in
   c.np = K;
   c.have_grid = false;
   c.xw_valid = false;
+  // removeEmptyParticles re-sorts the bucket lists from the current positions
+  // after a removal (TwoDScene.cpp:1734-1743): a merge later in the sub-step
+  // re-buckets the survivors before it pairs them
+  c.buckets_valid = false;
   return cudaStreamSynchronize(c.stream);
 }
 
@@ -2616,10 +2634,23 @@ cudaError_t merge_liquid_particles(Context& c, int selector, const int* perm, lo
 }
 
 cudaError_t substep(Context& c, double dt) {
-  // terminateParticles (WetClothCore.cpp:97) ahead of the particle maintenance
-  if (c.prm.terminator && c.np > 0) {
+  // terminateParticles (WetClothCore.cpp:97) ahead of the particle maintenance;
+  // its removeEmptyParticles also runs without a terminator, and then only
+  // matters after an upload that brought particles without fluid volume
+  bool run_term = c.prm.terminator != 0;
+  if (!run_term && c.maybe_empty && c.np > 0) {
+    int flag = 0;
+    WCG_TRY(cudaMemcpyAsync(&flag, empty_word(c), sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    WCG_TRY(cudaStreamSynchronize(c.stream));
+    run_term = flag != 0;
+  }
+  if (run_term && c.np > 0) {
     long long rem = 0;
     WCG_TRY(terminate_liquid_particles(c, &rem));
+  }
+  if (c.maybe_empty) {
+    WCG_TRY(cudaMemsetAsync(empty_word(c), 0, sizeof(int), c.stream));
+    c.maybe_empty = false;
   }
   // updateOptiVolume, splitLiquidParticles, mergeLiquidParticles
   // (WetClothCore.cpp:97-110): the merge works on the buckets of the previous

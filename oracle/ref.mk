@@ -28,7 +28,12 @@ STDCXX := $(firstword $(wildcard /usr/lib/x86_64-linux-gnu/libstdc++.so.6 /usr/l
 # OpenMP runtime linked directly (the compiler driver's libgomp.spec may be absent)
 GOMP := $(firstword $(wildcard /usr/lib/x86_64-linux-gnu/libgomp.so.1 /usr/lib64/libgomp.so.1))
 
-all: $(OUT)/libwcref.so $(OUT)/libwcref_omp.so
+# The compiled reference-side binding (binding/GpuWetClothCore.h) with its
+# test harness, linked against the serial reference and libwcgpu.so.
+WCGPU_DIR := $(abspath $(HERE)../libwetcloth_b200)
+BFLAGS := $(SFLAGS) -I$(HERE)binding -I$(HERE)../include
+
+all: $(OUT)/libwcref.so $(OUT)/libwcref_omp.so $(OUT)/libwcbinding.so
 
 $(OUT)/obj-serial/%.o: $(CORE)/%.cpp
 	@mkdir -p $(dir $@)
@@ -53,3 +58,11 @@ $(OUT)/libwcref_omp.so: $(OBJS_P) $(OUT)/harness-omp.o
 	$(CXX) -shared -o $@ $^ $(STDCXX) $(GOMP) -lpthread
 
 .PHONY: all
+
+$(OUT)/binding-harness.o: $(HERE)binding/binding_harness.cpp $(HERE)binding/GpuWetClothCore.h $(HERE)../include/wetcloth_gpu.h
+	@mkdir -p $(OUT)
+	$(CXX) $(BFLAGS) -c $< -o $@
+
+$(OUT)/libwcbinding.so: $(OUT)/binding-harness.o $(OUT)/libwcref.so $(WCGPU_DIR)/libwcgpu.so
+	$(CXX) -shared -o $@ $(OUT)/binding-harness.o -L$(OUT) -lwcref -L$(WCGPU_DIR) -lwcgpu \
+	  -Wl,-rpath,'$$ORIGIN' -Wl,-rpath,'$$ORIGIN/../../libwetcloth_b200' $(STDCXX) -lpthread

@@ -58,6 +58,9 @@ def _lib(omp: bool):
         L.wcref_set_correction.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int,
                                            ctypes.c_double, ctypes.c_uint]
         L.wcref_merge.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_int]
+        L.wcref_pcg_solve_csr.argtypes = [_L, _L, _D, ctypes.c_int, _D, _D, ctypes.c_double,
+                                          ctypes.c_int, _D, ctypes.POINTER(ctypes.c_int)]
+        L.wcref_pcg_solve_csr.restype = ctypes.c_int
         L.wcref_merge.restype = ctypes.c_int
         L.wcref_split.argtypes = [ctypes.c_void_p, ctypes.c_uint]
         L.wcref_split.restype = ctypes.c_int
@@ -191,3 +194,66 @@ class RefScene:
         out = np.zeros(12)
         self.L.wcref_timers(self.h, _dp(out))
         return out
+
+
+def pcg_solve_csr(rowstart, col, val, rhs, tolerance, maxiter):
+    """The reference's robertbridson::PCGSolver<double>::solve on a CSR matrix
+    (MIC(0), 0.97 / 0.25).  Returns (x, residual, iterations, converged)."""
+    L = _lib(False)
+    rs = np.ascontiguousarray(rowstart, dtype=np.int64)
+    cl = np.ascontiguousarray(col, dtype=np.int64)
+    vl = np.ascontiguousarray(val, dtype=np.float64)
+    b = np.ascontiguousarray(rhs, dtype=np.float64)
+    n = rs.shape[0] - 1
+    x = np.zeros(n, dtype=np.float64)
+    res = ctypes.c_double(0.0)
+    it = ctypes.c_int(0)
+    ok = L.wcref_pcg_solve_csr(rs.ctypes.data_as(_L), cl.ctypes.data_as(_L),
+                               vl.ctypes.data_as(_D), n, b.ctypes.data_as(_D),
+                               x.ctypes.data_as(_D), float(tolerance), int(maxiter),
+                               ctypes.byref(res), ctypes.byref(it))
+    return x, res.value, it.value, bool(ok)
+
+
+def binding_available() -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", "libwcbinding.so"))
+
+
+def binding_step_both(scene, steps, dt, solver, precision, cell_multiplier=None):
+    """Steps two reference scenes built from `scene`: one with the reference's
+    WetClothCore::stepSystem, one with the compiled GpuWetClothCore binding
+    (oracle/binding/GpuWetClothCore.h) passing the scene's criterion and
+    iteration limit.  Returns ((x, v, C) reference, (x, v, C) binding,
+    sub-steps of the binding's last step)."""
+    B = ctypes.CDLL(os.path.join(HERE, "_ref", "libwcbinding.so"))
+    B.wcbind_set_cell_multiplier.argtypes = [ctypes.c_void_p, ctypes.c_double]
+    B.wcbind_step_both.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                   ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                   ctypes.c_int, ctypes.c_int, ctypes.c_longlong, _D, _D,
+                                   _L, _L, ctypes.POINTER(ctypes.c_int), ctypes.c_char_p,
+                                   ctypes.c_int]
+    B.wcbind_step_both.restype = ctypes.c_int
+    ra = RefScene(scene, mic=False)
+    rb = RefScene(scene, mic=False)
+    if cell_multiplier is not None:
+        B.wcbind_set_cell_multiplier(ra.h, cell_multiplier)
+        B.wcbind_set_cell_multiplier(rb.h, cell_multiplier)
+    cap = 4 * scene.x.shape[0] + 16
+    oa = np.zeros(15 * cap)
+    ob = np.zeros(15 * cap)
+    na, nb = ctypes.c_longlong(0), ctypes.c_longlong(0)
+    sub = ctypes.c_int(0)
+    err = ctypes.create_string_buffer(512)
+    rc = B.wcbind_step_both(ra.h, rb.h, int(steps), float(dt), float(scene.params.criterion),
+                            int(scene.params.maxiters), int(solver), int(precision), cap,
+                            oa.ctypes.data_as(_D), ob.ctypes.data_as(_D), ctypes.byref(na),
+                            ctypes.byref(nb), ctypes.byref(sub), err, 512)
+    ra.close()
+    rb.close()
+    if rc != 0:
+        raise RuntimeError(err.value.decode(errors="replace"))
+
+    def split(o, n):
+        return (o[:3 * n].reshape(n, 3), o[3 * n:6 * n].reshape(n, 3),
+                o[6 * n:15 * n].reshape(n, 9))
+    return split(oa, na.value), split(ob, nb.value), sub.value

@@ -96,6 +96,7 @@ struct Harness {
   bool corr_on = false;       // correctLiquidParticles before G2P (WetClothCore.cpp:242)
   unsigned corr_seed = 0, corr_count = 0;
   bool term_on = false;       // terminateParticles first (WetClothCore.cpp:97)
+  bool grid_built = false;    // a grid exists for removeEmptyParticles' re-sort
 };
 
 double now() {
@@ -509,11 +510,24 @@ int wcref_substep(void* hp, double sub_dt, int snapshot) {
   LinearizedImplicitEuler& e = *h->stepper;
   double t0 = now(), t1;
 
-  if (h->term_on) {
+  // terminateParticles runs every sub-step (WetClothCore.cpp:97); without a
+  // terminator only its removeEmptyParticles can change anything, and only
+  // when a liquid particle has no fluid volume
+  bool any_empty = false;
+  for (int i = s.getNumElastoParticles(); i < s.getNumParticles() && !any_empty; ++i)
+    any_empty = s.m_fluid_vol(i) < 1e-20;
+  if (h->term_on || any_empty) {
+    if (!h->grid_built) {
+      // the scene parser builds the grid at load (App/TwoDSceneXMLParser.cpp:725-727)
+      s.updateParticleBoundingBox();
+      s.rebucketizeParticles();
+      s.resampleNodes();
+    }
     const int before = s.getNumParticles();
     s.terminateParticles();
     h->ii["terminate_removed"] = {(long long)(before - s.getNumParticles())};
   }
+  h->grid_built = true;
   s.updateParticleBoundingBox();
   s.rebucketizeParticles();
   s.resampleNodes();
@@ -756,6 +770,7 @@ void wcref_set_terminator(void* hp, const double* c, const double* half, double 
   s.rebucketizeParticles();
   s.resampleNodes();
   h->term_on = true;
+  h->grid_built = true;
 }
 
 // TwoDScene::terminateParticles: liquid particles inside the terminator's
@@ -949,6 +964,35 @@ void wcref_timers(void* hp, double* out12) {
 
 int wcref_num_particles(void* hp) {
   return ((Harness*)hp)->scene->getNumParticles();
+}
+
+// The scene objects of a harness (shared_ptr<TwoDScene>,
+// shared_ptr<LinearizedImplicitEuler>), for code that drives them itself: the
+// compiled GpuWetClothCore binding test steps them with WetClothCore.
+const void* wcref_scene_sp(void* hp) { return &((Harness*)hp)->scene; }
+const void* wcref_stepper_sp(void* hp) { return &((Harness*)hp)->stepper; }
+
+// robertbridson::PCGSolver<double>::solve on a matrix given in CSR form: the
+// rows become a SparseMatrix (set_element keeps each row's columns sorted),
+// set_solver_parameters(tolerance, maxiter, 0.97, 0.25).  Returns the
+// solver's bool; x, *res and *iters as it leaves them.
+int wcref_pcg_solve_csr(const long long* rowstart, const long long* col, const double* val,
+                        int n, const double* rhs, double* x, double tolerance, int maxiter,
+                        double* res, int* iters) {
+  robertbridson::SparseMatrix<double> A((unsigned)n);
+  for (int i = 0; i < n; ++i)
+    for (long long p = rowstart[i]; p < rowstart[i + 1]; ++p)
+      A.set_element((unsigned)i, (unsigned)col[p], val[p]);
+  robertbridson::PCGSolver<double> solver;
+  solver.set_solver_parameters(tolerance, maxiter, 0.97, 0.25);
+  std::vector<double> b(rhs, rhs + n), out(n, 0.0);
+  double r = 0;
+  int it = 0;
+  const bool ok = solver.solve(A, b, out, r, it);
+  for (int i = 0; i < n; ++i) x[i] = out[i];
+  *res = r;
+  *iters = it;
+  return ok ? 1 : 0;
 }
 
 }  // extern "C"

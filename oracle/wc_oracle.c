@@ -2432,7 +2432,11 @@ int wco_substep(Scene* s, double dt, int snapshot) {
    * (WetClothCore.cpp:97-110); a split that adds particles re-sorts the
    * buckets (TwoDScene.cpp:2471-2478), so the merge after it sees the new
    * positions in the buckets of the last grid build */
-  if (s->p.term_on) {
+  /* terminateParticles runs every sub-step; without a terminator its
+   * removeEmptyParticles still drops liquid particles without fluid volume */
+  int any_empty = 0;
+  for (int i = s->ne; i < s->np && !any_empty; ++i) any_empty = s->vol[i] < 1e-20;
+  if (s->p.term_on || any_empty) {
     const long long nrem = wco_terminate_liquid(s);
     snap_put_i(s, "terminate_removed", &nrem, 1);
   }

@@ -31,3 +31,29 @@ def assert_close(gpu, ref, rtol, name, atol_abs=0.0):
     assert err <= atol_abs + rtol * scale, (
         f"{name}: max abs err {err:.3e} > {atol_abs:.1e} + {rtol:.1e} * {scale:.3e}")
     return err / scale
+
+
+def assert_pointwise(gpu, ref, rtol, name, floor_rel):
+    """Pointwise relative agreement where the reference is not small: every
+    finite entry with |ref| >= floor_rel * max|ref| must satisfy
+    |gpu - ref| <= rtol * |ref|.  Complements the max-normalised checks, which
+    a field with a wide dynamic range could pass while its small entries are
+    wrong.  Returns the largest pointwise relative error over those entries."""
+    g = np.asarray(gpu, dtype=np.float64).reshape(-1)
+    r = np.asarray(ref, dtype=np.float64).reshape(-1)
+    assert g.shape == r.shape, f"{name}: shape {g.shape} vs {r.shape}"
+    fin = np.isfinite(r)
+    assert np.array_equal(fin, np.isfinite(g)), f"{name}: finite-entry sets differ"
+    if not fin.any():
+        return 0.0
+    a = np.abs(r[fin])
+    if a.max() == 0:
+        return 0.0
+    keep = a >= floor_rel * a.max()
+    rel = np.abs(g[fin][keep] - r[fin][keep]) / a[keep]
+    worst = float(rel.max())
+    k = int(np.argmax(rel))
+    assert worst <= rtol, (f"{name}: pointwise relative error {worst:.3e} > {rtol:.1e} at "
+                           f"|ref| = {a[keep][k]:.3e} (floor {floor_rel:.0e} x max {a.max():.3e}, "
+                           f"{int(keep.sum())} entries checked)")
+    return worst

@@ -129,3 +129,36 @@ def test_run_to_run_determinism(precision, wcg):
         g.close()
     for a, b in zip(res[0], res[1]):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("precision", [_capi.WCG_FP64, _capi.WCG_FP32_REFINE])
+def test_wavefront_wait_limit_reached(precision, wcg):
+    """The wavefront's bounded waits, run out on purpose: the last patch of
+    the pencil layout waits for an edge-word tag no producer writes, with a
+    limit of 200 polls.  The solve comes back (no hang) with WCG_ERR_DEVICE
+    naming the wait limit, as the reference's PCGSolver::solve would return
+    false; after the hook is cleared the same context steps again and matches
+    a fresh context bit for bit."""
+    sc = scenes.half_box(48, 2, 5, amplitude=0.5, sigma_cells=2.0)  # several patches
+    g = FluidScene(sc, precision=precision)
+    L = g.L
+    _capi.check(L.wcg_set_wait_limit(g.h, 200, 1 << 30))
+    g.rebucketize_and_resample()
+    g.map_particle_nodes()
+    g.step_velocity(1e-3)
+    with pytest.raises(_capi.WcgError) as e:
+        g.project_fine(1e-3)
+    assert e.value.code == _capi.WCG_ERR_DEVICE
+    assert "wait limit" in str(e.value)
+    # back to the default limit and no stale patch: the context works
+    _capi.check(L.wcg_set_wait_limit(g.h, 1 << 20, -1))
+    g.upload(sc.x, sc.v, sc.C, sc.mass, sc.vol, sc.radius)
+    g.step(1e-3)
+    x, v, C = g.download()
+    h = FluidScene(sc, precision=precision)
+    h.step(1e-3)
+    x2, v2, C2 = h.download()
+    assert np.array_equal(x, x2) and np.array_equal(v, v2) and np.array_equal(C, C2)
+    assert L.wcg_set_wait_limit(g.h, 0, -1) == _capi.WCG_ERR_ARG
+    g.close()
+    h.close()

@@ -223,3 +223,64 @@ def test_terminator_steps(prec, wcg):
             _close(v, o.get("g2p_v"), 1e-5, "g2p_v")
             _close(x, ox, 1e-6, "adv_x")
     g.close()
+
+
+@pytest.mark.parametrize("split", [False, True])
+def test_terminator_then_merge_steps(split, wcg):
+    """The terminator removes particles first in each sub-step; the merge
+    after it pairs the survivors in buckets re-sorted from their current
+    positions (removeEmptyParticles re-sorts them after any removal,
+    TwoDScene.cpp:1734-1743), optionally after a split.  Three FP64 steps:
+    the same removals and the same state as the oracle."""
+    sc = scenes.mixed_volumes(_terminator_scene(True), 17,
+                              mrel=(0.3, 0.7, 1.0, 2.5, 7.0) if split else
+                              (0.3, 0.7, 1.0, 1.5, 2.5))
+    sc.params.particle_merge = True
+    sc.params.merge_seed = 9
+    if split:
+        sc.params.particle_split = True
+        sc.params.split_seed = 21
+    o = oo.OracleScene(sc)
+    g = FluidScene(sc)
+    term = 0
+    for _ in range(3):
+        o.step(DT, snapshot=True)
+        g.step(DT)
+        term += int(o.get("terminate_removed")[0])
+    assert term > 0
+    n = int(o.get("adv_x").size // 3)
+    assert g.num_particles == n
+    x, v, C = g.download()
+    _close(v, o.get("g2p_v"), 1e-10, "g2p_v")
+    _close(x, o.get("adv_x"), 1e-12, "adv_x")
+    g.close()
+
+
+@pytest.mark.parametrize("prec", [_capi.WCG_FP64, _capi.WCG_FP32_REFINE])
+def test_zero_volume_particles_dropped_without_terminator(prec, wcg):
+    """terminateParticles runs every sub-step (WetClothCore.cpp:97) and its
+    removeEmptyParticles drops liquid particles below 1e-20 of fluid volume
+    even without a terminator: uploaded zero-volume particles are gone after
+    the first step, in the reference's swap-with-last order."""
+    sc = scenes.dam_break(16, 8, 0)
+    sc.vol = sc.vol.copy()
+    sc.vol[[3, 100, 101, len(sc.vol) - 2]] = 0.0
+    o = oo.OracleScene(sc)
+    g = FluidScene(sc, precision=prec)
+    o.step(DT, snapshot=True)
+    g.step(DT)
+    assert int(o.get("terminate_removed")[0]) == 4
+    n = int(o.get("adv_x").size // 3)
+    assert n == sc.x.shape[0] - 4 and g.num_particles == n
+    x, v, C = g.download()
+    if prec == _capi.WCG_FP64:
+        _close(v, o.get("g2p_v"), 1e-10, "g2p_v")
+        _close(x, o.get("adv_x"), 1e-12, "adv_x")
+    else:
+        _close(v, o.get("g2p_v"), 1e-5, "g2p_v fp32")
+        _close(x, o.get("adv_x"), 1e-6, "adv_x fp32")
+    # the second step has nothing left to remove
+    o.step(DT, snapshot=True)
+    g.step(DT)
+    assert g.num_particles == n
+    g.close()

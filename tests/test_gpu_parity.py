@@ -8,7 +8,11 @@ Tolerances: integer/index data bit-exact (sort keys, bucket ranges,
 activation masks, stencil indices, DOF numbering, matrix structure, valid
 masks); FP64 fields within 1e-10 relative to the field's max magnitude; the
 PCG-dependent pressure and everything after it within 1e-9 (the same MIC(0)
-iterates, accumulated in a different order).
+iterates, accumulated in a different order).  Pointwise: every entry above
+1e-6 of its field's largest magnitude agrees to 1e-10 of itself in the P2G and
+grid-update fields, and every entry above 1e-4 of the largest to 1e-6 of
+itself in the pressure and the fields after it (a PCG solution's small
+entries carry the rounding of the whole solve).
 """
 import numpy as np
 import pytest
@@ -17,7 +21,7 @@ from libwetcloth_b200 import scenes
 from libwetcloth_b200.solver import FluidScene
 from oracle import oracle as oo
 from oracle import ref as oref
-from tests.parity import assert_close, assert_dense_close
+from tests.parity import assert_close, assert_dense_close, assert_pointwise
 
 pytestmark = pytest.mark.gpu
 
@@ -133,12 +137,14 @@ def test_p2g_fields(pair):
     sc, r, out = pair
     for k in P2G_FIELDS:
         assert_dense_close(out[k], r.get(k), 1e-10, k)
+        assert_pointwise(out[k], r.get(k), 1e-10, k, 1e-6)
 
 
 def test_predict_fields(pair):
     sc, r, out = pair
     for k in PREDICT_FIELDS:
         assert_dense_close(out[k], r.get(k), 1e-10, k)
+        assert_pointwise(out[k], r.get(k), 1e-10, k, 1e-6)
 
 
 def test_pressure_system(pair):
@@ -159,6 +165,7 @@ def test_pressure_mic_pcg(pair):
     assert st["converged"] == 1
     assert st["residual"] <= sc.params.criterion * st["rhs_norm"]
     assert_dense_close(out["pressure"], r.get("pressure"), 1e-9, "pressure")
+    assert_pointwise(out["pressure"], r.get("pressure"), 1e-6, "pressure", 1e-4)
 
 
 def test_projection_and_constraint(pair):
@@ -167,6 +174,7 @@ def test_projection_and_constraint(pair):
         assert np.array_equal(out["valid_" + a], r.get("valid_" + a)), "valid_" + a
         assert_dense_close(out["u_proj_" + a], r.get("u_proj_" + a), 1e-9, "u_proj_" + a)
         assert_dense_close(out["u_final_" + a], r.get("u_final_" + a), 1e-9, "u_final_" + a)
+        assert_pointwise(out["u_final_" + a], r.get("u_final_" + a), 1e-6, "u_final_" + a, 1e-4)
 
 
 def test_g2p_and_advect(pair):
@@ -175,6 +183,8 @@ def test_g2p_and_advect(pair):
     assert_close(out["g2p_v"], r.get("g2p_v").reshape(n, 3), 1e-9, "G2P velocity")
     assert_close(out["g2p_C"], r.get("g2p_C").reshape(n, 9), 1e-9, "G2P affine C")
     assert_close(out["adv_x"], r.get("adv_x").reshape(n, 3), 1e-12, "advected x")
+    assert_pointwise(out["g2p_v"], r.get("g2p_v").reshape(n, 3), 1e-6, "G2P velocity", 1e-4)
+    assert_pointwise(out["adv_x"], r.get("adv_x").reshape(n, 3), 1e-12, "advected x", 1e-6)
 
 
 @pytest.mark.parametrize("chk", ["oracle", "reference"])

@@ -411,3 +411,23 @@ def test_terminate_particles(inside):
         assert a.shape == b.shape, k
         assert np.abs(a - b).max() <= 1e-10 * max(np.abs(a).max(), 1.0), k
     assert r.terminate() == 0 and o.terminate() == 0
+
+
+def test_zero_volume_particles_removed_every_substep():
+    """terminateParticles runs in every sub-step (WetClothCore.cpp:97), so its
+    removeEmptyParticles drops liquid particles without fluid volume even
+    with no terminator: the same particles leave, the survivors take the same
+    slots, and the step agrees to the step tolerances."""
+    sc = _scene("dam16")
+    sc.vol = sc.vol.copy()
+    sc.vol[[3, 100, 101, len(sc.vol) - 2]] = 0.0
+    r = oref.RefScene(sc, mic=True)
+    o = oo.OracleScene(sc)
+    r.step(DT, snapshot=True)
+    o.step(DT, snapshot=True)
+    assert int(r.get("terminate_removed")[0]) == 4
+    assert int(o.get("terminate_removed")[0]) == 4
+    for k in ("adv_x", "adv_v", "g2p_C"):
+        a, b = r.get(k), o.get(k)
+        assert a.shape == b.shape, k
+        assert np.abs(a - b).max() <= 1e-10 * max(np.abs(a).max(), 1.0), k

@@ -8,7 +8,9 @@ wcg_project_fine; its assembled system (DOF mask, diagonal, couplings, rhs) is
 copied into device buffers owned by the test and solved twice in a row by the
 allocation-free entry point.  Both results must match the pressure
 wcg_project_fine produced, within the 1e-9 relative tolerance the other
-pressure tests use.
+pressure tests use.  One scene's grid has exactly the 2048-bucket limit
+(16 x 8 x 16 buckets), so the copies and kernels reach the last offsets of
+the static array.
 """
 import ctypes
 
@@ -40,12 +42,22 @@ def _assembled(sc):
     return dims, dof, fields, iters, crit, maxit
 
 
-@pytest.mark.parametrize("kind", ["dam16", "curl32"])
+def _scene(kind):
+    if kind == "dam16":
+        return scenes.dam_break(16, 8, 0)
+    if kind == "curl32":
+        return scenes.half_box(32, 2, 5, amplitude=0.5, sigma_cells=2.0)
+    # a thin block whose grid is exactly 16 x 8 x 16 = 2048 buckets
+    return scenes.dam_break(48, 2, 0, block_hi=(0.7, 0.1, 0.7))
+
+
+@pytest.mark.parametrize("kind", ["dam16", "curl32", "limit2048"])
 def test_noalloc_matches_project_fine(kind, wcg):
     import torch
-    sc = scenes.dam_break(16, 8, 0) if kind == "dam16" else \
-        scenes.half_box(32, 2, 5, amplitude=0.5, sigma_cells=2.0)
+    sc = _scene(kind)
     dims, dof, f, iters_ref, crit, maxit = _assembled(sc)
+    if kind == "limit2048":
+        assert int(np.prod(dims)) == 2048, dims
     dev = torch.device("cuda:0")
     d_dof = torch.from_numpy(dof.astype(np.uint8)).to(dev)
     d = {k: torch.from_numpy(np.ascontiguousarray(f[k])).to(dev)
