@@ -51,6 +51,13 @@ def parse():
     ap.add_argument("--batch-scenes", type=int, default=32)
     ap.add_argument("--no-cloth", action="store_true",
                     help="skip the liquid-on-cloth measurement (128^3 sphere on a sheet)")
+    ap.add_argument("--no-config0", action="store_true",
+                    help="skip the 64^3 dam-break line (100 steps)")
+    ap.add_argument("--no-ref-mic", action="store_true",
+                    help="reference arm: skip the MIC(0)-PCG run")
+    ap.add_argument("--ref-budget-s", type=float, default=1500.0,
+                    help="reference arm: wall-clock budget of the timed steps")
+    ap.add_argument("--ref-child", default=None, help=argparse.SUPPRESS)
     return ap.parse_args()
 
 
@@ -517,9 +524,10 @@ class _quiet_stdout:
 
 
 def run_reference_cpu(args, sample_n, steps=2, warmup=1):
-    """The reference Core (oracle/_ref, OpenMP stand-in for TBB, all host
-    threads) on a bounded sample: the same scene type at sample_n^3, ms/step
-    scaled by particle count to the full workload."""
+    """cpu_baseline of this arm: the reference Core (oracle/_ref, OpenMP
+    stand-in for TBB, all host threads) on a bounded sample -- the same scene
+    generator at sample_n^3 -- ms/step scaled by particle count to the full
+    workload (the reference arm, --impl reference, times the full workload)."""
     from libwetcloth_b200 import scenes
     from oracle import ref as oref
     if not oref.available(omp=True):
@@ -527,7 +535,6 @@ def run_reference_cpu(args, sample_n, steps=2, warmup=1):
     cores = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(cores))
     sc = scenes.half_box(sample_n, args.ppc, seed=1)
-    full_np = None
     with _quiet_stdout():
         r = oref.RefScene(sc, mic=False, omp=True)
         for _ in range(warmup):
@@ -538,7 +545,6 @@ def run_reference_cpu(args, sample_n, steps=2, warmup=1):
         dt = (time.perf_counter() - t0) / steps
         r.close()
     n_sample = sc.x.shape[0]
-    # full-workload particle count of the same generator
     full_np = args.ppc * args.n * (args.n // 2) * args.n
     scale = full_np / n_sample
     return {"value": round(dt * 1000 * scale, 1), "unit": "ms/step",
@@ -546,7 +552,124 @@ def run_reference_cpu(args, sample_n, steps=2, warmup=1):
             "sample": f"reference Core (multigrid-PCG default solver) on half_box "
                       f"{sample_n}^3/{n_sample} particles, {steps} steps after {warmup} "
                       f"warm-up, {dt*1000:.1f} ms/step x {scale:.1f} (particle ratio); "
-                      f"OpenMP stand-in for TBB"}, None
+                      f"OpenMP stand-in for TBB; the full workload is timed by "
+                      f"--impl reference"}, None
+
+
+def _ref_child(spec):
+    """Child process of the reference arm: the reference Core on one scene,
+    `warmup` untimed then up to `steps` timed WetClothCore steps, stopping
+    early (and saying so) when the next step would pass the deadline.  Prints
+    one JSON line; progress with the resident set size goes to stderr."""
+    import resource
+    from libwetcloth_b200 import scenes
+    from oracle import ref as oref
+    t_start = time.time()
+    if spec["scene"] == "half_box":
+        sc = scenes.half_box(spec["n"], spec["ppc"], seed=1)
+    else:
+        sc = scenes.dam_break(spec["n"], 8, 0)
+    rss = lambda: resource.getrusage(resource.RUSAGE_SELF).ru_maxrss / 1e6
+    print(f"scene {sc.x.shape[0]} particles, rss {rss():.1f} GB", file=sys.stderr, flush=True)
+    with _quiet_stdout():
+        r = oref.RefScene(sc, mic=spec["mic"], omp=True)
+        print(f"created, rss {rss():.1f} GB", file=sys.stderr, flush=True)
+        for k in range(spec["warmup"]):
+            r.step(DT, snapshot=False)
+            print(f"warm-up step {k}, rss {rss():.1f} GB", file=sys.stderr, flush=True)
+        times = []
+        while len(times) < spec["steps"]:
+            if times and time.time() + max(times) > t_start + spec["budget_s"]:
+                break
+            t0 = time.perf_counter()
+            r.step(DT, snapshot=False)
+            times.append(time.perf_counter() - t0)
+            print(f"step {len(times)}: {times[-1]:.2f} s, rss {rss():.1f} GB", file=sys.stderr,
+                  flush=True)
+        iters = r.amg_stats()[0] if not spec["mic"] else r.solver_stats()[0]
+        r.close()
+    print(json.dumps({"ms_per_step": 1000.0 * sum(times) / len(times), "steps": len(times),
+                      "particles": int(sc.x.shape[0]), "rss_gb": round(rss(), 2),
+                      "last_solver_iters": int(iters)}), flush=True)
+
+
+def _run_ref_child(spec, timeout_s):
+    """Runs _ref_child in a fresh interpreter; returns (result, None) or
+    (None, why) when the child failed (out of memory, killed, timed out)."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--ref-child", json.dumps(spec)]
+    try:
+        out = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout_s, cwd=ROOT)
+    except subprocess.TimeoutExpired as e:
+        err = (e.stderr or b"").decode(errors="replace") if isinstance(e.stderr, bytes) else \
+            (e.stderr or "")
+        return None, f"timed out after {timeout_s} s; last progress: {err.strip()[-200:]}"
+    lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
+    if out.returncode != 0 or not lines:
+        return None, (f"reference process exited with status {out.returncode}; "
+                      f"last progress: {out.stderr.strip()[-300:]}")
+    return json.loads(lines[-1]), None
+
+
+def run_reference_arm(args, world):
+    """--impl reference: the reference's own CPU implementation of the path
+    (the compiled reference Core, oracle/_ref/libwcref_omp.so, OpenMP
+    stand-in for TBB, all host threads) on this arm's workload -- the
+    half_box n^3 scene at ppc particles per cell, seeded as in the GPU arm --
+    for the requested warm-up and timed steps, with its default solver
+    (multigrid-PCG, as solveNodePressure calls it).  A MIC(0)-PCG run of the
+    same scene (the GPU headline's solver) and the 64^3 dam break
+    (100 steps) follow as sub-objects."""
+    from oracle import ref as oref
+    if not oref.available(omp=True):
+        return {"impl": "reference", "unavailable": "oracle/_ref/libwcref_omp.so not built"}
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    threads = int(os.environ["OMP_NUM_THREADS"])
+    spec = {"scene": "half_box", "n": args.n, "ppc": args.ppc, "mic": False,
+            "warmup": args.warmup, "steps": args.steps, "budget_s": args.ref_budget_s}
+    main, why = _run_ref_child(spec, args.ref_budget_s + 900)
+    if main is None:
+        return {"impl": "reference",
+                "unavailable": f"reference Core on half_box {args.n}^3: {why}"}
+    value = round(main["ms_per_step"], 1)
+    workload = (f"half_box {args.n}^3, {args.ppc} ppc, {main['particles']} particles, dt {DT}, "
+                "reference Core WetClothCore::stepSystem, multigrid-PCG to 1e-6")
+    out = {
+        "metric": METRIC, "value": value, "unit": "ms/step", "impl": "reference",
+        "n_gpus": world, "steps": main["steps"], "warmup": args.warmup,
+        "ms_per_step": value, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded half-filled box, "
+                                                     "curl-noise velocity)",
+        "config": {"workload": workload, "grid": args.n, "particles": main["particles"],
+                   "threads": threads, "rss_gb": main["rss_gb"]},
+        "cpu_baseline": {"value": value, "unit": "ms/step", "cores": threads,
+                         "kind": "reference",
+                         "sample": f"the full workload: {main['steps']} steps after "
+                                   f"{args.warmup} warm-up (OpenMP stand-in for TBB)"},
+        "e2e": {"value": value, "unit": "ms/step", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    if main["steps"] < args.steps:
+        out["steps_requested"] = args.steps
+        out["note"] = (f"stopped after {main['steps']} timed steps: the next would have "
+                       f"passed the {args.ref_budget_s} s budget")
+    if not args.no_ref_mic:
+        spec_mic = dict(spec, mic=True, warmup=1, steps=1, budget_s=900)
+        mic, why = _run_ref_child(spec_mic, 1800)
+        out["mic0"] = ({"ms_per_step": round(mic["ms_per_step"], 1), "steps": mic["steps"],
+                        "warmup": 1, "pcg_iters": mic["last_solver_iters"],
+                        "note": "the same scene with the assembled system re-solved by the "
+                                "reference's own PCGSolver<double> (MIC(0)), the GPU "
+                                "headline's solver"} if mic else {"unavailable": why})
+    if not args.no_config0:
+        spec0 = {"scene": "dam_break", "n": 64, "ppc": 8, "mic": False, "warmup": 3,
+                 "steps": 97, "budget_s": 900}
+        c0, why = _run_ref_child(spec0, 1500)
+        out["config0"] = ({"workload": "dam break 64^3, 8 ppc, seed 0, 265302 particles, "
+                                       "100 steps (3 warm-up + 97 timed)",
+                           "ms_per_step": round(c0["ms_per_step"], 2), "steps": c0["steps"],
+                           "warmup": 3} if c0 else {"unavailable": why})
+    return out
 
 
 def main():
@@ -554,24 +677,13 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.ref_child:
+        _ref_child(json.loads(args.ref_child))
+        return 0
     if args.impl == "reference":
         if rank != 0:
             return 0
-        cpu, why = run_reference_cpu(args, args.cpu_sample_n, steps=max(1, min(args.steps, 3)),
-                                     warmup=min(args.warmup, 1))
-        if cpu is None:
-            print(json.dumps({"impl": "reference", "unavailable": why}))
-            return 0
-        print(json.dumps({
-            "metric": METRIC, "value": cpu["value"], "unit": "ms/step", "impl": "reference",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": cpu["value"], "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"half_box {args.n}^3, {args.ppc} ppc (bounded sample, "
-                                   "scaled)"},
-            "cpu_baseline": cpu,
-            "e2e": {"value": cpu["value"], "unit": "ms/step", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}))
+        print(json.dumps(run_reference_arm(args, world)))
         return 0
     import torch
     if world > 1:

@@ -76,9 +76,11 @@ typedef struct wcg_params {
   double elasto_advect_coeff;      /* LiquidInfo::elasto_advect_coeff (1.0) */
   double drag_viscosity;           /* LiquidInfo::viscosity as the liquid-solid drag reads it
                                       while the viscosity term is off (8.9e-3) */
-  double correction_strength;      /* LiquidInfo::correction_strength; 0 (default here) turns
-                                      correctLiquidParticles off, the reference's scene
-                                      parser defaults it to 0.2 */
+  double correction_strength;      /* LiquidInfo::correction_strength (default here 0; the
+                                      reference's scene parser defaults it to 0.2).
+                                      correctLiquidParticles runs in every sub-step; at 0
+                                      its springs vanish and it only projects its particle
+                                      subset out of the solid, as the reference does */
   int correction_step;             /* LiquidInfo::correction_step (8) */
   double correction_multiplier;    /* LiquidInfo::correction_multiplier (2.0) */
   unsigned long long correction_seed; /* seed of the stream that picks each sub-step's
@@ -236,7 +238,8 @@ int wcg_constrain_liquid_velocity(wcg_ctx* ctx);
  * WetClothCore::stepSystem does (WetClothCore.cpp:242); G2P then keeps the
  * weights of the positions before the correction.  Coincident pairs (closer
  * than 1e-4 re) are pushed by a SplitMix64 hash of their indices instead of
- * scalarRand. */
+ * scalarRand.  With correction_strength 0 the subset is only projected out
+ * of the solid (the springs vanish), one particle at a time. */
 int wcg_correct_liquid_particles(wcg_ctx* ctx, double dt, int selector);
 /* the subset wcg_substep corrects in its k-th call: SplitMix64 of the seed and
  * k, modulo step */

@@ -297,6 +297,8 @@ int wcg_create(const wcg_params* params, wcg_ctx** out) {
   if (const char* v = getenv("WCG_SWEEP_TILE")) ctx->c.sweep_variant = !strcmp(v, "warp") ? 1 : 0;
   // layout of the pressure solve (performance knob; same arithmetic)
   if (const char* v = getenv("WCG_PCG_LAYOUT")) ctx->c.pcg_layout = !strcmp(v, "tiles") ? 1 : 0;
+  // transfer formulation: bucket tiles (default) or the global gathers
+  if (const char* v = getenv("WCG_TRANSFERS")) ctx->c.xfer_mode = !strcmp(v, "gather") ? 1 : 0;
   // CTAs per thread-block cluster along c in the MIC(0) sweeps (1, 2, 4 or 8;
   // performance knob, identical results)
   if (const char* v = getenv("WCG_SWEEP_CLUSTER")) {

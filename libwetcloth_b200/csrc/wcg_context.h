@@ -237,6 +237,8 @@ struct Context {
   long long n_active = 0;
   int drange_h[6] = {0, 0, 0, 1, 1, 1};  // min/max stencil offset per axis
   DevBuf active_list;            // compacted active buckets (int32)
+  DevBuf p2g_halo;               // P2G halo tile per bucket (kTileVals Reals)
+  int xfer_mode = 0;             // 0: bucket-tile P2G/G2P where they apply, 1: global gathers
 
   // pressure solve in the pencil layout (default) or on 8^3 tiles
   int pcg_layout = 0;            // 0: pencil layout, 1: bucket-major tiles

@@ -139,4 +139,34 @@ __global__ void __launch_bounds__(128)
   }
 }
 
+// correctLiquidParticles at correction_strength 0 (TwoDScene.cpp:1967-2061):
+// every spring weight is 0, so a selected particle (original index % step ==
+// selector) only moves out of the solid -- phi_now = phi, and by -phi grad
+// when phi < 0 -- and reads nothing but its own position and the grid, so a
+// thread per particle gives the reference's result whatever the order.  XW
+// receives every particle's position before the pass (G2P keeps its weights).
+template <typename R>
+__global__ void k_correct_project(GridDesc g, R* __restrict__ P, long long pcap, long long np,
+                                  const int* __restrict__ pid, const long long* __restrict__ key,
+                                  const int* __restrict__ delta,
+                                  const unsigned char* __restrict__ active,
+                                  const R* __restrict__ F, long long fstride,
+                                  R* __restrict__ XW, int selector, int step) {
+  const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= np) return;
+  const R pos[3] = {P[PX * pcap + s], P[PY * pcap + s], P[PZ * pcap + s]};
+  for (int a = 0; a < 3; ++a) XW[a * pcap + s] = pos[a];
+  if (pid[s] % step != selector) return;
+  const long long kn = key[s];
+  if (kn < 0) return;
+  int KI, KJ, KK;
+  node_ijk(g, kn, KI, KJ, KK);
+  const int kp[3] = {KI - 1, KJ - 1, KK - 1};
+  R phi, gr[3];
+  solid_sample<R>(g, active, F, fstride, kp, delta[s], pos, pos, phi, gr);
+  const R phi_now = phi + (gr[0] * R(0) + gr[1] * R(0) + gr[2] * R(0));
+  if (phi_now < R(0))
+    for (int a = 0; a < 3; ++a) P[(PX + a) * pcap + s] = pos[a] - phi_now * gr[a];
+}
+
 }  // namespace wcg

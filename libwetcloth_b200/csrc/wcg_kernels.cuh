@@ -394,6 +394,246 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// ---- P2G as a particle scatter into bucket halo tiles -----------------------
+// The same sums as k_p2g (mapParticleNodesAPIC TwoDScene.cpp:6609-6919 liquid
+// branch, updateLiquidPhi :3286-3345, mapParticleSaturationPsiNodes
+// :5952-5992), computed particle by particle instead of node by node, so each
+// particle's per-axis weights are evaluated once.
+//
+// Halo tile of bucket B: every node the stencils of B's particles reach.  A
+// particle with key cell c (the p-stencil centre) and stencil offsets delta in
+// {0, 1} reaches cell-centre nodes c-1..c+1 on each axis and, for the face of
+// axis a, nodes c-1+delta_a..c+1+delta_a on axis a.  Over c in [4B, 4B+3] that
+// is [4B-1, 4B+4] (6 nodes) per axis and [4B-1, 4B+5] (7) on the face's own
+// axis.  Tile layout (R values): for each face axis a, mass, momentum and
+// volume (kHaloF each); then the cell-centre volume and liquid phi (kHaloC).
+constexpr int kHaloF = 7 * 6 * 6;
+constexpr int kHaloC = 6 * 6 * 6;
+constexpr int kTileVals = 9 * kHaloF + 2 * kHaloC;
+
+// index of halo node (x, y, z) (offsets from 4B - 1) in a face-a tile
+__device__ inline int halo_face(int a, int x, int y, int z) {
+  const int nx = a == 0 ? 7 : 6, ny = a == 1 ? 7 : 6;
+  return (z * ny + y) * nx + x;
+}
+__device__ inline int halo_centre(int x, int y, int z) { return (z * 6 + y) * 6 + x; }
+
+// Scatter: one warp per active bucket (WPB warps per block, each with its own
+// tile).  The bucket's particles (key cells in the bucket: one contiguous run
+// of the sorted arrays) are visited one at a time in sorted order; lane l < 27
+// is stencil slot (l % 3, l / 3 % 3, l / 9) of the visited particle, so the 27
+// lanes write 27 distinct nodes per node type and the warp adds into its tile
+// without atomics, every node receiving its contributions in sorted-particle
+// order: deterministic.  Lanes 0..17 evaluate the particle's 18 per-axis
+// weights (3 axes x offsets 0 and 1/2 x 3 nodes) once; the slot lanes take
+// theirs by shuffle.  Requires stencil offsets in {0, 1} (checked on the host).
+template <typename R, int WPB>
+__global__ void __launch_bounds__(32 * WPB)
+    k_p2g_scatter(GridDesc g, const int* __restrict__ active_list, long long n_active,
+                  const R* __restrict__ P, long long pcap, const int* __restrict__ start,
+                  const long long* __restrict__ key, const int* __restrict__ delta,
+                  R* __restrict__ halo) {
+  __shared__ R tiles[WPB][kTileVals];
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const long long ai = (long long)blockIdx.x * WPB + wid;
+  if (ai >= n_active) return;
+  const int b = active_list[ai];
+  const long long n0 = (long long)b * 64;
+  const int p0 = start[n0], p1 = start[n0 + 64];
+  if (p1 <= p0) return;  // no particles: the merge skips this bucket
+  R* T = tiles[wid];
+  const R bs = (R)g.bs, dx = (R)g.dx;
+  const R invh = R(1) / dx;
+  const R rmin = dx * (R)kLiquidPhiRadius;
+  const R three_bs = R(3) * bs;
+  for (int e = lane; e < kTileVals; e += 32) T[e] = e < 9 * kHaloF + kHaloC ? R(0) : three_bs;
+  __syncwarp();
+  const int bk = b / (g.ni * g.nj);
+  const int rem = b - bk * g.ni * g.nj;
+  const int bj = rem / g.ni;
+  const int bi = rem - bj * g.ni;
+  // weight lane (lane < 18): axis, offset (0 or 1/2), stencil node
+  const int wq = lane / 6, wo = (lane / 3) & 1, wn = lane % 3;
+  const R worg = wq == 0 ? (R)g.ox : (wq == 1 ? (R)g.oy : (R)g.oz);
+  const int wb4 = 4 * (wq == 0 ? bi : (wq == 1 ? bj : bk));
+  // slot lane (lane < 27)
+  const int si = lane % 3, sj = (lane / 3) % 3, sk = lane / 9;
+  const bool slot = lane < 27;
+  R* Tc = T + 9 * kHaloF;
+  R* Tphi = Tc + kHaloC;
+  for (int s0 = p0; s0 < p1; s0 += 32) {
+    const int s = s0 + lane;
+    R mine[kNumPCols];
+    int mdl = 0, mkl = 0;
+    if (s < p1) {
+#pragma unroll
+      for (int c = 0; c < kNumPCols; ++c) mine[c] = P[c * pcap + s];
+      mdl = delta[s];
+      mkl = (int)(key[s] & 63);
+    } else {
+#pragma unroll
+      for (int c = 0; c < kNumPCols; ++c) mine[c] = R(0);
+    }
+    const int cnt = min(32, p1 - s0);
+    for (int q = 0; q < cnt; ++q) {
+      R pc[kNumPCols];
+#pragma unroll
+      for (int c = 0; c < kNumPCols; ++c) pc[c] = __shfl_sync(full, mine[c], q);
+      const int dl = __shfl_sync(full, mdl, q);
+      const int kl = __shfl_sync(full, mkl, q);
+      const int cl0 = kl & 3, cl1 = (kl >> 2) & 3, cl2 = kl >> 4;  // key cell in the bucket
+      R wv = R(0), dv = R(0);
+      if (lane < 18) {
+        const int clq = wq == 0 ? cl0 : (wq == 1 ? cl1 : cl2);
+        const int node = wb4 + clq - 1 + (wo == 0 ? unpack_delta(dl, wq) : 0) + wn;
+        const R np = coord<R>(worg, bs, dx, node, wo ? R(0.5) : R(0));
+        dv = (wq == 0 ? pc[PX] : (wq == 1 ? pc[PY] : pc[PZ])) - np;
+        wv = quad_kernel<R>(dv * invh);
+      }
+      const R w0x = __shfl_sync(full, wv, si), w5x = __shfl_sync(full, wv, 3 + si);
+      const R w0y = __shfl_sync(full, wv, 6 + sj), w5y = __shfl_sync(full, wv, 9 + sj);
+      const R w0z = __shfl_sync(full, wv, 12 + sk), w5z = __shfl_sync(full, wv, 15 + sk);
+      const R d0x = __shfl_sync(full, dv, si), d5x = __shfl_sync(full, dv, 3 + si);
+      const R d0y = __shfl_sync(full, dv, 6 + sj), d5y = __shfl_sync(full, dv, 9 + sj);
+      const R d0z = __shfl_sync(full, dv, 12 + sk), d5z = __shfl_sync(full, dv, 15 + sk);
+      if (slot) {
+        // halo coordinates of this slot's cell-centre node: (c - 1 + s) - (4B - 1)
+        const int hx = cl0 + si, hy = cl1 + sj, hz = cl2 + sk;
+        const R m = pc[PM], vol = pc[PV];
+        // faces: offset 0 on the face's own axis; x_n - x_p = -(x_p - x_n)
+        {
+          const R w = (w0x * w5y) * w5z;
+          if (w > R(0)) {
+            const R vel = pc[VX] + (pc[C00] * (-d0x) + pc[C01] * (-d5y)) + pc[C02] * (-d5z);
+            const int t = halo_face(0, hx + unpack_delta(dl, 0), hy, hz);
+            T[t] += m * w;
+            T[kHaloF + t] += vel * m * w;
+            T[2 * kHaloF + t] += vol * w;
+          }
+        }
+        {
+          const R w = (w5x * w0y) * w5z;
+          if (w > R(0)) {
+            const R vel = pc[VY] + (pc[C10] * (-d5x) + pc[C11] * (-d0y)) + pc[C12] * (-d5z);
+            const int t = halo_face(1, hx, hy + unpack_delta(dl, 1), hz);
+            T[3 * kHaloF + t] += m * w;
+            T[4 * kHaloF + t] += vel * m * w;
+            T[5 * kHaloF + t] += vol * w;
+          }
+        }
+        {
+          const R w = (w5x * w5y) * w0z;
+          if (w > R(0)) {
+            const R vel = pc[VZ] + (pc[C20] * (-d5x) + pc[C21] * (-d5y)) + pc[C22] * (-d0z);
+            const int t = halo_face(2, hx, hy, hz + unpack_delta(dl, 2));
+            T[6 * kHaloF + t] += m * w;
+            T[7 * kHaloF + t] += vel * m * w;
+            T[8 * kHaloF + t] += vol * w;
+          }
+        }
+        // cell centre: liquid level set over every particle of the 27 key
+        // cells around the node, liquid volume over the positive weights
+        {
+          const int t = halo_centre(hx, hy, hz);
+          const R r = pc[PR];
+          const R d = sqrt((d5x * d5x + d5y * d5y) + d5z * d5z) - (rmin > r ? rmin : r);
+          if (d < Tphi[t]) Tphi[t] = d;
+          const R w = (w5x * w5y) * w5z;
+          if (w > R(0)) Tc[t] += vol * w;
+        }
+      }
+      __syncwarp();
+    }
+  }
+  R* H = halo + (long long)b * kTileVals;
+  for (int e = lane; e < kTileVals; e += 32) H[e] = T[e];
+}
+
+// Merge: one block per active bucket, threads [0,64) u-faces, [64,128)
+// v-faces, [128,192) w-faces, [192,256) cell centres (k_p2g's layout and
+// outputs).  A node sums the tiles of the buckets whose halo holds it (at
+// most two per axis: its own and, near the bucket's faces, the neighbour's),
+// in a fixed (z, y, x) order of those buckets; the liquid phi is their
+// minimum.  Buckets without particles have no tile and are skipped.
+template <typename R>
+__global__ void __launch_bounds__(256)
+    k_p2g_merge(GridDesc g, const int* __restrict__ active_list, const int* __restrict__ start,
+                const R* __restrict__ halo, R* __restrict__ F, long long fstride, Walls walls,
+                int raw_satp, int have_liquid) {
+  const int b = active_list[blockIdx.x];
+  const int type = threadIdx.x >> 6;
+  const int l = threadIdx.x & 63;
+  const int bk = b / (g.ni * g.nj);
+  const int rem = b - bk * g.ni * g.nj;
+  const int bj = rem / g.ni;
+  const int bi = rem - bj * g.ni;
+  const int li = l & 3, lj = (l >> 2) & 3, lk = l >> 4;
+  const int I = bi * 4 + li, J = bj * 4 + lj, K = bk * 4 + lk;
+  const long long n = (long long)b * 64 + l;
+  const int bq[3] = {bi, bj, bk};
+  const int nq[3] = {g.ni, g.nj, g.nk};
+  const int L[3] = {li, lj, lk};
+  // neighbour range per axis: bucket B-1 holds local node i when i + 5 < extent,
+  // B+1 when i == 3
+  int lo[3], hi[3];
+  for (int q = 0; q < 3; ++q) {
+    const int ext = (type < 3 && q == type) ? 7 : 6;
+    lo[q] = (L[q] + 5 < ext && bq[q] > 0) ? -1 : 0;
+    hi[q] = (L[q] == 3 && bq[q] + 1 < nq[q]) ? 1 : 0;
+  }
+  const R bs = (R)g.bs, dx = (R)g.dx;
+  const R dV = dx * dx * dx;
+  const R den = dV > R(1e-20) ? dV : R(1e-20);
+  if (type < 3) {
+    const int a = type;
+    R mass = 0, mom = 0, vol = 0;
+    for (int dz = lo[2]; dz <= hi[2]; ++dz)
+      for (int dy = lo[1]; dy <= hi[1]; ++dy)
+        for (int dxb = lo[0]; dxb <= hi[0]; ++dxb) {
+          const long long sb = ((long long)(bk + dz) * g.nj + (bj + dy)) * g.ni + (bi + dxb);
+          if (start[sb * 64 + 64] <= start[sb * 64]) continue;
+          const int t = halo_face(a, li + 1 - 4 * dxb, lj + 1 - 4 * dy, lk + 1 - 4 * dz);
+          const R* H = halo + sb * kTileVals + 3 * a * kHaloF;
+          mass += H[t];
+          mom += H[kHaloF + t];
+          vol += H[2 * kHaloF + t];
+        }
+    F[(G_MASS + a) * fstride + n] = mass;
+    F[(G_VEL + a) * fstride + n] = mass > R(1e-20) ? mom / mass : R(0);
+    F[(G_VOL + a) * fstride + n] = vol;
+    F[(G_SAT + a) * fstride + n] = clamp01<R>(vol / den);
+  } else {
+    R phi = R(3) * bs;
+    R vliq = 0;
+    for (int dz = lo[2]; dz <= hi[2]; ++dz)
+      for (int dy = lo[1]; dy <= hi[1]; ++dy)
+        for (int dxb = lo[0]; dxb <= hi[0]; ++dxb) {
+          const long long sb = ((long long)(bk + dz) * g.nj + (bj + dy)) * g.ni + (bi + dxb);
+          if (start[sb * 64 + 64] <= start[sb * 64]) continue;
+          const int t = halo_centre(li + 1 - 4 * dxb, lj + 1 - 4 * dy, lk + 1 - 4 * dz);
+          const R* H = halo + sb * kTileVals + 9 * kHaloF;
+          vliq += H[t];
+          const R p = H[kHaloC + t];
+          phi = p < phi ? p : phi;
+        }
+    const R org[3] = {(R)g.ox, (R)g.oy, (R)g.oz};
+    R np_[3];
+    const int IJK[3] = {I, J, K};
+    for (int q = 0; q < 3; ++q) np_[q] = coord<R>(org[q], bs, dx, IJK[q], R(0.5));
+    const double three_bs = 3.0 * g.bs;
+    const double sphi_c = wall_phi(walls, (double)np_[0], (double)np_[1], (double)np_[2],
+                                   three_bs);
+    if (have_liquid && sphi_c < 0.0) phi = R(-0.5) * dx;
+    F[G_LPHI * fstride + n] = phi;
+    F[G_SATP * fstride + n] = raw_satp ? vliq : clamp01<R>(vliq / den);
+    const double cx = (double)coord<R>(org[0], bs, dx, I, R(0));
+    const double cy = (double)coord<R>(org[1], bs, dx, J, R(0));
+    const double cz = (double)coord<R>(org[2], bs, dx, K, R(0));
+    F[G_SPHI * fstride + n] = (R)wall_phi(walls, cx, cy, cz, three_bs);
+  }
+}
+
 // Solid face weights: updateSolidWeights (TwoDScene.cpp:1871-1962); corner
 // phis of missing corner nodes (outside the grid or in an inactive bucket)
 // default to 0.5*dx.  Corner ordering per connectSolidPhiNodes (:4433-4596).
@@ -907,6 +1147,167 @@ __global__ void __launch_bounds__(128)
     R xn[3];
     advect_project<R>(g, active, F, fstride, kp, dl, xw, x, v, dt, xn);
     for (int q = 0; q < 3; ++q) P[(PX + q) * pcap + s] = xn[q];
+  }
+}
+
+// ---- G2P from a staged bucket neighbourhood ---------------------------------
+// k_g2p's arithmetic with every node value read from shared memory: one block
+// per active bucket stages the nodes its particles' stencils reach (the face
+// velocities u, v, w over the P2G halo extents, and the corner solid phi over
+// [4B-1, 4B+5] on each axis) once, then each thread advances particles of the
+// bucket.  Nodes of inactive buckets stage 0 for the velocities (k_g2p skips
+// them: the same sums) and 3 dx for the solid phi (solid_sample's value).
+// Requires stencil offsets in {0, 1} (checked on the host).
+constexpr int kCornerHalo = 7 * 7 * 7;
+constexpr int kG2PTile = 3 * kHaloF + kCornerHalo;
+
+template <typename R>
+__global__ void __launch_bounds__(128)
+    k_g2p_tile(GridDesc g, const int* __restrict__ active_list,
+               const unsigned char* __restrict__ active, R* __restrict__ P, long long pcap,
+               const int* __restrict__ start, const long long* __restrict__ key,
+               const int* __restrict__ delta, const R* __restrict__ F, long long fstride,
+               R flip, R dt, int advect, const R* __restrict__ XW) {
+  __shared__ R T[kG2PTile];
+  const int b = active_list[blockIdx.x];
+  const long long n0 = (long long)b * 64;
+  const int p0 = start[n0], p1 = start[n0 + 64];
+  if (p1 <= p0) return;
+  const int bk = b / (g.ni * g.nj);
+  const int rem = b - bk * g.ni * g.nj;
+  const int bj = rem / g.ni;
+  const int bi = rem - bj * g.ni;
+  const int h0[3] = {4 * bi - 1, 4 * bj - 1, 4 * bk - 1};
+  const R dx = (R)g.dx;
+  for (int e = threadIdx.x; e < kG2PTile; e += blockDim.x) {
+    int a, x, y, z;
+    if (e < 3 * kHaloF) {
+      a = e / kHaloF;
+      const int r = e - a * kHaloF;
+      const int nx = a == 0 ? 7 : 6, ny = a == 1 ? 7 : 6;
+      x = r % nx;
+      y = (r / nx) % ny;
+      z = r / (nx * ny);
+    } else {
+      a = 3;
+      const int r = e - 3 * kHaloF;
+      x = r % 7;
+      y = (r / 7) % 7;
+      z = r / 49;
+    }
+    const int NI_ = h0[0] + x, NJ_ = h0[1] + y, NK_ = h0[2] + z;
+    const bool on = in_grid(g, NI_, NJ_, NK_) && active[bucket_of(g, NI_, NJ_, NK_)];
+    R val;
+    if (a < 3)
+      val = on ? F[(G_U + a) * fstride + node_linear(g, NI_, NJ_, NK_)] : R(0);
+    else
+      val = on ? F[G_SPHI * fstride + node_linear(g, NI_, NJ_, NK_)] : R(3) * dx;
+    T[e] = val;
+  }
+  __syncthreads();
+  const R org[3] = {(R)g.ox, (R)g.oy, (R)g.oz};
+  const R bs = (R)g.bs;
+  const R invh = R(1) / dx;
+  const R invD = R(4) / (dx * dx);
+  for (int s = p0 + threadIdx.x; s < p1; s += blockDim.x) {
+    const R x[3] = {P[PX * pcap + s], P[PY * pcap + s], P[PZ * pcap + s]};
+    R xw[3] = {x[0], x[1], x[2]};
+    if (XW)
+      for (int q = 0; q < 3; ++q) xw[q] = XW[q * pcap + s];
+    const int kl = (int)(key[s] & 63);
+    const int cl[3] = {kl & 3, (kl >> 2) & 3, kl >> 4};
+    const int dl = delta[s];
+    R v[3], C[9];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      // stencil node 0 on each axis: halo coordinate and global node index
+      int hb[3];
+      R cx[3], cy[3], cz[3], wx[3], wy[3], wz[3];
+#pragma unroll
+      for (int q = 0; q < 3; ++q) hb[q] = cl[q] + (q == a ? unpack_delta(dl, a) : 0);
+#pragma unroll
+      for (int t = 0; t < 3; ++t) {
+        cx[t] = coord<R>(org[0], bs, dx, h0[0] + hb[0] + t, a == 0 ? R(0) : R(0.5));
+        cy[t] = coord<R>(org[1], bs, dx, h0[1] + hb[1] + t, a == 1 ? R(0) : R(0.5));
+        cz[t] = coord<R>(org[2], bs, dx, h0[2] + hb[2] + t, a == 2 ? R(0) : R(0.5));
+        wx[t] = quad_kernel<R>((xw[0] - cx[t]) * invh);
+        wy[t] = quad_kernel<R>((xw[1] - cy[t]) * invh);
+        wz[t] = quad_kernel<R>((xw[2] - cz[t]) * invh);
+      }
+      const R* U = T + a * kHaloF;
+      R fv = 0, b0 = 0, b1 = 0, b2 = 0;
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+          for (int i = 0; i < 3; ++i) {
+            const R un = U[halo_face(a, hb[0] + i, hb[1] + j, hb[2] + k)];
+            const R w = wx[i] * wy[j] * wz[k];
+            const R uw = un * w;
+            fv += uw;
+            b0 += uw * (cx[i] - x[0]) * invD;
+            b1 += uw * (cy[j] - x[1]) * invD;
+            b2 += uw * (cz[k] - x[2]) * invD;
+          }
+      v[a] = fv;
+      C[a * 3 + 0] = b0 * flip;
+      C[a * 3 + 1] = b1 * flip;
+      C[a * 3 + 2] = b2 * flip;
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) P[(VX + a) * pcap + s] = v[a];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) P[(C00 + q) * pcap + s] = C[q];
+    if (!advect) continue;
+    // advect_project with solid_sample over the staged corner phi
+    R pos[3], d[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      d[q] = v[q] * dt;
+      pos[q] = x[q] + d[q];
+    }
+    int hc[3];
+    R sc[3][3], sw[3][3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      hc[q] = cl[q] + unpack_delta(dl, q);
+#pragma unroll
+      for (int t = 0; t < 3; ++t) {
+        sc[q][t] = coord<R>(org[q], bs, dx, h0[q] + hc[q] + t, R(0));
+        sw[q][t] = quad_kernel<R>((xw[q] - sc[q][t]) * invh);
+      }
+    }
+    const R* S = T + 3 * kHaloF;
+    R phi = 0, g0 = 0, g1 = 0, g2 = 0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int j = 0; j < 3; ++j)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          const R ph = S[((hc[2] + k) * 7 + (hc[1] + j)) * 7 + (hc[0] + i)];
+          const R wn = sw[0][i] * sw[1][j] * sw[2][k];
+          phi += ph * wn;
+          const R cc = ph * invD * wn;
+          g0 += cc * (sc[0][i] - pos[0]);
+          g1 += cc * (sc[1][j] - pos[1]);
+          g2 += cc * (sc[2][k] - pos[2]);
+        }
+    const R nrm = sqrt(g0 * g0 + g1 * g1 + g2 * g2);
+    if (nrm > R(1e-20)) {
+      g0 /= nrm;
+      g1 /= nrm;
+      g2 /= nrm;
+    }
+    const R phi_now = phi + (g0 * d[0] + g1 * d[1] + g2 * d[2]);
+    if (phi_now < R(0)) {
+      pos[0] -= phi_now * g0;
+      pos[1] -= phi_now * g1;
+      pos[2] -= phi_now * g2;
+    }
+#pragma unroll
+    for (int q = 0; q < 3; ++q) P[(PX + q) * pcap + s] = pos[q];
   }
 }
 

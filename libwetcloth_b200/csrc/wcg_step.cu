@@ -74,7 +74,7 @@ void ctx_free(Context& c) {
                     &c.ebucket, &c.eperm, &c.estage, &c.ecell_start, &c.efield,
                     &c.active_pre, &c.active, &c.cell_start, &c.cell_cursor,
                     &c.gfield, &c.gvalid, &c.gdof, &c.wave_list, &c.wave_count,
-                    &c.tile_flag, &c.tile_active, &c.tile_part, &c.active_list,
+                    &c.tile_flag, &c.tile_active, &c.tile_part, &c.active_list, &c.p2g_halo,
                     &c.rx64, &c.rr64, &c.rb64,
                     &c.pl, &c.pl64, &c.pl_edge, &c.pl_order, &c.pl_corder, &c.pl_part,
                     &c.mg, &c.mg_mask, &c.mg_vec,
@@ -788,6 +788,17 @@ static Walls make_walls(const Context& c) {
   return w;
 }
 
+// The bucket-tile transfers (k_p2g_scatter + k_p2g_merge, k_g2p_tile) cover
+// stencil offsets in {0, 1}, which is every particle inside the grid; anything
+// else, or WCG_TRANSFERS=gather, takes the per-node gather P2G and the
+// per-particle global G2P.
+static bool tiled_transfers(const Context& c) {
+  if (c.xfer_mode == 1) return false;
+  for (int a = 0; a < 3; ++a)
+    if (c.drange_h[a] < 0 || c.drange_h[3 + a] > 1) return false;
+  return true;
+}
+
 template <typename R>
 static cudaError_t map_particles_to_grid_t(Context& c) {
   if (c.n_active == 0) return cudaSuccess;
@@ -800,10 +811,23 @@ static cudaError_t map_particles_to_grid_t(Context& c) {
   R* F = c.gfield.as<R>();
   const Walls w = make_walls(c);
   const bool elasto = c.ne > 0;
-  ++c.launches, k_p2g<R><<<(unsigned)c.n_active, 256, 0, c.stream>>>(
-      c.g, c.active_list.as<int>(), c.active.as<unsigned char>(), c.pbuf[c.cur].as<R>(),
-      c.pcap, c.cell_start.as<int>(), c.pdelta.as<int>() + c.cur * c.pcap, dr, F, c.gcap, w,
-      elasto ? 1 : 0, c.np > 0 ? 1 : 0);
+  if (tiled_transfers(c)) {
+    constexpr int wpb = sizeof(R) == 4 ? 4 : 2;  // warps (buckets) per block: 43 KB of tiles
+    WCG_TRY(c.p2g_halo.ensure((size_t)c.g.nb * kTileVals * sizeof(R)));
+    ++c.launches, k_p2g_scatter<R, wpb><<<(unsigned)((c.n_active + wpb - 1) / wpb), 32 * wpb, 0,
+                                          c.stream>>>(
+        c.g, c.active_list.as<int>(), c.n_active, c.pbuf[c.cur].as<R>(), c.pcap,
+        c.cell_start.as<int>(), c.pkey.as<long long>() + c.cur * c.pcap,
+        c.pdelta.as<int>() + c.cur * c.pcap, c.p2g_halo.as<R>());
+    ++c.launches, k_p2g_merge<R><<<(unsigned)c.n_active, 256, 0, c.stream>>>(
+        c.g, c.active_list.as<int>(), c.cell_start.as<int>(), c.p2g_halo.as<R>(), F, c.gcap,
+        w, elasto ? 1 : 0, c.np > 0 ? 1 : 0);
+  } else {
+    ++c.launches, k_p2g<R><<<(unsigned)c.n_active, 256, 0, c.stream>>>(
+        c.g, c.active_list.as<int>(), c.active.as<unsigned char>(), c.pbuf[c.cur].as<R>(),
+        c.pcap, c.cell_start.as<int>(), c.pdelta.as<int>() + c.cur * c.pcap, dr, F, c.gcap, w,
+        elasto ? 1 : 0, c.np > 0 ? 1 : 0);
+  }
   // solid phase of the same P2G, sat/psi/pore pressure with elasto volumes;
   // LiquidInfo surf_tension_coeff 72.8, rest_contact_angle 40.8 deg,
   // pore_radius 0.005 (App/TwoDSceneXMLParser.cpp:1851-1904 defaults)
@@ -1988,12 +2012,20 @@ template <typename R>
 static cudaError_t g2p_t(Context& c, double dt, bool advect) {
   if (c.np + c.ne == 0) return cudaSuccess;
   ProfScope prof(c, P_G2P);
-  if (c.np > 0)
-    ++c.launches, k_g2p<R><<<nblk(c.np, 128), 128, 0, c.stream>>>(
-        c.g, c.active.as<unsigned char>(), c.pbuf[c.cur].as<R>(), c.pcap, c.np,
-        c.pkey.as<long long>() + c.cur * c.pcap, c.pdelta.as<int>() + c.cur * c.pcap,
-        c.gfield.as<R>(), c.gcap, (R)c.prm.flip_coeff, (R)dt, advect ? 1 : 0,
-        c.xw_valid ? c.xw.as<R>() : nullptr);
+  if (c.np > 0) {
+    if (tiled_transfers(c))
+      ++c.launches, k_g2p_tile<R><<<(unsigned)c.n_active, 128, 0, c.stream>>>(
+          c.g, c.active_list.as<int>(), c.active.as<unsigned char>(), c.pbuf[c.cur].as<R>(),
+          c.pcap, c.cell_start.as<int>(), c.pkey.as<long long>() + c.cur * c.pcap,
+          c.pdelta.as<int>() + c.cur * c.pcap, c.gfield.as<R>(), c.gcap, (R)c.prm.flip_coeff,
+          (R)dt, advect ? 1 : 0, c.xw_valid ? c.xw.as<R>() : nullptr);
+    else
+      ++c.launches, k_g2p<R><<<nblk(c.np, 128), 128, 0, c.stream>>>(
+          c.g, c.active.as<unsigned char>(), c.pbuf[c.cur].as<R>(), c.pcap, c.np,
+          c.pkey.as<long long>() + c.cur * c.pcap, c.pdelta.as<int>() + c.cur * c.pcap,
+          c.gfield.as<R>(), c.gcap, (R)c.prm.flip_coeff, (R)dt, advect ? 1 : 0,
+          c.xw_valid ? c.xw.as<R>() : nullptr);
+  }
   if (c.ne > 0) elasto_g2p_t<R>(c, dt, true, advect);
   return cudaGetLastError();
 }
@@ -2222,11 +2254,12 @@ static cudaError_t substep_vjp_t(Context& c, double dt, const double* vbar, cons
     dr.lo[a] = c.drange_h[a];
     dr.hi[a] = c.drange_h[3 + a];
   }
-  // with the particle correction on, the positions G2P and the advection see:
-  // the correction of this sub-step (the next selector of the seeded stream)
-  // on the recomputed grid, into XC, the particle state restored after it
+  // the positions G2P and the advection see: the particle correction of this
+  // sub-step (the next selector of the seeded stream; at strength 0 only its
+  // projection out of the solid) on the recomputed grid, into XC, the
+  // particle state restored after it
   const R* XC = nullptr;
-  if (c.prm.correction_strength > 0.0) {
+  {
     R* P = c.pbuf[c.cur].as<R>();
     const int sel = correction_selector(c.prm.correction_seed, c.corr_count,
                                         c.prm.correction_step);
@@ -2311,11 +2344,21 @@ int correction_selector(unsigned long long seed, unsigned long long k, int step)
 template <typename R>
 static cudaError_t correct_liquid_t(Context& c, double dt, int selector) {
   const long long n = c.np;
-  if (n == 0 || c.n_active == 0 || !(c.prm.correction_strength > 0.0)) return cudaSuccess;
+  if (n == 0 || c.n_active == 0) return cudaSuccess;
   ProfScope prof(c, P_OTHER);
   R* P = c.pbuf[c.cur].as<R>();
   // positions before the correction: G2P keeps their weights
   WCG_TRY(c.xw.ensure((size_t)3 * c.pcap * sizeof(R)));
+  if (!(c.prm.correction_strength > 0.0)) {
+    // strength 0: the selected particles are only projected out of the solid
+    const int step = c.prm.correction_step > 0 ? c.prm.correction_step : 1;
+    ++c.launches, k_correct_project<R><<<nblk(n, 256), 256, 0, c.stream>>>(
+        c.g, P, c.pcap, n, c.pid[c.cur].as<int>(), c.pkey.as<long long>() + c.cur * c.pcap,
+        c.pdelta.as<int>() + c.cur * c.pcap, c.active.as<unsigned char>(), c.gfield.as<R>(),
+        c.gcap, c.xw.as<R>(), selector, step);
+    c.xw_valid = true;
+    return cudaGetLastError();
+  }
   WCG_TRY(cudaMemcpyAsync(c.xw.p, P + PX * c.pcap, 3 * c.pcap * sizeof(R),
                           cudaMemcpyDeviceToDevice, c.stream));
   c.xw_valid = true;
@@ -2672,8 +2715,10 @@ cudaError_t substep(Context& c, double dt) {
   WCG_TRY(project_fine(c, dt));
   WCG_TRY(apply_pressure_and_extrapolate(c, dt));
   WCG_TRY(constrain_liquid_velocity(c));
-  // correctLiquidParticles (WetClothCore.cpp:242), subset from the seeded stream
-  if (c.prm.correction_strength > 0.0 && c.np > 0) {
+  // correctLiquidParticles (WetClothCore.cpp:242) in every sub-step, subset
+  // from the seeded stream (at strength 0 it only projects the subset out of
+  // the solid)
+  if (c.np > 0) {
     const int sel = correction_selector(c.prm.correction_seed, c.corr_count++,
                                         c.prm.correction_step);
     WCG_TRY(correct_liquid_particles(c, dt, sel));

@@ -60,13 +60,6 @@ void store(TwoDScene& s, double* out) {
 
 extern "C" {
 
-// Sets LiquidInfo::particle_cell_multiplier of a harness scene (the scene
-// file's particle-cell multiplier; it decides the split/merge classes).
-void wcbind_set_cell_multiplier(void* h, double m) {
-  const auto& sp = *(const std::shared_ptr<TwoDScene>*)wcref_scene_sp(h);
-  sp->getLiquidInfo().particle_cell_multiplier = m;
-}
-
 // `steps` calls of stepSystem(dt) on each scene: href with WetClothCore,
 // hgpu with GpuWetClothCore (criterion, maxiters, solver, precision as the
 // integrator would pass them).  out_* receive x3 | v3 | C9 (15 n doubles) of

@@ -137,9 +137,11 @@ class OracleScene:
         if getattr(p, "terminator", False):
             L.wco_set_terminator(self.h, 1, arr(p.terminator_center), arr(p.terminator_half),
                                  p.terminator_radius, 1 if p.terminator_inside else 0)
-        if getattr(p, "correction_strength", 0.0) > 0.0:
-            L.wco_set_correction(self.h, p.correction_strength, p.correction_step,
-                                 p.correction_multiplier, p.correction_seed)
+        # the correction runs in every sub-step (strength 0: projection only)
+        L.wco_set_correction(self.h, getattr(p, "correction_strength", 0.0),
+                             getattr(p, "correction_step", 8),
+                             getattr(p, "correction_multiplier", 2.0),
+                             getattr(p, "correction_seed", 0))
 
     def close(self):
         if self.h:

@@ -58,6 +58,8 @@ def _lib(omp: bool):
         L.wcref_set_correction.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int,
                                            ctypes.c_double, ctypes.c_uint]
         L.wcref_merge.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_int]
+        L.wcref_core_step.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        L.wcref_set_cell_multiplier.argtypes = [ctypes.c_void_p, ctypes.c_double]
         L.wcref_pcg_solve_csr.argtypes = [_L, _L, _D, ctypes.c_int, _D, _D, ctypes.c_double,
                                           ctypes.c_int, _D, ctypes.POINTER(ctypes.c_int)]
         L.wcref_pcg_solve_csr.restype = ctypes.c_int
@@ -128,9 +130,13 @@ class RefScene:
         if getattr(p, "terminator", False):
             self.L.wcref_set_terminator(self.h, arr(p.terminator_center), arr(p.terminator_half),
                                         p.terminator_radius, 1 if p.terminator_inside else 0)
-        if getattr(p, "correction_strength", 0.0) > 0.0:
-            self.L.wcref_set_correction(self.h, p.correction_strength, p.correction_step,
-                                        p.correction_multiplier, p.correction_seed)
+        self.L.wcref_set_cell_multiplier(self.h, getattr(p, "particle_cell_multiplier",
+                                                         0.3535533906))
+        # the correction runs in every sub-step (strength 0: projection only)
+        self.L.wcref_set_correction(self.h, getattr(p, "correction_strength", 0.0),
+                                    getattr(p, "correction_step", 8),
+                                    getattr(p, "correction_multiplier", 2.0),
+                                    getattr(p, "correction_seed", 0))
 
     def close(self):
         if self.h:
@@ -145,6 +151,11 @@ class RefScene:
 
     def step(self, dt: float, snapshot: bool = True) -> int:
         return self.L.wcref_step(self.h, dt, 1 if snapshot else 0)
+
+    def core_step(self, dt: float) -> None:
+        """The reference's own WetClothCore::stepSystem on this scene (not the
+        harness's staged replay); the particle state lands in adv_*/g2p_*."""
+        self.L.wcref_core_step(self.h, dt)
 
     def merge(self, seed: int, step: int) -> int:
         """updateOptiVolume + mergeLiquidParticles after srand(seed); returns
@@ -219,14 +230,13 @@ def binding_available() -> bool:
     return os.path.exists(os.path.join(HERE, "_ref", "libwcbinding.so"))
 
 
-def binding_step_both(scene, steps, dt, solver, precision, cell_multiplier=None):
+def binding_step_both(scene, steps, dt, solver, precision):
     """Steps two reference scenes built from `scene`: one with the reference's
     WetClothCore::stepSystem, one with the compiled GpuWetClothCore binding
     (oracle/binding/GpuWetClothCore.h) passing the scene's criterion and
     iteration limit.  Returns ((x, v, C) reference, (x, v, C) binding,
     sub-steps of the binding's last step)."""
     B = ctypes.CDLL(os.path.join(HERE, "_ref", "libwcbinding.so"))
-    B.wcbind_set_cell_multiplier.argtypes = [ctypes.c_void_p, ctypes.c_double]
     B.wcbind_step_both.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                    ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                    ctypes.c_int, ctypes.c_int, ctypes.c_longlong, _D, _D,
@@ -235,9 +245,6 @@ def binding_step_both(scene, steps, dt, solver, precision, cell_multiplier=None)
     B.wcbind_step_both.restype = ctypes.c_int
     ra = RefScene(scene, mic=False)
     rb = RefScene(scene, mic=False)
-    if cell_multiplier is not None:
-        B.wcbind_set_cell_multiplier(ra.h, cell_multiplier)
-        B.wcbind_set_cell_multiplier(rb.h, cell_multiplier)
     cap = 4 * scene.x.shape[0] + 16
     oa = np.zeros(15 * cap)
     ob = np.zeros(15 * cap)

@@ -56,6 +56,7 @@
 #include "SimpleGravityForce.h"
 #include "TwoDScene.h"
 #include "DistanceFields.h"
+#include "WetClothCore.h"
 #undef private
 #undef protected
 
@@ -93,11 +94,24 @@ struct Harness {
   double timers[12];
   int last_iters_amg = 0, last_iters_mic = 0;
   double last_res_amg = 0, last_res_mic = 0;
-  bool corr_on = false;       // correctLiquidParticles before G2P (WetClothCore.cpp:242)
   unsigned corr_seed = 0, corr_count = 0;
   bool term_on = false;       // terminateParticles first (WetClothCore.cpp:97)
   bool grid_built = false;    // a grid exists for removeEmptyParticles' re-sort
 };
+
+// the correction subset of call k of a seeded stream: SplitMix64 (Steele,
+// Lea and Flood 2014) of the seed and k, modulo the step -- the stream the
+// oracle (wco_correction_selector) and the GPU (wcg_correction_selector) use
+uint64_t splitmix(uint64_t z) {
+  z += 0x9e3779b97f4a7c15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+
+int seeded_selector(uint64_t seed, uint64_t k, int step) {
+  return (int)(splitmix(seed ^ splitmix(k)) % (uint64_t)(step > 0 ? step : 1));
+}
 
 double now() {
   return std::chrono::duration<double>(
@@ -628,15 +642,23 @@ int wcref_substep(void* hp, double sub_dt, int snapshot) {
     dense(*h, "u_final_z", s.m_node_vel_fluid_z);
   }
 
-  if (h->corr_on) {
-    // the correction draws its particle subset with one rand(): seed it and
-    // record the value it will draw
-    const unsigned seed = h->corr_seed + h->corr_count++;
-    srand(seed);
-    const int sel = rand() % s.getLiquidInfo().correction_step;
+  {
+    // correctLiquidParticles runs in every sub-step (WetClothCore.cpp:242); at
+    // correction_strength 0 its spring weights vanish and it only projects
+    // its particle subset out of the solid.  The subset is one rand() draw
+    // modulo correction_step: rand() is seeded so that the draw equals the
+    // selector of the seeded stream the oracle and the GPU use
+    const int step = std::max(1, s.getLiquidInfo().correction_step);
+    const int want = seeded_selector(h->corr_seed, h->corr_count++, step);
+    unsigned seed = 0;
+    while (seed < (1u << 24)) {
+      srand(seed);
+      if (rand() % step == want) break;
+      ++seed;
+    }
     srand(seed);
     s.correctLiquidParticles(sub_dt);
-    h->ii["correction_selector"] = {sel};
+    h->ii["correction_selector"] = {want};
     if (snapshot) snap_particles(*h, "corr_");
   }
 
@@ -934,10 +956,11 @@ int wcref_transfer(void* hp, double dt) {
   return 0;
 }
 
-// TwoDScene::correctLiquidParticles between constrainLiquidVelocity and G2P,
-// as WetClothCore::stepSystem runs it, with LiquidInfo correction_strength,
-// correction_step and correction_multiplier; srand(seed + k) before the k-th
-// call fixes the subset it corrects (strength 0: off)
+// LiquidInfo correction_strength, correction_step and correction_multiplier
+// of TwoDScene::correctLiquidParticles (run in every sub-step between
+// constrainLiquidVelocity and G2P, as WetClothCore::stepSystem runs it; at
+// strength 0 it only projects its subset out of the solid); the k-th call
+// corrects the subset of call k of the seeded stream of `seed`
 void wcref_set_correction(void* hp, double strength, int step, double multiplier,
                           unsigned seed) {
   Harness* h = (Harness*)hp;
@@ -945,7 +968,6 @@ void wcref_set_correction(void* hp, double strength, int step, double multiplier
   li.correction_strength = strength;
   li.correction_step = step > 0 ? step : 1;
   li.correction_multiplier = multiplier;
-  h->corr_on = strength > 0.0;
   h->corr_seed = seed;
   h->corr_count = 0;
 }
@@ -964,6 +986,22 @@ void wcref_timers(void* hp, double* out12) {
 
 int wcref_num_particles(void* hp) {
   return ((Harness*)hp)->scene->getNumParticles();
+}
+
+// LiquidInfo::particle_cell_multiplier (V_fine of updateOptiVolume's classes)
+void wcref_set_cell_multiplier(void* hp, double m) {
+  ((Harness*)hp)->scene->getLiquidInfo().particle_cell_multiplier = m;
+}
+
+// The reference's own WetClothCore::stepSystem (WetClothCore.cpp:45-330) on
+// the harness's scene, instead of the harness's staged replay; snapshots the
+// particle state (adv_x, g2p_v, g2p_C) afterwards.
+void wcref_core_step(void* hp, double dt) {
+  Harness* h = (Harness*)hp;
+  WetClothCore core(h->scene, h->stepper);
+  core.stepSystem(dt);
+  snap_particles(*h, "adv_");
+  snap_particles(*h, "g2p_");
 }
 
 // The scene objects of a harness (shared_ptr<TwoDScene>,

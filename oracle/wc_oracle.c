@@ -2410,7 +2410,9 @@ static void transfer_in(Scene* s, int snapshot) {
  * (WetClothCore.cpp:241-262); G2P keeps the weights of the positions before
  * the correction and measures x_n - x_p from the corrected ones */
 static void transfer_out(Scene* s, double dt, int snapshot) {
-  if (s->p.corr_strength > 0.0 && s->np > s->ne) {
+  /* correctLiquidParticles runs in every sub-step; at strength 0 its spring
+   * weights vanish and it only projects its particle subset out of the solid */
+  if (s->np > s->ne) {
     int sel = s->corr_sel_once;
     if (sel < 0) sel = wco_correction_selector(s->corr_seed, s->corr_count, s->p.corr_step);
     s->corr_sel_once = -1;

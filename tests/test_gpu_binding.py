@@ -6,13 +6,16 @@ second TwoDScene built from the same inputs.
 
 The binding reads everything from the reference objects themselves: the
 liquid particles, LiquidInfo, the gravity of the scene's SimpleGravityForce
-and the solid box of its distance fields (fillGravityAndBox).  The particle
-cell multiplier makes every particle 'optimal', so the reference's
-split/merge and the binding's (which differ only in their random draws)
-leave the particles alone; the whole reference step runs, including its
-terminateParticles, updateOptiVolume, correctLiquidParticles (strength 0)
-and the calls that are no-ops for liquid.  With the reference's own solver
-(multigrid-PCG) the states agree to the multigrid parity tolerances."""
+and the solid box of its distance fields (fillGravityAndBox).  The whole
+reference step runs, including terminateParticles, updateOptiVolume, the
+split and merge, correctLiquidParticles and the calls that are no-ops for
+liquid.  Two scene settings make the reference's rand() draws irrelevant,
+so that the comparison is exact: the particle cell multiplier makes every
+particle 'optimal' (the split and merge leave the particles alone), and
+correction_step 1 makes every particle the correction's subset (at strength
+0 it projects the particles that reach into the walls back out).  With the
+reference's own solver (multigrid-PCG) the states agree to the multigrid
+parity tolerances."""
 import math
 
 import numpy as np
@@ -25,8 +28,11 @@ pytestmark = pytest.mark.gpu
 DT = 1e-3
 
 
-def _multiplier(sc, ppc):
-    return math.sqrt(3.0) * scenes.particle_radius(sc.params.dx, ppc) / sc.params.dx
+def _prepare(sc, ppc):
+    sc.params.particle_cell_multiplier = (math.sqrt(3.0) * scenes.particle_radius(sc.params.dx, ppc)
+                                          / sc.params.dx)
+    sc.params.correction_step = 1
+    return sc
 
 
 def _rel(a, b):
@@ -42,7 +48,7 @@ def test_binding_matches_reference_stepsystem_fp64(kind, wcg):
     else:
         sc, ppc = scenes.half_box(16, 2, 7, amplitude=1.0, sigma_cells=1.5), 2
     (xr, vr, Cr), (xg, vg, Cg), sub = oref.binding_step_both(
-        sc, 3, DT, _capi.WCG_SOLVER_MG, _capi.WCG_FP64, _multiplier(sc, ppc))
+        _prepare(sc, ppc), 3, DT, _capi.WCG_SOLVER_MG, _capi.WCG_FP64)
     assert xr.shape == xg.shape == sc.x.shape
     assert sub >= 1
     assert _rel(xg, xr) <= 1e-11, _rel(xg, xr)
@@ -57,6 +63,6 @@ def test_binding_matches_reference_stepsystem_fp32(wcg):
         pytest.skip("oracle/_ref/libwcbinding.so not built")
     sc = scenes.dam_break(16, 8, 0)
     (xr, vr, Cr), (xg, vg, Cg), _ = oref.binding_step_both(
-        sc, 2, DT, _capi.WCG_SOLVER_MG, _capi.WCG_FP32_REFINE, _multiplier(sc, 8))
+        _prepare(sc, 8), 2, DT, _capi.WCG_SOLVER_MG, _capi.WCG_FP32_REFINE)
     assert np.abs(xg - xr).max() <= 1e-6
     assert _rel(vg, vr) <= 1e-5, _rel(vg, vr)

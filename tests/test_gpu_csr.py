@@ -11,7 +11,8 @@ reference (oracle/_ref, wcref_pcg_solve_csr) on the same CSR matrices:
 
 The iteration counts are equal and the solutions agree to 1e-10 of their
 largest entry (the iterates differ only by the summation order of the dot
-products).  Edge cases: a zero right-hand side (no iteration), the iteration
+products); on the singular viscosity system the counts agree within one and
+A x agrees to the solve's tolerance.  Edge cases: a zero right-hand side (no iteration), the iteration
 limit (WCG_ERR_NOT_CONVERGED, as the reference's false), and malformed
 matrices (WCG_ERR_ARG before any device work)."""
 import numpy as np
@@ -138,16 +139,20 @@ def test_pcg_solve_csr_matches_reference(kind, wcg):
     assert ok_r
     x, res, it, st = _capi.pcg_solve_csr(rs, col, val, b, tol, maxit)
     assert st == _capi.WCG_OK
-    assert it == it_r, (it, it_r)
     if kind == "viscosity":
         # the viscosity matrix is singular (unknowns that touch liquid only
-        # across an edge); its null-space components follow each solver's
-        # rounding, so compare A x, which they do not touch
+        # across an edge): the Krylov iterates drift apart in its null space
+        # with the dot products' rounding, so the stop may come one iteration
+        # apart; compare A x, which the null-space components do not touch,
+        # to the solve's own tolerance
+        assert abs(it - it_r) <= 1, (it, it_r)
         ax, axr = csr_matvec(rs, col, val, x), csr_matvec(rs, col, val, xr)
-        err = np.abs(ax - axr).max() / max(np.abs(axr).max(), 1e-300)
+        err = np.abs(ax - axr).max() / max(np.abs(b).max(), 1e-300)
+        assert err <= 10 * tol, f"{kind}: A x differs by {err:.3e} of max|b|"
     else:
+        assert it == it_r, (it, it_r)
         err = np.abs(x - xr).max() / max(np.abs(xr).max(), 1e-300)
-    assert err <= 1e-10, f"{kind}: solution differs by {err:.3e} of max"
+        assert err <= 1e-10, f"{kind}: solution differs by {err:.3e} of max"
     assert res <= tol * np.abs(b).max()
     assert abs(res - res_r) <= 1e-6 * max(res_r, 1e-300) + 1e-12 * np.abs(b).max()
 

@@ -63,14 +63,18 @@ def test_bench_reference_arm_json():
         pytest.skip("oracle/_ref/libwcref_omp.so not built")
     env = dict(os.environ, OMP_NUM_THREADS="2")
     out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
-                          "--steps", "1", "--warmup", "1", "--cpu-sample-n", "16"],
+                          "--steps", "2", "--warmup", "1", "--n", "16", "--no-config0"],
                          capture_output=True, text=True, env=env, timeout=300, cwd=ROOT)
     assert out.returncode == 0, out.stderr[-2000:]
     line = [l for l in out.stdout.splitlines() if l.startswith("{")][-1]
     d = json.loads(line)
     assert d["impl"] == "reference" and d["unit"] == "ms/step" and d["value"] > 0
+    # the arm runs the workload it names, for the steps it reports
+    assert d["steps"] == 2 and d["warmup"] == 1
+    assert d["config"]["grid"] == 16 and d["config"]["particles"] > 0
     assert d["cpu_baseline"]["kind"] == "reference"
     assert d["e2e"]["h2d_bytes_per_step"] == 0
+    assert d["mic0"]["ms_per_step"] > 0 and d["mic0"]["pcg_iters"] > 0
 
 
 def _gloo_worker(rank, world, port, q):
