@@ -724,6 +724,116 @@ __global__ void __launch_bounds__(kRedThreads, sizeof(R) == 4 ? 8 : 4)
   if (threadIdx.x == 0) partial[blockIdx.x] = acc;
 }
 
+// k_pl_spmv_s's arithmetic, streamed: block (patch p, chunk k) walks rows
+// [t0, t1) of one patch in order, one thread per line.  s_new of rows t - 1,
+// t and t + 1 sits in a ring of three shared-memory rows and the couplings
+// A_s, A_a, A_c of row t - 1 in a second ring, so every in-patch neighbour
+// (one row back or ahead, the same line, line -+1 or line -+16) is read from
+// shared memory and each value is loaded from global memory once; only the
+// neighbours across a patch face (lines at a = 0 / 15, c = 0 / 15) are read
+// from global memory as k_pl_spmv_s reads them.  Terms are summed in the same
+// order as k_pl_spmv_s, missing neighbours skipped.  partial[block] = s_new.q
+// over the chunk (blocks ordered patch-major, then chunk).
+template <typename R>
+__global__ void __launch_bounds__(kRedThreads)
+    k_pl_spmv_stream(PencilGeom G, int rows_per_chunk, int nchunk, const R* __restrict__ AD,
+                     const R* __restrict__ AS, const R* __restrict__ AA,
+                     const R* __restrict__ AC, const R* __restrict__ z,
+                     const R* __restrict__ sold, R* __restrict__ snew, R* __restrict__ q,
+                     R* __restrict__ x, const double* __restrict__ sc,
+                     double* __restrict__ partial) {
+  __shared__ R ring[3][kPatchLines];
+  __shared__ R cs[2][kPatchLines], ca[2][kPatchLines], cc[2][kPatchLines];
+  __shared__ double sm[kRedThreads];
+  if (*(const int*)(sc + S_DONE)) return;
+  const R be = (R)sc[S_BETA];
+  const R al = (R)sc[S_ALPHA];
+  const int l = threadIdx.x;
+  const int p = blockIdx.x / nchunk;
+  const int k = blockIdx.x - p * nchunk;
+  const int t0 = k * rows_per_chunk;
+  const int t1 = min(G.R, t0 + rows_per_chunk);
+  double acc = 0;
+  if (t0 < t1) {
+    const long long base = (long long)p * G.R * kPatchLines + l;
+    // s_new and the couplings of row t0 - 1 (zero before the first row)
+    if (t0 > 0) {
+      const long long e = base + (long long)(t0 - 1) * kPatchLines;
+      ring[(t0 + 2) % 3][l] = z[e] + be * sold[e];
+      cs[(t0 + 1) & 1][l] = AS[e];
+      ca[(t0 + 1) & 1][l] = AA[e];
+      cc[(t0 + 1) & 1][l] = AC[e];
+    } else {
+      ring[2][l] = R(0);
+      cs[1][l] = ca[1][l] = cc[1][l] = R(0);
+    }
+    {
+      const long long e = base + (long long)t0 * kPatchLines;
+      ring[t0 % 3][l] = z[e] + be * sold[e];
+    }
+    for (int t = t0; t < t1; ++t) {
+      const long long e = base + (long long)t * kPatchLines;
+      // s_new of row t + 1
+      if (t + 1 < G.R) ring[(t + 1) % 3][l] = z[e + kPatchLines] + be * sold[e + kPatchLines];
+      const R ads = AD[e], as = AS[e], aa = AA[e], ac = AC[e];
+      cs[t & 1][l] = as;
+      ca[t & 1][l] = aa;
+      cc[t & 1][l] = ac;
+      __syncthreads();
+      const PlCell c = pl_cell(G, p * G.R + t, l);
+      if (c.live) {
+        const R* sm1 = ring[(t + 2) % 3];
+        const R* s0 = ring[t % 3];
+        const R* sp1 = ring[(t + 1) % 3];
+        const int pr = (t + 1) & 1;  // coupling ring slot of row t - 1
+        R r = 0;
+        // -c
+        if (c.cl > 0) {
+          r += cc[pr][l - kPatch] * sm1[l - kPatch];
+        } else if (c.PCi > 0) {
+          const long long n = pl_index(G, p - G.nPA, t + kPatch - 1, l + kPatch * (kPatch - 1));
+          r += AC[n] * (z[n] + be * sold[n]);
+        }
+        // -a
+        if (c.al > 0) {
+          r += ca[pr][l - 1] * sm1[l - 1];
+        } else if (c.PAi > 0) {
+          const long long n = pl_index(G, p - 1, t + kPatch - 1, l + kPatch - 1);
+          r += AA[n] * (z[n] + be * sold[n]);
+        }
+        // -s
+        if (c.s > 0) r += cs[pr][l] * sm1[l];
+        const R so = sold[e];
+        x[e] = x[e] + al * so;
+        const R sn = s0[l];
+        r += ads * sn;
+        // +s
+        if (c.s + 1 < G.Ls) r += as * sp1[l];
+        // +a
+        if (c.al < kPatch - 1) {
+          r += aa * sp1[l + 1];
+        } else if (c.PAi + 1 < G.nPA) {
+          const long long n = pl_index(G, p + 1, t - (kPatch - 1), l - (kPatch - 1));
+          r += aa * (z[n] + be * sold[n]);
+        }
+        // +c
+        if (c.cl < kPatch - 1) {
+          r += ac * sp1[l + kPatch];
+        } else if (c.PCi + 1 < G.nPC) {
+          const long long n = pl_index(G, p + G.nPA, t - (kPatch - 1), l - kPatch * (kPatch - 1));
+          r += ac * (z[n] + be * sold[n]);
+        }
+        snew[e] = sn;
+        q[e] = r;
+        acc += (double)sn * (double)r;
+      }
+      __syncthreads();
+    }
+  }
+  acc = block_sum<double>(acc, sm);
+  if (threadIdx.x == 0) partial[blockIdx.x] = acc;
+}
+
 // FP64 residual r64 = b - A x64 with the coefficients promoted; partial max|r64|
 template <typename R>
 __global__ void __launch_bounds__(kRedThreads)

@@ -1433,13 +1433,20 @@ static cudaError_t pl_pcg(Context& c, R* r, R* x, double tol_abs, int maxiters, 
   const R* AS = pl_field<R>(c, PL_AS);
   const R* AA = pl_field<R>(c, PL_AA);
   const R* AC = pl_field<R>(c, PL_AC);
-  const int spmv_blocks = sizeof(R) == 4 ? kPlSpmvBlocks32 : kPlBlocks;
+  // the streamed SpMV: chunks of consecutive rows of one patch per block,
+  // about kPlSpmvBlocks32 blocks in all
+  const int nchunk = (int)std::min<long long>(
+      G.R, std::max<long long>(1, (kPlSpmvBlocks32 + G.npatch - 1) / G.npatch));
+  const int rows_per_chunk = (G.R + nchunk - 1) / nchunk;
+  const int spmv_blocks = (int)(G.npatch * nchunk);
+  WCG_TRY(ensure_scratch(c, (size_t)spmv_blocks * sizeof(double)));
+  part = c.scratch.as<double>();
   for (;;) {
     for (int b = 0; b < kPcgBatch; ++b) {
       {
         ProfScope prof(c, P_PCGVEC);
-        ++c.launches, k_pl_spmv_s<R><<<spmv_blocks, kRedThreads, 0, c.stream>>>(
-            G, AD, AS, AA, AC, z, sold, snew, q, x, sc, part);
+        ++c.launches, k_pl_spmv_stream<R><<<spmv_blocks, kRedThreads, 0, c.stream>>>(
+            G, rows_per_chunk, nchunk, AD, AS, AA, AC, z, sold, snew, q, x, sc, part);
         ++c.launches, k_red_alpha<<<1, kRedThreads, 0, c.stream>>>(part, spmv_blocks, sc);
       }
       WCG_TRY((pl_sweep<R, kForward, true>(c, fa)));

@@ -67,6 +67,7 @@ def lib():
         L.wco_size.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
         L.wco_size.restype = ctypes.c_longlong
         L.wco_get_f.argtypes = [ctypes.c_void_p, ctypes.c_char_p, _D]
+        L.wco_snap_state.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
         L.wco_get_i.argtypes = [ctypes.c_void_p, ctypes.c_char_p, _L]
         L.wco_solver_stats.argtypes = [ctypes.c_void_p, _I, _D]
         L.wco_pcg_solve.restype = ctypes.c_int
@@ -187,6 +188,11 @@ class OracleScene:
     def set_correction_selector(self, selector):
         """Particle subset (fluid index % step) of the next correction."""
         self.L.wco_set_correction_selector(self.h, int(selector))
+
+    def snap_state(self, tag):
+        """The current particle state as tag + "x", "v", "C" (for steps run
+        without snapshots)."""
+        self.L.wco_snap_state(self.h, tag.encode())
 
     def get(self, name):
         n = self.L.wco_size(self.h, name.encode())

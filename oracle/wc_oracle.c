@@ -2732,6 +2732,10 @@ long long wco_size(Scene* s, const char* name) {
   return -1;
 }
 
+/* the particle state (positions, velocities, affine matrices) under
+ * tag + "x" / "v" / "C", without the per-stage snapshots of a step */
+void wco_snap_state(Scene* s, const char* tag) { snap_particles(s, tag); }
+
 int wco_get_f(Scene* s, const char* name, double* out) {
   for (int k = 0; k < s->nsnaps; ++k)
     if (!strcmp(s->snaps[k].name, name) && !s->snaps[k].is_int) {
