@@ -239,7 +239,9 @@ int wcg_constrain_liquid_velocity(wcg_ctx* ctx);
  * weights of the positions before the correction.  Coincident pairs (closer
  * than 1e-4 re) are pushed by a SplitMix64 hash of their indices instead of
  * scalarRand.  With correction_strength 0 the subset is only projected out
- * of the solid (the springs vanish), one particle at a time. */
+ * of the solid (the springs vanish), one particle at a time.  selector -1
+ * takes the next subset of the context's seeded stream, the one wcg_substep
+ * would draw (a stage-by-stage caller reproduces wcg_substep this way). */
 int wcg_correct_liquid_particles(wcg_ctx* ctx, double dt, int selector);
 /* the subset wcg_substep corrects in its k-th call: SplitMix64 of the seed and
  * k, modulo step */
@@ -247,6 +249,8 @@ int wcg_correction_selector(unsigned long long seed, unsigned long long k, int s
 /* sets the call count of the correction stream: the next sub-step (and the
  * sub-step wcg_substep_vjp differentiates) corrects the subset of call k */
 int wcg_set_correction_count(wcg_ctx* ctx, unsigned long long k);
+/* the call count of the correction stream: the call the next sub-step takes */
+unsigned long long wcg_correction_count(const wcg_ctx* ctx);
 /* TwoDScene::updateOptiVolume (relabelLiquidParticles TwoDScene.cpp:2484-2505),
  * mergeLiquidParticles (:2510-2666) and removeEmptyParticles (:1713-1745) on
  * the buckets of the last grid build, for the liquid particles with index %

@@ -166,6 +166,7 @@ SIGNATURES = {
                                                   ctypes.c_void_p, ctypes.c_void_p,
                                                   ctypes.c_void_p, ctypes.c_double,
                                                   ctypes.c_int, ctypes.c_void_p, _I, _D]),
+    "wcg_correction_count": (ctypes.c_ulonglong, [ctypes.c_void_p]),
     "wcg_set_wait_limit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_int]),
     "wcg_pcg_solve_csr": (ctypes.c_int, [_I, _I, _D, ctypes.c_int, _D, _D, ctypes.c_double,
                                          ctypes.c_int, _D, _I]),

@@ -596,8 +596,12 @@ int wcg_correct_liquid_particles(wcg_ctx* ctx, double dt, int selector) {
   WCG_CHECK_CTX(ctx);
   WCG_NEED_GRID(ctx);
   if (!(dt > 0)) return fail(WCG_ERR_ARG, "dt must be positive");
-  if (selector < 0 || selector >= ctx->c.prm.correction_step)
-    return fail(WCG_ERR_ARG, "selector must lie in [0, correction_step)");
+  const int step = ctx->c.prm.correction_step > 0 ? ctx->c.prm.correction_step : 1;
+  if (selector < -1 || selector >= step)
+    return fail(WCG_ERR_ARG, "selector must be -1 or lie in [0, correction_step)");
+  // -1: the next subset of the context's seeded stream, as wcg_substep draws it
+  if (selector < 0)
+    selector = wcg::correction_selector(ctx->c.prm.correction_seed, ctx->c.corr_count++, step);
   WCG_CALL(ctx, wcg::correct_liquid_particles(ctx->c, dt, selector), "correctLiquidParticles");
   return device_status(ctx->c, "correctLiquidParticles");
 }
@@ -645,6 +649,8 @@ int wcg_set_correction_count(wcg_ctx* ctx, unsigned long long k) {
   ctx->c.corr_count = k;
   return WCG_OK;
 }
+
+unsigned long long wcg_correction_count(const wcg_ctx* ctx) { return ctx ? ctx->c.corr_count : 0; }
 
 unsigned long long wcg_split_key(unsigned long long seed, unsigned long long k) {
   return wcg::split_key(seed, k);

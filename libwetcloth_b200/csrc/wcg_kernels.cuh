@@ -502,35 +502,31 @@ __global__ void __launch_bounds__(32 * WPB)
         const int hx = cl0 + si, hy = cl1 + sj, hz = cl2 + sk;
         const R m = pc[PM], vol = pc[PV];
         // faces: offset 0 on the face's own axis; x_n - x_p = -(x_p - x_n)
+        // (a zero weight adds +-0 to each sum, which leaves it unchanged:
+        // the same sums as k_p2g's skip of non-positive weights)
         {
           const R w = (w0x * w5y) * w5z;
-          if (w > R(0)) {
-            const R vel = pc[VX] + (pc[C00] * (-d0x) + pc[C01] * (-d5y)) + pc[C02] * (-d5z);
-            const int t = halo_face(0, hx + unpack_delta(dl, 0), hy, hz);
-            T[t] += m * w;
-            T[kHaloF + t] += vel * m * w;
-            T[2 * kHaloF + t] += vol * w;
-          }
+          const R vel = pc[VX] + (pc[C00] * (-d0x) + pc[C01] * (-d5y)) + pc[C02] * (-d5z);
+          const int t = halo_face(0, hx + unpack_delta(dl, 0), hy, hz);
+          T[t] += m * w;
+          T[kHaloF + t] += vel * m * w;
+          T[2 * kHaloF + t] += vol * w;
         }
         {
           const R w = (w5x * w0y) * w5z;
-          if (w > R(0)) {
-            const R vel = pc[VY] + (pc[C10] * (-d5x) + pc[C11] * (-d0y)) + pc[C12] * (-d5z);
-            const int t = halo_face(1, hx, hy + unpack_delta(dl, 1), hz);
-            T[3 * kHaloF + t] += m * w;
-            T[4 * kHaloF + t] += vel * m * w;
-            T[5 * kHaloF + t] += vol * w;
-          }
+          const R vel = pc[VY] + (pc[C10] * (-d5x) + pc[C11] * (-d0y)) + pc[C12] * (-d5z);
+          const int t = halo_face(1, hx, hy + unpack_delta(dl, 1), hz);
+          T[3 * kHaloF + t] += m * w;
+          T[4 * kHaloF + t] += vel * m * w;
+          T[5 * kHaloF + t] += vol * w;
         }
         {
           const R w = (w5x * w5y) * w0z;
-          if (w > R(0)) {
-            const R vel = pc[VZ] + (pc[C20] * (-d5x) + pc[C21] * (-d5y)) + pc[C22] * (-d0z);
-            const int t = halo_face(2, hx, hy, hz + unpack_delta(dl, 2));
-            T[6 * kHaloF + t] += m * w;
-            T[7 * kHaloF + t] += vel * m * w;
-            T[8 * kHaloF + t] += vol * w;
-          }
+          const R vel = pc[VZ] + (pc[C20] * (-d5x) + pc[C21] * (-d5y)) + pc[C22] * (-d0z);
+          const int t = halo_face(2, hx, hy, hz + unpack_delta(dl, 2));
+          T[6 * kHaloF + t] += m * w;
+          T[7 * kHaloF + t] += vel * m * w;
+          T[8 * kHaloF + t] += vol * w;
         }
         // cell centre: liquid level set over every particle of the 27 key
         // cells around the node, liquid volume over the positive weights
@@ -540,7 +536,7 @@ __global__ void __launch_bounds__(32 * WPB)
           const R d = sqrt((d5x * d5x + d5y * d5y) + d5z * d5z) - (rmin > r ? rmin : r);
           if (d < Tphi[t]) Tphi[t] = d;
           const R w = (w5x * w5y) * w5z;
-          if (w > R(0)) Tc[t] += vol * w;
+          Tc[t] += vol * w;
         }
       }
       __syncwarp();
@@ -556,11 +552,18 @@ __global__ void __launch_bounds__(32 * WPB)
 // most two per axis: its own and, near the bucket's faces, the neighbour's),
 // in a fixed (z, y, x) order of those buckets; the liquid phi is their
 // minimum.  Buckets without particles have no tile and are skipped.
+//
+// The same block also writes the solid face weights (k_solid_weights'
+// updateSolidWeights, TwoDScene.cpp:1871-1962) from the corner solid phi of
+// the bucket's 5 x 5 x 5 corner nodes, evaluated once into shared memory
+// (corners in missing buckets read 0.5 dx, as k_solid_weights reads them).
 template <typename R>
 __global__ void __launch_bounds__(256)
-    k_p2g_merge(GridDesc g, const int* __restrict__ active_list, const int* __restrict__ start,
+    k_p2g_merge(GridDesc g, const int* __restrict__ active_list,
+                const unsigned char* __restrict__ active, const int* __restrict__ start,
                 const R* __restrict__ halo, R* __restrict__ F, long long fstride, Walls walls,
                 int raw_satp, int have_liquid) {
+  __shared__ R corner[5][5][5];
   const int b = active_list[blockIdx.x];
   const int type = threadIdx.x >> 6;
   const int l = threadIdx.x & 63;
@@ -571,6 +574,36 @@ __global__ void __launch_bounds__(256)
   const int li = l & 3, lj = (l >> 2) & 3, lk = l >> 4;
   const int I = bi * 4 + li, J = bj * 4 + lj, K = bk * 4 + lk;
   const long long n = (long long)b * 64 + l;
+  {
+    const R org[3] = {(R)g.ox, (R)g.oy, (R)g.oz};
+    const R bs = (R)g.bs, dx = (R)g.dx;
+    const double three_bs = 3.0 * g.bs;
+    for (int e = threadIdx.x; e < 125; e += blockDim.x) {
+      const int ci = bi * 4 + e % 5, cj = bj * 4 + (e / 5) % 5, ck = bk * 4 + e / 25;
+      R v = R(0.5) * dx;
+      if (in_grid(g, ci, cj, ck) && active[bucket_of(g, ci, cj, ck)]) {
+        const double cx = (double)coord<R>(org[0], bs, dx, ci, R(0));
+        const double cy = (double)coord<R>(org[1], bs, dx, cj, R(0));
+        const double cz = (double)coord<R>(org[2], bs, dx, ck, R(0));
+        v = (R)wall_phi(walls, cx, cy, cz, three_bs);
+      }
+      corner[e / 25][(e / 5) % 5][e % 5] = v;
+    }
+    __syncthreads();
+    if (type < 3) {
+      R phi[4];
+      for (int r = 0; r < 2; ++r)
+        for (int s2 = 0; s2 < 2; ++s2) {
+          int ci = li, cj = lj, ck = lk;
+          if (type == 0) { cj += s2; ck += r; }
+          else if (type == 1) { ci += r; ck += s2; }
+          else { ci += r; cj += s2; }
+          phi[r * 2 + s2] = corner[ck][cj][ci];
+        }
+      F[(G_WEIGHT + type) * fstride + n] =
+          clamp01<R>(R(1) - fraction_inside4<R>(phi[0], phi[1], phi[2], phi[3]));
+    }
+  }
   const int bq[3] = {bi, bj, bk};
   const int nq[3] = {g.ni, g.nj, g.nk};
   const int L[3] = {li, lj, lk};
@@ -627,10 +660,9 @@ __global__ void __launch_bounds__(256)
     if (have_liquid && sphi_c < 0.0) phi = R(-0.5) * dx;
     F[G_LPHI * fstride + n] = phi;
     F[G_SATP * fstride + n] = raw_satp ? vliq : clamp01<R>(vliq / den);
-    const double cx = (double)coord<R>(org[0], bs, dx, I, R(0));
-    const double cy = (double)coord<R>(org[1], bs, dx, J, R(0));
-    const double cz = (double)coord<R>(org[2], bs, dx, K, R(0));
-    F[G_SPHI * fstride + n] = (R)wall_phi(walls, cx, cy, cz, three_bs);
+    // solid phi at the corner node (TwoDScene::updateSolidPhi :7940-7960): the
+    // bucket's own corner, active by definition
+    F[G_SPHI * fstride + n] = corner[lk][lj][li];
   }
 }
 

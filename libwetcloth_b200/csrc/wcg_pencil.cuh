@@ -767,18 +767,36 @@ __global__ void __launch_bounds__(kRedThreads)
       ring[2][l] = R(0);
       cs[1][l] = ca[1][l] = cc[1][l] = R(0);
     }
-    {
-      const long long e = base + (long long)t0 * kPatchLines;
-      ring[t0 % 3][l] = z[e] + be * sold[e];
+    // row t's own values and row t + 1's z, s_old, held one row ahead in
+    // registers so the loads of the next row overlap this row's work
+    long long e0 = base + (long long)t0 * kPatchLines;
+    R nz = z[e0], ns = sold[e0];
+    ring[t0 % 3][l] = nz + be * ns;
+    R ad = AD[e0], as = AS[e0], aa = AA[e0], ac = AC[e0], so = ns, xv = x[e0];
+    if (t0 + 1 < G.R) {
+      nz = z[e0 + kPatchLines];
+      ns = sold[e0 + kPatchLines];
     }
     for (int t = t0; t < t1; ++t) {
       const long long e = base + (long long)t * kPatchLines;
-      // s_new of row t + 1
-      if (t + 1 < G.R) ring[(t + 1) % 3][l] = z[e + kPatchLines] + be * sold[e + kPatchLines];
-      const R ads = AD[e], as = AS[e], aa = AA[e], ac = AC[e];
+      if (t + 1 < G.R) ring[(t + 1) % 3][l] = nz + be * ns;
       cs[t & 1][l] = as;
       ca[t & 1][l] = aa;
       cc[t & 1][l] = ac;
+      const R ns1 = ns;
+      // prefetch: row t + 1's own values, row t + 2's z and s_old
+      R ad_n = 0, as_n = 0, aa_n = 0, ac_n = 0, xv_n = 0;
+      if (t + 1 < t1) {
+        ad_n = AD[e + kPatchLines];
+        as_n = AS[e + kPatchLines];
+        aa_n = AA[e + kPatchLines];
+        ac_n = AC[e + kPatchLines];
+        xv_n = x[e + kPatchLines];
+        if (t + 2 < G.R) {
+          nz = z[e + 2 * kPatchLines];
+          ns = sold[e + 2 * kPatchLines];
+        }
+      }
       __syncthreads();
       const PlCell c = pl_cell(G, p * G.R + t, l);
       if (c.live) {
@@ -803,10 +821,9 @@ __global__ void __launch_bounds__(kRedThreads)
         }
         // -s
         if (c.s > 0) r += cs[pr][l] * sm1[l];
-        const R so = sold[e];
-        x[e] = x[e] + al * so;
+        x[e] = xv + al * so;
         const R sn = s0[l];
-        r += ads * sn;
+        r += ad * sn;
         // +s
         if (c.s + 1 < G.Ls) r += as * sp1[l];
         // +a
@@ -827,6 +844,12 @@ __global__ void __launch_bounds__(kRedThreads)
         q[e] = r;
         acc += (double)sn * (double)r;
       }
+      ad = ad_n;
+      as = as_n;
+      aa = aa_n;
+      ac = ac_n;
+      xv = xv_n;
+      so = ns1;
       __syncthreads();
     }
   }

@@ -819,9 +819,10 @@ static cudaError_t map_particles_to_grid_t(Context& c) {
         c.g, c.active_list.as<int>(), c.n_active, c.pbuf[c.cur].as<R>(), c.pcap,
         c.cell_start.as<int>(), c.pkey.as<long long>() + c.cur * c.pcap,
         c.pdelta.as<int>() + c.cur * c.pcap, c.p2g_halo.as<R>());
+    // the merge writes the solid face weights too
     ++c.launches, k_p2g_merge<R><<<(unsigned)c.n_active, 256, 0, c.stream>>>(
-        c.g, c.active_list.as<int>(), c.cell_start.as<int>(), c.p2g_halo.as<R>(), F, c.gcap,
-        w, elasto ? 1 : 0, c.np > 0 ? 1 : 0);
+        c.g, c.active_list.as<int>(), c.active.as<unsigned char>(), c.cell_start.as<int>(),
+        c.p2g_halo.as<R>(), F, c.gcap, w, elasto ? 1 : 0, c.np > 0 ? 1 : 0);
   } else {
     ++c.launches, k_p2g<R><<<(unsigned)c.n_active, 256, 0, c.stream>>>(
         c.g, c.active_list.as<int>(), c.active.as<unsigned char>(), c.pbuf[c.cur].as<R>(),
@@ -836,8 +837,9 @@ static cudaError_t map_particles_to_grid_t(Context& c) {
         c.g, c.active_list.as<int>(), c.ebuf[c.ecur].as<R>(), c.ecap,
         c.ecell_start.as<int>(), c.edelta.as<int>() + c.ecur * c.ecap, dr, F, c.gcap,
         c.efield.as<R>(), 72.8, std::cos(40.8 / 180.0 * M_PI), 0.005);
-  ++c.launches, k_solid_weights<R><<<(unsigned)c.n_active, 192, 0, c.stream>>>(
-      c.g, c.active_list.as<int>(), c.active.as<unsigned char>(), F, c.gcap, w);
+  if (!tiled_transfers(c))
+    ++c.launches, k_solid_weights<R><<<(unsigned)c.n_active, 192, 0, c.stream>>>(
+        c.g, c.active_list.as<int>(), c.active.as<unsigned char>(), F, c.gcap, w);
   // liquid volume fractions for the viscosity (updateLiquidPhi :3353-3367)
   if (c.prm.viscosity > 0.0 && c.np > 0)
     ++c.launches, k_volume_fractions<R><<<(unsigned)c.n_active, 64, 0, c.stream>>>(
@@ -1434,9 +1436,9 @@ static cudaError_t pl_pcg(Context& c, R* r, R* x, double tol_abs, int maxiters, 
   const R* AA = pl_field<R>(c, PL_AA);
   const R* AC = pl_field<R>(c, PL_AC);
   // the streamed SpMV: chunks of consecutive rows of one patch per block,
-  // about kPlSpmvBlocks32 blocks in all
+  // about four blocks of resident capacity (kPlSpmvBlocks32) in all
   const int nchunk = (int)std::min<long long>(
-      G.R, std::max<long long>(1, (kPlSpmvBlocks32 + G.npatch - 1) / G.npatch));
+      G.R, std::max<long long>(1, (4 * kPlSpmvBlocks32 + G.npatch - 1) / G.npatch));
   const int rows_per_chunk = (G.R + nchunk - 1) / nchunk;
   const int spmv_blocks = (int)(G.npatch * nchunk);
   WCG_TRY(ensure_scratch(c, (size_t)spmv_blocks * sizeof(double)));

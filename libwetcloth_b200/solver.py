@@ -221,13 +221,20 @@ class FluidScene:
         check(self.L.wcg_merge_liquid_particles(self.h, int(selector), pm, ctypes.byref(rem)))
         return rem.value
 
+    @property
+    def correction_count(self):
+        """The call of the correction stream the next sub-step takes."""
+        return int(self.L.wcg_correction_count(self.h))
+
     def set_correction_count(self, k):
         """Call count of the correction stream (the next sub-step corrects the
         subset of call k)."""
         check(self.L.wcg_set_correction_count(self.h, int(k)))
 
-    def correct_liquid_particles(self, dt, selector):
-        """correctLiquidParticles for the particles with index % step == selector."""
+    def correct_liquid_particles(self, dt, selector=-1):
+        """correctLiquidParticles for the particles with index % step ==
+        selector; -1 takes the next subset of the context's seeded stream,
+        as a sub-step does (WetClothCore.cpp:242 runs it in every sub-step)."""
         check(self.L.wcg_correct_liquid_particles(self.h, dt, int(selector)))
 
     def map_node_particles(self):

@@ -2409,10 +2409,10 @@ static void transfer_in(Scene* s, int snapshot) {
 /* particle correction, G2P and advection of a sub-step
  * (WetClothCore.cpp:241-262); G2P keeps the weights of the positions before
  * the correction and measures x_n - x_p from the corrected ones */
-static void transfer_out(Scene* s, double dt, int snapshot) {
+static void transfer_out(Scene* s, double dt, int snapshot, int correct) {
   /* correctLiquidParticles runs in every sub-step; at strength 0 its spring
    * weights vanish and it only projects its particle subset out of the solid */
-  if (s->np > s->ne) {
+  if (correct && s->np > s->ne) {
     int sel = s->corr_sel_once;
     if (sel < 0) sel = wco_correction_selector(s->corr_seed, s->corr_count, s->p.corr_step);
     s->corr_sel_once = -1;
@@ -2515,7 +2515,7 @@ int wco_substep(Scene* s, double dt, int snapshot) {
       snap_node(s, nm, s->vel[a]);
     }
   }
-  transfer_out(s, dt, snapshot);
+  transfer_out(s, dt, snapshot, 1);
   return 0;
 }
 
@@ -2523,7 +2523,7 @@ int wco_substep(Scene* s, double dt, int snapshot) {
  * velocities and advection (no solve), snapshots as in a step */
 int wco_transfer(Scene* s, double dt) {
   transfer_in(s, 1);
-  transfer_out(s, dt, 1);
+  transfer_out(s, dt, 1, 0);
   return 0;
 }
 

@@ -34,8 +34,12 @@ def _scene(kind):
     return sc
 
 
-def _forward(g, x, v, C):
+def _forward(g, x, v, C, call=0):
+    """One sub-step; the particle correction (run in every sub-step) takes
+    the subset of call `call` of the seeded stream, so every evaluation of
+    the forward (and the reverse mode) uses the same one."""
     g.set_state(x, v, C)
+    g.set_correction_count(call)
     g.substep(DT)
     x1, v1, C1 = g.download()
     return np.concatenate([v1.ravel(), C1.ravel(), x1.ravel()])
@@ -60,9 +64,10 @@ def _directions(n, seed):
     return dv, dC, y
 
 
-def _vjp(g, sc, y):
+def _vjp(g, sc, y, call=0):
     n = sc.x.shape[0]
     g.set_state(sc.x, sc.v, sc.C)
+    g.set_correction_count(call)
     vb, Cb, xb = g.substep_vjp(DT, y[:3 * n].reshape(n, 3), y[3 * n:12 * n].reshape(n, 9),
                                y[12 * n:].reshape(n, 3))
     assert np.array_equal(xb.ravel(), y[12 * n:])
@@ -128,7 +133,7 @@ def test_autograd_against_central_differences(wcg):
     target = torch.from_numpy(rng.normal(size=(n, 3)))
 
     def loss_of(v, C):
-        x1, v1, C1 = substep(g, torch.from_numpy(sc.x), v, C, DT)
+        x1, v1, C1 = substep(g, torch.from_numpy(sc.x), v, C, DT, correction_call=0)
         return ((v1 - target) ** 2).sum() + (x1 * wx).sum() + 1e-3 * (C1 ** 2).sum()
 
     v = torch.from_numpy(sc.v.copy()).requires_grad_(True)
@@ -171,6 +176,7 @@ def test_adjoint_identity_with_viscosity(substeps, wcg):
     Jd = (_forward(g, sc.x, sc.v + h * dv, sc.C + h * dC) -
           _forward(g, sc.x, sc.v - h * dv, sc.C - h * dC)) / (2 * h)
     g.set_state(sc.x, sc.v, sc.C)
+    g.set_correction_count(0)
     vb, Cb, xb, mub = g.substep_vjp(DT, y[:3 * n].reshape(n, 3), y[3 * n:12 * n].reshape(n, 9),
                                     y[12 * n:].reshape(n, 3), with_viscosity=True)
     lhs = float(y @ Jd)
@@ -196,7 +202,8 @@ def test_autograd_viscosity_gradient(wcg):
 
     def loss_of(m):
         x1, v1, C1 = substep(g, torch.from_numpy(sc.x), torch.from_numpy(sc.v),
-                             torch.from_numpy(sc.C), DT, viscosity=m, viscosity_substeps=2)
+                             torch.from_numpy(sc.C), DT, viscosity=m, viscosity_substeps=2,
+                             correction_call=0)
         return (v1 ** 2).sum() + (C1 ** 2).sum() * 1e-4
 
     L = loss_of(mu)
@@ -224,20 +231,17 @@ def test_adjoint_identity_with_correction(kind, wcg):
     h = 1e-2
 
     def fwd(v, C):
-        g.set_correction_count(3)
-        return _forward(g, sc.x, v, C)
+        return _forward(g, sc.x, v, C, call=3)
 
     Jd = (fwd(sc.v + h * dv, sc.C + h * dC) - fwd(sc.v - h * dv, sc.C - h * dC)) / (2 * h)
-    g.set_correction_count(3)
-    vb, Cb = _vjp(g, sc, y)
+    vb, Cb = _vjp(g, sc, y, call=3)
     lhs = float(y @ Jd)
     rhs = float((vb * dv).sum() + (Cb * dC).sum())
     assert abs(lhs - rhs) <= 1e-9 * abs(lhs), (lhs, rhs)
     # the correction moved particles, so the corrected path was exercised
-    g.set_correction_count(3)
-    x_on = _forward(g, sc.x, sc.v, sc.C)[12 * n:]
+    x_on = _forward(g, sc.x, sc.v, sc.C, call=3)[12 * n:]
     g0 = FluidScene(_scene(kind))
-    x_off = _forward(g0, sc.x, sc.v, sc.C)[12 * n:]
+    x_off = _forward(g0, sc.x, sc.v, sc.C, call=3)[12 * n:]
     assert np.abs(x_on - x_off).max() > 1e-6
     g.close()
     g0.close()

@@ -74,6 +74,7 @@ def test_solid_projection_separate_advect(wcg):
     g.project_fine(DT)
     g.apply_pressure_drag_fluid(DT)
     g.constrain_liquid_velocity()
+    g.correct_liquid_particles(DT)  # every sub-step (projection only at strength 0)
     g.map_node_particles()
     g.advect(DT)
     _close(g.download()[0], o.get("adv_x"), 1e-12, "adv_x")

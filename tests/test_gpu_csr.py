@@ -149,12 +149,13 @@ def test_pcg_solve_csr_matches_reference(kind, wcg):
         ax, axr = csr_matvec(rs, col, val, x), csr_matvec(rs, col, val, xr)
         err = np.abs(ax - axr).max() / max(np.abs(b).max(), 1e-300)
         assert err <= 10 * tol, f"{kind}: A x differs by {err:.3e} of max|b|"
+        assert res <= tol * np.abs(b).max()
     else:
         assert it == it_r, (it, it_r)
         err = np.abs(x - xr).max() / max(np.abs(xr).max(), 1e-300)
         assert err <= 1e-10, f"{kind}: solution differs by {err:.3e} of max"
-    assert res <= tol * np.abs(b).max()
-    assert abs(res - res_r) <= 1e-6 * max(res_r, 1e-300) + 1e-12 * np.abs(b).max()
+        assert res <= tol * np.abs(b).max()
+        assert abs(res - res_r) <= 1e-6 * max(res_r, 1e-300) + 1e-12 * np.abs(b).max()
 
 
 @pytest.mark.gpu

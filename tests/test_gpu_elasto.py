@@ -128,6 +128,7 @@ def test_elasto_coupled_step_fp64(surfel_every, wcg):
     _close(g.field("pressure"), o.get("pressure"), 1e-10, "pressure")
     g.apply_pressure_drag_fluid(DT)
     g.constrain_liquid_velocity()
+    g.correct_liquid_particles(DT)  # every sub-step (projection only at strength 0)
     g.map_node_particles()
     g.advect(DT)
     ne = sc.elasto.n

@@ -39,6 +39,7 @@ def test_fp32_refine_against_fp64_oracle(kind, wcg):
     assert np.abs(p[m] - po[m]).max() <= 1e-5 * np.abs(po[m]).max()
     g.apply_pressure_drag_fluid(DT)
     g.constrain_liquid_velocity()
+    g.correct_liquid_particles(DT)  # every sub-step (projection only at strength 0)
     g.map_node_particles()
     g.advect(DT)
     x, v, C = g.download()

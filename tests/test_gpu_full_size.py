@@ -10,7 +10,9 @@ oracle (which cannot run at this size):
   (final FP64 residual <= 1e-6 of the rhs);
 - a step is bit-identical run to run;
 - the particles stay inside the box (the solid projection puts any that
-  would end inside a wall back on its surface)."""
+  would end inside a wall back on its surface);
+- the FP32 + refinement form against the FP64 form, with the one place they
+  may part (next to tiny ghost-fluid theta) identified per particle."""
 import numpy as np
 import pytest
 
@@ -58,15 +60,48 @@ def test_full_size_step_fp32_refine(full_scene, wcg):
     assert x0.min() > -1e-9 and x0.max() < 1.0 + 1e-9
 
 
+def _theta_min_near(phi_dense, dims, cell, radius=1):
+    """Smallest ghost-fluid theta = phi_l / (phi_l - phi_a) of the liquid/air
+    cell faces within `radius` cells of each particle's cell (2 where there
+    is none); phi_dense is the cell-centre liquid phi, bucket-major."""
+    from scipy.ndimage import minimum_filter
+    ni, nj, nk = (int(d) for d in dims)
+    phi = np.nan_to_num(phi_dense, nan=1.0).reshape(nk, nj, ni, 4, 4, 4)
+    phi = phi.transpose(0, 3, 1, 4, 2, 5).reshape(4 * nk, 4 * nj, 4 * ni)
+    tmin = np.full(phi.shape, 2.0)
+    for ax in range(3):
+        n = phi.shape[ax]
+        p0 = np.take(phi, range(0, n - 1), axis=ax)
+        p1 = np.take(phi, range(1, n), axis=ax)
+        face = (p0 < 0) != (p1 < 0)
+        pl = np.where(p0 < 0, p0, p1)
+        pa = np.where(p0 < 0, p1, p0)
+        th = np.where(face, pl / np.where(face, pl - pa, 1.0), 2.0)
+        lo = [slice(None)] * 3
+        hi = [slice(None)] * 3
+        lo[ax] = slice(0, n - 1)
+        hi[ax] = slice(1, n)
+        tmin[tuple(lo)] = np.minimum(tmin[tuple(lo)], th)
+        tmin[tuple(hi)] = np.minimum(tmin[tuple(hi)], th)
+    tn = minimum_filter(tmin, size=2 * radius + 1)
+    c = np.clip(cell, 0, np.array(tn.shape[::-1]) - 1)
+    return tn[c[:, 2], c[:, 1], c[:, 0]]
+
+
 def test_full_size_fp32_refine_against_fp64(full_scene, wcg):
-    """The precision configuration at full size: three steps of the FP32 +
-    refinement form against the FP64 GPU form (the FP64 form is pinned to the
-    oracle at small sizes), both solved to the configuration's tighter 1e-8
-    criterion.  All but a few particles agree to 1e-4 of the largest
-    velocity and 1e-6 in position; a few (141 of 16.8M when measured) differ
-    more, as FP32 rounding can take the other side of a discrete decision (a
-    valid face, the ghost-fluid clamp, the solid projection), and stay within
-    1e-2."""
+    """The precision configuration at full size: one step of the FP32 +
+    refinement form against the FP64 GPU form (itself pinned to the oracle at
+    this size through tests/test_gpu_configs.py), both solved to the
+    configuration's tighter 1e-8 criterion.  The two forms take the same
+    discrete decisions (DOF flags and valid faces agree everywhere when
+    measured); they differ most where the liquid surface grazes a cell
+    centre: there the ghost-fluid theta of a liquid/air face is tiny, the
+    matrix clamps it to 0.01, and the pressure difference across the face is
+    divided by dx theta, so FP32 rounding of the pressure is amplified up to
+    100 times.  Every particle farther than one cell from a face with
+    theta < 0.05 (99 % of them) agrees to 1e-5 of the largest velocity, the
+    north star's FP32 tolerance; every particle to 1e-3 (2.3e-4 measured);
+    positions to 1e-6."""
     sc = full_scene
     out = {}
     crit = sc.params.criterion
@@ -74,25 +109,31 @@ def test_full_size_fp32_refine_against_fp64(full_scene, wcg):
     try:
         for prec in (_capi.WCG_FP64, _capi.WCG_FP32_REFINE):
             g = FluidScene(sc, precision=prec)
-            for _ in range(3):
-                g.step(DT)
-            assert g.stats()["converged"] == 1
+            g.step(DT)
+            st = g.stats()
+            assert st["converged"] == 1 and st["residual"] <= 1e-8 * st["rhs_norm"]
             x, v, _ = g.download()
-            out[prec] = (x, v)
+            dims, origin, _ = g.grid_info()
+            out[prec] = (x, v, g.field("liquid_phi"), g.ifield("dof_index") >= 0,
+                         dims, origin)
             g.close()
     finally:
         sc.params.criterion = crit
-    (x64, v64), (x32, v32) = out[_capi.WCG_FP64], out[_capi.WCG_FP32_REFINE]
+    x64, v64, phi64, dof64, dims, origin = out[_capi.WCG_FP64]
+    x32, v32, _, dof32, dims32, origin32 = out[_capi.WCG_FP32_REFINE]
+    assert np.array_equal(dims, dims32) and np.array_equal(origin, origin32)
+    assert np.array_equal(dof64, dof32), "the two forms took different DOF decisions"
     vmax = np.abs(v64).max()
-    dv = np.abs(v32 - v64).max(axis=1)
-    dx = np.abs(x32 - x64).max(axis=1)
-    print(f"FP32 vs FP64 after 3 steps: max dv {dv.max() / vmax:.2e} of max|v|, "
-          f"{np.mean(dv > 1e-4 * vmax):.2e} of particles above 1e-4, "
-          f"99.99th percentile {np.quantile(dv, 0.9999) / vmax:.2e}; max dx {dx.max():.2e}")
-    # the bulk agrees to 1e-4 of the largest velocity, every particle to 1e-2
-    assert np.mean(dv > 1e-4 * vmax) <= 1e-4
-    assert dv.max() <= 1e-2 * vmax
-    assert np.quantile(dx, 0.9999) <= 1e-6 and dx.max() <= 1e-4
+    dv = np.abs(v32 - v64).max(axis=1) / vmax
+    cell = np.floor((sc.x - origin) / sc.params.dx).astype(np.int64)
+    theta = _theta_min_near(phi64, dims, cell, radius=1)
+    clear = theta >= 0.05
+    print(f"FP32 vs FP64, one step at 1e-8: max dv {dv.max():.2e} of max|v|; "
+          f"{clear.mean():.4f} of particles clear of theta < 0.05, their max {dv[clear].max():.2e}")
+    assert clear.mean() >= 0.99
+    assert dv[clear].max() <= 1e-5
+    assert dv.max() <= 1e-3
+    assert np.abs(x32 - x64).max() <= 1e-6
 
 
 def test_full_size_terminator_fp64(full_scene, wcg):

@@ -115,6 +115,7 @@ def pair(request, wcg):
     g.constrain_liquid_velocity()
     for a in "xyz":
         out["u_final_" + a] = g.field("u_" + a)
+    g.correct_liquid_particles(DT)  # every sub-step (projection only at strength 0)
     g.map_node_particles()
     out["g2p_x"], out["g2p_v"], out["g2p_C"] = g.download()
     g.advect(DT)

@@ -56,6 +56,7 @@ def test_viscosity_fp64_against_oracle(kind, mu, wcg):
     _close(g.field("pressure"), o.get("pressure"), 1e-10, "pressure")
     g.apply_pressure_drag_fluid(DT)
     g.constrain_liquid_velocity()
+    g.correct_liquid_particles(DT)  # every sub-step (projection only at strength 0)
     g.map_node_particles()
     g.advect(DT)
     x, v, C = g.download()
