@@ -269,6 +269,22 @@ int wcg_merge_liquid_particles(wcg_ctx* ctx, int selector, const int* perm9,
  * key ^ parent index (the reference: its compiled sphere-pattern table and
  * Matrix3s::Random()); *added (may be NULL) receives their count. */
 int wcg_split_liquid_particles(wcg_ctx* ctx, unsigned long long key, long long* added);
+/* The reference's own split placement, for a caller that holds the
+ * reference's draws.  wcg_split_parents gives the number of particles the
+ * split would split now (the liquid particles above 2 V_fine).
+ * wcg_split_liquid_particles_with splits them with the caller's sphere-pattern
+ * table -- TwoDScene::m_sphere_pattern[n] for n = 2..32 concatenated, 3n
+ * doubles each, WCG_SPLIT_PATTERN_LEN in all -- and one row-major 3x3 rotation
+ * per splitting parent in original-index order: the Q of the QR
+ * decomposition of the Matrix3s::Random() that splitLiquidParticles draws for
+ * that parent (TwoDScene.cpp:2390-2392).  The parent moves to
+ * centre + pattern[n][0..2] s, child i (1 <= i < n) sits at
+ * centre + Q pattern[n][3i..3i+2] s.  nparents must equal the count
+ * wcg_split_parents gives (else WCG_ERR_ARG, nothing changed). */
+#define WCG_SPLIT_PATTERN_LEN 1581
+int wcg_split_parents(wcg_ctx* ctx, long long* nparents);
+int wcg_split_liquid_particles_with(wcg_ctx* ctx, const double* pattern, const double* rot9,
+                                    long long nparents, long long* added);
 /* TwoDScene::terminateParticles (TwoDScene.cpp:1756-1771): the liquid
  * particles where the terminator box's phi is negative (outside it for
  * terminator_inside = 1) and every liquid particle without volume are
@@ -300,10 +316,16 @@ int wcg_num_substeps(wcg_ctx* ctx, double dt, int* n_out);
  * particles unchanged.  In: cotangents of the sub-step's outputs v' (3n),
  * C' (9n, rows as in wcg_download_liquid) and x' (3n).  Out: cotangents of
  * the inputs v (3n) and C (9n), of the liquid viscosity (viscosity_bar, may be
- * NULL; 0 when the viscosity is off); xbar0 = xbar3 (positions are held
- * fixed: the weights' dependence on x is not differentiated).  Liquid scenes;
- * the solve is the forward's solver on the same (symmetric) matrix.  The
- * advection's solid projection is differentiated; with the particle
+ * NULL; 0 when the viscosity is off) and of the positions x (3n): xbar0 holds
+ * xbar3 (the advection's identity part) plus the derivative through the
+ * quadratic B-spline weights and the APIC offsets x_node - x of P2G and G2P
+ * (TwoDScene::updateParticleWeights TwoDScene.cpp:2084-2174).  The grid's
+ * discrete structure, the liquid phi of the ghost-fluid fractions and the
+ * solid projections are held at the checkpoint's values (with uniform
+ * density the pressure matrix does not move with x).
+ * wcg_set_adjoint_positions(ctx, 0) holds x fixed instead (xbar0 = xbar3).
+ * Liquid scenes; the solve is the forward's solver on the same (symmetric)
+ * matrix.  The advection's solid projection is differentiated; with the particle
  * correction on, the sub-step differentiated corrects the subset of the
  * correction stream's next call (wcg_set_correction_count).  Refused
  * (WCG_ERR_UNSUPPORTED) with elasto particles, the implicit viscosity, or the
@@ -311,6 +333,9 @@ int wcg_num_substeps(wcg_ctx* ctx, double dt, int* n_out);
 int wcg_substep_vjp(wcg_ctx* ctx, double dt, const double* vbar3, const double* Cbar9,
                     const double* xbar3, double* vbar0, double* Cbar0, double* xbar0,
                     double* viscosity_bar);
+/* 1 (default): wcg_substep_vjp differentiates through the particle positions;
+ * 0: positions held fixed (xbar0 = xbar3). */
+int wcg_set_adjoint_positions(wcg_ctx* ctx, int differentiate);
 /* LiquidInfo::viscosity and the explicit viscosity sub-steps of a context
  * (0: off), as wcg_params sets them at creation. */
 int wcg_set_viscosity(wcg_ctx* ctx, double viscosity, int substeps);

@@ -129,6 +129,12 @@ SIGNATURES = {
     "wcg_set_correction_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_ulonglong]),
     "wcg_split_liquid_particles": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_ulonglong,
                                                   ctypes.POINTER(ctypes.c_longlong)]),
+    "wcg_split_parents": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]),
+    "wcg_split_liquid_particles_with": (ctypes.c_int, [ctypes.c_void_p,
+                                                       ctypes.POINTER(ctypes.c_double),
+                                                       ctypes.POINTER(ctypes.c_double),
+                                                       ctypes.c_longlong,
+                                                       ctypes.POINTER(ctypes.c_longlong)]),
     "wcg_terminate_liquid_particles": (ctypes.c_int, [ctypes.c_void_p,
                                                       ctypes.POINTER(ctypes.c_longlong)]),
     "wcg_split_key": (ctypes.c_ulonglong, [ctypes.c_ulonglong, ctypes.c_ulonglong]),
@@ -148,6 +154,7 @@ SIGNATURES = {
     "wcg_substep_vjp": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _D, _D, _D, _D, _D, _D,
                                        _D]),
     "wcg_set_viscosity": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]),
+    "wcg_set_adjoint_positions": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "wcg_get_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(WcgStats)]),
     "wcg_grid_info": (ctypes.c_int, [ctypes.c_void_p, _I, _D, _D]),
     "wcg_field_size": (ctypes.c_longlong, [ctypes.c_void_p, ctypes.c_char_p]),

@@ -15,8 +15,15 @@
 // order; A is symmetric, so the adjoint solve reuses the forward solver on the
 // same matrix.  After G2P come advection and the solid projection of the
 // particles that end inside the solid (piecewise smooth in v'; k_adj_load).
-// Gradients through the weights' dependence on x are not formed (x-bar
-// passes straight through).  Every sum is a gather in fixed order.
+// The positions' own cotangent x-bar0 = d(loss)/d(x) at the start of the
+// sub-step follows the weights' dependence on x (quadratic B-spline weights,
+// TwoDScene::updateParticleWeights TwoDScene.cpp:2084-2174, and the APIC
+// offsets d) through P2G and G2P, plus the identity part of the advection.
+// The grid's discrete structure (activation, DOFs, valid faces, heavy nodes),
+// the liquid phi of the ghost-fluid fractions, the solid weights and the
+// solid projections are held at their recomputed values.  Uniform density
+// makes V_f inv_C = 1/rho on every heavy face, so the pressure system itself
+// does not move with x.  Every sum is a gather in fixed order.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -26,6 +33,16 @@
 #include "wcg_kernels.cuh"
 
 namespace wcg {
+
+// d/dr of quad_kernel (MathUtilities.h:416): -2r inside |r| < 1/2,
+// -(3/2 - |r|) sign(r) on 1/2 <= |r| < 3/2, 0 outside.
+template <typename R>
+__device__ inline R quad_kernel_d(R r) {
+  const R d = fabs(r);
+  if (d < R(0.5)) return R(-2) * r;
+  if (d < R(1.5)) return r > R(0) ? -(R(1.5) - d) : (R(1.5) - d);
+  return R(0);
+}
 
 // Adjoint grid fields (adj buffer, gcap each).
 enum AdjField : int { A_UBAR = 0, A_UTMP = 3, A_VSBAR = 6, kNumAdjFields = 9 };
@@ -41,6 +58,11 @@ enum AdjField : int { A_UBAR = 0, A_UTMP = 3, A_VSBAR = 6, kNumAdjFields = 9 };
 //   d-bar = x-bar - (g + s M d)(g . x-bar) - phi_now s M x-bar;
 // any other particle has d-bar = x-bar.  v' is recomputed by G2P from the
 // face velocities with constrainLiquidVelocity applied on the fly (friction).
+//
+// With XB: XB = x-bar + G2P's x-part (sorted order, 3 columns), from
+//   v'_a = sum w u_a,  C'_aq = f sum w u_a d_q  (f = flip 4/h^2, d = x_n - x_c):
+//   x-bar += sum_a sum_n u_a [(vb_a + f sum_q Cb_aq d_q) grad w - f w Cb_a.]
+// with vb and Cb the cotangents just formed (grad w from the weights' x).
 template <typename R>
 __global__ void __launch_bounds__(128)
     k_adj_load(GridDesc g, const unsigned char* __restrict__ active, const R* __restrict__ P,
@@ -49,12 +71,13 @@ __global__ void __launch_bounds__(128)
                R flip, R friction, const int* __restrict__ pid,
                const double* __restrict__ vbar, const double* __restrict__ Cbar,
                const double* __restrict__ xbar, double dt, R* __restrict__ B,
-               const R* __restrict__ XC) {
+               const R* __restrict__ XC, R* __restrict__ XB) {
   const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= np) return;
   const long long i = pid[s];
   double db[3] = {xbar[i * 3 + 0], xbar[i * 3 + 1], xbar[i * 3 + 2]};
   const long long kn = key[s];
+  R xg[3] = {R(0), R(0), R(0)};
   if (kn >= 0) {
     const R x[3] = {P[PX * pcap + s], P[PY * pcap + s], P[PZ * pcap + s]};
     // the corrected position (the particle correction ran before G2P), or x
@@ -88,9 +111,55 @@ __global__ void __launch_bounds__(128)
       }
       for (int q = 0; q < 3; ++q) db[q] = out[q];
     }
+    if (XB) {
+      const R org[3] = {(R)g.ox, (R)g.oy, (R)g.oz};
+      const R bs = (R)g.bs, dx = (R)g.dx;
+      const R invh = R(1) / dx;
+      const R fi = flip * (R(4) / (dx * dx));
+      for (int a = 0; a < 3; ++a) {
+        const R vb = (R)(vbar[i * 3 + a] + dt * db[a]);
+        const R cb[3] = {(R)Cbar[i * 9 + a * 3], (R)Cbar[i * 9 + a * 3 + 1],
+                         (R)Cbar[i * 9 + a * 3 + 2]};
+        int base[3];
+        for (int q = 0; q < 3; ++q) base[q] = kp[q] + (q == a ? unpack_delta(dl, a) : 0);
+        R cx[3], cy[3], cz[3], wx[3], wy[3], wz[3], gx[3], gy[3], gz[3];
+        for (int t = 0; t < 3; ++t) {
+          cx[t] = coord<R>(org[0], bs, dx, base[0] + t, a == 0 ? R(0) : R(0.5));
+          cy[t] = coord<R>(org[1], bs, dx, base[1] + t, a == 1 ? R(0) : R(0.5));
+          cz[t] = coord<R>(org[2], bs, dx, base[2] + t, a == 2 ? R(0) : R(0.5));
+          wx[t] = quad_kernel<R>((x[0] - cx[t]) * invh);
+          wy[t] = quad_kernel<R>((x[1] - cy[t]) * invh);
+          wz[t] = quad_kernel<R>((x[2] - cz[t]) * invh);
+          gx[t] = quad_kernel_d<R>((x[0] - cx[t]) * invh) * invh;
+          gy[t] = quad_kernel_d<R>((x[1] - cy[t]) * invh) * invh;
+          gz[t] = quad_kernel_d<R>((x[2] - cz[t]) * invh) * invh;
+        }
+        const R* U = F + (G_U + a) * fstride;
+        const R* W = F + (G_WEIGHT + a) * fstride;
+        for (int k = 0; k < 3; ++k)
+          for (int j = 0; j < 3; ++j)
+            for (int ii = 0; ii < 3; ++ii) {
+              const int NI_ = base[0] + ii, NJ_ = base[1] + j, NK_ = base[2] + k;
+              if (!in_grid(g, NI_, NJ_, NK_) || !active[bucket_of(g, NI_, NJ_, NK_)]) continue;
+              const long long nn = node_linear(g, NI_, NJ_, NK_);
+              R un = U[nn];
+              if (W[nn] == R(0)) un = (R(1) - friction) * un;
+              const R w = wx[ii] * wy[j] * wz[k];
+              const R cd = (cb[0] * (cx[ii] - xc[0]) + cb[1] * (cy[j] - xc[1])) +
+                           cb[2] * (cz[k] - xc[2]);
+              const R t = un * (vb + fi * cd);
+              const R uw = un * fi * w;
+              xg[0] += t * (gx[ii] * wy[j] * wz[k]) - uw * cb[0];
+              xg[1] += t * (wx[ii] * gy[j] * wz[k]) - uw * cb[1];
+              xg[2] += t * (wx[ii] * wy[j] * gz[k]) - uw * cb[2];
+            }
+      }
+    }
   }
   for (int a = 0; a < 3; ++a) B[a * pcap + s] = (R)(vbar[i * 3 + a] + dt * db[a]);
   for (int q = 0; q < 9; ++q) B[(3 + q) * pcap + s] = (R)Cbar[i * 9 + q];
+  if (XB)
+    for (int q = 0; q < 3; ++q) XB[q * pcap + s] = (R)xbar[i * 3 + q] + xg[q];
 }
 
 // G2P^T and constrain^T: per face node, over the particles whose stencil
@@ -327,19 +396,28 @@ __global__ void __launch_bounds__(192)
 // stepVelocity^T and P2G^T per particle over its own face stencils (nodes of
 // inactive buckets skipped): mom-bar = v*-bar / m_node on heavy nodes,
 //   v-bar_a = sum m w mom-bar,  C-bar_aq = sum m w mom-bar d_q;
-// results in original particle order.
+// results in original particle order.  With XB (the x-bar of the later stages,
+// sorted order) the weights' part of u_f = mom / m_node is added,
+//   x-bar += sum_a sum_n (m / m_node) v*-bar [(phi_a - u_f) grad w - w C_a.],
+//   phi_a = v_a + C_a. d  (m-bar and mom-bar of the same node combined),
+// and x-bar0 written in original order.
 template <typename R>
 __global__ void __launch_bounds__(128)
     k_adj_p2g(GridDesc g, const unsigned char* __restrict__ active, const R* __restrict__ P,
               long long pcap, long long np, const int* __restrict__ pid,
               const long long* __restrict__ key, const int* __restrict__ delta,
               const R* __restrict__ F, const R* __restrict__ AG, long long fstride,
-              double* __restrict__ vbar0, double* __restrict__ Cbar0) {
+              double* __restrict__ vbar0, double* __restrict__ Cbar0,
+              const R* __restrict__ XB, double* __restrict__ xbar0) {
   const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= np) return;
   const long long i = pid[s];
   const long long kn = key[s];
-  if (kn < 0) return;
+  if (kn < 0) {
+    if (XB)
+      for (int q = 0; q < 3; ++q) xbar0[i * 3 + q] = (double)XB[q * pcap + s];
+    return;
+  }
   const R org[3] = {(R)g.ox, (R)g.oy, (R)g.oz};
   const R bs = (R)g.bs, dx = (R)g.dx;
   const R invh = R(1) / dx;
@@ -349,10 +427,11 @@ __global__ void __launch_bounds__(128)
   node_ijk(g, kn, KI, KJ, KK);
   const int kp[3] = {KI - 1, KJ - 1, KK - 1};
   const int dl = delta[s];
+  R xg[3] = {R(0), R(0), R(0)};
   for (int a = 0; a < 3; ++a) {
     int base[3];
     for (int q = 0; q < 3; ++q) base[q] = kp[q] + (q == a ? unpack_delta(dl, a) : 0);
-    R cx[3], cy[3], cz[3], wx[3], wy[3], wz[3];
+    R cx[3], cy[3], cz[3], wx[3], wy[3], wz[3], gx[3], gy[3], gz[3];
     for (int t = 0; t < 3; ++t) {
       cx[t] = coord<R>(org[0], bs, dx, base[0] + t, a == 0 ? R(0) : R(0.5));
       cy[t] = coord<R>(org[1], bs, dx, base[1] + t, a == 1 ? R(0) : R(0.5));
@@ -360,9 +439,16 @@ __global__ void __launch_bounds__(128)
       wx[t] = quad_kernel<R>((x - cx[t]) * invh);
       wy[t] = quad_kernel<R>((y - cy[t]) * invh);
       wz[t] = quad_kernel<R>((z - cz[t]) * invh);
+      gx[t] = quad_kernel_d<R>((x - cx[t]) * invh) * invh;
+      gy[t] = quad_kernel_d<R>((y - cy[t]) * invh) * invh;
+      gz[t] = quad_kernel_d<R>((z - cz[t]) * invh) * invh;
     }
     const R* VS = AG + (A_VSBAR + a) * fstride;
     const R* MS = F + (G_MASS + a) * fstride;
+    const R* UF = F + (G_VEL + a) * fstride;
+    const R va = P[(VX + a) * pcap + s];
+    const R ca[3] = {P[(C00 + 3 * a) * pcap + s], P[(C00 + 3 * a + 1) * pcap + s],
+                     P[(C00 + 3 * a + 2) * pcap + s]};
     R vb = 0, b0 = 0, b1 = 0, b2 = 0;
     for (int k = 0; k < 3; ++k)
       for (int j = 0; j < 3; ++j)
@@ -372,17 +458,29 @@ __global__ void __launch_bounds__(128)
           const long long nn = node_linear(g, NI_, NJ_, NK_);
           const R mn = MS[nn];
           if (!(mn > R(1e-20))) continue;
-          const R mw = (m * (wx[ii] * wy[j] * wz[k])) * (VS[nn] / mn);
+          const R w = wx[ii] * wy[j] * wz[k];
+          const R mw = (m * w) * (VS[nn] / mn);
           vb += mw;
           b0 += mw * (cx[ii] - x);
           b1 += mw * (cy[j] - y);
           b2 += mw * (cz[k] - z);
+          if (XB) {
+            const R r = m * (VS[nn] / mn);
+            const R phi = va + (ca[0] * (cx[ii] - x) + ca[1] * (cy[j] - y)) + ca[2] * (cz[k] - z);
+            const R t = r * (phi - UF[nn]);
+            const R rw = r * w;
+            xg[0] += t * (gx[ii] * wy[j] * wz[k]) - rw * ca[0];
+            xg[1] += t * (wx[ii] * gy[j] * wz[k]) - rw * ca[1];
+            xg[2] += t * (wx[ii] * wy[j] * gz[k]) - rw * ca[2];
+          }
         }
     vbar0[i * 3 + a] = (double)vb;
     Cbar0[i * 9 + a * 3 + 0] = (double)b0;
     Cbar0[i * 9 + a * 3 + 1] = (double)b1;
     Cbar0[i * 9 + a * 3 + 2] = (double)b2;
   }
+  if (XB)
+    for (int q = 0; q < 3; ++q) xbar0[i * 3 + q] = (double)XB[q * pcap + s] + (double)xg[q];
 }
 
 // ---- explicit viscosity (k_viscosity_explicit) ------------------------------

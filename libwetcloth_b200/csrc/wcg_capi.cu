@@ -299,6 +299,9 @@ int wcg_create(const wcg_params* params, wcg_ctx** out) {
   if (const char* v = getenv("WCG_PCG_LAYOUT")) ctx->c.pcg_layout = !strcmp(v, "tiles") ? 1 : 0;
   // transfer formulation: bucket tiles (default) or the global gathers
   if (const char* v = getenv("WCG_TRANSFERS")) ctx->c.xfer_mode = !strcmp(v, "gather") ? 1 : 0;
+  // the PCG's SpMV: row-parallel (default) or patch-streamed (performance
+  // knob; the dot products' partial sums are grouped differently)
+  if (const char* v = getenv("WCG_SPMV")) ctx->c.spmv_rows = !strcmp(v, "stream") ? 0 : 1;
   // CTAs per thread-block cluster along c in the MIC(0) sweeps (1, 2, 4 or 8;
   // performance knob, identical results)
   if (const char* v = getenv("WCG_SWEEP_CLUSTER")) {
@@ -636,6 +639,32 @@ int wcg_split_liquid_particles(wcg_ctx* ctx, unsigned long long key, long long* 
   return device_status(ctx->c, "splitLiquidParticles");
 }
 
+int wcg_split_parents(wcg_ctx* ctx, long long* nparents) {
+  WCG_CHECK_CTX(ctx);
+  if (!nparents) return fail(WCG_ERR_ARG, "nparents must not be NULL");
+  long long k = 0;
+  WCG_CALL(ctx, wcg::split_liquid_parents(ctx->c, &k), "splitLiquidParticles");
+  *nparents = k;
+  return device_status(ctx->c, "splitLiquidParticles");
+}
+
+int wcg_split_liquid_particles_with(wcg_ctx* ctx, const double* pattern, const double* rot9,
+                                    long long nparents, long long* added) {
+  WCG_CHECK_CTX(ctx);
+  if (!pattern || nparents < 0 || (nparents > 0 && !rot9))
+    return fail(WCG_ERR_ARG, "a pattern table and nparents rotations are required");
+  long long have = 0;
+  WCG_CALL(ctx, wcg::split_liquid_parents(ctx->c, &have), "splitLiquidParticles");
+  if (have != nparents)
+    return fail(WCG_ERR_ARG, "nparents differs from the particles that split (" +
+                                 std::to_string(have) + ")");
+  long long add = 0;
+  WCG_CALL(ctx, wcg::split_liquid_particles_with(ctx->c, pattern, rot9, nparents, &add),
+           "splitLiquidParticles");
+  if (added) *added = add;
+  return device_status(ctx->c, "splitLiquidParticles");
+}
+
 int wcg_terminate_liquid_particles(wcg_ctx* ctx, long long* removed) {
   WCG_CHECK_CTX(ctx);
   long long rem = 0;
@@ -702,14 +731,22 @@ int wcg_substep_vjp(wcg_ctx* ctx, double dt, const double* vbar3, const double* 
   const long long n = ctx->c.np;
   if (n > 0 && (!vbar3 || !Cbar9 || !xbar3 || !vbar0 || !Cbar0 || !xbar0))
     return fail(WCG_ERR_ARG, "null cotangent array");
-  WCG_CALL(ctx, wcg::substep_vjp(ctx->c, dt, vbar3, Cbar9, xbar3, vbar0, Cbar0, viscosity_bar),
+  WCG_CALL(ctx, wcg::substep_vjp(ctx->c, dt, vbar3, Cbar9, xbar3, vbar0, Cbar0,
+                                 ctx->c.adjoint_fixed_x ? nullptr : xbar0, viscosity_bar),
            "substep_vjp");
   int st = device_status(ctx->c, "substep_vjp");
   if (st) return st;
-  for (long long i = 0; i < 3 * n; ++i) xbar0[i] = xbar3[i];
+  if (ctx->c.adjoint_fixed_x)
+    for (long long i = 0; i < 3 * n; ++i) xbar0[i] = xbar3[i];
   ctx->c.have_grid = true;
   if (!ctx->c.stats.converged)
     return fail(WCG_ERR_NOT_CONVERGED, "adjoint pressure solve did not converge");
+  return WCG_OK;
+}
+
+int wcg_set_adjoint_positions(wcg_ctx* ctx, int differentiate) {
+  WCG_CHECK_CTX(ctx);
+  ctx->c.adjoint_fixed_x = differentiate ? 0 : 1;
   return WCG_OK;
 }
 

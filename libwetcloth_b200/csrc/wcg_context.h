@@ -249,10 +249,12 @@ struct Context {
   DevBuf pl_order;               // patches in wave order (int32)
   DevBuf pl_corder;              // cluster columns in wave order (sweep_cluster > 1)
   int sweep_cluster = 1;         // CTAs per cluster along c in the MIC(0) sweeps
+  int spmv_rows = 1;             // 0: the patch-streamed SpMV instead of the row-parallel one
   DevBuf pl_part;                // per-patch partials (double)
   long long pl_cap = 0;
   int pl_tickets = 0;            // sweep tickets handed out in this solve
   long long spin_limit = 1ll << 20;  // polls of a wavefront edge word before giving up
+  int adjoint_fixed_x = 0;       // substep_vjp: 1 = positions held fixed (x-bar passes)
   int stale_patch = -1;          // failure-path test: a patch whose waits cannot succeed
   std::vector<int> pl_order_h;
 
@@ -268,6 +270,9 @@ struct Context {
   DevBuf xw;
   bool xw_valid = false;
   DevBuf corr_start, corr_cursor, corr_list;
+  // the reference-exact split: ranks of the splitting parents, the sphere
+  // pattern table and the caller's rotations on the device
+  DevBuf split_rank, split_pat, split_rot;
   unsigned long long corr_count = 0;
   // particle merge (wcg_merge.cuh): classes, flags, gathered volume and
   // momentum, index maps; the merge's draw counter
@@ -397,6 +402,13 @@ cudaError_t merge_liquid_particles(Context& c, int selector, const int* perm, lo
 // splitLiquidParticles with the rotations of key (after relabelling);
 // *added = particles appended
 cudaError_t split_liquid_particles(Context& c, unsigned long long key, long long* added);
+// the number of particles the split would split (after the volume update)
+cudaError_t split_liquid_parents(Context& c, long long* nparents);
+// the split with the caller's pattern table (kSplitPatternLen doubles) and
+// nparents row-major rotations (host arrays)
+cudaError_t split_liquid_particles_with(Context& c, const double* pattern, const double* rot,
+                                        long long nparents, long long* added);
+constexpr int kSplitPatternLen = 3 * (32 * 33 / 2 - 1);  // points of n = 2..32
 cudaError_t terminate_liquid_particles(Context& c, long long* removed);
 unsigned long long split_key(unsigned long long seed, unsigned long long k);
 // draws of merge call k of a seeded stream: selector, then three Fisher-Yates
@@ -406,8 +418,11 @@ void merge_draws(unsigned long long seed, unsigned long long k, int step, int* s
 // positions held fixed: cotangents of (v', C', x') in, of (v, C) and of the
 // viscosity (mubar, may be null) out (host arrays, original order; x-bar
 // passes through unchanged).
+// xbar0 null: positions held fixed (x-bar passes through); else the full
+// x-cotangent through the transfer weights
 cudaError_t substep_vjp(Context& c, double dt, const double* vbar, const double* Cbar,
-                        const double* xbar, double* vbar0, double* Cbar0, double* mubar);
+                        const double* xbar, double* vbar0, double* Cbar0, double* xbar0,
+                        double* mubar);
 // record the message returned by wcg_last_error() on this thread; returns code
 int set_last_error(int code, const std::string& msg);
 // FP64 MIC(0)-PCG on a system already placed in the context's fields

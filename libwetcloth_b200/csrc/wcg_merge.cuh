@@ -305,10 +305,20 @@ __global__ void k_split_count(const R* __restrict__ P, long long pcap, long long
 
 // the parent moves to centre + p_0 s and takes volume V/n; its children are
 // appended at np + (exclusive sum of the children of lower original index)
+//
+// With `pattern` given, the children sit as the reference places them: the
+// caller's sphere-pattern table (points of n = 2..32, 3n doubles each,
+// concatenated; TwoDScene::m_sphere_pattern) and one caller rotation per
+// splitting parent (row-major, parents ranked by original index in
+// `rank_pid`; the Q of the QR decomposition of the reference's
+// Matrix3s::Random(), TwoDScene.cpp:2390-2402).
 template <typename R>
 __global__ void k_split(R* P, long long pcap, long long np, int* pid,
                         const int* __restrict__ add_slot, const int* __restrict__ off_pid,
-                        unsigned long long key, double rho) {
+                        unsigned long long key, double rho,
+                        const double* __restrict__ pattern = nullptr,
+                        const double* __restrict__ rot = nullptr,
+                        const int* __restrict__ rank_pid = nullptr) {
   const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= np) return;
   const int add = add_slot[s];
@@ -322,11 +332,21 @@ __global__ void k_split(R* P, long long pcap, long long np, int* pid,
   const double new_rad = pow(new_vol / M_PI * 0.75, 1.0 / 3.0);
   const double splat = (new_rad > rad - new_rad ? new_rad : rad - new_rad) * 0.75;
   double Q[9];
-  split_rotation(splitmix64(key ^ (unsigned long long)f), Q);
+  const double* pat = pattern ? pattern + 3 * ((n - 1) * n / 2 - 1) : nullptr;
+  if (pattern)
+    for (int r = 0; r < 9; ++r) Q[r] = rot[(long long)rank_pid[f] * 9 + r];
+  else
+    split_rotation(splitmix64(key ^ (unsigned long long)f), Q);
   const long long base = np + off_pid[f];
   for (int i = 1; i < n; ++i) {
     double pt[3];
-    sphere_point(n, i, pt);
+    if (pat) {
+      pt[0] = pat[3 * i];
+      pt[1] = pat[3 * i + 1];
+      pt[2] = pat[3 * i + 2];
+    } else {
+      sphere_point(n, i, pt);
+    }
     const long long q = base + i - 1;
     for (int a = 0; a < 3; ++a) {
       const double rq = Q[a * 3] * pt[0] + Q[a * 3 + 1] * pt[1] + Q[a * 3 + 2] * pt[2];
@@ -340,11 +360,24 @@ __global__ void k_split(R* P, long long pcap, long long np, int* pid,
     pid[q] = (int)q;
   }
   double p0[3];
-  sphere_point(n, 0, p0);
+  if (pat) {
+    p0[0] = pat[0];
+    p0[1] = pat[1];
+    p0[2] = pat[2];
+  } else {
+    sphere_point(n, 0, p0);
+  }
   for (int a = 0; a < 3; ++a) P[(PX + a) * pcap + s] = (R)(c[a] + p0[a] * splat);
   P[PR * pcap + s] = (R)new_rad;
   P[PV * pcap + s] = (R)new_vol;
   P[PM * pcap + s] = (R)(new_vol * rho);
+}
+
+// 1 for a splitting parent (by original index), for the ranks of k_split
+__global__ void k_split_parent_flag(long long np, const int* __restrict__ add_pid,
+                                    int* __restrict__ flag) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < np) flag[i] = add_pid[i] > 0 ? 1 : 0;
 }
 
 // bucket of every particle's current position in the last build's bucket grid

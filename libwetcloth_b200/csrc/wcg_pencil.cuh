@@ -595,9 +595,14 @@ __global__ void __launch_bounds__(kPatchLines, 1)
           if (lv && ec_src) epc[v][k] = ld_relaxed_u64(ec_src + sn * ES + k);
         }
       }
+      // Every thread passed row u - 1's barrier, so slot (u - 1) % D is free:
+      // refill it with row u - 1 + D, before this row's barrier, from a lane
+      // that waits on no c-face edge word in this direction.  (Refills
+      // issued by thread 0 after each row's barrier -- of slot u % D, or of
+      // slot (u - 1) % D -- gave solves that differed from run to run at 256
+      // patches; this order repeats bit for bit.)
+      if (tid == (BWD ? 31 : kPatchLines - 1) && u >= 1 && u - 1 + D < NR) issue(u - 1 + D);
       __syncthreads();
-      // every thread is done with slot u % D: refill it with row u + D
-      if (tid == 0 && u + D < NR) issue(u + D);
     }
   }
   if (gave_up) {

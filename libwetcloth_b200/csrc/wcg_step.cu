@@ -81,6 +81,7 @@ void ctx_free(Context& c) {
                     &c.adj, &c.adjp, &c.adjmask, &c.adjstage, &c.adjvisc, &c.adjxc,
                     &c.visc, &c.viscflag, &c.dstage, &c.ustage,
                     &c.xw, &c.corr_start, &c.corr_cursor, &c.corr_list, &c.mwork,
+                    &c.split_rank, &c.split_pat, &c.split_rot,
                     &c.scratch, &c.dscalars, &c.derr, &c.ticket};
   for (DevBuf* b : bufs) b->release();
   if (c.hscalars) cudaFreeHost(c.hscalars);
@@ -1447,9 +1448,14 @@ static cudaError_t pl_pcg(Context& c, R* r, R* x, double tol_abs, int maxiters, 
     for (int b = 0; b < kPcgBatch; ++b) {
       {
         ProfScope prof(c, P_PCGVEC);
-        ++c.launches, k_pl_spmv_stream<R><<<spmv_blocks, kRedThreads, 0, c.stream>>>(
-            G, rows_per_chunk, nchunk, AD, AS, AA, AC, z, sold, snew, q, x, sc, part);
-        ++c.launches, k_red_alpha<<<1, kRedThreads, 0, c.stream>>>(part, spmv_blocks, sc);
+        if (c.spmv_rows)
+          ++c.launches, k_pl_spmv_s<R><<<kPlSpmvBlocks32, kRedThreads, 0, c.stream>>>(
+              G, AD, AS, AA, AC, z, sold, snew, q, x, sc, part);
+        else
+          ++c.launches, k_pl_spmv_stream<R><<<spmv_blocks, kRedThreads, 0, c.stream>>>(
+              G, rows_per_chunk, nchunk, AD, AS, AA, AC, z, sold, snew, q, x, sc, part);
+        ++c.launches, k_red_alpha<<<1, kRedThreads, 0, c.stream>>>(
+            part, c.spmv_rows ? kPlSpmvBlocks32 : spmv_blocks, sc);
       }
       WCG_TRY((pl_sweep<R, kForward, true>(c, fa)));
       {
@@ -1554,6 +1560,7 @@ static cudaError_t pl_project(Context& c, double bnorm, const int* lo, const int
     double ires = 0;
     WCG_TRY(pl_pcg<R>(c, r, x, want, c.prm.maxiters - total, &iters, &ic, &ires));
     total += iters;
+    part = c.scratch.as<double>();  // the inner solve may have grown the scratch buffer
     ProfScope prof3(c, P_REFINE);
     ++c.launches, k_pl_accumulate<R><<<kPlBlocks, kRedThreads, 0, c.stream>>>(G.len, x, dsc + 5, x64);
     ++c.launches, k_pl_residual64<R><<<kPlBlocks, kRedThreads, 0, c.stream>>>(
@@ -1803,6 +1810,7 @@ static cudaError_t mg_project(Context& c, double bnorm) {
     double ires = 0;
     WCG_TRY(mg_pcg<R>(c, r, x, want, c.prm.maxiters - total, &iters, &ic, &ires));
     total += iters;
+    part = c.scratch.as<double>();  // the inner solve may have grown the scratch buffer
     ProfScope prof3(c, P_REFINE);
     ++c.launches, k_pl_accumulate<R><<<nb, kMgThreads, 0, c.stream>>>(n, x, dsc + 5, x64);
     ++c.launches, k_mg_residual64<R><<<nb, kMgThreads, 0, c.stream>>>(L0, rhs, x64, r64, part);
@@ -1947,6 +1955,7 @@ static cudaError_t solve_assembled_t(Context& c) {
     double ires = 0;
     WCG_TRY(pcg_inner<R>(c, r, x, want, c.prm.maxiters - total, &iters, &ic, &ires));
     total += iters;
+    part = c.scratch.as<double>();  // the inner solve may have grown the scratch buffer
     ProfScope prof3(c, P_REFINE);
     ++c.launches, k_accumulate<R><<<kRedBlocks, kRedThreads, 0, c.stream>>>(al, nent, dof, x, dsc + 5, x64);
     ++c.launches, k_residual64<R><<<kRedBlocks, kRedThreads, 0, c.stream>>>(
@@ -2195,7 +2204,7 @@ cudaError_t prepared_solve_fp64(Context& c, double* out, int* iters, double* res
 template <typename R>
 static cudaError_t substep_vjp_t(Context& c, double dt, const double* vbar, const double* Cbar,
                                  const double* xbar, double* vbar0, double* Cbar0,
-                                 double* mubar) {
+                                 double* xbar0, double* mubar) {
   const long long np = c.np;
   const int rb = c.real_bytes();
   const bool visc = c.prm.viscosity > 0.0;
@@ -2237,12 +2246,13 @@ static cudaError_t substep_vjp_t(Context& c, double dt, const double* vbar, cons
   if (np == 0 || c.n_active == 0) {
     std::fill(vbar0, vbar0 + 3 * np, 0.0);
     std::fill(Cbar0, Cbar0 + 9 * np, 0.0);
+    if (xbar0) std::copy(xbar, xbar + 3 * np, xbar0);
     return cudaSuccess;
   }
   WCG_TRY(c.adj.ensure((size_t)kNumAdjFields * c.gcap * rb));
   WCG_TRY(c.adjmask.ensure((size_t)3 * c.gcap));
-  WCG_TRY(c.adjp.ensure((size_t)12 * c.pcap * rb));
-  WCG_TRY(c.adjstage.ensure((size_t)15 * np * sizeof(double)));
+  WCG_TRY(c.adjp.ensure((size_t)15 * c.pcap * rb));  // B (12 columns), XB (3)
+  WCG_TRY(c.adjstage.ensure((size_t)18 * np * sizeof(double)));
   double* st = c.adjstage.as<double>();
   WCG_TRY(cudaMemcpyAsync(st, vbar, 3 * np * sizeof(double), cudaMemcpyHostToDevice, c.stream));
   WCG_TRY(cudaMemcpyAsync(st + 3 * np, Cbar, 9 * np * sizeof(double), cudaMemcpyHostToDevice,
@@ -2252,6 +2262,7 @@ static cudaError_t substep_vjp_t(Context& c, double dt, const double* vbar, cons
   R* F = c.gfield.as<R>();
   R* AG = c.adj.as<R>();
   R* B = c.adjp.as<R>();
+  R* XB = xbar0 ? B + 12 * c.pcap : nullptr;
   const int* al = c.active_list.as<int>();
   const unsigned char* act = c.active.as<unsigned char>();
   const unsigned char* dof = c.gdof.as<unsigned char>();
@@ -2285,7 +2296,7 @@ static cudaError_t substep_vjp_t(Context& c, double dt, const double* vbar, cons
       c.g, act, c.pbuf[c.cur].as<R>(), c.pcap, np, c.pkey.as<long long>() + c.cur * c.pcap,
       c.pdelta.as<int>() + c.cur * c.pcap, F, c.gcap, (R)c.prm.flip_coeff,
       (R)c.prm.liquid_boundary_friction, c.pid[c.cur].as<int>(), st, st + 3 * np,
-      st + 12 * np, dt, B, XC);
+      st + 12 * np, dt, B, XC, XB);
   ++c.launches, k_adj_g2p<R><<<nb, 192, 0, c.stream>>>(
       c.g, al, c.pbuf[c.cur].as<R>(), c.pcap, c.cell_start.as<int>(),
       c.pdelta.as<int>() + c.cur * c.pcap, dr, B, F, c.gcap, AG, (R)c.prm.flip_coeff,
@@ -2331,19 +2342,23 @@ static cudaError_t substep_vjp_t(Context& c, double dt, const double* vbar, cons
   ++c.launches, k_adj_p2g<R><<<nblk(np, 128), 128, 0, c.stream>>>(
       c.g, act, c.pbuf[c.cur].as<R>(), c.pcap, np, c.pid[c.cur].as<int>(),
       c.pkey.as<long long>() + c.cur * c.pcap, c.pdelta.as<int>() + c.cur * c.pcap, F, AG,
-      c.gcap, st, st + 3 * np);
+      c.gcap, st, st + 3 * np, XB, st + 15 * np);
   WCG_TRY(cudaGetLastError());
   WCG_TRY(cudaMemcpyAsync(vbar0, st, 3 * np * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
   WCG_TRY(cudaMemcpyAsync(Cbar0, st + 3 * np, 9 * np * sizeof(double), cudaMemcpyDeviceToHost,
                           c.stream));
+  if (xbar0)
+    WCG_TRY(cudaMemcpyAsync(xbar0, st + 15 * np, 3 * np * sizeof(double),
+                            cudaMemcpyDeviceToHost, c.stream));
   return cudaStreamSynchronize(c.stream);
 }
 
 cudaError_t substep_vjp(Context& c, double dt, const double* vbar, const double* Cbar,
-                        const double* xbar, double* vbar0, double* Cbar0, double* mubar) {
+                        const double* xbar, double* vbar0, double* Cbar0, double* xbar0,
+                        double* mubar) {
   return c.prm.precision == 0
-             ? substep_vjp_t<double>(c, dt, vbar, Cbar, xbar, vbar0, Cbar0, mubar)
-             : substep_vjp_t<float>(c, dt, vbar, Cbar, xbar, vbar0, Cbar0, mubar);
+             ? substep_vjp_t<double>(c, dt, vbar, Cbar, xbar, vbar0, Cbar0, xbar0, mubar)
+             : substep_vjp_t<float>(c, dt, vbar, Cbar, xbar, vbar0, Cbar0, xbar0, mubar);
 }
 
 int correction_selector(unsigned long long seed, unsigned long long k, int step) {
@@ -2635,33 +2650,68 @@ static cudaError_t grow_particles(Context& c, long long cap) {
   return cudaSuccess;
 }
 
+// Children per particle (add_slot, by slot) and their exclusive offsets by
+// original index (off_pid); with `nparents`, also the rank of every splitting
+// parent by original index (split_rank).  Returns the child total in *total.
 template <typename R>
-static cudaError_t split_liquid_t(Context& c, unsigned long long key, long long* added) {
-  *added = 0;
+static cudaError_t split_count_t(Context& c, int* total, long long* nparents) {
   const long long n = c.np;
-  if (n == 0) return cudaSuccess;
-  ProfScope prof(c, P_OTHER);
   const double rad_fine = 1.0 / std::sqrt(3.0) * c.prm.dx * c.prm.cell_multiplier;
   const double vf = 4.0 / 3.0 * M_PI * rad_fine * rad_fine * rad_fine;
   WCG_TRY(c.corr_cursor.ensure((size_t)(n + 1) * sizeof(int)));
   WCG_TRY(c.corr_list.ensure((size_t)(n + 1) * sizeof(int)));
   const long long scan_tiles = (n + 1 + kScanTile - 1) / kScanTile + 1;
   WCG_TRY(ensure_scratch(c, (size_t)scan_tiles * sizeof(long long) + 64));
+  if (nparents) WCG_TRY(c.split_rank.ensure((size_t)(n + 1) * sizeof(int)));
   int* add_slot = c.corr_cursor.as<int>();
   int* off_pid = c.corr_list.as<int>();
+  int* dtot = (int*)(c.dscalars.as<double>() + 50);
   ++c.launches, k_split_count<R><<<nblk(n, 256), 256, 0, c.stream>>>(
       c.pbuf[c.cur].as<R>(), c.pcap, n, c.pid[c.cur].as<int>(), vf, add_slot, off_pid);
-  int* dtot = (int*)(c.dscalars.as<double>() + 50);
+  if (nparents) {
+    int* rank = c.split_rank.as<int>();
+    ++c.launches, k_split_parent_flag<<<nblk(n, 256), 256, 0, c.stream>>>(n, off_pid, rank);
+    exclusive_scan<int, int>(rank, n, rank, c.scratch.as<int>(), dtot + 1, c.stream);
+  }
   exclusive_scan<int, int>(off_pid, n, off_pid, c.scratch.as<int>(), dtot, c.stream);
-  int total = 0;
-  WCG_TRY(cudaMemcpyAsync(&total, dtot, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  int tot[2] = {0, 0};
+  WCG_TRY(cudaMemcpyAsync(tot, dtot, sizeof(tot), cudaMemcpyDeviceToHost, c.stream));
   WCG_TRY(cudaStreamSynchronize(c.stream));
-  if (total == 0) return cudaGetLastError();
+  *total = tot[0];
+  if (nparents) *nparents = tot[1];
+  return cudaGetLastError();
+}
+
+template <typename R>
+static cudaError_t split_liquid_t(Context& c, unsigned long long key, long long* added,
+                                  const double* pattern = nullptr, const double* rot = nullptr,
+                                  long long nparents = 0) {
+  *added = 0;
+  const long long n = c.np;
+  if (n == 0) return nparents == 0 ? cudaSuccess : cudaErrorInvalidValue;
+  ProfScope prof(c, P_OTHER);
+  int total = 0;
+  long long have = 0;
+  WCG_TRY(split_count_t<R>(c, &total, pattern ? &have : nullptr));
+  // a rotation per splitting parent, no more and no fewer
+  if (pattern && have != nparents) return cudaErrorInvalidValue;
+  if (total == 0) return cudaSuccess;
   if (n + total > 2000000000ll) return cudaErrorInvalidValue;
+  if (pattern) {
+    WCG_TRY(c.split_pat.ensure((size_t)kSplitPatternLen * sizeof(double)));
+    WCG_TRY(c.split_rot.ensure((size_t)nparents * 9 * sizeof(double)));
+    WCG_TRY(cudaMemcpyAsync(c.split_pat.p, pattern, (size_t)kSplitPatternLen * sizeof(double),
+                            cudaMemcpyHostToDevice, c.stream));
+    WCG_TRY(cudaMemcpyAsync(c.split_rot.p, rot, (size_t)nparents * 9 * sizeof(double),
+                            cudaMemcpyHostToDevice, c.stream));
+  }
   WCG_TRY(grow_particles(c, n + total));
+  int* add_slot = c.corr_cursor.as<int>();
+  int* off_pid = c.corr_list.as<int>();
   ++c.launches, k_split<R><<<nblk(n, 128), 128, 0, c.stream>>>(
       c.pbuf[c.cur].as<R>(), c.pcap, n, c.pid[c.cur].as<int>(), add_slot, off_pid, key,
-      c.prm.liquid_density);
+      c.prm.liquid_density, pattern ? c.split_pat.as<double>() : nullptr,
+      pattern ? c.split_rot.as<double>() : nullptr, pattern ? c.split_rank.as<int>() : nullptr);
   c.np = n + total;
   c.have_grid = false;
   c.xw_valid = false;
@@ -2678,6 +2728,21 @@ static cudaError_t split_liquid_t(Context& c, unsigned long long key, long long*
 cudaError_t split_liquid_particles(Context& c, unsigned long long key, long long* added) {
   return c.prm.precision == 0 ? split_liquid_t<double>(c, key, added)
                               : split_liquid_t<float>(c, key, added);
+}
+
+cudaError_t split_liquid_parents(Context& c, long long* nparents) {
+  *nparents = 0;
+  if (c.np == 0) return cudaSuccess;
+  int total = 0;
+  return c.prm.precision == 0 ? split_count_t<double>(c, &total, nparents)
+                              : split_count_t<float>(c, &total, nparents);
+}
+
+cudaError_t split_liquid_particles_with(Context& c, const double* pattern, const double* rot,
+                                        long long nparents, long long* added) {
+  return c.prm.precision == 0
+             ? split_liquid_t<double>(c, 0, added, pattern, rot, nparents)
+             : split_liquid_t<float>(c, 0, added, pattern, rot, nparents);
 }
 
 cudaError_t merge_liquid_particles(Context& c, int selector, const int* perm, long long* removed) {

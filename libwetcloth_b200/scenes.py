@@ -271,6 +271,19 @@ def dam_break(n_cells: int = 64, ppc: int = 8, seed: int = 0,
                  name=f"dam_break_{n_cells}^3_{ppc}ppc")
 
 
+def differentiation_block(n_cells: int = 64, ppc: int = 8, seed: int = 2,
+                          sigma: float = 0.2, viscosity: float = 1e-3) -> Scene:
+    """The dam-break block [0,0.4]x[0,0.8]x[0,0.4] (particle seed 0) with a
+    seeded Gaussian initial velocity (each component N(0, sigma^2), seed
+    `seed`) and the explicit viscosity on: the scene of the 200-step
+    gradient run."""
+    sc = dam_break(n_cells, ppc, 0)
+    sc.v = np.random.default_rng(seed).normal(0.0, sigma, sc.x.shape)
+    sc.params.viscosity = viscosity
+    sc.name = f"differentiation_{n_cells}^3_{ppc}ppc"
+    return sc
+
+
 def fine_volume(dx: float, cell_multiplier: float = 0.3535533906) -> float:
     """V_fine of relabelLiquidParticles (TwoDScene.cpp:2484-2489): the
     volume of a sphere of radius dx * cell_multiplier / sqrt(3)."""

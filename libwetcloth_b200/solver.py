@@ -102,9 +102,10 @@ class FluidScene:
         self.upload(x, v, C, *self._attrs)
 
     def substep_vjp(self, dt, vbar, Cbar, xbar, with_viscosity=False):
-        """Reverse mode of substep(dt) at the current (pre-step) state with the
-        positions held fixed: cotangents of (v', C', x') -> of (v, C, x), and of
-        the viscosity when with_viscosity."""
+        """Reverse mode of substep(dt) at the current (pre-step) state:
+        cotangents of (v', C', x') -> of (v, C, x), and of the viscosity when
+        with_viscosity.  The x-cotangent follows the transfer weights' x
+        (set_adjoint_positions(False) holds the positions fixed instead)."""
         n = self.num_particles
         arr = lambda a, k: np.ascontiguousarray(a, dtype=np.float64).reshape(n * k)
         vb, Cb, xb = arr(vbar, 3), arr(Cbar, 9), arr(xbar, 3)
@@ -116,6 +117,10 @@ class FluidScene:
                                      _dp(x0), ctypes.byref(mu)))
         out = (v0.reshape(n, 3), C0.reshape(n, 9), x0.reshape(n, 3))
         return out + (mu.value,) if with_viscosity else out
+
+    def set_adjoint_positions(self, differentiate=True):
+        """Whether substep_vjp differentiates through the particle positions."""
+        check(self.L.wcg_set_adjoint_positions(self.h, 1 if differentiate else 0))
 
     def set_viscosity(self, mu, substeps=1):
         """LiquidInfo::viscosity and its explicit sub-steps (0: off)."""
@@ -203,6 +208,25 @@ class FluidScene:
         the number of particles added."""
         add = ctypes.c_longlong(0)
         check(self.L.wcg_split_liquid_particles(self.h, int(key), ctypes.byref(add)))
+        return add.value
+
+    def split_parents(self):
+        """The number of particles the split would split now."""
+        k = ctypes.c_longlong(0)
+        check(self.L.wcg_split_parents(self.h, ctypes.byref(k)))
+        return k.value
+
+    def split_liquid_particles_with(self, pattern, rotations):
+        """splitLiquidParticles placed by the reference's sphere-pattern table
+        (1581 doubles: the points of n = 2..32) and one row-major rotation per
+        splitting parent (original-index order); returns the number added."""
+        pat = np.ascontiguousarray(pattern, dtype=np.float64).ravel()
+        rot = np.ascontiguousarray(rotations, dtype=np.float64).reshape(-1, 9)
+        if pat.size != 1581:
+            raise ValueError("pattern must hold 1581 doubles")
+        add = ctypes.c_longlong(0)
+        check(self.L.wcg_split_liquid_particles_with(self.h, _dp(pat), _dp(rot), rot.shape[0],
+                                                     ctypes.byref(add)))
         return add.value
 
     def terminate_liquid_particles(self):

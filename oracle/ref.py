@@ -66,6 +66,10 @@ def _lib(omp: bool):
         L.wcref_merge.restype = ctypes.c_int
         L.wcref_split.argtypes = [ctypes.c_void_p, ctypes.c_uint]
         L.wcref_split.restype = ctypes.c_int
+        L.wcref_split_inputs.argtypes = [ctypes.c_void_p, ctypes.c_uint, _D, _D, ctypes.c_int]
+        L.wcref_split_inputs.restype = ctypes.c_int
+        L.wcref_num_particles.argtypes = [ctypes.c_void_p]
+        L.wcref_num_particles.restype = ctypes.c_int
         L.wcref_set_terminator.argtypes = [ctypes.c_void_p, _D, _D, ctypes.c_double, ctypes.c_int]
         L.wcref_terminate.argtypes = [ctypes.c_void_p]
         L.wcref_terminate.restype = ctypes.c_int
@@ -165,6 +169,17 @@ class RefScene:
     def terminate(self) -> int:
         """terminateParticles; returns the particles removed."""
         return self.L.wcref_terminate(self.h)
+
+    def split_inputs(self, seed: int):
+        """The reference's sphere-pattern table (n = 2..32, 1581 doubles) and
+        the rotations its split draws after srand(seed), one row-major 3x3 per
+        splitting parent (call before split(seed))."""
+        pattern = np.zeros(3 * sum(range(2, 33)))
+        cap = max(1, self.L.wcref_num_particles(self.h))
+        rot = np.zeros(9 * cap)
+        k = self.L.wcref_split_inputs(self.h, int(seed), pattern.ctypes.data_as(_D),
+                                      rot.ctypes.data_as(_D), cap)
+        return pattern, rot[:9 * k].reshape(k, 9)
 
     def split(self, seed: int) -> int:
         """updateOptiVolume + splitLiquidParticles after srand(seed);

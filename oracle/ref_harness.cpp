@@ -807,6 +807,42 @@ int wcref_terminate(void* hp) {
   return before - s.getNumParticles();
 }
 
+// The inputs of the reference's split placement: the sphere-pattern table
+// TwoDScene::m_sphere_pattern[n] for n = 2..32 (3n doubles each, concatenated
+// into `pattern`) and the Q of the QR decomposition of each Matrix3s::Random()
+// that splitLiquidParticles (TwoDScene.cpp:2362-2480, serial build) draws
+// after srand(seed), one per splitting parent in fluid-index order, row
+// major.  Call before wcref_split with the same seed.  Returns the number of
+// splitting parents (rotations written up to `max`).
+int wcref_split_inputs(void* hp, unsigned seed, double* pattern, double* rot, int max) {
+  Harness* h = (Harness*)hp;
+  TwoDScene& s = *h->scene;
+  s.updateOptiVolume();
+  int off = 0;
+  for (int n = 2; n <= 32; ++n)
+    for (int i = 0; i < 3 * n; ++i) pattern[off++] = s.m_sphere_pattern[n](i);
+  const scalar rad_fine = mathutils::defaultRadiusMultiplier() * s.getCellSize() *
+                          s.getLiquidInfo().particle_cell_multiplier;
+  const scalar V_fine = 4.0 / 3.0 * M_PI * rad_fine * rad_fine * rad_fine;
+  srand(seed);
+  int k = 0;
+  const int nf = s.getNumFluidParticles();
+  for (int fidx = 0; fidx < nf; ++fidx) {
+    const int pidx = s.m_fluids[fidx];
+    if (s.m_classifier[pidx] != PC_L) continue;
+    const int n_split = std::min((int)ceil(s.m_fluid_vol(pidx) / V_fine), 32);
+    if (n_split <= 1) continue;
+    Matrix3s M = Matrix3s::Random();
+    Matrix3s Q, R;
+    mathutils::QRDecompose<scalar, 3>(M, Q, R);
+    if (k < max)
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) rot[k * 9 + a * 3 + b] = Q(a, b);
+    ++k;
+  }
+  return k;
+}
+
 // TwoDScene::updateOptiVolume and splitLiquidParticles, as
 // WetClothCore::stepSystem runs them before a step's grid build; the
 // children's rotations come from Matrix3s::Random() (rand()), seeded by

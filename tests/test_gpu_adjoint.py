@@ -1,8 +1,13 @@
-"""Reverse mode of one liquid sub-step (wcg_substep_vjp, libwetcloth_b200.autograd).
+"""Reverse mode of liquid sub-steps (wcg_substep_vjp, libwetcloth_b200.autograd).
 
-With the positions fixed the sub-step is affine in the particles' velocities
-v and affine matrices C, so central differences of the forward are exact up
-to rounding and the solver tolerance.  Checks, at a 1e-12 pressure criterion:
+At fixed positions the sub-step is affine in the particles' velocities v and
+affine matrices C, so central differences of the forward are exact up to
+rounding and the solver tolerance.  In the positions it is smooth away from
+the free surface and the walls (the transfer weights are C^1 quadratic
+B-splines; the grid's structure and the ghost-fluid fractions only move with
+particles near the surface), so the position derivative is checked on
+directions carried by interior particles.  Checks, at a 1e-12 pressure
+criterion:
 - the adjoint identity <y, J d> = <J^T y, d> for random d and y, with J d from
   central differences of the GPU forward (FP64: 1e-9 relative; FP32 with FP64
   refinement: 1e-4);
@@ -11,7 +16,12 @@ to rounding and the solver tolerance.  Checks, at a 1e-12 pressure criterion:
 - torch.autograd gradients of a scalar loss against per-entry central
   differences (1e-4 relative, the tolerance the plan states);
 - with the explicit viscosity on: the same identity, and the viscosity's
-  cotangent against a central difference in mu."""
+  cotangent against a central difference in mu;
+- the position cotangent: the identity for directions in x (interior
+  particles), FP64 and FP32 with refinement; wcg_set_adjoint_positions(0)
+  passing x-bar through;
+- rollout (checkpointed every k sub-steps, recomputed in the backward):
+  gradients equal to the chain of single sub-steps."""
 import numpy as np
 import pytest
 
@@ -70,7 +80,6 @@ def _vjp(g, sc, y, call=0):
     g.set_correction_count(call)
     vb, Cb, xb = g.substep_vjp(DT, y[:3 * n].reshape(n, 3), y[3 * n:12 * n].reshape(n, 9),
                                y[12 * n:].reshape(n, 3))
-    assert np.array_equal(xb.ravel(), y[12 * n:])
     return vb, Cb
 
 
@@ -245,3 +254,92 @@ def test_adjoint_identity_with_correction(kind, wcg):
     assert np.abs(x_on - x_off).max() > 1e-6
     g.close()
     g0.close()
+
+
+def _interior(sc, margin=3.0):
+    """Particles at least `margin` cells from the walls and the free surface."""
+    d = margin * sc.params.dx
+    x = sc.x
+    top = x[:, 1].max()
+    return ((x[:, 0] > d) & (x[:, 0] < 1.0 - d) & (x[:, 2] > d) & (x[:, 2] < 1.0 - d) &
+            (x[:, 1] > d) & (x[:, 1] < top - d))
+
+
+@pytest.mark.parametrize("precision,h,tol", [(_capi.WCG_FP64, 1e-6, 1e-6),
+                                             (_capi.WCG_FP32_REFINE, 1e-4, 2e-3)])
+def test_position_adjoint_identity(precision, h, tol, wcg):
+    """<y, J_x d> = <J_x^T y, d> for directions d in the positions of interior
+    particles: the x-cotangent through P2G's and G2P's weights and offsets.
+    The advection's identity part <y_x, d> is taken out of both sides, so the
+    tolerance bounds the weights' part."""
+    sc = _scene("curl24")
+    n = sc.x.shape[0]
+    mask = _interior(sc)
+    assert mask.sum() > 1000
+    rng = np.random.default_rng(17)
+    d = rng.normal(size=(n, 3)) * mask[:, None]
+    y = rng.normal(size=15 * n)
+    g = FluidScene(sc, precision=precision)
+    Jd = (_forward(g, sc.x + h * d, sc.v, sc.C) - _forward(g, sc.x - h * d, sc.v, sc.C)) / (2 * h)
+    g.set_state(sc.x, sc.v, sc.C)
+    g.set_correction_count(0)
+    _, _, xb = g.substep_vjp(DT, y[:3 * n].reshape(n, 3), y[3 * n:12 * n].reshape(n, 9),
+                             y[12 * n:].reshape(n, 3))
+    ident = float((y[12 * n:].reshape(n, 3) * d).sum())
+    lhs = float(y @ Jd) - ident
+    rhs = float((xb * d).sum()) - ident
+    assert abs(lhs - rhs) <= tol * abs(lhs), (lhs, rhs, ident)
+    g.close()
+
+
+def test_fixed_position_adjoint_passes_x_bar(wcg):
+    sc = _scene("dam16")
+    n = sc.x.shape[0]
+    y = np.random.default_rng(4).normal(size=15 * n)
+    g = FluidScene(sc)
+    outs = []
+    for diff in (False, True):
+        g.set_adjoint_positions(diff)
+        g.set_state(sc.x, sc.v, sc.C)
+        g.set_correction_count(0)
+        outs.append(g.substep_vjp(DT, y[:3 * n].reshape(n, 3), y[3 * n:12 * n].reshape(n, 9),
+                                  y[12 * n:].reshape(n, 3)))
+    (vb, Cb, xb), (vb2, Cb2, xb2) = outs
+    assert np.array_equal(xb.ravel(), y[12 * n:])
+    assert np.array_equal(vb, vb2) and np.array_equal(Cb, Cb2)
+    assert not np.array_equal(xb2.ravel(), y[12 * n:])
+    g.close()
+
+
+def test_rollout_checkpointing_matches_substep_chain(wcg):
+    """A 5-sub-step rollout with a checkpoint every 2 sub-steps gives the
+    loss and the gradients of the chain of single sub-step nodes, bit for
+    bit (the recomputation repeats the forward exactly)."""
+    torch = pytest.importorskip("torch")
+    from libwetcloth_b200.autograd import rollout, substep
+    sc = _scene("curl24")
+    n = sc.x.shape[0]
+    rng = np.random.default_rng(8)
+    wx = torch.from_numpy(rng.normal(size=(n, 3)))
+    target = torch.from_numpy(rng.normal(size=(n, 3)))
+    g = FluidScene(sc)
+    res = []
+    for mode in ("chain", "rollout"):
+        x = torch.from_numpy(sc.x.copy()).requires_grad_(True)
+        v = torch.from_numpy(sc.v.copy()).requires_grad_(True)
+        C = torch.from_numpy(sc.C.copy()).requires_grad_(True)
+        if mode == "chain":
+            xs, vs, Cs = x, v, C
+            for k in range(5):
+                xs, vs, Cs = substep(g, xs, vs, Cs, DT, correction_call=k)
+        else:
+            xs, vs, Cs = rollout(g, x, v, C, DT, 5, checkpoint_every=2, correction_call=0)
+        L = ((vs - target) ** 2).sum() + (xs * wx).sum() + 1e-3 * (Cs ** 2).sum()
+        L.backward()
+        res.append((L.item(), x.grad.numpy().copy(), v.grad.numpy().copy(),
+                    C.grad.numpy().copy()))
+    (l0, *g0), (l1, *g1) = res
+    assert l0 == l1
+    for a, b in zip(g0, g1):
+        assert np.array_equal(a, b)
+    g.close()

@@ -15,6 +15,7 @@ import pytest
 from libwetcloth_b200 import _capi, scenes
 from libwetcloth_b200.solver import FluidScene
 from oracle import oracle as oo
+from oracle import ref as oref
 
 pytestmark = pytest.mark.gpu
 DT = 1e-3
@@ -133,6 +134,48 @@ def test_split_after_step_fp64(kind, seed, wcg):
     _close(v, o.get("g2p_v"), 1e-10, "g2p_v")
     _close(x, o.get("adv_x"), 1e-12, "adv_x")
     g.close()
+
+
+@pytest.mark.parametrize("kind,seed", [("dam16", 3), ("curl16", 5)])
+def test_split_reference_placement_fp64(kind, seed, wcg):
+    """splitLiquidParticles placed as the reference places it
+    (TwoDScene.cpp:2362-2480): the reference's sphere-pattern table and the
+    rotations its serial build draws after srand(seed) go in through
+    wcg_split_liquid_particles_with.  After one step on both sides, the
+    particles added, their order, positions, velocities and affine matrices
+    agree with the reference's own splitLiquidParticles, and so does the next
+    step, which reads the children's volumes, masses and radii.  A rotation
+    count other than the number of splitting parents is refused with the
+    state unchanged."""
+    if not oref.available():
+        pytest.skip("oracle/_ref not built")
+    sc = _scene(kind, seed)
+    scenes.mixed_volumes(sc, seed, mrel=(0.3, 1.0, 2.5, 7.0, 40.0))
+    r = oref.RefScene(sc, mic=True)
+    r.step(DT, snapshot=True)
+    g = FluidScene(sc)
+    g.step(DT)
+    n0 = g.num_particles
+    pattern, rot = r.split_inputs(seed)
+    assert pattern.shape == (1581,)
+    assert g.split_parents() == rot.shape[0] > 0
+    with pytest.raises(_capi.WcgError) as e:
+        g.split_liquid_particles_with(pattern, rot[:-1])
+    assert e.value.code == _capi.WCG_ERR_ARG and g.num_particles == n0
+    added = g.split_liquid_particles_with(pattern, rot)
+    assert added == r.split(seed) and added > 0
+    assert g.num_particles == n0 + added
+    x, v, C = g.download()
+    _close(x, r.get("split_x"), 1e-12, "x")
+    _close(v, r.get("split_v"), 1e-9, "v")
+    _close(C, r.get("split_C"), 1e-9, "C", scale=4 * 16 * np.abs(v).max())
+    r.step(DT, snapshot=True)
+    g.step(DT)
+    x, v, C = g.download()
+    _close(v, r.get("g2p_v"), 1e-9, "g2p_v")
+    _close(x, r.get("adv_x"), 1e-12, "adv_x")
+    g.close()
+    r.close()
 
 
 def test_split_and_merge_seeded_steps(wcg):
