@@ -89,6 +89,28 @@ def test_pencil_deterministic(wcg):
     assert np.array_equal(a[m], b[m])
 
 
+@pytest.mark.parametrize("precision", [_capi.WCG_FP32_REFINE, _capi.WCG_FP64])
+def test_pencil_deterministic_256_patches(precision, wcg):
+    """The 256^3 half box (256 patches, more than the SMs hold at one CTA
+    each): three solves of the same system give the same pressures and
+    iteration counts bit for bit."""
+    sc = scenes.half_box(256, 2, seed=1)
+    res = []
+    for _ in range(3):
+        g = FluidScene(sc, precision=precision)
+        g.set_correction_count(0)
+        g.rebucketize_and_resample()
+        g.map_particle_nodes()
+        g.step_velocity(DT)
+        g.project_fine(DT)
+        st = g.stats()
+        res.append((np.nan_to_num(g.field("pressure")), st["pcg_iters"], st["refinements"]))
+        g.close()
+    for p, it, rf in res[1:]:
+        assert it == res[0][1] and rf == res[0][2]
+        assert np.array_equal(p, res[0][0])
+
+
 @pytest.mark.parametrize("cluster", [2, 4, 8])
 @pytest.mark.parametrize("kind,precision", [("curl48", _capi.WCG_FP64),
                                             ("slab64_x", _capi.WCG_FP64),
