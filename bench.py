@@ -387,10 +387,49 @@ def run_ours(args, rank, world, dev):
     if mg:
         out["multigrid_pcg"] = dict(mg, note="same step with the reference's default "
                                               "pressure solver (AMGPCGSolveSparse restated)")
+    if not args.no_config0:
+        out["config0"] = run_config0(dev)
     if not args.no_batch:
         out["batch"] = run_batch(args)
     if not args.no_cloth:
         out["cloth"] = run_cloth(dev)
+    return out
+
+
+def run_config0(dev, warmup=3, steps=97):
+    """The 64^3 dam break (8 per cell, seed 0, 265,302 particles), 100 steps
+    from the initial state as the reference arm's config0 runs them (3
+    warm-up + 97 timed): ms per step in FP64 and FP32 + refinement with
+    MIC(0)-PCG, and FP64 with the multigrid-PCG the reference uses by
+    default.  Device time with CUDA events on the context's stream."""
+    import torch
+    from libwetcloth_b200 import scenes
+    from libwetcloth_b200._capi import (WCG_FP32_REFINE, WCG_FP64, WCG_SOLVER_MG,
+                                        WCG_SOLVER_MIC0)
+    from libwetcloth_b200.solver import FluidScene
+    sc = scenes.dam_break(64, 8, 0)
+    out = {"workload": f"dam break 64^3, 8 ppc, seed 0, {sc.x.shape[0]} particles, "
+                       f"100 steps ({warmup} warm-up + {steps} timed)"}
+    for name, prec, solver in (("fp64_mic0", WCG_FP64, WCG_SOLVER_MIC0),
+                               ("fp32_refine_mic0", WCG_FP32_REFINE, WCG_SOLVER_MIC0),
+                               ("fp64_multigrid", WCG_FP64, WCG_SOLVER_MG)):
+        g = FluidScene(sc, precision=prec, solver=solver)
+        for _ in range(warmup):
+            g.step(DT)
+        stream = torch.cuda.ExternalStream(g.stream_ptr, device=f"cuda:{dev}")
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        iters = 0
+        for _ in range(steps):
+            g.step(DT)
+            iters += g.stats()["pcg_iters"]
+        e1.record(stream)
+        e1.synchronize()
+        out[name] = {"ms_per_step": round(e0.elapsed_time(e1) / steps, 3),
+                     "mean_pcg_iters": round(iters / steps, 1)}
+        g.close()
     return out
 
 

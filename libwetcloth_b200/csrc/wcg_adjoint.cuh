@@ -45,7 +45,11 @@ __device__ inline R quad_kernel_d(R r) {
 }
 
 // Adjoint grid fields (adj buffer, gcap each).
-enum AdjField : int { A_UBAR = 0, A_UTMP = 3, A_VSBAR = 6, kNumAdjFields = 9 };
+// A_PF: the forward pressure (kept across the adjoint solve); A_PHIB: the
+// cotangent of the cell-centred liquid phi through the ghost-fluid fractions.
+enum AdjField : int {
+  A_UBAR = 0, A_UTMP = 3, A_VSBAR = 6, A_PF = 9, A_PHIB = 10, kNumAdjFields = 11
+};
 
 // Original-order cotangents of (v', C', x') into sorted-order columns:
 // Cb = C-bar, vb = v-bar + dt d-bar, where d-bar is the cotangent of the step
@@ -58,6 +62,9 @@ enum AdjField : int { A_UBAR = 0, A_UTMP = 3, A_VSBAR = 6, kNumAdjFields = 9 };
 //   d-bar = x-bar - (g + s M d)(g . x-bar) - phi_now s M x-bar;
 // any other particle has d-bar = x-bar.  v' is recomputed by G2P from the
 // face velocities with constrainLiquidVelocity applied on the fly (friction).
+// A projected particle's x-cotangent also follows phi's and G's weights at x
+// and pos = x + d (see the block below); the particle correction before G2P
+// is taken as the identity in x.
 //
 // With XB: XB = x-bar + G2P's x-part (sorted order, 3 columns), from
 //   v'_a = sum w u_a,  C'_aq = f sum w u_a d_q  (f = flip 4/h^2, d = x_n - x_c):
@@ -108,6 +115,53 @@ __global__ void __launch_bounds__(128)
         const double Md = unit ? (double)d[q] - gr[q] * gd : (double)d[q];
         const double Mx = unit ? db[q] - gr[q] * gx : db[q];
         out[q] = db[q] - ((double)gr[q] + sc * Md) * gx - phi_now * sc * Mx;
+      }
+      if (XB) {
+        // the projected particle's own x (the weights of phi and G at x, and
+        // pos = x + d): x-bar_c = d-bar + (g - J) (g . x-bar)
+        //   - K^T M_s (d (g . x-bar) + phi_now x-bar),
+        // J = sum phi_n grad w_n, K^T v = sum phi_n iD ((x_n - pos) . v) grad w_n,
+        // M_s = (I - g g^T) / |G| (I when G is used unnormalised)
+        double vv[3];
+        for (int q = 0; q < 3; ++q) vv[q] = (double)d[q] * gx + phi_now * db[q];
+        if (unit) {
+          const double gv = gr[0] * vv[0] + gr[1] * vv[1] + gr[2] * vv[2];
+          for (int q = 0; q < 3; ++q) vv[q] = (vv[q] - gr[q] * gv) / (double)nrm;
+        }
+        const R org[3] = {(R)g.ox, (R)g.oy, (R)g.oz};
+        const R bs = (R)g.bs, dxr = (R)g.dx;
+        const R invh = R(1) / dxr;
+        int base[3];
+        R cn[3][3], wn[3][3], dn[3][3];
+        for (int q = 0; q < 3; ++q) {
+          base[q] = kp[q] + unpack_delta(dl, q);
+          for (int t = 0; t < 3; ++t) {
+            cn[q][t] = coord<R>(org[q], bs, dxr, base[q] + t, R(0));
+            wn[q][t] = quad_kernel<R>((x[q] - cn[q][t]) * invh);
+            dn[q][t] = quad_kernel_d<R>((x[q] - cn[q][t]) * invh) * invh;
+          }
+        }
+        const R* S = F + G_SPHI * fstride;
+        double J[3] = {0, 0, 0}, Kv[3] = {0, 0, 0};
+        for (int k = 0; k < 3; ++k)
+          for (int j = 0; j < 3; ++j)
+            for (int ii = 0; ii < 3; ++ii) {
+              const int NI_ = base[0] + ii, NJ_ = base[1] + j, NK_ = base[2] + k;
+              const bool on = in_grid(g, NI_, NJ_, NK_) && active[bucket_of(g, NI_, NJ_, NK_)];
+              const double ph = on ? (double)S[node_linear(g, NI_, NJ_, NK_)] : 3.0 * g.dx;
+              const double gw[3] = {(double)(dn[0][ii] * wn[1][j] * wn[2][k]),
+                                    (double)(wn[0][ii] * dn[1][j] * wn[2][k]),
+                                    (double)(wn[0][ii] * wn[1][j] * dn[2][k])};
+              const double pv = ((double)cn[0][ii] - (double)pos[0]) * vv[0] +
+                                ((double)cn[1][j] - (double)pos[1]) * vv[1] +
+                                ((double)cn[2][k] - (double)pos[2]) * vv[2];
+              for (int q = 0; q < 3; ++q) {
+                J[q] += ph * gw[q];
+                Kv[q] += ph * iD * pv * gw[q];
+              }
+            }
+        for (int q = 0; q < 3; ++q)
+          xg[q] += (R)(out[q] + ((double)gr[q] - J[q]) * gx - Kv[q] - db[q]);
       }
       for (int q = 0; q < 3; ++q) db[q] = out[q];
     }
@@ -393,6 +447,110 @@ __global__ void __launch_bounds__(192)
   AG[(A_VSBAR + a) * fstride + n] = ub + k * lam;
 }
 
+// The ghost-fluid fraction's part of the position cotangent.  On a face with
+// solid weight w > 0 between a liquid cell (phi < 0) and an air cell the
+// fraction theta = phi_neg / (phi_neg - phi_pos) (fraction_inside,
+// MathUtilities.h:286-293; clamped below at 0.01, Pressure.cpp:20) enters
+//   the apply step   u = inv_C (rhs - dt V_f (p_r - p_l) / (dx theta)), and
+//   the matrix       diag(liquid cell) += w dt inv_C V_f / (dx^2 theta)
+// (k_apply_pressure, k_assemble).  With u-bar the cotangent of u, lambda the
+// adjoint solve's solution and p the forward pressure:
+//   theta-bar = u-bar s (p_r - p_l) / theta + lambda_L p_L term / theta^2,
+// s = dt V_f inv_C / (dx theta); nothing where theta is clamped.  Per cell,
+//   phi-bar = sum over its six faces of theta-bar d(theta)/d(phi_cell),
+// and, where phi-bar is nonzero, the particle that sets the cell's phi
+// (updateLiquidPhi TwoDScene.cpp:3286-3376: phi = min over the particles of
+// the 27 cells around of |x_c - x_p| - max(0.883644 dx, r_p); none where the
+// wall rule or no particle sets it) goes to AM (sorted index, or -1).
+template <typename R>
+__global__ void __launch_bounds__(64)
+    k_adj_theta(GridDesc g, const int* __restrict__ active_list,
+                const unsigned char* __restrict__ active, const unsigned char* __restrict__ dof,
+                const R* __restrict__ F, long long fstride, R* __restrict__ AG, R dt,
+                const R* __restrict__ P, long long pcap, const int* __restrict__ start,
+                Walls walls, int have_liquid, int* __restrict__ AM) {
+  const int b = active_list[blockIdx.x];
+  const int l = threadIdx.x;
+  const int bk = b / (g.ni * g.nj);
+  const int rem = b - bk * g.ni * g.nj;
+  const int bj = rem / g.ni;
+  const int bi = rem - bj * g.ni;
+  const int I = bi * 4 + (l & 3), J = bj * 4 + ((l >> 2) & 3), K = bk * 4 + (l >> 4);
+  const long long n = (long long)b * 64 + l;
+  const R dx = (R)g.dx;
+  const R phic = F[G_LPHI * fstride + n];
+  const R* PF = AG + A_PF * fstride;
+  R phib = 0;
+  for (int f = 0; f < 6; ++f) {
+    const int a = f >> 1;
+    const bool upper = f & 1;
+    // the face node and the neighbour cell across it
+    const int qI = I + (upper && a == 0), qJ = J + (upper && a == 1), qK = K + (upper && a == 2);
+    const int mI = upper ? qI : I - (a == 0), mJ = upper ? qJ : J - (a == 1),
+              mK = upper ? qK : K - (a == 2);
+    if (!in_grid(g, qI, qJ, qK) || !active[bucket_of(g, qI, qJ, qK)]) continue;
+    const long long q = node_linear(g, qI, qJ, qK);
+    const R w = F[(G_WEIGHT + a) * fstride + q];
+    if (!(w > R(0))) continue;
+    const bool hm = in_grid(g, mI, mJ, mK) && active[bucket_of(g, mI, mJ, mK)];
+    const long long m = hm ? node_linear(g, mI, mJ, mK) : -1;
+    const R phim = hm ? F[G_LPHI * fstride + m] : R(0);
+    const R phil = upper ? phic : phim, phir = upper ? phim : phic;
+    if (!(phil < R(0) || phir < R(0))) continue;
+    if (phil < R(0) && phir < R(0)) continue;  // theta = 1
+    if (!upper && !hm) continue;                // a missing left cell is no particle's phi
+    const R neg = phil < R(0) ? phil : phir, pos = phil < R(0) ? phir : phil;
+    const R den = neg - pos;
+    const R theta = neg / den;
+    if (!(theta > R(kThetaCriterion))) continue;
+    const R V = F[(G_VOL + a) * fstride + q], invC = F[(G_INVC + a) * fstride + q];
+    const R pl = upper ? PF[n] : (hm ? PF[m] : R(0));
+    const R pr = upper ? PF[m] : PF[n];
+    const R sc = ((dt * V) * invC) / (dx * theta);
+    R tb = AG[(A_UBAR + a) * fstride + q] * sc * (pr - pl) / theta;
+    // the liquid side's diagonal, when it is a DOF and the air cell exists
+    const long long L = phil < R(0) ? (upper ? n : m) : (upper ? m : n);
+    if (hm && (dof[L] & 1)) {
+      const R term = (w * (dt / (dx * dx))) * (invC * V);
+      tb += F[G_PRESSURE * fstride + L] * PF[L] * term / (theta * theta);
+    }
+    // d(theta)/d(phi) of this cell
+    const bool cneg = phic < R(0);
+    phib += tb * (cneg ? -pos / (den * den) : neg / (den * den));
+  }
+  AG[A_PHIB * fstride + n] = phib;
+  int am = -1;
+  if (phib != R(0)) {
+    const R org[3] = {(R)g.ox, (R)g.oy, (R)g.oz};
+    const R bs = (R)g.bs;
+    R np_[3];
+    const int IJK[3] = {I, J, K};
+    for (int q = 0; q < 3; ++q) np_[q] = coord<R>(org[q], bs, dx, IJK[q], R(0.5));
+    const double sphi = wall_phi(walls, (double)np_[0], (double)np_[1], (double)np_[2],
+                                 3.0 * g.bs);
+    if (!(have_liquid && sphi < 0.0)) {
+      const R rmin = dx * (R)kLiquidPhiRadius;
+      R best = R(3) * bs;
+      for (int KZ = (K > 0 ? K - 1 : 0); KZ <= (K + 1 < g.NK ? K + 1 : g.NK - 1); ++KZ)
+        for (int KY = (J > 0 ? J - 1 : 0); KY <= (J + 1 < g.NJ ? J + 1 : g.NJ - 1); ++KY)
+          for (int KX = (I > 0 ? I - 1 : 0); KX <= (I + 1 < g.NI ? I + 1 : g.NI - 1); ++KX) {
+            const long long c = node_linear(g, KX, KY, KZ);
+            for (int s = start[c]; s < start[c + 1]; ++s) {
+              const R ddx = P[PX * pcap + s] - np_[0], ddy = P[PY * pcap + s] - np_[1],
+                      ddz = P[PZ * pcap + s] - np_[2];
+              const R r = P[PR * pcap + s];
+              const R d = sqrt((ddx * ddx + ddy * ddy) + ddz * ddz) - (rmin > r ? rmin : r);
+              if (d < best) {
+                best = d;
+                am = s;
+              }
+            }
+          }
+    }
+  }
+  AM[n] = am;
+}
+
 // stepVelocity^T and P2G^T per particle over its own face stencils (nodes of
 // inactive buckets skipped): mom-bar = v*-bar / m_node on heavy nodes,
 //   v-bar_a = sum m w mom-bar,  C-bar_aq = sum m w mom-bar d_q;
@@ -408,7 +566,8 @@ __global__ void __launch_bounds__(128)
               const long long* __restrict__ key, const int* __restrict__ delta,
               const R* __restrict__ F, const R* __restrict__ AG, long long fstride,
               double* __restrict__ vbar0, double* __restrict__ Cbar0,
-              const R* __restrict__ XB, double* __restrict__ xbar0) {
+              const R* __restrict__ XB, double* __restrict__ xbar0,
+              const int* __restrict__ AM) {
   const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= np) return;
   const long long i = pid[s];
@@ -478,6 +637,26 @@ __global__ void __launch_bounds__(128)
     Cbar0[i * 9 + a * 3 + 0] = (double)b0;
     Cbar0[i * 9 + a * 3 + 1] = (double)b1;
     Cbar0[i * 9 + a * 3 + 2] = (double)b2;
+  }
+  if (XB && AM) {
+    // the liquid phi of the cells this particle sets: d(phi)/dx = (x - x_c) / |x - x_c|
+    const R* PB = AG + A_PHIB * fstride;
+    for (int KZ = (KK > 0 ? KK - 1 : 0); KZ <= (KK + 1 < g.NK ? KK + 1 : g.NK - 1); ++KZ)
+      for (int KY = (KJ > 0 ? KJ - 1 : 0); KY <= (KJ + 1 < g.NJ ? KJ + 1 : g.NJ - 1); ++KY)
+        for (int KX = (KI > 0 ? KI - 1 : 0); KX <= (KI + 1 < g.NI ? KI + 1 : g.NI - 1); ++KX) {
+          if (!active[bucket_of(g, KX, KY, KZ)]) continue;
+          const long long c = node_linear(g, KX, KY, KZ);
+          if (AM[c] != (int)s) continue;
+          const R ex = x - coord<R>(org[0], bs, dx, KX, R(0.5));
+          const R ey = y - coord<R>(org[1], bs, dx, KY, R(0.5));
+          const R ez = z - coord<R>(org[2], bs, dx, KZ, R(0.5));
+          const R dist = sqrt((ex * ex + ey * ey) + ez * ez);
+          if (!(dist > R(0))) continue;
+          const R pb = PB[c] / dist;
+          xg[0] += pb * ex;
+          xg[1] += pb * ey;
+          xg[2] += pb * ez;
+        }
   }
   if (XB)
     for (int q = 0; q < 3; ++q) xbar0[i * 3 + q] = (double)XB[q * pcap + s] + (double)xg[q];

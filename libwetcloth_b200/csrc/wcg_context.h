@@ -289,6 +289,7 @@ struct Context {
   // host staging
   DevBuf adj, adjp, adjmask, adjstage, adjvisc;
   DevBuf adjxc;  // corrected positions of the sub-step (3 Reals per particle)
+  DevBuf adjam;  // per cell: the sorted index of the particle that sets its liquid phi
 
   // implicit viscosity (wcg_visc.cuh): PCG vectors x, r, p, q and the
   // diagonal (3 face fields each), face flags

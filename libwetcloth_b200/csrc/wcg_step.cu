@@ -78,7 +78,7 @@ void ctx_free(Context& c) {
                     &c.rx64, &c.rr64, &c.rb64,
                     &c.pl, &c.pl64, &c.pl_edge, &c.pl_order, &c.pl_corder, &c.pl_part,
                     &c.mg, &c.mg_mask, &c.mg_vec,
-                    &c.adj, &c.adjp, &c.adjmask, &c.adjstage, &c.adjvisc, &c.adjxc,
+                    &c.adj, &c.adjp, &c.adjmask, &c.adjstage, &c.adjvisc, &c.adjxc, &c.adjam,
                     &c.visc, &c.viscflag, &c.dstage, &c.ustage,
                     &c.xw, &c.corr_start, &c.corr_cursor, &c.corr_list, &c.mwork,
                     &c.split_rank, &c.split_pat, &c.split_rot,
@@ -2310,7 +2310,18 @@ static cudaError_t substep_vjp_t(Context& c, double dt, const double* vbar, cons
       c.g, al, act, AG + A_UTMP * c.gcap, AG + A_UBAR * c.gcap, v0, c.gcap);
   ++c.launches, k_adj_apply<R><<<nb, 64, 0, c.stream>>>(c.g, al, act, dof, AG, F, c.gcap, (R)dt);
   WCG_TRY(cudaGetLastError());
+  if (xbar0)  // the forward pressure, for the ghost-fluid fractions' part
+    WCG_TRY(cudaMemcpyAsync(AG + A_PF * c.gcap, F + G_PRESSURE * c.gcap, c.gcap * sizeof(R),
+                            cudaMemcpyDeviceToDevice, c.stream));
   WCG_TRY(solve_assembled_t<R>(c));  // A lambda = p-bar, A symmetric
+  int* AM = nullptr;
+  if (xbar0) {
+    WCG_TRY(c.adjam.ensure((size_t)c.gcap * sizeof(int)));
+    AM = c.adjam.as<int>();
+    ++c.launches, k_adj_theta<R><<<nb, 64, 0, c.stream>>>(
+        c.g, al, act, dof, F, c.gcap, AG, (R)dt, c.pbuf[c.cur].as<R>(), c.pcap,
+        c.cell_start.as<int>(), make_walls(c), c.np > 0 ? 1 : 0, AM);
+  }
   ++c.launches, k_adj_div<R><<<nb, 192, 0, c.stream>>>(c.g, al, act, dof, F, c.gcap, AG,
                                                         visc ? 1 : 0);
   if (visc) {
@@ -2342,7 +2353,7 @@ static cudaError_t substep_vjp_t(Context& c, double dt, const double* vbar, cons
   ++c.launches, k_adj_p2g<R><<<nblk(np, 128), 128, 0, c.stream>>>(
       c.g, act, c.pbuf[c.cur].as<R>(), c.pcap, np, c.pid[c.cur].as<int>(),
       c.pkey.as<long long>() + c.cur * c.pcap, c.pdelta.as<int>() + c.cur * c.pcap, F, AG,
-      c.gcap, st, st + 3 * np, XB, st + 15 * np);
+      c.gcap, st, st + 3 * np, XB, st + 15 * np, AM);
   WCG_TRY(cudaGetLastError());
   WCG_TRY(cudaMemcpyAsync(vbar0, st, 3 * np * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
   WCG_TRY(cudaMemcpyAsync(Cbar0, st + 3 * np, 9 * np * sizeof(double), cudaMemcpyDeviceToHost,

@@ -292,6 +292,36 @@ def test_position_adjoint_identity(precision, h, tol, wcg):
     g.close()
 
 
+def test_position_adjoint_identity_free_surface(wcg):
+    """The same identity for directions carried by particles within two cells
+    of the free surface (away from the walls): their positions set the
+    liquid phi of the surface cells, hence the ghost-fluid fractions of the
+    pressure matrix and of the pressure gradient (k_adj_theta)."""
+    sc = _scene("curl24")
+    n = sc.x.shape[0]
+    dx = sc.params.dx
+    x = sc.x
+    top = x[:, 1].max()
+    mask = ((x[:, 0] > 3 * dx) & (x[:, 0] < 1 - 3 * dx) & (x[:, 2] > 3 * dx) &
+            (x[:, 2] < 1 - 3 * dx) & (x[:, 1] > top - 2 * dx))
+    assert mask.sum() > 500
+    rng = np.random.default_rng(23)
+    d = rng.normal(size=(n, 3)) * mask[:, None]
+    y = rng.normal(size=15 * n)
+    g = FluidScene(sc)
+    h = 1e-7
+    Jd = (_forward(g, sc.x + h * d, sc.v, sc.C) - _forward(g, sc.x - h * d, sc.v, sc.C)) / (2 * h)
+    g.set_state(sc.x, sc.v, sc.C)
+    g.set_correction_count(0)
+    _, _, xb = g.substep_vjp(DT, y[:3 * n].reshape(n, 3), y[3 * n:12 * n].reshape(n, 9),
+                             y[12 * n:].reshape(n, 3))
+    ident = float((y[12 * n:].reshape(n, 3) * d).sum())
+    lhs = float(y @ Jd) - ident
+    rhs = float((xb * d).sum()) - ident
+    assert abs(lhs - rhs) <= 1e-5 * abs(lhs), (lhs, rhs, ident)
+    g.close()
+
+
 def test_fixed_position_adjoint_passes_x_bar(wcg):
     sc = _scene("dam16")
     n = sc.x.shape[0]

@@ -15,10 +15,10 @@ Checks:
 - the FP32 (with FP64 refinement, 1e-6 residual) gradient against the FP64
   one.
 
-The reverse mode holds the grid's discrete structure and the ghost-fluid
-fractions of the free surface at their forward values, so it is the
-derivative of the step with those fixed; the tolerances below bound what
-that leaves out over 200 sub-steps as measured here."""
+The reverse mode follows the positions through the transfer weights, the
+liquid phi of the ghost-fluid fractions and the solid projection; the grid's
+discrete structure (activation, DOFs, valid faces) is held at its forward
+values, which central differences of this size do not cross."""
 import time
 
 import numpy as np
@@ -111,8 +111,9 @@ def test_config3_fp64_gradient_against_central_differences(fp64_run):
           f"mu fd {fd_mu:.6e} adjoint {gmu:.6e} rel {abs(fd_mu - gmu) / abs(fd_mu):.2e}")
     for (f, a_), r in zip(rows, rel):
         print(f"  fd {f:+.6e}  adjoint {a_:+.6e}  rel {r:.2e}")
-    assert np.median(rel) <= 1e-2
-    assert abs(fd_mu - gmu) <= 1e-1 * abs(fd_mu)
+    assert np.median(rel) <= 1e-4
+    assert rel.max() <= 1e-3
+    assert abs(fd_mu - gmu) <= 1e-4 * abs(fd_mu)
 
 
 def test_config3_fp32_gradient_against_fp64(fp64_run):
@@ -128,6 +129,6 @@ def test_config3_fp32_gradient_against_fp64(fp64_run):
     print(f"\nconfig3 FP32: loss {L:.6e} (FP64 {L64:.6e}), gradient {t:.1f} s; "
           f"|g32 - g64| / |g64| = {err:.2e}, cosine {cos:.6f}; "
           f"mu {gmu:.6e} (FP64 {gmu64:.6e})")
-    assert abs(L - L64) <= 1e-3 * abs(L64)
-    assert err <= 1e-1
-    assert abs(gmu - gmu64) <= 1e-1 * abs(gmu64)
+    assert abs(L - L64) <= 1e-5 * abs(L64)
+    assert err <= 1e-2
+    assert abs(gmu - gmu64) <= 5e-2 * abs(gmu64)
