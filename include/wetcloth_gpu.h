@@ -293,6 +293,34 @@ int wcg_split_liquid_particles_with(wcg_ctx* ctx, const double* pattern, const d
  * only particles without volume are removed.  wcg_substep runs it first when
  * params.terminator is set. */
 int wcg_terminate_liquid_particles(wcg_ctx* ctx, long long* removed);
+/* Terminator shapes: the DistanceFieldObjects of the scene whose usage is
+ * DFU_TERMINATOR (DistanceFields.cpp:477-520), any of box, sphere, capsule
+ * and cylinder, rotated and inside or not.  A particle is removed where
+ *   phi = min(3 bucket size, min over the shapes of their phi)
+ * is negative -- TwoDScene::computePhiVel (TwoDScene.cpp:5427-5447) over the
+ * distance-field groups, each a union of its members
+ * (DistanceFieldOperator, DistanceFields.cpp:835-849).  A shape's phi is
+ * DistanceFieldObject::compute_phi (DistanceFields.cpp:601-660): the position
+ * is taken into the object's frame by the quaternion sandwich
+ * conj(rot) (0, p - c) conj(rot)^-1 (box, capsule, cylinder), then
+ *   box      param = half extents x, y, z, corner radius
+ *   sphere   param[0] = radius
+ *   capsule  param = radius, half length (axis along x)
+ *   cylinder param = outer radius, corner radius, half height (axis along y)
+ * and negated for an inside object.  rot is the object's rotation
+ * (Eigen::AngleAxis of its axis and angle, w x y z).  wcg_set_terminators
+ * replaces the terminator of wcg_params (n = 0: none); while any shape is
+ * set, wcg_substep runs terminateParticles first. */
+enum { WCG_SHAPE_BOX = 0, WCG_SHAPE_SPHERE = 1, WCG_SHAPE_CAPSULE = 2, WCG_SHAPE_CYLINDER = 3 };
+#define WCG_MAX_TERMINATOR_SHAPES 16
+typedef struct {
+  int type;           /* WCG_SHAPE_* */
+  int inside;         /* the object's inside flag: phi negated */
+  double center[3];
+  double rot[4];      /* w, x, y, z */
+  double param[4];
+} wcg_shape;
+int wcg_set_terminators(wcg_ctx* ctx, int n, const wcg_shape* shapes);
 /* the key wcg_substep uses for its k-th split */
 unsigned long long wcg_split_key(unsigned long long seed, unsigned long long k);
 /* the draws wcg_substep uses for its k-th merge: SplitMix64 of the seed and k

@@ -72,6 +72,19 @@ class WcgParams(ctypes.Structure):
     ]
 
 
+WCG_SHAPE_BOX, WCG_SHAPE_SPHERE, WCG_SHAPE_CAPSULE, WCG_SHAPE_CYLINDER = 0, 1, 2, 3
+
+
+class WcgShape(ctypes.Structure):
+    _fields_ = [
+        ("type", ctypes.c_int),
+        ("inside", ctypes.c_int),
+        ("center", ctypes.c_double * 3),
+        ("rot", ctypes.c_double * 4),
+        ("param", ctypes.c_double * 4),
+    ]
+
+
 class WcgStats(ctypes.Structure):
     _fields_ = [
         ("substeps", ctypes.c_int),
@@ -137,6 +150,8 @@ SIGNATURES = {
                                                        ctypes.POINTER(ctypes.c_longlong)]),
     "wcg_terminate_liquid_particles": (ctypes.c_int, [ctypes.c_void_p,
                                                       ctypes.POINTER(ctypes.c_longlong)]),
+    "wcg_set_terminators": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
+                                           ctypes.POINTER(WcgShape)]),
     "wcg_split_key": (ctypes.c_ulonglong, [ctypes.c_ulonglong, ctypes.c_ulonglong]),
     "wcg_merge_draws": (ctypes.c_int, [ctypes.c_ulonglong, ctypes.c_ulonglong, ctypes.c_int,
                                        ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),

@@ -308,6 +308,20 @@ int wcg_create(const wcg_params* params, wcg_ctx** out) {
     const int k = atoi(v);
     ctx->c.sweep_cluster = (k == 2 || k == 4 || k == 8) ? k : 1;
   }
+  // the params' terminator box as the one terminator shape (identity rotation)
+  if (p.terminator) {
+    wcg::TermShape& t = ctx->c.term.s[0];
+    t.type = 0;
+    t.sign = p.term_inside ? -1.0 : 1.0;
+    for (int a = 0; a < 3; ++a) {
+      t.c[a] = p.term_center[a];
+      t.par[a] = p.term_half[a];
+    }
+    t.par[3] = p.term_radius;
+    t.q[0] = 1.0;
+    t.q[1] = t.q[2] = t.q[3] = 0.0;
+    ctx->c.term.n = 1;
+  }
   cudaError_t e = wcg::ctx_init(ctx->c);
   if (e != cudaSuccess) {
     std::string m = std::string("context init: ") + cudaGetErrorString(e);
@@ -671,6 +685,36 @@ int wcg_terminate_liquid_particles(wcg_ctx* ctx, long long* removed) {
   WCG_CALL(ctx, wcg::terminate_liquid_particles(ctx->c, &rem), "terminateParticles");
   if (removed) *removed = rem;
   return device_status(ctx->c, "terminateParticles");
+}
+
+int wcg_set_terminators(wcg_ctx* ctx, int n, const wcg_shape* shapes) {
+  WCG_CHECK_CTX(ctx);
+  if (n < 0 || n > WCG_MAX_TERMINATOR_SHAPES || (n > 0 && !shapes))
+    return fail(WCG_ERR_ARG, "between 0 and 16 terminator shapes");
+  wcg::TermSet t{};
+  for (int k = 0; k < n; ++k) {
+    const wcg_shape& h = shapes[k];
+    if (h.type < WCG_SHAPE_BOX || h.type > WCG_SHAPE_CYLINDER)
+      return fail(WCG_ERR_ARG, "unknown terminator shape type");
+    bool finite = true;
+    for (int a = 0; a < 3; ++a) finite = finite && std::isfinite(h.center[a]);
+    for (int a = 0; a < 4; ++a) finite = finite && std::isfinite(h.rot[a]) && std::isfinite(h.param[a]);
+    const double q2 = h.rot[0] * h.rot[0] + h.rot[1] * h.rot[1] + h.rot[2] * h.rot[2] +
+                      h.rot[3] * h.rot[3];
+    if (!finite || !(q2 > 0.0)) return fail(WCG_ERR_ARG, "terminator shape not finite");
+    wcg::TermShape& s = t.s[k];
+    s.type = h.type;
+    s.sign = h.inside ? -1.0 : 1.0;
+    for (int a = 0; a < 3; ++a) s.c[a] = h.center[a];
+    for (int a = 0; a < 4; ++a) {
+      s.q[a] = h.rot[a];
+      s.par[a] = h.param[a];
+    }
+  }
+  t.n = n;
+  ctx->c.term = t;
+  ctx->c.prm.terminator = n > 0 ? 1 : 0;
+  return WCG_OK;
 }
 
 int wcg_set_correction_count(wcg_ctx* ctx, unsigned long long k) {

@@ -175,6 +175,132 @@ struct Walls {
   int enabled;
 };
 
+// Terminator shapes (DistanceFieldObject::compute_phi, DistanceFields.cpp:
+// 601-660; the SDFs sphere_phi, capsule_phi, box_phi, cylinder_phi :32-114).
+// Products and sums in the reference's order, rounded one by one.
+constexpr int kMaxTermShapes = 16;
+struct TermShape {
+  int type;        // 0 box, 1 sphere, 2 capsule, 3 cylinder
+  double sign;     // -1 for inside objects
+  double c[3];
+  double q[4];     // rotation w, x, y, z
+  double par[4];
+};
+struct TermSet {
+  int n;
+  TermShape s[kMaxTermShapes];
+};
+
+__host__ __device__ inline double rn_add(double a, double b) {
+#ifdef __CUDA_ARCH__
+  return __dadd_rn(a, b);
+#else
+  return a + b;
+#endif
+}
+__host__ __device__ inline double rn_sub(double a, double b) {
+#ifdef __CUDA_ARCH__
+  return __dsub_rn(a, b);
+#else
+  return a - b;
+#endif
+}
+__host__ __device__ inline double rn_mul(double a, double b) {
+#ifdef __CUDA_ARCH__
+  return __dmul_rn(a, b);
+#else
+  return a * b;
+#endif
+}
+
+// Eigen's quaternion product (w, x, y, z), terms left to right
+__device__ inline void quat_mul(const double a[4], const double b[4], double o[4]) {
+  o[0] = rn_sub(rn_sub(rn_sub(rn_mul(a[0], b[0]), rn_mul(a[1], b[1])), rn_mul(a[2], b[2])),
+                rn_mul(a[3], b[3]));
+  o[1] = rn_sub(rn_add(rn_add(rn_mul(a[0], b[1]), rn_mul(a[1], b[0])), rn_mul(a[2], b[3])),
+                rn_mul(a[3], b[2]));
+  o[2] = rn_sub(rn_add(rn_add(rn_mul(a[0], b[2]), rn_mul(a[2], b[0])), rn_mul(a[3], b[1])),
+                rn_mul(a[1], b[3]));
+  o[3] = rn_sub(rn_add(rn_add(rn_mul(a[0], b[3]), rn_mul(a[3], b[0])), rn_mul(a[1], b[2])),
+                rn_mul(a[2], b[1]));
+}
+
+// the position in the object's frame: conj(q) (0, p - c) conj(q)^-1 + c
+__device__ inline void term_frame(const TermShape& t, const double p[3], double r[3]) {
+  const double iq[4] = {t.q[0], -t.q[1], -t.q[2], -t.q[3]};
+  const double p0[4] = {0.0, rn_sub(p[0], t.c[0]), rn_sub(p[1], t.c[1]), rn_sub(p[2], t.c[2])};
+  // squaredNorm over the coefficients (x, y, z, w) in halves
+  const double n2 = rn_add(rn_add(rn_mul(iq[1], iq[1]), rn_mul(iq[2], iq[2])),
+                           rn_add(rn_mul(iq[3], iq[3]), rn_mul(iq[0], iq[0])));
+  const double inv[4] = {iq[0] / n2, -iq[1] / n2, -iq[2] / n2, -iq[3] / n2};
+  double a[4], b[4];
+  quat_mul(iq, p0, a);
+  quat_mul(a, inv, b);
+  for (int k = 0; k < 3; ++k) r[k] = rn_add(b[k + 1], t.c[k]);
+}
+
+__device__ inline double norm3(double x, double y, double z) {
+  return sqrt(rn_add(rn_add(rn_mul(x, x), rn_mul(y, y)), rn_mul(z, z)));
+}
+
+__device__ inline double term_shape_phi(const TermShape& t, const double p[3]) {
+  double phi = 0.0;
+  if (t.type == 1) {  // sphere
+    phi = rn_sub(norm3(rn_sub(p[0], t.c[0]), rn_sub(p[1], t.c[1]), rn_sub(p[2], t.c[2])),
+                 t.par[0]);
+  } else {
+    double r[3];
+    term_frame(t, p, r);
+    if (t.type == 0) {  // box
+      double d[3], da[3];
+      for (int k = 0; k < 3; ++k) {
+        d[k] = rn_sub(fabs(rn_sub(r[k], t.c[k])), t.par[k]);
+        da[k] = d[k] > 0.0 ? d[k] : 0.0;
+      }
+      double m = d[0] > d[1] ? d[0] : d[1];
+      m = m > d[2] ? m : d[2];
+      m = m < 0.0 ? m : 0.0;
+      phi = rn_sub(rn_add(m, norm3(da[0], da[1], da[2])), t.par[3]);
+    } else if (t.type == 2) {  // capsule along x
+      const double hl = t.par[1];
+      const double pa[3] = {rn_sub(r[0], rn_sub(t.c[0], hl)), rn_sub(r[1], t.c[1]),
+                            rn_sub(r[2], t.c[2])};
+      const double ba0 = rn_mul(2.0, hl);
+      // pa . ba with ba = (2 hl, 0, 0), then / (4 hl hl), clamped to [0, 1]
+      const double dot = rn_add(rn_add(rn_mul(pa[0], ba0), rn_mul(pa[1], 0.0)),
+                                rn_mul(pa[2], 0.0));
+      double h = dot / rn_mul(rn_mul(4.0, hl), hl);
+      h = h < 0.0 ? 0.0 : (h > 1.0 ? 1.0 : h);
+      phi = rn_sub(norm3(rn_sub(pa[0], rn_mul(ba0, h)), rn_sub(pa[1], rn_mul(0.0, h)),
+                         rn_sub(pa[2], rn_mul(0.0, h))),
+                   t.par[0]);
+    } else {  // cylinder along y
+      const double q0 = rn_sub(r[0], t.c[0]), q1 = rn_sub(r[1], t.c[1]), q2 = rn_sub(r[2], t.c[2]);
+      const double d0 =
+          rn_add(rn_sub(sqrt(rn_add(rn_mul(q0, q0), rn_mul(q2, q2))), t.par[0]), t.par[1]);
+      const double d1 = rn_sub(fabs(q1), t.par[2]);
+      double m = d0 > d1 ? d0 : d1;
+      m = m < 0.0 ? m : 0.0;
+      const double e0 = d0 > 0.0 ? d0 : 0.0, e1 = d1 > 0.0 ? d1 : 0.0;
+      phi = rn_sub(rn_add(m, sqrt(rn_add(rn_mul(e0, e0), rn_mul(e1, e1)))), t.par[1]);
+    }
+  }
+  return t.sign * phi;
+}
+
+// TwoDScene::computePhiVel over the terminator groups: the running minimum
+// from 3 bucket sizes of each group's union (from 1e20)
+__device__ inline double term_phi(const TermSet& T, double px, double py, double pz,
+                                  double three_bs) {
+  const double p[3] = {px, py, pz};
+  double u = 1e20;
+  for (int k = 0; k < T.n; ++k) {
+    const double f = term_shape_phi(T.s[k], p);
+    u = f < u ? f : u;
+  }
+  return u < three_bs ? u : three_bs;
+}
+
 __device__ inline double wall_phi(const Walls& w, double px, double py,
                                   double pz, double three_bs) {
   if (!w.enabled) return three_bs;

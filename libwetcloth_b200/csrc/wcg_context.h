@@ -255,6 +255,7 @@ struct Context {
   int pl_tickets = 0;            // sweep tickets handed out in this solve
   long long spin_limit = 1ll << 20;  // polls of a wavefront edge word before giving up
   int adjoint_fixed_x = 0;       // substep_vjp: 1 = positions held fixed (x-bar passes)
+  TermSet term{};                // terminator shapes (the params' box, or wcg_set_terminators)
   int stale_patch = -1;          // failure-path test: a patch whose waits cannot succeed
   std::vector<int> pl_order_h;
 

@@ -185,17 +185,17 @@ __global__ void k_merge_gather(R* __restrict__ P, long long pcap, long long np,
 }
 
 // TwoDScene::terminateParticles (TwoDScene.cpp:1756-1771): a liquid particle
-// where the terminator box's phi (the running minimum of computePhiVel over
-// the terminator group) is negative loses its fluid volume; every particle
+// where the terminator shapes' phi (the running minimum of computePhiVel over
+// the terminator groups) is negative loses its fluid volume; every particle
 // without volume (below 1e-20, removeEmptyParticles) is flagged for removal
 template <typename R>
 __global__ void k_terminate(R* __restrict__ P, long long pcap, long long np,
-                            const int* __restrict__ pid, Walls term, double three_bs,
+                            const int* __restrict__ pid, const TermSet term, double three_bs,
                             int* __restrict__ alive_slot, int* __restrict__ alive_pid) {
   const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= np) return;
-  if (wall_phi(term, (double)P[PX * pcap + s], (double)P[(PX + 1) * pcap + s],
-               (double)P[(PX + 2) * pcap + s], three_bs) < 0.0)
+  if (term.n > 0 && term_phi(term, (double)P[PX * pcap + s], (double)P[(PX + 1) * pcap + s],
+                             (double)P[(PX + 2) * pcap + s], three_bs) < 0.0)
     P[PV * pcap + s] = R(0);
   const int al = P[PV * pcap + s] < R(1e-20) ? 0 : 1;
   alive_slot[s] = al;

@@ -2606,12 +2606,8 @@ static cudaError_t terminate_liquid_t(Context& c, long long* removed) {
   WCG_TRY(c.corr_list.ensure((size_t)n * sizeof(int)));
   const long long scan_tiles = (n + kScanTile - 1) / kScanTile + 1;
   WCG_TRY(ensure_scratch(c, (size_t)scan_tiles * sizeof(long long) + 64));
-  Walls t;
-  t.cx = c.prm.term_center[0]; t.cy = c.prm.term_center[1]; t.cz = c.prm.term_center[2];
-  t.ex = c.prm.term_half[0]; t.ey = c.prm.term_half[1]; t.ez = c.prm.term_half[2];
-  t.radius = c.prm.term_radius;
-  t.sign = c.prm.term_inside ? -1.0 : 1.0;
-  t.enabled = c.prm.terminator;
+  TermSet t = c.term;
+  if (!c.prm.terminator) t.n = 0;
   ++c.launches, k_terminate<R><<<nblk(n, 256), 256, 0, c.stream>>>(
       c.pbuf[c.cur].as<R>(), cap, n, c.pid[c.cur].as<int>(), t, 3.0 * 4.0 * c.prm.dx, iw,
       iw + cap);

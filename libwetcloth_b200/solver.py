@@ -250,6 +250,23 @@ class FluidScene:
         """The call of the correction stream the next sub-step takes."""
         return int(self.L.wcg_correction_count(self.h))
 
+    def set_terminators(self, shapes):
+        """Terminator shapes: a list of dicts with keys type ("box", "sphere",
+        "capsule", "cylinder"), inside (bool), center (3), rot (w, x, y, z;
+        identity by default) and param (up to 4 values, as
+        DistanceFieldObject's parameter).  An empty list removes them."""
+        kinds = {"box": _capi.WCG_SHAPE_BOX, "sphere": _capi.WCG_SHAPE_SPHERE,
+                 "capsule": _capi.WCG_SHAPE_CAPSULE, "cylinder": _capi.WCG_SHAPE_CYLINDER}
+        arr = (_capi.WcgShape * max(1, len(shapes)))()
+        for k, sh in enumerate(shapes):
+            arr[k].type = kinds[sh["type"]]
+            arr[k].inside = 1 if sh.get("inside", False) else 0
+            arr[k].center[:] = [float(v) for v in sh["center"]]
+            arr[k].rot[:] = [float(v) for v in sh.get("rot", (1.0, 0.0, 0.0, 0.0))]
+            par = [float(v) for v in sh["param"]] + [0.0] * 4
+            arr[k].param[:] = par[:4]
+        check(self.L.wcg_set_terminators(self.h, len(shapes), arr))
+
     def set_correction_count(self, k):
         """Call count of the correction stream (the next sub-step corrects the
         subset of call k)."""

@@ -151,6 +151,7 @@ class GpuWetClothCore : public WetClothCore {
     p.split_seed = opt_.seed ^ 0x73706c74ull;
     fillGravityAndBox(s, &p);
     check(wcg_create(&p, &ctx_));
+    setTerminators(s);
     const long long n = s.getNumFluidParticles();
     std::vector<double> x(3 * n), v(3 * n), C(9 * n), m(n), vol(n), r(n);
     const MatrixXs& fB = wcgbind::fluidB(s);
@@ -166,6 +167,44 @@ class GpuWetClothCore : public WetClothCore {
     }
     check(wcg_upload_liquid(ctx_, n, x.data(), v.data(), C.data(), m.data(), vol.data(),
                             r.data()));
+  }
+
+  // the scene's terminator objects (usage DFU_TERMINATOR, analytic shapes,
+  // fixed), which terminateParticles removes the liquid with
+  // (TwoDScene.cpp:1756-1771); the groups they sit in are unions
+  void setTerminators(const TwoDScene& s) {
+    std::vector<wcg_shape> shapes;
+    for (const std::shared_ptr<DistanceField>& df : s.getDistanceFields()) {
+      if (df->usage != DFU_TERMINATOR) continue;
+      const auto obj = std::dynamic_pointer_cast<DistanceFieldObject>(df);
+      int type = -1;
+      if (obj) {
+        switch (obj->type) {
+          case DFT_BOX: type = WCG_SHAPE_BOX; break;
+          case DFT_SPHERE: type = WCG_SHAPE_SPHERE; break;
+          case DFT_CAPSULE: type = WCG_SHAPE_CAPSULE; break;
+          case DFT_CYLINDER: type = WCG_SHAPE_CYLINDER; break;
+          default: break;
+        }
+      }
+      if (type < 0 || obj->V.squaredNorm() != 0.0 || obj->omega.squaredNorm() != 0.0)
+        throw std::runtime_error("GpuWetClothCore: terminators other than fixed boxes, "
+                                 "spheres, capsules and cylinders are not bound here");
+      wcg_shape sh;
+      sh.type = type;
+      sh.inside = obj->sign < 0.0 ? 1 : 0;
+      for (int a = 0; a < 3; ++a) sh.center[a] = obj->center(a);
+      sh.rot[0] = obj->rot.w();
+      sh.rot[1] = obj->rot.x();
+      sh.rot[2] = obj->rot.y();
+      sh.rot[3] = obj->rot.z();
+      for (int a = 0; a < 4; ++a) sh.param[a] = a < obj->parameter.size() ? obj->parameter(a) : 0.0;
+      shapes.push_back(sh);
+    }
+    if (shapes.size() > WCG_MAX_TERMINATOR_SHAPES)
+      throw std::runtime_error("GpuWetClothCore: more terminators than the library takes");
+    if (!shapes.empty())
+      check(wcg_set_terminators(ctx_, (int)shapes.size(), shapes.data()));
   }
 
   // gravity: the sum of the scene's SimpleGravityForce terms (each adds

@@ -57,6 +57,9 @@ def lib():
         L.wco_terminate_liquid.restype = ctypes.c_int
         L.wco_set_terminator.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, _D, ctypes.c_double,
                                          ctypes.c_int]
+        L.wco_set_terminators.argtypes = [ctypes.c_void_p, ctypes.c_int,
+                                          ctypes.POINTER(ctypes.c_int),
+                                          ctypes.POINTER(ctypes.c_int), _D, _D, _D]
         L.wco_correction_selector.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int]
         L.wco_correction_selector.restype = ctypes.c_int
         L.wco_step.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
@@ -179,6 +182,23 @@ class OracleScene:
         """splitLiquidParticles with the rotations of key; returns the
         particles added."""
         return self.L.wco_split_liquid(self.h, int(key))
+
+    def set_terminators(self, shapes):
+        """Terminator shapes (dicts: type, inside, center, rot (w, x, y, z),
+        param); an empty list removes them."""
+        kinds = {"box": 0, "sphere": 1, "capsule": 2, "cylinder": 3}
+        n = len(shapes)
+        ty = np.array([kinds[s["type"]] for s in shapes] or [0], dtype=np.int32)
+        ins = np.array([1 if s.get("inside") else 0 for s in shapes] or [0], dtype=np.int32)
+        c = np.array([s["center"] for s in shapes] or [[0, 0, 0]], dtype=np.float64)
+        q = np.array([s.get("rot", (1, 0, 0, 0)) for s in shapes] or [[1, 0, 0, 0]],
+                     dtype=np.float64)
+        par = np.array([(list(s["param"]) + [0.0] * 4)[:4] for s in shapes] or [[0] * 4],
+                       dtype=np.float64)
+        self._keep_term = (ty, ins, c, q, par)
+        ip = ctypes.POINTER(ctypes.c_int)
+        self.L.wco_set_terminators(self.h, n, ty.ctypes.data_as(ip), ins.ctypes.data_as(ip),
+                                   _dp(c), _dp(q), _dp(par))
 
     def terminate(self):
         """terminateParticles with the scene's terminator box; returns the

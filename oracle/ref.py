@@ -71,6 +71,8 @@ def _lib(omp: bool):
         L.wcref_num_particles.argtypes = [ctypes.c_void_p]
         L.wcref_num_particles.restype = ctypes.c_int
         L.wcref_set_terminator.argtypes = [ctypes.c_void_p, _D, _D, ctypes.c_double, ctypes.c_int]
+        L.wcref_add_terminator.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _D, _D,
+                                           ctypes.c_double, _D, ctypes.c_int, _D]
         L.wcref_terminate.argtypes = [ctypes.c_void_p]
         L.wcref_terminate.restype = ctypes.c_int
         _libs[omp] = L
@@ -166,6 +168,24 @@ class RefScene:
         the particles removed (draws in "merge_selector", "merge_perm")."""
         return self.L.wcref_merge(self.h, seed, step)
 
+    def add_terminators(self, shapes):
+        """Terminator DistanceFieldObjects, each a dict: type ("box",
+        "sphere", "capsule", "cylinder"), inside, center, axis, angle, param
+        (4), group (>= 1).  Returns the shapes with the rotation quaternion
+        the reference built ("rot": w, x, y, z)."""
+        kinds = {"box": 0, "sphere": 1, "capsule": 2, "cylinder": 3}
+        out = []
+        for sh in shapes:
+            rot = np.zeros(4)
+            arr = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+            c, ax, par = arr(sh["center"]), arr(sh.get("axis", (0.0, 1.0, 0.0))), arr(sh["param"])
+            self.L.wcref_add_terminator(self.h, kinds[sh["type"]], 1 if sh.get("inside") else 0,
+                                        c.ctypes.data_as(_D), ax.ctypes.data_as(_D),
+                                        float(sh.get("angle", 0.0)), par.ctypes.data_as(_D),
+                                        int(sh.get("group", 1)), rot.ctypes.data_as(_D))
+            out.append(dict(sh, rot=tuple(rot)))
+        return out
+
     def terminate(self) -> int:
         """terminateParticles; returns the particles removed."""
         return self.L.wcref_terminate(self.h)
@@ -245,12 +265,14 @@ def binding_available() -> bool:
     return os.path.exists(os.path.join(HERE, "_ref", "libwcbinding.so"))
 
 
-def binding_step_both(scene, steps, dt, solver, precision):
+def binding_step_both(scene, steps, dt, solver, precision, terminators=()):
     """Steps two reference scenes built from `scene`: one with the reference's
     WetClothCore::stepSystem, one with the compiled GpuWetClothCore binding
     (oracle/binding/GpuWetClothCore.h) passing the scene's criterion and
     iteration limit.  Returns ((x, v, C) reference, (x, v, C) binding,
-    sub-steps of the binding's last step)."""
+    sub-steps of the binding's last step).  terminators: shapes added to both
+    scenes as add_terminators takes them (the binding reads them from its
+    scene)."""
     B = ctypes.CDLL(os.path.join(HERE, "_ref", "libwcbinding.so"))
     B.wcbind_step_both.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                    ctypes.c_double, ctypes.c_double, ctypes.c_int,
@@ -260,6 +282,9 @@ def binding_step_both(scene, steps, dt, solver, precision):
     B.wcbind_step_both.restype = ctypes.c_int
     ra = RefScene(scene, mic=False)
     rb = RefScene(scene, mic=False)
+    if terminators:
+        ra.add_terminators(terminators)
+        rb.add_terminators(terminators)
     cap = 4 * scene.x.shape[0] + 16
     oa = np.zeros(15 * cap)
     ob = np.zeros(15 * cap)

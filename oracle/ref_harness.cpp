@@ -795,6 +795,43 @@ void wcref_set_terminator(void* hp, const double* c, const double* half, double 
   h->grid_built = true;
 }
 
+// One terminator DistanceFieldObject of any of the four analytic types
+// (0 box, 1 sphere, 2 capsule, 3 cylinder; DistanceFields.cpp:477-520), built
+// as the scene parser builds it from its rotation axis and angle, in
+// distance-field group `group` (>= 1; groups are unions).  rot_out receives
+// the rotation quaternion the object holds (w, x, y, z).
+void wcref_add_terminator(void* hp, int type, int inside, const double* c, const double* axis,
+                          double angle, const double* par4, int group, double* rot_out) {
+  Harness* h = (Harness*)hp;
+  TwoDScene& s = *h->scene;
+  VectorXs par(4);
+  par << par4[0], par4[1], par4[2], par4[3];
+  static const DISTANCE_FIELD_TYPE types[4] = {DFT_BOX, DFT_SPHERE, DFT_CAPSULE, DFT_CYLINDER};
+  std::vector<DF_SOURCE_DURATION> dur;
+  auto term = std::make_shared<DistanceFieldObject>(
+      Vector3s(c[0], c[1], c[2]), par, types[type], DFU_TERMINATOR, inside != 0,
+      Vector3s(axis[0], axis[1], axis[2]), angle, group, 0, false, dur);
+  rot_out[0] = term->rot.w();
+  rot_out[1] = term->rot.x();
+  rot_out[2] = term->rot.y();
+  rot_out[3] = term->rot.z();
+  s.m_distance_fields.push_back(term);
+  int ngroups = 1;
+  for (auto& df : s.m_distance_fields) {
+    df->parent.reset();
+    ngroups = std::max(ngroups, df->group + 1);
+  }
+  s.resizeGroups(ngroups);
+  s.initGroupPos();
+  if (!h->grid_built) {
+    s.updateParticleBoundingBox();
+    s.rebucketizeParticles();
+    s.resampleNodes();
+    h->grid_built = true;
+  }
+  h->term_on = true;
+}
+
 // TwoDScene::terminateParticles: liquid particles inside the terminator's
 // negative region lose their volume and removeEmptyParticles drops them.
 // Returns the particles removed.

@@ -43,6 +43,11 @@ typedef struct {
    * its own): centre, half extents, radius, sign (-1: inside=true) */
   int term_on;
   double tc[3], th[3], tr, tsign;
+  /* terminator shapes (wco_set_terminators): when nshape > 0 they replace
+   * the box above */
+  int nshape;
+  int stype[16];
+  double ssign[16], sc[16][3], sq[16][4], spar[16][4];
 } Params;
 
 typedef struct {
@@ -276,7 +281,78 @@ static double wall_phi(const Scene* s, double px, double py, double pz) {
  * its own group, whose DFT_UNION operator votes the terminator usage
  * (DistanceFieldOperator::vote_usage, DistanceFields.cpp:922-938), read by
  * computePhiVel through the terminator selector (TwoDScene.cpp:1757-1759). */
+/* Eigen's quaternion product (w, x, y, z), Quaternion.h quat_product */
+static void quat_mul(const double a[4], const double b[4], double o[4]) {
+  o[0] = a[0] * b[0] - a[1] * b[1] - a[2] * b[2] - a[3] * b[3];
+  o[1] = a[0] * b[1] + a[1] * b[0] + a[2] * b[3] - a[3] * b[2];
+  o[2] = a[0] * b[2] + a[2] * b[0] + a[3] * b[1] - a[1] * b[3];
+  o[3] = a[0] * b[3] + a[3] * b[0] + a[1] * b[2] - a[2] * b[1];
+}
+
+/* DistanceFieldObject::compute_phi (DistanceFields.cpp:601-660) of shape k,
+ * with the SDFs of DistanceFields.cpp:32-114; the frame change is
+ * conj(q) (0, p - c) conj(q)^-1 + c */
+static double shape_phi(const Scene* s, int k, const double p[3]) {
+  const double* c = s->p.sc[k];
+  const double* par = s->p.spar[k];
+  const int type = s->p.stype[k];
+  double phi;
+  if (type == 1) {
+    const double d0 = p[0] - c[0], d1 = p[1] - c[1], d2 = p[2] - c[2];
+    phi = sqrt(d0 * d0 + d1 * d1 + d2 * d2) - par[0];
+  } else {
+    const double* q = s->p.sq[k];
+    const double iq[4] = {q[0], -q[1], -q[2], -q[3]};
+    const double p0[4] = {0.0, p[0] - c[0], p[1] - c[1], p[2] - c[2]};
+    const double n2 = (iq[1] * iq[1] + iq[2] * iq[2]) + (iq[3] * iq[3] + iq[0] * iq[0]);
+    const double inv[4] = {iq[0] / n2, -iq[1] / n2, -iq[2] / n2, -iq[3] / n2};
+    double a[4], b[4], r[3];
+    quat_mul(iq, p0, a);
+    quat_mul(a, inv, b);
+    for (int j = 0; j < 3; ++j) r[j] = b[j + 1] + c[j];
+    if (type == 0) { /* box_phi */
+      double d[3], da[3];
+      for (int j = 0; j < 3; ++j) {
+        d[j] = fabs(r[j] - c[j]) - par[j];
+        da[j] = d[j] > 0.0 ? d[j] : 0.0;
+      }
+      double m = d[0] > d[1] ? d[0] : d[1];
+      m = m > d[2] ? m : d[2];
+      m = m < 0.0 ? m : 0.0;
+      phi = m + sqrt(da[0] * da[0] + da[1] * da[1] + da[2] * da[2]) - par[3];
+    } else if (type == 2) { /* capsule_phi, axis x */
+      const double hl = par[1];
+      const double pa[3] = {r[0] - (c[0] - hl), r[1] - c[1], r[2] - c[2]};
+      const double ba0 = 2.0 * hl;
+      const double dot = pa[0] * ba0 + pa[1] * 0.0 + pa[2] * 0.0;
+      double h = dot / (4.0 * hl * hl);
+      h = h < 0.0 ? 0.0 : (h > 1.0 ? 1.0 : h);
+      const double e0 = pa[0] - ba0 * h, e1 = pa[1] - 0.0 * h, e2 = pa[2] - 0.0 * h;
+      phi = sqrt(e0 * e0 + e1 * e1 + e2 * e2) - par[0];
+    } else { /* cylinder_phi, axis y */
+      const double q0 = r[0] - c[0], q1 = r[1] - c[1], q2 = r[2] - c[2];
+      const double d0 = sqrt(q0 * q0 + q2 * q2) - par[0] + par[1];
+      const double d1 = fabs(q1) - par[2];
+      double m = d0 > d1 ? d0 : d1;
+      m = m < 0.0 ? m : 0.0;
+      const double e0 = d0 > 0.0 ? d0 : 0.0, e1 = d1 > 0.0 ? d1 : 0.0;
+      phi = m + sqrt(e0 * e0 + e1 * e1) - par[1];
+    }
+  }
+  return s->p.ssign[k] * phi;
+}
+
 static double term_phi(const Scene* s, double px, double py, double pz) {
+  if (s->p.nshape > 0) {
+    const double p[3] = {px, py, pz};
+    double u = 1e20;
+    for (int k = 0; k < s->p.nshape; ++k) {
+      const double f = shape_phi(s, k, p);
+      if (f < u) u = f;
+    }
+    const double r = 3.0 * s->bs;
+    return u < r ? u : r;
+  }
   const double p[3] = {px, py, pz};
   double d[3], da[3];
   for (int a = 0; a < 3; ++a) {
@@ -2233,6 +2309,24 @@ void wco_set_terminator(Scene* s, int on, const double* c, const double* h, doub
   }
   s->p.tr = r;
   s->p.tsign = inside ? -1.0 : 1.0;
+}
+
+/* terminator shapes: type (0 box, 1 sphere, 2 capsule, 3 cylinder), inside,
+ * centre (3 each), rotation quaternion w x y z (4 each), parameters (4 each);
+ * n = 0 removes them */
+void wco_set_terminators(Scene* s, int n, const int* type, const int* inside,
+                         const double* c, const double* q, const double* par) {
+  s->p.nshape = n < 0 ? 0 : (n > 16 ? 16 : n);
+  for (int k = 0; k < s->p.nshape; ++k) {
+    s->p.stype[k] = type[k];
+    s->p.ssign[k] = inside[k] ? -1.0 : 1.0;
+    for (int j = 0; j < 3; ++j) s->p.sc[k][j] = c[3 * k + j];
+    for (int j = 0; j < 4; ++j) {
+      s->p.sq[k][j] = q[4 * k + j];
+      s->p.spar[k][j] = par[4 * k + j];
+    }
+  }
+  s->p.term_on = s->p.nshape > 0;
 }
 
 /* split before each sub-step with the seeded keys */

@@ -57,3 +57,18 @@ def assert_pointwise(gpu, ref, rtol, name, floor_rel):
                            f"|ref| = {a[keep][k]:.3e} (floor {floor_rel:.0e} x max {a.max():.3e}, "
                            f"{int(keep.sum())} entries checked)")
     return worst
+
+
+# Rotated terminator objects of the four analytic types in three distance-field
+# groups, for the terminator tests (scenes in the unit box, liquid below y = 0.5).
+TERMINATOR_SHAPES = [
+    {"type": "sphere", "inside": False, "center": (0.5, 0.3, 0.5), "param": (0.12, 0, 0, 0),
+     "group": 1},
+    {"type": "capsule", "inside": False, "center": (0.3, 0.2, 0.6), "axis": (0.0, 0.0, 1.0),
+     "angle": 0.7, "param": (0.06, 0.15, 0, 0), "group": 1},
+    {"type": "cylinder", "inside": False, "center": (0.7, 0.25, 0.3), "axis": (1.0, 0.0, 0.0),
+     "angle": 0.4, "param": (0.1, 0.02, 0.08, 0), "group": 2},
+    {"type": "box", "inside": True, "center": (0.5, 0.5, 0.5), "axis": (0.0, 1.0, 0.0),
+     "angle": 0.3, "param": (0.45, 0.45, 0.45, 0.01), "group": 3},
+]
+

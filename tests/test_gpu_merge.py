@@ -16,6 +16,7 @@ from libwetcloth_b200 import _capi, scenes
 from libwetcloth_b200.solver import FluidScene
 from oracle import oracle as oo
 from oracle import ref as oref
+from tests.parity import TERMINATOR_SHAPES
 
 pytestmark = pytest.mark.gpu
 DT = 1e-3
@@ -265,6 +266,59 @@ def test_terminator_steps(prec, wcg):
         if x.shape[0] == ox.shape[0]:
             _close(v, o.get("g2p_v"), 1e-5, "g2p_v")
             _close(x, ox, 1e-6, "adv_x")
+    g.close()
+
+
+def _terminator_shapes():
+    """Rotated terminator objects of all four analytic types (the set the
+    oracle is pinned to the reference with), rotations from their axes and
+    angles."""
+    out = []
+    for sh in TERMINATOR_SHAPES:
+        ax = np.array(sh.get("axis", (0.0, 1.0, 0.0)), dtype=np.float64)
+        ang = float(sh.get("angle", 0.0))
+        out.append(dict(sh, rot=(np.cos(0.5 * ang), *(np.sin(0.5 * ang) * ax))))
+    return out
+
+
+@pytest.mark.parametrize("prec", [_capi.WCG_FP64, _capi.WCG_FP32_REFINE])
+def test_terminator_shapes(prec, wcg):
+    """wcg_set_terminators with a rotated sphere, capsule, cylinder and
+    inside box: a call on its own removes the same particles as the oracle
+    with the survivors in the same order (FP64 bit-exact; FP32 within two
+    particles, whose rounded positions may fall on the other side of a
+    surface), then three steps with the terminator first in each sub-step
+    agree with the oracle's (FP64 step tolerances); clearing the shapes
+    stops the removals."""
+    sc = scenes.half_box(16, 2, 7, amplitude=1.0, sigma_cells=1.5)
+    shapes = _terminator_shapes()
+    o = oo.OracleScene(sc)
+    o.set_terminators(shapes)
+    g = FluidScene(sc, precision=prec)
+    g.set_terminators(shapes)
+    rem = g.terminate_liquid_particles()
+    orem = o.terminate()
+    assert orem > 0
+    if prec == _capi.WCG_FP64:
+        assert rem == orem
+        x, v, _ = g.download()
+        assert np.array_equal(x.reshape(-1), o.get("term_x").reshape(-1))
+        assert np.array_equal(v.reshape(-1), o.get("term_v").reshape(-1))
+        removed = 0
+        for _ in range(3):
+            o.step(DT, snapshot=True)
+            g.step(DT)
+            removed += int(o.get("terminate_removed")[0])
+        x, v, C = g.download()
+        assert x.shape[0] == o.get("adv_x").size // 3
+        _close(v, o.get("g2p_v"), 1e-10, "g2p_v")
+        _close(x, o.get("adv_x"), 1e-12, "adv_x")
+    else:
+        assert abs(rem - orem) <= 2
+    g.set_terminators([])
+    n = g.num_particles
+    g.step(DT)
+    assert g.num_particles == n
     g.close()
 
 

@@ -6,6 +6,7 @@ import pytest
 from libwetcloth_b200 import scenes
 from oracle import oracle as oo
 from oracle import ref as oref
+from tests.parity import TERMINATOR_SHAPES
 
 pytestmark = pytest.mark.skipif(not (oref.available() and oo.available()),
                                 reason="oracle/_ref or the oracle not built")
@@ -411,6 +412,37 @@ def test_terminate_particles(inside):
         assert a.shape == b.shape, k
         assert np.abs(a - b).max() <= 1e-10 * max(np.abs(a).max(), 1.0), k
     assert r.terminate() == 0 and o.terminate() == 0
+
+
+
+
+def test_terminate_particles_shapes():
+    """terminateParticles with rotated terminator objects of all four
+    analytic types in three distance-field groups (a sphere and a capsule
+    removing what enters them, a cylinder, and a rotated box removing what
+    leaves it): the restatement takes the reference's own rotation
+    quaternions and removes the same particles, with the survivors in the
+    same slots, in a step and in a call of its own after it."""
+    sc = _scene("curl16")
+    r = oref.RefScene(sc, mic=True)
+    shapes = r.add_terminators(TERMINATOR_SHAPES)
+    o = oo.OracleScene(sc)
+    o.set_terminators(shapes)
+    r.step(DT, snapshot=True)
+    o.step(DT, snapshot=True)
+    removed = int(r.get("terminate_removed")[0])
+    assert 0 < removed < sc.x.shape[0] // 2
+    assert int(o.get("terminate_removed")[0]) == removed
+    for k in ("adv_x", "adv_v", "g2p_C"):
+        a, b = r.get(k), o.get(k)
+        assert a.shape == b.shape, k
+        assert np.abs(a - b).max() <= 1e-10 * max(np.abs(a).max(), 1.0), k
+    n = r.terminate()
+    assert o.terminate() == n
+    for k in ("term_x", "term_v", "term_C"):
+        a, b = r.get(k), o.get(k)
+        assert a.shape == b.shape, k
+        assert np.abs(a - b).max() <= 1e-10 * max(np.abs(a).max(), 1.0), k
 
 
 def test_zero_volume_particles_removed_every_substep():
