@@ -308,6 +308,13 @@ int wcg_create(const wcg_params* params, wcg_ctx** out) {
     const int k = atoi(v);
     ctx->c.sweep_cluster = (k == 2 || k == 4 || k == 8) ? k : 1;
   }
+  // and along a: 2-D clusters of CC x CA CTAs (CA 4 or 8 with CC 1, 2 or 4;
+  // CA 8 with CC 1 or 2), a-face neighbours through shared memory as well
+  if (const char* v = getenv("WCG_SWEEP_CLUSTER_A")) {
+    const int k = atoi(v), cc = ctx->c.sweep_cluster;
+    const bool ok = (k == 4 && cc <= 4) || (k == 8 && cc <= 2);
+    ctx->c.sweep_cluster_a = ok ? k : 1;
+  }
   // the params' terminator box as the one terminator shape (identity rotation)
   if (p.terminator) {
     wcg::TermShape& t = ctx->c.term.s[0];

@@ -186,6 +186,19 @@ template <typename R>
 __host__ __device__ constexpr size_t sweep_cedge_bytes(int mode, int Ls) {
   return (size_t)Ls * 16 * (mode == 0 ? 2 : 1) * (sizeof(R) / 4) * 8;
 }
+// dynamic shared memory of a cluster sweep: the ring, then the edge words of
+// the clustered faces
+template <typename R>
+__host__ __device__ constexpr size_t sweep_cluster_smem(int mode, bool upd, int Ls, int cc,
+                                                        int ca) {
+  return sweep_cedge_off<R>(mode, upd) + (cc > 1 ? sweep_cedge_bytes<R>(mode, Ls) : 0) +
+         (ca > 1 ? sweep_cedge_bytes<R>(mode, Ls) : 0);
+}
+// the a-face words of a 2-D cluster, after the c-face ones (when present)
+template <typename R>
+__host__ __device__ constexpr size_t sweep_aedge_off(int mode, bool upd, int Ls, bool cfaces) {
+  return sweep_cedge_off<R>(mode, upd) + (cfaces ? sweep_cedge_bytes<R>(mode, Ls) : 0);
+}
 
 // Words of the edge buffer: entry (producer patch, side, s, k), EW words each.
 // side 0: the a-face (k = cl), side 1: the c-face (k = al).
@@ -258,9 +271,14 @@ struct PencilSweepArgs {
 // cluster started earlier.  The cluster syncs after the edge buffers are
 // cleared and before any CTA exits, so no CTA writes into a peer that has not
 // started or has already left.
-template <typename R, int MODE, bool UPD, int CL>
+//
+// CA > 1 as well: clusters of CC x CA CTAs, a tile of CC c-patches by CA
+// a-patches (rank = ra + CA rc); a-face neighbours inside the tile exchange
+// through shared memory the same way (their words after the c-face ones).
+template <typename R, int MODE, bool UPD, int CC, int CA>
 __global__ void __launch_bounds__(kPatchLines, 1)
     k_pencil_sweep(const PencilSweepArgs<R> A) {
+  constexpr int CL = CC * CA;
   constexpr bool BWD = MODE == kBackward;
   constexpr int PW = MODE == kFactor ? 2 : 1;  // values sent across an edge
   constexpr int TW = TagWords<R>::W;
@@ -290,15 +308,21 @@ __global__ void __launch_bounds__(kPatchLines, 1)
   // any cross-CTA access
   if (*(const int*)(A.sc + S_DONE)) return;
   for (int i = tid; i < 2 * NW * kPatch * PW; i += kPatchLines) (&xc[0][0][0][0])[i] = R(0);
-  u64* const cedge = CL > 1 ? reinterpret_cast<u64*>(dsm + sweep_cedge_off<R>(MODE, UPD)) : nullptr;
-  if (CL > 1)
+  u64* const cedge = CC > 1 ? reinterpret_cast<u64*>(dsm + sweep_cedge_off<R>(MODE, UPD)) : nullptr;
+  u64* const aedge =
+      CA > 1 ? reinterpret_cast<u64*>(dsm + sweep_aedge_off<R>(MODE, UPD, G.Ls, CC > 1)) : nullptr;
+  if (CC > 1)
     for (int i = tid; i < G.Ls * kPatch * EW; i += kPatchLines) cedge[i] = 0ull;
+  if (CA > 1)
+    for (int i = tid; i < G.Ls * kPatch * EW; i += kPatchLines) aedge[i] = 0ull;
   if (CL > 1)
     cluster_sync();
   else
     __syncthreads();
   const int tk = CL > 1 ? (int)ld_cluster_u32(cluster_map(smem_u32(&s_ticket), 0)) : s_ticket;
-  const int nunits = CL > 1 ? G.nPA * ((G.nPC + CL - 1) / CL) : (int)G.npatch;
+  const int nTA = (G.nPA + CA - 1) / CA;
+  const int nunits = CL > 1 ? nTA * ((G.nPC + CC - 1) / CC) : (int)G.npatch;
+  const int ra = crank % CA, rc = crank / CA;
   bool run = true;
   if (tk < 0 || tk >= nunits) {
     if (tid == 0) record_error(A.err, kErrIndex);
@@ -307,9 +331,9 @@ __global__ void __launch_bounds__(kPatchLines, 1)
   int p = 0, PAi = 0, PCi = 0;
   if (run) {
     const int unit = BWD ? A.order[nunits - 1 - tk] : A.order[tk];
-    PAi = unit % G.nPA;
-    PCi = CL > 1 ? (unit / G.nPA) * CL + crank : unit / G.nPA;
-    run = PCi < G.nPC;  // the last cluster column may reach past the box
+    PAi = CL > 1 ? (unit % nTA) * CA + ra : unit % G.nPA;
+    PCi = CL > 1 ? (unit / nTA) * CC + rc : unit / G.nPA;
+    run = PCi < G.nPC && PAi < G.nPA;  // the last tiles may reach past the box
     p = PCi * G.nPA + PAi;
   }
   if (run) {
@@ -333,12 +357,18 @@ __global__ void __launch_bounds__(kPatchLines, 1)
   }
   if (!line) up_a = up_c = -1;
   // c-face neighbours in the same cluster exchange through shared memory
-  const bool c_loc = CL > 1 && up_c >= 0 && (BWD ? (PCi + 1) % CL != 0 : PCi % CL != 0);
-  const bool c_rem = CL > 1 && pub_c && (BWD ? PCi % CL != 0 : (PCi + 1) % CL != 0);
+  const bool c_loc = CC > 1 && up_c >= 0 && (BWD ? rc < CC - 1 : rc > 0);
+  const bool c_rem = CC > 1 && pub_c && (BWD ? rc > 0 : rc < CC - 1);
+  const bool a_loc = CA > 1 && up_a >= 0 && (BWD ? ra < CA - 1 : ra > 0);
+  const bool a_rem = CA > 1 && pub_a && (BWD ? ra > 0 : ra < CA - 1);
   if (c_loc) up_c = -1;
   if (c_rem) pub_c = false;
-  const unsigned cedge_own = CL > 1 ? smem_u32(cedge) : 0u;
-  const unsigned cedge_dst = c_rem ? cluster_map(cedge_own, BWD ? crank - 1 : crank + 1) : 0u;
+  if (a_loc) up_a = -1;
+  if (a_rem) pub_a = false;
+  const unsigned cedge_own = CC > 1 ? smem_u32(cedge) : 0u;
+  const unsigned cedge_dst = c_rem ? cluster_map(cedge_own, BWD ? crank - CA : crank + CA) : 0u;
+  const unsigned aedge_own = CA > 1 ? smem_u32(aedge) : 0u;
+  const unsigned aedge_dst = a_rem ? cluster_map(aedge_own, BWD ? crank - 1 : crank + 1) : 0u;
   const bool a_edge = al == (BWD ? kPatch - 1 : 0);  // no in-warp a source
   const bool c_prod = BWD ? lane < 16 : lane >= 16;  // half read by the next warp
   const int w_src = BWD ? w + 1 : w - 1;
@@ -473,7 +503,26 @@ __global__ void __launch_bounds__(kPatchLines, 1)
 #pragma unroll
         for (int k = 0; k < PW; ++k) in_c[k] = TagWords<R>::unpack(epc[v] + k * TW);
       }
-      if (CL > 1 && live && c_loc) {
+      if (CA > 1 && live && a_loc) {
+        u64 wd[EW];
+        const unsigned a0 = aedge_own + (unsigned)((s * kPatch + cl) * EW) * 8u;
+#pragma unroll
+        for (int k = 0; k < EW; ++k) {
+          wd[k] = ld_own_u64(a0 + 8u * k);
+          long long it = 0;
+          while ((unsigned)(wd[k] >> 32) != ep_want) {
+            if (gave_up || ++it > spin_limit) {
+              if (!gave_up) record_error(A.err, kErrWaitTimeout);
+              gave_up = true;
+              break;
+            }
+            wd[k] = ld_own_u64(a0 + 8u * k);
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < PW; ++k) in_a[k] = TagWords<R>::unpack(wd + k * TW);
+      }
+      if (CC > 1 && live && c_loc) {
         u64 wd[EW];
         const unsigned a0 = cedge_own + (unsigned)((s * kPatch + al) * EW) * 8u;
 #pragma unroll
@@ -569,11 +618,19 @@ __global__ void __launch_bounds__(kPatchLines, 1)
 #pragma unroll
         for (int k = 0; k < EW; ++k) st_relaxed_u64(ec_dst + s * ES + k, wd[k]);
       }
-      if (CL > 1 && live && c_rem) {
+      if (CC > 1 && live && c_rem) {
         u64 wd[EW];
 #pragma unroll
         for (int k = 0; k < PW; ++k) TagWords<R>::pack(out_c[k], ep, wd + k * TW);
         const unsigned a0 = cedge_dst + (unsigned)((s * kPatch + al) * EW) * 8u;
+#pragma unroll
+        for (int k = 0; k < EW; ++k) st_cluster_u64(a0 + 8u * k, wd[k]);
+      }
+      if (CA > 1 && live && a_rem) {
+        u64 wd[EW];
+#pragma unroll
+        for (int k = 0; k < PW; ++k) TagWords<R>::pack(out_a[k], ep, wd + k * TW);
+        const unsigned a0 = aedge_dst + (unsigned)((s * kPatch + cl) * EW) * 8u;
 #pragma unroll
         for (int k = 0; k < EW; ++k) st_cluster_u64(a0 + 8u * k, wd[k]);
       }

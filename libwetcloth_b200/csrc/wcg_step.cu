@@ -76,7 +76,8 @@ void ctx_free(Context& c) {
                     &c.gfield, &c.gvalid, &c.gdof, &c.wave_list, &c.wave_count,
                     &c.tile_flag, &c.tile_active, &c.tile_part, &c.active_list, &c.p2g_halo,
                     &c.rx64, &c.rr64, &c.rb64,
-                    &c.pl, &c.pl64, &c.pl_edge, &c.pl_order, &c.pl_corder, &c.pl_part,
+                    &c.pl, &c.pl64, &c.pl_edge, &c.pl_order, &c.pl_corder, &c.pl_corder2,
+                    &c.pl_part,
                     &c.mg, &c.mg_mask, &c.mg_vec,
                     &c.adj, &c.adjp, &c.adjmask, &c.adjstage, &c.adjvisc, &c.adjxc, &c.adjam,
                     &c.visc, &c.viscflag, &c.dstage, &c.ustage,
@@ -1279,6 +1280,22 @@ static cudaError_t pl_setup(Context& c, const int* lo, const int* hi) {
     WCG_TRY(cudaMemcpyAsync(c.pl_order.p, c.pl_order_h.data(), G.npatch * sizeof(int),
                             cudaMemcpyHostToDevice, c.stream));
   }
+  if (c.sweep_cluster_a > 1) {
+    // tiles of sweep_cluster c-patches by sweep_cluster_a a-patches, in wave order
+    const int CC = c.sweep_cluster, CA = c.sweep_cluster_a;
+    const int nTA = (G.nPA + CA - 1) / CA, nTC = (G.nPC + CC - 1) / CC;
+    std::vector<int> co;
+    co.reserve((size_t)nTA * nTC);
+    for (int w = 0; w <= nTA + nTC - 2; ++w)
+      for (int tc = 0; tc < nTC; ++tc) {
+        const int ta = w - tc;
+        if (ta >= 0 && ta < nTA) co.push_back(tc * nTA + ta);
+      }
+    WCG_TRY(c.pl_corder2.ensure(co.size() * sizeof(int)));
+    WCG_TRY(cudaMemcpyAsync(c.pl_corder2.p, co.data(), co.size() * sizeof(int),
+                            cudaMemcpyHostToDevice, c.stream));
+    WCG_TRY(cudaStreamSynchronize(c.stream));  // co is a host temporary
+  }
   if (c.sweep_cluster > 1) {
     // cluster columns (PAi, PCc) of sweep_cluster c-patches, in wave order
     const int CL = c.sweep_cluster;
@@ -1331,30 +1348,36 @@ static PencilSweepArgs<R> pl_args(Context& c) {
 
 // dynamic shared memory a cluster sweep may use (the kernel's static
 // arrays take under 8 KB of the 227 KB per CTA)
-constexpr size_t kSweepSmemMax = 200 * 1024;
+constexpr size_t kSweepSmemMax = 216 * 1024;
 
-template <typename R, int MODE, bool UPD, int CL>
+template <typename R, int MODE, bool UPD, int CC, int CA>
 static cudaError_t pl_sweep_cl(Context& c, PencilSweepArgs<R> a) {
+  constexpr int CL = CC * CA;
   ProfScope prof(c, MODE == kFactor ? P_MICFACTOR : P_MICSWEEP);
   const PencilGeom& G = c.plg;
-  const int nunits = CL > 1 ? G.nPA * ((G.nPC + CL - 1) / CL) : (int)G.npatch;
+  const int nTA = (G.nPA + CA - 1) / CA, nTC = (G.nPC + CC - 1) / CC;
+  const int nunits = CL > 1 ? nTA * nTC : (int)G.npatch;
   a.epoch = (unsigned)(++c.tile_epoch);
   a.ticket_base = c.pl_tickets;
   c.pl_tickets += nunits;
-  const size_t smem = CL > 1 ? sweep_cedge_off<R>(MODE, UPD) + sweep_cedge_bytes<R>(MODE, G.Ls)
+  const size_t smem = CL > 1 ? sweep_cluster_smem<R>(MODE, UPD, G.Ls, CC, CA)
                              : sweep_dyn_smem<R>(MODE, UPD);
   static bool attr_set = false;  // per instantiation, once per process
   if (!attr_set) {
-    WCG_TRY(cudaFuncSetAttribute(k_pencil_sweep<R, MODE, UPD, CL>,
+    WCG_TRY(cudaFuncSetAttribute(k_pencil_sweep<R, MODE, UPD, CC, CA>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(CL > 1 ? kSweepSmemMax : smem)));
+    if (CL > 8)
+      WCG_TRY(cudaFuncSetAttribute(k_pencil_sweep<R, MODE, UPD, CC, CA>,
+                                   cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     attr_set = true;
   }
   if (CL == 1) {
-    ++c.launches, k_pencil_sweep<R, MODE, UPD, 1><<<(unsigned)G.npatch, kPatchLines, smem, c.stream>>>(a);
+    ++c.launches, k_pencil_sweep<R, MODE, UPD, 1, 1><<<(unsigned)G.npatch, kPatchLines, smem,
+                                                       c.stream>>>(a);
     return cudaGetLastError();
   }
-  a.order = c.pl_corder.as<int>();
+  a.order = CA > 1 ? c.pl_corder2.as<int>() : c.pl_corder.as<int>();
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)(nunits * CL));
   cfg.blockDim = dim3(kPatchLines);
@@ -1368,21 +1391,29 @@ static cudaError_t pl_sweep_cl(Context& c, PencilSweepArgs<R> a) {
   cfg.attrs = at;
   cfg.numAttrs = 1;
   ++c.launches;
-  return cudaLaunchKernelEx(&cfg, k_pencil_sweep<R, MODE, UPD, CL>, a);
+  return cudaLaunchKernelEx(&cfg, k_pencil_sweep<R, MODE, UPD, CC, CA>, a);
 }
 
-// The cluster form needs the c-edge buffer of a patch (Ls x 16 tagged
-// entries) in shared memory; longer boxes use the plain form.
+// The cluster forms need the edge buffers of a patch (Ls x 16 tagged entries
+// per clustered face) in shared memory; when they do not fit, a 2-D cluster
+// falls back to its c-clusters and those to the plain form.
 template <typename R, int MODE, bool UPD>
 static cudaError_t pl_sweep(Context& c, PencilSweepArgs<R> a) {
-  const int CL = c.sweep_cluster;
-  if (CL > 1 &&
-      sweep_cedge_off<R>(MODE, UPD) + sweep_cedge_bytes<R>(MODE, c.plg.Ls) <= kSweepSmemMax) {
-    if (CL == 2) return pl_sweep_cl<R, MODE, UPD, 2>(c, a);
-    if (CL == 4) return pl_sweep_cl<R, MODE, UPD, 4>(c, a);
-    if (CL == 8) return pl_sweep_cl<R, MODE, UPD, 8>(c, a);
+  const int CC = c.sweep_cluster, CA = c.sweep_cluster_a;
+  const int Ls = c.plg.Ls;
+  if (CA > 1 && sweep_cluster_smem<R>(MODE, UPD, Ls, CC, CA) <= kSweepSmemMax) {
+    if (CC == 1 && CA == 4) return pl_sweep_cl<R, MODE, UPD, 1, 4>(c, a);
+    if (CC == 1 && CA == 8) return pl_sweep_cl<R, MODE, UPD, 1, 8>(c, a);
+    if (CC == 2 && CA == 4) return pl_sweep_cl<R, MODE, UPD, 2, 4>(c, a);
+    if (CC == 2 && CA == 8) return pl_sweep_cl<R, MODE, UPD, 2, 8>(c, a);
+    if (CC == 4 && CA == 4) return pl_sweep_cl<R, MODE, UPD, 4, 4>(c, a);
   }
-  return pl_sweep_cl<R, MODE, UPD, 1>(c, a);
+  if (CC > 1 && sweep_cluster_smem<R>(MODE, UPD, Ls, CC, 1) <= kSweepSmemMax) {
+    if (CC == 2) return pl_sweep_cl<R, MODE, UPD, 2, 1>(c, a);
+    if (CC == 4) return pl_sweep_cl<R, MODE, UPD, 4, 1>(c, a);
+    if (CC == 8) return pl_sweep_cl<R, MODE, UPD, 8, 1>(c, a);
+  }
+  return pl_sweep_cl<R, MODE, UPD, 1, 1>(c, a);
 }
 
 // PCGSolver<T>::solve (PCGSolver.h:260-308) in the pencil layout on the

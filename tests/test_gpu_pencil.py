@@ -33,7 +33,8 @@ def _scene(kind):
 
 
 def _solve(sc, layout, precision, cluster=1):
-    env = {"WCG_PCG_LAYOUT": layout, "WCG_SWEEP_CLUSTER": str(cluster)}
+    cc, ca = (str(cluster).split("x") + ["1"])[:2] if "x" in str(cluster) else (str(cluster), "1")
+    env = {"WCG_PCG_LAYOUT": layout, "WCG_SWEEP_CLUSTER": cc, "WCG_SWEEP_CLUSTER_A": ca}
     old = {k: os.environ.get(k) for k in env}
     os.environ.update(env)
     try:
@@ -111,16 +112,18 @@ def test_pencil_deterministic_256_patches(precision, wcg):
         assert np.array_equal(p, res[0][0])
 
 
-@pytest.mark.parametrize("cluster", [2, 4, 8])
+@pytest.mark.parametrize("cluster", [2, 4, 8, "1x4", "2x4", "4x4", "1x8", "2x8"])
 @pytest.mark.parametrize("kind,precision", [("curl48", _capi.WCG_FP64),
                                             ("slab64_x", _capi.WCG_FP64),
                                             ("curl96", _capi.WCG_FP64),
                                             ("curl48", _capi.WCG_FP32_REFINE)])
 def test_pencil_cluster_sweeps_bit_identical(kind, precision, cluster, wcg):
-    """Clusters only change how c-face edge values travel (shared memory of
-    the neighbouring CTA instead of a global round trip): the arithmetic is
-    the same, so pressures and iteration counts are bit-identical, also when
-    the patch count along c is not a multiple of the cluster size."""
+    """Clusters only change how edge values travel (shared memory of the
+    neighbouring CTA instead of a global round trip): c-faces with clusters
+    along c ("8"), both faces with 2-D clusters ("CCxCA": CC c-patches by CA
+    a-patches).  The arithmetic is the same, so pressures and iteration
+    counts are bit-identical, also when the patch counts are not multiples
+    of the cluster extents."""
     sc = _scene(kind)
     a, sa = _solve(sc, "pencil", precision, 1)
     b, sb = _solve(sc, "pencil", precision, cluster)
