@@ -251,6 +251,7 @@ struct Context {
   DevBuf pl_corder2;             // 2-D cluster tiles in wave order (sweep_cluster_a > 1)
   int sweep_cluster = 1;         // CTAs per cluster along c in the MIC(0) sweeps
   int sweep_cluster_a = 1;       // ... and along a (2-D clusters: 4 or 8)
+  int pl_cc = 1;                 // the c-extent the current solve uses (<= patches along c)
   int spmv_rows = 1;             // 0: the patch-streamed SpMV instead of the row-parallel one
   DevBuf pl_part;                // per-patch partials (double)
   long long pl_cap = 0;

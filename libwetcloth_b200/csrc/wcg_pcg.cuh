@@ -484,11 +484,13 @@ __global__ void __launch_bounds__(kRedThreads)
 }
 
 // alpha = rho / sum(partials)
-__global__ void k_red_alpha(const double* __restrict__ partial, int n, double* sc) {
-  __shared__ double sm[kRedThreads];
-  if (*(const int*)(sc + S_DONE)) return;
+// The three per-iteration reductions, as block bodies: a kernel of their own
+// (k_red_*) or the last block of the kernel that wrote the partials
+// (last_block).  Partials are summed thread-strided, then by the block tree,
+// so both forms give the same bits.
+__device__ inline void red_alpha_body(const double* partial, int n, double* sc, double* sm) {
   double s = 0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) s += partial[i];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s += __ldcg(partial + i);
   s = block_sum<double>(s, sm);
   if (threadIdx.x == 0) {
     sc[S_SQ] = s;
@@ -496,13 +498,12 @@ __global__ void k_red_alpha(const double* __restrict__ partial, int n, double* s
   }
 }
 
-// res = max(partials); stop (done = 1) when res <= tol, or (done = 2) when
-// the iteration budget is spent (PCGSolver::solve, PCGSolver.h:282-307)
-__global__ void k_red_conv(const double* __restrict__ partial, int n, double* sc) {
-  __shared__ double sm[kRedThreads];
-  if (*(const int*)(sc + S_DONE)) return;
+__device__ inline void red_conv_body(const double* partial, int n, double* sc, double* sm) {
   double m = 0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) m = partial[i] > m ? partial[i] : m;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const double v = __ldcg(partial + i);
+    m = v > m ? v : m;
+  }
   m = block_max<double>(m, sm);
   if (threadIdx.x == 0) {
     sc[S_RES] = m;
@@ -512,13 +513,10 @@ __global__ void k_red_conv(const double* __restrict__ partial, int n, double* sc
   }
 }
 
-// rho_new = sum(partials); beta = rho_new / rho; rho = rho_new.  With init,
-// only rho is set (the first direction is s = z).
-__global__ void k_red_beta(const double* __restrict__ partial, int n, double* sc, int init) {
-  __shared__ double sm[kRedThreads];
-  if (*(const int*)(sc + S_DONE)) return;
+__device__ inline void red_beta_body(const double* partial, int n, double* sc, double* sm,
+                                     int init) {
   double s = 0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) s += partial[i];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s += __ldcg(partial + i);
   s = block_sum<double>(s, sm);
   if (threadIdx.x == 0) {
     if (init) {
@@ -528,6 +526,48 @@ __global__ void k_red_beta(const double* __restrict__ partial, int n, double* sc
     }
     sc[S_RHO] = s;
   }
+}
+
+// True in the block that reaches the counter last (every block calls it
+// once, after writing its partial); that block resets the counter for the
+// next launch.  The fences order the partials before the count and the
+// count before the last block's reads.
+__device__ inline bool last_block(int* ctr, int nblocks) {
+  __shared__ int s_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const int k = atomicAdd(ctr, 1);
+    s_last = k == nblocks - 1 ? 1 : 0;
+    if (s_last) {
+      atomicExch(ctr, 0);
+      __threadfence();
+    }
+  }
+  __syncthreads();
+  return s_last != 0;
+}
+
+__global__ void k_red_alpha(const double* __restrict__ partial, int n, double* sc) {
+  __shared__ double sm[kRedThreads];
+  if (*(const int*)(sc + S_DONE)) return;
+  red_alpha_body(partial, n, sc, sm);
+}
+
+// res = max(partials); stop (done = 1) when res <= tol, or (done = 2) when
+// the iteration budget is spent (PCGSolver::solve, PCGSolver.h:282-307)
+__global__ void k_red_conv(const double* __restrict__ partial, int n, double* sc) {
+  __shared__ double sm[kRedThreads];
+  if (*(const int*)(sc + S_DONE)) return;
+  red_conv_body(partial, n, sc, sm);
+}
+
+// rho_new = sum(partials); beta = rho_new / rho; rho = rho_new.  With init,
+// only rho is set (the first direction is s = z).
+__global__ void k_red_beta(const double* __restrict__ partial, int n, double* sc, int init) {
+  __shared__ double sm[kRedThreads];
+  if (*(const int*)(sc + S_DONE)) return;
+  red_beta_body(partial, n, sc, sm, init);
 }
 
 template <typename R>

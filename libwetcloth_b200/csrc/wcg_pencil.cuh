@@ -244,10 +244,14 @@ struct PencilSweepArgs {
   R* out;       // forward: y; backward: z
   R* r;         // forward (update): r updated in place; backward: r for z.r
   const R* q;   // forward (update)
-  const double* sc;
+  double* sc;            // device scalars (the last CTA of a reducing sweep writes them)
   double* part;  // per-patch partial: forward max|r|, backward z.r
   R omega, min_ratio;
   int* err;
+  int* done_ctr;         // with part: the last CTA reduces the partials (forward with
+                         // update: max|r| and the stop test; backward: z.r and beta)
+  int red_init;          // backward: the first z.r of a solve (beta = 0)
+  int npart;             // partials (patches)
   long long spin_limit;  // polls of an edge word before the wait gives up
   int stale_patch;       // failure-path test: this patch waits for a tag nothing
                          // writes (-1: none)
@@ -682,6 +686,14 @@ __global__ void __launch_bounds__(kPatchLines, 1)
     if (tid == 0) A.part[p] = sm;
   }
   }  // run
+  // every CTA counts, running or not; the last one reduces the partials
+  if (A.done_ctr && A.part && ((MODE == kForward && UPD) || MODE == kBackward) &&
+      last_block(A.done_ctr, (int)gridDim.x)) {
+    if (MODE == kForward)
+      red_conv_body(A.part, A.npart, A.sc, red);
+    else
+      red_beta_body(A.part, A.npart, A.sc, red, A.red_init);
+  }
   if (CL > 1) cluster_sync();
 }
 
@@ -754,8 +766,8 @@ __global__ void __launch_bounds__(kRedThreads, sizeof(R) == 4 ? 8 : 4)
     k_pl_spmv_s(PencilGeom G, const R* __restrict__ AD, const R* __restrict__ AS,
                 const R* __restrict__ AA, const R* __restrict__ AC, const R* __restrict__ z,
                 const R* __restrict__ sold, R* __restrict__ snew, R* __restrict__ q,
-                R* __restrict__ x, const double* __restrict__ sc,
-                double* __restrict__ partial) {
+                R* __restrict__ x, double* __restrict__ sc,
+                double* __restrict__ partial, int* __restrict__ done_ctr) {
   __shared__ double sm[kRedThreads];
   if (*(const int*)(sc + S_DONE)) return;
   const R be = (R)sc[S_BETA];
@@ -784,6 +796,9 @@ __global__ void __launch_bounds__(kRedThreads, sizeof(R) == 4 ? 8 : 4)
   }
   acc = block_sum<double>(acc, sm);
   if (threadIdx.x == 0) partial[blockIdx.x] = acc;
+  // the last block: alpha = rho / s.q (k_red_alpha's body)
+  if (done_ctr && last_block(done_ctr, (int)gridDim.x))
+    red_alpha_body(partial, (int)gridDim.x, sc, sm);
 }
 
 // k_pl_spmv_s's arithmetic, streamed: block (patch p, chunk k) walks rows

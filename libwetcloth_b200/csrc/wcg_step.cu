@@ -1280,9 +1280,12 @@ static cudaError_t pl_setup(Context& c, const int* lo, const int* hi) {
     WCG_TRY(cudaMemcpyAsync(c.pl_order.p, c.pl_order_h.data(), G.npatch * sizeof(int),
                             cudaMemcpyHostToDevice, c.stream));
   }
+  // clusters no longer along c than the box has patches (a power of two)
+  c.pl_cc = c.sweep_cluster;
+  while (c.pl_cc > 1 && c.pl_cc > G.nPC) c.pl_cc >>= 1;
   if (c.sweep_cluster_a > 1) {
-    // tiles of sweep_cluster c-patches by sweep_cluster_a a-patches, in wave order
-    const int CC = c.sweep_cluster, CA = c.sweep_cluster_a;
+    // tiles of pl_cc c-patches by sweep_cluster_a a-patches, in wave order
+    const int CC = c.pl_cc, CA = c.sweep_cluster_a;
     const int nTA = (G.nPA + CA - 1) / CA, nTC = (G.nPC + CC - 1) / CC;
     std::vector<int> co;
     co.reserve((size_t)nTA * nTC);
@@ -1296,9 +1299,9 @@ static cudaError_t pl_setup(Context& c, const int* lo, const int* hi) {
                             cudaMemcpyHostToDevice, c.stream));
     WCG_TRY(cudaStreamSynchronize(c.stream));  // co is a host temporary
   }
-  if (c.sweep_cluster > 1) {
-    // cluster columns (PAi, PCc) of sweep_cluster c-patches, in wave order
-    const int CL = c.sweep_cluster;
+  if (c.pl_cc > 1) {
+    // cluster columns (PAi, PCc) of pl_cc c-patches, in wave order
+    const int CL = c.pl_cc;
     const int nPCc = (G.nPC + CL - 1) / CL;
     std::vector<int> co;
     co.reserve((size_t)G.nPA * nPCc);
@@ -1315,7 +1318,8 @@ static cudaError_t pl_setup(Context& c, const int* lo, const int* hi) {
   // every array starts at zero (rows and lines outside the box stay zero)
   WCG_TRY(cudaMemsetAsync(c.pl.p, 0, (size_t)kNumPlFields * G.len * sizeof(R), c.stream));
   c.pl_tickets = 0;
-  WCG_TRY(cudaMemsetAsync(c.ticket.as<int>() + 1, 0, sizeof(int), c.stream));
+  // the sweep ticket and the done counters of the SpMV and the sweeps
+  WCG_TRY(cudaMemsetAsync(c.ticket.as<int>() + 1, 0, 3 * sizeof(int), c.stream));
   return cudaSuccess;
 }
 
@@ -1399,7 +1403,7 @@ static cudaError_t pl_sweep_cl(Context& c, PencilSweepArgs<R> a) {
 // falls back to its c-clusters and those to the plain form.
 template <typename R, int MODE, bool UPD>
 static cudaError_t pl_sweep(Context& c, PencilSweepArgs<R> a) {
-  const int CC = c.sweep_cluster, CA = c.sweep_cluster_a;
+  const int CC = c.pl_cc, CA = c.sweep_cluster_a;
   const int Ls = c.plg.Ls;
   if (CA > 1 && sweep_cluster_smem<R>(MODE, UPD, Ls, CC, CA) <= kSweepSmemMax) {
     if (CC == 1 && CA == 4) return pl_sweep_cl<R, MODE, UPD, 1, 4>(c, a);
@@ -1450,17 +1454,22 @@ static cudaError_t pl_pcg(Context& c, R* r, R* x, double tol_abs, int maxiters, 
   ba.out = z;
   ba.r = r;
   ba.part = ppart;
+  // the sweeps' last CTAs reduce their partials (z.r and beta; max|r| and the
+  // stop test), in place of separate reduction launches
+  int* const done_ctr = c.ticket.as<int>() + 3;
+  ba.done_ctr = done_ctr;
+  ba.npart = np;
+  ba.red_init = 1;
   WCG_TRY((pl_sweep<R, kBackward, false>(c, ba)));
-  {
-    ProfScope prof(c, P_PCGVEC);
-    ++c.launches, k_red_beta<<<1, kRedThreads, 0, c.stream>>>(ppart, np, sc, 1);
-  }
+  ba.red_init = 0;
   double h[9];
   WCG_TRY(fetch(c, sc + S_RHO, 1, h));
   if (h[0] == 0 || h[0] != h[0]) return cudaSuccess;  // PCGSolver.h:276-279
   fa.r = r;
   fa.q = q;
   fa.part = ppart;
+  fa.done_ctr = done_ctr;
+  fa.npart = np;
   R* sold = s0;
   R* snew = s1;
   const R* AD = pl_field<R>(c, PL_AD);
@@ -1479,25 +1488,17 @@ static cudaError_t pl_pcg(Context& c, R* r, R* x, double tol_abs, int maxiters, 
     for (int b = 0; b < kPcgBatch; ++b) {
       {
         ProfScope prof(c, P_PCGVEC);
-        if (c.spmv_rows)
+        if (c.spmv_rows) {  // its last block forms alpha
           ++c.launches, k_pl_spmv_s<R><<<kPlSpmvBlocks32, kRedThreads, 0, c.stream>>>(
-              G, AD, AS, AA, AC, z, sold, snew, q, x, sc, part);
-        else
+              G, AD, AS, AA, AC, z, sold, snew, q, x, sc, part, c.ticket.as<int>() + 2);
+        } else {
           ++c.launches, k_pl_spmv_stream<R><<<spmv_blocks, kRedThreads, 0, c.stream>>>(
               G, rows_per_chunk, nchunk, AD, AS, AA, AC, z, sold, snew, q, x, sc, part);
-        ++c.launches, k_red_alpha<<<1, kRedThreads, 0, c.stream>>>(
-            part, c.spmv_rows ? kPlSpmvBlocks32 : spmv_blocks, sc);
+          ++c.launches, k_red_alpha<<<1, kRedThreads, 0, c.stream>>>(part, spmv_blocks, sc);
+        }
       }
       WCG_TRY((pl_sweep<R, kForward, true>(c, fa)));
-      {
-        ProfScope prof(c, P_PCGVEC);
-        ++c.launches, k_red_conv<<<1, kRedThreads, 0, c.stream>>>(ppart, np, sc);
-      }
       WCG_TRY((pl_sweep<R, kBackward, false>(c, ba)));
-      {
-        ProfScope prof(c, P_PCGVEC);
-        ++c.launches, k_red_beta<<<1, kRedThreads, 0, c.stream>>>(ppart, np, sc, 0);
-      }
       R* t = sold;
       sold = snew;
       snew = t;
