@@ -49,6 +49,10 @@ def parse():
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the many-scenes measurement (batched vs sequential)")
     ap.add_argument("--batch-scenes", type=int, default=32)
+    ap.add_argument("--batch-full", action="store_true",
+                    help="the many-scenes configuration at its stated size: 256 scenes of "
+                         "32..96^3 and 10k..1M particles, 50 steps, one pass per arm "
+                         "(minutes; not part of the default run)")
     ap.add_argument("--no-cloth", action="store_true",
                     help="skip the liquid-on-cloth measurement (128^3 sphere on a sheet)")
     ap.add_argument("--no-config0", action="store_true",
@@ -389,7 +393,7 @@ def run_ours(args, rank, world, dev):
                                               "pressure solver (AMGPCGSolveSparse restated)")
     if not args.no_config0:
         out["config0"] = run_config0(dev)
-    if not args.no_batch:
+    if not args.no_batch or args.batch_full:
         out["batch"] = run_batch(args)
     if not args.no_cloth:
         out["cloth"] = run_cloth(dev)
@@ -489,24 +493,31 @@ def run_batch(args, steps=3):
     a short run): aggregate particle-steps/s stepped one after another
     against the batch (separate streams, host thread pool, thread count
     autotuned during warm-up).  Device-synchronised wall time around each
-    whole pass."""
+    whole pass (best of three; one pass each with --batch-full, which runs
+    the configuration at its stated size)."""
     import torch
     from libwetcloth_b200 import scenes
     from libwetcloth_b200._capi import WCG_FP32_REFINE
     from libwetcloth_b200.solver import FluidBatch, FluidScene
-    specs = scenes.batch_scenes(args.batch_scenes, 4, (32, 64), (10_000, 200_000))
+    full = getattr(args, "batch_full", False)
+    if full:
+        specs = scenes.batch_scenes(256, 4, (32, 96), (10_000, 1_000_000))
+        steps = 50
+    else:
+        specs = scenes.batch_scenes(args.batch_scenes, 4, (32, 64), (10_000, 200_000))
+    passes = 1 if full else 3
     total_p = sum(sc.x.shape[0] for sc in specs)
 
     def make():
         return [FluidScene(sc, precision=WCG_FP32_REFINE) for sc in specs]
 
     # sequential: one scene after another, each its own steps (best of three
-    # passes: the passes are short, so host jitter would dominate a single one)
+    # passes when they are short, so host jitter does not dominate)
     gs = make()
     for g in gs:
         g.step(DT)
     seq_s = float("inf")
-    for _ in range(3):
+    for _ in range(passes):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for g in gs:
@@ -522,7 +533,7 @@ def run_batch(args, steps=3):
     b.step(DT)  # first-step allocations outside the autotuning trials
     tune = b.autotune(DT, candidates=(1, 2, 4, 8, 16))
     bat_s = float("inf")
-    for _ in range(3):
+    for _ in range(passes):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         b.step(DT, nsteps=steps)
@@ -538,8 +549,8 @@ def run_batch(args, steps=3):
             "batched_particle_steps_per_s": round(total_p * steps / bat_s, 1),
             "speedup": round(seq_s / bat_s, 3), "threads": threads,
             "autotune_ms": {str(k): round(v, 2) for k, v in tune.items()},
-            "note": "wall time, device-synchronised, warm-up excluded, best of 3 passes "
-                    "per arm"}
+            "note": f"wall time, device-synchronised, warm-up excluded, best of {passes} "
+                    "pass(es) per arm"}
 
 
 # ---------------------------------------------------------------------------

@@ -112,7 +112,7 @@ def test_pencil_deterministic_256_patches(precision, wcg):
         assert np.array_equal(p, res[0][0])
 
 
-@pytest.mark.parametrize("cluster", [2, 4, 8, "1x4", "2x4", "4x4", "1x8", "2x8"])
+@pytest.mark.parametrize("cluster", [2, 4, 8, 16, "1x4", "2x4", "4x4", "1x8", "2x8"])
 @pytest.mark.parametrize("kind,precision", [("curl48", _capi.WCG_FP64),
                                             ("slab64_x", _capi.WCG_FP64),
                                             ("curl96", _capi.WCG_FP64),
