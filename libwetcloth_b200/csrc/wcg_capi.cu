@@ -302,14 +302,14 @@ int wcg_create(const wcg_params* params, wcg_ctx** out) {
   // the PCG's SpMV: row-parallel (default) or patch-streamed (performance
   // knob; the dot products' partial sums are grouped differently)
   if (const char* v = getenv("WCG_SPMV")) ctx->c.spmv_rows = !strcmp(v, "stream") ? 0 : 1;
-  // CTAs per thread-block cluster along c in the MIC(0) sweeps (1, 2, 4, 8 or 16;
+  // CTAs per thread-block cluster along c in the MIC(0) sweeps (1, 2, 3, 4, 8, 9 or 16;
   // performance knob, identical results).  Default: 8 in FP32 (the c-face
   // words of 7 of 8 c-hops through shared memory: 0.426 against 0.455 ms per
   // sweep at 256^3), none in FP64 (0.729 against 0.589 ms).
   ctx->c.sweep_cluster = p.precision != 0 ? 8 : 1;
   if (const char* v = getenv("WCG_SWEEP_CLUSTER")) {
     const int k = atoi(v);
-    ctx->c.sweep_cluster = (k == 2 || k == 4 || k == 8 || k == 16) ? k : 1;
+    ctx->c.sweep_cluster = (k == 2 || k == 3 || k == 4 || k == 8 || k == 9 || k == 16) ? k : 1;
   }
   // and along a: 2-D clusters of CC x CA CTAs (CA 4 or 8 with CC 1, 2 or 4;
   // CA 8 with CC 1 or 2), a-face neighbours through shared memory as well

@@ -1417,7 +1417,9 @@ static cudaError_t pl_sweep(Context& c, PencilSweepArgs<R> a) {
   if (CC > 1 && sweep_cluster_smem<R>(MODE, UPD, Ls, CC, 1) <= kSweepSmemMax) {
     if (CC == 2) return pl_sweep_cl<R, MODE, UPD, 2, 1>(c, a);
     if (CC == 4) return pl_sweep_cl<R, MODE, UPD, 4, 1>(c, a);
+    if (CC == 3) return pl_sweep_cl<R, MODE, UPD, 3, 1>(c, a);
     if (CC == 8) return pl_sweep_cl<R, MODE, UPD, 8, 1>(c, a);
+    if (CC == 9) return pl_sweep_cl<R, MODE, UPD, 9, 1>(c, a);
     if (CC == 16) return pl_sweep_cl<R, MODE, UPD, 16, 1>(c, a);
   }
   return pl_sweep_cl<R, MODE, UPD, 1, 1>(c, a);
