@@ -302,11 +302,10 @@ int wcg_create(const wcg_params* params, wcg_ctx** out) {
   // the PCG's SpMV: row-parallel (default) or patch-streamed (performance
   // knob; the dot products' partial sums are grouped differently)
   if (const char* v = getenv("WCG_SPMV")) ctx->c.spmv_rows = !strcmp(v, "stream") ? 0 : 1;
-  // CTAs per thread-block cluster along c in the MIC(0) sweeps (1, 2, 3, 4, 8, 9 or 16;
-  // performance knob, identical results).  Default: 8 in FP32 (the c-face
-  // words of 7 of 8 c-hops through shared memory: 0.426 against 0.455 ms per
-  // sweep at 256^3), none in FP64 (0.729 against 0.589 ms).
-  ctx->c.sweep_cluster = p.precision != 0 ? 8 : 1;
+  // CTAs per thread-block cluster along c in the MIC(0) sweeps (1, 2, 3, 4,
+  // 8, 9 or 16; performance knob, identical results).  Default 0: chosen per
+  // solve from the patches along c (pl_setup).
+  ctx->c.sweep_cluster = 0;
   if (const char* v = getenv("WCG_SWEEP_CLUSTER")) {
     const int k = atoi(v);
     ctx->c.sweep_cluster = (k == 2 || k == 3 || k == 4 || k == 8 || k == 9 || k == 16) ? k : 1;

@@ -1280,11 +1280,29 @@ static cudaError_t pl_setup(Context& c, const int* lo, const int* hi) {
     WCG_TRY(cudaMemcpyAsync(c.pl_order.p, c.pl_order_h.data(), G.npatch * sizeof(int),
                             cudaMemcpyHostToDevice, c.stream));
   }
-  // clusters along c only where the box has more patches along c than half
-  // a cluster (on small boxes they cost more than they save: the 64^3 dam
-  // break, 2 patches along c, ran 7.4 ms per step in 2-CTA clusters against
-  // 7.0 ms plain)
-  c.pl_cc = G.nPC > c.sweep_cluster / 2 ? c.sweep_cluster : 1;
+  // The cluster's extent along c.  Chosen (sweep_cluster 0): a cluster that
+  // tiles the patches along c exactly, so no CTA idles, at most 9 CTAs in
+  // FP32 (two CTAs per SM fit) and 3 in FP64 (one per SM).  At 256^3 (9
+  // patches along c, ms per sweep launch): FP32 plain 0.461, 3 0.436, 8
+  // 0.423, 9 0.415, 16 0.521; FP64 plain 0.594, 3 0.550, 8 0.721, 9 0.638.
+  // On small boxes they cost more than they save (the 64^3 dam break, 2
+  // patches along c: 7.4 ms per step in 2-CTA clusters, 7.0 ms plain).
+  // Given: used where the box has more patches along c than half a cluster.
+  if (c.sweep_cluster == 0) {
+    c.pl_cc = 1;
+    const int fp32[] = {9, 8}, fp64[] = {3};
+    const int* cand = c.prm.precision != 0 ? fp32 : fp64;
+    const int ncand = c.prm.precision != 0 ? 2 : 1;
+    if (G.nPC >= 6)
+      for (int k = 0; k < ncand; ++k)
+        if (G.nPC % cand[k] == 0) {
+          c.pl_cc = cand[k];
+          break;
+        }
+    if (c.pl_cc == 1 && c.prm.precision != 0 && G.nPC > 4) c.pl_cc = 8;
+  } else {
+    c.pl_cc = G.nPC > c.sweep_cluster / 2 ? c.sweep_cluster : 1;
+  }
   if (c.sweep_cluster_a > 1) {
     // tiles of pl_cc c-patches by sweep_cluster_a a-patches, in wave order
     const int CC = c.pl_cc, CA = c.sweep_cluster_a;
