@@ -1299,7 +1299,7 @@ static cudaError_t pl_setup(Context& c, const int* lo, const int* hi) {
           c.pl_cc = cand[k];
           break;
         }
-    if (c.pl_cc == 1 && c.prm.precision != 0 && G.nPC > 4) c.pl_cc = 8;
+    if (c.pl_cc == 1 && c.prm.precision != 0 && G.nPC >= 6) c.pl_cc = 8;
   } else {
     c.pl_cc = G.nPC > c.sweep_cluster / 2 ? c.sweep_cluster : 1;
   }
