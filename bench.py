@@ -492,13 +492,14 @@ def run_batch(args, steps=3):
     seeded densities and viscosities; the many-scenes configuration scaled to
     a short run): aggregate particle-steps/s stepped one after another
     against the batch (separate streams, host thread pool, thread count
-    autotuned during warm-up).  Device-synchronised wall time around each
+    autotuned during warm-up), and the batch again after each scene's launch
+    schedule is chosen from timed trials.  Device-synchronised wall time around each
     whole pass (best of three; one pass each with --batch-full, which runs
     the configuration at its stated size)."""
     import torch
     from libwetcloth_b200 import scenes
     from libwetcloth_b200._capi import WCG_FP32_REFINE
-    from libwetcloth_b200.solver import FluidBatch, FluidScene
+    from libwetcloth_b200.solver import DEFAULT_SCHEDULES, FluidBatch, FluidScene
     full = getattr(args, "batch_full", False)
     if full:
         specs = scenes.batch_scenes(256, 4, (32, 96), (10_000, 1_000_000))
@@ -540,6 +541,20 @@ def run_batch(args, steps=3):
         torch.cuda.synchronize()
         bat_s = min(bat_s, time.perf_counter() - t0)
     threads = b.threads
+    # per-scene launch schedules from timed trials, then the same passes again
+    cands = DEFAULT_SCHEDULES
+    chosen, _ = b.autotune_schedules(DT, cands)
+    sched_s = float("inf")
+    for _ in range(passes):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        b.step(DT, nsteps=steps)
+        torch.cuda.synchronize()
+        sched_s = min(sched_s, time.perf_counter() - t0)
+    hist = {}
+    for k in chosen:
+        key = "x".join(str(v) for v in cands[k])
+        hist[key] = hist.get(key, 0) + 1
     b.close()
     for g in gs:
         g.close()
@@ -549,6 +564,10 @@ def run_batch(args, steps=3):
             "batched_particle_steps_per_s": round(total_p * steps / bat_s, 1),
             "speedup": round(seq_s / bat_s, 3), "threads": threads,
             "autotune_ms": {str(k): round(v, 2) for k, v in tune.items()},
+            "batched_tuned_particle_steps_per_s": round(total_p * steps / sched_s, 1),
+            "speedup_tuned": round(seq_s / sched_s, 3),
+            "schedules_chosen": hist,
+            "schedule_key": "sweep_cluster x sweep_cluster_a x pcg_batch",
             "note": f"wall time, device-synchronised, warm-up excluded, best of {passes} "
                     "pass(es) per arm"}
 

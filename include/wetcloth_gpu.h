@@ -347,14 +347,16 @@ int wcg_num_substeps(wcg_ctx* ctx, double dt, int* n_out);
  * NULL; 0 when the viscosity is off) and of the positions x (3n): xbar0 holds
  * xbar3 (the advection's identity part) plus the derivative through the
  * quadratic B-spline weights and the APIC offsets x_node - x of P2G and G2P
- * (TwoDScene::updateParticleWeights TwoDScene.cpp:2084-2174).  The grid's
- * discrete structure, the liquid phi of the ghost-fluid fractions and the
- * solid projections are held at the checkpoint's values (with uniform
- * density the pressure matrix does not move with x).
+ * (TwoDScene::updateParticleWeights TwoDScene.cpp:2084-2174), through the
+ * liquid phi behind the ghost-fluid fractions of the pressure matrix, and
+ * through the solid projection of the particle correction.  The grid's
+ * discrete structure (activation, DOFs, valid faces) and the nearest
+ * particle chosen for each node's liquid phi are held at the checkpoint's
+ * values.
  * wcg_set_adjoint_positions(ctx, 0) holds x fixed instead (xbar0 = xbar3).
  * Liquid scenes; the solve is the forward's solver on the same (symmetric)
- * matrix.  The advection's solid projection is differentiated; with the particle
- * correction on, the sub-step differentiated corrects the subset of the
+ * matrix (its ghost-fluid fractions' own derivative enters the right-hand
+ * side).  With the particle correction on, the sub-step differentiated corrects the subset of the
  * correction stream's next call (wcg_set_correction_count).  Refused
  * (WCG_ERR_UNSUPPORTED) with elasto particles, the implicit viscosity, or the
  * particle split or merge on. */
@@ -441,6 +443,33 @@ int wcg_batch_threads(const wcg_batch* b);
  * scene by one step), keeps the fastest; ms[k] (may be NULL) gets the times. */
 int wcg_batch_autotune(wcg_batch* b, const double* dt, const int* candidates, int ncand,
                        double* ms);
+
+/* Launch schedule of a context's pressure solve (no reference counterpart).
+ * Performance only: every schedule gives bit-identical results.
+ *   sweep_cluster    CTAs per thread-block cluster along c in the MIC(0)
+ *                    sweeps: 0 chosen per solve from the patches along c
+ *                    (the default), 1 plain, or 2, 3, 4, 8, 9, 16 (used when
+ *                    the box has more than half that many patches along c);
+ *   sweep_cluster_a  CTAs along a as well (2-D clusters): 1, 4 (with
+ *                    sweep_cluster 1..4) or 8 (with sweep_cluster 1..2);
+ *   pcg_batch        PCG iterations launched per convergence check on the
+ *                    host (1..64; default 8). */
+typedef struct wcg_schedule {
+  int sweep_cluster;
+  int sweep_cluster_a;
+  int pcg_batch;
+} wcg_schedule;
+int wcg_set_schedule(wcg_ctx* ctx, const wcg_schedule* s);
+int wcg_get_schedule(const wcg_ctx* ctx, wcg_schedule* s);
+/* Chooses each scene's schedule from timed trials: for each candidate k in
+ * turn every scene takes that schedule and the batch is stepped `trials`
+ * times (each trial advances every scene by one step, all scenes at once on
+ * the thread count set); a scene's time is the device time of its step on
+ * its own stream (CUDA events), minimum over the trials.  Each scene keeps
+ * its fastest candidate.  ms (may be NULL) gets n x ncand times (scene-major),
+ * chosen (may be NULL) the candidate index per scene. */
+int wcg_batch_autotune_schedules(wcg_batch* b, const double* dt, const wcg_schedule* cand,
+                                 int ncand, int trials, double* ms, int* chosen);
 
 /* ---- instrumentation ---- */
 /* the cudaStream_t all of this context's kernels run on */

@@ -85,6 +85,14 @@ class WcgShape(ctypes.Structure):
     ]
 
 
+class WcgSchedule(ctypes.Structure):
+    _fields_ = [
+        ("sweep_cluster", ctypes.c_int),
+        ("sweep_cluster_a", ctypes.c_int),
+        ("pcg_batch", ctypes.c_int),
+    ]
+
+
 class WcgStats(ctypes.Structure):
     _fields_ = [
         ("substeps", ctypes.c_int),
@@ -126,6 +134,11 @@ SIGNATURES = {
     "wcg_batch_set_threads": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "wcg_batch_threads": (ctypes.c_int, [ctypes.c_void_p]),
     "wcg_batch_autotune": (ctypes.c_int, [ctypes.c_void_p, _D, _I, ctypes.c_int, _D]),
+    "wcg_batch_autotune_schedules": (ctypes.c_int, [ctypes.c_void_p, _D,
+                                                    ctypes.POINTER(WcgSchedule), ctypes.c_int,
+                                                    ctypes.c_int, _D, _I]),
+    "wcg_set_schedule": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(WcgSchedule)]),
+    "wcg_get_schedule": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(WcgSchedule)]),
     "wcg_save_positions": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
     "wcg_load_positions": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
     "wcg_write_fluid_obj": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),

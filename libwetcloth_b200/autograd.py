@@ -5,9 +5,10 @@ wcg_substep_vjp); the arithmetic is all in libwcgpu.so.
 tensors and records a node whose backward restores the checkpoint (x, v, C)
 in the scene, recomputes the forward grid there and runs the reverse-mode
 kernels; an optional 0-d ``viscosity`` tensor gets its gradient too.  The
-gradient in x follows the transfer weights' dependence on the positions
-(P2G, G2P and the advection); the grid's discrete structure and the liquid
-phi of the ghost-fluid fractions are held at the checkpoint's values.  The
+gradient in x follows the positions through the transfer weights (P2G, G2P
+and the advection), the liquid phi behind the ghost-fluid fractions and the
+solid projection of the particle correction; the grid's discrete structure
+(activation, DOFs, valid faces) is held at the checkpoint's values.  The
 scene's particle state after backward is the checkpoint of the last node
 differentiated.
 

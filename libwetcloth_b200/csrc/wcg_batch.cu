@@ -5,8 +5,12 @@
 // first.  The kernels of different scenes then overlap on the GPU: small
 // scenes leave most SMs idle and their launches are short, so running several
 // at once fills the machine.  The thread count is chosen by
-// wcg_batch_autotune, which times one batch step per candidate.  Results are
-// those of stepping each scene alone (the same kernels on the same data).
+// wcg_batch_autotune, which times one batch step per candidate, and each
+// scene's launch schedule (the sweep clusters' shape, the PCG iterations per
+// host check) by wcg_batch_autotune_schedules, from the device time of each
+// scene's step under each candidate.  Results are those of stepping each
+// scene alone (the same kernels on the same data; the schedules do not change
+// them).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -23,6 +27,8 @@ struct wcg_batch {
   std::vector<wcg_ctx*> scenes;
   std::vector<int> order;  // largest particle count first
   int nthreads = 1;
+  std::vector<int> device;      // per scene, taken at creation
+  std::vector<cudaEvent_t> ev;  // per scene: start, end of a timed step (created on first use)
 };
 
 namespace {
@@ -32,7 +38,9 @@ int fail(int code, const std::string& msg) { return wcg::set_last_error(code, ms
 // One batch step: every scene takes nsteps calls of wcg_step with its dt.
 // Returns the first hard error; WCG_ERR_NOT_CONVERGED (which the reference
 // treats as a warning) only if no hard error occurred.
-int run_batch(wcg_batch* b, const double* dt, int nsteps, int nthreads, int* status) {
+// With `timed`, each scene's steps are bracketed by its two events.
+int run_batch(wcg_batch* b, const double* dt, int nsteps, int nthreads, int* status,
+              bool timed = false) {
   const int n = (int)b->scenes.size();
   std::atomic<int> next(0);
   std::vector<int> st((size_t)n, WCG_OK);
@@ -48,6 +56,8 @@ int run_batch(wcg_batch* b, const double* dt, int nsteps, int nthreads, int* sta
         cudaSetDevice(ctx->c.device);
         dev = ctx->c.device;
       }
+      cudaStream_t strm = (cudaStream_t)wcg_stream(ctx);
+      if (timed) cudaEventRecord(b->ev[2 * i], strm);
       for (int s = 0; s < nsteps; ++s) {
         int sub = 0;
         const int r = wcg_step(ctx, dt[i], &sub);
@@ -60,6 +70,7 @@ int run_batch(wcg_batch* b, const double* dt, int nsteps, int nthreads, int* sta
         msg[i] = wcg_last_error();
         break;
       }
+      if (timed) cudaEventRecord(b->ev[2 * i + 1], strm);
     }
   };
   const int nt = std::max(1, std::min(nthreads, n));
@@ -93,6 +104,7 @@ int wcg_batch_create(int n, wcg_ctx* const* scenes, wcg_batch** out) {
     if (!scenes[i]) return fail(WCG_ERR_ARG, "null scene in batch");
   wcg_batch* b = new wcg_batch();
   b->scenes.assign(scenes, scenes + n);
+  for (int i = 0; i < n; ++i) b->device.push_back(scenes[i]->c.device);
   b->order.resize((size_t)n);
   for (int i = 0; i < n; ++i) b->order[i] = i;
   std::stable_sort(b->order.begin(), b->order.end(), [&](int x, int y) {
@@ -104,6 +116,12 @@ int wcg_batch_create(int n, wcg_ctx* const* scenes, wcg_batch** out) {
 }
 
 int wcg_batch_destroy(wcg_batch* b) {
+  if (!b) return WCG_OK;
+  // the scenes may already be destroyed: only the batch's own records are used
+  for (size_t i = 0; i < b->ev.size(); ++i) {
+    cudaSetDevice(b->device[i / 2]);
+    cudaEventDestroy(b->ev[i]);
+  }
   delete b;
   return WCG_OK;
 }
@@ -144,6 +162,66 @@ int wcg_batch_autotune(wcg_batch* b, const double* dt, const int* candidates, in
     }
   }
   b->nthreads = best_t;
+  return WCG_OK;
+}
+
+// Each candidate in turn: every scene takes it, the batch steps `trials`
+// times with each scene's step timed on its stream; a scene keeps the
+// candidate with its smallest time.
+int wcg_batch_autotune_schedules(wcg_batch* b, const double* dt, const wcg_schedule* cand,
+                                 int ncand, int trials, double* ms_out, int* chosen_out) {
+  if (!b || !dt || !cand || ncand <= 0 || trials < 1)
+    return fail(WCG_ERR_ARG, "bad schedule autotune arguments");
+  const int n = (int)b->scenes.size();
+  for (int i = 0; i < n; ++i)
+    if (!(dt[i] > 0)) return fail(WCG_ERR_ARG, "dt must be positive");
+  std::vector<wcg_schedule> keep((size_t)n);
+  for (int i = 0; i < n; ++i) wcg_get_schedule(b->scenes[i], &keep[(size_t)i]);
+  // every candidate must be accepted by every scene before any trial runs
+  for (int k = 0; k < ncand; ++k)
+    for (int i = 0; i < n; ++i) {
+      const int r = wcg_set_schedule(b->scenes[i], &cand[k]);
+      wcg_set_schedule(b->scenes[i], &keep[(size_t)i]);
+      if (r != WCG_OK) return r;
+    }
+  if (b->ev.empty()) {
+    b->ev.resize((size_t)2 * n);
+    for (int i = 0; i < 2 * n; ++i) {
+      cudaSetDevice(b->device[(size_t)i / 2]);
+      if (cudaEventCreate(&b->ev[(size_t)i]) != cudaSuccess) {
+        b->ev.resize((size_t)i);
+        return fail(WCG_ERR_CUDA, "cudaEventCreate failed");
+      }
+    }
+  }
+  std::vector<double> best((size_t)n * ncand, 1e300);
+  for (int k = 0; k < ncand; ++k) {
+    for (int i = 0; i < n; ++i) wcg_set_schedule(b->scenes[i], &cand[k]);
+    for (int t = 0; t < trials; ++t) {
+      const int r = run_batch(b, dt, 1, b->nthreads, nullptr, true);
+      if (r != WCG_OK && r != WCG_ERR_NOT_CONVERGED) {
+        for (int i = 0; i < n; ++i) wcg_set_schedule(b->scenes[i], &keep[(size_t)i]);
+        return r;
+      }
+      for (int i = 0; i < n; ++i) {
+        cudaSetDevice(b->device[(size_t)i]);
+        float ms = 0.f;
+        if (cudaEventSynchronize(b->ev[2 * i + 1]) != cudaSuccess ||
+            cudaEventElapsedTime(&ms, b->ev[2 * i], b->ev[2 * i + 1]) != cudaSuccess)
+          return fail(WCG_ERR_CUDA, "timing a scene's step failed");
+        double& m = best[(size_t)i * ncand + k];
+        m = std::min(m, (double)ms);
+      }
+    }
+  }
+  for (int i = 0; i < n; ++i) {
+    int kb = 0;
+    for (int k = 1; k < ncand; ++k)
+      if (best[(size_t)i * ncand + k] < best[(size_t)i * ncand + kb]) kb = k;
+    wcg_set_schedule(b->scenes[i], &cand[kb]);
+    if (chosen_out) chosen_out[i] = kb;
+  }
+  if (ms_out) std::copy(best.begin(), best.end(), ms_out);
   return WCG_OK;
 }
 

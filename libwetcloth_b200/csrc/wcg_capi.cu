@@ -812,6 +812,30 @@ int wcg_set_viscosity(wcg_ctx* ctx, double viscosity, int substeps) {
   return WCG_OK;
 }
 
+int wcg_set_schedule(wcg_ctx* ctx, const wcg_schedule* s) {
+  WCG_CHECK_CTX(ctx);
+  if (!s) return fail(WCG_ERR_ARG, "null schedule");
+  const int cc = s->sweep_cluster, ca = s->sweep_cluster_a;
+  if (!(cc == 0 || cc == 1 || cc == 2 || cc == 3 || cc == 4 || cc == 8 || cc == 9 || cc == 16))
+    return fail(WCG_ERR_ARG, "sweep_cluster must be 0, 1, 2, 3, 4, 8, 9 or 16");
+  if (!(ca == 1 || (ca == 4 && cc >= 1 && cc <= 4) || (ca == 8 && cc >= 1 && cc <= 2)))
+    return fail(WCG_ERR_ARG, "sweep_cluster_a must be 1, 4 (sweep_cluster 1..4) or 8 "
+                             "(sweep_cluster 1..2)");
+  if (s->pcg_batch < 1 || s->pcg_batch > 64) return fail(WCG_ERR_ARG, "pcg_batch must lie in [1, 64]");
+  ctx->c.sweep_cluster = cc;
+  ctx->c.sweep_cluster_a = ca;
+  ctx->c.pcg_batch = s->pcg_batch;
+  return WCG_OK;
+}
+
+int wcg_get_schedule(const wcg_ctx* ctx, wcg_schedule* s) {
+  if (!ctx || !s) return fail(WCG_ERR_ARG, "null argument");
+  s->sweep_cluster = ctx->c.sweep_cluster;
+  s->sweep_cluster_a = ctx->c.sweep_cluster_a;
+  s->pcg_batch = ctx->c.pcg_batch;
+  return WCG_OK;
+}
+
 int wcg_set_wait_limit(wcg_ctx* ctx, long long spin_limit, int stale_patch) {
   WCG_CHECK_CTX(ctx);
   if (spin_limit < 1 || spin_limit > (1ll << 40))

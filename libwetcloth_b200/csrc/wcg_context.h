@@ -253,6 +253,7 @@ struct Context {
   int sweep_cluster_a = 1;       // ... and along a (2-D clusters: 4 or 8)
   int pl_cc = 1;                 // the c-extent the current solve uses (<= patches along c)
   int spmv_rows = 1;             // 0: the patch-streamed SpMV instead of the row-parallel one
+  int pcg_batch = 8;             // PCG iterations launched per host convergence check
   DevBuf pl_part;                // per-patch partials (double)
   long long pl_cap = 0;
   int pl_tickets = 0;            // sweep tickets handed out in this solve
@@ -261,6 +262,10 @@ struct Context {
   TermSet term{};                // terminator shapes (the params' box, or wcg_set_terminators)
   int stale_patch = -1;          // failure-path test: a patch whose waits cannot succeed
   std::vector<int> pl_order_h;
+  // host copies of pl_corder / pl_corder2 and the (nPA, nPC, CC, CA) they
+  // were built for: re-uploaded only when that changes
+  std::vector<int> pl_corder_h, pl_corder2_h;
+  long long pl_corder_key = -1, pl_corder2_key = -1;
 
   // multigrid-PCG: dense levels (d, ax, ay, az, x, b per cell; masks) and the
   // level-0 PCG vectors

@@ -1041,13 +1041,12 @@ static cudaError_t set_scalars(Context& c, int slot, const double* v, int k) {
                          cudaMemcpyHostToDevice, c.stream);
 }
 
-constexpr int kPcgBatch = 8;  // iterations launched per host check
-
 // Inner MIC(0)-PCG (PCGSolver<T>::solve, PCGSolver.h:260-308) on the system
 // already assembled and factored: solves A x = r0 from x = 0 (x must be zero
 // on entry), r is overwritten with the residual.  tol_abs is the absolute
 // infinity-norm target.  Convergence is tested on the device after every
-// iteration; the host checks every kPcgBatch iterations.
+// iteration; the host checks every c.pcg_batch iterations (the launches of a
+// batch after convergence return at once, so results do not depend on it).
 template <typename R>
 static cudaError_t pcg_inner(Context& c, R* r, R* x, double tol_abs, int maxiters,
                              int* iters, int* conv, double* res) {
@@ -1102,7 +1101,7 @@ static cudaError_t pcg_inner(Context& c, R* r, R* x, double tol_abs, int maxiter
   R* sold = s0;
   R* snew = s1;
   for (;;) {
-    for (int b = 0; b < kPcgBatch; ++b) {
+    for (int b = 0; b < c.pcg_batch; ++b) {
       {
         ProfScope prof(c, P_PCGVEC);
         ++c.launches, k_spmv_s<R><<<kRedBlocks, kRedThreads, 0, c.stream>>>(
@@ -1303,12 +1302,16 @@ static cudaError_t pl_setup(Context& c, const int* lo, const int* hi) {
   } else {
     c.pl_cc = G.nPC > c.sweep_cluster / 2 ? c.sweep_cluster : 1;
   }
-  if (c.sweep_cluster_a > 1) {
+  // the cluster orders are rebuilt only when the patch grid or the cluster
+  // shape changes (a pageable upload waits for the stream)
+  const long long okey = ((long long)G.nPA << 40) | ((long long)G.nPC << 16) |
+                         ((long long)c.pl_cc << 8) | c.sweep_cluster_a;
+  if (c.sweep_cluster_a > 1 && okey != c.pl_corder2_key) {
     // tiles of pl_cc c-patches by sweep_cluster_a a-patches, in wave order
     const int CC = c.pl_cc, CA = c.sweep_cluster_a;
     const int nTA = (G.nPA + CA - 1) / CA, nTC = (G.nPC + CC - 1) / CC;
-    std::vector<int> co;
-    co.reserve((size_t)nTA * nTC);
+    std::vector<int>& co = c.pl_corder2_h;
+    co.clear();
     for (int w = 0; w <= nTA + nTC - 2; ++w)
       for (int tc = 0; tc < nTC; ++tc) {
         const int ta = w - tc;
@@ -1317,14 +1320,14 @@ static cudaError_t pl_setup(Context& c, const int* lo, const int* hi) {
     WCG_TRY(c.pl_corder2.ensure(co.size() * sizeof(int)));
     WCG_TRY(cudaMemcpyAsync(c.pl_corder2.p, co.data(), co.size() * sizeof(int),
                             cudaMemcpyHostToDevice, c.stream));
-    WCG_TRY(cudaStreamSynchronize(c.stream));  // co is a host temporary
+    c.pl_corder2_key = okey;
   }
-  if (c.pl_cc > 1) {
+  if (c.pl_cc > 1 && okey != c.pl_corder_key) {
     // cluster columns (PAi, PCc) of pl_cc c-patches, in wave order
     const int CL = c.pl_cc;
     const int nPCc = (G.nPC + CL - 1) / CL;
-    std::vector<int> co;
-    co.reserve((size_t)G.nPA * nPCc);
+    std::vector<int>& co = c.pl_corder_h;
+    co.clear();
     for (int w = 0; w <= G.nPA + nPCc - 2; ++w)
       for (int pc = 0; pc < nPCc; ++pc) {
         const int pa = w - pc;
@@ -1333,7 +1336,7 @@ static cudaError_t pl_setup(Context& c, const int* lo, const int* hi) {
     WCG_TRY(c.pl_corder.ensure(co.size() * sizeof(int)));
     WCG_TRY(cudaMemcpyAsync(c.pl_corder.p, co.data(), co.size() * sizeof(int),
                             cudaMemcpyHostToDevice, c.stream));
-    WCG_TRY(cudaStreamSynchronize(c.stream));  // co is a host temporary
+    c.pl_corder_key = okey;
   }
   // every array starts at zero (rows and lines outside the box stay zero)
   WCG_TRY(cudaMemsetAsync(c.pl.p, 0, (size_t)kNumPlFields * G.len * sizeof(R), c.stream));
@@ -1508,7 +1511,7 @@ static cudaError_t pl_pcg(Context& c, R* r, R* x, double tol_abs, int maxiters, 
   WCG_TRY(ensure_scratch(c, (size_t)spmv_blocks * sizeof(double)));
   part = c.scratch.as<double>();
   for (;;) {
-    for (int b = 0; b < kPcgBatch; ++b) {
+    for (int b = 0; b < c.pcg_batch; ++b) {
       {
         ProfScope prof(c, P_PCGVEC);
         if (c.spmv_rows) {  // its last block forms alpha

@@ -267,6 +267,19 @@ class FluidScene:
             arr[k].param[:] = par[:4]
         check(self.L.wcg_set_terminators(self.h, len(shapes), arr))
 
+    @property
+    def schedule(self):
+        """The pressure solve's launch schedule (sweep_cluster,
+        sweep_cluster_a, pcg_batch); performance only, results unchanged."""
+        s = _capi.WcgSchedule()
+        check(self.L.wcg_get_schedule(self.h, ctypes.byref(s)))
+        return (s.sweep_cluster, s.sweep_cluster_a, s.pcg_batch)
+
+    @schedule.setter
+    def schedule(self, sched):
+        s = _capi.WcgSchedule(*[int(v) for v in sched])
+        check(self.L.wcg_set_schedule(self.h, ctypes.byref(s)))
+
     def set_correction_count(self, k):
         """Call count of the correction stream (the next sub-step corrects the
         subset of call k)."""
@@ -363,6 +376,12 @@ class FluidScene:
 
 
 
+# launch schedules the batch autotuner tries by default: the sweep clusters
+# chosen per solve, plain, 2 and 4 along c, and 4 or 8 PCG iterations per
+# host check
+DEFAULT_SCHEDULES = ((0, 1, 8), (1, 1, 8), (2, 1, 8), (4, 1, 8), (1, 1, 4), (2, 1, 4))
+
+
 class FluidBatch:
     """Independent scenes stepped together (wcg_batch_*): each scene is a
     FluidScene with its own stream; a pool of host threads steps them largest
@@ -415,3 +434,20 @@ class FluidBatch:
         ms = (ctypes.c_double * len(candidates))()
         check(self.L.wcg_batch_autotune(self.h, _dp(d), c, len(candidates), ms))
         return dict(zip(candidates, list(ms)))
+
+    def autotune_schedules(self, dt, candidates=DEFAULT_SCHEDULES, trials=1):
+        """Choose each scene's launch schedule (sweep_cluster,
+        sweep_cluster_a, pcg_batch) from timed trials: every candidate is
+        stepped `trials` times (each advances every scene by one step) and
+        each scene keeps the one with its smallest step time.  Returns (the
+        chosen candidate index per scene, the times in ms as an array
+        scenes x candidates)."""
+        n = len(self.scenes)
+        d = np.ascontiguousarray(np.broadcast_to(np.asarray(dt, dtype=np.float64), (n,)))
+        cand = (_capi.WcgSchedule * len(candidates))(
+            *[_capi.WcgSchedule(*[int(v) for v in c]) for c in candidates])
+        ms = np.zeros((n, len(candidates)))
+        chosen = (ctypes.c_int * n)()
+        check(self.L.wcg_batch_autotune_schedules(self.h, _dp(d), cand, len(candidates),
+                                                  int(trials), _dp(ms), chosen))
+        return list(chosen), ms

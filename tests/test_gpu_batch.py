@@ -86,3 +86,51 @@ def test_batch_with_particle_maintenance_matches_alone(wcg):
     b.close()
     for g in gs:
         g.close()
+
+
+def test_schedule_autotune_keeps_results(wcg):
+    """The per-scene schedule autotuner (sweep-cluster shape and PCG
+    iterations per host check, chosen from each scene's timed steps) changes
+    no result: after the tuning trials (one step per candidate) and two more
+    batch steps, every scene is bit-identical to the same number of steps
+    taken alone with the default schedule.  Scenes up to 96^3 so the
+    clustered sweeps have patches to cluster."""
+    specs = scenes.batch_scenes(5, 11, (32, 96), (20000, 400000))
+    cands = [(0, 1, 8), (1, 1, 8), (2, 1, 8), (4, 1, 4), (1, 4, 16), (2, 8, 2)]
+    nsteps = len(cands) + 2
+    alone = []
+    for sc in specs:
+        g = FluidScene(sc, precision=_capi.WCG_FP32_REFINE)
+        for _ in range(nsteps):
+            g.step(DT)
+        alone.append(g.download())
+        g.close()
+    gs = [FluidScene(sc, precision=_capi.WCG_FP32_REFINE) for sc in specs]
+    b = FluidBatch(gs)
+    b.threads = 3
+    chosen, ms = b.autotune_schedules(DT, cands)
+    assert ms.shape == (len(specs), len(cands)) and np.all(ms > 0)
+    for g, k in zip(gs, chosen):
+        assert g.schedule == cands[k]
+        assert k == int(np.argmin(ms[gs.index(g)]))
+    st = b.step(DT, nsteps=2)
+    assert all(s == _capi.WCG_OK for s in st), st
+    for g, ref in zip(gs, alone):
+        for a, r in zip(g.download(), ref):
+            assert np.array_equal(a, r)
+    b.close()
+    for g in gs:
+        g.close()
+
+
+def test_schedule_arguments(wcg):
+    sc = scenes.batch_scenes(1, 3, (16, 16), (2000, 2000))[0]
+    g = FluidScene(sc)
+    assert g.schedule == (0, 1, 8)
+    g.schedule = (9, 1, 32)
+    assert g.schedule == (9, 1, 32)
+    for bad in [(5, 1, 8), (8, 4, 8), (0, 4, 8), (4, 8, 8), (1, 2, 8), (1, 1, 0), (1, 1, 65)]:
+        with pytest.raises(_capi.WcgError):
+            g.schedule = bad
+    assert g.schedule == (9, 1, 32)
+    g.close()

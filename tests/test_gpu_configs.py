@@ -8,7 +8,9 @@ plan's own configurations, at their stated sizes.
   after it to 1e-9); ten steps against the C oracle run live; and 100 steps
   against the oracle's committed digest (tests/golden/config0_dam64.npz).
 * Config 1 (128^3 liquid sphere falling onto a 128 x 128-vertex sheet,
-  dt 5e-4): the first step against the oracle -- liquid and sheet state.
+  dt 5e-4): the first step against the oracle -- liquid and sheet state --
+  and 200 steps against the oracle's committed digest
+  (tests/golden/config1_sheet128.npz).
 * Config 2 (256^3 half box, 16.8M particles): a 64^3 replica of the same
   generator for three steps against the oracle run live, and the first
   full-size FP64 step against the oracle's committed digest
@@ -167,6 +169,43 @@ def test_config1_first_step_vs_oracle(wcg):
     assert_close(x4, o.get("adv_x4").reshape(-1, 4)[:ne], 1e-12, "sheet x")
     assert_close(v4, o.get("adv_ev4").reshape(-1, 4)[:ne], 1e-9, "sheet v")
     o.close()
+    g.close()
+
+
+def test_config1_two_hundred_steps_vs_oracle_digest(wcg):
+    """Config 1 for its stated 200 steps (dt 5e-4) against the oracle's
+    committed digest (tests/golden/config1_sheet128.npz): the liquid sample,
+    sums and norms after 20 and 200 steps, the sheet's positions and
+    velocities at a sample of its vertices and summed over all of them, and
+    the MIC(0) iteration count of every step (within one)."""
+    dt = 5e-4
+    d = np.load(os.path.join(GOLDEN, "config1_sheet128.npz"))
+    sc = scenes.liquid_on_sheet(128, 8, 3, sheet_spacing=0.8 / 127)
+    ne = sc.elasto.n
+    assert sc.x.shape[0] == int(d["n"][0]) and ne == int(d["ne"][0])
+    idx, sidx = d["idx"], d["sheet_idx"]
+    g = FluidScene(sc)
+    iters = []
+    for k in range(1, 201):
+        g.step(dt)
+        iters.append(g.stats()["pcg_iters"])
+        if k in (20, 200):
+            x, v, C = g.download()
+            p = f"s{k}_"
+            xtol, vtol = (1e-10, 1e-8) if k == 20 else (1e-8, 1e-6)
+            _state_close(x[idx], v[idx], C[idx], d[p + "x"], d[p + "v"], d[p + "C"], xtol, vtol,
+                         f"{k} steps")
+            vs = np.abs(d[p + "v_sum"]).max() + np.sqrt(d[p + "v_sq"][0])
+            assert np.abs(v.sum(axis=0) - d[p + "v_sum"]).max() <= vtol * vs
+            assert abs((v * v).sum() - d[p + "v_sq"][0]) <= vtol * d[p + "v_sq"][0]
+            x4, v4, _ = g.download_elasto()
+            assert_close(x4[sidx], d[p + "sheet_x4"], xtol, f"sheet x, {k} steps")
+            assert_close(v4[sidx], d[p + "sheet_v4"], vtol, f"sheet v, {k} steps")
+            xs = np.abs(d[p + "sheet_x4_sum"]).max()
+            assert np.abs(x4.sum(axis=0) - d[p + "sheet_x4_sum"]).max() <= xtol * xs
+            vs = np.abs(d[p + "sheet_v4_sum"]).max() + np.sqrt(d[p + "sheet_v4_sq"][0])
+            assert np.abs(v4.sum(axis=0) - d[p + "sheet_v4_sum"]).max() <= vtol * vs
+    assert np.abs(np.array(iters) - d["iters"]).max() <= 1
     g.close()
 
 
