@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -1389,15 +1390,19 @@ static cudaError_t pl_sweep_cl(Context& c, PencilSweepArgs<R> a) {
   c.pl_tickets += nunits;
   const size_t smem = CL > 1 ? sweep_cluster_smem<R>(MODE, UPD, G.Ls, CC, CA)
                              : sweep_dyn_smem<R>(MODE, UPD);
-  static bool attr_set = false;  // per instantiation, once per process
-  if (!attr_set) {
+  // function attributes are per device: set once per instantiation and
+  // device (the batch may step contexts of several devices from several
+  // threads; setting them twice is harmless)
+  static std::atomic<unsigned long long> attr_set{0};
+  const unsigned long long dbit = 1ull << (c.device & 63);
+  if (!(attr_set.load(std::memory_order_acquire) & dbit)) {
     WCG_TRY(cudaFuncSetAttribute(k_pencil_sweep<R, MODE, UPD, CC, CA>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(CL > 1 ? kSweepSmemMax : smem)));
     if (CL > 8)
       WCG_TRY(cudaFuncSetAttribute(k_pencil_sweep<R, MODE, UPD, CC, CA>,
                                    cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-    attr_set = true;
+    attr_set.fetch_or(dbit, std::memory_order_release);
   }
   if (CL == 1) {
     ++c.launches, k_pencil_sweep<R, MODE, UPD, 1, 1><<<(unsigned)G.npatch, kPatchLines, smem,
