@@ -266,6 +266,7 @@ def run_ours(args, rank, world, dev):
         e1 = torch.cuda.Event(enable_timing=True)
         nsub = __import__("ctypes").c_int(0)
         k_e2e = max(2, args.steps)
+        e2e_iters = []
         barrier()
         torch.cuda.synchronize(dev)
         e0.record(stream)
@@ -277,6 +278,7 @@ def run_ours(args, rank, world, dev):
             if k + 1 < k_e2e:
                 stage()  # the next step's input crosses PCIe while this step runs
             check(L.wcg_step(sim.h, DT, __import__("ctypes").byref(nsub)))
+            e2e_iters.append(sim.stats()["pcg_iters"])  # host-side record, no wait
             ox, ov, oC = outs[k % 2]
             check(L.wcg_download_liquid_async(sim.h, ptr(ox), ptr(ov), ptr(oC)))
             if k + 1 < k_e2e:
@@ -289,6 +291,7 @@ def run_ours(args, rank, world, dev):
         d2h = np_ * (3 + 3 + 9) * 8
         e2e = {"value": round(e2e_ms, 3), "unit": "ms/step",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": k_e2e,
+               "pcg_iters_per_step": e2e_iters,
                "input": "the same seeded state uploaded every step",
                "overlap": "input of step k + 1 staged during step k; read-back of step k "
                           "during step k + 1 (separate copy streams)"}
@@ -297,7 +300,12 @@ def run_ours(args, rank, world, dev):
     fp64 = None
     if not args.no_fp64:
         k64 = args.fp64_steps if args.fp64_steps is not None else args.steps
-        sim64, info64 = timed(WCG_FP64, k64, args.warmup)
+        sim64, info64 = timed(WCG_FP64, k64, args.warmup, sample_clocks=True)
+        # its phases, as for the headline arm
+        sim64.profile_begin()
+        for _ in range(args.profile_steps):
+            sim64.step(DT)
+        info64["phases"] = sim64.profile_end()
         sim64.close()
         fp64 = info64
     # FP32 + refinement at the tighter criterion of the precision configuration
@@ -341,9 +349,12 @@ def run_ours(args, rank, world, dev):
                 "peak_kind": peak_kind, "traffic": traffic,
                 "bytes_per_launch": int(bytes_launch),
                 "ms_per_launch": round(per_launch_ms, 4)}
-    phases = {k: {"ms_per_step": round(v[0] / args.profile_steps, 3),
-                  "launches_per_step": v[1] // args.profile_steps}
-              for k, v in prof.items()}
+    def phases_of(pr):
+        return {k: {"ms_per_step": round(v[0] / args.profile_steps, 3),
+                    "launches_per_step": v[1] // args.profile_steps}
+                for k, v in pr.items()}
+
+    phases = phases_of(prof)
     # transfer-kernel HBM fractions
     transfers = {}
     for k in ("p2g", "g2p_advect"):
@@ -387,7 +398,8 @@ def run_ours(args, rank, world, dev):
     }
     if fp64:
         out["fp64"] = {"ms_per_step": round(fp64["ms"], 3), "pcg_iters_per_step": fp64["iters"],
-                       "speedup_fp32_refine_vs_fp64": round(fp64["ms"] / main["ms"], 3)}
+                       "speedup_fp32_refine_vs_fp64": round(fp64["ms"] / main["ms"], 3),
+                       "clocks": fp64["clocks"], "phases": phases_of(fp64["phases"])}
     if tight:
         out["fp32_refine_1e-8"] = tight
     if mg:
@@ -494,8 +506,9 @@ def run_batch(args, steps=3):
     seeded densities and viscosities; the many-scenes configuration scaled to
     a short run): aggregate particle-steps/s stepped one after another
     against the batch (separate streams, host thread pool, thread count
-    autotuned during warm-up), and the batch again after each scene's launch
-    schedule is chosen from timed trials.  Device-synchronised wall time around each
+    autotuned during warm-up), the batch again after each scene's launch
+    schedule is chosen from timed trials, and again with the shared solve
+    (every waiting scene's PCG iterations in one launch per kernel).  Device-synchronised wall time around each
     whole pass (best of three; one pass each with --batch-full, which runs
     the configuration at its stated size)."""
     import torch
@@ -557,6 +570,18 @@ def run_batch(args, steps=3):
     for k in chosen:
         key = "x".join(str(v) for v in cands[k])
         hist[key] = hist.get(key, 0) + 1
+    # the shared solve: the scenes' PCG iterations in shared launches
+    b.set_shared_solve(True)
+    b.step(DT)  # untimed: first use of the shared tables
+    shared_s = float("inf")
+    for _ in range(passes):
+        torch.cuda.synchronize()
+        l0 = b.shared_launches
+        t0 = time.perf_counter()
+        b.step(DT, nsteps=steps)
+        torch.cuda.synchronize()
+        shared_s = min(shared_s, time.perf_counter() - t0)
+        shared_launches = b.shared_launches - l0
     b.close()
     for g in gs:
         g.close()
@@ -570,6 +595,9 @@ def run_batch(args, steps=3):
             "speedup_tuned": round(seq_s / sched_s, 3),
             "schedules_chosen": hist,
             "schedule_key": "sweep_cluster x sweep_cluster_a x pcg_batch",
+            "batched_shared_solve_particle_steps_per_s": round(total_p * steps / shared_s, 1),
+            "speedup_shared_solve": round(seq_s / shared_s, 3),
+            "shared_solve_launches_per_pass": shared_launches,
             "note": f"wall time, device-synchronised, warm-up excluded, best of {passes} "
                     "pass(es) per arm"}
 

@@ -439,6 +439,18 @@ int wcg_batch_destroy(wcg_batch* b);
 int wcg_batch_step(wcg_batch* b, const double* dt, int nsteps, int* status);
 int wcg_batch_set_threads(wcg_batch* b, int nthreads);
 int wcg_batch_threads(const wcg_batch* b);
+/* The shared solve (on: 1, off: 0; default off).  On, the PCG iterations of
+ * every scene that reaches its pressure solve during a batch step run in
+ * shared launches: one launch per kernel (SpMV, forward and backward MIC(0)
+ * sweep) over all waiting scenes of one precision, chunks of 8 iterations,
+ * each scene's status read once per chunk, converged scenes released and new
+ * ones admitted between chunks.  Each scene's arithmetic, block counts and
+ * partial sums are those of its solve alone, so results are unchanged.
+ * Needs every scene on one device; the scenes' own sweeps outside the
+ * iterations keep their schedules. */
+int wcg_batch_set_shared_solve(wcg_batch* b, int on);
+/* kernel launches the batch's shared solves have made (-1: null batch) */
+long long wcg_batch_shared_launches(const wcg_batch* b);
 /* Times one batch step per candidate thread count (each trial advances every
  * scene by one step), keeps the fastest; ms[k] (may be NULL) gets the times. */
 int wcg_batch_autotune(wcg_batch* b, const double* dt, const int* candidates, int ncand,

@@ -138,6 +138,8 @@ SIGNATURES = {
                                                     ctypes.POINTER(WcgSchedule), ctypes.c_int,
                                                     ctypes.c_int, _D, _I]),
     "wcg_set_schedule": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(WcgSchedule)]),
+    "wcg_batch_set_shared_solve": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "wcg_batch_shared_launches": (ctypes.c_longlong, [ctypes.c_void_p]),
     "wcg_get_schedule": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(WcgSchedule)]),
     "wcg_save_positions": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
     "wcg_load_positions": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),

@@ -8,9 +8,12 @@
 // wcg_batch_autotune, which times one batch step per candidate, and each
 // scene's launch schedule (the sweep clusters' shape, the PCG iterations per
 // host check) by wcg_batch_autotune_schedules, from the device time of each
-// scene's step under each candidate.  Results are those of stepping each
-// scene alone (the same kernels on the same data; the schedules do not change
-// them).
+// scene's step under each candidate.  With the shared solve on
+// (wcg_batch_set_shared_solve), the PCG iterations of all scenes waiting in
+// their pressure solve run as one launch per kernel from a coordinator
+// thread (wcg_step.cu), in place of one launch per scene.  Results are those
+// of stepping each scene alone (the same arithmetic on the same data; the
+// schedules and the shared solve do not change them).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -29,6 +32,8 @@ struct wcg_batch {
   int nthreads = 1;
   std::vector<int> device;      // per scene, taken at creation
   std::vector<cudaEvent_t> ev;  // per scene: start, end of a timed step (created on first use)
+  wcg::SharedSolve* ss = nullptr;  // the shared solve, when on
+  long long ss_launches = 0;       // launches of shared solves turned off since
 };
 
 namespace {
@@ -73,12 +78,16 @@ int run_batch(wcg_batch* b, const double* dt, int nsteps, int nthreads, int* sta
       if (timed) cudaEventRecord(b->ev[2 * i + 1], strm);
     }
   };
+  // the scenes' solves join the shared launches for this step only (a
+  // scene stepped on its own afterwards solves alone)
+  for (int i = 0; i < n; ++i) b->scenes[i]->c.shared_solve = b->ss;
   const int nt = std::max(1, std::min(nthreads, n));
   std::vector<std::thread> pool;
   pool.reserve((size_t)nt - 1);
   for (int t = 1; t < nt; ++t) pool.emplace_back(worker);
   worker();
   for (std::thread& t : pool) t.join();
+  for (int i = 0; i < n; ++i) b->scenes[i]->c.shared_solve = nullptr;
   int first = WCG_OK;
   for (int i = 0; i < n; ++i) {
     if (status) status[i] = st[i];
@@ -118,6 +127,7 @@ int wcg_batch_create(int n, wcg_ctx* const* scenes, wcg_batch** out) {
 int wcg_batch_destroy(wcg_batch* b) {
   if (!b) return WCG_OK;
   // the scenes may already be destroyed: only the batch's own records are used
+  wcg::shared_solve_destroy(b->ss);
   for (size_t i = 0; i < b->ev.size(); ++i) {
     cudaSetDevice(b->device[i / 2]);
     cudaEventDestroy(b->ev[i]);
@@ -140,6 +150,28 @@ int wcg_batch_set_threads(wcg_batch* b, int nthreads) {
 }
 
 int wcg_batch_threads(const wcg_batch* b) { return b ? b->nthreads : -1; }
+
+int wcg_batch_set_shared_solve(wcg_batch* b, int on) {
+  if (!b) return fail(WCG_ERR_ARG, "null batch");
+  if (!on) {
+    b->ss_launches += wcg::shared_solve_launches(b->ss);
+    wcg::shared_solve_destroy(b->ss);
+    b->ss = nullptr;
+    return WCG_OK;
+  }
+  if (b->ss) return WCG_OK;
+  for (int d : b->device)
+    if (d != b->device[0])
+      return fail(WCG_ERR_ARG, "the shared solve needs every scene on one device");
+  std::string err;
+  b->ss = wcg::shared_solve_create(b->device[0], &err);
+  if (!b->ss) return fail(WCG_ERR_CUDA, "shared solve: " + err);
+  return WCG_OK;
+}
+
+long long wcg_batch_shared_launches(const wcg_batch* b) {
+  return b ? b->ss_launches + wcg::shared_solve_launches(b->ss) : -1;
+}
 
 // Times one batch step for each candidate thread count (each trial advances
 // every scene by one step) and keeps the fastest.

@@ -34,8 +34,7 @@ int cuda_status(wcg::Context& c, cudaError_t e, const char* what) {
 // check the device error word after a stage
 int device_status(wcg::Context& c, const char* what) {
   int h = 0;
-  cudaError_t e = cudaMemcpyAsync(&h, c.derr.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
+  const cudaError_t e = wcg::read_small(c, c.derr.p, sizeof(int), &h);
   if (e != cudaSuccess) return cuda_status(c, e, what);
   if (h != 0) {
     cudaMemsetAsync(c.derr.p, 0, sizeof(int), c.stream);

@@ -170,6 +170,8 @@ enum PlField : int {
 };
 enum Pl64Field : int { PL64_X = 0, PL64_R, kNumPl64Fields };
 
+struct SharedSolve;  // a batch's shared PCG iterations (wcg_step.cu)
+
 struct Context {
   Params prm;
   cudaStream_t stream = nullptr;
@@ -183,6 +185,10 @@ struct Context {
   cudaStream_t in_stream = nullptr;
   cudaEvent_t ev_staged = nullptr, ev_loaded = nullptr;
   DevBuf ustage;
+  // set by a batch step with the shared solve on: the PCG iterations of the
+  // pressure solve join the batch's launches (ordered by the two events)
+  SharedSolve* shared_solve = nullptr;
+  cudaEvent_t ev_ss_ready = nullptr, ev_ss_done = nullptr;
   long long staged_n = -1;
   bool staged_C = false;
   int device = 0;
@@ -311,6 +317,9 @@ struct Context {
   DevBuf scratch;                // scan tiles and reduction partials
   DevBuf dscalars;               // device scalars (doubles)
   double* hscalars = nullptr;    // pinned mirror
+  // mapped pinned words the small reads of a step land in (read_small)
+  unsigned* hmap = nullptr;
+  unsigned* hmap_dev = nullptr;
   DevBuf derr;                   // device error word
   DevBuf ticket;                 // wavefront ticket counters
 
@@ -375,6 +384,20 @@ cudaError_t stage_particles_async(Context& c, long long n, const double* x3, con
                                   const double* C9, const double* mass, const double* vol,
                                   const double* radius);
 cudaError_t load_staged(Context& c);
+// Small device-to-host reads of a step (scalars, counts, the error word;
+// bytes a multiple of 4, at most kReadSmallBytes): a kernel on `stream`
+// stores them into mapped pinned memory, then the stream is synchronised.
+// No copy engine is involved, so a large read-back running on copy_stream
+// cannot hold them back.
+constexpr size_t kReadSmallBytes = 4096;
+cudaError_t read_small(Context& c, const void* d, size_t bytes, void* h);
+// The shared solve of a batch of contexts on one device: a coordinator thread
+// runs the PCG iterations of every context waiting in its pressure solve as
+// one launch per kernel, chunks of 8 iterations, admitting new solves between
+// chunks.  Results are those of each solve alone.
+SharedSolve* shared_solve_create(int device, std::string* err);
+void shared_solve_destroy(SharedSolve* s);
+long long shared_solve_launches(const SharedSolve* s);
 // positions in the reference's m_x layout (x, y, z, 0 per particle) and radii,
 // original order, host buffers
 cudaError_t download_positions(Context& c, double* x4, double* radius);

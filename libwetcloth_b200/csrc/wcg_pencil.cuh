@@ -279,9 +279,11 @@ struct PencilSweepArgs {
 // CA > 1 as well: clusters of CC x CA CTAs, a tile of CC c-patches by CA
 // a-patches (rank = ra + CA rc); a-face neighbours inside the tile exchange
 // through shared memory the same way (their words after the c-face ones).
+//
+// The body takes the launch's CTA count (nblocks) as an argument so a launch
+// over several solves (k_pencil_sweep_batch) can run it per solve.
 template <typename R, int MODE, bool UPD, int CC, int CA>
-__global__ void __launch_bounds__(kPatchLines, 1)
-    k_pencil_sweep(const PencilSweepArgs<R> A) {
+__device__ __forceinline__ void pencil_sweep_run(const PencilSweepArgs<R>& A, int nblocks) {
   constexpr int CL = CC * CA;
   constexpr bool BWD = MODE == kBackward;
   constexpr int PW = MODE == kFactor ? 2 : 1;  // values sent across an edge
@@ -688,13 +690,49 @@ __global__ void __launch_bounds__(kPatchLines, 1)
   }  // run
   // every CTA counts, running or not; the last one reduces the partials
   if (A.done_ctr && A.part && ((MODE == kForward && UPD) || MODE == kBackward) &&
-      last_block(A.done_ctr, (int)gridDim.x)) {
+      last_block(A.done_ctr, nblocks)) {
     if (MODE == kForward)
       red_conv_body(A.part, A.npart, A.sc, red);
     else
       red_beta_body(A.part, A.npart, A.sc, red, A.red_init);
   }
   if (CL > 1) cluster_sync();
+}
+
+template <typename R, int MODE, bool UPD, int CC, int CA>
+__global__ void __launch_bounds__(kPatchLines, 1)
+    k_pencil_sweep(const PencilSweepArgs<R> A) {
+  pencil_sweep_run<R, MODE, UPD, CC, CA>(A, (int)gridDim.x);
+}
+
+// The solve of block b in a launch over several solves: first[] holds each
+// solve's first block (first[n] = the grid), so b lies in [first[s],
+// first[s + 1]).
+__device__ inline int batch_solve_of(const int* __restrict__ first, int n, int b) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(first + mid) <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// One sweep launch over several solves (the shared solve of a batch of
+// scenes): solve s owns first[s + 1] - first[s] CTAs (its patches, plain
+// form) and its arguments come from tab[s].  Launch k of a chunk advances
+// each solve's edge-word epoch by k and its ticket base by k launches of its
+// patches, as k separate launches would.
+template <typename R, int MODE, bool UPD>
+__global__ void __launch_bounds__(kPatchLines, 1)
+    k_pencil_sweep_batch(const PencilSweepArgs<R>* __restrict__ tab, const int* __restrict__ first,
+                         int nsolve, int k) {
+  const int s = batch_solve_of(first, nsolve, (int)blockIdx.x);
+  PencilSweepArgs<R> A = tab[s];
+  const int nb = __ldg(first + s + 1) - __ldg(first + s);
+  A.epoch += (unsigned)k;
+  A.ticket_base += k * nb;
+  pencil_sweep_run<R, MODE, UPD, 1, 1>(A, nb);
 }
 
 // x += alpha s (the update of the last PCG iteration, which no SpMV follows)
@@ -761,6 +799,50 @@ __device__ inline PlNbr pl_nbr(const PencilGeom& G, const PlCell& c, long long e
 //
 // The previous iteration's x += alpha s_old is applied here too (alpha is
 // still the previous iteration's when this kernel runs; 0 before the first).
+//
+// Block bid of nblk: the arithmetic of k_pl_spmv_s (below) for one solve of a
+// launch over several solves (k_pl_spmv_batch).
+template <typename R>
+__device__ __forceinline__ void pl_spmv_run(
+    const PencilGeom& G, const R* __restrict__ AD, const R* __restrict__ AS,
+    const R* __restrict__ AA, const R* __restrict__ AC, const R* __restrict__ z,
+    const R* __restrict__ sold, R* __restrict__ snew, R* __restrict__ q, R* __restrict__ x,
+    double* __restrict__ sc, double* __restrict__ partial, int* __restrict__ done_ctr, int bid,
+    int nblk) {
+  __shared__ double sm[kRedThreads];
+  if (*(const int*)(sc + S_DONE)) return;
+  const R be = (R)sc[S_BETA];
+  const R al = (R)sc[S_ALPHA];
+  double acc = 0;
+  const int nrow = (int)(G.npatch * G.R);
+  for (int row = bid; row < nrow; row += nblk) {
+    const long long e = (long long)row * kPatchLines + threadIdx.x;
+    const PlCell c = pl_cell(G, row, threadIdx.x);
+    if (!c.live) continue;
+    const PlNbr n = pl_nbr(G, c, e);
+    R r = 0;
+    if (n.mc >= 0) r += AC[n.mc] * (z[n.mc] + be * sold[n.mc]);
+    if (n.ma >= 0) r += AA[n.ma] * (z[n.ma] + be * sold[n.ma]);
+    if (n.ms >= 0) r += AS[n.ms] * (z[n.ms] + be * sold[n.ms]);
+    const R so = sold[e];
+    x[e] = x[e] + al * so;
+    const R sn = z[e] + be * so;
+    r += AD[e] * sn;
+    if (n.ps >= 0) r += AS[e] * (z[n.ps] + be * sold[n.ps]);
+    if (n.pa >= 0) r += AA[e] * (z[n.pa] + be * sold[n.pa]);
+    if (n.pc >= 0) r += AC[e] * (z[n.pc] + be * sold[n.pc]);
+    snew[e] = sn;
+    q[e] = r;
+    acc += (double)sn * (double)r;
+  }
+  acc = block_sum<double>(acc, sm);
+  if (threadIdx.x == 0) partial[bid] = acc;
+  // the last block: alpha = rho / s.q (k_red_alpha's body)
+  if (done_ctr && last_block(done_ctr, nblk)) red_alpha_body(partial, nblk, sc, sm);
+}
+
+// (written out rather than through pl_spmv_run: the launch alone ran about
+// 10 % slower through the shared body)
 template <typename R>
 __global__ void __launch_bounds__(kRedThreads, sizeof(R) == 4 ? 8 : 4)
     k_pl_spmv_s(PencilGeom G, const R* __restrict__ AD, const R* __restrict__ AS,
@@ -799,6 +881,57 @@ __global__ void __launch_bounds__(kRedThreads, sizeof(R) == 4 ? 8 : 4)
   // the last block: alpha = rho / s.q (k_red_alpha's body)
   if (done_ctr && last_block(done_ctr, (int)gridDim.x))
     red_alpha_body(partial, (int)gridDim.x, sc, sm);
+}
+
+// Blocks of k_pl_spmv_s for a layout: about four rows per block, at most the
+// resident capacity (kPlSpmvBlocks32).  The partial sums of s.q follow the
+// block count, so a solve alone and in a launch over several solves use this
+// same count and give the same bits.
+__host__ __device__ inline int pl_spmv_blocks(const PencilGeom& G) {
+  const long long nrow = G.npatch * G.R;
+  const long long b = (nrow + 3) / 4;
+  return (int)(b < 1 ? 1 : (b > kPlSpmvBlocks32 ? kPlSpmvBlocks32 : b));
+}
+
+// One SpMV launch over several solves: solve s owns first[s + 1] - first[s]
+// blocks; iteration it of a chunk takes s_old / s_new from s0 / s1 by the
+// solve's iteration parity.
+template <typename R>
+struct PlSpmvArgs {
+  PencilGeom G;
+  const R* AD;
+  const R* AS;
+  const R* AA;
+  const R* AC;
+  const R* z;
+  R* s0;
+  R* s1;
+  R* q;
+  R* x;
+  double* sc;
+  double* part;
+  int* done_ctr;
+  int parity;  // iterations the solve ran before the chunk, mod 2
+};
+
+template <typename R>
+__global__ void __launch_bounds__(kRedThreads, sizeof(R) == 4 ? 6 : 3)
+    k_pl_spmv_batch(const PlSpmvArgs<R>* __restrict__ tab, const int* __restrict__ first,
+                    int nsolve, int it) {
+  const int s = batch_solve_of(first, nsolve, (int)blockIdx.x);
+  const PlSpmvArgs<R>& a = tab[s];
+  const int b0 = __ldg(first + s);
+  const bool odd = ((a.parity + it) & 1) != 0;
+  pl_spmv_run<R>(a.G, a.AD, a.AS, a.AA, a.AC, a.z, odd ? a.s1 : a.s0, odd ? a.s0 : a.s1, a.q,
+                 a.x, a.sc, a.part, a.done_ctr, (int)blockIdx.x - b0, __ldg(first + s + 1) - b0);
+}
+
+// status[6 s + j] = sc_s[S_RES + j] (residual, beta, tolerance, iteration,
+// iteration limit, done) for each solve of a chunk
+__global__ void k_pl_batch_status(double* const* __restrict__ scs, int nsolve,
+                                  double* __restrict__ status) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < 6 * nsolve) status[i] = __ldcg(scs[i / 6] + S_RES + i % 6);
 }
 
 // k_pl_spmv_s's arithmetic, streamed: block (patch p, chunk k) walks rows

@@ -4,8 +4,12 @@
 
 #include <algorithm>
 #include <atomic>
+#include <climits>
 #include <cmath>
+#include <condition_variable>
 #include <cstring>
+#include <mutex>
+#include <thread>
 #include <vector>
 
 #include "wcg_context.h"
@@ -59,7 +63,11 @@ cudaError_t ctx_init(Context& c) {
   WCG_TRY(cudaStreamCreateWithFlags(&c.in_stream, cudaStreamNonBlocking));
   WCG_TRY(cudaEventCreateWithFlags(&c.ev_staged, cudaEventDisableTiming));
   WCG_TRY(cudaEventCreateWithFlags(&c.ev_loaded, cudaEventDisableTiming));
+  WCG_TRY(cudaEventCreateWithFlags(&c.ev_ss_ready, cudaEventDisableTiming));
+  WCG_TRY(cudaEventCreateWithFlags(&c.ev_ss_done, cudaEventDisableTiming));
   WCG_TRY(cudaMallocHost((void**)&c.hscalars, 64 * sizeof(double)));
+  WCG_TRY(cudaHostAlloc((void**)&c.hmap, kReadSmallBytes, cudaHostAllocMapped));
+  WCG_TRY(cudaHostGetDevicePointer((void**)&c.hmap_dev, c.hmap, 0));
   WCG_TRY(c.dscalars.ensure(64 * sizeof(double)));
   WCG_TRY(c.derr.ensure(sizeof(int)));
   WCG_TRY(c.ticket.ensure(16 * sizeof(int)));
@@ -88,6 +96,8 @@ void ctx_free(Context& c) {
   for (DevBuf* b : bufs) b->release();
   if (c.hscalars) cudaFreeHost(c.hscalars);
   c.hscalars = nullptr;
+  if (c.hmap) cudaFreeHost(c.hmap);
+  c.hmap = c.hmap_dev = nullptr;
   for (Context::ProfRec& r : c.prof_recs) {
     cudaEventDestroy(r.a);
     cudaEventDestroy(r.b);
@@ -108,6 +118,9 @@ void ctx_free(Context& c) {
   if (c.ev_staged) cudaEventDestroy(c.ev_staged);
   if (c.ev_loaded) cudaEventDestroy(c.ev_loaded);
   c.ev_staged = c.ev_loaded = nullptr;
+  if (c.ev_ss_ready) cudaEventDestroy(c.ev_ss_ready);
+  if (c.ev_ss_done) cudaEventDestroy(c.ev_ss_done);
+  c.ev_ss_ready = c.ev_ss_done = nullptr;
   if (c.ev_store) cudaEventDestroy(c.ev_store);
   if (c.ev_d2h) cudaEventDestroy(c.ev_d2h);
   c.ev_store = c.ev_d2h = nullptr;
@@ -138,6 +151,23 @@ ProfScope::~ProfScope() {
   }
   cudaEventRecord(b, c.stream);
   c.prof_recs.push_back({cat, (int)(c.launches - l0), a, b});
+}
+
+__global__ void k_read_words(const unsigned* __restrict__ src, unsigned* __restrict__ dst,
+                             int nwords) {
+  for (int i = threadIdx.x; i < nwords; i += blockDim.x) dst[i] = src[i];
+}
+
+cudaError_t read_small(Context& c, const void* d, size_t bytes, void* h) {
+  if (bytes == 0) return cudaSuccess;
+  if (bytes % 4 != 0 || bytes > kReadSmallBytes || ((size_t)d & 3) != 0)
+    return cudaErrorInvalidValue;
+  ++c.launches, k_read_words<<<1, 128, 0, c.stream>>>(static_cast<const unsigned*>(d),
+                                                       c.hmap_dev, (int)(bytes / 4));
+  WCG_TRY(cudaGetLastError());
+  WCG_TRY(cudaStreamSynchronize(c.stream));
+  std::memcpy(h, c.hmap, bytes);
+  return cudaSuccess;
 }
 
 // ---------------------------------------------------------------------------
@@ -570,8 +600,7 @@ static cudaError_t build_grid_t(Context& c) {
                                                                       part + kRedBlocks * 6);
   ++c.launches, k_minmax_final<<<1, 32, 0, c.stream>>>(part, ne > 0 ? 2 * kRedBlocks : kRedBlocks,
                                                         dsc);
-  WCG_TRY(cudaMemcpyAsync(c.hscalars, dsc, 6 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
-  WCG_TRY(cudaStreamSynchronize(c.stream));
+  WCG_TRY(read_small(c, dsc, 6 * sizeof(double), c.hscalars));
   double bbmin[3] = {1e20, 1e20, 1e20}, bbmax[3] = {-1e20, -1e20, -1e20};
   if (n + ne > 0)
     for (int a = 0; a < 3; ++a) {
@@ -701,8 +730,7 @@ static cudaError_t build_grid_t(Context& c) {
   exclusive_scan<int, int>(ttmp, ntot, ttmp, (int*)part, dtotal + 1, c.stream);
   ++c.launches, k_compact<<<nblk(ntot, 256), 256, 0, c.stream>>>(
       c.tile_active.as<unsigned char>(), ttmp, ntot, tlist);
-  WCG_TRY(cudaMemcpyAsync(c.hscalars + 8, dsc + 8, 9 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
-  WCG_TRY(cudaStreamSynchronize(c.stream));
+  WCG_TRY(read_small(c, dsc + 8, 9 * sizeof(double), c.hscalars + 8));
   {
     const int* hr = (const int*)(c.hscalars + 8);
     c.n_active = *(const int*)(c.hscalars + 16);
@@ -1033,8 +1061,7 @@ static void absmax(Context& c, const R* a, double* out) {
 }
 
 static cudaError_t fetch(Context& c, const double* d, int k, double* h) {
-  WCG_TRY(cudaMemcpyAsync(h, d, k * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
-  return cudaStreamSynchronize(c.stream);
+  return read_small(c, d, (size_t)k * sizeof(double), h);
 }
 
 static cudaError_t set_scalars(Context& c, int slot, const double* v, int k) {
@@ -1451,6 +1478,247 @@ static cudaError_t pl_sweep(Context& c, PencilSweepArgs<R> a) {
   return pl_sweep_cl<R, MODE, UPD, 1, 1>(c, a);
 }
 
+// ---------------------------------------------------------------------------
+// The shared solve of a batch (no reference counterpart: the reference steps
+// one scene per process).  Every context of a batch step that reaches the
+// iterations of its pressure solve hands them to the batch's coordinator
+// thread and waits; the coordinator runs the iterations of all waiting solves
+// of one precision as one launch per kernel (SpMV, forward sweep, backward
+// sweep), chunks of kSharedChunk iterations, reads every solve's status once
+// per chunk, releases the converged ones and admits new ones between chunks.
+// Each solve's arithmetic, block counts and partial sums are those it has
+// alone, so results are bit-identical.
+
+constexpr int kSharedChunk = 8;
+
+struct SolveReq {
+  Context* c = nullptr;
+  int prec = 0;  // 0: FP64, 1: FP32
+  PencilSweepArgs<double> fa64{}, ba64{};
+  PencilSweepArgs<float> fa32{}, ba32{};
+  PlSpmvArgs<double> sa64{};
+  PlSpmvArgs<float> sa32{};
+  int npatch = 0, nspmv = 0;
+  int launched = 0;  // iterations launched so far
+  bool finished = false;
+  cudaError_t cerr = cudaSuccess;
+  double status[6] = {};
+};
+
+struct SharedSolve {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::mutex m;
+  std::condition_variable cv;       // the coordinator: requests or stop
+  std::condition_variable cv_done;  // the requesters: a request finished
+  std::vector<SolveReq*> queue, active;
+  bool stop = false;
+  std::thread th;
+  DevBuf dtab;                    // argument tables, block offsets, status
+  unsigned char* hpin = nullptr;  // their pinned host image
+  size_t hpin_bytes = 0;
+  std::atomic<long long> launches{0};
+};
+
+static size_t ss_align(size_t b) { return (b + 255) & ~(size_t)255; }
+
+template <typename R>
+static PencilSweepArgs<R>& ss_fa(SolveReq& q);
+template <>
+PencilSweepArgs<double>& ss_fa<double>(SolveReq& q) { return q.fa64; }
+template <>
+PencilSweepArgs<float>& ss_fa<float>(SolveReq& q) { return q.fa32; }
+template <typename R>
+static PencilSweepArgs<R>& ss_ba(SolveReq& q);
+template <>
+PencilSweepArgs<double>& ss_ba<double>(SolveReq& q) { return q.ba64; }
+template <>
+PencilSweepArgs<float>& ss_ba<float>(SolveReq& q) { return q.ba32; }
+template <typename R>
+static PlSpmvArgs<R>& ss_sa(SolveReq& q);
+template <>
+PlSpmvArgs<double>& ss_sa<double>(SolveReq& q) { return q.sa64; }
+template <>
+PlSpmvArgs<float>& ss_sa<float>(SolveReq& q) { return q.sa32; }
+
+// One chunk of kSharedChunk iterations over the solves L (one precision).
+template <typename R>
+static cudaError_t ss_chunk(SharedSolve& S, const std::vector<SolveReq*>& L) {
+  const int n = (int)L.size();
+  const size_t o_sa = 0;
+  const size_t o_fa = o_sa + ss_align(n * sizeof(PlSpmvArgs<R>));
+  const size_t o_ba = o_fa + ss_align(n * sizeof(PencilSweepArgs<R>));
+  const size_t o_f1 = o_ba + ss_align(n * sizeof(PencilSweepArgs<R>));
+  const size_t o_f2 = o_f1 + ss_align((n + 1) * sizeof(int));
+  const size_t o_sc = o_f2 + ss_align((n + 1) * sizeof(int));
+  const size_t o_st = o_sc + ss_align(n * sizeof(double*));
+  const size_t bytes = o_st + ss_align(6 * n * sizeof(double));
+  WCG_TRY(S.dtab.ensure(bytes));
+  if (bytes > S.hpin_bytes) {
+    if (S.hpin) cudaFreeHost(S.hpin);
+    S.hpin = nullptr;
+    S.hpin_bytes = 0;
+    WCG_TRY(cudaMallocHost((void**)&S.hpin, bytes));
+    S.hpin_bytes = bytes;
+  }
+  auto* sa = reinterpret_cast<PlSpmvArgs<R>*>(S.hpin + o_sa);
+  auto* fa = reinterpret_cast<PencilSweepArgs<R>*>(S.hpin + o_fa);
+  auto* ba = reinterpret_cast<PencilSweepArgs<R>*>(S.hpin + o_ba);
+  int* f1 = reinterpret_cast<int*>(S.hpin + o_f1);
+  int* f2 = reinterpret_cast<int*>(S.hpin + o_f2);
+  double** scs = reinterpret_cast<double**>(S.hpin + o_sc);
+  long long n1 = 0, n2 = 0;
+  for (int i = 0; i < n; ++i) {
+    SolveReq& q = *L[(size_t)i];
+    Context& c = *q.c;
+    sa[i] = ss_sa<R>(q);
+    sa[i].parity = q.launched & 1;
+    fa[i] = ss_fa<R>(q);
+    ba[i] = ss_ba<R>(q);
+    // launch k of the chunk (forward 2b, backward 2b + 1) adds k to these
+    fa[i].epoch = ba[i].epoch = (unsigned)(c.tile_epoch + 1);
+    fa[i].ticket_base = ba[i].ticket_base = c.pl_tickets;
+    f1[i] = (int)n1;
+    f2[i] = (int)n2;
+    n1 += q.nspmv;
+    n2 += q.npatch;
+    scs[i] = c.dscalars.as<double>();
+  }
+  if (n1 > INT_MAX || n2 > INT_MAX) return cudaErrorInvalidValue;
+  f1[n] = (int)n1;
+  f2[n] = (int)n2;
+  unsigned char* d = S.dtab.as<unsigned char>();
+  WCG_TRY(cudaMemcpyAsync(d, S.hpin, o_st, cudaMemcpyHostToDevice, S.stream));
+  const auto* dsa = reinterpret_cast<const PlSpmvArgs<R>*>(d + o_sa);
+  const auto* dfa = reinterpret_cast<const PencilSweepArgs<R>*>(d + o_fa);
+  const auto* dba = reinterpret_cast<const PencilSweepArgs<R>*>(d + o_ba);
+  const int* df1 = reinterpret_cast<const int*>(d + o_f1);
+  const int* df2 = reinterpret_cast<const int*>(d + o_f2);
+  double* const* dsc = reinterpret_cast<double* const*>(d + o_sc);
+  double* dst = reinterpret_cast<double*>(d + o_st);
+  const size_t smf = sweep_dyn_smem<R>(kForward, true), smb = sweep_dyn_smem<R>(kBackward, false);
+  static std::atomic<unsigned long long> attr_set{0};
+  const unsigned long long dbit = 1ull << (S.device & 63);
+  if (!(attr_set.load(std::memory_order_acquire) & dbit)) {
+    WCG_TRY(cudaFuncSetAttribute(k_pencil_sweep_batch<R, kForward, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smf));
+    WCG_TRY(cudaFuncSetAttribute(k_pencil_sweep_batch<R, kBackward, false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smb));
+    attr_set.fetch_or(dbit, std::memory_order_release);
+  }
+  for (int b = 0; b < kSharedChunk; ++b) {
+    k_pl_spmv_batch<R><<<(unsigned)n1, kRedThreads, 0, S.stream>>>(dsa, df1, n, b);
+    k_pencil_sweep_batch<R, kForward, true><<<(unsigned)n2, kPatchLines, smf, S.stream>>>(
+        dfa, df2, n, 2 * b);
+    k_pencil_sweep_batch<R, kBackward, false><<<(unsigned)n2, kPatchLines, smb, S.stream>>>(
+        dba, df2, n, 2 * b + 1);
+  }
+  k_pl_batch_status<<<(unsigned)((6 * n + 255) / 256), 256, 0, S.stream>>>(dsc, n, dst);
+  WCG_TRY(cudaGetLastError());
+  S.launches += 3 * kSharedChunk + 1;
+  double* hst = reinterpret_cast<double*>(S.hpin + o_st);
+  WCG_TRY(cudaMemcpyAsync(hst, dst, 6 * n * sizeof(double), cudaMemcpyDeviceToHost, S.stream));
+  WCG_TRY(cudaStreamSynchronize(S.stream));
+  for (int i = 0; i < n; ++i) {
+    SolveReq& q = *L[(size_t)i];
+    Context& c = *q.c;
+    c.tile_epoch += 2 * kSharedChunk;
+    c.pl_tickets += 2 * kSharedChunk * q.npatch;
+    q.launched += kSharedChunk;
+    std::memcpy(q.status, hst + 6 * i, sizeof(q.status));
+  }
+  return cudaSuccess;
+}
+
+static bool ss_done(const SolveReq& q) {
+  int done = 0;
+  std::memcpy(&done, &q.status[5], sizeof(int));
+  return done != 0;
+}
+
+static void ss_loop(SharedSolve* S) {
+  cudaSetDevice(S->device);
+  std::unique_lock<std::mutex> lk(S->m);
+  for (;;) {
+    S->cv.wait(lk, [&] { return S->stop || !S->queue.empty() || !S->active.empty(); });
+    if (S->active.empty() && S->queue.empty()) break;  // stop
+    for (SolveReq* q : S->queue) {
+      // the chunk's launches follow the solve's own work on its stream
+      const cudaError_t e = cudaStreamWaitEvent(S->stream, q->c->ev_ss_ready, 0);
+      if (e != cudaSuccess) q->cerr = e;
+      S->active.push_back(q);
+    }
+    S->queue.clear();
+    std::vector<SolveReq*> act = S->active;
+    lk.unlock();
+    std::vector<SolveReq*> L64, L32;
+    for (SolveReq* q : act)
+      if (q->cerr == cudaSuccess) (q->prec == 0 ? L64 : L32).push_back(q);
+    cudaError_t e = cudaSuccess;
+    if (!L64.empty()) e = ss_chunk<double>(*S, L64);
+    if (e == cudaSuccess && !L32.empty()) e = ss_chunk<float>(*S, L32);
+    lk.lock();
+    std::vector<SolveReq*> keep;
+    for (SolveReq* q : act) {
+      if (e != cudaSuccess && q->cerr == cudaSuccess) q->cerr = e;
+      if (q->cerr != cudaSuccess || ss_done(*q)) {
+        // the solve's stream waits for its last iterations
+        const cudaError_t r = cudaEventRecord(q->c->ev_ss_done, S->stream);
+        if (r != cudaSuccess && q->cerr == cudaSuccess) q->cerr = r;
+        q->finished = true;
+      } else {
+        keep.push_back(q);
+      }
+    }
+    S->active.swap(keep);
+    S->cv_done.notify_all();
+  }
+}
+
+// Called by a context in its pressure solve: waits until the coordinator
+// has run the solve's iterations to convergence (or the iteration limit).
+static cudaError_t shared_solve_run(SharedSolve& S, SolveReq& q) {
+  std::unique_lock<std::mutex> lk(S.m);
+  S.queue.push_back(&q);
+  S.cv.notify_one();
+  S.cv_done.wait(lk, [&] { return q.finished; });
+  return q.cerr;
+}
+
+SharedSolve* shared_solve_create(int device, std::string* err) {
+  SharedSolve* S = new SharedSolve();
+  S->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    if (err) *err = cudaGetErrorString(e);
+    delete S;
+    return nullptr;
+  }
+  S->th = std::thread(ss_loop, S);
+  return S;
+}
+
+void shared_solve_destroy(SharedSolve* S) {
+  if (!S) return;
+  {
+    std::lock_guard<std::mutex> lk(S->m);
+    S->stop = true;
+  }
+  S->cv.notify_all();
+  if (S->th.joinable()) S->th.join();
+  cudaSetDevice(S->device);
+  if (S->stream) {
+    cudaStreamSynchronize(S->stream);
+    cudaStreamDestroy(S->stream);
+  }
+  S->dtab.release();
+  if (S->hpin) cudaFreeHost(S->hpin);
+  delete S;
+}
+
+long long shared_solve_launches(const SharedSolve* S) { return S ? S->launches.load() : 0; }
+
 // PCGSolver<T>::solve (PCGSolver.h:260-308) in the pencil layout on the
 // factored system: A x = r from x = 0; r is overwritten with the residual.
 template <typename R>
@@ -1513,14 +1781,47 @@ static cudaError_t pl_pcg(Context& c, R* r, R* x, double tol_abs, int maxiters, 
       G.R, std::max<long long>(1, (4 * kPlSpmvBlocks32 + G.npatch - 1) / G.npatch));
   const int rows_per_chunk = (G.R + nchunk - 1) / nchunk;
   const int spmv_blocks = (int)(G.npatch * nchunk);
-  WCG_TRY(ensure_scratch(c, (size_t)spmv_blocks * sizeof(double)));
+  const int rows_blocks = pl_spmv_blocks(G);
+  WCG_TRY(ensure_scratch(c, (size_t)std::max(spmv_blocks, rows_blocks) * sizeof(double)));
   part = c.scratch.as<double>();
+  if (c.shared_solve && c.spmv_rows) {
+    // the iterations run in the batch's shared launches
+    SolveReq req;
+    req.c = &c;
+    req.prec = c.prm.precision == 0 ? 0 : 1;
+    ss_fa<R>(req) = fa;
+    ss_ba<R>(req) = ba;
+    PlSpmvArgs<R>& sa = ss_sa<R>(req);
+    sa.G = G;
+    sa.AD = AD;
+    sa.AS = AS;
+    sa.AA = AA;
+    sa.AC = AC;
+    sa.z = z;
+    sa.s0 = s0;
+    sa.s1 = s1;
+    sa.q = q;
+    sa.x = x;
+    sa.sc = sc;
+    sa.part = part;
+    sa.done_ctr = c.ticket.as<int>() + 2;
+    req.npatch = (int)G.npatch;
+    req.nspmv = rows_blocks;
+    WCG_TRY(cudaEventRecord(c.ev_ss_ready, c.stream));
+    WCG_TRY(shared_solve_run(*c.shared_solve, req));
+    WCG_TRY(cudaStreamWaitEvent(c.stream, c.ev_ss_done, 0));
+    int done = 0;
+    std::memcpy(&done, &req.status[5], sizeof(int));
+    *res = req.status[0];
+    *iters = (int)req.status[3];
+    *conv = done == 1 ? 1 : 0;
+  } else {
   for (;;) {
     for (int b = 0; b < c.pcg_batch; ++b) {
       {
         ProfScope prof(c, P_PCGVEC);
         if (c.spmv_rows) {  // its last block forms alpha
-          ++c.launches, k_pl_spmv_s<R><<<kPlSpmvBlocks32, kRedThreads, 0, c.stream>>>(
+          ++c.launches, k_pl_spmv_s<R><<<rows_blocks, kRedThreads, 0, c.stream>>>(
               G, AD, AS, AA, AC, z, sold, snew, q, x, sc, part, c.ticket.as<int>() + 2);
         } else {
           ++c.launches, k_pl_spmv_stream<R><<<spmv_blocks, kRedThreads, 0, c.stream>>>(
@@ -1542,6 +1843,7 @@ static cudaError_t pl_pcg(Context& c, R* r, R* x, double tol_abs, int maxiters, 
       *conv = done == 1 ? 1 : 0;
       break;
     }
+  }
   }
   // x += alpha s of the last iteration (iteration i searched along s1 for even
   // i, s0 for odd i; later launches of the batch returned early)
@@ -1947,9 +2249,7 @@ static cudaError_t solve_assembled_t(Context& c) {
     ++c.launches, k_dof_box<<<kRedBlocks, kRedThreads, 0, c.stream>>>(c.g, al, nent, dof, dbox, part);
     ++c.launches, k_reduce_sum<<<1, kRedThreads, 0, c.stream>>>(part, kRedBlocks, dsc + 5);
   }
-  WCG_TRY(cudaMemcpyAsync(c.hscalars + 4, dsc + 4, 31 * sizeof(double), cudaMemcpyDeviceToHost,
-                          c.stream));
-  WCG_TRY(cudaStreamSynchronize(c.stream));
+  WCG_TRY(read_small(c, dsc + 4, 31 * sizeof(double), c.hscalars + 4));
   h[0] = c.hscalars[4];
   h[1] = c.hscalars[5];
   int box[6];
@@ -2543,8 +2843,7 @@ static cudaError_t remove_flagged_t(Context& c, long long n, int* alive_slot, in
   int* dtot = (int*)(c.dscalars.as<double>() + 48);
   exclusive_scan<int, int>(alive_slot, n, alive_slot, c.scratch.as<int>(), dtot, c.stream);
   int K = 0;
-  WCG_TRY(cudaMemcpyAsync(&K, dtot, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
-  WCG_TRY(cudaStreamSynchronize(c.stream));
+  WCG_TRY(read_small(c, dtot, sizeof(int), &K));
   c.have_grid = false;  // volumes, masses and radii changed
   c.xw_valid = false;
   if (K == n) return cudaGetLastError();
@@ -2554,12 +2853,11 @@ static cudaError_t remove_flagged_t(Context& c, long long n, int* alive_slot, in
   exclusive_scan<int, int>(high_rank, n, high_rank, c.scratch.as<int>(), dtot + 1, c.stream);
   ++c.launches, k_merge_holes<<<nblk(n, 256), 256, 0, c.stream>>>(n, K, alive_pid, hole_rank, holes);
   int counts[2] = {0, 0};
-  WCG_TRY(cudaMemcpyAsync(counts, dtot, 2 * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
   // surviving slots: alive_slot now holds their ranks; the flags come back
   // from alive_pid through pid
   ++c.launches, k_merge_alive_slots<<<nblk(n, 256), 256, 0, c.stream>>>(n, pid, alive_pid, cursor);
   ++c.launches, k_merge_compact<<<nblk(n, 256), 256, 0, c.stream>>>(n, cursor, alive_slot, list);
-  WCG_TRY(cudaStreamSynchronize(c.stream));
+  WCG_TRY(read_small(c, dtot, 2 * sizeof(int), counts));  // (the two kernels leave dtot)
   const int nxt = c.cur ^ 1;
   ++c.launches, k_gather_particles<R><<<nblk(K, 256), 256, 0, c.stream>>>(
       list, K, cap, P, c.pbuf[nxt].as<R>(), pid, c.pid[nxt].as<int>(),
@@ -2745,8 +3043,7 @@ static cudaError_t split_count_t(Context& c, int* total, long long* nparents) {
   }
   exclusive_scan<int, int>(off_pid, n, off_pid, c.scratch.as<int>(), dtot, c.stream);
   int tot[2] = {0, 0};
-  WCG_TRY(cudaMemcpyAsync(tot, dtot, sizeof(tot), cudaMemcpyDeviceToHost, c.stream));
-  WCG_TRY(cudaStreamSynchronize(c.stream));
+  WCG_TRY(read_small(c, dtot, sizeof(tot), tot));
   *total = tot[0];
   if (nparents) *nparents = tot[1];
   return cudaGetLastError();

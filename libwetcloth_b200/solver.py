@@ -417,6 +417,15 @@ class FluidBatch:
             check(rc)
         return list(st)
 
+    def set_shared_solve(self, on=True):
+        """Run the scenes' PCG iterations in shared launches over all scenes
+        waiting in their solve (results unchanged)."""
+        check(self.L.wcg_batch_set_shared_solve(self.h, 1 if on else 0))
+
+    @property
+    def shared_launches(self):
+        return int(self.L.wcg_batch_shared_launches(self.h))
+
     @property
     def threads(self):
         return self.L.wcg_batch_threads(self.h)

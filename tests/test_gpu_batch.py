@@ -134,3 +134,46 @@ def test_schedule_arguments(wcg):
             g.schedule = bad
     assert g.schedule == (9, 1, 32)
     g.close()
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_shared_solve_matches_alone(mixed, wcg):
+    """The shared solve (the PCG iterations of all scenes waiting in their
+    pressure solve run as one launch per kernel) changes no result: every
+    scene after three batch steps is bit-identical to three steps alone.
+    Scenes of uneven size; FP32 + refinement, and a batch mixing FP64 and
+    FP32 scenes (two shared launch sets); some scenes on cluster schedules,
+    whose sweeps outside the iterations keep them."""
+    specs = scenes.batch_scenes(6, 13, (24, 72), (5000, 150000))
+    precs = [(_capi.WCG_FP64 if (mixed and k % 2) else _capi.WCG_FP32_REFINE)
+             for k in range(len(specs))]
+    alone = []
+    for sc, pr in zip(specs, precs):
+        g = FluidScene(sc, precision=pr)
+        for _ in range(3):
+            g.step(DT)
+        alone.append((g.download(), g.stats()["pcg_iters"]))
+        g.close()
+    gs = [FluidScene(sc, precision=pr) for sc, pr in zip(specs, precs)]
+    for k, g in enumerate(gs):
+        if k % 3 == 1:
+            g.schedule = (2, 1, 4)
+    b = FluidBatch(gs)
+    b.threads = 4
+    b.set_shared_solve(True)
+    st = b.step(DT, nsteps=3)
+    assert all(s == _capi.WCG_OK for s in st), st
+    assert b.shared_launches > 0
+    for g, (ref, it) in zip(gs, alone):
+        assert g.stats()["pcg_iters"] == it
+        for a, r in zip(g.download(), ref):
+            assert np.array_equal(a, r)
+    # off again: the scenes solve alone
+    b.set_shared_solve(False)
+    n0 = b.shared_launches
+    st = b.step(DT)
+    assert all(s == _capi.WCG_OK for s in st), st
+    assert b.shared_launches == n0
+    b.close()
+    for g in gs:
+        g.close()
