@@ -75,6 +75,15 @@ def test_argument_errors_without_device():
     assert L.wcg_step(None, 1e-3, None) == _capi.WCG_ERR_ARG
     assert L.wcg_rebucketize_and_resample(None) == _capi.WCG_ERR_ARG
     assert L.wcg_num_particles(None) == -1
+    # schedules and batches: null handles refused before any device work
+    sched = _capi.WcgSchedule(1, 1, 8)
+    assert L.wcg_set_schedule(None, ctypes.byref(sched)) == _capi.WCG_ERR_ARG
+    assert L.wcg_get_schedule(None, ctypes.byref(sched)) == _capi.WCG_ERR_ARG
+    assert L.wcg_batch_set_shared_solve(None, 1) == _capi.WCG_ERR_ARG
+    assert L.wcg_batch_shared_launches(None) == -1
+    assert L.wcg_batch_autotune_schedules(None, None, None, 0, 1, None, None) == _capi.WCG_ERR_ARG
+    b = ctypes.c_void_p()
+    assert L.wcg_batch_create(0, None, ctypes.byref(b)) == _capi.WCG_ERR_ARG
 
 
 def test_noalloc_size_limit_checked_before_device_work():
