@@ -388,7 +388,8 @@ cudaError_t load_staged(Context& c);
 // bytes a multiple of 4, at most kReadSmallBytes): a kernel on `stream`
 // stores them into mapped pinned memory, then the stream is synchronised.
 // No copy engine is involved, so a large read-back running on copy_stream
-// cannot hold them back.
+// cannot hold them back.  A context without the mapped words (hmap null:
+// one not set up by ctx_init) reads with a plain copy instead.
 constexpr size_t kReadSmallBytes = 4096;
 cudaError_t read_small(Context& c, const void* d, size_t bytes, void* h);
 // The shared solve of a batch of contexts on one device: a coordinator thread

@@ -160,6 +160,12 @@ __global__ void k_read_words(const unsigned* __restrict__ src, unsigned* __restr
 
 cudaError_t read_small(Context& c, const void* d, size_t bytes, void* h) {
   if (bytes == 0) return cudaSuccess;
+  if (!c.hmap || !c.hmap_dev) {
+    // a context without the mapped words (the allocation-free solve builds
+    // its context from caller memory and allocates nothing): a plain copy
+    WCG_TRY(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, c.stream));
+    return cudaStreamSynchronize(c.stream);
+  }
   if (bytes % 4 != 0 || bytes > kReadSmallBytes || ((size_t)d & 3) != 0)
     return cudaErrorInvalidValue;
   ++c.launches, k_read_words<<<1, 128, 0, c.stream>>>(static_cast<const unsigned*>(d),
