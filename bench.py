@@ -505,10 +505,13 @@ def run_batch(args, steps=3):
     """Many independent scenes (grid 32..64 cells, 10k..200k particles,
     seeded densities and viscosities; the many-scenes configuration scaled to
     a short run): aggregate particle-steps/s stepped one after another
-    against the batch (separate streams, host thread pool, thread count
-    autotuned during warm-up), the batch again after each scene's launch
-    schedule is chosen from timed trials, and again with the shared solve
-    (every waiting scene's PCG iterations in one launch per kernel).  Device-synchronised wall time around each
+    against the batch (separate streams, host thread pool), the batch with
+    each scene's launch schedule chosen from timed trials, and the batch
+    with the shared solve (every waiting scene's PCG iterations in one launch
+    per kernel).  The thread count and the schedules are chosen first on a
+    tuning copy of the scenes; every arm then starts from fresh scenes (the
+    same initial state), takes one untimed step and times its passes, so all
+    arms simulate the same steps.  Device-synchronised wall time around each
     whole pass (best of three; one pass each with --batch-full, which runs
     the configuration at its stated size)."""
     import torch
@@ -527,64 +530,67 @@ def run_batch(args, steps=3):
     def make():
         return [FluidScene(sc, precision=WCG_FP32_REFINE) for sc in specs]
 
-    # sequential: one scene after another, each its own steps (best of three
-    # passes when they are short, so host jitter does not dominate)
-    gs = make()
-    for g in gs:
-        g.step(DT)
-    seq_s = float("inf")
-    for _ in range(passes):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for g in gs:
-            for _ in range(steps):
-                g.step(DT)
-        torch.cuda.synchronize()
-        seq_s = min(seq_s, time.perf_counter() - t0)
-    for g in gs:
-        g.close()
-    # batched
+    def timed_passes(step_all):
+        best = float("inf")
+        for _ in range(passes):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            step_all()
+            torch.cuda.synchronize()
+            best = min(best, time.perf_counter() - t0)
+        return best
+
+    # tuning copy: thread count, then each scene's launch schedule
     gs = make()
     b = FluidBatch(gs)
-    b.step(DT)  # first-step allocations outside the autotuning trials
+    b.step(DT)  # first-step allocations outside the trials
     tune = b.autotune(DT, candidates=(1, 2, 4, 8, 16))
-    bat_s = float("inf")
-    for _ in range(passes):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        b.step(DT, nsteps=steps)
-        torch.cuda.synchronize()
-        bat_s = min(bat_s, time.perf_counter() - t0)
     threads = b.threads
-    # per-scene launch schedules from timed trials, then the same passes again
     cands = DEFAULT_SCHEDULES
     chosen, _ = b.autotune_schedules(DT, cands)
-    sched_s = float("inf")
-    for _ in range(passes):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        b.step(DT, nsteps=steps)
-        torch.cuda.synchronize()
-        sched_s = min(sched_s, time.perf_counter() - t0)
+    b.close()
+    for g in gs:
+        g.close()
     hist = {}
     for k in chosen:
         key = "x".join(str(v) for v in cands[k])
         hist[key] = hist.get(key, 0) + 1
-    # the shared solve: the scenes' PCG iterations in shared launches
-    b.set_shared_solve(True)
-    b.step(DT)  # untimed: first use of the shared tables
-    shared_s = float("inf")
-    for _ in range(passes):
-        torch.cuda.synchronize()
-        l0 = b.shared_launches
-        t0 = time.perf_counter()
-        b.step(DT, nsteps=steps)
-        torch.cuda.synchronize()
-        shared_s = min(shared_s, time.perf_counter() - t0)
-        shared_launches = b.shared_launches - l0
-    b.close()
+
+    # sequential: one scene after another, each its own steps
+    gs = make()
+    for g in gs:
+        g.step(DT)
+
+    def seq_all():
+        for g in gs:
+            for _ in range(steps):
+                g.step(DT)
+
+    seq_s = timed_passes(seq_all)
     for g in gs:
         g.close()
+
+    def batch_arm(schedules, shared):
+        gs = make()
+        if schedules:
+            for g, k in zip(gs, chosen):
+                g.schedule = cands[k]
+        b = FluidBatch(gs)
+        b.threads = threads
+        if shared:
+            b.set_shared_solve(True)
+        b.step(DT)
+        l0 = b.shared_launches
+        t = timed_passes(lambda: b.step(DT, nsteps=steps))
+        launches = (b.shared_launches - l0) // passes
+        b.close()
+        for g in gs:
+            g.close()
+        return t, launches
+
+    bat_s, _ = batch_arm(False, False)
+    sched_s, _ = batch_arm(True, False)
+    shared_s, shared_launches = batch_arm(False, True)
     return {"scenes": len(specs), "particles": total_p, "steps": steps,
             "precision": "fp32_refine",
             "sequential_particle_steps_per_s": round(total_p * steps / seq_s, 1),
@@ -599,7 +605,7 @@ def run_batch(args, steps=3):
             "speedup_shared_solve": round(seq_s / shared_s, 3),
             "shared_solve_launches_per_pass": shared_launches,
             "note": f"wall time, device-synchronised, warm-up excluded, best of {passes} "
-                    "pass(es) per arm"}
+                    "pass(es) per arm, every arm from the same initial state"}
 
 
 # ---------------------------------------------------------------------------
