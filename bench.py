@@ -570,7 +570,7 @@ def run_batch(args, steps=3):
     for g in gs:
         g.close()
 
-    def batch_arm(schedules, shared):
+    def batch_arm(schedules, shared, max_patches=None):
         gs = make()
         if schedules:
             for g, k in zip(gs, chosen):
@@ -578,7 +578,7 @@ def run_batch(args, steps=3):
         b = FluidBatch(gs)
         b.threads = threads
         if shared:
-            b.set_shared_solve(True)
+            b.set_shared_solve(True, max_patches=max_patches)
         b.step(DT)
         l0 = b.shared_launches
         t = timed_passes(lambda: b.step(DT, nsteps=steps))
@@ -591,6 +591,9 @@ def run_batch(args, steps=3):
     bat_s, _ = batch_arm(False, False)
     sched_s, _ = batch_arm(True, False)
     shared_s, shared_launches = batch_arm(False, True)
+    # the tuned schedules with the shared solve for the scenes of at most 16
+    # pencil patches (the larger ones iterate alone on their own streams)
+    shared16_s, _ = batch_arm(True, True, 16)
     return {"scenes": len(specs), "particles": total_p, "steps": steps,
             "precision": "fp32_refine",
             "sequential_particle_steps_per_s": round(total_p * steps / seq_s, 1),
@@ -604,6 +607,8 @@ def run_batch(args, steps=3):
             "batched_shared_solve_particle_steps_per_s": round(total_p * steps / shared_s, 1),
             "speedup_shared_solve": round(seq_s / shared_s, 3),
             "shared_solve_launches_per_pass": shared_launches,
+            "batched_tuned_shared16_particle_steps_per_s": round(total_p * steps / shared16_s, 1),
+            "speedup_tuned_shared16": round(seq_s / shared16_s, 3),
             "note": f"wall time, device-synchronised, warm-up excluded, best of {passes} "
                     "pass(es) per arm, every arm from the same initial state"}
 

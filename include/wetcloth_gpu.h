@@ -449,6 +449,11 @@ int wcg_batch_threads(const wcg_batch* b);
  * Needs every scene on one device; the scenes' own sweeps outside the
  * iterations keep their schedules. */
 int wcg_batch_set_shared_solve(wcg_batch* b, int on);
+/* Scenes whose pressure solve spans more than max_patches pencil patches
+ * (16 x 16 lines of the solve's DOF box across its stream axis) iterate
+ * alone instead, so the largest scenes do not set the length of every
+ * shared chunk (default: no limit; results unchanged either way). */
+int wcg_batch_set_shared_solve_limit(wcg_batch* b, int max_patches);
 /* kernel launches the batch's shared solves have made (-1: null batch) */
 long long wcg_batch_shared_launches(const wcg_batch* b);
 /* Times one batch step per candidate thread count (each trial advances every

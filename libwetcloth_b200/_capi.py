@@ -140,6 +140,7 @@ SIGNATURES = {
     "wcg_set_schedule": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(WcgSchedule)]),
     "wcg_batch_set_shared_solve": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "wcg_batch_shared_launches": (ctypes.c_longlong, [ctypes.c_void_p]),
+    "wcg_batch_set_shared_solve_limit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "wcg_get_schedule": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(WcgSchedule)]),
     "wcg_save_positions": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
     "wcg_load_positions": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),

@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <climits>
 #include <string>
 #include <thread>
 #include <vector>
@@ -34,6 +35,7 @@ struct wcg_batch {
   std::vector<cudaEvent_t> ev;  // per scene: start, end of a timed step (created on first use)
   wcg::SharedSolve* ss = nullptr;  // the shared solve, when on
   long long ss_launches = 0;       // launches of shared solves turned off since
+  int ss_limit = INT_MAX;          // patches of the largest solve that joins
 };
 
 namespace {
@@ -166,6 +168,15 @@ int wcg_batch_set_shared_solve(wcg_batch* b, int on) {
   std::string err;
   b->ss = wcg::shared_solve_create(b->device[0], &err);
   if (!b->ss) return fail(WCG_ERR_CUDA, "shared solve: " + err);
+  wcg::shared_solve_set_limit(b->ss, b->ss_limit);
+  return WCG_OK;
+}
+
+int wcg_batch_set_shared_solve_limit(wcg_batch* b, int max_patches) {
+  if (!b) return fail(WCG_ERR_ARG, "null batch");
+  if (max_patches < 1) return fail(WCG_ERR_ARG, "max_patches must be >= 1");
+  b->ss_limit = max_patches;
+  wcg::shared_solve_set_limit(b->ss, max_patches);
   return WCG_OK;
 }
 

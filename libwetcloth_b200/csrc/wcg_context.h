@@ -399,6 +399,8 @@ cudaError_t read_small(Context& c, const void* d, size_t bytes, void* h);
 SharedSolve* shared_solve_create(int device, std::string* err);
 void shared_solve_destroy(SharedSolve* s);
 long long shared_solve_launches(const SharedSolve* s);
+// solves of more pencil patches than this iterate alone (default: no limit)
+void shared_solve_set_limit(SharedSolve* s, int max_patches);
 // positions in the reference's m_x layout (x, y, z, 0 per particle) and radii,
 // original order, host buffers
 cudaError_t download_positions(Context& c, double* x4, double* radius);

@@ -1513,6 +1513,7 @@ struct SolveReq {
 
 struct SharedSolve {
   int device = 0;
+  std::atomic<int> max_patches{INT_MAX};  // larger solves iterate alone
   cudaStream_t stream = nullptr;
   std::mutex m;
   std::condition_variable cv;       // the coordinator: requests or stop
@@ -1725,6 +1726,10 @@ void shared_solve_destroy(SharedSolve* S) {
 
 long long shared_solve_launches(const SharedSolve* S) { return S ? S->launches.load() : 0; }
 
+void shared_solve_set_limit(SharedSolve* S, int max_patches) {
+  if (S) S->max_patches = max_patches;
+}
+
 // PCGSolver<T>::solve (PCGSolver.h:260-308) in the pencil layout on the
 // factored system: A x = r from x = 0; r is overwritten with the residual.
 template <typename R>
@@ -1790,7 +1795,7 @@ static cudaError_t pl_pcg(Context& c, R* r, R* x, double tol_abs, int maxiters, 
   const int rows_blocks = pl_spmv_blocks(G);
   WCG_TRY(ensure_scratch(c, (size_t)std::max(spmv_blocks, rows_blocks) * sizeof(double)));
   part = c.scratch.as<double>();
-  if (c.shared_solve && c.spmv_rows) {
+  if (c.shared_solve && c.spmv_rows && G.npatch <= c.shared_solve->max_patches.load()) {
     // the iterations run in the batch's shared launches
     SolveReq req;
     req.c = &c;

@@ -417,9 +417,12 @@ class FluidBatch:
             check(rc)
         return list(st)
 
-    def set_shared_solve(self, on=True):
+    def set_shared_solve(self, on=True, max_patches=None):
         """Run the scenes' PCG iterations in shared launches over all scenes
-        waiting in their solve (results unchanged)."""
+        waiting in their solve (results unchanged); solves of more than
+        max_patches pencil patches iterate alone (None: no limit)."""
+        lim = 2**31 - 1 if max_patches is None else int(max_patches)
+        check(self.L.wcg_batch_set_shared_solve_limit(self.h, lim))
         check(self.L.wcg_batch_set_shared_solve(self.h, 1 if on else 0))
 
     @property

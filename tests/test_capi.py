@@ -81,6 +81,7 @@ def test_argument_errors_without_device():
     assert L.wcg_get_schedule(None, ctypes.byref(sched)) == _capi.WCG_ERR_ARG
     assert L.wcg_batch_set_shared_solve(None, 1) == _capi.WCG_ERR_ARG
     assert L.wcg_batch_shared_launches(None) == -1
+    assert L.wcg_batch_set_shared_solve_limit(None, 4) == _capi.WCG_ERR_ARG
     assert L.wcg_batch_autotune_schedules(None, None, None, 0, 1, None, None) == _capi.WCG_ERR_ARG
     b = ctypes.c_void_p()
     assert L.wcg_batch_create(0, None, ctypes.byref(b)) == _capi.WCG_ERR_ARG

@@ -136,15 +136,23 @@ def test_schedule_arguments(wcg):
     g.close()
 
 
-@pytest.mark.parametrize("mixed", [False, True])
-def test_shared_solve_matches_alone(mixed, wcg):
+@pytest.mark.parametrize("mixed,limit", [(False, None), (True, None), (False, 4)])
+def test_shared_solve_matches_alone(mixed, limit, wcg):
     """The shared solve (the PCG iterations of all scenes waiting in their
     pressure solve run as one launch per kernel) changes no result: every
     scene after three batch steps is bit-identical to three steps alone.
     Scenes of uneven size; FP32 + refinement, and a batch mixing FP64 and
     FP32 scenes (two shared launch sets); some scenes on cluster schedules,
-    whose sweeps outside the iterations keep them."""
-    specs = scenes.batch_scenes(6, 13, (24, 72), (5000, 150000))
+    whose sweeps outside the iterations keep them; and a patch limit under
+    which the larger scene iterates alone beside the shared launches."""
+    if limit is None:
+        specs = scenes.batch_scenes(6, 13, (24, 72), (5000, 150000))
+    else:
+        # the two 16^3 dam breaks solve on a 20 x 28 x 20-cell DOF box (2 x 2
+        # pencil patches) and share the launches; the 48^3 half box (3 x 4
+        # patches) iterates alone
+        specs = [scenes.dam_break(16, 8, 0), scenes.dam_break(16, 8, 1),
+                 scenes.half_box(48, 2, 5, amplitude=0.5, sigma_cells=2.0)]
     precs = [(_capi.WCG_FP64 if (mixed and k % 2) else _capi.WCG_FP32_REFINE)
              for k in range(len(specs))]
     alone = []
@@ -160,7 +168,7 @@ def test_shared_solve_matches_alone(mixed, wcg):
             g.schedule = (2, 1, 4)
     b = FluidBatch(gs)
     b.threads = 4
-    b.set_shared_solve(True)
+    b.set_shared_solve(True, max_patches=limit)
     st = b.step(DT, nsteps=3)
     assert all(s == _capi.WCG_OK for s in st), st
     assert b.shared_launches > 0
