@@ -100,7 +100,7 @@ def test_full_size_fp32_refine_against_fp64(full_scene, wcg):
     divided by dx theta, so FP32 rounding of the pressure is amplified up to
     100 times.  Every particle farther than one cell from a face with
     theta < 0.05 (99 % of them) agrees to 1e-5 of the largest velocity, the
-    north star's FP32 tolerance; every particle to 1e-3 (2.3e-4 measured);
+    FP32-with-refinement tolerance; every particle to 1e-3 (2.3e-4 measured);
     positions to 1e-6."""
     sc = full_scene
     out = {}
